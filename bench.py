@@ -1,0 +1,382 @@
+"""Benchmark of the Zynum B200 GEMM backend.
+
+Headline workload: DGEMM C = A B, M = N = K = 8192, column-major FP64,
+entries u * 10^e, u ~ U[-1, 1], e ~ U[-phi, phi] with phi = 0 (seeded,
+synthetic), alpha = 1, beta = 0.  Metric: effective DGEMM TFLOP/s
+(2 * 8192^3 flop per call) of the Ozaki-emulated DGEMM, with the native FP64
+DGEMM measured in the same run on the same inputs and both errors stated
+against a double-double oracle on sampled entries.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` times the device entry point with inputs resident in HBM (3 x 512 MiB,
+larger than the 126 MB L2, so no flush is needed).  `e2e` times the Fortran
+`dgemm_` entry point on pinned host buffers: host->device copies of A and B,
+the GEMM, and the device->host copy of C are inside the timed region.
+With --gpus N > 1 every rank runs an independent replica (GEMM does not shard
+without an exchange step; the product is single-GPU).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12  # 64 DFMA/clk/SM at the 1965 MHz max clock
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        d["_source"] = "measured"
+        return d
+    d = dict(PEAKS_FALLBACK)
+    d["_source"] = "fallback"
+    return d
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"zb_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ inputs
+def make_inputs(torch, n, phi, seed, device):
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+
+    def one():
+        u = torch.rand((n, n), generator=g, device=device, dtype=torch.float64) * 2 - 1
+        if phi:
+            e = torch.rand((n, n), generator=g, device=device, dtype=torch.float64) * 2 * phi - phi
+            u = u * torch.pow(10.0, e)
+        return u
+
+    return one(), one()
+
+
+def sampled_error(oracle, a_h, b_h, c_h, n, count=2048, seed=1):
+    """Max / median relative error of c against a double-double oracle at sampled (i, j)."""
+    rng = np.random.default_rng(seed)
+    rows = rng.integers(0, n, count)
+    cols = rng.integers(0, n, count)
+    hi, lo, ab = oracle.ddgemm_sampled("N", "N", n, a_h, n, b_h, n, rows, cols)
+    exact = hi + lo
+    got = c_h[rows, cols]
+    rel = np.abs(got - exact) / np.maximum(np.abs(exact), 1e-300)
+    rel_ab = np.abs(got - exact) / np.maximum(ab, 1e-300)
+    return {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+            "max_err_over_abs_ab": float(rel_ab.max()), "samples": int(count)}
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_gemm_lib():
+    import ctypes as C
+    from oracle import build as ob
+    ob.build()
+    L = C.CDLL(str(ROOT / "oracle" / "lib" / "libzynum_cpu.so"))
+    L.zynum_cpu_dgemm.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                                  C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int]
+    L.zynum_cpu_threads.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.zynum_cpu_threads.restype = C.c_int
+    return L
+
+
+def cpu_baseline(n, slab, min_seconds=10.0, max_reps=20):
+    """Restated Zynum CPU DGEMM on an n x slab x n slab of the headline problem."""
+    L = cpu_gemm_lib()
+    rng = np.random.default_rng(5)
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, slab)))
+    c = np.zeros((n, slab), order="F")
+    times = []
+    t_end = time.perf_counter() + min_seconds
+    while len(times) < max_reps and (len(times) < 2 or time.perf_counter() < t_end):
+        t0 = time.perf_counter()
+        L.zynum_cpu_dgemm(b"N", b"N", n, slab, n, 1.0, a.ctypes.data, n, b.ctypes.data, n, 0.0, c.ctypes.data, n)
+        times.append(time.perf_counter() - t0)
+    best = min(times)
+    return {"value": 2.0 * n * slab * n / best / 1e12, "unit": "TFLOP/s",
+            "cores": int(L.zynum_cpu_threads(n, slab, n)), "kind": "port",
+            "sample": f"DGEMM {n}x{slab}x{n} column slab of the {n}^3 problem, best of {len(times)}; "
+                      f"restated Zynum x86-64 packed-SIMD path (AVX-512 8x2x8 tile, planner column split)"}
+
+
+# --------------------------------------------------------------- reference
+def run_reference(args, rank, world):
+    metric, unit = "DGEMM TFLOP/s @8192^3 (effective 2n^3)", "TFLOP/s"
+    if rank != 0:
+        return 0
+    n = args.size
+    slab = max(256, n // 4)
+    L = cpu_gemm_lib()
+    rng = np.random.default_rng(5)
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, slab)))
+    c = np.zeros((n, slab), order="F")
+
+    def step():
+        L.zynum_cpu_dgemm(b"N", b"N", n, slab, n, 1.0, a.ctypes.data, n, b.ctypes.data, n, 0.0, c.ctypes.data, n)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 2.0 * n * slab * n / dt / 1e12
+    cores = int(L.zynum_cpu_threads(n, slab, n))
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic U[-1,1], seeded",
+            "config": {"workload": f"DGEMM M=N=K={n} column-major FP64, alpha=1, beta=0",
+                       "step_sample": f"{n}x{slab}x{n} column slab per step"},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
+                             "sample": f"{n}x{slab}x{n} slab per step; restated Zynum x86-64 packed-SIMD path "
+                                       "(reference is Zig 0.16, no zig toolchain in the image)"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def time_device(torch, fn, steps, warmup, stream):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / steps
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from zynum_b200 import blas
+    from zynum_b200._lib import load
+
+    L = load()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.size
+    flop = 2.0 * n ** 3
+    peaks = _peaks()
+    A, B = make_inputs(torch, n, args.phi, 1234 + rank, dev)  # column-major view: storage of A^T row-major
+    C = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def call(method):
+        blas.set_dgemm_method(method)
+        return lambda: blas.dgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+
+    methods = []
+    if args.method in ("ozaki", "both"):
+        methods.append(("ozaki", blas.METHOD_OZAKI))
+    if args.method in ("native", "both"):
+        methods.append(("native", blas.METHOD_NATIVE))
+
+    results = {}
+    with ClockSampler(local_rank) as clocks:
+        for name, mid in methods:
+            fn = call(mid)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            launches0 = L.zynum_blas_gpu_launch_count()
+            L.zynum_blas_gpu_profile(1)
+            ms = time_device(torch, fn, args.steps, args.warmup, stream)
+            # one event pair per call around the dominant kernel: keep the timed steps' records
+            buf = np.zeros(4096)
+            cnt = L.zynum_blas_gpu_profile_read(buf.ctypes.data, 4096)
+            L.zynum_blas_gpu_profile(0)
+            launches = (L.zynum_blas_gpu_launch_count() - launches0) // (args.steps + args.warmup)
+            kern_ms = float(np.mean(buf[cnt - args.steps:cnt])) if cnt >= args.steps else None
+            if world > 1:
+                t = torch.tensor([ms], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
+            results[name] = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12, "launches_per_step": int(launches),
+                             "kernel_ms": kern_ms}
+    clk = clocks.summary()
+
+    # errors of both methods vs the double-double oracle (rank 0, sampled entries)
+    err = {}
+    if rank == 0 and not args.no_error:
+        from oracle import oracle as orc
+        a_h = np.asfortranarray(A.cpu().numpy().T)
+        b_h = np.asfortranarray(B.cpu().numpy().T)
+        for name, mid in methods:
+            call(mid)()
+            torch.cuda.synchronize()
+            c_h = np.asfortranarray(C.cpu().numpy().T)
+            err[name] = sampled_error(orc, a_h, b_h, c_h, n)
+
+    # end-to-end through the Fortran ABI with pinned host buffers
+    head = methods[0]
+    blas.set_dgemm_method(head[1])
+    a_p = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    b_p = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    c_p = torch.zeros((n, n), dtype=torch.float64).pin_memory()
+    a_p.copy_(A)
+    b_p.copy_(B)
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def host_call():
+        blas.dgemm("N", "N", n, n, n, 1.0, a_p, n, b_p, n, 0.0, c_p, n)
+
+    host_call()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_call()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank != 0:
+        return 0
+    hr = results[head[0]]
+    value = world * hr["tflops"]
+    # roofline of the dominant kernel
+    if head[0] == "ozaki":
+        from zynum_b200 import ozaki_info
+        info = ozaki_info(n, n, n)
+        ops = info["slice_products"] * flop
+        int8_peak = 2.0 * peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"])
+        achieved = ops / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
+        roof = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (int8)",
+                "frac": (achieved / int8_peak) if achieved else None, "traffic": None,
+                "kernel": "ozaki int8 slice-product GEMM (tcgen05 kind::i8)",
+                "peak_source": f"2 x bf16_tflops of {peaks['_source']} peaks (int8 dense rate is 2x bf16 on sm_100)",
+                "work_per_launch": f"{info['slice_products']} slice products x 2*{n}^3 int8 ops"}
+    else:
+        achieved = flop / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
+        roof = {"bound": "tensor", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                "frac": (achieved / FP64_NOMINAL_TFLOPS) if achieved else None, "traffic": None,
+                "kernel": "native DGEMM (DMMA m16n8k8 f64)",
+                "peak_source": "nominal FP64 pipe: 148 SMs x 128 flop/clk x 1.965 GHz (no measured FP64 peak)"}
+    line = {
+        "metric": "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error",
+        "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": f"synthetic u*10^e, u~U[-1,1], e~U[-{args.phi},{args.phi}], seeded",
+        "config": {"workload": f"DGEMM M=N=K={n} NN column-major FP64 alpha=1 beta=0 ({head[0]})",
+                   "method": head[0], "l2": "inputs 3 x 512 MiB > 126 MB L2 (no flush needed)",
+                   "parallelism": "replicas" if world > 1 else "single-GPU"},
+        "methods": {k: {**v, **({"error": err[k]} if k in err else {})} for k, v in results.items()},
+        "roofline": roof,
+        "clocks": clk,
+        "gpu_launches": int(hr["launches_per_step"] * args.steps),
+        "e2e": {"value": world * flop / e2e_s / 1e12, "unit": "TFLOP/s", "ms_per_step": e2e_s * 1e3,
+                "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8,
+                "path": "dgemm_ Fortran ABI, pinned host buffers"},
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(n if n <= 8192 else 8192, 256)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--method", choices=["ozaki", "native", "both"], default="both")
+    ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--phi", type=float, default=0.0)
+    ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank, world)
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,112 @@
+/*
+ * zynum_blas_gpu.h — C ABI of the B200 GEMM backend for Zynum BLAS.
+ *
+ * The Fortran and CBLAS entry points have exactly the signatures, argument
+ * checks, error reports and quick returns of the reference library's exports,
+ * so a program linked against libzynum_blas can link against
+ * libzynum_blas_gpu.so instead.  Each declaration cites the reference export
+ * it replaces (paths inside the Zynum project).
+ *
+ * Host entry points take HOST pointers, stage them to the GPU, compute there
+ * and copy the result window back; padding rows [m, ldc) of C are never
+ * written.  The *_device entry points take DEVICE pointers and a CUDA stream
+ * (as `void *`, a cudaStream_t), enqueue the work and return a status:
+ *   0              success (work enqueued),
+ *   1 .. 13        index of the first illegal argument (same numbering as the
+ *                  Fortran routine; nothing was enqueued),
+ *   < 0            a CUDA error (negated cudaError_t); zynum_blas_gpu_last_error()
+ *                  gives the text.
+ */
+#ifndef ZYNUM_BLAS_GPU_H
+#define ZYNUM_BLAS_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ZYNUM_BLAS_GPU_API __attribute__((visibility("default")))
+#else
+#define ZYNUM_BLAS_GPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t zynum_blas_int; /* BlasInt = i32: src/blas/types.zig:4; include/zynum/blas/cblas.h:18 */
+
+/* ------------------------------------------------------------- Fortran ABI */
+
+/* src/blas/abi/fortran.zig:20 xerbla_ — prints
+ * " ** On entry to NAME parameter number N had an illegal value". */
+ZYNUM_BLAS_GPU_API void xerbla_(const char *srname, const zynum_blas_int *info);
+/* src/blas/abi/fortran.zig:16 lsame_ */
+ZYNUM_BLAS_GPU_API int lsame_(const char *ca, const char *cb);
+/* src/blas/abi/fortran.zig:41-47 zynum_blas_shutdown(_) — also frees every GPU buffer of the shim. */
+ZYNUM_BLAS_GPU_API void zynum_blas_shutdown(void);
+ZYNUM_BLAS_GPU_API void zynum_blas_shutdown_(void);
+
+/* src/blas/abi/fortran.zig:760 sgemm_ */
+ZYNUM_BLAS_GPU_API void sgemm_(const char *transa, const char *transb, const zynum_blas_int *m, const zynum_blas_int *n,
+            const zynum_blas_int *k, const float *alpha, const float *a, const zynum_blas_int *lda, const float *b,
+            const zynum_blas_int *ldb, const float *beta, float *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:764 dgemm_ */
+ZYNUM_BLAS_GPU_API void dgemm_(const char *transa, const char *transb, const zynum_blas_int *m, const zynum_blas_int *n,
+            const zynum_blas_int *k, const double *alpha, const double *a, const zynum_blas_int *lda,
+            const double *b, const zynum_blas_int *ldb, const double *beta, double *c, const zynum_blas_int *ldc);
+
+/* ---------------------------------------------------------------- CBLAS ABI */
+
+enum CBLAS_LAYOUT { CblasRowMajor = 101, CblasColMajor = 102 };          /* cblas.zig:123-124 */
+enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 }; /* :125-127 */
+enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };                  /* :128-129 */
+enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 };                 /* :130-131 */
+enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 };                   /* :132-133 */
+
+/* src/blas/abi/cblas.zig:1415 cblas_sgemm */
+ZYNUM_BLAS_GPU_API void cblas_sgemm(int layout, int transa, int transb, int m, int n, int k, float alpha, const float *a, int lda,
+                 const float *b, int ldb, float beta, float *c, int ldc);
+/* src/blas/abi/cblas.zig:1428 cblas_dgemm */
+ZYNUM_BLAS_GPU_API void cblas_dgemm(int layout, int transa, int transb, int m, int n, int k, double alpha, const double *a, int lda,
+                 const double *b, int ldb, double beta, double *c, int ldc);
+
+/* ------------------------------------------------------ GPU device entry points
+ * Added by the GPU backend (no counterpart in the reference's ABI; the planned
+ * addition is described for src/blas/abi/fortran.zig's dgemm_ path).  Same
+ * argument meaning as dgemm_/sgemm_, passed by value, device pointers. */
+
+/* Native FP64 (DMMA tensor pipe) or Ozaki-emulated DGEMM, chosen by
+ * zynum_blas_gpu_set_dgemm_method / ZYNUM_GPU_DGEMM_METHOD (default native). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_device(char transa, char transb, int m, int n, int k, double alpha, const double *a,
+                                int lda, const double *b, int ldb, double beta, double *c, int ldc, void *stream);
+/* Native FP32 (FFMA) or 3xBF16 SGEMM, chosen by zynum_blas_gpu_set_sgemm_method. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_sgemm_device(char transa, char transb, int m, int n, int k, float alpha, const float *a, int lda,
+                                const float *b, int ldb, float beta, float *c, int ldc, void *stream);
+
+/* -------------------------------------------------------------- control */
+/* 0 = native FP64, 1 = Ozaki INT8 emulation, 2 = automatic. Returns the previous value. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);
+/* 0 = native FP32, 1 = 3xBF16 split product. Returns the previous value. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_sgemm_method(int method);
+/* Ozaki slice count (2..12), 0 = automatic. Returns the previous value. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_slices(int slices);
+/* Text of the last error seen by this thread ("" if none). */
+ZYNUM_BLAS_GPU_API const char *zynum_blas_gpu_last_error(void);
+/* Host-side fault injection for tests: the next `count` device-memory
+ * reservations fail (kind 1), or the next stream synchronisation reports
+ * CUDA error `count` (kind 2).  Never touches the GPU. */
+ZYNUM_BLAS_GPU_API void zynum_blas_gpu_inject_fault(int kind, int count);
+/* Dominant-kernel timing: enable != 0 starts recording CUDA events around the
+ * main contraction kernel of every call (on the launching stream) and clears
+ * earlier records; returns the previous state. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_profile(int enable);
+/* Writes up to `max` recorded kernel durations (milliseconds, in launch order)
+ * to `ms`, waiting for them to complete; returns the count, or -1. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_profile_read(double *ms, int max);
+/* Number of kernels this library has launched in this process so far. */
+ZYNUM_BLAS_GPU_API long long zynum_blas_gpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZYNUM_BLAS_GPU_H */

@@ -1,0 +1,110 @@
+"""numpy front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker or the timed CPU reference.  The product
+(zynum_b200) never imports it.
+
+All matrices are numpy arrays in Fortran (column-major) order with an explicit
+leading dimension: a matrix with ld rows of storage and `cols` columns is an
+array of shape (ld, cols), order='F'.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        path = _HERE / "lib" / "liboracle.so"
+        if not path.exists():
+            from oracle import build as _b  # noqa: WPS433
+            _b.build()
+        _LIB = C.CDLL(str(path))
+        _declare(_LIB)
+    return _LIB
+
+
+def _declare(L):
+    i32, f64, f32, ch = C.c_int32, C.c_double, C.c_float, C.c_char
+    vp = C.c_void_p
+    L.oracle_dgemm.argtypes = [ch, ch, i32, i32, i32, f64, vp, i32, vp, i32, f64, vp, i32]
+    L.oracle_sgemm.argtypes = [ch, ch, i32, i32, i32, f32, vp, i32, vp, i32, f32, vp, i32]
+    L.oracle_zgemm.argtypes = [ch, ch, i32, i32, i32, vp, vp, i32, vp, i32, vp, vp, i32]
+    L.oracle_cgemm.argtypes = [ch, ch, i32, i32, i32, vp, vp, i32, vp, i32, vp, vp, i32]
+    L.oracle_ddgemm.argtypes = [ch, ch, i32, i32, i32, vp, i32, vp, i32, vp, vp, i32]
+    L.oracle_ddgemm_sampled.argtypes = [ch, ch, i32, vp, i32, vp, i32, C.c_int64, vp, vp, vp, vp, vp]
+    L.oracle_ddgemm_sampled_f32.argtypes = [ch, ch, i32, vp, i32, vp, i32, C.c_int64, vp, vp, vp, vp, vp]
+    L.oracle_dtrsm.argtypes = [ch, ch, ch, ch, i32, i32, f64, vp, i32, vp, i32]
+    L.oracle_strsm.argtypes = [ch, ch, ch, ch, i32, i32, f32, vp, i32, vp, i32]
+    L.oracle_dsyrk.argtypes = [ch, ch, i32, i32, f64, vp, i32, f64, vp, i32]
+    L.oracle_ssyrk.argtypes = [ch, ch, i32, i32, f32, vp, i32, f32, vp, i32]
+
+
+def _p(a: np.ndarray):
+    assert a.flags.f_contiguous or a.ndim == 1
+    return a.ctypes.data
+
+
+def _b(c: str) -> bytes:
+    return c.encode()[:1]
+
+
+def gemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """In-place C update, dtype picked from `c` (f64, f32, c128, c64)."""
+    L = lib()
+    if c.dtype == np.float64:
+        L.oracle_dgemm(_b(ta), _b(tb), m, n, k, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
+    elif c.dtype == np.float32:
+        L.oracle_sgemm(_b(ta), _b(tb), m, n, k, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
+    elif c.dtype == np.complex128:
+        al = np.array([complex(alpha)], np.complex128)
+        be = np.array([complex(beta)], np.complex128)
+        L.oracle_zgemm(_b(ta), _b(tb), m, n, k, _p(al), _p(a), lda, _p(b), ldb, _p(be), _p(c), ldc)
+    elif c.dtype == np.complex64:
+        al = np.array([complex(alpha)], np.complex64)
+        be = np.array([complex(beta)], np.complex64)
+        L.oracle_cgemm(_b(ta), _b(tb), m, n, k, _p(al), _p(a), lda, _p(b), ldb, _p(be), _p(c), ldc)
+    else:
+        raise TypeError(c.dtype)
+    return c
+
+
+def ddgemm(ta, tb, m, n, k, a, lda, b, ldb):
+    """Double-double op(A) op(B): returns (hi, lo) m x n arrays."""
+    hi = np.zeros((m, n), np.float64, order="F")
+    lo = np.zeros((m, n), np.float64, order="F")
+    lib().oracle_ddgemm(_b(ta), _b(tb), m, n, k, _p(a), lda, _p(b), ldb, _p(hi), _p(lo), m)
+    return hi, lo
+
+
+def ddgemm_sampled(ta, tb, k, a, lda, b, ldb, rows, cols):
+    """Double-double entries (hi, lo, sum|a||b|) of op(A) op(B) at (rows[q], cols[q])."""
+    rows = np.ascontiguousarray(rows, np.int64)
+    cols = np.ascontiguousarray(cols, np.int64)
+    n = rows.size
+    hi, lo, ab = (np.zeros(n, np.float64) for _ in range(3))
+    fn = lib().oracle_ddgemm_sampled if a.dtype == np.float64 else lib().oracle_ddgemm_sampled_f32
+    fn(_b(ta), _b(tb), k, _p(a), lda, _p(b), ldb, n, rows.ctypes.data, cols.ctypes.data,
+       hi.ctypes.data, lo.ctypes.data, ab.ctypes.data)
+    return hi, lo, ab
+
+
+def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    L = lib()
+    f = L.oracle_dtrsm if b.dtype == np.float64 else L.oracle_strsm
+    f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha, _p(a), lda, _p(b), ldb)
+    return b
+
+
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    L = lib()
+    f = L.oracle_dsyrk if c.dtype == np.float64 else L.oracle_ssyrk
+    f(_b(uplo), _b(trans), n, k, alpha, _p(a), lda, beta, _p(c), ldc)
+    return c

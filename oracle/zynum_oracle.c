@@ -1,0 +1,316 @@
+/*
+ * CPU oracle for the Zynum GEMM / TRSM / SYRK path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker: the tests, the smoke
+ * check and the CPU-baseline leg of bench.py may call it; the product library
+ * (zynum_b200/lib/libzynum_blas_gpu.so) never links or calls it.
+ *
+ * Every routine restates the reference's scalar semantics in plain C
+ * (compiled with -ffp-contract=off so that `a*b + c` rounds twice, exactly as
+ * Zig's default float mode does):
+ *
+ *   oracle_?gemm   gemm.zig:1392-1430 (quick returns :1407-1414, portable
+ *                  triple loop :1422-1429) and gemmComplexPortable :1234-1246,
+ *                  with matrixValue (matrix_vector/access.zig:23-29) for N/T/C.
+ *   oracle_?trsm   triangular.zig:233-249 (alpha pre-scale :51-58, then one
+ *                  trsv per right-hand side, matrix_vector/triangular.zig
+ *                  :400-435, triValue access.zig:54-64) and the right-side
+ *                  row solve solveRightRow triangular.zig:72-88.
+ *   oracle_?syrk   symmetric.zig:180-199 (runSyrkColumns).
+ *   oracle_ddgemm  a double-double (error-free TwoProd/TwoSum, Dekker 1971 /
+ *                  Knuth) accumulation of op(A)op(B); used to state the error
+ *                  of every GPU result.  No counterpart in the reference.
+ *
+ * Complex numbers are interleaved (re, im) pairs, column-major, exactly like
+ * the reference's ComplexF32/ComplexF64 extern structs (types.zig).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string.h>
+
+typedef int32_t blas_int;
+
+static inline size_t ix(blas_int ld, size_t row, size_t col) { return row + col * (size_t)ld; }
+
+static inline int upc(char c) { return (c >= 'a' && c <= 'z') ? c - 32 : c; }
+
+/* ---------------------------------------------------------------- real GEMM */
+
+#define DEFINE_REAL_GEMM(NAME, T)                                                              \
+    void NAME(char ta, char tb, blas_int m, blas_int n, blas_int k, T alpha, const T *a,      \
+              blas_int lda, const T *b, blas_int ldb, T beta, T *c, blas_int ldc) {            \
+        ta = (char)upc(ta);                                                                    \
+        tb = (char)upc(tb);                                                                    \
+        if (m <= 0 || n <= 0) return;                                                          \
+        if (k <= 0 || alpha == (T)0) {                                                         \
+            for (size_t j = 0; j < (size_t)n; ++j)                                             \
+                for (size_t i = 0; i < (size_t)m; ++i) {                                       \
+                    size_t q = ix(ldc, i, j);                                                  \
+                    c[q] = (beta == (T)0) ? (T)0 : beta * c[q];                                \
+                }                                                                              \
+            return;                                                                            \
+        }                                                                                      \
+        for (size_t j = 0; j < (size_t)n; ++j)                                                 \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                           \
+                T sum = 0;                                                                     \
+                for (size_t p = 0; p < (size_t)k; ++p) {                                       \
+                    T av = (ta == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];                  \
+                    T bv = (tb == 'N') ? b[ix(ldb, p, j)] : b[ix(ldb, j, p)];                  \
+                    sum = sum + av * bv;                                                       \
+                }                                                                              \
+                size_t q = ix(ldc, i, j);                                                      \
+                c[q] = alpha * sum + ((beta == (T)0) ? (T)0 : beta * c[q]);                    \
+            }                                                                                  \
+    }
+
+DEFINE_REAL_GEMM(oracle_dgemm, double)
+DEFINE_REAL_GEMM(oracle_sgemm, float)
+
+/* ------------------------------------------------------------- complex GEMM */
+
+#define DEFINE_COMPLEX_GEMM(NAME, T)                                                              \
+    void NAME(char ta, char tb, blas_int m, blas_int n, blas_int k, const T *alpha, const T *a,  \
+              blas_int lda, const T *b, blas_int ldb, const T *beta, T *c, blas_int ldc) {        \
+        ta = (char)upc(ta);                                                                       \
+        tb = (char)upc(tb);                                                                       \
+        if (m <= 0 || n <= 0) return;                                                             \
+        const T ar = alpha[0], ai = alpha[1], br = beta[0], bi = beta[1];                         \
+        const int beta_zero = (br == (T)0 && bi == (T)0);                                         \
+        if (k <= 0 || (ar == (T)0 && ai == (T)0)) {                                               \
+            for (size_t j = 0; j < (size_t)n; ++j)                                                \
+                for (size_t i = 0; i < (size_t)m; ++i) {                                          \
+                    T *cv = c + 2 * ix(ldc, i, j);                                                \
+                    if (beta_zero) {                                                              \
+                        cv[0] = 0;                                                                \
+                        cv[1] = 0;                                                                \
+                    } else {                                                                      \
+                        T r = br * cv[0] - bi * cv[1], s = br * cv[1] + bi * cv[0];               \
+                        cv[0] = r;                                                                \
+                        cv[1] = s;                                                                \
+                    }                                                                             \
+                }                                                                                 \
+            return;                                                                               \
+        }                                                                                         \
+        for (size_t j = 0; j < (size_t)n; ++j)                                                    \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                              \
+                T sr = 0, si = 0;                                                                 \
+                for (size_t p = 0; p < (size_t)k; ++p) {                                          \
+                    const T *av = a + 2 * ((ta == 'N') ? ix(lda, i, p) : ix(lda, p, i));          \
+                    const T *bv = b + 2 * ((tb == 'N') ? ix(ldb, p, j) : ix(ldb, j, p));          \
+                    T xr = av[0], xi = (ta == 'C') ? -av[1] : av[1];                              \
+                    T yr = bv[0], yi = (tb == 'C') ? -bv[1] : bv[1];                              \
+                    T pr = xr * yr - xi * yi, pi = xr * yi + xi * yr;                             \
+                    sr = sr + pr;                                                                 \
+                    si = si + pi;                                                                 \
+                }                                                                                 \
+                T *cv = c + 2 * ix(ldc, i, j);                                                    \
+                T tr = ar * sr - ai * si, ti = ar * si + ai * sr;                                 \
+                T ur = 0, ui = 0;                                                                 \
+                if (!beta_zero) {                                                                 \
+                    ur = br * cv[0] - bi * cv[1];                                                 \
+                    ui = br * cv[1] + bi * cv[0];                                                 \
+                }                                                                                 \
+                cv[0] = tr + ur;                                                                  \
+                cv[1] = ti + ui;                                                                  \
+            }                                                                                     \
+    }
+
+DEFINE_COMPLEX_GEMM(oracle_zgemm, double)
+DEFINE_COMPLEX_GEMM(oracle_cgemm, float)
+
+/* ------------------------------------------------- double-double reference */
+
+/* TwoSum (Knuth) and TwoProd (via FMA): error-free transformations. */
+static inline void two_sum(double a, double b, double *s, double *e) {
+    double x = a + b;
+    double z = x - a;
+    *e = (a - (x - z)) + (b - z);
+    *s = x;
+}
+static inline void two_prod(double a, double b, double *p, double *e) {
+    double x = a * b;
+    *e = fma(a, b, -x);
+    *p = x;
+}
+/* (hi, lo) += (p, q) with the usual double-double add (Bailey's QD "sloppy"
+ * add is not enough under heavy cancellation, so both halves are renormalised). */
+static inline void dd_add(double *hi, double *lo, double p, double q) {
+    double s, e, t, f;
+    two_sum(*hi, p, &s, &e);
+    two_sum(*lo, q, &t, &f);
+    e += t;
+    double u, v;
+    two_sum(s, e, &u, &v);
+    v += f;
+    two_sum(u, v, hi, lo);
+}
+
+/* C_hi + C_lo = op(A) op(B) in double-double (alpha = 1, beta = 0).  The
+ * caller forms alpha/beta itself in extended precision when it needs them. */
+void oracle_ddgemm(char ta, char tb, blas_int m, blas_int n, blas_int k, const double *a, blas_int lda,
+                   const double *b, blas_int ldb, double *c_hi, double *c_lo, blas_int ldc) {
+    ta = (char)upc(ta);
+    tb = (char)upc(tb);
+    for (size_t j = 0; j < (size_t)n; ++j)
+        for (size_t i = 0; i < (size_t)m; ++i) {
+            double hi = 0, lo = 0;
+            for (size_t p = 0; p < (size_t)k; ++p) {
+                double av = (ta == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];
+                double bv = (tb == 'N') ? b[ix(ldb, p, j)] : b[ix(ldb, j, p)];
+                double pp, pe;
+                two_prod(av, bv, &pp, &pe);
+                dd_add(&hi, &lo, pp, pe);
+            }
+            c_hi[ix(ldc, i, j)] = hi;
+            c_lo[ix(ldc, i, j)] = lo;
+        }
+}
+
+/* Sampled double-double entries: out_hi[q] + out_lo[q] = (op(A) op(B))[rows[q], cols[q]]. */
+void oracle_ddgemm_sampled(char ta, char tb, blas_int k, const double *a, blas_int lda, const double *b,
+                           blas_int ldb, int64_t count, const int64_t *rows, const int64_t *cols,
+                           double *out_hi, double *out_lo, double *out_abs) {
+    ta = (char)upc(ta);
+    tb = (char)upc(tb);
+    for (int64_t q = 0; q < count; ++q) {
+        size_t i = (size_t)rows[q], j = (size_t)cols[q];
+        double hi = 0, lo = 0, absum = 0;
+        for (size_t p = 0; p < (size_t)k; ++p) {
+            double av = (ta == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];
+            double bv = (tb == 'N') ? b[ix(ldb, p, j)] : b[ix(ldb, j, p)];
+            double pp, pe;
+            two_prod(av, bv, &pp, &pe);
+            dd_add(&hi, &lo, pp, pe);
+            absum += fabs(av * bv);
+        }
+        out_hi[q] = hi;
+        out_lo[q] = lo;
+        if (out_abs) out_abs[q] = absum;
+    }
+}
+
+/* Sampled float-input double-double reference for SGEMM error statements. */
+void oracle_ddgemm_sampled_f32(char ta, char tb, blas_int k, const float *a, blas_int lda, const float *b,
+                               blas_int ldb, int64_t count, const int64_t *rows, const int64_t *cols,
+                               double *out_hi, double *out_lo, double *out_abs) {
+    ta = (char)upc(ta);
+    tb = (char)upc(tb);
+    for (int64_t q = 0; q < count; ++q) {
+        size_t i = (size_t)rows[q], j = (size_t)cols[q];
+        double hi = 0, lo = 0, absum = 0;
+        for (size_t p = 0; p < (size_t)k; ++p) {
+            double av = (ta == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];
+            double bv = (tb == 'N') ? b[ix(ldb, p, j)] : b[ix(ldb, j, p)];
+            double pp, pe;
+            two_prod(av, bv, &pp, &pe);
+            dd_add(&hi, &lo, pp, pe);
+            absum += fabs(av * bv);
+        }
+        out_hi[q] = hi;
+        out_lo[q] = lo;
+        if (out_abs) out_abs[q] = absum;
+    }
+}
+
+/* ---------------------------------------------------------------- real TRSM */
+
+/* triValue (access.zig:54-64): element (row, col) of op(A) for a triangular A. */
+#define DEFINE_TRI_VALUE(NAME, T)                                                                   \
+    static inline T NAME(char uplo, char diag, char trans, const T *a, blas_int lda, size_t row,    \
+                         size_t col) {                                                              \
+        size_t ar = (trans == 'N') ? row : col, ac = (trans == 'N') ? col : row;                    \
+        if (ar == ac && diag == 'U') return (T)1;                                                   \
+        if (uplo == 'U' && ar > ac) return (T)0;                                                    \
+        if (uplo == 'L' && ar < ac) return (T)0;                                                    \
+        return a[ix(lda, ar, ac)];                                                                  \
+    }
+DEFINE_TRI_VALUE(tri_d, double)
+DEFINE_TRI_VALUE(tri_s, float)
+
+/* op(A) is upper triangular (triangular.zig:47-49 opIsUpper). */
+static inline int op_is_upper(char uplo, char trans) {
+    return (trans == 'N' && uplo == 'U') || (trans != 'N' && uplo == 'L');
+}
+
+#define DEFINE_REAL_TRSM(NAME, T, TRI)                                                                 \
+    void NAME(char side, char uplo, char trans, char diag, blas_int m, blas_int n, T alpha,          \
+              const T *a, blas_int lda, T *b, blas_int ldb) {                                          \
+        side = (char)upc(side); uplo = (char)upc(uplo); trans = (char)upc(trans); diag = (char)upc(diag); \
+        if (m <= 0 || n <= 0) return;                                                                  \
+        if (alpha != (T)1)                                                                             \
+            for (size_t j = 0; j < (size_t)n; ++j)                                                     \
+                for (size_t i = 0; i < (size_t)m; ++i) b[ix(ldb, i, j)] = alpha * b[ix(ldb, i, j)];    \
+        if (side == 'L') {                                                                             \
+            for (size_t j = 0; j < (size_t)n; ++j) {                                                   \
+                T *x = b + (size_t)ldb * j;                                                            \
+                if (op_is_upper(uplo, trans)) {                                                        \
+                    for (size_t r = (size_t)m; r-- > 0;) {                                             \
+                        T t = x[r];                                                                    \
+                        for (size_t q = r + 1; q < (size_t)m; ++q) t = t - TRI(uplo, diag, trans, a, lda, r, q) * x[q]; \
+                        if (diag == 'N') t = t / TRI(uplo, diag, trans, a, lda, r, r);                 \
+                        x[r] = t;                                                                      \
+                    }                                                                                  \
+                } else {                                                                               \
+                    for (size_t r = 0; r < (size_t)m; ++r) {                                           \
+                        T t = x[r];                                                                    \
+                        for (size_t q = 0; q < r; ++q) t = t - TRI(uplo, diag, trans, a, lda, r, q) * x[q]; \
+                        if (diag == 'N') t = t / TRI(uplo, diag, trans, a, lda, r, r);                 \
+                        x[r] = t;                                                                      \
+                    }                                                                                  \
+                }                                                                                      \
+            }                                                                                          \
+        } else {                                                                                       \
+            /* X op(A) = B, row by row: x^T = solve(op(A)^T, b^T). */                                  \
+            char tt = (trans == 'N') ? 'T' : 'N';                                                      \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                   \
+                if (op_is_upper(uplo, tt)) {                                                           \
+                    for (size_t r = (size_t)n; r-- > 0;) {                                             \
+                        T t = b[ix(ldb, i, r)];                                                        \
+                        for (size_t q = r + 1; q < (size_t)n; ++q)                                     \
+                            t = t - TRI(uplo, diag, tt, a, lda, r, q) * b[ix(ldb, i, q)];              \
+                        if (diag == 'N') t = t / TRI(uplo, diag, tt, a, lda, r, r);                    \
+                        b[ix(ldb, i, r)] = t;                                                          \
+                    }                                                                                  \
+                } else {                                                                               \
+                    for (size_t r = 0; r < (size_t)n; ++r) {                                           \
+                        T t = b[ix(ldb, i, r)];                                                        \
+                        for (size_t q = 0; q < r; ++q) t = t - TRI(uplo, diag, tt, a, lda, r, q) * b[ix(ldb, i, q)]; \
+                        if (diag == 'N') t = t / TRI(uplo, diag, tt, a, lda, r, r);                    \
+                        b[ix(ldb, i, r)] = t;                                                          \
+                    }                                                                                  \
+                }                                                                                      \
+            }                                                                                          \
+        }                                                                                              \
+    }
+
+DEFINE_REAL_TRSM(oracle_dtrsm, double, tri_d)
+DEFINE_REAL_TRSM(oracle_strsm, float, tri_s)
+
+/* ---------------------------------------------------------------- real SYRK */
+
+#define DEFINE_REAL_SYRK(NAME, T)                                                                  \
+    void NAME(char uplo, char trans, blas_int n, blas_int k, T alpha, const T *a, blas_int lda,   \
+              T beta, T *c, blas_int ldc) {                                                        \
+        uplo = (char)upc(uplo); trans = (char)upc(trans);                                          \
+        if (n <= 0) return;                                                                        \
+        for (size_t j = 0; j < (size_t)n; ++j) {                                                   \
+            size_t r0 = (uplo == 'U') ? 0 : j, r1 = (uplo == 'U') ? j + 1 : (size_t)n;             \
+            for (size_t i = r0; i < r1; ++i) {                                                     \
+                T sum = 0;                                                                         \
+                for (size_t p = 0; p < (size_t)(k > 0 ? k : 0); ++p) {                              \
+                    T ai = (trans == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];                   \
+                    T aj = (trans == 'N') ? a[ix(lda, j, p)] : a[ix(lda, p, j)];                   \
+                    sum = sum + ai * aj;                                                           \
+                }                                                                                  \
+                size_t q = ix(ldc, i, j);                                                          \
+                c[q] = alpha * sum + ((beta == (T)0) ? (T)0 : beta * c[q]);                        \
+            }                                                                                      \
+        }                                                                                          \
+    }
+
+DEFINE_REAL_SYRK(oracle_dsyrk, double)
+DEFINE_REAL_SYRK(oracle_ssyrk, float)
+
+/* Library self-identification for the loader in the tests. */
+int oracle_version(void) { return 1; }

@@ -1,0 +1,75 @@
+"""ctypes loader for libzynum_blas_gpu.so (the C ABI of the GPU backend).
+
+The product path has no fallback: if the shared library is missing or does
+not load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libzynum_blas_gpu.so"
+_lib = None
+
+
+class ZynumGpuError(RuntimeError):
+    """A GPU entry point returned a non-zero status."""
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m zynum_b200.build` "
+            "(the GPU backend has no CPU fallback)")
+    L = C.CDLL(str(LIB_PATH))
+    _declare(L)
+    _lib = L
+    return L
+
+
+P = C.c_void_p
+I32P = C.POINTER(C.c_int32)
+
+
+def _declare(L: C.CDLL) -> None:
+    ch, i, d, f = C.c_char, C.c_int, C.c_double, C.c_float
+    cp = C.c_char_p
+    L.xerbla_.argtypes = [cp, I32P]
+    L.lsame_.argtypes = [cp, cp]
+    L.lsame_.restype = i
+    L.zynum_blas_shutdown.argtypes = []
+    # Fortran GEMM: everything by pointer
+    for name in ("sgemm_", "dgemm_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    L.cblas_dgemm.argtypes = [i, i, i, i, i, i, d, P, i, P, i, d, P, i]
+    L.cblas_sgemm.argtypes = [i, i, i, i, i, i, f, P, i, P, i, f, P, i]
+    L.zynum_blas_gpu_dgemm_device.argtypes = [ch, ch, i, i, i, d, P, i, P, i, d, P, i, P]
+    L.zynum_blas_gpu_dgemm_device.restype = i
+    L.zynum_blas_gpu_sgemm_device.argtypes = [ch, ch, i, i, i, f, P, i, P, i, f, P, i, P]
+    L.zynum_blas_gpu_sgemm_device.restype = i
+    for name in ("zynum_blas_gpu_set_dgemm_method", "zynum_blas_gpu_set_sgemm_method",
+                 "zynum_blas_gpu_set_ozaki_slices"):
+        getattr(L, name).argtypes = [i]
+        getattr(L, name).restype = i
+    L.zynum_blas_gpu_last_error.argtypes = []
+    L.zynum_blas_gpu_last_error.restype = cp
+    L.zynum_blas_gpu_inject_fault.argtypes = [i, i]
+    L.zynum_blas_gpu_inject_fault.restype = None
+    L.zynum_blas_gpu_profile.argtypes = [i]
+    L.zynum_blas_gpu_profile.restype = i
+    L.zynum_blas_gpu_profile_read.argtypes = [P, i]
+    L.zynum_blas_gpu_profile_read.restype = i
+    L.zynum_blas_gpu_launch_count.argtypes = []
+    L.zynum_blas_gpu_launch_count.restype = C.c_longlong
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        msg = load().zynum_blas_gpu_last_error().decode(errors="replace")
+        if status > 0:
+            raise ValueError(f"{what}: parameter number {status} had an illegal value")
+        raise ZynumGpuError(f"{what} failed with status {status}: {msg}")

@@ -1,0 +1,117 @@
+"""Python mirror of the Zynum BLAS GEMM-path interface over the C ABI.
+
+Host functions (`dgemm`, `sgemm`, `cblas_dgemm`, ...) take numpy arrays in
+column-major storage exactly like the Fortran routines take pointers: a matrix
+with leading dimension `ld` is an array of shape (ld, cols), order='F'.  They
+call the library's `dgemm_` / `cblas_dgemm` symbols, so they behave exactly
+like a C or Fortran caller: xerbla_ on an illegal argument, C untouched.
+
+Device functions (`dgemm_device`, ...) take CUDA torch tensors (column-major
+views, i.e. tensors whose stride is (1, ld)) and run on the current torch
+stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, load
+
+CblasRowMajor, CblasColMajor = 101, 102
+CblasNoTrans, CblasTrans, CblasConjTrans = 111, 112, 113
+CblasUpper, CblasLower = 121, 122
+CblasNonUnit, CblasUnit = 131, 132
+CblasLeft, CblasRight = 141, 142
+
+METHOD_NATIVE, METHOD_OZAKI, METHOD_AUTO = 0, 1, 2
+SMETHOD_NATIVE, SMETHOD_BF16X3 = 0, 1
+
+
+def _i(v: int):
+    return C.byref(C.c_int32(int(v)))
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor
+
+
+def _ch(c: str) -> bytes:
+    return c.encode()[:1]
+
+
+def dgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran dgemm_ on host arrays (in-place on c)."""
+    al, be = np.array([alpha], np.float64), np.array([beta], np.float64)
+    load().dgemm_(_ch(transa), _ch(transb), _i(m), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+                  _i(ldb), be.ctypes.data, _ptr(c), _i(ldc))
+    return c
+
+
+def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    al, be = np.array([alpha], np.float32), np.array([beta], np.float32)
+    load().sgemm_(_ch(transa), _ch(transb), _i(m), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+                  _i(ldb), be.ctypes.data, _ptr(c), _i(ldc))
+    return c
+
+
+def cblas_dgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    load().cblas_dgemm(layout, transa, transb, m, n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta),
+                       _ptr(c), ldc)
+    return c
+
+
+def cblas_sgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    load().cblas_sgemm(layout, transa, transb, m, n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta),
+                       _ptr(c), ldc)
+    return c
+
+
+def _stream(stream=None) -> int:
+    if stream is not None:
+        return int(stream)
+    import torch
+    return int(torch.cuda.current_stream().cuda_stream)
+
+
+def dgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    """Device dgemm on torch CUDA tensors / raw device pointers; raises on a non-zero status."""
+    st = load().zynum_blas_gpu_dgemm_device(_ch(transa), _ch(transb), m, n, k, float(alpha), _ptr(a), lda,
+                                            _ptr(b), ldb, float(beta), _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_dgemm_device")
+    return c
+
+
+def sgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    st = load().zynum_blas_gpu_sgemm_device(_ch(transa), _ch(transb), m, n, k, float(alpha), _ptr(a), lda,
+                                            _ptr(b), ldb, float(beta), _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_sgemm_device")
+    return c
+
+
+def set_dgemm_method(method: int) -> int:
+    return load().zynum_blas_gpu_set_dgemm_method(method)
+
+
+def set_sgemm_method(method: int) -> int:
+    return load().zynum_blas_gpu_set_sgemm_method(method)
+
+
+def set_ozaki_slices(slices: int) -> int:
+    return load().zynum_blas_gpu_set_ozaki_slices(slices)
+
+
+def inject_fault(kind: int, count: int) -> None:
+    load().zynum_blas_gpu_inject_fault(kind, count)
+
+
+def last_error() -> str:
+    return load().zynum_blas_gpu_last_error().decode(errors="replace")
+
+
+def shutdown() -> None:
+    load().zynum_blas_shutdown()

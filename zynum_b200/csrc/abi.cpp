@@ -1,0 +1,340 @@
+// Fortran / CBLAS ABI of the GPU backend and the device-pointer entry points.
+//
+// Mirrors, symbol for symbol, the reference's exports in
+// src/blas/abi/fortran.zig and src/blas/abi/cblas.zig:
+//   * argument validation and parameter numbering of gemmError (fortran.zig:88-102),
+//   * xerbla_ reporting (fortran.zig:20, :277) with C left untouched,
+//   * CBLAS enum validation with silent return and the row-major -> column-major
+//     swap (cblas.zig:1415-1465),
+//   * quick returns: m <= 0 or n <= 0 does nothing; k == 0 or alpha == 0 gives
+//     C = beta * C with beta == 0 writing exact zeros (gemm.zig:1392-1414).
+// The compute always runs on the GPU; there is no CPU fallback.
+#include <cctype>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/zynum_blas_gpu.h"
+#include "kernels.h"
+#include "ozaki.h"
+#include "runtime.h"
+
+using namespace zb;
+
+namespace {
+
+inline char up(const char* p) { return (char)std::toupper((unsigned char)p[0]); }
+inline bool valid_trans(char c) { return c == 'N' || c == 'T' || c == 'C'; }
+inline int max1(int x) { return x > 1 ? x : 1; }
+
+// fortran.zig:88-102 gemmError
+int gemm_error(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc) {
+    if (!valid_trans(ta)) return 1;
+    if (!valid_trans(tb)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    if (k < 0) return 5;
+    const int nrowa = (ta == 'N') ? m : k;
+    const int nrowb = (tb == 'N') ? k : n;
+    if (lda < max1(nrowa)) return 8;
+    if (ldb < max1(nrowb)) return 10;
+    if (ldc < max1(m)) return 13;
+    return 0;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return -(int)e;
+}
+
+void report_gpu_failure(const char* routine) {
+    std::fprintf(stderr, " ** zynum_blas_gpu: %s did not run on the GPU (%s); C is unchanged\n", routine,
+                 last_error());
+}
+
+// Scratch providers: the host ABI uses the context's own buffer on its stream;
+// the device entry points use a per-caller-stream buffer.
+struct HostScratch {
+    Context* cx;
+    cudaError_t operator()(size_t bytes, cudaStream_t st, void** out) {
+        cudaError_t e = cx->reserve(cx->work, bytes, st);
+        *out = cx->work.ptr;
+        return e;
+    }
+};
+struct StreamScratch {
+    Context* cx;
+    cudaError_t operator()(size_t bytes, cudaStream_t st, void** out) { return cx->stream_scratch(st, bytes, out); }
+};
+
+template <typename T>
+cudaError_t scale_matrix(int m, int n, T beta, T* c, long ldc, cudaStream_t st);
+template <>
+cudaError_t scale_matrix<double>(int m, int n, double beta, double* c, long ldc, cudaStream_t st) {
+    return scale_matrix_f64(m, n, beta, c, ldc, st);
+}
+template <>
+cudaError_t scale_matrix<float>(int m, int n, float beta, float* c, long ldc, cudaStream_t st) {
+    return scale_matrix_f32(m, n, beta, c, ldc, st);
+}
+
+// Device-pointer real GEMM on `st`; arguments already validated, m, n > 0.
+template <typename Scratch>
+cudaError_t run_dgemm(const GemmArgsF64& g, cudaStream_t st, Scratch scratch) {
+    Context& cx = context();
+    if (g.k == 0 || g.alpha == 0.0) return scale_matrix<double>(g.m, g.n, g.beta, g.c, g.ldc, st);
+    int method = cx.dgemm_method;
+    if (method == METHOD_AUTO) method = ozaki_preferred(g.m, g.n, g.k) ? METHOD_OZAKI : METHOD_NATIVE;
+    if (method == METHOD_OZAKI) {
+        OzakiPlan op = plan_ozaki(g.m, g.n, g.k, cx.ozaki_slices);
+        void* ws = nullptr;
+        cudaError_t e = scratch(ozaki_workspace_bytes(op), st, &ws);
+        if (e != cudaSuccess) return e;
+        return dgemm_ozaki(g, op, ws, st);
+    }
+    GemmPlan p = plan_native_gemm(g.m, g.n, g.k, 8, cx.sm_count);
+    void* ws = nullptr;
+    size_t need = splitk_workspace_elems(g.m, g.n, p.splits) * sizeof(double);
+    if (need) {
+        cudaError_t e = scratch(need, st, &ws);
+        if (e != cudaSuccess) return e;
+    }
+    return dgemm_native(g, p, static_cast<double*>(ws), st);
+}
+
+template <typename Scratch>
+cudaError_t run_sgemm(const GemmArgsF32& g, cudaStream_t st, Scratch scratch) {
+    Context& cx = context();
+    if (g.k == 0 || g.alpha == 0.0f) return scale_matrix<float>(g.m, g.n, g.beta, g.c, g.ldc, st);
+    if (cx.sgemm_method == SMETHOD_BF16X3) {
+        void* ws = nullptr;
+        cudaError_t e = scratch(bf16x3_workspace_bytes(g.m, g.n, g.k), st, &ws);
+        if (e != cudaSuccess) return e;
+        return sgemm_bf16x3(g, ws, st);
+    }
+    GemmPlan p = plan_native_gemm(g.m, g.n, g.k, 4, cx.sm_count);
+    void* ws = nullptr;
+    size_t need = splitk_workspace_elems(g.m, g.n, p.splits) * sizeof(float);
+    if (need) {
+        cudaError_t e = scratch(need, st, &ws);
+        if (e != cudaSuccess) return e;
+    }
+    return sgemm_native(g, p, static_cast<float*>(ws), st);
+}
+
+cudaError_t run_gemm(const GemmArgsF64& g, cudaStream_t st, HostScratch s) { return run_dgemm(g, st, s); }
+cudaError_t run_gemm(const GemmArgsF32& g, cudaStream_t st, HostScratch s) { return run_sgemm(g, st, s); }
+
+// Host-pointer GEMM: stage -> compute -> copy the C window back.
+template <typename T>
+void host_gemm(const char* routine, char ta, char tb, int m, int n, int k, T alpha, const T* a, int lda, const T* b,
+               int ldb, T beta, T* c, int ldc) {
+    if (m <= 0 || n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const bool quick = (k == 0 || alpha == T(0));
+    const int ra = (ta == 'N') ? m : k, ca = (ta == 'N') ? k : m;
+    const int rb = (tb == 'N') ? k : n, cb = (tb == 'N') ? n : k;
+    const size_t es = sizeof(T);
+    // Acquire every device buffer before touching C (failure before write).
+    if (!quick) {
+        if ((e = cx.reserve(cx.stage_a, (size_t)ra * ca * es, st)) != cudaSuccess ||
+            (e = cx.reserve(cx.stage_b, (size_t)rb * cb * es, st)) != cudaSuccess) {
+            cuda_status(e, "staging reservation");
+            report_gpu_failure(routine);
+            return;
+        }
+    }
+    if ((e = cx.reserve(cx.stage_c, (size_t)m * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* db = static_cast<T*>(cx.stage_b.ptr);
+    T* dc = static_cast<T*>(cx.stage_c.ptr);
+    if (!quick) {
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(db, (size_t)rb * es, b, (size_t)ldb * es, (size_t)rb * es, cb, cudaMemcpyHostToDevice,
+                                  st);
+    }
+    if (e == cudaSuccess && beta != T(0))
+        e = cudaMemcpy2DAsync(dc, (size_t)m * es, c, (size_t)ldc * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        GemmArgs<T> g{ta, tb, m, n, k, alpha, da, ra, db, rb, beta, dc, m};
+        e = run_gemm(g, st, HostScratch{&cx});
+    }
+    if (e == cudaSuccess) e = cx.sync(st);  // compute finished without error before C is written
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)m * es, (size_t)m * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+inline char cblas_trans_char(int t) {
+    switch (t) {
+        case CblasNoTrans: return 'N';
+        case CblasTrans: return 'T';
+        case CblasConjTrans: return 'C';
+        default: return 'X';
+    }
+}
+inline bool cblas_valid_layout(int l) { return l == CblasRowMajor || l == CblasColMajor; }
+inline bool cblas_valid_trans(int t) { return t == CblasNoTrans || t == CblasTrans || t == CblasConjTrans; }
+
+}  // namespace
+
+extern "C" {
+
+int lsame_(const char* ca, const char* cb) {
+    return std::toupper((unsigned char)ca[0]) == std::toupper((unsigned char)cb[0]) ? 1 : 0;
+}
+
+void xerbla_(const char* srname, const zynum_blas_int* info) { report_xerbla(srname, *info); }
+
+void zynum_blas_shutdown(void) { context().shutdown(); }
+void zynum_blas_shutdown_(void) { context().shutdown(); }
+
+void sgemm_(const char* transa, const char* transb, const zynum_blas_int* m, const zynum_blas_int* n,
+            const zynum_blas_int* k, const float* alpha, const float* a, const zynum_blas_int* lda, const float* b,
+            const zynum_blas_int* ldb, const float* beta, float* c, const zynum_blas_int* ldc) {
+    const char ta = up(transa), tb = up(transb);
+    int info = gemm_error(ta, tb, *m, *n, *k, *lda, *ldb, *ldc);
+    if (info) {
+        report_xerbla("SGEMM ", info);
+        return;
+    }
+    host_gemm<float>("SGEMM", ta, tb, *m, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);
+}
+
+void dgemm_(const char* transa, const char* transb, const zynum_blas_int* m, const zynum_blas_int* n,
+            const zynum_blas_int* k, const double* alpha, const double* a, const zynum_blas_int* lda,
+            const double* b, const zynum_blas_int* ldb, const double* beta, double* c, const zynum_blas_int* ldc) {
+    const char ta = up(transa), tb = up(transb);
+    int info = gemm_error(ta, tb, *m, *n, *k, *lda, *ldb, *ldc);
+    if (info) {
+        report_xerbla("DGEMM ", info);
+        return;
+    }
+    host_gemm<double>("DGEMM", ta, tb, *m, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);
+}
+
+// cblas.zig:1415-1439: silent return on a bad enum; row-major C = A B is
+// computed as column-major C^T = B^T A^T by swapping the operands.
+void cblas_sgemm(int layout, int transa, int transb, int m, int n, int k, float alpha, const float* a, int lda,
+                 const float* b, int ldb, float beta, float* c, int ldc) {
+    if (!cblas_valid_layout(layout) || !cblas_valid_trans(transa) || !cblas_valid_trans(transb)) return;
+    const bool rm = layout == CblasRowMajor;
+    char ta = cblas_trans_char(rm ? transb : transa), tb = cblas_trans_char(rm ? transa : transb);
+    zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, kk = k, la = rm ? ldb : lda, lb = rm ? lda : ldb, lc = ldc;
+    if (rm)
+        sgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, b, &la, a, &lb, &beta, c, &lc);
+    else
+        sgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, a, &la, b, &lb, &beta, c, &lc);
+}
+
+void cblas_dgemm(int layout, int transa, int transb, int m, int n, int k, double alpha, const double* a, int lda,
+                 const double* b, int ldb, double beta, double* c, int ldc) {
+    if (!cblas_valid_layout(layout) || !cblas_valid_trans(transa) || !cblas_valid_trans(transb)) return;
+    const bool rm = layout == CblasRowMajor;
+    char ta = cblas_trans_char(rm ? transb : transa), tb = cblas_trans_char(rm ? transa : transb);
+    zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, kk = k, la = rm ? ldb : lda, lb = rm ? lda : ldb, lc = ldc;
+    if (rm)
+        dgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, b, &la, a, &lb, &beta, c, &lc);
+    else
+        dgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, a, &la, b, &lb, &beta, c, &lc);
+}
+
+int zynum_blas_gpu_dgemm_device(char transa, char transb, int m, int n, int k, double alpha, const double* a,
+                                int lda, const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+    const char ta = up(&transa), tb = up(&transb);
+    int info = gemm_error(ta, tb, m, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GemmArgsF64 g{ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc};
+    return cuda_status(run_dgemm(g, st, StreamScratch{&cx}), "dgemm_device");
+}
+
+int zynum_blas_gpu_sgemm_device(char transa, char transb, int m, int n, int k, float alpha, const float* a, int lda,
+                                const float* b, int ldb, float beta, float* c, int ldc, void* stream) {
+    const char ta = up(&transa), tb = up(&transb);
+    int info = gemm_error(ta, tb, m, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GemmArgsF32 g{ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc};
+    return cuda_status(run_sgemm(g, st, StreamScratch{&cx}), "sgemm_device");
+}
+
+int zynum_blas_gpu_set_dgemm_method(int method) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.dgemm_method;
+    if (method >= METHOD_NATIVE && method <= METHOD_AUTO) cx.dgemm_method = method;
+    return old;
+}
+
+int zynum_blas_gpu_set_sgemm_method(int method) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.sgemm_method;
+    if (method == SMETHOD_NATIVE || method == SMETHOD_BF16X3) cx.sgemm_method = method;
+    return old;
+}
+
+int zynum_blas_gpu_set_ozaki_slices(int slices) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.ozaki_slices;
+    if (slices == 0 || (slices >= 2 && slices <= kOzakiMaxSlices)) cx.ozaki_slices = slices;
+    return old;
+}
+
+const char* zynum_blas_gpu_last_error(void) { return last_error(); }
+
+int zynum_blas_gpu_profile(int enable) { return profile_control(enable); }
+int zynum_blas_gpu_profile_read(double* ms, int max) { return profile_read(ms, max); }
+long long zynum_blas_gpu_launch_count(void) { return launch_count(); }
+
+void zynum_blas_gpu_inject_fault(int kind, int count) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    if (kind == 1) cx.faults.fail_next_reservations = count;
+    if (kind == 2) cx.faults.fail_next_sync = count;
+}
+
+}  // extern "C"

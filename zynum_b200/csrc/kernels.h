@@ -1,0 +1,68 @@
+// Internal interface between the C-ABI layer, the planner and the kernels.
+// Nothing here is exported from the shared library; the public surface is
+// include/zynum_blas_gpu.h.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace zb {
+
+// Column-major GEMM operands, BLAS conventions: op(X) = X for 'N', X^T for
+// 'T' (and for 'C' on real types).  Leading dimensions are in elements.
+template <typename T>
+struct GemmArgs {
+    char transa, transb;
+    int m, n, k;
+    T alpha;
+    const T* a;
+    long lda;
+    const T* b;
+    long ldb;
+    T beta;
+    T* c;
+    long ldc;
+};
+using GemmArgsF64 = GemmArgs<double>;
+using GemmArgsF32 = GemmArgs<float>;
+
+enum TileShape : int { TILE_128x128 = 0, TILE_128x64 = 1 };
+
+// What the planner decided for one native GEMM call.
+struct GemmPlan {
+    int tile = TILE_128x128;
+    int splits = 1;  // > 1: split-K over `splits` K ranges, needs a workspace
+};
+
+// Workspace (in elements of T) a plan needs.
+inline size_t splitk_workspace_elems(int m, int n, int splits) {
+    return splits > 1 ? (size_t)splits * (size_t)m * (size_t)n : 0;
+}
+
+// ---------------------------------------------------------------- kernels
+cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st);
+cudaError_t sgemm_native(const GemmArgsF32& g, const GemmPlan& plan, float* workspace, cudaStream_t st);
+
+// C = beta * C on the m x n window (beta == 0 writes exact zeros, clearing NaNs),
+// the reference's k == 0 / alpha == 0 quick return (gemm.zig:1407-1414).
+cudaError_t scale_matrix_f64(int m, int n, double beta, double* c, long ldc, cudaStream_t st);
+cudaError_t scale_matrix_f32(int m, int n, float beta, float* c, long ldc, cudaStream_t st);
+// Complex (interleaved) scale by a complex beta.
+cudaError_t scale_matrix_z(int m, int n, const double* beta, double* c, long ldc, cudaStream_t st);
+cudaError_t scale_matrix_c(int m, int n, const float* beta, float* c, long ldc, cudaStream_t st);
+
+// ------------------------------------------------------------ profiling
+// When enabled (zynum_blas_gpu_profile), CUDA events are recorded on the
+// launching stream around the dominant kernel of each call; the host reads
+// the per-launch durations afterwards.  Disabled: no cost beyond a branch.
+void prof_begin(cudaStream_t st);
+// Every kernel launch of the library is counted (reported by
+// zynum_blas_gpu_launch_count) so a caller can see the GPU work it caused.
+void count_launch();
+void prof_end(cudaStream_t st);
+
+// ---------------------------------------------------------------- planner
+GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count);
+
+}  // namespace zb

@@ -1,0 +1,33 @@
+// Ozaki-scheme DGEMM (INT8 tcgen05 slices) and 3xBF16 SGEMM.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace zb {
+
+constexpr int kOzakiMaxSlices = 12;
+
+struct OzakiPlan {
+    int slices = 7;   // INT8 slices per operand (7 bits each)
+    int m_pad = 0;    // rows of A padded to the 128-row UMMA tile
+    int n_pad = 0;    // columns of B padded to the 256-column UMMA tile
+    int k_pad = 0;    // K padded to the 128-byte TMA box
+};
+
+// Whether the automatic method should prefer Ozaki for this shape.
+bool ozaki_preferred(int m, int n, int k);
+// slices == 0 picks the count automatically from k.
+OzakiPlan plan_ozaki(int m, int n, int k, int slices);
+size_t ozaki_workspace_bytes(const OzakiPlan& p);
+// C = alpha op(A) op(B) + beta C through INT8 slice products; `ws` holds
+// ozaki_workspace_bytes(p) bytes of device scratch.
+cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st);
+
+size_t bf16x3_workspace_bytes(int m, int n, int k);
+// C = alpha op(A) op(B) + beta C as a 3xBF16 split product with FP32 accumulation.
+cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st);
+
+}  // namespace zb

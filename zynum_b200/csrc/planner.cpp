@@ -1,0 +1,31 @@
+// GPU planner for one native GEMM call: block tile shape and split-K.
+//
+// Replaces the reference's CPU planner (core/matrix_matrix/planner.zig):
+// desiredThreadCount :88 / rowTaskCount :170 / runPlannedTasks :296 split C
+// into at most 64 disjoint column/row tasks for host threads.  On the GPU the
+// equivalent decision is how many CTAs cover C (tile shape) and, when C has
+// too few tiles to fill the 148 SMs, how far to split K.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace zb {
+
+GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count) {
+    GemmPlan p;
+    // Narrow-N, tall-M shapes (e.g. 131072 x 64 x 64) are HBM-bound: a 64-wide
+    // tile avoids computing (and staging) a half-empty 128-wide tile.
+    if (elem_bytes == 8 && n <= 64 && m >= 1024) p.tile = TILE_128x64;
+    const int bn = (p.tile == TILE_128x64) ? 64 : 128;
+    const long tiles = (long)((m + 127) / 128) * ((n + bn - 1) / bn);
+    p.splits = 1;
+    if (tiles < sm_count && k >= 2048) {
+        long s = sm_count / std::max<long>(tiles, 1);
+        s = std::min<long>(s, k / 512);
+        s = std::min<long>(s, 64);
+        if (s >= 2) p.splits = (int)s;
+    }
+    return p;
+}
+
+}  // namespace zb

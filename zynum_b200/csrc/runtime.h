@@ -1,0 +1,79 @@
+// Per-process GPU context of the shim: device, host-ABI stream, staging and
+// workspace buffers, method switches and the last-error string.
+//
+// Replaces the reference's CPU runtime/thread pool (runtime.zig:54 maxThreads,
+// execution/thread_pool.zig:247-264) for the GPU product: the "pool" here is
+// one CUDA stream per host-ABI context plus grow-on-demand device buffers.
+// Ownership follows the reference's rule that internal workspace is acquired
+// before any write to caller memory (gemm.zig:48-53): every host entry point
+// reserves all of its device memory first and returns with C untouched if that
+// fails.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include <cuda_runtime.h>
+
+namespace zb {
+
+enum DgemmMethod : int { METHOD_NATIVE = 0, METHOD_OZAKI = 1, METHOD_AUTO = 2 };
+enum SgemmMethod : int { SMETHOD_NATIVE = 0, SMETHOD_BF16X3 = 1 };
+
+// A device buffer that only grows.  Growing synchronises `stream` first so the
+// old allocation is no longer in use.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t need, cudaStream_t stream);
+    void release();
+};
+
+// Host-side fault injection used by the tests (no GPU fault is ever made):
+// the next reservation fails with cudaErrorMemoryAllocation, or the next
+// stream synchronisation reports the given error.
+struct InjectedFaults {
+    int fail_next_reservations = 0;
+    int fail_next_sync = 0;  // cudaError_t code
+};
+
+struct Context {
+    int device = -1;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;  // stream of the host (Fortran / CBLAS) entry points
+    std::recursive_mutex mutex;     // host entry points are callable from any thread
+    DeviceBuffer stage_a, stage_b, stage_c;
+    DeviceBuffer work;  // scratch of the host entry points (split-K partials, slices)
+    // Scratch of the device entry points, one per caller stream so that calls
+    // on different streams never share scratch memory.
+    std::unordered_map<cudaStream_t, DeviceBuffer> stream_work;
+    int dgemm_method = METHOD_NATIVE;
+    int sgemm_method = SMETHOD_NATIVE;
+    int ozaki_slices = 0;  // 0 = automatic
+    InjectedFaults faults;
+    bool initialised = false;
+    cudaError_t init();
+    void shutdown();
+    // Scratch for a device entry point running on `stream`.
+    cudaError_t stream_scratch(cudaStream_t stream, size_t bytes, void** out);
+    cudaError_t reserve(DeviceBuffer& buf, size_t bytes, cudaStream_t stream);
+    cudaError_t sync(cudaStream_t stream);
+};
+
+Context& context();
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+// Dominant-kernel timing (see prof_begin / prof_end in kernels.h).
+int profile_control(int enable);
+int profile_read(double* ms, int max);
+long long launch_count();
+
+// Reference-style error report (fortran.zig:277 reportError -> xerbla_ :20).
+void report_xerbla(const char* routine, int info);
+
+}  // namespace zb
