@@ -89,6 +89,10 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_sgemm_method(int method);
 /* Ozaki slice count (2..12), 0 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_slices(int slices);
+/* Slice count the Ozaki method uses for an m x n x k DGEMM under the current
+ * setting (with the automatic setting: the count the most recent call chose
+ * from its data), and the number of INT8 slice-product GEMMs (s(s+1)/2). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int *slices, int *products);
 /* Text of the last error seen by this thread ("" if none). */
 ZYNUM_BLAS_GPU_API const char *zynum_blas_gpu_last_error(void);
 /* Host-side fault injection for tests: the next `count` device-memory

@@ -55,6 +55,8 @@ def _declare(L: C.CDLL) -> None:
                  "zynum_blas_gpu_set_ozaki_slices"):
         getattr(L, name).argtypes = [i]
         getattr(L, name).restype = i
+    L.zynum_blas_gpu_ozaki_plan.argtypes = [i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.zynum_blas_gpu_ozaki_plan.restype = i
     L.zynum_blas_gpu_last_error.argtypes = []
     L.zynum_blas_gpu_last_error.restype = cp
     L.zynum_blas_gpu_inject_fault.argtypes = [i, i]

@@ -324,6 +324,19 @@ int zynum_blas_gpu_set_ozaki_slices(int slices) {
     return old;
 }
 
+int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int* slices, int* products) {
+    Context& cx = context();
+    int s;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        s = plan_ozaki(m, n, k, cx.ozaki_slices).slices;
+    }
+    if (s == 0) s = ozaki_last_slices();  // automatic: the count the last call chose
+    if (slices) *slices = s;
+    if (products) *products = s * (s + 1) / 2;
+    return 0;
+}
+
 const char* zynum_blas_gpu_last_error(void) { return last_error(); }
 
 int zynum_blas_gpu_profile(int enable) { return profile_control(enable); }

@@ -1,10 +1,781 @@
-// placeholder, replaced by the Ozaki implementation
+// Ozaki-scheme DGEMM on INT8 tensor cores, and SGEMM as a 3xBF16 split product.
+//
+// DGEMM by error-free splitting (Ozaki, Ogita, Oishi, Rump 2012; integer
+// variant Ootomo, Ozaki, Yokota 2024), restated from the mathematics:
+//
+//   op(A)[i,p] = 2^{e_i} * (sum_{t=1..s} 2^{-7t} A_t[i,p] + r_ip),  |r_ip| < 2^{-7s}
+//   op(B)[p,j] = 2^{f_j} * (sum_{u=1..s} 2^{-7u} B_u[p,j] + r'_pj)
+//
+// with e_i / f_j the binary exponents of the row / column maxima (so the
+// scaled values lie in (-1, 1)) and A_t, B_u int8 digits in [-127, 127]
+// produced by exact FP64 steps y <- 128 y, d = trunc(y), y <- y - d.  Then
+//
+//   C ~= sum_{g=2..s+1} 2^{e_i + f_j - 7g} * D_g,   D_g = sum_{t+u=g} A_t B_u
+//
+// Every D_g is an exact INT32 tensor-core product (|D_g| <= s k 127^2 is kept
+// below 2^31 by splitting K into segments).  FP64 is used only for the
+// exponent scan, the digit extraction and the recombination of the D_g.
+//
+// Kernels:
+//   ozaki_absmax     row / column max |x| (bit patterns, atomicMax)       HBM-bound
+//   ozaki_split      exponents + s int8 digit planes, K-major, padded    HBM-bound
+//   umma_slice_gemm  persistent tcgen05 GEMM: TMA -> smem ring -> UMMA
+//                    (kind::i8, INT32 accumulators in TMEM, two 256-column
+//                    buffers) -> epilogue warps scale D_g to FP64 and
+//                    accumulate into C (alpha, beta, ldc)                 tensor-bound
+//
+// 3xBF16 SGEMM: x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and
+// C ~= hi_A hi_B + hi_A lo_B + lo_A hi_B, one FP32 TMEM accumulator
+// (kind::f16 with BF16 inputs), same GEMM kernel with a FP32 epilogue.
+//
+// Replaces, for the GPU, the reference's dense real GEMM body
+// (kernels/shared/matrix_matrix/packed_simd.zig:306) when the Ozaki method is
+// selected; argument semantics are those of gemm.zig:1392.
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+
+#include "common.cuh"
+#include "kernels.h"
 #include "ozaki.h"
+
 namespace zb {
-bool ozaki_preferred(int, int, int) { return false; }
-OzakiPlan plan_ozaki(int, int, int, int) { return OzakiPlan{}; }
-size_t ozaki_workspace_bytes(const OzakiPlan&) { return 0; }
-cudaError_t dgemm_ozaki(const GemmArgsF64&, const OzakiPlan&, void*, cudaStream_t) { return cudaErrorNotSupported; }
-size_t bf16x3_workspace_bytes(int, int, int) { return 0; }
-cudaError_t sgemm_bf16x3(const GemmArgsF32&, void*, cudaStream_t) { return cudaErrorNotSupported; }
+namespace {
+
+// ------------------------------------------------------------ geometry
+constexpr int kUM = 128;        // C rows per tile (TMEM lanes)
+constexpr int kUN = 256;        // C columns per tile (TMEM columns per buffer)
+constexpr int kChunkBytes = 128;  // K bytes per pipeline stage (one 128B swizzle row)
+constexpr int kStages = 4;
+constexpr int kAStage = kUM * kChunkBytes;  // 16 KB
+constexpr int kBStage = kUN * kChunkBytes;  // 32 KB
+constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kMaxPairs = 96;
+constexpr int kMaxGroups = 16;
+constexpr size_t kSmemBytes = 1024 /*align slack*/ + kStages * (kAStage + kBStage) + 256;
+
+enum Kind : int { KIND_I8 = 0, KIND_BF16 = 1 };
+enum Epi : int { EPI_OZAKI_F64 = 0, EPI_F32 = 1 };
+
+struct UmmaParams {
+    int m, n;                // C extent
+    int m_pad, n_pad;        // rows per plane of the A / B digit tensors
+    int k_chunks;            // total 128-byte K chunks
+    int kseg_chunks;         // K chunks per accumulation segment
+    int num_kseg;
+    int tiles_m, tiles_n, num_tiles;
+    int num_groups;
+    int group_first[kMaxGroups];
+    int group_count[kMaxGroups];
+    int group_shift[kMaxGroups];  // 7 g for Ozaki
+    int pair_a[kMaxPairs];        // digit plane of A
+    int pair_b[kMaxPairs];        // digit plane of B
+    double alpha, beta;
+    float alpha_f, beta_f;
+    void* c;
+    long ldc;
+    const int* row_exp;
+    const int* col_exp;
+    int* status;
+};
+
+// ------------------------------------------------------ bounded waiting
+// Wait for phase `parity` of `bar`; give up (and raise the CTA abort flag and
+// the device status) after ~2^28 polls or as soon as another role aborted.
+ZB_DEVICE bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status, int where) {
+    for (uint32_t i = 0; i < (1u << 28); ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023) == 1023 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    if (status) atomicCAS(status, 0, where);
+    return false;
 }
+
+ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn) {
+    // Groups of 8 tile-rows sweep the tile-columns, so CTAs running together
+    // share A row blocks and B column blocks in L2.
+    constexpr int G = 8;
+    int band = tile / (G * tiles_n);
+    int rows_in_band = min(G, tiles_m - band * G);
+    int r = tile - band * G * tiles_n;
+    tm = band * G + r % rows_in_band;
+    tn = r / rows_in_band;
+}
+
+ZB_DEVICE double pow2(int e) {
+    // exact 2^e for the normal range; ldexp handles the rest
+    if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
+    return ldexp(1.0, e);
+}
+
+template <int KIND, int EPI>
+__global__ void __launch_bounds__(kThreads, 1)
+umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ UmmaParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + kStages * kAStage;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + kStages * kBStage);
+    uint64_t* empty = full + kStages;
+    uint64_t* tfull = empty + kStages;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
+                int tm, tn;
+                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
+                for (int g = 0; ok && g < P.num_groups; ++g)
+                    for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                        const int c0 = ks * P.kseg_chunks;
+                        const int c1 = min(P.k_chunks, c0 + P.kseg_chunks);
+                        for (int q = 0; ok && q < P.group_count[g]; ++q) {
+                            const int pa = P.pair_a[P.group_first[g] + q], pb = P.pair_b[P.group_first[g] + q];
+                            for (int kc = c0; kc < c1; ++kc) {
+                                if (!wait_phase(&empty[stage], phase ^ 1, abort_flag, P.status, 1)) {
+                                    ok = false;
+                                    break;
+                                }
+                                mbar_arrive_expect_tx(&full[stage], kAStage + kBStage);
+                                tma_load_2d(smem_u32(sA + stage * kAStage), &tmA, &full[stage], kc * elems_per_chunk,
+                                            pa * P.m_pad + tm * kUM);
+                                tma_load_2d(smem_u32(sB + stage * kBStage), &tmB, &full[stage], kc * elems_per_chunk,
+                                            pb * P.n_pad + tn * kUN);
+                                if (++stage == kStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        }
+                    }
+            }
+            // Let every issued copy land before the CTA can retire (bounded).
+            for (int i = 0; i < kStages; ++i) {
+                wait_phase(&empty[stage], phase ^ 1, abort_flag, nullptr, 0);
+                if (++stage == kStages) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, kUM, kUN) : umma_idesc(1, 1, kUM, kUN);
+            int stage = 0;
+            uint32_t phase = 0;
+            int job = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x)
+                for (int g = 0; ok && g < P.num_groups; ++g)
+                    for (int ks = 0; ok && ks < P.num_kseg; ++ks, ++job) {
+                        const int b = job & 1, use = job >> 1;
+                        if (!wait_phase(&tempty[b], (use & 1) ^ 1, abort_flag, P.status, 2)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t d = tmem_base + b * kUN;
+                        const int c0 = ks * P.kseg_chunks;
+                        const int c1 = min(P.k_chunks, c0 + P.kseg_chunks);
+                        uint32_t acc = 0;
+                        for (int q = 0; ok && q < P.group_count[g]; ++q)
+                            for (int kc = c0; kc < c1; ++kc) {
+                                if (!wait_phase(&full[stage], phase, abort_flag, P.status, 3)) {
+                                    ok = false;
+                                    break;
+                                }
+                                tc_fence_after();
+                                const uint32_t a0 = smem_u32(sA + stage * kAStage);
+                                const uint32_t b0 = smem_u32(sB + stage * kBStage);
+#pragma unroll
+                                for (int kk = 0; kk < kChunkBytes / 32; ++kk) {
+                                    const uint64_t ad = umma_desc_sw128(a0 + kk * 32);
+                                    const uint64_t bd = umma_desc_sw128(b0 + kk * 32);
+                                    if (KIND == KIND_I8)
+                                        umma_i8(d, ad, bd, idesc, acc);
+                                    else
+                                        umma_f16(d, ad, bd, idesc, acc);
+                                    acc = 1;
+                                }
+                                umma_commit(&empty[stage]);
+                                if (++stage == kStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        if (ok) umma_commit(&tfull[b]);
+                    }
+        }
+    } else {
+        // ---------------------------------------------- epilogue warps
+        const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+        const int row_in_tile = quarter * 32 + lane;
+        int job = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
+            int tm, tn;
+            tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
+            const int row = tm * kUM + row_in_tile;
+            const bool row_ok = row < P.m;
+            int er = 0;
+            if (EPI == EPI_OZAKI_F64 && row_ok) er = P.row_exp[row];
+            bool first = true;
+            for (int g = 0; ok && g < P.num_groups; ++g)
+                for (int ks = 0; ok && ks < P.num_kseg; ++ks, ++job) {
+                    const int b = job & 1, use = job >> 1;
+                    if (!wait_phase(&tfull[b], use & 1, abort_flag, P.status, 4)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    double rowscale = 1.0;
+                    if (EPI == EPI_OZAKI_F64) rowscale = pow2(er - P.group_shift[g]) * P.alpha;
+#pragma unroll 1
+                    for (int ch = 0; ch < kUN / 32; ++ch) {
+                        uint32_t r[32];
+                        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + b * kUN + ch * 32, r);
+                        tmem_ld_wait();
+                        const int col0 = tn * kUN + ch * 32;
+                        if (!row_ok) continue;
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            const int col = col0 + c;
+                            if (col >= P.n) continue;
+                            if (EPI == EPI_OZAKI_F64) {
+                                double* cp = static_cast<double*>(P.c) + (long)col * P.ldc + row;
+                                const double v = (double)(int)r[c] * rowscale * pow2(P.col_exp[col]);
+                                double out;
+                                if (first)
+                                    out = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
+                                else
+                                    out = *cp + v;
+                                *cp = out;
+                            } else {
+                                float* cp = static_cast<float*>(P.c) + (long)col * P.ldc + row;
+                                const float v = P.alpha_f * __uint_as_float(r[c]);
+                                float out;
+                                if (first)
+                                    out = (P.beta_f == 0.0f) ? v : fmaf(P.beta_f, *cp, v);
+                                else
+                                    out = *cp + v;
+                                *cp = out;
+                            }
+                        }
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&tempty[b]);
+                    first = false;
+                }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem_base, 512);
+}
+
+// ------------------------------------------------------------- splitting
+// View of a matrix X (rows r, cols c): element at base[r * rs + c * cs];
+// exactly one of rs / cs is 1.
+struct View {
+    const double* base;
+    long rs, cs;
+    int rows, cols;
+};
+
+// Row maxima of |X| as FP64 bit patterns (non-negative doubles order like
+// unsigned integers; NaN patterns sort above +Inf and so propagate).
+// Also accumulates the row sums of |x| (used by the automatic slice count).
+__global__ void ozaki_absmax(View X, unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
+    if (X.rs == 1) {
+        const int r = blockIdx.x * blockDim.x + threadIdx.x;
+        if (r >= X.rows) return;
+        const int c0 = blockIdx.y * 64, c1 = min(X.cols, c0 + 64);
+        unsigned long long mx = 0;
+        double sm = 0.0;
+        for (int c = c0; c < c1; ++c) {
+            const double a = fabs(X.base[r + (long)c * X.cs]);
+            const unsigned long long v = (unsigned long long)__double_as_longlong(a);
+            mx = v > mx ? v : mx;
+            sm += a;
+        }
+        if (mx) atomicMax(&maxbits[r], mx);
+        if (sm != 0.0) atomicAdd(&sums[r], sm);
+    } else {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int r = blockIdx.x * (blockDim.x / 32) + warp;
+        if (r >= X.rows) return;
+        const int c0 = blockIdx.y * 1024, c1 = min(X.cols, c0 + 1024);
+        unsigned long long mx = 0;
+        double sm = 0.0;
+        for (int c = c0 + lane; c < c1; c += 32) {
+            const double a = fabs(X.base[(long)r * X.rs + c]);
+            const unsigned long long v = (unsigned long long)__double_as_longlong(a);
+            mx = v > mx ? v : mx;
+            sm += a;
+        }
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, mx, o);
+            mx = w > mx ? w : mx;
+            sm += __shfl_xor_sync(0xffffffffu, sm, o);
+        }
+        if (lane == 0 && mx) atomicMax(&maxbits[r], mx);
+        if (lane == 0 && sm != 0.0) atomicAdd(&sums[r], sm);
+    }
+}
+
+// Largest "spread" over rows: e_r - log2(mean_c |x_rc|), the number of bits
+// between a row's scaling exponent and its typical magnitude.  The digits of
+// a typical entry start this many bits below the top of the first slice.
+__global__ void ozaki_spread(const unsigned long long* __restrict__ maxbits, const double* __restrict__ sums,
+                             int rows, int cols, float* __restrict__ out) {
+    float best = 0.f;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+        if (maxbits[r] == 0 || sums[r] <= 0.0) continue;
+        int e;
+        frexp(__longlong_as_double((long long)maxbits[r]), &e);
+        const float sp = (float)(e - log2(sums[r] / cols));
+        best = sp > best ? sp : best;
+    }
+    for (int o = 16; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = fmaxf(b, part[w]);
+        *out = b;
+    }
+}
+
+// Exponent e with max * 2^-e in [0.5, 1): the frexp exponent of the maximum.
+ZB_DEVICE int row_exponent(unsigned long long bits) {
+    if (bits == 0) return 0;
+    int e;
+    frexp(__longlong_as_double((long long)bits), &e);
+    return e;
+}
+
+// Swizzled [32][128] double tile: conflict-free both for 32 consecutive rows
+// of one column and for 16 consecutive columns of two adjacent rows.
+ZB_DEVICE int swz(int r, int c) {
+    const int h = ((r & 1) << 3) | ((r >> 1) & 7);
+    return r * 128 + (c ^ ((h ^ (c >> 4)) & 15));
+}
+
+// Each block: 32 rows x 128 columns of X -> s int8 digit planes
+// (plane t: rows_pad x cols_pad bytes, K-major) and the row exponents.
+__global__ void __launch_bounds__(256)
+ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, int rows_pad, int cols_pad,
+            int8_t* __restrict__ planes, int* __restrict__ exps) {
+    __shared__ double tile[32 * 128];
+    __shared__ int sexp[32];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
+    const int t = threadIdx.x;
+    if (t < 32) {
+        const int r = r0 + t;
+        const int e = (r < X.rows) ? row_exponent(maxbits[r]) : 0;
+        sexp[t] = e;
+        if (blockIdx.x == 0 && r < rows_pad) exps[r] = e;
+    }
+    // load (coalesced along the contiguous dimension of X)
+#pragma unroll 4
+    for (int it = 0; it < 16; ++it) {
+        const int idx = it * 256 + t;
+        int r, c;
+        if (X.rs == 1) {
+            r = idx & 31;
+            c = idx >> 5;
+        } else {
+            r = idx >> 7;
+            c = idx & 127;
+        }
+        const int gr = r0 + r, gc = c0 + c;
+        double v = 0.0;
+        if (gr < X.rows && gc < X.cols) v = X.base[(long)gr * X.rs + (long)gc * X.cs];
+        tile[swz(r, c)] = v;
+    }
+    __syncthreads();
+    // digits: thread -> row t / 8, 16 consecutive columns
+    const int r = t >> 3, q = t & 7;
+    const double sc = ldexp(1.0, -sexp[r]);
+    double y[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) y[i] = tile[swz(r, q * 16 + i)] * sc;
+    const long plane = (long)rows_pad * cols_pad;
+    int8_t* out = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
+    for (int s = 0; s < slices; ++s) {
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double z = y[i] * 128.0;
+            const double d = trunc(z);
+            y[i] = z - d;
+            w[i >> 2] |= ((uint32_t)(int)d & 0xFFu) << (8 * (i & 3));
+        }
+        if (r0 + r < rows_pad) *reinterpret_cast<uint4*>(out + s * plane) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// 3xBF16 split of a float matrix view into hi / lo planes (bf16, K-major).
+struct ViewF {
+    const float* base;
+    long rs, cs;
+    int rows, cols;
+};
+
+__global__ void __launch_bounds__(256)
+bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ planes) {
+    __shared__ float tile[32][129];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
+    const int t = threadIdx.x;
+#pragma unroll 4
+    for (int it = 0; it < 16; ++it) {
+        const int idx = it * 256 + t;
+        int r, c;
+        if (X.rs == 1) {
+            r = idx & 31;
+            c = idx >> 5;
+        } else {
+            r = idx >> 7;
+            c = idx & 127;
+        }
+        const int gr = r0 + r, gc = c0 + c;
+        float v = 0.f;
+        if (gr < X.rows && gc < X.cols) v = X.base[(long)gr * X.rs + (long)gc * X.cs];
+        tile[r][c] = v;
+    }
+    __syncthreads();
+    const int r = t >> 3, q = t & 7;
+    if (r0 + r >= rows_pad) return;
+    const long plane = (long)rows_pad * cols_pad;
+    __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const float x = tile[r][q * 16 + i];
+        hi[i] = __float2bfloat16_rn(x);
+        lo[i] = __float2bfloat16_rn(x - __bfloat162float(hi[i]));
+    }
+    __nv_bfloat16* o = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
+    *reinterpret_cast<uint4*>(o) = *reinterpret_cast<uint4*>(hi);
+    *reinterpret_cast<uint4*>(o + 8) = *reinterpret_cast<uint4*>(hi + 8);
+    *reinterpret_cast<uint4*>(o + plane) = *reinterpret_cast<uint4*>(lo);
+    *reinterpret_cast<uint4*>(o + plane + 8) = *reinterpret_cast<uint4*>(lo + 8);
+}
+
+// ------------------------------------------------------------ host side
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 2-D K-major digit tensor: inner dim = K (cols_pad elements), outer = planes * rows_pad rows.
+cudaError_t make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int elem_bytes, long cols_pad,
+                     long total_rows, int box_rows) {
+    auto enc = get_encode();
+    if (!enc) return cudaErrorNotSupported;
+    cuuint64_t dims[2] = {(cuuint64_t)cols_pad, (cuuint64_t)total_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(cols_pad * elem_bytes)};
+    cuuint32_t box[2] = {(cuuint32_t)(kChunkBytes / elem_bytes), (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
+
+// Workspace layout: the small statistics block first, the digit planes after it.
+struct Layout {
+    long maxa_off, maxb_off, suma_off, sumb_off, expa_off, expb_off, spread_off, status_off, stats_end;
+    long a_planes_off, b_planes_off, total;
+};
+
+Layout ozaki_layout(const OzakiPlan& p) {
+    Layout L{};
+    long off = 0;
+    auto take = [&](long bytes) {
+        long o = off;
+        off = round_up(off + bytes, 256);
+        return o;
+    };
+    L.maxa_off = take((long)p.m_pad * 8);
+    L.maxb_off = take((long)p.n_pad * 8);
+    L.suma_off = take((long)p.m_pad * 8);
+    L.sumb_off = take((long)p.n_pad * 8);
+    L.expa_off = take((long)p.m_pad * 4);
+    L.expb_off = take((long)p.n_pad * 4);
+    L.spread_off = take(16);
+    L.status_off = take(64);
+    L.stats_end = off;
+    off = round_up(off, 1024);
+    const int s = p.slices > 0 ? p.slices : kOzakiAutoMaxSlices;
+    L.a_planes_off = take((long)s * p.m_pad * p.k_pad);
+    L.b_planes_off = take((long)s * p.n_pad * p.k_pad);
+    L.total = off;
+    return L;
+}
+
+int sm_count_cached() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <int KIND, int EPI>
+cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
+    auto kern = umma_slice_gemm<KIND, EPI>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (e != cudaSuccess) return e;
+    const int grid = P.num_tiles < sm_count_cached() ? P.num_tiles : sm_count_cached();
+    prof_begin(st);
+    kern<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, P);
+    count_launch();
+    prof_end(st);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// Largest K (in 128-byte chunks) whose INT32 group sums cannot overflow:
+// pairs_per_group * K * 127^2 < 2^31.
+static int max_kseg_chunks(int slices) {
+    const long limit = (2147483647L / (long)(slices * 127 * 127)) / kChunkBytes;
+    return limit < 1 ? 1 : (int)limit;
+}
+
+bool ozaki_preferred(int m, int n, int k) { return (long)m * n >= 512L * 512 && k >= 256; }
+
+int ozaki_auto_slices(float spread_a, float spread_b) {
+    // 52 + spread bits must be covered by 7-bit digits for the truncation
+    // error to stay at or below the FP64 rounding error of native DGEMM
+    // (calibrated on U[-1,1] * 10^U[-phi,phi] data, phi in {0, 4, 8}).
+    int s = (int)ceilf((52.0f + spread_a + spread_b) / 7.0f);
+    if (s < 6) s = 6;
+    if (s > kOzakiAutoMaxSlices) s = kOzakiAutoMaxSlices;
+    return s;
+}
+
+namespace {
+std::atomic<int> g_last_slices{0};
+}
+int ozaki_last_slices() { return g_last_slices.load(); }
+
+OzakiPlan plan_ozaki(int m, int n, int k, int slices) {
+    OzakiPlan p;
+    if (slices > kOzakiMaxSlices) slices = kOzakiMaxSlices;
+    if (slices < 0) slices = 0;
+    p.slices = slices;  // 0: chosen from the data at run time
+    p.m_pad = (int)round_up(m, kUM);
+    p.n_pad = (int)round_up(n, kUN);
+    p.k_pad = (int)round_up(k, kChunkBytes);
+    return p;
+}
+
+size_t ozaki_workspace_bytes(const OzakiPlan& p) { return (size_t)ozaki_layout(p).total; }
+
+cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, cudaStream_t st) {
+    OzakiPlan p = plan;
+    const Layout L = ozaki_layout(p);
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    int8_t* a_planes = reinterpret_cast<int8_t*>(w + L.a_planes_off);
+    int8_t* b_planes = reinterpret_cast<int8_t*>(w + L.b_planes_off);
+    auto* maxa = reinterpret_cast<unsigned long long*>(w + L.maxa_off);
+    auto* maxb = reinterpret_cast<unsigned long long*>(w + L.maxb_off);
+    auto* suma = reinterpret_cast<double*>(w + L.suma_off);
+    auto* sumb = reinterpret_cast<double*>(w + L.sumb_off);
+    int* expa = reinterpret_cast<int*>(w + L.expa_off);
+    int* expb = reinterpret_cast<int*>(w + L.expb_off);
+    float* spread = reinterpret_cast<float*>(w + L.spread_off);
+    int* status = reinterpret_cast<int*>(w + L.status_off);
+
+    // op(A) as rows i / cols p; op(B)^T as rows j / cols p.
+    View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
+    View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
+
+    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);
+    if (e != cudaSuccess) return e;
+    for (int side = 0; side < 2; ++side) {
+        const View& v = side ? vb : va;
+        if (v.rs == 1) {
+            dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
+            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+        } else {
+            dim3 grid((v.rows + 7) / 8, (v.cols + 1023) / 1024);
+            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+        }
+        count_launch();
+    }
+    if (p.slices <= 0) {
+        // Automatic slice count from the data's dynamic range (one small
+        // device -> host read; the stream is synchronised here).
+        ozaki_spread<<<1, 1024, 0, st>>>(maxa, suma, g.m, g.k, spread);
+        count_launch();
+        ozaki_spread<<<1, 1024, 0, st>>>(maxb, sumb, g.n, g.k, spread + 1);
+        count_launch();
+        float h[2] = {0.f, 0.f};
+        if ((e = cudaMemcpyAsync(h, spread, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        p.slices = ozaki_auto_slices(h[0], h[1]);
+    }
+    g_last_slices.store(p.slices);
+    for (int side = 0; side < 2; ++side) {
+        const View& v = side ? vb : va;
+        const int rows_pad = side ? p.n_pad : p.m_pad;
+        dim3 sgrid(p.k_pad / 128, rows_pad / 32);
+        ozaki_split<<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, p.slices, rows_pad, p.k_pad,
+                                           side ? b_planes : a_planes, side ? expb : expa);
+        count_launch();
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    CUtensorMap ma, mb;
+    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)p.slices * p.m_pad, kUM)) !=
+        cudaSuccess)
+        return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)p.slices * p.n_pad, kUN)) !=
+        cudaSuccess)
+        return e;
+
+    UmmaParams P{};
+    P.m = g.m;
+    P.n = g.n;
+    P.m_pad = p.m_pad;
+    P.n_pad = p.n_pad;
+    P.k_chunks = p.k_pad / kChunkBytes;
+    P.kseg_chunks = max_kseg_chunks(p.slices);
+    if (P.kseg_chunks > P.k_chunks) P.kseg_chunks = P.k_chunks;
+    P.num_kseg = (P.k_chunks + P.kseg_chunks - 1) / P.kseg_chunks;
+    P.tiles_m = p.m_pad / kUM;
+    P.tiles_n = p.n_pad / kUN;
+    P.num_tiles = P.tiles_m * P.tiles_n;
+    // groups g = s+1 .. 2 (smallest contributions first), pairs t + u = g
+    int np = 0, ng = 0;
+    for (int gg = p.slices + 1; gg >= 2; --gg) {
+        P.group_first[ng] = np;
+        for (int t = 1; t <= p.slices; ++t) {
+            const int u = gg - t;
+            if (u < 1 || u > p.slices) continue;
+            P.pair_a[np] = t - 1;
+            P.pair_b[np] = u - 1;
+            ++np;
+        }
+        P.group_count[ng] = np - P.group_first[ng];
+        P.group_shift[ng] = 7 * gg;
+        ++ng;
+    }
+    P.num_groups = ng;
+    P.alpha = g.alpha;
+    P.beta = g.beta;
+    P.c = g.c;
+    P.ldc = g.ldc;
+    P.row_exp = expa;
+    P.col_exp = expb;
+    P.status = status;
+    return launch_umma<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
+}
+
+size_t bf16x3_workspace_bytes(int m, int n, int k) {
+    const long mp = round_up(m, kUM), np = round_up(n, kUN), kp = round_up(k, 128);
+    return (size_t)(2 * mp * kp * 2 + 2 * np * kp * 2 + 1024);
+}
+
+cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
+    // K is padded to 128 elements: the split kernel writes 128 columns per block.
+    const int mp = (int)round_up(g.m, kUM), np = (int)round_up(g.n, kUN), kp = (int)round_up(g.k, 128);
+    __nv_bfloat16* a_planes = static_cast<__nv_bfloat16*>(ws);
+    __nv_bfloat16* b_planes = a_planes + 2L * mp * kp;
+    ViewF va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
+    ViewF vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
+    bf16_split<<<dim3((kp + 127) / 128, mp / 32), 256, 0, st>>>(va, mp, kp, a_planes);
+    count_launch();
+    bf16_split<<<dim3((kp + 127) / 128, np / 32), 256, 0, st>>>(vb, np, kp, b_planes);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    CUtensorMap ma, mb;
+    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * mp, kUM)) != cudaSuccess) return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * np, kUN)) != cudaSuccess) return e;
+    UmmaParams P{};
+    P.m = g.m;
+    P.n = g.n;
+    P.m_pad = mp;
+    P.n_pad = np;
+    P.k_chunks = kp / 64;
+    P.kseg_chunks = P.k_chunks;
+    P.num_kseg = 1;
+    P.tiles_m = mp / kUM;
+    P.tiles_n = np / kUN;
+    P.num_tiles = P.tiles_m * P.tiles_n;
+    P.num_groups = 1;
+    P.group_first[0] = 0;
+    P.group_count[0] = 3;
+    P.group_shift[0] = 0;
+    // lo*hi, hi*lo first (small), then hi*hi; plane 0 = hi, 1 = lo
+    P.pair_a[0] = 1; P.pair_b[0] = 0;
+    P.pair_a[1] = 0; P.pair_b[1] = 1;
+    P.pair_a[2] = 0; P.pair_b[2] = 0;
+    P.alpha_f = g.alpha;
+    P.beta_f = g.beta;
+    P.c = g.c;
+    P.ldc = g.ldc;
+    return launch_umma<KIND_BF16, EPI_F32>(ma, mb, P, st);
+}
+
+}  // namespace zb
