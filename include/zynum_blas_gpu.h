@@ -82,6 +82,23 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_device(char transa, char transb, int
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_sgemm_device(char transa, char transb, int m, int n, int k, float alpha, const float *a, int lda,
                                 const float *b, int ldb, float beta, float *c, int ldc, void *stream);
 
+/* Allocation-free DGEMM (no counterpart in the reference: an addition of the
+ * GPU backend).  For callers that cannot let the library call cudaMalloc —
+ * code whose device memory belongs to its own pool allocator, or latency-
+ * critical loops where cudaMalloc/cudaFree would synchronise the device.
+ * Same arguments and result as zynum_blas_gpu_dgemm_device with the native
+ * method; `splits` > 0 forces that many split-K ranges, 0 lets the planner
+ * choose.  Split-K partial sums go to a fixed 32 MiB device array inside the
+ * library (held on every GPU that loads it until exit), so
+ * splits * m * n must not exceed 4194304; larger requests are rejected with a
+ * negative status and a message in zynum_blas_gpu_last_error().  The first
+ * call on a device looks up that array's device address (make that first call
+ * before any stream capture).  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race on it. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_noalloc_device(char transa, char transb, int m, int n, int k, double alpha,
+                                                           const double *a, int lda, const double *b, int ldb,
+                                                           double beta, double *c, int ldc, int splits, void *stream);
+
 /* -------------------------------------------------------------- control */
 /* 0 = native FP64, 1 = Ozaki INT8 emulation, 2 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);

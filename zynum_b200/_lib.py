@@ -51,6 +51,8 @@ def _declare(L: C.CDLL) -> None:
     L.zynum_blas_gpu_dgemm_device.restype = i
     L.zynum_blas_gpu_sgemm_device.argtypes = [ch, ch, i, i, i, f, P, i, P, i, f, P, i, P]
     L.zynum_blas_gpu_sgemm_device.restype = i
+    L.zynum_blas_gpu_dgemm_noalloc_device.argtypes = [ch, ch, i, i, i, d, P, i, P, i, d, P, i, i, P]
+    L.zynum_blas_gpu_dgemm_noalloc_device.restype = i
     for name in ("zynum_blas_gpu_set_dgemm_method", "zynum_blas_gpu_set_sgemm_method",
                  "zynum_blas_gpu_set_ozaki_slices"):
         getattr(L, name).argtypes = [i]

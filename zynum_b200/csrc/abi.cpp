@@ -200,6 +200,10 @@ inline bool cblas_valid_trans(int t) { return t == CblasNoTrans || t == CblasTra
 
 }  // namespace
 
+int zb::gemm_arg_error(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc) {
+    return gemm_error(ta, tb, m, n, k, lda, ldb, ldc);
+}
+
 extern "C" {
 
 int lsame_(const char* ca, const char* cb) {

@@ -62,6 +62,10 @@ void prof_begin(cudaStream_t st);
 void count_launch();
 void prof_end(cudaStream_t st);
 
+// Fortran GEMM argument check (fortran.zig:88-102 gemmError): 0 or the index
+// of the first illegal argument.  trans characters must already be upper case.
+int gemm_arg_error(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc);
+
 // ---------------------------------------------------------------- planner
 GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count);
 
