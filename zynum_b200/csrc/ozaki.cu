@@ -47,33 +47,41 @@ namespace zb {
 namespace {
 
 // ------------------------------------------------------------ geometry
-constexpr int kUM = 128;        // C rows per tile (TMEM lanes)
-constexpr int kUN = 256;        // C columns per tile (TMEM columns per buffer)
-constexpr int kChunkBytes = 128;  // K bytes per pipeline stage (one 128B swizzle row)
-constexpr int kStages = 4;
-constexpr int kAStage = kUM * kChunkBytes;  // 16 KB
-constexpr int kBStage = kUN * kChunkBytes;  // 32 KB
+constexpr int kUM = 128;          // C rows per tile (TMEM lanes)
+constexpr int kUN = 256;          // C columns per tile (TMEM columns per accumulator)
+constexpr int kChunkBytes = 128;  // K bytes per operand chunk (one 128-byte swizzle row)
+constexpr int kASlots = 4;        // ring of A digit chunks (128 x 128 B each)
+constexpr int kBSlots = 4;        // ring of B digit chunks (256 x 128 B each)
+constexpr int kAChunk = kUM * kChunkBytes;  // 16 KB
+constexpr int kBChunk = kUN * kChunkBytes;  // 32 KB
 constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
-constexpr int kMaxPairs = 96;
-constexpr int kMaxGroups = 16;
-constexpr size_t kSmemBytes = 1024 /*align slack*/ + kStages * (kAStage + kBStage) + 256;
+constexpr int kMaxSteps = 96;
+constexpr int kMaxJobs = 16;
+constexpr size_t kSmemBytes = 1024 /*align slack*/ + kASlots * kAChunk + kBSlots * kBChunk + 256 + kUN * 8;
 
 enum Kind : int { KIND_I8 = 0, KIND_BF16 = 1 };
 enum Epi : int { EPI_OZAKI_F64 = 0, EPI_F32 = 1 };
 
+// Work of one C tile is a list of "group jobs".  A job owns one or two
+// accumulators (TMEM columns [0,256) and [256,512)); it sweeps K chunk by
+// chunk and, for every chunk, walks its steps (digit pairs).  Consecutive
+// steps are ordered so that they share the A or the B digit chunk, which is
+// then loaded once and used twice.
 struct UmmaParams {
-    int m, n;                // C extent
-    int m_pad, n_pad;        // rows per plane of the A / B digit tensors
-    int k_chunks;            // total 128-byte K chunks
-    int kseg_chunks;         // K chunks per accumulation segment
+    int m, n;            // C extent
+    int m_pad, n_pad;    // rows per plane of the A / B digit tensors
+    int k_chunks;        // total K chunks
+    int kseg_chunks;     // K chunks per accumulation segment (INT32 overflow bound)
     int num_kseg;
     int tiles_m, tiles_n, num_tiles;
-    int num_groups;
-    int group_first[kMaxGroups];
-    int group_count[kMaxGroups];
-    int group_shift[kMaxGroups];  // 7 g for Ozaki
-    int pair_a[kMaxPairs];        // digit plane of A
-    int pair_b[kMaxPairs];        // digit plane of B
+    int num_jobs;
+    int job_first_step[kMaxJobs];
+    int job_num_steps[kMaxJobs];
+    int job_groups[kMaxJobs];     // 1 or 2 accumulators
+    int job_shift[kMaxJobs][2];   // 7 g of the group held by accumulator 0 / 1
+    int step_a[kMaxSteps];        // digit plane of A
+    int step_b[kMaxSteps];        // digit plane of B
+    int step_acc[kMaxSteps];      // accumulator 0 / 1
     double alpha, beta;
     float alpha_f, beta_f;
     void* c;
@@ -97,7 +105,7 @@ ZB_DEVICE bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort_fl
 }
 
 ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn) {
-    // Groups of 8 tile-rows sweep the tile-columns, so CTAs running together
+    // Bands of 8 tile-rows sweep the tile-columns, so CTAs running together
     // share A row blocks and B column blocks in L2.
     constexpr int G = 8;
     int band = tile / (G * tiles_n);
@@ -113,6 +121,25 @@ ZB_DEVICE double pow2(int e) {
     return ldexp(1.0, e);
 }
 
+// 2 KB after the barriers: per-tile column scale factors of the epilogue.
+ZB_DEVICE uint8_t* smem_tail_scratch(uint8_t* smem) {
+    return smem + kASlots * kAChunk + kBSlots * kBChunk + 256;
+}
+// Barrier among the four epilogue warps only (named barrier 1, 128 threads).
+ZB_DEVICE void epilogue_bar_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+// Slot ring bookkeeping shared by the producer and the MMA issuer.
+struct Ring {
+    int slot = 0;
+    uint32_t phase = 0;
+    ZB_DEVICE void advance(int n) {
+        if (++slot == n) {
+            slot = 0;
+            phase ^= 1;
+        }
+    }
+};
+
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
 umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -120,24 +147,28 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
-    uint8_t* sB = smem + kStages * kAStage;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + kStages * kBStage);
-    uint64_t* empty = full + kStages;
-    uint64_t* tfull = empty + kStages;
-    uint64_t* tempty = tfull + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint8_t* sB = smem + kASlots * kAChunk;
+    uint64_t* fullA = reinterpret_cast<uint64_t*>(sB + kBSlots * kBChunk);
+    uint64_t* emptyA = fullA + kASlots;
+    uint64_t* fullB = emptyA + kASlots;
+    uint64_t* emptyB = fullB + kBSlots;
+    uint64_t* tfull = emptyB + kBSlots;
+    uint64_t* tempty = tfull + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < kStages; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
+        for (int i = 0; i < kASlots; ++i) {
+            mbar_init(&fullA[i], 1);
+            mbar_init(&emptyA[i], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 4);
+        for (int i = 0; i < kBSlots; ++i) {
+            mbar_init(&fullB[i], 1);
+            mbar_init(&emptyB[i], 1);
         }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 4);
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -158,99 +189,118 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     if (warp == 0) {
         // ------------------------------------------------ TMA producer
         if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
+            Ring ra, rb;
             bool ok = true;
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
                 int tm, tn;
                 tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
-                for (int g = 0; ok && g < P.num_groups; ++g)
+                for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                        const int c0 = ks * P.kseg_chunks;
-                        const int c1 = min(P.k_chunks, c0 + P.kseg_chunks);
-                        for (int q = 0; ok && q < P.group_count[g]; ++q) {
-                            const int pa = P.pair_a[P.group_first[g] + q], pb = P.pair_b[P.group_first[g] + q];
-                            for (int kc = c0; kc < c1; ++kc) {
-                                if (!wait_phase(&empty[stage], phase ^ 1, abort_flag, P.status, 1)) {
-                                    ok = false;
-                                    break;
+                        const int c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        for (int kc = ks * P.kseg_chunks; ok && kc < c1; ++kc) {
+                            int prev_a = -1, prev_b = -1;
+                            for (int q = 0; q < P.job_num_steps[j]; ++q) {
+                                const int st = P.job_first_step[j] + q;
+                                const int pa = P.step_a[st], pb = P.step_b[st];
+                                if (pa != prev_a) {
+                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, P.status, 1)))
+                                        break;
+                                    mbar_arrive_expect_tx(&fullA[ra.slot], kAChunk);
+                                    tma_load_2d(smem_u32(sA + ra.slot * kAChunk), &tmA, &fullA[ra.slot],
+                                                kc * elems_per_chunk, pa * P.m_pad + tm * kUM);
+                                    ra.advance(kASlots);
+                                    prev_a = pa;
                                 }
-                                mbar_arrive_expect_tx(&full[stage], kAStage + kBStage);
-                                tma_load_2d(smem_u32(sA + stage * kAStage), &tmA, &full[stage], kc * elems_per_chunk,
-                                            pa * P.m_pad + tm * kUM);
-                                tma_load_2d(smem_u32(sB + stage * kBStage), &tmB, &full[stage], kc * elems_per_chunk,
-                                            pb * P.n_pad + tn * kUN);
-                                if (++stage == kStages) {
-                                    stage = 0;
-                                    phase ^= 1;
+                                if (pb != prev_b) {
+                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, P.status, 2)))
+                                        break;
+                                    mbar_arrive_expect_tx(&fullB[rb.slot], kBChunk);
+                                    tma_load_2d(smem_u32(sB + rb.slot * kBChunk), &tmB, &fullB[rb.slot],
+                                                kc * elems_per_chunk, pb * P.n_pad + tn * kUN);
+                                    rb.advance(kBSlots);
+                                    prev_b = pb;
                                 }
                             }
                         }
                     }
             }
             // Let every issued copy land before the CTA can retire (bounded).
-            for (int i = 0; i < kStages; ++i) {
-                wait_phase(&empty[stage], phase ^ 1, abort_flag, nullptr, 0);
-                if (++stage == kStages) {
-                    stage = 0;
-                    phase ^= 1;
-                }
+            for (int i = 0; i < kASlots; ++i) {
+                wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, nullptr, 0);
+                ra.advance(kASlots);
+            }
+            for (int i = 0; i < kBSlots; ++i) {
+                wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, nullptr, 0);
+                rb.advance(kBSlots);
             }
         }
     } else if (warp == 1) {
         // ------------------------------------------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, kUM, kUN) : umma_idesc(1, 1, kUM, kUN);
-            int stage = 0;
-            uint32_t phase = 0;
-            int job = 0;
+            Ring ra, rb;
+            uint32_t tphase = 0;
             bool ok = true;
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x)
-                for (int g = 0; ok && g < P.num_groups; ++g)
-                    for (int ks = 0; ok && ks < P.num_kseg; ++ks, ++job) {
-                        const int b = job & 1, use = job >> 1;
-                        if (!wait_phase(&tempty[b], (use & 1) ^ 1, abort_flag, P.status, 2)) {
-                            ok = false;
-                            break;
-                        }
+                for (int j = 0; ok && j < P.num_jobs; ++j)
+                    for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                        // both accumulators must have been drained by the epilogue
+                        if (!(ok = wait_phase(tempty, tphase ^ 1, abort_flag, P.status, 3))) break;
+                        tphase ^= 1;
                         tc_fence_after();
-                        const uint32_t d = tmem_base + b * kUN;
-                        const int c0 = ks * P.kseg_chunks;
-                        const int c1 = min(P.k_chunks, c0 + P.kseg_chunks);
-                        uint32_t acc = 0;
-                        for (int q = 0; ok && q < P.group_count[g]; ++q)
-                            for (int kc = c0; kc < c1; ++kc) {
-                                if (!wait_phase(&full[stage], phase, abort_flag, P.status, 3)) {
-                                    ok = false;
-                                    break;
+                        uint32_t started = 0;  // bit per accumulator
+                        const int c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        const int n_steps = P.job_num_steps[j];
+                        for (int kc = ks * P.kseg_chunks; ok && kc < c1; ++kc) {
+                            int prev_a = -1, prev_b = -1;
+                            int a_slot = 0, b_slot = 0;
+                            for (int q = 0; q < n_steps; ++q) {
+                                const int st = P.job_first_step[j] + q;
+                                const int pa = P.step_a[st], pb = P.step_b[st], acc_i = P.step_acc[st];
+                                if (pa != prev_a) {
+                                    a_slot = ra.slot;
+                                    if (!(ok = wait_phase(&fullA[ra.slot], ra.phase, abort_flag, P.status, 4))) break;
+                                    ra.advance(kASlots);
+                                    prev_a = pa;
+                                }
+                                if (pb != prev_b) {
+                                    b_slot = rb.slot;
+                                    if (!(ok = wait_phase(&fullB[rb.slot], rb.phase, abort_flag, P.status, 5))) break;
+                                    rb.advance(kBSlots);
+                                    prev_b = pb;
                                 }
                                 tc_fence_after();
-                                const uint32_t a0 = smem_u32(sA + stage * kAStage);
-                                const uint32_t b0 = smem_u32(sB + stage * kBStage);
+                                const uint32_t d = tmem_base + acc_i * kUN;
+                                const uint32_t a0 = smem_u32(sA + a_slot * kAChunk);
+                                const uint32_t b0 = smem_u32(sB + b_slot * kBChunk);
 #pragma unroll
                                 for (int kk = 0; kk < kChunkBytes / 32; ++kk) {
                                     const uint64_t ad = umma_desc_sw128(a0 + kk * 32);
                                     const uint64_t bd = umma_desc_sw128(b0 + kk * 32);
+                                    const uint32_t accumulate = (started >> acc_i) & 1u;
                                     if (KIND == KIND_I8)
-                                        umma_i8(d, ad, bd, idesc, acc);
+                                        umma_i8(d, ad, bd, idesc, accumulate);
                                     else
-                                        umma_f16(d, ad, bd, idesc, acc);
-                                    acc = 1;
+                                        umma_f16(d, ad, bd, idesc, accumulate);
+                                    started |= 1u << acc_i;
                                 }
-                                umma_commit(&empty[stage]);
-                                if (++stage == kStages) {
-                                    stage = 0;
-                                    phase ^= 1;
-                                }
+                                // release a chunk after the last step that reads it
+                                const bool last = (q + 1 == n_steps);
+                                if (last || P.step_a[st + 1] != pa) umma_commit(&emptyA[a_slot]);
+                                if (last || P.step_b[st + 1] != pb) umma_commit(&emptyB[b_slot]);
                             }
-                        if (ok) umma_commit(&tfull[b]);
+                        }
+                        if (ok) umma_commit(tfull);
                     }
         }
     } else {
         // ---------------------------------------------- epilogue warps
         const int quarter = warp & 3;  // TMEM lane quarter this warp may access
         const int row_in_tile = quarter * 32 + lane;
-        int job = 0;
+        const int et = threadIdx.x - 64;  // 0..127 among the epilogue threads
+        const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
+        double* colscale = reinterpret_cast<double*>(smem_tail_scratch(smem));  // kUN doubles
+        uint32_t tphase = 0;
         bool ok = true;
         for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
             int tm, tn;
@@ -258,53 +308,75 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const int row = tm * kUM + row_in_tile;
             const bool row_ok = row < P.m;
             int er = 0;
-            if (EPI == EPI_OZAKI_F64 && row_ok) er = P.row_exp[row];
+            if (EPI == EPI_OZAKI_F64) {
+                if (row_ok) er = P.row_exp[row];
+                // 2^{f_j} of this tile's columns, staged once per tile
+                epilogue_bar_sync();  // previous tile's readers are done
+                for (int c = et; c < kUN; c += 128) {
+                    const int col = tn * kUN + c;
+                    colscale[c] = (col < P.n) ? pow2(P.col_exp[col]) : 0.0;
+                }
+                epilogue_bar_sync();
+            }
             bool first = true;
-            for (int g = 0; ok && g < P.num_groups; ++g)
-                for (int ks = 0; ok && ks < P.num_kseg; ++ks, ++job) {
-                    const int b = job & 1, use = job >> 1;
-                    if (!wait_phase(&tfull[b], use & 1, abort_flag, P.status, 4)) {
-                        ok = false;
-                        break;
-                    }
+            for (int j = 0; ok && j < P.num_jobs; ++j)
+                for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                    if (!(ok = wait_phase(tfull, tphase, abort_flag, P.status, 6))) break;
+                    tphase ^= 1;
                     tc_fence_after();
-                    double rowscale = 1.0;
-                    if (EPI == EPI_OZAKI_F64) rowscale = pow2(er - P.group_shift[g]) * P.alpha;
+                    const bool two = P.job_groups[j] == 2;
+                    // accumulator 1 holds group g_a - 1, worth 2^7 times accumulator 0:
+                    // D0 + 128 D1 is exact in int64 and converts exactly to FP64.
+                    const double s0 = (EPI == EPI_OZAKI_F64) ? pow2(er - P.job_shift[j][0]) * P.alpha : 1.0;
 #pragma unroll 1
                     for (int ch = 0; ch < kUN / 32; ++ch) {
-                        uint32_t r[32];
-                        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + b * kUN + ch * 32, r);
+                        uint32_t r0[32], r1[32];
+                        tmem_ld_32x32b_x32(lane_addr + ch * 32, r0);
+                        if (two) tmem_ld_32x32b_x32(lane_addr + kUN + ch * 32, r1);
                         tmem_ld_wait();
                         const int col0 = tn * kUN + ch * 32;
                         if (!row_ok) continue;
+                        const bool full_chunk = col0 + 32 <= P.n;
+                        // Issue all loads of C before any store so their
+                        // round trips overlap.
+                        if (EPI == EPI_OZAKI_F64) {
+                            double* cb = static_cast<double*>(P.c) + (long)col0 * P.ldc + row;
+                            double cin[32];
+                            const bool need_c = !first || P.beta != 0.0;
+                            if (need_c) {
 #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int col = col0 + c;
-                            if (col >= P.n) continue;
-                            if (EPI == EPI_OZAKI_F64) {
-                                double* cp = static_cast<double*>(P.c) + (long)col * P.ldc + row;
-                                const double v = (double)(int)r[c] * rowscale * pow2(P.col_exp[col]);
-                                double out;
-                                if (first)
-                                    out = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
-                                else
-                                    out = *cp + v;
-                                *cp = out;
-                            } else {
-                                float* cp = static_cast<float*>(P.c) + (long)col * P.ldc + row;
-                                const float v = P.alpha_f * __uint_as_float(r[c]);
-                                float out;
-                                if (first)
-                                    out = (P.beta_f == 0.0f) ? v : fmaf(P.beta_f, *cp, v);
-                                else
-                                    out = *cp + v;
-                                *cp = out;
+                                for (int c = 0; c < 32; ++c)
+                                    cin[c] = (full_chunk || col0 + c < P.n) ? __ldcg(cb + (long)c * P.ldc) : 0.0;
+                            }
+                            const double* cs = colscale + ch * 32;
+#pragma unroll
+                            for (int c = 0; c < 32; ++c) {
+                                long long d = (int)r0[c];
+                                if (two) d += (long long)(int)r1[c] << 7;
+                                const double v = (double)d * s0 * cs[c];
+                                const double out = !need_c ? v : (first ? fma(P.beta, cin[c], v) : cin[c] + v);
+                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
+                            }
+                        } else {
+                            float* cb = static_cast<float*>(P.c) + (long)col0 * P.ldc + row;
+                            float cin[32];
+                            const bool need_c = !first || P.beta_f != 0.0f;
+                            if (need_c) {
+#pragma unroll
+                                for (int c = 0; c < 32; ++c)
+                                    cin[c] = (full_chunk || col0 + c < P.n) ? __ldcg(cb + (long)c * P.ldc) : 0.0f;
+                            }
+#pragma unroll
+                            for (int c = 0; c < 32; ++c) {
+                                const float v = P.alpha_f * __uint_as_float(r0[c]);
+                                const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
+                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
                             }
                         }
                     }
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(&tempty[b]);
+                    if (lane == 0) mbar_arrive(tempty);
                     first = false;
                 }
         }
@@ -705,22 +777,31 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     P.tiles_m = p.m_pad / kUM;
     P.tiles_n = p.n_pad / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
-    // groups g = s+1 .. 2 (smallest contributions first), pairs t + u = g
-    int np = 0, ng = 0;
-    for (int gg = p.slices + 1; gg >= 2; --gg) {
-        P.group_first[ng] = np;
+    // Groups g = s+1 .. 2 (smallest contributions first), two per job: the
+    // job's steps walk t upwards emitting (t, g_a - t) then (t, g_b - t), so
+    // consecutive steps share A_t or B_{g_b - t}.
+    int nsteps = 0, njobs = 0;
+    for (int ga = p.slices + 1; ga >= 2; ga -= 2) {
+        const int gb = ga - 1;
+        const bool two = gb >= 2;
+        P.job_first_step[njobs] = nsteps;
+        P.job_groups[njobs] = two ? 2 : 1;
+        P.job_shift[njobs][0] = 7 * ga;
+        P.job_shift[njobs][1] = two ? 7 * gb : 0;
         for (int t = 1; t <= p.slices; ++t) {
-            const int u = gg - t;
-            if (u < 1 || u > p.slices) continue;
-            P.pair_a[np] = t - 1;
-            P.pair_b[np] = u - 1;
-            ++np;
+            for (int h = 0; h < (two ? 2 : 1); ++h) {
+                const int u = (h ? gb : ga) - t;
+                if (u < 1 || u > p.slices) continue;
+                P.step_a[nsteps] = t - 1;
+                P.step_b[nsteps] = u - 1;
+                P.step_acc[nsteps] = h;
+                ++nsteps;
+            }
         }
-        P.group_count[ng] = np - P.group_first[ng];
-        P.group_shift[ng] = 7 * gg;
-        ++ng;
+        P.job_num_steps[njobs] = nsteps - P.job_first_step[njobs];
+        ++njobs;
     }
-    P.num_groups = ng;
+    P.num_jobs = njobs;
     P.alpha = g.alpha;
     P.beta = g.beta;
     P.c = g.c;
@@ -763,14 +844,20 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     P.tiles_m = mp / kUM;
     P.tiles_n = np / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
-    P.num_groups = 1;
-    P.group_first[0] = 0;
-    P.group_count[0] = 3;
-    P.group_shift[0] = 0;
-    // lo*hi, hi*lo first (small), then hi*hi; plane 0 = hi, 1 = lo
-    P.pair_a[0] = 1; P.pair_b[0] = 0;
-    P.pair_a[1] = 0; P.pair_b[1] = 1;
-    P.pair_a[2] = 0; P.pair_b[2] = 0;
+    // one job, one FP32 accumulator: hi*lo, hi*hi, lo*hi (consecutive steps
+    // share an operand); plane 0 = hi, 1 = lo
+    P.num_jobs = 1;
+    P.job_first_step[0] = 0;
+    P.job_num_steps[0] = 3;
+    P.job_groups[0] = 1;
+    P.job_shift[0][0] = 0;
+    P.job_shift[0][1] = 0;
+    const int sa[3] = {0, 0, 1}, sb[3] = {1, 0, 0};
+    for (int q = 0; q < 3; ++q) {
+        P.step_a[q] = sa[q];
+        P.step_b[q] = sb[q];
+        P.step_acc[q] = 0;
+    }
     P.alpha_f = g.alpha;
     P.beta_f = g.beta;
     P.c = g.c;
