@@ -54,6 +54,30 @@ ZYNUM_BLAS_GPU_API void dgemm_(const char *transa, const char *transb, const zyn
             const zynum_blas_int *k, const double *alpha, const double *a, const zynum_blas_int *lda,
             const double *b, const zynum_blas_int *ldb, const double *beta, double *c, const zynum_blas_int *ldc);
 
+/* src/blas/abi/fortran.zig:768 cgemm_ (alpha, beta, a, b, c: interleaved single-precision complex) */
+ZYNUM_BLAS_GPU_API void cgemm_(const char *transa, const char *transb, const zynum_blas_int *m, const zynum_blas_int *n,
+            const zynum_blas_int *k, const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+            const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:772 zgemm_ (interleaved double-precision complex) */
+ZYNUM_BLAS_GPU_API void zgemm_(const char *transa, const char *transb, const zynum_blas_int *m, const zynum_blas_int *n,
+            const zynum_blas_int *k, const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+            const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+
+/* src/blas/abi/fortran.zig:869-883 strsm_ / dtrsm_ (B := alpha op(A)^-1 B or B op(A)^-1) */
+ZYNUM_BLAS_GPU_API void strsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const float *alpha, const float *a,
+                               const zynum_blas_int *lda, float *b, const zynum_blas_int *ldb);
+ZYNUM_BLAS_GPU_API void dtrsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const double *alpha, const double *a,
+                               const zynum_blas_int *lda, double *b, const zynum_blas_int *ldb);
+/* src/blas/abi/fortran.zig:802-809 ssyrk_ / dsyrk_ (C := alpha op(A) op(A)^T + beta C, one triangle) */
+ZYNUM_BLAS_GPU_API void ssyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const float *alpha, const float *a, const zynum_blas_int *lda, const float *beta,
+                               float *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void dsyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const double *alpha, const double *a, const zynum_blas_int *lda, const double *beta,
+                               double *c, const zynum_blas_int *ldc);
+
 /* ---------------------------------------------------------------- CBLAS ABI */
 
 enum CBLAS_LAYOUT { CblasRowMajor = 101, CblasColMajor = 102 };          /* cblas.zig:123-124 */
@@ -68,6 +92,24 @@ ZYNUM_BLAS_GPU_API void cblas_sgemm(int layout, int transa, int transb, int m, i
 /* src/blas/abi/cblas.zig:1428 cblas_dgemm */
 ZYNUM_BLAS_GPU_API void cblas_dgemm(int layout, int transa, int transb, int m, int n, int k, double alpha, const double *a, int lda,
                  const double *b, int ldb, double beta, double *c, int ldc);
+
+/* src/blas/abi/cblas.zig:1441 cblas_cgemm */
+ZYNUM_BLAS_GPU_API void cblas_cgemm(int layout, int transa, int transb, int m, int n, int k, const void *alpha, const void *a,
+                 int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+/* src/blas/abi/cblas.zig:1454 cblas_zgemm */
+ZYNUM_BLAS_GPU_API void cblas_zgemm(int layout, int transa, int transb, int m, int n, int k, const void *alpha, const void *a,
+                 int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+
+/* src/blas/abi/cblas.zig:1729-1756 cblas_strsm / cblas_dtrsm */
+ZYNUM_BLAS_GPU_API void cblas_strsm(int layout, int side, int uplo, int transa, int diag, int m, int n, float alpha,
+                                    const float *a, int lda, float *b, int ldb);
+ZYNUM_BLAS_GPU_API void cblas_dtrsm(int layout, int side, int uplo, int transa, int diag, int m, int n, double alpha,
+                                    const double *a, int lda, double *b, int ldb);
+/* src/blas/abi/cblas.zig:1539-1560 cblas_ssyrk / cblas_dsyrk */
+ZYNUM_BLAS_GPU_API void cblas_ssyrk(int layout, int uplo, int trans, int n, int k, float alpha, const float *a,
+                                    int lda, float beta, float *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_dsyrk(int layout, int uplo, int trans, int n, int k, double alpha, const double *a,
+                                    int lda, double beta, double *c, int ldc);
 
 /* ------------------------------------------------------ GPU device entry points
  * Added by the GPU backend (no counterpart in the reference's ABI; the planned
@@ -99,7 +141,32 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_noalloc_device(char transa, char tra
                                                            const double *a, int lda, const double *b, int ldb,
                                                            double beta, double *c, int ldc, int splits, void *stream);
 
+/* Complex GEMM through real GEMMs (expanded-real 4M or 3M, zynum_blas_gpu_set_complex_method);
+ * alpha / beta point to HOST (re, im) pairs, matrices are device pointers. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zgemm_device(char transa, char transb, int m, int n, int k, const double *alpha,
+                                                   const double *a, int lda, const double *b, int ldb,
+                                                   const double *beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_cgemm_device(char transa, char transb, int m, int n, int k, const float *alpha,
+                                                   const float *a, int lda, const float *b, int ldb, const float *beta,
+                                                   float *c, int ldc, void *stream);
+
+/* TRSM on device pointers: blocked, inverted 64 x 64 diagonal blocks + GEMM updates
+ * (the GEMMs follow the DGEMM / SGEMM method).  Argument numbering as dtrsm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrsm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   double alpha, const double *a, int lda, double *b, int ldb,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_strsm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   float alpha, const float *a, int lda, float *b, int ldb,
+                                                   void *stream);
+/* SYRK on device pointers: the native GEMM tiles in triangle mode.  Argument numbering as dsyrk_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alpha, const double *a,
+                                                   int lda, double beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
+                                                   int lda, float beta, float *c, int ldc, void *stream);
+
 /* -------------------------------------------------------------- control */
+/* 0 = expanded-real 4M (one real GEMM of 2m x n x 2k), 1 = 3M (three real GEMMs). Returns the previous value. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_complex_method(int method);
 /* 0 = native FP64, 1 = Ozaki INT8 emulation, 2 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);
 /* 0 = native FP32, 1 = 3xBF16 split product. Returns the previous value. */

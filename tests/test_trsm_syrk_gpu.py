@@ -1,0 +1,128 @@
+"""TRSM and SYRK on the GEMM tiles against the CPU oracle (GPU).
+
+TRSM mirrors src/blas/triangular_parallel_test.zig (every side / uplo / trans /
+diag) with sizes that cross several 64-row diagonal blocks, padded leading
+dimensions and alpha != 1; the bound is |X - X_ref| <= 1e-11 (1 + |X_ref|)
+for the well-conditioned triangles used (diagonal 2 + |N(0,1)|).
+SYRK mirrors symmetric.zig:180-199: only the chosen triangle changes (the
+other one must stay bit-identical), bound 4 k u (|alpha| |A||A^T| + |beta| |C|).
+"""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _tri_matrix(rng, n, ld, dtype):
+    a = rng.standard_normal((ld, n)) * 0.3
+    for i in range(n):
+        a[i, i] = 2.0 + abs(a[i, i])
+    a[n:] = -999.0
+    return np.asfortranarray(a.astype(dtype))
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", list(itertools.product("LR", "UL", "NT", "NU")))
+def test_dtrsm_all_cases(blas, oracle, side, uplo, trans, diag):
+    rng = np.random.default_rng(abs(hash((side, uplo, trans, diag))) % 2**32)
+    m, n = (150, 37) if side == "L" else (37, 150)
+    na = m if side == "L" else n
+    lda, ldb = na + 3, m + 2
+    a = _tri_matrix(rng, na, lda, np.float64)
+    b = np.asfortranarray(rng.standard_normal((ldb, n)))
+    b[m:] = -999.0
+    b0 = b.copy(order="F")
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, trans, diag, m, n, 0.75, a, lda, ref, ldb)
+    blas.trsm(side, uplo, trans, diag, m, n, 0.75, a, lda, b, ldb)
+    err = np.abs(b[:m] - ref[:m])
+    assert np.all(err <= 1e-11 * (1 + np.abs(ref[:m]))), float(err.max())
+    assert np.array_equal(b[m:], b0[m:])
+
+
+@pytest.mark.parametrize("side,uplo", [("L", "L"), ("R", "U")])
+def test_strsm(blas, oracle, side, uplo):
+    rng = np.random.default_rng(2)
+    m, n = (130, 20) if side == "L" else (20, 130)
+    na = m if side == "L" else n
+    a = _tri_matrix(rng, na, na, np.float32)
+    b = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, "N", "N", m, n, 1.0, a, na, ref, m)
+    blas.trsm(side, uplo, "N", "N", m, n, 1.0, a, na, b, m)
+    assert np.all(np.abs(b - ref) <= 2e-4 * (1 + np.abs(ref)))
+
+
+def test_dtrsm_differentiation_shape(blas, oracle):
+    """L lower with off-diagonals N(0, 1/n), diagonal 1 + |N(0,1)| (the chain's TRSM), n = 512, 64 RHS."""
+    rng = np.random.default_rng(11)
+    n, r = 512, 64
+    L = np.tril(rng.standard_normal((n, n)) / np.sqrt(n), -1) + np.diag(1 + np.abs(rng.standard_normal(n)))
+    L = np.asfortranarray(L)
+    B = np.asfortranarray(rng.standard_normal((n, r)))
+    ref = B.copy(order="F")
+    oracle.trsm("L", "L", "N", "N", n, r, 1.0, L, n, ref, n)
+    blas.trsm("L", "L", "N", "N", n, r, 1.0, L, n, B, n)
+    assert np.abs(B - ref).max() <= 1e-11 * (1 + np.abs(ref).max())
+
+
+def test_cblas_dtrsm_row_major(blas):
+    rng = np.random.default_rng(3)
+    m, n = 70, 90
+    A = np.tril(rng.standard_normal((m, m)) * 0.3) + np.diag(2 + np.abs(rng.standard_normal(m)))
+    B = rng.standard_normal((m, n))
+    want = np.linalg.solve(A, 0.5 * B)
+    a = np.ascontiguousarray(A)
+    b = np.ascontiguousarray(B)
+    blas.cblas_dtrsm(blas.CblasRowMajor, blas.CblasLeft, blas.CblasLower, blas.CblasNoTrans, blas.CblasNonUnit,
+                     m, n, 0.5, a, m, b, n)
+    assert np.abs(b - want).max() <= 1e-11 * (1 + np.abs(want).max())
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("uplo,trans", list(itertools.product("UL", "NT")))
+def test_syrk(blas, oracle, dtype, uplo, trans):
+    rng = np.random.default_rng(5)
+    n, k = 150, 77
+    lda = (n if trans == "N" else k) + 2
+    ldc = n + 3
+    a = np.asfortranarray(rng.uniform(-1, 1, (lda, k if trans == "N" else n)).astype(dtype))
+    c = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)).astype(dtype))
+    c[n:] = -777.0
+    c0 = c.copy(order="F")
+    ref = c.copy(order="F")
+    oracle.syrk(uplo, trans, n, k, 1.5, a, lda, 0.5, ref, ldc)
+    blas.syrk(uplo, trans, n, k, 1.5, a, lda, 0.5, c, ldc)
+    opA = (a[:n, :k] if trans == "N" else a[:k, :n].T).astype(np.float64)
+    u = 2.0 ** -53 if dtype == np.float64 else 2.0 ** -24
+    bound = 4 * k * u * (1.5 * np.abs(opA) @ np.abs(opA).T + 0.5 * np.abs(c0[:n, :n]))
+    mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    err = np.abs(c[:n, :n].astype(np.float64) - ref[:n, :n])
+    assert np.all(err[mask] <= bound[mask])
+    assert np.array_equal(c[:n, :n][~mask], c0[:n, :n][~mask]), "the other triangle changed"
+    assert np.array_equal(c[n:], c0[n:])
+
+
+def test_syrk_k_zero_and_split(blas, oracle):
+    rng = np.random.default_rng(6)
+    n = 40
+    c = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    ref = c.copy(order="F")
+    a = np.zeros((n, 1), order="F")
+    oracle.syrk("L", "N", n, 0, 1.0, a, n, 2.0, ref, n)
+    blas.syrk("L", "N", n, 0, 1.0, a, n, 2.0, c, n)
+    assert np.array_equal(c, ref)
+    # long K, few tiles: split-K with the triangle mask in the reduction
+    n, k = 96, 30000
+    a = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    c = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    c0 = c.copy(order="F")
+    ref = c.copy(order="F")
+    oracle.syrk("U", "T", n, k, 1.0, a, k, -1.0, ref, n)
+    blas.syrk("U", "T", n, k, 1.0, a, k, -1.0, c, n)
+    mask = np.triu(np.ones((n, n), bool))
+    assert np.abs(c - ref)[mask].max() <= 4 * k * 2.0 ** -53 * (np.abs(a).T @ np.abs(a) + 1)[mask].max()
+    assert np.array_equal(c[~mask], c0[~mask])

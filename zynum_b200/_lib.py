@@ -47,6 +47,34 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, name).restype = None
     L.cblas_dgemm.argtypes = [i, i, i, i, i, i, d, P, i, P, i, d, P, i]
     L.cblas_sgemm.argtypes = [i, i, i, i, i, i, f, P, i, P, i, f, P, i]
+    for name in ("cgemm_", "zgemm_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("cblas_cgemm", "cblas_zgemm"):
+        getattr(L, name).argtypes = [i, i, i, i, i, i, P, P, i, P, i, P, P, i]
+        getattr(L, name).restype = None
+    for name in ("zynum_blas_gpu_zgemm_device", "zynum_blas_gpu_cgemm_device"):
+        getattr(L, name).argtypes = [ch, ch, i, i, i, P, P, i, P, i, P, P, i, P]
+        getattr(L, name).restype = i
+    for name, T in (("dtrsm_", d), ("strsm_", f)):
+        getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("dsyrk_", "ssyrk_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    L.cblas_dtrsm.argtypes = [i, i, i, i, i, i, i, d, P, i, P, i]
+    L.cblas_strsm.argtypes = [i, i, i, i, i, i, i, f, P, i, P, i]
+    L.cblas_dsyrk.argtypes = [i, i, i, i, i, d, P, i, d, P, i]
+    L.cblas_ssyrk.argtypes = [i, i, i, i, i, f, P, i, f, P, i]
+    L.zynum_blas_gpu_dtrsm_device.argtypes = [ch, ch, ch, ch, i, i, d, P, i, P, i, P]
+    L.zynum_blas_gpu_strsm_device.argtypes = [ch, ch, ch, ch, i, i, f, P, i, P, i, P]
+    L.zynum_blas_gpu_dsyrk_device.argtypes = [ch, ch, i, i, d, P, i, d, P, i, P]
+    L.zynum_blas_gpu_ssyrk_device.argtypes = [ch, ch, i, i, f, P, i, f, P, i, P]
+    for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
+                 "zynum_blas_gpu_ssyrk_device"):
+        getattr(L, name).restype = i
+    L.zynum_blas_gpu_set_complex_method.argtypes = [i]
+    L.zynum_blas_gpu_set_complex_method.restype = i
     L.zynum_blas_gpu_dgemm_device.argtypes = [ch, ch, i, i, i, d, P, i, P, i, d, P, i, P]
     L.zynum_blas_gpu_dgemm_device.restype = i
     L.zynum_blas_gpu_sgemm_device.argtypes = [ch, ch, i, i, i, f, P, i, P, i, f, P, i, P]

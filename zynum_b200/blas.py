@@ -71,6 +71,75 @@ def cblas_sgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
     return c
 
 
+def _cscalar(dtype, v):
+    return np.array([complex(v)], dtype=dtype)
+
+
+def zgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran zgemm_ on complex128 host arrays (in-place on c)."""
+    al, be = _cscalar(np.complex128, alpha), _cscalar(np.complex128, beta)
+    load().zgemm_(_ch(transa), _ch(transb), _i(m), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+                  _i(ldb), be.ctypes.data, _ptr(c), _i(ldc))
+    return c
+
+
+def cgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    al, be = _cscalar(np.complex64, alpha), _cscalar(np.complex64, beta)
+    load().cgemm_(_ch(transa), _ch(transb), _i(m), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+                  _i(ldb), be.ctypes.data, _ptr(c), _i(ldc))
+    return c
+
+
+def cblas_zgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    al, be = _cscalar(np.complex128, alpha), _cscalar(np.complex128, beta)
+    load().cblas_zgemm(layout, transa, transb, m, n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data,
+                       _ptr(c), ldc)
+    return c
+
+
+def cblas_cgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    al, be = _cscalar(np.complex64, alpha), _cscalar(np.complex64, beta)
+    load().cblas_cgemm(layout, transa, transb, m, n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data,
+                       _ptr(c), ldc)
+    return c
+
+
+def trsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """Fortran dtrsm_ / strsm_ on host arrays (dtype from b; in-place on b)."""
+    L = load()
+    fn, dt = (L.dtrsm_, np.float64) if b.dtype == np.float64 else (L.strsm_, np.float32)
+    al = np.array([alpha], dt)
+    fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+       _i(ldb))
+    return b
+
+
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """Fortran dsyrk_ / ssyrk_ on host arrays (dtype from c; in-place on c's triangle)."""
+    L = load()
+    fn, dt = (L.dsyrk_, np.float64) if c.dtype == np.float64 else (L.ssyrk_, np.float32)
+    al, be = np.array([alpha], dt), np.array([beta], dt)
+    fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), be.ctypes.data, _ptr(c), _i(ldc))
+    return c
+
+
+def cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    load().cblas_dtrsm(layout, side, uplo, transa, diag, m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb)
+    return b
+
+
+def cblas_dsyrk(layout, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    load().cblas_dsyrk(layout, uplo, trans, n, k, float(alpha), _ptr(a), lda, float(beta), _ptr(c), ldc)
+    return c
+
+
+def set_complex_method(method: int) -> int:
+    return load().zynum_blas_gpu_set_complex_method(method)
+
+
+COMPLEX_4M, COMPLEX_3M = 0, 1
+
+
 def _stream(stream=None) -> int:
     if stream is not None:
         return int(stream)
@@ -90,6 +159,37 @@ def sgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, s
     st = load().zynum_blas_gpu_sgemm_device(_ch(transa), _ch(transb), m, n, k, float(alpha), _ptr(a), lda,
                                             _ptr(b), ldb, float(beta), _ptr(c), ldc, _stream(stream))
     check(st, "zynum_blas_gpu_sgemm_device")
+    return c
+
+
+def zgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    """Device zgemm on complex128 torch CUDA tensors (alpha / beta are Python numbers)."""
+    al, be = _cscalar(np.complex128, alpha), _cscalar(np.complex128, beta)
+    st = load().zynum_blas_gpu_zgemm_device(_ch(transa), _ch(transb), m, n, k, al.ctypes.data, _ptr(a), lda,
+                                            _ptr(b), ldb, be.ctypes.data, _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_zgemm_device")
+    return c
+
+
+def cgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    al, be = _cscalar(np.complex64, alpha), _cscalar(np.complex64, beta)
+    st = load().zynum_blas_gpu_cgemm_device(_ch(transa), _ch(transb), m, n, k, al.ctypes.data, _ptr(a), lda,
+                                            _ptr(b), ldb, be.ctypes.data, _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_cgemm_device")
+    return c
+
+
+def dtrsm_device(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream=None):
+    st = load().zynum_blas_gpu_dtrsm_device(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, float(alpha),
+                                            _ptr(a), lda, _ptr(b), ldb, _stream(stream))
+    check(st, "zynum_blas_gpu_dtrsm_device")
+    return b
+
+
+def dsyrk_device(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
+    st = load().zynum_blas_gpu_dsyrk_device(_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, float(beta),
+                                            _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_dsyrk_device")
     return c
 
 

@@ -16,7 +16,9 @@
 
 #include "../../include/zynum_blas_gpu.h"
 #include "kernels.h"
+#include "complex.h"
 #include "ozaki.h"
+#include "trsm_syrk.h"
 #include "runtime.h"
 
 using namespace zb;
@@ -187,6 +189,353 @@ void host_gemm(const char* routine, char ta, char tb, int m, int n, int k, T alp
     }
 }
 
+// ---------------------------------------------------------------- complex
+// Scratch the real GEMM of run_dgemm / run_sgemm would request for this shape.
+size_t real_scratch_bytes(int m, int n, int k, double*) {
+    Context& cx = context();
+    int method = cx.dgemm_method;
+    if (method == METHOD_AUTO) method = ozaki_preferred(m, n, k) ? METHOD_OZAKI : METHOD_NATIVE;
+    if (method == METHOD_OZAKI) return ozaki_workspace_bytes(plan_ozaki(m, n, k, cx.ozaki_slices));
+    GemmPlan p = plan_native_gemm(m, n, k, 8, cx.sm_count);
+    return splitk_workspace_elems(m, n, p.splits) * sizeof(double);
+}
+size_t real_scratch_bytes(int m, int n, int k, float*) {
+    Context& cx = context();
+    if (cx.sgemm_method == SMETHOD_BF16X3) return bf16x3_workspace_bytes(m, n, k);
+    GemmPlan p = plan_native_gemm(m, n, k, 4, cx.sm_count);
+    return splitk_workspace_elems(m, n, p.splits) * sizeof(float);
+}
+
+// A fixed region handed to the real GEMMs of a complex call.
+struct FixedScratch {
+    void* base;
+    size_t cap;
+    cudaError_t operator()(size_t bytes, cudaStream_t, void** out) {
+        if (bytes > cap) return cudaErrorInvalidValue;
+        *out = base;
+        return cudaSuccess;
+    }
+};
+
+cudaError_t run_real(const GemmArgsF64& g, cudaStream_t st, FixedScratch s) { return run_dgemm(g, st, s); }
+cudaError_t run_real(const GemmArgsF32& g, cudaStream_t st, FixedScratch s) { return run_sgemm(g, st, s); }
+
+cudaError_t scale_complex(int m, int n, const double* beta, double* c, long ldc, cudaStream_t st) {
+    return scale_matrix_z(m, n, beta, c, ldc, st);
+}
+cudaError_t scale_complex(int m, int n, const float* beta, float* c, long ldc, cudaStream_t st) {
+    return scale_matrix_c(m, n, beta, c, ldc, st);
+}
+
+// Device-pointer complex GEMM on `st`; arguments validated, m, n > 0.
+template <typename T, typename Scratch>
+cudaError_t run_complex(const ComplexArgs<T>& g, cudaStream_t st, Scratch scratch) {
+    Context& cx = context();
+    if (g.k == 0 || (g.alpha[0] == T(0) && g.alpha[1] == T(0)))
+        return scale_complex(g.m, g.n, g.beta, g.c, g.ldc, st);
+    const int method = cx.complex_method;
+    const size_t planes = complex_plane_bytes<T>(method, g.m, g.n, g.k);
+    const size_t real = (method == COMPLEX_3M) ? real_scratch_bytes(g.m, g.n, g.k, (T*)nullptr)
+                                               : real_scratch_bytes(2 * g.m, g.n, 2 * g.k, (T*)nullptr);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    RealGemm<T> rg = [&](int m, int n, int k, const T* a, long lda, const T* b, long ldb, T* c, long ldc) {
+        GemmArgs<T> rgs{'N', 'N', m, n, k, T(1), a, lda, b, ldb, T(0), c, ldc};
+        return run_real(rgs, st, fs);
+    };
+    return complex_gemm<T>(g, method, ws, rg, st);
+}
+
+// Host-pointer complex GEMM: stage -> compute -> copy the C window back.
+template <typename T>
+void host_complex_gemm(const char* routine, char ta, char tb, int m, int n, int k, const T* alpha, const T* a,
+                       int lda, const T* b, int ldb, const T* beta, T* c, int ldc) {
+    if (m <= 0 || n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const bool quick = (k == 0 || (alpha[0] == T(0) && alpha[1] == T(0)));
+    const bool beta0 = (beta[0] == T(0) && beta[1] == T(0));
+    const int ra = (ta == 'N') ? m : k, ca = (ta == 'N') ? k : m;
+    const int rb = (tb == 'N') ? k : n, cb = (tb == 'N') ? n : k;
+    const size_t es = 2 * sizeof(T);
+    if (!quick) {
+        if ((e = cx.reserve(cx.stage_a, (size_t)ra * ca * es, st)) != cudaSuccess ||
+            (e = cx.reserve(cx.stage_b, (size_t)rb * cb * es, st)) != cudaSuccess) {
+            cuda_status(e, "staging reservation");
+            report_gpu_failure(routine);
+            return;
+        }
+    }
+    if ((e = cx.reserve(cx.stage_c, (size_t)m * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* db = static_cast<T*>(cx.stage_b.ptr);
+    T* dc = static_cast<T*>(cx.stage_c.ptr);
+    if (!quick) {
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(db, (size_t)rb * es, b, (size_t)ldb * es, (size_t)rb * es, cb, cudaMemcpyHostToDevice,
+                                  st);
+    }
+    if (e == cudaSuccess && !beta0)
+        e = cudaMemcpy2DAsync(dc, (size_t)m * es, c, (size_t)ldc * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        ComplexArgs<T> g{ta, tb, m, n, k, {alpha[0], alpha[1]}, da, ra, db, rb, {beta[0], beta[1]}, dc, m};
+        e = run_complex(g, st, HostScratch{&cx});
+    }
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)m * es, (size_t)m * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+template <typename T>
+int device_complex_gemm(const char* what, char transa, char transb, int m, int n, int k, const T* alpha, const T* a,
+                        int lda, const T* b, int ldb, const T* beta, T* c, int ldc, void* stream) {
+    const char ta = up(&transa), tb = up(&transb);
+    int info = gemm_error(ta, tb, m, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    ComplexArgs<T> g{ta, tb, m, n, k, {alpha[0], alpha[1]}, a, lda, b, ldb, {beta[0], beta[1]}, c, ldc};
+    return cuda_status(run_complex(g, static_cast<cudaStream_t>(stream), StreamScratch{&cx}), what);
+}
+
+// ------------------------------------------------------------ TRSM / SYRK
+inline bool valid_uplo(char c) { return c == 'U' || c == 'L'; }
+inline bool valid_diag(char c) { return c == 'N' || c == 'U'; }
+inline bool valid_side(char c) { return c == 'L' || c == 'R'; }
+
+// fortran.zig:105-118 triangularMatrixError
+int trsm_error(char side, char uplo, char trans, char diag, int m, int n, int lda, int ldb) {
+    if (!valid_side(side)) return 1;
+    if (!valid_uplo(uplo)) return 2;
+    if (!valid_trans(trans)) return 3;
+    if (!valid_diag(diag)) return 4;
+    if (m < 0) return 5;
+    if (n < 0) return 6;
+    const int nrowa = (side == 'L') ? m : n;
+    if (lda < max1(nrowa)) return 9;
+    if (ldb < max1(m)) return 11;
+    return 0;
+}
+
+// fortran.zig:252-263 rankKMatrixError
+int syrk_error(char uplo, char trans, int n, int k, int lda, int ldc) {
+    if (!valid_uplo(uplo)) return 1;
+    if (!valid_trans(trans)) return 2;
+    if (n < 0) return 3;
+    if (k < 0) return 4;
+    const int nrowa = (trans == 'N') ? n : k;
+    if (lda < max1(nrowa)) return 7;
+    if (ldc < max1(n)) return 10;
+    return 0;
+}
+
+// GEMMs inside TRSM: the real GEMM route with a fixed scratch region.
+template <typename T>
+GemmFn<T> gemm_fn(cudaStream_t st, FixedScratch* fs) {
+    return [st, fs](const GemmArgs<T>& g) -> cudaError_t {
+        if (g.m <= 0 || g.n <= 0) return cudaSuccess;
+        return run_real(g, st, *fs);
+    };
+}
+
+template <typename T, typename Scratch>
+cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
+    if (t.m <= 0 || t.n <= 0) return cudaSuccess;
+    const size_t planes = trsm_plane_bytes<T>(t.side, t.m, t.n);
+    // largest GEMM of the solve: the first trailing update
+    const int big_m = (t.side == 'L') ? t.m : t.m, big_n = (t.side == 'L') ? t.n : t.n;
+    const size_t real = real_scratch_bytes(big_m, big_n, 64, (T*)nullptr);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return trsm<T>(t, ws, gemm_fn<T>(st, &fs), st);
+}
+
+template <typename T, typename Scratch>
+cudaError_t run_syrk(char uplo, char trans, int n, int k, T alpha, const T* a, long lda, T beta, T* c, long ldc,
+                     cudaStream_t st, Scratch scratch) {
+    if (n <= 0) return cudaSuccess;
+    if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
+    Context& cx = context();
+    GemmArgs<T> g{trans == 'N' ? 'N' : 'T', trans == 'N' ? 'T' : 'N', n, n, k, alpha, a, lda, a, lda, beta, c, ldc};
+    g.tri = (uplo == 'U') ? 1 : 2;
+    GemmPlan p = plan_native_gemm(n, n, k, sizeof(T), cx.sm_count);
+    void* ws = nullptr;
+    const size_t need = splitk_workspace_elems(n, n, p.splits) * sizeof(T);
+    if (need) {
+        cudaError_t e = scratch(need, st, &ws);
+        if (e != cudaSuccess) return e;
+    }
+    if constexpr (sizeof(T) == 8)
+        return dgemm_native(g, p, static_cast<double*>(ws), st);
+    else
+        return sgemm_native(g, p, static_cast<float*>(ws), st);
+}
+
+template <typename T>
+void host_trsm(const char* routine, char side, char uplo, char trans, char diag, int m, int n, T alpha, const T* a,
+               int lda, T* b, int ldb) {
+    if (m <= 0 || n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const int na = (side == 'L') ? m : n;
+    const size_t es = sizeof(T);
+    if ((e = cx.reserve(cx.stage_a, (size_t)na * na * es, st)) != cudaSuccess ||
+        (e = cx.reserve(cx.stage_b, (size_t)m * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* db = static_cast<T*>(cx.stage_b.ptr);
+    e = cudaMemcpy2DAsync(da, (size_t)na * es, a, (size_t)lda * es, (size_t)na * es, na, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(db, (size_t)m * es, b, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = run_trsm(TrsmArgs<T>{side, uplo, trans, diag, m, n, alpha, da, na, db, m}, st,
+                                       HostScratch{&cx});
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(b, (size_t)ldb * es, db, (size_t)m * es, (size_t)m * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+template <typename T>
+void host_syrk(const char* routine, char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T beta, T* c,
+               int ldc) {
+    if (n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const int ra = (trans == 'N') ? n : k, ca = (trans == 'N') ? k : n;
+    const size_t es = sizeof(T);
+    if ((k > 0 && (e = cx.reserve(cx.stage_a, (size_t)ra * ca * es, st)) != cudaSuccess) ||
+        (e = cx.reserve(cx.stage_c, (size_t)n * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* dc = static_cast<T*>(cx.stage_c.ptr);
+    e = cudaSuccess;
+    if (k > 0)
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice,
+                              st);
+    // C is copied in whole so the other triangle comes back bit-identical
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dc, (size_t)n * es, c, (size_t)ldc * es, (size_t)n * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = run_syrk<T>(uplo, trans, n, k, alpha, da, ra, beta, dc, n, st, HostScratch{&cx});
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)n * es, (size_t)n * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+template <typename T>
+int device_trsm(const char* what, char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
+                int lda, T* b, int ldb, void* stream) {
+    const char sd = up(&side), ul = up(&uplo), tr = up(&transa), dg = up(&diag);
+    int info = trsm_error(sd, ul, tr, dg, m, n, lda, ldb);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_trsm(TrsmArgs<T>{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb},
+                                static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+                       what);
+}
+
+template <typename T>
+int device_syrk(const char* what, char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T beta, T* c,
+                int ldc, void* stream) {
+    const char ul = up(&uplo), tr = up(&trans);
+    int info = syrk_error(ul, tr, n, k, lda, ldc);
+    if (info) return info;
+    if (n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(
+        run_syrk<T>(ul, tr, n, k, alpha, a, lda, beta, c, ldc, static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+        what);
+}
+
+inline char cblas_uplo_char(int u) { return u == CblasUpper ? 'U' : (u == CblasLower ? 'L' : 'X'); }
+inline char cblas_row_uplo_char(int u) { return u == CblasUpper ? 'L' : (u == CblasLower ? 'U' : 'X'); }
+inline char cblas_side_char(int s) { return s == CblasLeft ? 'L' : (s == CblasRight ? 'R' : 'X'); }
+inline char cblas_row_side_char(int s) { return s == CblasLeft ? 'R' : (s == CblasRight ? 'L' : 'X'); }
+inline char cblas_diag_char(int d) { return d == CblasNonUnit ? 'N' : (d == CblasUnit ? 'U' : 'X'); }
+inline char cblas_row_trans_char(int t) {
+    return t == CblasNoTrans ? 'T' : (t == CblasTrans ? 'N' : (t == CblasConjTrans ? 'C' : 'X'));
+}
+
 inline char cblas_trans_char(int t) {
     switch (t) {
         case CblasNoTrans: return 'N';
@@ -263,6 +612,165 @@ void cblas_dgemm(int layout, int transa, int transb, int m, int n, int k, double
         dgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, b, &la, a, &lb, &beta, c, &lc);
     else
         dgemm_(&ta, &tb, &mm, &nn, &kk, &alpha, a, &la, b, &lb, &beta, c, &lc);
+}
+
+void cgemm_(const char* transa, const char* transb, const zynum_blas_int* m, const zynum_blas_int* n,
+            const zynum_blas_int* k, const void* alpha, const void* a, const zynum_blas_int* lda, const void* b,
+            const zynum_blas_int* ldb, const void* beta, void* c, const zynum_blas_int* ldc) {
+    const char ta = up(transa), tb = up(transb);
+    int info = gemm_error(ta, tb, *m, *n, *k, *lda, *ldb, *ldc);
+    if (info) {
+        report_xerbla("CGEMM ", info);
+        return;
+    }
+    host_complex_gemm<float>("CGEMM", ta, tb, *m, *n, *k, static_cast<const float*>(alpha),
+                             static_cast<const float*>(a), *lda, static_cast<const float*>(b), *ldb,
+                             static_cast<const float*>(beta), static_cast<float*>(c), *ldc);
+}
+
+void zgemm_(const char* transa, const char* transb, const zynum_blas_int* m, const zynum_blas_int* n,
+            const zynum_blas_int* k, const void* alpha, const void* a, const zynum_blas_int* lda, const void* b,
+            const zynum_blas_int* ldb, const void* beta, void* c, const zynum_blas_int* ldc) {
+    const char ta = up(transa), tb = up(transb);
+    int info = gemm_error(ta, tb, *m, *n, *k, *lda, *ldb, *ldc);
+    if (info) {
+        report_xerbla("ZGEMM ", info);
+        return;
+    }
+    host_complex_gemm<double>("ZGEMM", ta, tb, *m, *n, *k, static_cast<const double*>(alpha),
+                              static_cast<const double*>(a), *lda, static_cast<const double*>(b), *ldb,
+                              static_cast<const double*>(beta), static_cast<double*>(c), *ldc);
+}
+
+// cblas.zig:1441-1465: complex alpha / beta by pointer, same row-major swap.
+void cblas_cgemm(int layout, int transa, int transb, int m, int n, int k, const void* alpha, const void* a, int lda,
+                 const void* b, int ldb, const void* beta, void* c, int ldc) {
+    if (!cblas_valid_layout(layout) || !cblas_valid_trans(transa) || !cblas_valid_trans(transb)) return;
+    const bool rm = layout == CblasRowMajor;
+    char ta = cblas_trans_char(rm ? transb : transa), tb = cblas_trans_char(rm ? transa : transb);
+    zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, kk = k, la = rm ? ldb : lda, lb = rm ? lda : ldb, lc = ldc;
+    if (rm)
+        cgemm_(&ta, &tb, &mm, &nn, &kk, alpha, b, &la, a, &lb, beta, c, &lc);
+    else
+        cgemm_(&ta, &tb, &mm, &nn, &kk, alpha, a, &la, b, &lb, beta, c, &lc);
+}
+
+void cblas_zgemm(int layout, int transa, int transb, int m, int n, int k, const void* alpha, const void* a, int lda,
+                 const void* b, int ldb, const void* beta, void* c, int ldc) {
+    if (!cblas_valid_layout(layout) || !cblas_valid_trans(transa) || !cblas_valid_trans(transb)) return;
+    const bool rm = layout == CblasRowMajor;
+    char ta = cblas_trans_char(rm ? transb : transa), tb = cblas_trans_char(rm ? transa : transb);
+    zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, kk = k, la = rm ? ldb : lda, lb = rm ? lda : ldb, lc = ldc;
+    if (rm)
+        zgemm_(&ta, &tb, &mm, &nn, &kk, alpha, b, &la, a, &lb, beta, c, &lc);
+    else
+        zgemm_(&ta, &tb, &mm, &nn, &kk, alpha, a, &la, b, &lb, beta, c, &lc);
+}
+
+int zynum_blas_gpu_zgemm_device(char transa, char transb, int m, int n, int k, const double* alpha, const double* a,
+                                int lda, const double* b, int ldb, const double* beta, double* c, int ldc,
+                                void* stream) {
+    return device_complex_gemm<double>("zgemm_device", transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                                       stream);
+}
+
+int zynum_blas_gpu_cgemm_device(char transa, char transb, int m, int n, int k, const float* alpha, const float* a,
+                                int lda, const float* b, int ldb, const float* beta, float* c, int ldc, void* stream) {
+    return device_complex_gemm<float>("cgemm_device", transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                                      stream);
+}
+
+int zynum_blas_gpu_set_complex_method(int method) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.complex_method;
+    if (method == COMPLEX_4M || method == COMPLEX_3M) cx.complex_method = method;
+    return old;
+}
+
+// fortran.zig:869-883 ?trsm_, :802-816 ?syrk_
+#define ZB_TRSM(NAME, T, RNAME)                                                                                    \
+    void NAME(const char* side, const char* uplo, const char* transa, const char* diag, const zynum_blas_int* m,  \
+              const zynum_blas_int* n, const T* alpha, const T* a, const zynum_blas_int* lda, T* b,               \
+              const zynum_blas_int* ldb) {                                                                        \
+        const char sd = up(side), ul = up(uplo), tr = up(transa), dg = up(diag);                                   \
+        int info = trsm_error(sd, ul, tr, dg, *m, *n, *lda, *ldb);                                                 \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        host_trsm<T>(RNAME, sd, ul, tr, dg, *m, *n, *alpha, a, *lda, b, *ldb);                                     \
+    }
+ZB_TRSM(dtrsm_, double, "DTRSM ")
+ZB_TRSM(strsm_, float, "STRSM ")
+#undef ZB_TRSM
+
+#define ZB_SYRK(NAME, T, RNAME)                                                                                     \
+    void NAME(const char* uplo, const char* trans, const zynum_blas_int* n, const zynum_blas_int* k, const T* alpha, \
+              const T* a, const zynum_blas_int* lda, const T* beta, T* c, const zynum_blas_int* ldc) {             \
+        const char ul = up(uplo), tr = up(trans);                                                                   \
+        int info = syrk_error(ul, tr, *n, *k, *lda, *ldc);                                                          \
+        if (info) {                                                                                                 \
+            report_xerbla(RNAME, info);                                                                             \
+            return;                                                                                                 \
+        }                                                                                                           \
+        host_syrk<T>(RNAME, ul, tr, *n, *k, *alpha, a, *lda, *beta, c, *ldc);                                       \
+    }
+ZB_SYRK(dsyrk_, double, "DSYRK ")
+ZB_SYRK(ssyrk_, float, "SSYRK ")
+#undef ZB_SYRK
+
+// cblas.zig:1729-1756 cblas_?trsm: invalid enums return silently; row-major
+// flips side and uplo and swaps m / n, keeping the transpose.
+#define ZB_CBLAS_TRSM(NAME, FNAME, T)                                                                            \
+    void NAME(int layout, int side, int uplo, int transa, int diag, int m, int n, T alpha, const T* a, int lda, \
+              T* b, int ldb) {                                                                                   \
+        if (!cblas_valid_layout(layout) || (side != CblasLeft && side != CblasRight) ||                          \
+            (uplo != CblasUpper && uplo != CblasLower) || !cblas_valid_trans(transa) ||                          \
+            (diag != CblasNonUnit && diag != CblasUnit))                                                         \
+            return;                                                                                              \
+        const bool rm = layout == CblasRowMajor;                                                                 \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                        \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                        \
+        char tt = cblas_trans_char(transa), dd = cblas_diag_char(diag);                                          \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb;                                     \
+        FNAME(&ss, &uu, &tt, &dd, &mm, &nn, &alpha, a, &la, b, &lb);                                             \
+    }
+ZB_CBLAS_TRSM(cblas_dtrsm, dtrsm_, double)
+ZB_CBLAS_TRSM(cblas_strsm, strsm_, float)
+#undef ZB_CBLAS_TRSM
+
+// cblas.zig:1539-1560 cblas_?syrk: only the layout is checked here; a bad
+// uplo / trans reaches the Fortran routine as 'X' and is reported by xerbla.
+#define ZB_CBLAS_SYRK(NAME, FNAME, T)                                                                              \
+    void NAME(int layout, int uplo, int trans, int n, int k, T alpha, const T* a, int lda, T beta, T* c, int ldc) { \
+        if (!cblas_valid_layout(layout)) return;                                                                   \
+        const bool rm = layout == CblasRowMajor;                                                                   \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                          \
+        char tt = rm ? cblas_row_trans_char(trans) : cblas_trans_char(trans);                                      \
+        zynum_blas_int nn = n, kk = k, la = lda, lc = ldc;                                                         \
+        FNAME(&uu, &tt, &nn, &kk, &alpha, a, &la, &beta, c, &lc);                                                  \
+    }
+ZB_CBLAS_SYRK(cblas_dsyrk, dsyrk_, double)
+ZB_CBLAS_SYRK(cblas_ssyrk, ssyrk_, float)
+#undef ZB_CBLAS_SYRK
+
+int zynum_blas_gpu_dtrsm_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+                                const double* a, int lda, double* b, int ldb, void* stream) {
+    return device_trsm<double>("dtrsm_device", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream);
+}
+int zynum_blas_gpu_strsm_device(char side, char uplo, char transa, char diag, int m, int n, float alpha,
+                                const float* a, int lda, float* b, int ldb, void* stream) {
+    return device_trsm<float>("strsm_device", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream);
+}
+int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+                                double beta, double* c, int ldc, void* stream) {
+    return device_syrk<double>("dsyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
+}
+int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float* a, int lda, float beta,
+                                float* c, int ldc, void* stream) {
+    return device_syrk<float>("ssyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
 }
 
 int zynum_blas_gpu_dgemm_device(char transa, char transb, int m, int n, int k, double alpha, const double* a,

@@ -63,12 +63,14 @@ template <bool A_MNFAST, bool B_MNFAST, int VEC, bool PARTIAL>
 __global__ void __launch_bounds__(kThreads, 2)
 sgemm_ffma_kernel(int M, int N, int K, int k_chunk, float alpha, const float* __restrict__ A, long lda,
                   const float* __restrict__ B, long ldb, float beta, float* __restrict__ C, long ldc,
-                  float* __restrict__ W) {
+                  float* __restrict__ W, int tri) {
     extern __shared__ __align__(128) float smf[];
     float* As = smf;
     float* Bs = smf + kStages * kBK * kPitch;
 
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    // triangle mode: skip tiles that hold no element of the stored triangle
+    if ((tri == 1 && m0 > n0 + kBN - 1) || (tri == 2 && m0 + kBM - 1 < n0)) return;
     const int kb = blockIdx.z * k_chunk;
     const int ke = min(K, kb + k_chunk);
     const int KT = (ke - kb + kBK - 1) / kBK;
@@ -124,6 +126,7 @@ sgemm_ffma_kernel(int M, int N, int K, int k_chunk, float alpha, const float* __
         for (int i = 0; i < 8; ++i) {
             const int row = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
             if (row >= M) continue;
+            if (tri == 1 ? row > col : (tri == 2 && row < col)) continue;
             if (PARTIAL) {
                 W[(long)blockIdx.z * M * N + (long)col * M + row] = acc[i][j];
             } else {
@@ -137,12 +140,13 @@ sgemm_ffma_kernel(int M, int N, int K, int k_chunk, float alpha, const float* __
 }
 
 __global__ void sgemm_splitk_reduce(int M, int N, int splits, const float* __restrict__ W, float alpha, float beta,
-                                    float* __restrict__ C, long ldc) {
+                                    float* __restrict__ C, long ldc, int tri) {
     long total = (long)M * N;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+        int row = (int)(q % M), col = (int)(q / M);
+        if (tri == 1 ? row > col : (tri == 2 && row < col)) continue;
         float s = 0.f;
         for (int z = 0; z < splits; ++z) s += W[(long)z * total + q];
-        int row = (int)(q % M), col = (int)(q / M);
         float* cp = C + (long)col * ldc + row;
         float out = alpha * s;
         if (beta != 0.f) out = fmaf(beta, *cp, out);
@@ -158,7 +162,8 @@ cudaError_t launch_f32(const GemmArgsF32& g, int splits, int k_chunk, float* W, 
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + kBM - 1) / kBM, (g.n + kBN - 1) / kBN, splits);
     prof_begin(st);
-    kern<<<grid, kThreads, SMEM, st>>>(g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b, g.ldb, g.beta, g.c, g.ldc, W);
+    kern<<<grid, kThreads, SMEM, st>>>(g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b, g.ldb, g.beta, g.c, g.ldc, W,
+                                       g.tri);
     count_launch();
     prof_end(st);
     return cudaGetLastError();
@@ -196,7 +201,7 @@ cudaError_t sgemm_native(const GemmArgsF32& g, const GemmPlan& plan, float* work
         long total = (long)g.m * g.n;
         int blocks = (int)((total + 255) / 256);
         if (blocks > 148 * 16) blocks = 148 * 16;
-        sgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used, workspace, g.alpha, g.beta, g.c, g.ldc);
+        sgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used, workspace, g.alpha, g.beta, g.c, g.ldc, g.tri);
         count_launch();
         return cudaGetLastError();
     }

@@ -64,7 +64,7 @@ template <int BM, int BN, int WM, int WN, int STAGES, bool A_KFAST, bool B_KFAST
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 1)
 dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* __restrict__ A, long lda,
                   const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
-                  double* __restrict__ W) {
+                  double* __restrict__ W, int tri) {
     constexpr int NTHREADS = (BM / WM) * (BN / WN) * 32;
     constexpr int WARPS_N = BN / WN;
     constexpr int MI = WM / 16;
@@ -80,6 +80,8 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
 
     const int m0 = blockIdx.x * BM;
     const int n0 = blockIdx.y * BN;
+    // triangle mode: skip tiles that hold no element of the stored triangle
+    if ((tri == 1 && m0 > n0 + BN - 1) || (tri == 2 && m0 + BM - 1 < n0)) return;
     const int kb = blockIdx.z * k_chunk;
     const int ke = min(K, kb + k_chunk);
     const int KT = (ke - kb + kBK - 1) / kBK;
@@ -168,7 +170,8 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
             for (int v = 0; v < 4; ++v) {
                 const int row = m0 + wm + i * 16 + g + 8 * (v >> 1);
                 const int col = n0 + wn + j * 8 + 2 * t + (v & 1);
-                if (row < M && col < N) {
+                const bool in_tri = tri == 0 || (tri == 1 ? row <= col : row >= col);
+                if (row < M && col < N && in_tri) {
                     if (PARTIAL) {
                         W[(long)blockIdx.z * M * N + (long)col * M + row] = acc[i][j][v];
                     } else {
@@ -182,12 +185,13 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
 }
 
 __global__ void dgemm_splitk_reduce(int M, int N, int splits, const double* __restrict__ W, double alpha, double beta,
-                                    double* __restrict__ C, long ldc) {
+                                    double* __restrict__ C, long ldc, int tri) {
     long total = (long)M * N;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+        int row = (int)(q % M), col = (int)(q / M);
+        if (tri == 1 ? row > col : (tri == 2 && row < col)) continue;
         double s = 0.0;
         for (int z = 0; z < splits; ++z) s += W[(long)z * total + q];
-        int row = (int)(q % M), col = (int)(q / M);
         double* cp = C + (long)col * ldc + row;
         double out = alpha * s;
         if (beta != 0.0) out = fma(beta, *cp, out);
@@ -206,7 +210,8 @@ cudaError_t launch_one(const GemmArgsF64& g, int splits, int k_chunk, double* W,
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, splits);
     prof_begin(st);
-    kern<<<grid, NTHREADS, SMEM, st>>>(g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b, g.ldb, g.beta, g.c, g.ldc, W);
+    kern<<<grid, NTHREADS, SMEM, st>>>(g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b, g.ldb, g.beta, g.c, g.ldc, W,
+                                       g.tri);
     count_launch();
     prof_end(st);
     return cudaGetLastError();
@@ -247,7 +252,8 @@ cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* wor
         long total = (long)g.m * g.n;
         int blocks = (int)((total + 255) / 256);
         if (blocks > 148 * 16) blocks = 148 * 16;
-        dgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used_splits, workspace, g.alpha, g.beta, g.c, g.ldc);
+        dgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used_splits, workspace, g.alpha, g.beta, g.c, g.ldc,
+                                                    g.tri);
         count_launch();
         return cudaGetLastError();
     }

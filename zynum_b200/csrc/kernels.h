@@ -23,6 +23,9 @@ struct GemmArgs {
     T beta;
     T* c;
     long ldc;
+    // 0: full C; 1: only the upper triangle (row <= col); 2: only the lower
+    // triangle (row >= col).  Tiles entirely outside are skipped (SYRK).
+    int tri = 0;
 };
 using GemmArgsF64 = GemmArgs<double>;
 using GemmArgsF32 = GemmArgs<float>;

@@ -25,6 +25,10 @@ int parse_smethod_env() {
     if (v && !std::strcmp(v, "bf16x3")) return SMETHOD_BF16X3;
     return SMETHOD_NATIVE;
 }
+int parse_complex_env() {
+    const char* v = std::getenv("ZYNUM_GPU_COMPLEX_METHOD");
+    return (v && !std::strcmp(v, "3m")) ? 1 : 0;
+}
 int parse_slices_env() {
     const char* v = std::getenv("ZYNUM_GPU_OZAKI_SLICES");
     if (!v || !std::strcmp(v, "auto")) return 0;
@@ -98,6 +102,7 @@ cudaError_t Context::init() {
     dgemm_method = parse_method_env();
     sgemm_method = parse_smethod_env();
     ozaki_slices = parse_slices_env();
+    complex_method = parse_complex_env();
     initialised = true;
     return cudaSuccess;
 }

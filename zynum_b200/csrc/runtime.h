@@ -53,6 +53,7 @@ struct Context {
     int dgemm_method = METHOD_NATIVE;
     int sgemm_method = SMETHOD_NATIVE;
     int ozaki_slices = 0;  // 0 = automatic
+    int complex_method = 0;  // 0 = expanded-real 4M, 1 = 3M
     InjectedFaults faults;
     bool initialised = false;
     cudaError_t init();
