@@ -34,6 +34,7 @@ sys.path.insert(0, str(ROOT))
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12  # 64 DFMA/clk/SM at the 1965 MHz max clock
+METRIC = "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error; batch GFLOP/s"
 
 
 def _peaks():
@@ -163,7 +164,7 @@ def cpu_baseline(n, slab, min_seconds=10.0, max_reps=20):
 
 # --------------------------------------------------------------- reference
 def run_reference(args, rank, world):
-    metric, unit = "DGEMM TFLOP/s @8192^3 (effective 2n^3)", "TFLOP/s"
+    metric, unit = METRIC, "TFLOP/s"
     if rank != 0:
         return 0
     n = args.size
@@ -188,14 +189,80 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic U[-1,1], seeded",
-            "config": {"workload": f"DGEMM M=N=K={n} column-major FP64, alpha=1, beta=0",
-                       "step_sample": f"{n}x{slab}x{n} column slab per step"},
+            "config": {"workload": f"DGEMM M=N=K={n} NN column-major FP64 alpha=1 beta=0",
+                       "step_sample": f"{n}x{slab}x{n} column slab of the {n}^3 problem per step"},
             "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                              "sample": f"{n}x{slab}x{n} slab per step; restated Zynum x86-64 packed-SIMD path "
                                        "(reference is Zig 0.16, no zig toolchain in the image)"},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------ batches
+def bench_batched(torch, blas, steps, warmup, seed=7):
+    """20,000 variable-size DGEMM and SGEMM problems (M, N, K log-uniform on [8, 512], alpha 1, beta 0)
+    and 5,000 left-lower TRSMs (n log-uniform on [16, 1024], 1..64 right-hand sides, L = tril(N(0,1))
+    with diagonal 2 + |N(0,1)|), each batch one persistent launch replayed from a CUDA graph."""
+    rng = np.random.default_rng(seed)
+    dev = torch.device("cuda")
+    out = {}
+
+    def lu(lo, hi, size):
+        return np.exp(rng.uniform(np.log(lo), np.log(hi), size)).astype(np.int64)
+
+    def carve(sizes, dtype, fill):
+        """One flat buffer holding every problem's matrix; returns (buffer, pointer tensor)."""
+        esz = 8 if dtype == torch.float64 else 4
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        buf = torch.empty(int(sizes.sum()) + 1, dtype=dtype, device=dev)
+        fill(buf)
+        ptrs = torch.from_numpy(offs * esz + buf.data_ptr()).to(dev)
+        return buf, ptrs
+
+    count = 20000
+    m, n, k = lu(8, 512, count), lu(8, 512, count), lu(8, 512, count)
+    flops = float(np.sum(2.0 * m * n * k))
+    for name, tdt in (("dgemm", torch.float64), ("sgemm", torch.float32)):
+        g = torch.Generator(device=dev).manual_seed(seed)
+        ufill = lambda b: b.uniform_(-1, 1, generator=g)  # noqa: E731
+        A, pa = carve(m * k, tdt, ufill)
+        B, pb = carve(k * n, tdt, ufill)
+        Cb, pc = carve(m * n, tdt, lambda b: b.zero_())
+        la = torch.from_numpy(m.astype(np.int32)).to(dev)
+        lb = torch.from_numpy(k.astype(np.int32)).to(dev)
+        t0 = time.perf_counter()
+        batch = blas.GemmBatch(m, n, k, dtype="f64" if tdt == torch.float64 else "f32", tune=True)
+        plan_s = time.perf_counter() - t0
+        run = lambda: batch.run(1.0, pa, la, pb, lb, 0.0, pc, la, use_graph=True)  # noqa: E731
+        ms = time_device(torch, run, steps, warmup, torch.cuda.current_stream())
+        out[name] = {"problems": count, "gflop": flops / 1e9, "ms": ms, "gflops": flops / (ms * 1e-3) / 1e9,
+                     "plan_and_tune_s": plan_s, **batch.info()}
+        batch.close()
+        del A, B, Cb
+    tcount = 5000
+    tn = lu(16, 1024, tcount)
+    tr = rng.integers(1, 65, tcount).astype(np.int64)
+    tflops = float(np.sum(tn.astype(np.float64) ** 2 * tr))
+
+    def lfill(buf):
+        buf.normal_(0, 1)
+
+    A, pa = carve(tn * tn, torch.float64, lfill)
+    # make every A_q lower triangular with diagonal 2 + |N(0,1)| (upper part is never read)
+    offs = np.concatenate([[0], np.cumsum(tn * tn)[:-1]])
+    for q in range(tcount):
+        a = A[offs[q]: offs[q] + tn[q] * tn[q]].view(int(tn[q]), int(tn[q]))
+        a.diagonal().abs_().add_(2.0)
+    B, pb = carve(tn * tr, torch.float64, lfill)
+    la = torch.from_numpy(tn.astype(np.int32)).to(dev)
+    batch = blas.TrsmBatch(tn, tr, dtype="f64", uplo="L")
+    run = lambda: batch.run(1.0, pa, la, pb, la, use_graph=True)  # noqa: E731
+    ms = time_device(torch, run, steps, warmup, torch.cuda.current_stream())
+    out["dtrsm"] = {"problems": tcount, "gflop": tflops / 1e9, "ms": ms, "gflops": tflops / (ms * 1e-3) / 1e9,
+                    "note": "GFLOP = sum n^2 * nrhs", **batch.info()}
+    batch.close()
+    return out
 
 
 # ---------------------------------------------------------------- our arm
@@ -323,11 +390,11 @@ def run_ours(args, rank, world, local_rank):
                 "kernel": "native DGEMM (DMMA m16n8k8 f64)",
                 "peak_source": "nominal FP64 pipe: 148 SMs x 128 flop/clk x 1.965 GHz (no measured FP64 peak)"}
     line = {
-        "metric": "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error",
+        "metric": METRIC,
         "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": f"synthetic u*10^e, u~U[-1,1], e~U[-{args.phi},{args.phi}], seeded",
-        "config": {"workload": f"DGEMM M=N=K={n} NN column-major FP64 alpha=1 beta=0 ({head[0]})",
+        "config": {"workload": f"DGEMM M=N=K={n} NN column-major FP64 alpha=1 beta=0",
                    "method": head[0], "l2": "inputs 3 x 512 MiB > 126 MB L2 (no flush needed)",
                    "parallelism": "replicas" if world > 1 else "single-GPU"},
         "methods": {k: {**v, **({"error": err[k]} if k in err else {})} for k, v in results.items()},
@@ -338,6 +405,8 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8,
                 "path": "dgemm_ Fortran ABI, pinned host buffers"},
     }
+    if not args.no_batched:
+        line["batched"] = bench_batched(torch, blas, max(3, args.steps), args.warmup)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(n if n <= 8192 else 8192, 256)
     print(json.dumps(line), flush=True)
@@ -355,6 +424,7 @@ def main(argv=None):
     ap.add_argument("--phi", type=float, default=0.0)
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -164,6 +164,43 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n,
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
                                                    int lda, float beta, float *c, int ldc, void *stream);
 
+/* ------------------------------------------------- variable-size batches
+ * No counterpart in the reference (Zynum has no batched API).  A batch plan is
+ * created once from HOST arrays of problem sizes; running it is one
+ * persistent-kernel launch (or a replay of a CUDA graph holding that launch
+ * when use_graph != 0) with no allocation.  The per-problem operand arrays
+ * passed to *_run (pointers and leading dimensions) are DEVICE arrays with one
+ * entry per problem.  dtype: 0 = FP64, 1 = FP32.  Create returns 0 or the
+ * index of the first illegal argument; run returns 0 or a negated CUDA error. */
+typedef struct zynum_blas_gpu_batch *zynum_blas_gpu_batch_t;
+/* GEMM batch: C_q = alpha op(A_q) op(B_q) + beta C_q with m[q] x n[q] x k[q] sizes and
+ * the same transposes.  tune != 0 times the candidate tile configs of every size
+ * bucket not yet in the tuning table (kept in the JSON file ZYNUM_GPU_TUNE_CACHE names). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t *out, int dtype, char transa,
+                                                        char transb, int count, const int *m, const int *n,
+                                                        const int *k, int tune);
+/* Left-side TRSM batch: B_q (m[q] x n[q], n[q] <= 64) := alpha op(A_q)^-1 B_q, A_q m[q] x m[q] triangular. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_trsm_batch_create(zynum_blas_gpu_batch_t *out, int dtype, char side, char uplo,
+                                                        char transa, char diag, int count, const int *m,
+                                                        const int *n);
+ZYNUM_BLAS_GPU_API void zynum_blas_gpu_batch_destroy(zynum_blas_gpu_batch_t batch);
+/* Number of scheduled work items, persistent grid size and tiles per config (32, 64, 128). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_batch_info(zynum_blas_gpu_batch_t batch, int *items, int *grid, int *cfg_counts);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_batch_run(zynum_blas_gpu_batch_t batch, double alpha,
+                                                      const double *const *a, const int *lda, const double *const *b,
+                                                      const int *ldb, double beta, double *const *c, const int *ldc,
+                                                      void *stream, int use_graph);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_sgemm_batch_run(zynum_blas_gpu_batch_t batch, float alpha, const float *const *a,
+                                                      const int *lda, const float *const *b, const int *ldb,
+                                                      float beta, float *const *c, const int *ldc, void *stream,
+                                                      int use_graph);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrsm_batch_run(zynum_blas_gpu_batch_t batch, double alpha,
+                                                      const double *const *a, const int *lda, double *const *b,
+                                                      const int *ldb, void *stream, int use_graph);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_strsm_batch_run(zynum_blas_gpu_batch_t batch, float alpha, const float *const *a,
+                                                      const int *lda, float *const *b, const int *ldb, void *stream,
+                                                      int use_graph);
+
 /* -------------------------------------------------------------- control */
 /* 0 = expanded-real 4M (one real GEMM of 2m x n x 2k), 1 = 3M (three real GEMMs). Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_complex_method(int method);

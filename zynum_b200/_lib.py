@@ -73,6 +73,22 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
                  "zynum_blas_gpu_ssyrk_device"):
         getattr(L, name).restype = i
+    IP = C.POINTER(C.c_int)
+    L.zynum_blas_gpu_gemm_batch_create.argtypes = [C.POINTER(P), i, ch, ch, i, P, P, P, i]
+    L.zynum_blas_gpu_gemm_batch_create.restype = i
+    L.zynum_blas_gpu_trsm_batch_create.argtypes = [C.POINTER(P), i, ch, ch, ch, ch, i, P, P]
+    L.zynum_blas_gpu_trsm_batch_create.restype = i
+    L.zynum_blas_gpu_batch_destroy.argtypes = [P]
+    L.zynum_blas_gpu_batch_destroy.restype = None
+    L.zynum_blas_gpu_batch_info.argtypes = [P, IP, IP, P]
+    L.zynum_blas_gpu_batch_info.restype = i
+    L.zynum_blas_gpu_dgemm_batch_run.argtypes = [P, d, P, P, P, P, d, P, P, P, i]
+    L.zynum_blas_gpu_sgemm_batch_run.argtypes = [P, f, P, P, P, P, f, P, P, P, i]
+    L.zynum_blas_gpu_dtrsm_batch_run.argtypes = [P, d, P, P, P, P, P, i]
+    L.zynum_blas_gpu_strsm_batch_run.argtypes = [P, f, P, P, P, P, P, i]
+    for name in ("zynum_blas_gpu_dgemm_batch_run", "zynum_blas_gpu_sgemm_batch_run",
+                 "zynum_blas_gpu_dtrsm_batch_run", "zynum_blas_gpu_strsm_batch_run"):
+        getattr(L, name).restype = i
     L.zynum_blas_gpu_set_complex_method.argtypes = [i]
     L.zynum_blas_gpu_set_complex_method.restype = i
     L.zynum_blas_gpu_dgemm_device.argtypes = [ch, ch, i, i, i, d, P, i, P, i, d, P, i, P]

@@ -215,3 +215,75 @@ def last_error() -> str:
 
 def shutdown() -> None:
     load().zynum_blas_shutdown()
+
+
+# ------------------------------------------------------------------ batches
+class _Batch:
+    def __init__(self, handle):
+        self.handle = handle
+
+    def info(self):
+        items, grid = C.c_int(0), C.c_int(0)
+        cfg = (C.c_int * 3)()
+        load().zynum_blas_gpu_batch_info(self.handle, C.byref(items), C.byref(grid), cfg)
+        return {"items": items.value, "grid": grid.value, "tiles_per_cfg": {32: cfg[0], 64: cfg[1], 128: cfg[2]}}
+
+    def close(self):
+        if self.handle:
+            load().zynum_blas_gpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _int_array(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+
+
+class GemmBatch(_Batch):
+    """Variable-size batched GEMM plan (one persistent kernel per run).
+
+    m, n, k: per-problem sizes (host sequences).  run() takes torch CUDA
+    tensors (or raw device pointers) for the per-problem operands.
+    """
+
+    def __init__(self, m, n, k, dtype="f64", transa="N", transb="N", tune=False):
+        self.dt = 0 if dtype in ("f64", np.float64) else 1
+        m, n, k = _int_array(m), _int_array(n), _int_array(k)
+        h = C.c_void_p()
+        st = load().zynum_blas_gpu_gemm_batch_create(C.byref(h), self.dt, _ch(transa), _ch(transb), len(m),
+                                                     m.ctypes.data, n.ctypes.data, k.ctypes.data, int(tune))
+        check(st, "zynum_blas_gpu_gemm_batch_create")
+        super().__init__(h)
+        self.count = len(m)
+
+    def run(self, alpha, a_ptrs, lda, b_ptrs, ldb, beta, c_ptrs, ldc, stream=None, use_graph=False):
+        """a_ptrs / b_ptrs / c_ptrs: int64 CUDA tensors of device addresses; lda/ldb/ldc: int32 CUDA tensors."""
+        fn = load().zynum_blas_gpu_dgemm_batch_run if self.dt == 0 else load().zynum_blas_gpu_sgemm_batch_run
+        st = fn(self.handle, float(alpha), _ptr(a_ptrs), _ptr(lda), _ptr(b_ptrs), _ptr(ldb), float(beta),
+                _ptr(c_ptrs), _ptr(ldc), _stream(stream), int(use_graph))
+        check(st, "gemm_batch_run")
+
+
+class TrsmBatch(_Batch):
+    """Left-side variable-size batched TRSM plan: B_q (m_q x n_q, n_q <= 64) := alpha op(A_q)^-1 B_q."""
+
+    def __init__(self, m, n, dtype="f64", uplo="L", transa="N", diag="N"):
+        self.dt = 0 if dtype in ("f64", np.float64) else 1
+        m, n = _int_array(m), _int_array(n)
+        h = C.c_void_p()
+        st = load().zynum_blas_gpu_trsm_batch_create(C.byref(h), self.dt, b"L", _ch(uplo), _ch(transa), _ch(diag),
+                                                     len(m), m.ctypes.data, n.ctypes.data)
+        check(st, "zynum_blas_gpu_trsm_batch_create")
+        super().__init__(h)
+        self.count = len(m)
+
+    def run(self, alpha, a_ptrs, lda, b_ptrs, ldb, stream=None, use_graph=False):
+        fn = load().zynum_blas_gpu_dtrsm_batch_run if self.dt == 0 else load().zynum_blas_gpu_strsm_batch_run
+        st = fn(self.handle, float(alpha), _ptr(a_ptrs), _ptr(lda), _ptr(b_ptrs), _ptr(ldb), _stream(stream),
+                int(use_graph))
+        check(st, "trsm_batch_run")

@@ -1,0 +1,445 @@
+// Variable-size batched GEMM and TRSM: one persistent kernel per batch.
+//
+// No counterpart in the reference (Zynum has no batched API); the per-problem
+// semantics are those of gemm.zig:1392 and triangular.zig:233.
+//
+// GEMM: the host turns the batch into a list of output tiles (problem, m0, n0,
+// tile config) ordered longest-first and dealt round-robin to a fixed grid of
+// persistent CTAs (deterministic, no atomics, so one launch is graph-capturable
+// and replayable).  Each size bucket gets its tile config from the autotuner
+// (tuner.cpp).  FP64 tiles use DMMA (mma.sync m16n8k8 .f64), FP32 tiles FFMA;
+// operands are staged with cp.async (8- / 4-byte copies: per-problem leading
+// dimensions need not be aligned).
+//
+// TRSM (left side): one CTA solves one whole problem B := alpha op(A)^-1 B:
+// for every 64-row diagonal block, substitution on the block held in shared
+// memory, then the rank-64 update of the rows below (above) it with the
+// solved rows kept in shared memory.
+#include <algorithm>
+
+#include "batched.h"
+#include "common.cuh"
+
+namespace zb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBK = 16;
+constexpr int kStages = 3;
+
+template <typename T>
+struct Prob {
+    int m, n, k, lda, ldb, ldc;
+    const T* a;
+    const T* b;
+    T* c;
+};
+
+// ------------------------------------------------------------- loaders
+template <typename T, int ROWS, int COLS>
+ZB_DEVICE void load_tile(T* smem, int pitch, const T* __restrict__ base, long ld, int r0, int c0, int r_lim,
+                         int c_lim) {
+    constexpr int TOTAL = ROWS * COLS;
+#pragma unroll
+    for (int it = 0; it < (TOTAL + kThreads - 1) / kThreads; ++it) {
+        const int q = it * kThreads + threadIdx.x;
+        if (TOTAL % kThreads != 0 && q >= TOTAL) break;
+        const int r = q / COLS, c = q % COLS;
+        const int gr = r0 + r, gc = c0 + c;
+        const bool ok = gr < r_lim && gc < c_lim;
+        const T* src = ok ? base + (long)gr * ld + gc : base;
+        if (sizeof(T) == 8)
+            cp_async_8(smem_u32(smem + r * pitch + c), src, ok ? 8 : 0);
+        else
+            cp_async_4(smem_u32(smem + r * pitch + c), src, ok ? 4 : 0);
+    }
+}
+
+// ------------------------------------------------------- FP64 DMMA tile
+// BM x BN tile, 8 warps as 2 x 4, warp tile (BM/2) x (BN/4).
+template <int BM, int BN, bool AK, bool BKF>
+ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, double beta, double* smem) {
+    constexpr int WM = BM / 2, WN = BN / 4, MI = WM / 16, NI = WN / 8;
+    constexpr int A_ROWS = AK ? BM : kBK, A_COLS = AK ? kBK : BM, A_PITCH = A_COLS + 4;
+    constexpr int B_ROWS = BKF ? BN : kBK, B_COLS = BKF ? kBK : BN, B_PITCH = B_COLS + 4;
+    constexpr int A_STAGE = A_ROWS * A_PITCH, B_STAGE = B_ROWS * B_PITCH;
+    double* As = smem;
+    double* Bs = smem + kStages * A_STAGE;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = (warp / 4) * WM, wn = (warp % 4) * WN;
+    const int g = lane >> 2, t = lane & 3;
+    const int KT = (alpha == 0.0) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
+    double acc[MI][NI][4];
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+    auto load_stage = [&](int stage, int kt) {
+        const int k0 = kt * kBK;
+        if (AK)
+            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, m0, k0, p.m, p.k);
+        else
+            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, k0, m0, p.k, p.m);
+        if (BKF)
+            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, n0, k0, p.n, p.k);
+        else
+            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, k0, n0, p.k, p.n);
+    };
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
+        cp_async_commit();
+        const double* as = As + (kt % kStages) * A_STAGE;
+        const double* bs = Bs + (kt % kStages) * B_STAGE;
+#pragma unroll
+        for (int ks = 0; ks < kBK; ks += 8) {
+            double af[MI][4], bf[NI][2];
+#pragma unroll
+            for (int i = 0; i < MI; ++i)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int rr = wm + i * 16 + g + 8 * (v & 1), kk = ks + t + 4 * (v >> 1);
+                    af[i][v] = AK ? as[rr * A_PITCH + kk] : as[kk * A_PITCH + rr];
+                }
+#pragma unroll
+            for (int j = 0; j < NI; ++j)
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const int cc = wn + j * 8 + g, kk = ks + t + 4 * v;
+                    bf[j][v] = BKF ? bs[cc * B_PITCH + kk] : bs[kk * B_PITCH + cc];
+                }
+#pragma unroll
+            for (int i = 0; i < MI; ++i)
+#pragma unroll
+                for (int j = 0; j < NI; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int row = m0 + wm + i * 16 + g + 8 * (v >> 1);
+                const int col = n0 + wn + j * 8 + 2 * t + (v & 1);
+                if (row < p.m && col < p.n) {
+                    double* cp = p.c + (long)col * p.ldc + row;
+                    double out = alpha * acc[i][j][v];
+                    if (beta != 0.0) out = fma(beta, *cp, out);
+                    *cp = out;
+                }
+            }
+    __syncthreads();  // shared memory is reused by the next work item
+}
+
+// ------------------------------------------------------- FP32 FFMA tile
+// BM x BN tile, 256 threads as 16 x 16, each thread (BM/16) x (BN/16) outputs.
+template <int BM, int BN, bool AM, bool BMF>
+ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, float beta, float* smem) {
+    constexpr int TM = BM / 16, TN = BN / 16;
+    constexpr int PA = BM + 4, PB = BN + 4;
+    float* As = smem;                        // [stage][kBK][PA]  (m fast)
+    float* Bs = smem + kStages * kBK * PA;   // [stage][kBK][PB]  (n fast)
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int KT = (alpha == 0.f) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
+    float acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
+    auto load_stage = [&](int stage, int kt) {
+        const int k0 = kt * kBK;
+        float* as = As + stage * kBK * PA;
+        float* bs = Bs + stage * kBK * PB;
+        // element (mn, kk) of the tile -> shared [kk][mn]
+        for (int q = threadIdx.x; q < kBK * BM; q += kThreads) {
+            int kk, mm;
+            if (AM) { kk = q / BM; mm = q % BM; } else { mm = q / kBK; kk = q % kBK; }
+            const int gm = m0 + mm, gk = k0 + kk;
+            const bool ok = gm < p.m && gk < p.k;
+            const float* src = ok ? (AM ? p.a + gm + (long)gk * p.lda : p.a + gk + (long)gm * p.lda) : p.a;
+            cp_async_4(smem_u32(as + kk * PA + mm), src, ok ? 4 : 0);
+        }
+        for (int q = threadIdx.x; q < kBK * BN; q += kThreads) {
+            int kk, nn;
+            if (BMF) { kk = q / BN; nn = q % BN; } else { nn = q / kBK; kk = q % kBK; }
+            const int gn = n0 + nn, gk = k0 + kk;
+            const bool ok = gn < p.n && gk < p.k;
+            const float* src = ok ? (BMF ? p.b + gn + (long)gk * p.ldb : p.b + gk + (long)gn * p.ldb) : p.b;
+            cp_async_4(smem_u32(bs + kk * PB + nn), src, ok ? 4 : 0);
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
+        cp_async_commit();
+        const float* as = As + (kt % kStages) * kBK * PA;
+        const float* bs = Bs + (kt % kStages) * kBK * PB;
+#pragma unroll
+        for (int kk = 0; kk < kBK; ++kk) {
+            float a[TM], b[TN];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = as[kk * PA + ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < TN; ++j) b[j] = bs[kk * PB + tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        const int col = n0 + tx + 16 * j;
+        if (col >= p.n) continue;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int row = m0 + ty + 16 * i;
+            if (row >= p.m) continue;
+            float* cp = p.c + (long)col * p.ldc + row;
+            float out = alpha * acc[i][j];
+            if (beta != 0.f) out = fmaf(beta, *cp, out);
+            *cp = out;
+        }
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------- persistent kernels
+template <bool AK, bool BKF>
+__global__ void __launch_bounds__(kThreads, 1)
+dgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
+                     const double* const* __restrict__ a, const int* __restrict__ lda,
+                     const double* const* __restrict__ b, const int* __restrict__ ldb, double alpha, double beta,
+                     double* const* __restrict__ c, const int* __restrict__ ldc) {
+    extern __shared__ __align__(128) double sm_d[];
+    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const BatchWork it = work[w];
+        const int q = it.prob;
+        if (q < 0) continue;  // padding item of the per-CTA schedule
+        Prob<double> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
+        if (it.cfg == TILE_CFG_128)
+            dgemm_tile<128, 128, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+        else if (it.cfg == TILE_CFG_64)
+            dgemm_tile<64, 64, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+        else
+            dgemm_tile<32, 32, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+    }
+}
+
+template <bool AM, bool BMF>
+__global__ void __launch_bounds__(kThreads, 1)
+sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
+                     const float* const* __restrict__ a, const int* __restrict__ lda,
+                     const float* const* __restrict__ b, const int* __restrict__ ldb, float alpha, float beta,
+                     float* const* __restrict__ c, const int* __restrict__ ldc) {
+    extern __shared__ __align__(128) float sm_f[];
+    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const BatchWork it = work[w];
+        const int q = it.prob;
+        if (q < 0) continue;  // padding item of the per-CTA schedule
+        Prob<float> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
+        if (it.cfg == TILE_CFG_128)
+            sgemm_tile<128, 128, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
+        else if (it.cfg == TILE_CFG_64)
+            sgemm_tile<64, 64, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
+        else
+            sgemm_tile<32, 32, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
+    }
+}
+
+size_t dsmem_bytes() {
+    // largest config (128 x 128), worst orientation
+    const size_t a = (size_t)128 * (kBK + 4) > (size_t)kBK * (128 + 4) ? (size_t)128 * (kBK + 4) : (size_t)kBK * 132;
+    return kStages * 2 * a * sizeof(double);
+}
+size_t ssmem_bytes() { return (size_t)kStages * kBK * (132 + 132) * sizeof(float); }
+
+// -------------------------------------------------------- batched TRSM
+constexpr int kTB = 64;  // diagonal block
+constexpr int kMaxRhs = 64;
+
+template <typename T>
+ZB_DEVICE T tri_el(const T* a, long lda, char uplo, char trans, char diag, int r, int c) {
+    const int ar = (trans == 'N') ? r : c, ac = (trans == 'N') ? c : r;
+    if (ar == ac && diag == 'U') return T(1);
+    if (uplo == 'U' && ar > ac) return T(0);
+    if (uplo == 'L' && ar < ac) return T(0);
+    return a[ar + (long)ac * lda];
+}
+
+// One CTA per problem (left side): B (n x r) := alpha op(A)^-1 B.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
+                    char diag, T alpha, const T* const* __restrict__ a, const int* __restrict__ lda,
+                    T* const* __restrict__ b, const int* __restrict__ ldb) {
+    extern __shared__ __align__(16) unsigned char trsm_smem[];
+    T(*D)[kTB + 1] = reinterpret_cast<T(*)[kTB + 1]>(trsm_smem);             // diagonal block of op(A)
+    T(*X)[kMaxRhs + 1] = reinterpret_cast<T(*)[kMaxRhs + 1]>(D + kTB);       // solved rows of this block
+    const bool upper = (trans == 'N' && uplo == 'U') || (trans != 'N' && uplo == 'L');
+    for (int w = blockIdx.x; w < count; w += gridDim.x) {
+        const int q = order[w];
+        if (q < 0) continue;  // padding item of the per-CTA schedule
+        const int n = dims[2 * q], r = dims[2 * q + 1];
+        const T* A = a[q];
+        T* B = b[q];
+        const long la = lda[q], lb = ldb[q];
+        if (alpha != T(1))
+            for (long e = threadIdx.x; e < (long)n * r; e += kThreads) {
+                T* p = B + (e % n) + (e / n) * lb;
+                *p = alpha * *p;
+            }
+        __syncthreads();
+        const int nblk = (n + kTB - 1) / kTB;
+        for (int s = 0; s < nblk; ++s) {
+            const int bi = upper ? nblk - 1 - s : s;
+            const int kb = bi * kTB, sz = min(kTB, n - kb);
+            for (int e = threadIdx.x; e < kTB * kTB; e += kThreads) {
+                const int rr = e % kTB, cc = e / kTB;
+                D[rr][cc] = (rr < sz && cc < sz) ? tri_el(A, la, uplo, trans, diag, kb + rr, kb + cc) : T(0);
+            }
+            for (int e = threadIdx.x; e < kTB * r; e += kThreads) {
+                const int rr = e % kTB, cc = e / kTB;
+                X[rr][cc] = (rr < sz) ? B[kb + rr + (long)cc * lb] : T(0);
+            }
+            __syncthreads();
+            // substitution: one thread per right-hand side
+            if (threadIdx.x < r) {
+                const int j = threadIdx.x;
+                if (!upper) {
+                    for (int i = 0; i < sz; ++i) {
+                        T v = X[i][j];
+                        for (int p = 0; p < i; ++p) v -= D[i][p] * X[p][j];
+                        X[i][j] = (diag == 'U') ? v : v / D[i][i];
+                    }
+                } else {
+                    for (int i = sz - 1; i >= 0; --i) {
+                        T v = X[i][j];
+                        for (int p = i + 1; p < sz; ++p) v -= D[i][p] * X[p][j];
+                        X[i][j] = (diag == 'U') ? v : v / D[i][i];
+                    }
+                }
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < sz * r; e += kThreads) {
+                const int rr = e % sz, cc = e / sz;
+                B[kb + rr + (long)cc * lb] = X[rr][cc];
+            }
+            // rank-sz update of the rows still to solve
+            const int u0 = upper ? 0 : kb + sz, u1 = upper ? kb : n;
+            for (int row = u0 + threadIdx.x; row < u1; row += kThreads) {
+                T acc[kMaxRhs];
+#pragma unroll
+                for (int j = 0; j < kMaxRhs; ++j) acc[j] = T(0);
+                for (int p = 0; p < sz; ++p) {
+                    const T l = tri_el(A, la, uplo, trans, diag, row, kb + p);
+#pragma unroll
+                    for (int j = 0; j < kMaxRhs; ++j)
+                        if (j < r) acc[j] = fma(l, X[p][j], acc[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < kMaxRhs; ++j)
+                    if (j < r) B[row + (long)j * lb] -= acc[j];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, char transb, const void* alpha,
+                                const void* const* a, const int* lda, const void* const* b, const int* ldb,
+                                const void* beta, void* const* c, const int* ldc, int grid, cudaStream_t st) {
+    if (d.n_work == 0) return cudaSuccess;
+    cudaError_t e;
+    if (dtype == BATCH_F64) {
+        const bool ak = transa != 'N', bk = transb == 'N';
+        const double al = *static_cast<const double*>(alpha), be = *static_cast<const double*>(beta);
+        auto A = reinterpret_cast<const double* const*>(a);
+        auto B = reinterpret_cast<const double* const*>(b);
+        auto Cp = reinterpret_cast<double* const*>(c);
+        const size_t sm = dsmem_bytes();
+#define ZB_DB(AKV, BKV)                                                                                         \
+    if (ak == AKV && bk == BKV) {                                                                               \
+        auto kern = dgemm_batched_kernel<AKV, BKV>;                                                             \
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess) \
+            return e;                                                                                           \
+        prof_begin(st);                                                                                         \
+        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
+        count_launch();                                                                                         \
+        prof_end(st);                                                                                           \
+        return cudaGetLastError();                                                                              \
+    }
+        ZB_DB(false, false) ZB_DB(false, true) ZB_DB(true, false) ZB_DB(true, true)
+#undef ZB_DB
+    } else {
+        const bool am = transa == 'N', bm = transb != 'N';
+        const float al = *static_cast<const float*>(alpha), be = *static_cast<const float*>(beta);
+        auto A = reinterpret_cast<const float* const*>(a);
+        auto B = reinterpret_cast<const float* const*>(b);
+        auto Cp = reinterpret_cast<float* const*>(c);
+        const size_t sm = ssmem_bytes();
+#define ZB_SB(AMV, BMV)                                                                                         \
+    if (am == AMV && bm == BMV) {                                                                               \
+        auto kern = sgemm_batched_kernel<AMV, BMV>;                                                             \
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess) \
+            return e;                                                                                           \
+        prof_begin(st);                                                                                         \
+        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
+        count_launch();                                                                                         \
+        prof_end(st);                                                                                           \
+        return cudaGetLastError();                                                                              \
+    }
+        ZB_SB(false, false) ZB_SB(false, true) ZB_SB(true, false) ZB_SB(true, true)
+#undef ZB_SB
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, int dtype, char uplo, char trans,
+                                char diag, const void* alpha, const void* const* a, const int* lda, void* const* b,
+                                const int* ldb, int grid, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    const int sm = (kTB * (kTB + 1) + kTB * (kMaxRhs + 1)) * (dtype == BATCH_F64 ? 8 : 4);
+    cudaError_t e = dtype == BATCH_F64
+                        ? cudaFuncSetAttribute(trsm_batched_kernel<double>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm)
+                        : cudaFuncSetAttribute(trsm_batched_kernel<float>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    prof_begin(st);
+    if (dtype == BATCH_F64)
+        trsm_batched_kernel<double><<<grid, kThreads, sm, st>>>(
+            order, count, dims, uplo, trans, diag, *static_cast<const double*>(alpha),
+            reinterpret_cast<const double* const*>(a), lda, reinterpret_cast<double* const*>(b), ldb);
+    else
+        trsm_batched_kernel<float><<<grid, kThreads, sm, st>>>(
+            order, count, dims, uplo, trans, diag, *static_cast<const float*>(alpha),
+            reinterpret_cast<const float* const*>(a), lda, reinterpret_cast<float* const*>(b), ldb);
+    count_launch();
+    prof_end(st);
+    return cudaGetLastError();
+}
+
+int batched_tile_edge(int cfg) { return cfg == TILE_CFG_128 ? 128 : (cfg == TILE_CFG_64 ? 64 : 32); }
+
+}  // namespace zb

@@ -1,0 +1,541 @@
+// Host side of the batched GEMM / TRSM: plans, LPT schedule, autotuner with a
+// persistent JSON cache, and CUDA-graph replay.
+//
+// Plan (create): the problem sizes are given once on the host.  Each problem
+// is assigned a tile config by its size bucket (the autotuner's table), cut
+// into output tiles, and the tiles (TRSM: whole problems) are scheduled onto
+// a fixed grid of persistent CTAs longest-processing-time first; the
+// per-CTA lists are interleaved so that CTA b runs items b, b + G, b + 2G, ...
+// Run: one kernel launch (optionally replayed from a captured CUDA graph),
+// no allocation, so it can itself be captured by the caller.
+//
+// Autotuner: for every size bucket present in a batch (bucket = ceil(log2 of
+// max(m, n)), K class), each candidate tile config is timed on that bucket's
+// problems with CUDA events on synthetic operands; the winner is kept in an
+// in-process table and, when ZYNUM_GPU_TUNE_CACHE names a file, in a JSON
+// cache keyed by GPU name, SM count, dtype, transposes and bucket.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <queue>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/zynum_blas_gpu.h"
+#include "batched.h"
+#include "runtime.h"
+
+namespace zb {
+namespace {
+
+inline char upc(char c) { return (c >= 'a' && c <= 'z') ? (char)(c - 32) : c; }
+
+int ceil_log2(int x) {
+    int r = 0;
+    while ((1 << r) < x) ++r;
+    return r;
+}
+
+// Size bucket of a GEMM problem: log2 class of max(m, n) (3..9) x K class (3).
+int gemm_bucket(int m, int n, int k) {
+    int mn = std::max(1, std::max(m, n));
+    int c = std::min(9, std::max(3, ceil_log2(mn)));
+    int kc = k <= 64 ? 0 : (k <= 256 ? 1 : 2);
+    return (c - 3) * 3 + kc;
+}
+constexpr int kBuckets = 7 * 3;
+
+int default_cfg(int m, int n) {
+    const int mn = std::max(m, n);
+    if (mn <= 48) return TILE_CFG_32;
+    if (mn <= 160) return TILE_CFG_64;
+    return TILE_CFG_128;
+}
+
+std::vector<int> candidates(int bucket) {
+    const int c = bucket / 3 + 3;  // log2 class
+    if (c <= 5) return {TILE_CFG_32, TILE_CFG_64};
+    if (c <= 7) return {TILE_CFG_32, TILE_CFG_64, TILE_CFG_128};
+    return {TILE_CFG_64, TILE_CFG_128};
+}
+
+// ------------------------------------------------------------ tune cache
+struct TuneCache {
+    std::mutex mu;
+    std::map<std::string, int> table;
+    bool loaded = false;
+    std::string path() {
+        const char* p = std::getenv("ZYNUM_GPU_TUNE_CACHE");
+        return p ? std::string(p) : std::string();
+    }
+    void load() {
+        if (loaded) return;
+        loaded = true;
+        const std::string p = path();
+        if (p.empty()) return;
+        std::ifstream f(p);
+        if (!f) return;
+        std::stringstream ss;
+        ss << f.rdbuf();
+        const std::string s = ss.str();
+        // flat {"key": int, ...}
+        size_t i = 0;
+        while ((i = s.find('"', i)) != std::string::npos) {
+            const size_t j = s.find('"', i + 1);
+            if (j == std::string::npos) break;
+            const std::string key = s.substr(i + 1, j - i - 1);
+            const size_t c = s.find(':', j);
+            if (c == std::string::npos) break;
+            table[key] = std::atoi(s.c_str() + c + 1);
+            i = s.find_first_of(",}", c);
+            if (i == std::string::npos) break;
+        }
+    }
+    void save() {
+        const std::string p = path();
+        if (p.empty()) return;
+        std::ofstream f(p);
+        f << "{\n";
+        size_t q = 0;
+        for (auto& kv : table) f << "  \"" << kv.first << "\": " << kv.second << (++q < table.size() ? ",\n" : "\n");
+        f << "}\n";
+    }
+};
+TuneCache& tune_cache() {
+    static TuneCache* c = new TuneCache();
+    return *c;
+}
+
+std::string device_key() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, dev);
+    std::string name(prop.name);
+    for (auto& ch : name)
+        if (ch == ' ' || ch == '"') ch = '_';
+    return name + "|" + std::to_string(prop.multiProcessorCount);
+}
+
+int sm_count() {
+    int dev = 0, n = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+// LPT: returns per-CTA interleaved order of item indices (-1 padding).
+std::vector<int> lpt_schedule(const std::vector<double>& cost, int grid) {
+    std::vector<int> idx(cost.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<std::vector<int>> lists(grid);
+    using Slot = std::pair<double, int>;
+    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> pq;
+    for (int g = 0; g < grid; ++g) pq.push({0.0, g});
+    for (int i : idx) {
+        Slot s = pq.top();
+        pq.pop();
+        lists[s.second].push_back(i);
+        s.first += cost[i];
+        pq.push(s);
+    }
+    size_t depth = 0;
+    for (auto& l : lists) depth = std::max(depth, l.size());
+    std::vector<int> out(depth * grid, -1);
+    for (int g = 0; g < grid; ++g)
+        for (size_t r = 0; r < lists[g].size(); ++r) out[r * grid + g] = lists[g][r];
+    return out;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ batch object
+struct Batch {
+    int kind = 0;  // 0 GEMM, 1 TRSM
+    int dtype = BATCH_F64;
+    char ta = 'N', tb = 'N';
+    char side = 'L', uplo = 'L', diag = 'N';
+    int count = 0;
+    std::vector<int> m, n, k;
+    int grid = 148;
+    // device
+    int* d_dims = nullptr;
+    BatchWork* d_work = nullptr;
+    int* d_order = nullptr;
+    int n_items = 0;
+    int cfg_counts[3] = {0, 0, 0};
+    // graph replay
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    std::vector<unsigned char> graph_args;
+    cudaStream_t capture_stream = nullptr;
+
+    ~Batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        cudaFree(d_dims);
+        cudaFree(d_work);
+        cudaFree(d_order);
+    }
+};
+
+namespace {
+
+// Build the GEMM work list with one tile config per problem.
+std::vector<BatchWork> build_work(const Batch& b, const std::vector<int>& cfg, int grid, std::vector<int>* counts) {
+    std::vector<BatchWork> items;
+    std::vector<double> cost;
+    for (int q = 0; q < b.count; ++q) {
+        if (b.m[q] <= 0 || b.n[q] <= 0) continue;
+        const int e = batched_tile_edge(cfg[q]);
+        for (int n0 = 0; n0 < b.n[q]; n0 += e)
+            for (int m0 = 0; m0 < b.m[q]; m0 += e) {
+                items.push_back({q, m0, n0, cfg[q]});
+                // a tile costs its full edge^2 x k on the tensor pipe plus a fixed overhead
+                cost.push_back((double)e * e * std::max(b.k[q], 16) + 2.0e5);
+                if (counts) (*counts)[cfg[q]]++;
+            }
+    }
+    std::vector<int> order = lpt_schedule(cost, grid);
+    std::vector<BatchWork> out(order.size());
+    for (size_t i = 0; i < order.size(); ++i) out[i] = order[i] < 0 ? BatchWork{-1, 0, 0, 0} : items[order[i]];
+    return out;
+}
+
+cudaError_t upload_work(Batch& b, const std::vector<BatchWork>& w) {
+    cudaFree(b.d_work);
+    b.d_work = nullptr;
+    b.n_items = (int)w.size();
+    if (w.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&b.d_work, w.size() * sizeof(BatchWork));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(b.d_work, w.data(), w.size() * sizeof(BatchWork), cudaMemcpyHostToDevice);
+}
+
+// Time one tile config on the problems of one bucket with synthetic operands.
+float time_bucket(const Batch& b, const std::vector<int>& probs, int cfg, cudaStream_t st, void* buf,
+                  void** d_ptrs, int* d_lds) {
+    Batch sub;
+    sub.dtype = b.dtype;
+    sub.ta = b.ta;
+    sub.tb = b.tb;
+    sub.count = (int)probs.size();
+    for (int q : probs) {
+        sub.m.push_back(b.m[q]);
+        sub.n.push_back(b.n[q]);
+        sub.k.push_back(b.k[q]);
+    }
+    std::vector<int> dims;
+    for (int q = 0; q < sub.count; ++q) {
+        dims.push_back(sub.m[q]);
+        dims.push_back(sub.n[q]);
+        dims.push_back(sub.k[q]);
+    }
+    if (cudaMalloc(&sub.d_dims, dims.size() * sizeof(int)) != cudaSuccess) return 1e30f;
+    cudaMemcpy(sub.d_dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
+    std::vector<int> cfgv(sub.count, cfg);
+    if (upload_work(sub, build_work(sub, cfgv, b.grid, nullptr)) != cudaSuccess) return 1e30f;
+    // every problem reads / writes the same synthetic buffers (leading dimension 512)
+    std::vector<void*> ptrs(sub.count, buf);
+    std::vector<int> lds(sub.count, 512);
+    cudaMemcpy(d_ptrs, ptrs.data(), sub.count * sizeof(void*), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_lds, lds.data(), sub.count * sizeof(int), cudaMemcpyHostToDevice);
+    BatchDevice dev{sub.d_work, sub.n_items, sub.d_dims};
+    const double one = 1.0, zero = 0.0;
+    const float onef = 1.f, zerof = 0.f;
+    const void* al = b.dtype == BATCH_F64 ? (const void*)&one : (const void*)&onef;
+    const void* be = b.dtype == BATCH_F64 ? (const void*)&zero : (const void*)&zerof;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0, st);
+        launch_gemm_batched(dev, b.dtype, b.ta, b.tb, al, (const void* const*)d_ptrs, d_lds,
+                            (const void* const*)d_ptrs, d_lds, be, (void* const*)d_ptrs, d_lds, b.grid, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best = std::min(best, ms);  // first run warms up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+// Per-bucket tile configs for this batch: cached, tuned, or the default rule.
+std::vector<int> choose_cfgs(Batch& b, bool tune) {
+    std::vector<int> cfg(b.count);
+    TuneCache& tc = tune_cache();
+    std::lock_guard<std::mutex> lock(tc.mu);
+    tc.load();
+    const std::string dk = device_key() + "|" + (b.dtype == BATCH_F64 ? "f64" : "f32") + "|" + b.ta + b.tb + "|";
+    std::map<int, std::vector<int>> by_bucket;
+    for (int q = 0; q < b.count; ++q) by_bucket[gemm_bucket(b.m[q], b.n[q], b.k[q])].push_back(q);
+    std::map<int, int> chosen;
+    bool changed = false;
+    void* buf = nullptr;
+    void** d_ptrs = nullptr;
+    int* d_lds = nullptr;
+    cudaStream_t st = nullptr;
+    for (auto& kv : by_bucket) {
+        const std::string key = dk + std::to_string(kv.first);
+        auto it = tc.table.find(key);
+        if (it != tc.table.end()) {
+            chosen[kv.first] = it->second;
+            continue;
+        }
+        if (!tune) continue;
+        if (!buf) {
+            const size_t elt = b.dtype == BATCH_F64 ? 8 : 4;
+            if (cudaMalloc(&buf, (size_t)512 * 512 * 2 * elt + 1024 * 1024) != cudaSuccess) break;
+            cudaMemset(buf, 0, (size_t)512 * 512 * 2 * elt);
+            cudaMalloc(&d_ptrs, b.count * sizeof(void*));
+            cudaMalloc(&d_lds, b.count * sizeof(int));
+            cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        }
+        // tune on at most 512 problems of the bucket
+        std::vector<int> probs(kv.second.begin(), kv.second.begin() + std::min<size_t>(kv.second.size(), 512));
+        int best_cfg = -1;
+        float best_ms = 1e30f;
+        for (int c : candidates(kv.first)) {
+            const float ms = time_bucket(b, probs, c, st, buf, d_ptrs, d_lds);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_cfg = c;
+            }
+        }
+        if (best_cfg >= 0) {
+            tc.table[key] = best_cfg;
+            chosen[kv.first] = best_cfg;
+            changed = true;
+        }
+    }
+    if (buf) {
+        cudaStreamSynchronize(st);
+        cudaFree(buf);
+        cudaFree(d_ptrs);
+        cudaFree(d_lds);
+        cudaStreamDestroy(st);
+    }
+    if (changed) tc.save();
+    for (int q = 0; q < b.count; ++q) {
+        auto it = chosen.find(gemm_bucket(b.m[q], b.n[q], b.k[q]));
+        cfg[q] = it != chosen.end() ? it->second : default_cfg(b.m[q], b.n[q]);
+    }
+    return cfg;
+}
+
+int status_of(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return -(int)e;
+}
+
+// Launch `fn` directly, or through a graph captured once per distinct argument set.
+template <typename Fn>
+cudaError_t run_maybe_graph(Batch& b, const void* args, size_t args_len, bool use_graph, cudaStream_t st, Fn fn) {
+    if (!use_graph) return fn(st);
+    const unsigned char* p = static_cast<const unsigned char*>(args);
+    if (!b.exec || b.graph_args.size() != args_len || std::memcmp(b.graph_args.data(), p, args_len) != 0) {
+        if (b.exec) cudaGraphExecDestroy(b.exec);
+        if (b.graph) cudaGraphDestroy(b.graph);
+        b.exec = nullptr;
+        b.graph = nullptr;
+        cudaError_t e;
+        if (!b.capture_stream &&
+            (e = cudaStreamCreateWithFlags(&b.capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamBeginCapture(b.capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        cudaError_t le = fn(b.capture_stream);
+        e = cudaStreamEndCapture(b.capture_stream, &b.graph);
+        if (le != cudaSuccess) return le;
+        if (e != cudaSuccess) return e;
+        if ((e = cudaGraphInstantiate(&b.exec, b.graph, 0)) != cudaSuccess) return e;
+        b.graph_args.assign(p, p + args_len);
+    }
+    return cudaGraphLaunch(b.exec, st);
+}
+
+}  // namespace
+}  // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, char transa, char transb, int count,
+                                     const int* m, const int* n, const int* k, int tune) {
+    if (!out) return 1;
+    *out = nullptr;
+    if (dtype != BATCH_F64 && dtype != BATCH_F32) return 2;
+    const char ta = upc(transa), tb = upc(transb);
+    if (ta != 'N' && ta != 'T' && ta != 'C') return 3;
+    if (tb != 'N' && tb != 'T' && tb != 'C') return 4;
+    if (count < 0) return 5;
+    for (int q = 0; q < count; ++q)
+        if (m[q] < 0 || n[q] < 0 || k[q] < 0) return 6;
+    Batch* b = new Batch();
+    b->kind = 0;
+    b->dtype = dtype;
+    b->ta = ta;
+    b->tb = tb;
+    b->count = count;
+    b->m.assign(m, m + count);
+    b->n.assign(n, n + count);
+    b->k.assign(k, k + count);
+    b->grid = sm_count();
+    std::vector<int> dims;
+    for (int q = 0; q < count; ++q) {
+        dims.push_back(m[q]);
+        dims.push_back(n[q]);
+        dims.push_back(k[q]);
+    }
+    cudaError_t e = cudaSuccess;
+    if (count) {
+        if ((e = cudaMalloc(&b->d_dims, dims.size() * sizeof(int))) == cudaSuccess)
+            e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) {
+        std::vector<int> cfg = choose_cfgs(*b, tune != 0);
+        std::vector<int> counts(3, 0);
+        e = upload_work(*b, build_work(*b, cfg, b->grid, &counts));
+        for (int i = 0; i < 3; ++i) b->cfg_counts[i] = counts[i];
+    }
+    if (e != cudaSuccess) {
+        delete b;
+        return status_of(e, "gemm_batch_create");
+    }
+    *out = reinterpret_cast<zynum_blas_gpu_batch_t>(b);
+    return 0;
+}
+
+int zynum_blas_gpu_trsm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, char side, char uplo, char transa,
+                                     char diag, int count, const int* m, const int* n) {
+    if (!out) return 1;
+    *out = nullptr;
+    if (dtype != BATCH_F64 && dtype != BATCH_F32) return 2;
+    const char sd = upc(side), ul = upc(uplo), tr = upc(transa), dg = upc(diag);
+    if (sd != 'L') return 3;  // left-side solves (right-hand sides as columns of B)
+    if (ul != 'U' && ul != 'L') return 4;
+    if (tr != 'N' && tr != 'T' && tr != 'C') return 5;
+    if (dg != 'N' && dg != 'U') return 6;
+    if (count < 0) return 7;
+    for (int q = 0; q < count; ++q)
+        if (m[q] < 0 || n[q] < 0 || n[q] > 64) return 8;  // at most 64 right-hand sides per problem
+    Batch* b = new Batch();
+    b->kind = 1;
+    b->dtype = dtype;
+    b->side = sd;
+    b->uplo = ul;
+    b->ta = tr;
+    b->diag = dg;
+    b->count = count;
+    b->m.assign(m, m + count);
+    b->n.assign(n, n + count);
+    b->grid = sm_count();
+    std::vector<int> dims;
+    std::vector<double> cost;
+    for (int q = 0; q < count; ++q) {
+        dims.push_back(m[q]);
+        dims.push_back(n[q]);
+        cost.push_back((double)m[q] * m[q] * std::max(n[q], 8) + 1.0e4 * m[q]);
+    }
+    std::vector<int> order = lpt_schedule(cost, b->grid);
+    for (int& o : order)
+        if (o >= 0 && (m[o] == 0 || n[o] == 0)) o = -1;
+    b->n_items = (int)order.size();
+    cudaError_t e = cudaSuccess;
+    if (count) {
+        if ((e = cudaMalloc(&b->d_dims, dims.size() * sizeof(int))) == cudaSuccess)
+            e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && (e = cudaMalloc(&b->d_order, order.size() * sizeof(int))) == cudaSuccess)
+            e = cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        delete b;
+        return status_of(e, "trsm_batch_create");
+    }
+    *out = reinterpret_cast<zynum_blas_gpu_batch_t>(b);
+    return 0;
+}
+
+void zynum_blas_gpu_batch_destroy(zynum_blas_gpu_batch_t batch) { delete reinterpret_cast<Batch*>(batch); }
+
+int zynum_blas_gpu_batch_info(zynum_blas_gpu_batch_t batch, int* items, int* grid, int* cfg_counts) {
+    Batch* b = reinterpret_cast<Batch*>(batch);
+    if (!b) return 1;
+    if (items) *items = b->n_items;
+    if (grid) *grid = b->grid;
+    if (cfg_counts)
+        for (int i = 0; i < 3; ++i) cfg_counts[i] = b->cfg_counts[i];
+    return 0;
+}
+
+#define ZB_GEMM_BATCH_RUN(NAME, T, DT)                                                                              \
+    int NAME(zynum_blas_gpu_batch_t batch, T alpha, const T* const* a, const int* lda, const T* const* b,          \
+             const int* ldb, T beta, T* const* c, const int* ldc, void* stream, int use_graph) {                    \
+        Batch* bt = reinterpret_cast<Batch*>(batch);                                                                \
+        if (!bt || bt->kind != 0 || bt->dtype != DT) return 1;                                                      \
+        struct {                                                                                                    \
+            T al, be;                                                                                               \
+            const void *a, *lda, *b, *ldb, *c, *ldc;                                                                \
+        } args;                                                                                                     \
+        std::memset(&args, 0, sizeof(args)); /* padding takes part in the graph-argument comparison */            \
+        args.al = alpha;                                                                                            \
+        args.be = beta;                                                                                             \
+        args.a = a;                                                                                                 \
+        args.lda = lda;                                                                                             \
+        args.b = b;                                                                                                 \
+        args.ldb = ldb;                                                                                             \
+        args.c = c;                                                                                                 \
+        args.ldc = ldc;                                                                                             \
+        BatchDevice dev{bt->d_work, bt->n_items, bt->d_dims};                                                       \
+        auto fn = [&](cudaStream_t s) {                                                                             \
+            return launch_gemm_batched(dev, DT, bt->ta, bt->tb, &alpha, (const void* const*)a, lda,                \
+                                       (const void* const*)b, ldb, &beta, (void* const*)c, ldc, bt->grid, s);       \
+        };                                                                                                          \
+        return status_of(run_maybe_graph(*bt, &args, sizeof(args), use_graph != 0, (cudaStream_t)stream, fn),      \
+                         #NAME);                                                                                    \
+    }
+ZB_GEMM_BATCH_RUN(zynum_blas_gpu_dgemm_batch_run, double, BATCH_F64)
+ZB_GEMM_BATCH_RUN(zynum_blas_gpu_sgemm_batch_run, float, BATCH_F32)
+#undef ZB_GEMM_BATCH_RUN
+
+#define ZB_TRSM_BATCH_RUN(NAME, T, DT)                                                                              \
+    int NAME(zynum_blas_gpu_batch_t batch, T alpha, const T* const* a, const int* lda, T* const* b, const int* ldb, \
+             void* stream, int use_graph) {                                                                         \
+        Batch* bt = reinterpret_cast<Batch*>(batch);                                                                \
+        if (!bt || bt->kind != 1 || bt->dtype != DT) return 1;                                                      \
+        struct {                                                                                                    \
+            T al;                                                                                                   \
+            const void *a, *lda, *b, *ldb;                                                                          \
+        } args;                                                                                                     \
+        std::memset(&args, 0, sizeof(args));                                                                        \
+        args.al = alpha;                                                                                            \
+        args.a = a;                                                                                                 \
+        args.lda = lda;                                                                                             \
+        args.b = b;                                                                                                 \
+        args.ldb = ldb;                                                                                             \
+        auto fn = [&](cudaStream_t s) {                                                                             \
+            return launch_trsm_batched(bt->d_order, bt->n_items, bt->d_dims, DT, bt->uplo, bt->ta, bt->diag,       \
+                                       &alpha, (const void* const*)a, lda, (void* const*)b, ldb, bt->grid, s);     \
+        };                                                                                                          \
+        return status_of(run_maybe_graph(*bt, &args, sizeof(args), use_graph != 0, (cudaStream_t)stream, fn),      \
+                         #NAME);                                                                                    \
+    }
+ZB_TRSM_BATCH_RUN(zynum_blas_gpu_dtrsm_batch_run, double, BATCH_F64)
+ZB_TRSM_BATCH_RUN(zynum_blas_gpu_strsm_batch_run, float, BATCH_F32)
+#undef ZB_TRSM_BATCH_RUN
+
+}  // extern "C"
