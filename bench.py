@@ -265,6 +265,30 @@ def bench_batched(torch, blas, steps, warmup, seed=7):
     return out
 
 
+# ----------------------------------------------------------- differentiation
+def bench_differentiation(torch, steps, warmup, n=4096, r=512, seed=11):
+    """X = TRSM(L, B), C = SYRK(X^T) = X^T X, loss = sum(sin(C)); forward + backward with X recomputed.
+    L: n x n lower, off-diagonals N(0, 1/n), diagonal 1 + |N(0,1)|; B: n x r N(0,1)."""
+    from zynum_b200 import autograd as ag
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    L = torch.tril(torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64) / np.sqrt(n), -1)
+    L += torch.diag(1 + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
+    B = torch.randn(n, r, generator=g, device="cuda", dtype=torch.float64)
+    L.requires_grad_(True)
+    B.requires_grad_(True)
+
+    def step():
+        loss = ag.chain_loss(L, B, recompute=True)
+        torch.autograd.grad(loss, (L, B))
+
+    ms = time_device(torch, step, steps, warmup, torch.cuda.current_stream())
+    # nominal flops: forward TRSM n^2 r + SYRK r(r+1)n; backward TRSM (dB) n^2 r + recompute n^2 r
+    # + dL = -tril(dB X^T) n^2 r + dX = X (G + G^T) 4 n r^2
+    gflop = (3 * n * n * r + n * n * r + r * (r + 1) * n + 4 * n * r * r) / 1e9
+    return {"n": n, "nrhs": r, "ms_fwd_bwd": ms, "gflop_nominal": gflop, "gflops": gflop / (ms * 1e-3),
+            "recompute": True}
+
+
 # ---------------------------------------------------------------- our arm
 def time_device(torch, fn, steps, warmup, stream):
     for _ in range(warmup):
@@ -407,6 +431,7 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_batched:
         line["batched"] = bench_batched(torch, blas, max(3, args.steps), args.warmup)
+        line["differentiation"] = bench_differentiation(torch, max(3, args.steps), args.warmup)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(n if n <= 8192 else 8192, 256)
     print(json.dumps(line), flush=True)

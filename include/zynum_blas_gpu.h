@@ -164,6 +164,17 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n,
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
                                                    int lda, float beta, float *c, int ldc, void *stream);
 
+/* Triangle-restricted GEMM ("gemmt"; no counterpart in the reference, used by
+ * the TRSM adjoint): C := alpha op(A) op(B) + beta C computed and written only
+ * on the uplo triangle of the n x n matrix C (A: n x k after op, B: k x n).
+ * Argument numbering: uplo 1, transa 2, transb 3, n 4, k 5, lda 8, ldb 10, ldc 13. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemmt_device(char uplo, char transa, char transb, int n, int k, double alpha,
+                                                    const double *a, int lda, const double *b, int ldb, double beta,
+                                                    double *c, int ldc, void *stream);
+/* Copy the uplo triangle of an n x n device matrix onto the other triangle
+ * (turns a SYRK result into the full symmetric matrix). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsymmetrize_device(char uplo, int n, double *c, int ldc, void *stream);
+
 /* ------------------------------------------------- variable-size batches
  * No counterpart in the reference (Zynum has no batched API).  A batch plan is
  * created once from HOST arrays of problem sizes; running it is one

@@ -73,6 +73,10 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
                  "zynum_blas_gpu_ssyrk_device"):
         getattr(L, name).restype = i
+    L.zynum_blas_gpu_dgemmt_device.argtypes = [ch, ch, ch, i, i, d, P, i, P, i, d, P, i, P]
+    L.zynum_blas_gpu_dgemmt_device.restype = i
+    L.zynum_blas_gpu_dsymmetrize_device.argtypes = [ch, i, P, i, P]
+    L.zynum_blas_gpu_dsymmetrize_device.restype = i
     IP = C.POINTER(C.c_int)
     L.zynum_blas_gpu_gemm_batch_create.argtypes = [C.POINTER(P), i, ch, ch, i, P, P, P, i]
     L.zynum_blas_gpu_gemm_batch_create.restype = i

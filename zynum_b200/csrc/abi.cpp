@@ -9,6 +9,7 @@
 //   * quick returns: m <= 0 or n <= 0 does nothing; k == 0 or alpha == 0 gives
 //     C = beta * C with beta == 0 writing exact zeros (gemm.zig:1392-1414).
 // The compute always runs on the GPU; there is no CPU fallback.
+#include <algorithm>
 #include <cctype>
 #include <cstdio>
 #include <cstring>
@@ -206,6 +207,17 @@ size_t real_scratch_bytes(int m, int n, int k, float*) {
     return splitk_workspace_elems(m, n, p.splits) * sizeof(float);
 }
 
+// Scratch that covers every GEMM of shape up to m x n x k (TRSM's recursive
+// updates): split-K partials never exceed sm_count x 128 x 128 elements
+// (splits <= sm_count / tiles and tiles >= m n / 128^2), and the Ozaki planes
+// grow with every dimension.
+template <typename T>
+size_t real_scratch_bound(int m, int n, int k) {
+    Context& cx = context();
+    const size_t splitk = (size_t)cx.sm_count * 128 * 128 * sizeof(T) + 4096;
+    return std::max(splitk, real_scratch_bytes(m, n, k, (T*)nullptr));
+}
+
 // A fixed region handed to the real GEMMs of a complex call.
 struct FixedScratch {
     void* base;
@@ -371,9 +383,9 @@ template <typename T, typename Scratch>
 cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
     if (t.m <= 0 || t.n <= 0) return cudaSuccess;
     const size_t planes = trsm_plane_bytes<T>(t.side, t.m, t.n);
-    // largest GEMM of the solve: the first trailing update
-    const int big_m = (t.side == 'L') ? t.m : t.m, big_n = (t.side == 'L') ? t.n : t.n;
-    const size_t real = real_scratch_bytes(big_m, big_n, 64, (T*)nullptr);
+    // the GEMMs of the recursive solve are at most m x n x (order of A)
+    const int na = (t.side == 'L') ? t.m : t.n;
+    const size_t real = real_scratch_bound<T>(t.m, t.n, na);
     void* ws = nullptr;
     cudaError_t e = scratch(planes + real, st, &ws);
     if (e != cudaSuccess) return e;
@@ -771,6 +783,42 @@ int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alph
 int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float* a, int lda, float beta,
                                 float* c, int ldc, void* stream) {
     return device_syrk<float>("ssyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
+}
+
+// GEMM restricted to one triangle of C (the "gemmt" extension): only elements
+// with row <= col (uplo 'U') or row >= col ('L') are computed and written.
+int zynum_blas_gpu_dgemmt_device(char uplo, char transa, char transb, int n, int k, double alpha, const double* a,
+                                 int lda, const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+    const char ul = up(&uplo), ta = up(&transa), tb = up(&transb);
+    if (!valid_uplo(ul)) return 1;
+    int info = gemm_error(ta, tb, n, n, k, lda, ldb, ldc);
+    // dgemm_ numbering -> (uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    if (info) return info <= 2 ? info + 1 : (info <= 4 ? 4 : info);
+    if (n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GemmArgsF64 g{ta, tb, n, n, k, alpha, a, lda, b, ldb, beta, c, ldc};
+    g.tri = (ul == 'U') ? 1 : 2;
+    if (k == 0) return cuda_status(syrk_scale_only<double>(n, ul, beta, c, ldc, st), "dgemmt_device");
+    GemmPlan p = plan_native_gemm(n, n, k, 8, cx.sm_count);
+    void* ws = nullptr;
+    const size_t need = splitk_workspace_elems(n, n, p.splits) * sizeof(double);
+    if (need && (e = cx.stream_scratch(st, need, &ws)) != cudaSuccess) return cuda_status(e, "dgemmt_device");
+    return cuda_status(dgemm_native(g, p, static_cast<double*>(ws), st), "dgemmt_device");
+}
+
+int zynum_blas_gpu_dsymmetrize_device(char uplo, int n, double* c, int ldc, void* stream) {
+    const char ul = up(&uplo);
+    if (!valid_uplo(ul)) return 1;
+    if (n < 0) return 2;
+    if (ldc < max1(n)) return 4;
+    return cuda_status(symmetrize_matrix<double>(ul, n, c, ldc, static_cast<cudaStream_t>(stream)), "dsymmetrize");
 }
 
 int zynum_blas_gpu_dgemm_device(char transa, char transb, int m, int n, int k, double alpha, const double* a,

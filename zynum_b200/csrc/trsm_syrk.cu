@@ -15,6 +15,8 @@
 //   (one dot product per (i, j) of the triangle).  GPU algorithm: the GEMM
 //   kernel in triangle mode: tiles outside the triangle are skipped and
 //   elements outside it are never written.
+#include <functional>
+
 #include "common.cuh"
 #include "trsm_syrk.h"
 
@@ -104,7 +106,27 @@ __global__ void scale_triangle(int n, int tri, T beta, T* __restrict__ c, long l
     }
 }
 
+// Copy the stored triangle of an n x n matrix onto the other one.
+template <typename T>
+__global__ void symmetrize(int n, int from_upper, T* __restrict__ c, long ldc) {
+    const long total = (long)n * n;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % n), j = (int)(q / n);
+        if (from_upper ? (i > j) : (i < j)) c[i + (long)j * ldc] = c[j + (long)i * ldc];
+    }
+}
+
 }  // namespace
+
+template <typename T>
+cudaError_t symmetrize_matrix(char uplo, int n, T* c, long ldc, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    symmetrize<T><<<grid_for((long)n * n), 256, 0, st>>>(n, uplo == 'U' ? 1 : 0, c, ldc);
+    count_launch();
+    return cudaGetLastError();
+}
+template cudaError_t symmetrize_matrix<double>(char, int, double*, long, cudaStream_t);
+template cudaError_t symmetrize_matrix<float>(char, int, float*, long, cudaStream_t);
 
 template <typename T>
 size_t trsm_plane_bytes(char side, int m, int n) {
@@ -138,51 +160,60 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     const bool upper = op_is_upper(t.uplo, t.trans);
     const char ta = (t.trans == 'N') ? 'N' : 'T';
     const long lda = t.lda, ldb = t.ldb;
-    // Left: lower -> blocks top-down; upper -> bottom-up.
-    // Right (X op(A) = B): upper -> column blocks left to right; lower -> right to left.
-    const bool forward = left ? !upper : upper;
-    for (int q = 0; q < nblk; ++q) {
-        const int bi = forward ? q : nblk - 1 - q;
-        const int kb = bi * kNB, s = std::min(kNB, na - kb);
-        const T* invb = inv + (long)bi * kNB * kNB;
-        if (left) {
-            // X_J = inv_J * B[kb:kb+s, :]  (s x n) -> W, then back into B
-            if ((e = gemm({'N', 'N', s, n, s, T(1), invb, kNB, t.b + kb, ldb, T(0), W, s})) != cudaSuccess) return e;
-            if ((e = cudaMemcpy2DAsync(t.b + kb, ldb * sizeof(T), W, (size_t)s * sizeof(T), (size_t)s * sizeof(T), n,
-                                       cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
-                return e;
-            if (!upper && kb + s < m) {
-                const int r0 = kb + s;
-                const T* asub = (ta == 'N') ? t.a + r0 + (long)kb * lda : t.a + kb + (long)r0 * lda;
-                if ((e = gemm({ta, 'N', m - r0, n, s, T(-1), asub, lda, t.b + kb, ldb, T(1), t.b + r0, ldb})) !=
-                    cudaSuccess)
-                    return e;
+    // op(A)[r0:r1, c0:c1] as a GEMM operand (pointer, transpose flag)
+    auto opa = [&](int r0, int c0) -> const T* {
+        return (ta == 'N') ? t.a + r0 + (long)c0 * lda : t.a + c0 + (long)r0 * lda;
+    };
+    // Recursive halving on 64-aligned boundaries: the two halves are solved
+    // recursively and coupled by one GEMM whose K is half the range, so most
+    // of the work runs as large GEMMs; 64-blocks use the inverted diagonal.
+    std::function<cudaError_t(int, int)> solve = [&](int p0, int p1) -> cudaError_t {
+        cudaError_t err;
+        const int len = p1 - p0;
+        if (len <= kNB) {
+            const T* invb = inv + (long)(p0 / kNB) * kNB * kNB;
+            if (left) {
+                if ((err = gemm({'N', 'N', len, n, len, T(1), invb, kNB, t.b + p0, ldb, T(0), W, len})) != cudaSuccess)
+                    return err;
+                return cudaMemcpy2DAsync(t.b + p0, ldb * sizeof(T), W, (size_t)len * sizeof(T), (size_t)len * sizeof(T),
+                                         n, cudaMemcpyDeviceToDevice, st);
             }
-            if (upper && kb > 0) {
-                const T* asub = (ta == 'N') ? t.a + (long)kb * lda : t.a + kb;
-                if ((e = gemm({ta, 'N', kb, n, s, T(-1), asub, lda, t.b + kb, ldb, T(1), t.b, ldb})) != cudaSuccess)
-                    return e;
-            }
-        } else {
-            // X_J = B[:, kb:kb+s] * inv_J  (m x s) -> W, then back into B
-            T* bj = t.b + (long)kb * ldb;
-            if ((e = gemm({'N', 'N', m, s, s, T(1), bj, ldb, invb, kNB, T(0), W, m})) != cudaSuccess) return e;
-            if ((e = cudaMemcpy2DAsync(bj, ldb * sizeof(T), W, (size_t)m * sizeof(T), (size_t)m * sizeof(T), s,
-                                       cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
-                return e;
-            if (upper && kb + s < n) {
-                const int c0 = kb + s;
-                const T* asub = (ta == 'N') ? t.a + kb + (long)c0 * lda : t.a + c0 + (long)kb * lda;
-                if ((e = gemm({'N', ta, m, n - c0, s, T(-1), bj, ldb, asub, lda, T(1), t.b + (long)c0 * ldb, ldb})) !=
-                    cudaSuccess)
-                    return e;
-            }
-            if (!upper && kb > 0) {
-                const T* asub = (ta == 'N') ? t.a + kb : t.a + (long)kb * lda;
-                if ((e = gemm({'N', ta, m, kb, s, T(-1), bj, ldb, asub, lda, T(1), t.b, ldb})) != cudaSuccess) return e;
-            }
+            T* bj = t.b + (long)p0 * ldb;
+            if ((err = gemm({'N', 'N', m, len, len, T(1), bj, ldb, invb, kNB, T(0), W, m})) != cudaSuccess) return err;
+            return cudaMemcpy2DAsync(bj, ldb * sizeof(T), W, (size_t)m * sizeof(T), (size_t)m * sizeof(T), len,
+                                     cudaMemcpyDeviceToDevice, st);
         }
-    }
+        const int mid = p0 + ((len / 2 + kNB - 1) / kNB) * kNB;
+        const int h1 = mid - p0, h2 = p1 - mid;
+        if (left) {
+            if (!upper) {  // rows p0..mid first, then update mid..p1
+                if ((err = solve(p0, mid)) != cudaSuccess) return err;
+                if ((err = gemm({ta, 'N', h2, n, h1, T(-1), opa(mid, p0), lda, t.b + p0, ldb, T(1), t.b + mid,
+                                 ldb})) != cudaSuccess)
+                    return err;
+                return solve(mid, p1);
+            }
+            if ((err = solve(mid, p1)) != cudaSuccess) return err;
+            if ((err = gemm({ta, 'N', h1, n, h2, T(-1), opa(p0, mid), lda, t.b + mid, ldb, T(1), t.b + p0, ldb})) !=
+                cudaSuccess)
+                return err;
+            return solve(p0, mid);
+        }
+        // right side: X op(A) = B over column ranges
+        if (upper) {
+            if ((err = solve(p0, mid)) != cudaSuccess) return err;
+            if ((err = gemm({'N', ta, m, h2, h1, T(-1), t.b + (long)p0 * ldb, ldb, opa(p0, mid), lda, T(1),
+                             t.b + (long)mid * ldb, ldb})) != cudaSuccess)
+                return err;
+            return solve(mid, p1);
+        }
+        if ((err = solve(mid, p1)) != cudaSuccess) return err;
+        if ((err = gemm({'N', ta, m, h1, h2, T(-1), t.b + (long)mid * ldb, ldb, opa(mid, p0), lda, T(1),
+                         t.b + (long)p0 * ldb, ldb})) != cudaSuccess)
+            return err;
+        return solve(p0, mid);
+    };
+    if ((e = solve(0, na)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

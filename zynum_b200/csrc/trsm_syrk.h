@@ -33,6 +33,10 @@ size_t trsm_plane_bytes(char side, int m, int n);
 template <typename T>
 cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
 
+// Copy the uplo triangle of the n x n matrix c onto the other triangle.
+template <typename T>
+cudaError_t symmetrize_matrix(char uplo, int n, T* c, long ldc, cudaStream_t st);
+
 // SYRK with k == 0: C := beta C on the triangle.
 template <typename T>
 cudaError_t syrk_scale_only(int n, char uplo, T beta, T* c, long ldc, cudaStream_t st);
