@@ -438,6 +438,102 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+# ------------------------------------------------------------------ suites
+def suite_precision(args):
+    """DGEMM 8192^3 native vs Ozaki for phi in {0, 4, 8} and SGEMM 8192^3 3xBF16 vs native FP32:
+    TFLOP/s and max / median relative error against the double-double oracle on sampled entries."""
+    import torch
+    from oracle import oracle as orc
+    from zynum_b200 import blas
+    n = args.size
+    flop = 2.0 * n ** 3
+    stream = torch.cuda.current_stream()
+    out = {"suite": "precision", "n": n, "dgemm": {}, "sgemm": {}}
+    for phi in (0.0, 4.0, 8.0):
+        A, B = make_inputs(torch, n, phi, 1234, torch.device("cuda"))
+        C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        a_h = np.asfortranarray(A.cpu().numpy().T)
+        b_h = np.asfortranarray(B.cpu().numpy().T)
+        row = {}
+        for name, mid in (("native", blas.METHOD_NATIVE), ("ozaki", blas.METHOD_OZAKI)):
+            blas.set_dgemm_method(mid)
+            fn = lambda: blas.dgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
+            ms = time_device(torch, fn, args.steps, args.warmup, stream)
+            fn()
+            torch.cuda.synchronize()
+            err = sampled_error(orc, a_h, b_h, np.asfortranarray(C.cpu().numpy().T), n)
+            row[name] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, **err}
+            if name == "ozaki":
+                from zynum_b200 import ozaki_info
+                row[name]["slices"] = ozaki_info(n, n, n)["slices"]
+        blas.set_dgemm_method(blas.METHOD_NATIVE)
+        out["dgemm"][f"phi={phi:g}"] = row
+        del A, B, C
+    g = torch.Generator(device="cuda").manual_seed(99)
+    A = torch.rand((n, n), generator=g, device="cuda", dtype=torch.float32) * 2 - 1
+    B = torch.rand((n, n), generator=g, device="cuda", dtype=torch.float32) * 2 - 1
+    C = torch.zeros((n, n), dtype=torch.float32, device="cuda")
+    a_h = np.asfortranarray(A.cpu().numpy().T)
+    b_h = np.asfortranarray(B.cpu().numpy().T)
+    for name, mid in (("native_fp32", blas.SMETHOD_NATIVE), ("bf16x3", blas.SMETHOD_BF16X3)):
+        blas.set_sgemm_method(mid)
+        fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
+        ms = time_device(torch, fn, args.steps, args.warmup, stream)
+        fn()
+        torch.cuda.synchronize()
+        err = sampled_error(orc, a_h, b_h, np.asfortranarray(C.cpu().numpy().T.astype(np.float32)), n)
+        out["sgemm"][name] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, **err}
+    blas.set_sgemm_method(blas.SMETHOD_NATIVE)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def suite_sweep(args):
+    """Native GEMM shape sweep (FP64 and FP32): square n^3, tall-skinny 131072 x 64 x 64,
+    K-dominant 256 x 256 x 262144, beta in {0, 1}; ZGEMM / CGEMM 4096^3."""
+    import torch
+    from zynum_b200 import blas
+    stream = torch.cuda.current_stream()
+    rows = []
+    shapes = [(n, n, n) for n in (256, 1024, 4096, 8192, 16384)] + [(131072, 64, 64), (256, 256, 262144)]
+    for dt, tdt, fn in (("f64", torch.float64, blas.dgemm_device), ("f32", torch.float32, blas.sgemm_device)):
+        for (m, n, k) in shapes:
+            if dt == "f64" and m == 16384:
+                pass
+            g = torch.Generator(device="cuda").manual_seed(m + n + k)
+            A = torch.rand((k, m), generator=g, device="cuda", dtype=tdt) * 2 - 1   # column-major m x k
+            B = torch.rand((n, k), generator=g, device="cuda", dtype=tdt) * 2 - 1   # column-major k x n
+            C = torch.rand((n, m), generator=g, device="cuda", dtype=tdt) * 2 - 1
+            for beta in (0.0, 1.0):
+                f = lambda: fn("N", "N", m, n, k, 1.0, A, m, B, k, beta, C, m)  # noqa: E731
+                steps = max(2, min(args.steps, int(2e12 / (2.0 * m * n * k)) + 2))
+                ms = time_device(torch, f, steps, max(1, args.warmup), stream)
+                esz = 8 if dt == "f64" else 4
+                byts = esz * (m * k + k * n + m * n * (2 if beta else 1))
+                rows.append({"dtype": dt, "m": m, "n": n, "k": k, "beta": beta, "ms": ms,
+                             "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12, "gbs": byts / (ms * 1e-3) / 1e9})
+            del A, B, C
+    for dt, tdt, fn in (("z", torch.complex128, blas.zgemm_device), ("c", torch.complex64, blas.cgemm_device)):
+        n = 4096
+        g = torch.Generator(device="cuda").manual_seed(5)
+        real = torch.float64 if dt == "z" else torch.float32
+        A = torch.complex(torch.rand((n, n), generator=g, device="cuda", dtype=real) * 2 - 1,
+                          torch.rand((n, n), generator=g, device="cuda", dtype=real) * 2 - 1)
+        B = torch.complex(torch.rand((n, n), generator=g, device="cuda", dtype=real) * 2 - 1,
+                          torch.rand((n, n), generator=g, device="cuda", dtype=real) * 2 - 1)
+        C = torch.zeros((n, n), device="cuda", dtype=tdt)
+        for cm, cname in ((blas.COMPLEX_4M, "4M"), (blas.COMPLEX_3M, "3M")):
+            blas.set_complex_method(cm)
+            f = lambda: fn("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
+            ms = time_device(torch, f, max(2, args.steps), max(1, args.warmup), stream)
+            rows.append({"dtype": dt, "m": n, "n": n, "k": n, "beta": 0.0, "method": cname, "ms": ms,
+                         "tflops": 8.0 * n ** 3 / (ms * 1e-3) / 1e12})
+        blas.set_complex_method(blas.COMPLEX_4M)
+        del A, B, C
+    print(json.dumps({"suite": "sweep", "rows": rows}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,6 +546,8 @@ def main(argv=None):
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep"], default="headline",
+                    help="precision / sweep: secondary measurement suites (one JSON line each)")
     args = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -466,6 +564,10 @@ def main(argv=None):
     try:
         if args.impl == "reference":
             return run_reference(args, rank, world)
+        if args.suite == "precision":
+            return suite_precision(args)
+        if args.suite == "sweep":
+            return suite_sweep(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
