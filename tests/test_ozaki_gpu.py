@@ -106,6 +106,33 @@ def test_ozaki_config1_matches_native_error(blas, oracle):
     assert errs[blas.METHOD_OZAKI] <= errs[blas.METHOD_NATIVE], errs
 
 
+@pytest.mark.parametrize("phi", [0.0, 2.0, 4.0, 8.0])
+def test_ozaki_auto_slices_match_native_error(blas, oracle, phi):
+    """Automatic slice count on u * 10^e data (u ~ U[-1,1], e ~ U[-phi,phi]), 2048^2 x 2048:
+    the max relative error on 4096 sampled entries of C (double-double oracle) is no worse
+    than native FP64's on the same entries."""
+    rng = np.random.default_rng(int(phi) + 77)
+    n = 2048
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-phi, phi, (n, n)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-phi, phi, (n, n)))
+    rows = rng.integers(0, n, 4096)
+    cols = rng.integers(0, n, 4096)
+    hi, lo, _ = oracle.ddgemm_sampled("N", "N", n, a, n, b, n, rows, cols)
+    exact = hi + lo
+    errs = {}
+    for method in (blas.METHOD_NATIVE, blas.METHOD_OZAKI):
+        c = np.zeros((n, n), order="F")
+        blas.set_dgemm_method(method)
+        old = blas.set_ozaki_slices(0)
+        try:
+            blas.dgemm("N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c, n)
+        finally:
+            blas.set_ozaki_slices(old)
+            blas.set_dgemm_method(blas.METHOD_NATIVE)
+        errs[method] = float((np.abs(c[rows, cols] - exact) / np.abs(exact)).max())
+    assert errs[blas.METHOD_OZAKI] <= errs[blas.METHOD_NATIVE], errs
+
+
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T"), ("N", "T")])
 def test_sgemm_bf16x3(blas, oracle, ta, tb):
     rng = np.random.default_rng(3)

@@ -34,9 +34,11 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 
 #include "common.cuh"
@@ -57,7 +59,7 @@ constexpr int kBChunk = kUN * kChunkBytes;  // 32 KB
 constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int kMaxSteps = 96;
 constexpr int kMaxJobs = 16;
-constexpr size_t kSmemBytes = 1024 /*align slack*/ + kASlots * kAChunk + kBSlots * kBChunk + 256 + kUN * 8;
+constexpr size_t kSmemBytes = 1024 /*align slack*/ + kASlots * kAChunk + kBSlots * kBChunk + 256 + kUN * 8 + 3 * kMaxSteps;
 
 enum Kind : int { KIND_I8 = 0, KIND_BF16 = 1 };
 enum Epi : int { EPI_OZAKI_F64 = 0, EPI_F32 = 1 };
@@ -140,6 +142,73 @@ struct Ring {
     }
 };
 
+// Per-step flags of the job schedule, staged in shared memory once per CTA so
+// the single MMA-issuing thread reads one byte per step instead of indexing
+// the parameter space.
+enum : uint8_t { SF_ACC1 = 1, SF_NEW_A = 2, SF_NEW_B = 4, SF_REL_A = 8, SF_REL_B = 16 };
+
+struct Sched {
+    uint8_t flags[kMaxSteps];
+    uint8_t a[kMaxSteps];
+    uint8_t b[kMaxSteps];
+};
+
+ZB_DEVICE void build_sched(const UmmaParams& P, Sched* s) {
+    for (int j = 0; j < P.num_jobs; ++j) {
+        const int f0 = P.job_first_step[j], n = P.job_num_steps[j];
+        for (int q = 0; q < n; ++q) {
+            const int st = f0 + q;
+            uint8_t f = P.step_acc[st] ? SF_ACC1 : 0;
+            if (q == 0 || P.step_a[st] != P.step_a[st - 1]) f |= SF_NEW_A;
+            if (q == 0 || P.step_b[st] != P.step_b[st - 1]) f |= SF_NEW_B;
+            if (q == n - 1 || P.step_a[st + 1] != P.step_a[st]) f |= SF_REL_A;
+            if (q == n - 1 || P.step_b[st + 1] != P.step_b[st]) f |= SF_REL_B;
+            s->flags[st] = f;
+            s->a[st] = (uint8_t)P.step_a[st];
+            s->b[st] = (uint8_t)P.step_b[st];
+        }
+    }
+}
+
+// MMA issue for one job over K chunks [c0, c1): 4 UMMAs (K = 4 x 32 bytes)
+// per step, operand descriptors built once per slot and advanced by 32 bytes
+// (+2 in the descriptor's 16-byte address units) per UMMA.
+template <int ASLOTS, int BSLOTS, int ACHUNK, int BCHUNK, class Mma, class Commit>
+ZB_DEVICE bool mma_job(const uint8_t* flags, int n_steps, int c0, int c1, Ring& ra, Ring& rb, uint64_t* fullA,
+                       uint64_t* fullB, uint64_t* emptyA, uint64_t* emptyB, uint32_t sA0, uint32_t sB0,
+                       uint32_t tmem_base, volatile int* abort_flag, int* status, Mma mma, Commit commit) {
+    uint32_t started = 0;
+    uint64_t adesc = 0, bdesc = 0;
+    int a_slot = 0, b_slot = 0;
+    for (int kc = c0; kc < c1; ++kc) {
+        for (int q = 0; q < n_steps; ++q) {
+            const uint32_t f = flags[q];
+            if (f & SF_NEW_A) {
+                a_slot = ra.slot;
+                if (!wait_phase(&fullA[a_slot], ra.phase, abort_flag, status, 4)) return false;
+                ra.advance(ASLOTS);
+                adesc = umma_desc_sw128(sA0 + a_slot * ACHUNK);
+            }
+            if (f & SF_NEW_B) {
+                b_slot = rb.slot;
+                if (!wait_phase(&fullB[b_slot], rb.phase, abort_flag, status, 5)) return false;
+                rb.advance(BSLOTS);
+                bdesc = umma_desc_sw128(sB0 + b_slot * BCHUNK);
+            }
+            const uint32_t acc_i = f & SF_ACC1;
+            const uint32_t d = tmem_base + acc_i * kUN;
+            mma(d, adesc, bdesc, (started >> acc_i) & 1u);
+            mma(d, adesc + 2, bdesc + 2, 1u);
+            mma(d, adesc + 4, bdesc + 4, 1u);
+            mma(d, adesc + 6, bdesc + 6, 1u);
+            started |= 1u << acc_i;
+            if (f & SF_REL_A) commit(&emptyA[a_slot]);
+            if (f & SF_REL_B) commit(&emptyB[b_slot]);
+        }
+    }
+    return true;
+}
+
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
 umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -156,8 +225,10 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     uint64_t* tempty = tfull + 1;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    Sched* sched = reinterpret_cast<Sched*>(smem_tail_scratch(smem) + kUN * 8);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 32) build_sched(P, sched);
     if (threadIdx.x == 0) {
         for (int i = 0; i < kASlots; ++i) {
             mbar_init(&fullA[i], 1);
@@ -177,6 +248,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         prefetch_tmap(&tmB);
     }
     if (warp == 1) {
+        __syncwarp();  // lane 0 built the schedule; the allocation is warp-wide
         tmem_alloc(tmem_slot, 512);
         tmem_relinquish();
     }
@@ -197,28 +269,25 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         const int c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        const int f0 = P.job_first_step[j], n_steps = P.job_num_steps[j];
                         for (int kc = ks * P.kseg_chunks; ok && kc < c1; ++kc) {
-                            int prev_a = -1, prev_b = -1;
-                            for (int q = 0; q < P.job_num_steps[j]; ++q) {
-                                const int st = P.job_first_step[j] + q;
-                                const int pa = P.step_a[st], pb = P.step_b[st];
-                                if (pa != prev_a) {
+                            for (int q = 0; q < n_steps; ++q) {
+                                const uint32_t f = sched->flags[f0 + q];
+                                if (f & SF_NEW_A) {
                                     if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, P.status, 1)))
                                         break;
                                     mbar_arrive_expect_tx(&fullA[ra.slot], kAChunk);
                                     tma_load_2d(smem_u32(sA + ra.slot * kAChunk), &tmA, &fullA[ra.slot],
-                                                kc * elems_per_chunk, pa * P.m_pad + tm * kUM);
+                                                kc * elems_per_chunk, sched->a[f0 + q] * P.m_pad + tm * kUM);
                                     ra.advance(kASlots);
-                                    prev_a = pa;
                                 }
-                                if (pb != prev_b) {
+                                if (f & SF_NEW_B) {
                                     if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, P.status, 2)))
                                         break;
                                     mbar_arrive_expect_tx(&fullB[rb.slot], kBChunk);
                                     tma_load_2d(smem_u32(sB + rb.slot * kBChunk), &tmB, &fullB[rb.slot],
-                                                kc * elems_per_chunk, pb * P.n_pad + tn * kUN);
+                                                kc * elems_per_chunk, sched->b[f0 + q] * P.n_pad + tn * kUN);
                                     rb.advance(kBSlots);
-                                    prev_b = pb;
                                 }
                             }
                         }
@@ -248,48 +317,17 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         if (!(ok = wait_phase(tempty, tphase ^ 1, abort_flag, P.status, 3))) break;
                         tphase ^= 1;
                         tc_fence_after();
-                        uint32_t started = 0;  // bit per accumulator
-                        const int c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
-                        const int n_steps = P.job_num_steps[j];
-                        for (int kc = ks * P.kseg_chunks; ok && kc < c1; ++kc) {
-                            int prev_a = -1, prev_b = -1;
-                            int a_slot = 0, b_slot = 0;
-                            for (int q = 0; q < n_steps; ++q) {
-                                const int st = P.job_first_step[j] + q;
-                                const int pa = P.step_a[st], pb = P.step_b[st], acc_i = P.step_acc[st];
-                                if (pa != prev_a) {
-                                    a_slot = ra.slot;
-                                    if (!(ok = wait_phase(&fullA[ra.slot], ra.phase, abort_flag, P.status, 4))) break;
-                                    ra.advance(kASlots);
-                                    prev_a = pa;
-                                }
-                                if (pb != prev_b) {
-                                    b_slot = rb.slot;
-                                    if (!(ok = wait_phase(&fullB[rb.slot], rb.phase, abort_flag, P.status, 5))) break;
-                                    rb.advance(kBSlots);
-                                    prev_b = pb;
-                                }
-                                tc_fence_after();
-                                const uint32_t d = tmem_base + acc_i * kUN;
-                                const uint32_t a0 = smem_u32(sA + a_slot * kAChunk);
-                                const uint32_t b0 = smem_u32(sB + b_slot * kBChunk);
-#pragma unroll
-                                for (int kk = 0; kk < kChunkBytes / 32; ++kk) {
-                                    const uint64_t ad = umma_desc_sw128(a0 + kk * 32);
-                                    const uint64_t bd = umma_desc_sw128(b0 + kk * 32);
-                                    const uint32_t accumulate = (started >> acc_i) & 1u;
-                                    if (KIND == KIND_I8)
-                                        umma_i8(d, ad, bd, idesc, accumulate);
-                                    else
-                                        umma_f16(d, ad, bd, idesc, accumulate);
-                                    started |= 1u << acc_i;
-                                }
-                                // release a chunk after the last step that reads it
-                                const bool last = (q + 1 == n_steps);
-                                if (last || P.step_a[st + 1] != pa) umma_commit(&emptyA[a_slot]);
-                                if (last || P.step_b[st + 1] != pb) umma_commit(&emptyB[b_slot]);
-                            }
-                        }
+                        const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        auto mma = [idesc](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
+                            if (KIND == KIND_I8)
+                                umma_i8(d, ad, bd, idesc, acc);
+                            else
+                                umma_f16(d, ad, bd, idesc, acc);
+                        };
+                        auto commit = [](uint64_t* bar) { umma_commit(bar); };
+                        ok = mma_job<kASlots, kBSlots, kAChunk, kBChunk>(
+                            sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
                         if (ok) umma_commit(tfull);
                     }
         }
@@ -386,6 +424,234 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     __syncthreads();
     tc_fence_after();
     if (warp == 1) tmem_dealloc(tmem_base, 512);
+}
+
+// ------------------------------------------------- 2-CTA (cta_group::2)
+// The same schedule on a CTA pair: one M = 256 x N = 256 UMMA per K step,
+// issued by the even CTA.  CTA r loads A rows [256 tm + 128 r, +128) and B
+// rows [256 tn + 128 r, +128) into its own shared memory (the tensor cores
+// read both halves), and its TMEM receives C rows [256 tm + 128 r, +128) x 256.
+// Per SM this halves the B bytes of every chunk.  TMA completion bytes of both
+// CTAs are counted on the even CTA's "full" barriers; the MMA commits arrive on
+// the "empty" / "tfull" barriers of both CTAs (tcgen05.commit multicast); the
+// odd CTA's epilogue arrives on the even CTA's "tempty" barrier remotely.
+constexpr int kSlots2 = 6;                      // A and B rings, 128 x 128 B each
+constexpr int kChunk2 = 128 * kChunkBytes;      // 16 KB
+constexpr size_t kSmemBytes2 = 1024 + 2 * kSlots2 * kChunk2 + 512 + kUN * 8 + 3 * kMaxSteps;
+
+template <int KIND, int EPI>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const __grid_constant__ UmmaParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + kSlots2 * kChunk2;
+    uint64_t* fullA = reinterpret_cast<uint64_t*>(sB + kSlots2 * kChunk2);
+    uint64_t* emptyA = fullA + kSlots2;
+    uint64_t* fullB = emptyA + kSlots2;
+    uint64_t* emptyB = fullB + kSlots2;
+    uint64_t* tfull = emptyB + kSlots2;
+    uint64_t* tempty = tfull + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    double* colscale = reinterpret_cast<double*>(sB + kSlots2 * kChunk2 + 512);
+    Sched* sched = reinterpret_cast<Sched*>(sB + kSlots2 * kChunk2 + 512 + kUN * 8);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 32) build_sched(P, sched);
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kSlots2; ++i) {
+            mbar_init(&fullA[i], 1);
+            mbar_init(&emptyA[i], 1);
+            mbar_init(&fullB[i], 1);
+            mbar_init(&emptyB[i], 1);
+        }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 8);  // 4 epilogue warps in each CTA of the pair
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+    }
+    if (warp == 1) {
+        __syncwarp();  // lane 0 built the schedule; the allocation is warp-wide
+        tmem_alloc_2sm(tmem_slot, 512);
+        tmem_relinquish_2sm();
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // the peer's barriers exist before any remote arrival
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer (both CTAs)
+        if (lane == 0) {
+            Ring ra, rb;
+            bool ok = true;
+            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
+                int tm, tn;
+                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
+                const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
+                for (int j = 0; ok && j < P.num_jobs; ++j)
+                    for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                        const int c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        const int f0 = P.job_first_step[j], n_steps = P.job_num_steps[j];
+                        for (int kc = ks * P.kseg_chunks; ok && kc < c1; ++kc) {
+                            for (int q = 0; q < n_steps; ++q) {
+                                const uint32_t f = sched->flags[f0 + q];
+                                if (f & SF_NEW_A) {
+                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, P.status, 1)))
+                                        break;
+                                    if (leader) mbar_arrive_expect_tx(&fullA[ra.slot], 2 * kChunk2);
+                                    tma_load_2d_2sm(smem_u32(sA + ra.slot * kChunk2), &tmA,
+                                                    smem_u32(&fullA[ra.slot]) & 0xFEFFFFFFu, kc * elems_per_chunk,
+                                                    sched->a[f0 + q] * P.m_pad + arow);
+                                    ra.advance(kSlots2);
+                                }
+                                if (f & SF_NEW_B) {
+                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, P.status, 2)))
+                                        break;
+                                    if (leader) mbar_arrive_expect_tx(&fullB[rb.slot], 2 * kChunk2);
+                                    tma_load_2d_2sm(smem_u32(sB + rb.slot * kChunk2), &tmB,
+                                                    smem_u32(&fullB[rb.slot]) & 0xFEFFFFFFu, kc * elems_per_chunk,
+                                                    sched->b[f0 + q] * P.n_pad + brow);
+                                    rb.advance(kSlots2);
+                                }
+                            }
+                        }
+                    }
+            }
+            for (int i = 0; i < kSlots2; ++i) {
+                wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, nullptr, 0);
+                ra.advance(kSlots2);
+                wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, nullptr, 0);
+                rb.advance(kSlots2);
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------- MMA issuer (even CTA)
+        if (lane == 0 && leader) {
+            const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, 256, kUN) : umma_idesc(1, 1, 256, kUN);
+            Ring ra, rb;
+            uint32_t tphase = 0;
+            bool ok = true;
+            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
+                for (int j = 0; ok && j < P.num_jobs; ++j)
+                    for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                        if (!(ok = wait_phase(tempty, tphase ^ 1, abort_flag, P.status, 3))) break;
+                        tphase ^= 1;
+                        tc_fence_after();
+                        const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
+                        auto mma = [idesc](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
+                            if (KIND == KIND_I8)
+                                umma_i8_2sm(d, ad, bd, idesc, acc);
+                            else
+                                umma_f16_2sm(d, ad, bd, idesc, acc);
+                        };
+                        auto commit = [](uint64_t* bar) { umma_commit_2sm(bar, 0x3); };
+                        ok = mma_job<kSlots2, kSlots2, kChunk2, kChunk2>(
+                            sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
+                        if (ok) umma_commit_2sm(tfull, 0x3);
+                    }
+        }
+    } else {
+        // ---------------------------------------------- epilogue warps (both CTAs)
+        const int quarter = warp & 3;
+        const int row_in_tile = rank * 128 + quarter * 32 + lane;
+        const int et = threadIdx.x - 64;
+        const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
+        const uint32_t tempty_cta0 = mapa_shared(smem_u32(tempty), 0);
+        uint32_t tphase = 0;
+        bool ok = true;
+        for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
+            int tm, tn;
+            tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
+            const int row = tm * 256 + row_in_tile;
+            const bool row_ok = row < P.m;
+            int er = 0;
+            if (EPI == EPI_OZAKI_F64) {
+                if (row_ok) er = P.row_exp[row];
+                epilogue_bar_sync();
+                for (int c = et; c < kUN; c += 128) {
+                    const int col = tn * kUN + c;
+                    colscale[c] = (col < P.n) ? pow2(P.col_exp[col]) : 0.0;
+                }
+                epilogue_bar_sync();
+            }
+            bool first = true;
+            for (int j = 0; ok && j < P.num_jobs; ++j)
+                for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
+                    if (!(ok = wait_phase(tfull, tphase, abort_flag, P.status, 6))) break;
+                    tphase ^= 1;
+                    tc_fence_after();
+                    const bool two = P.job_groups[j] == 2;
+                    const double s0 = (EPI == EPI_OZAKI_F64) ? pow2(er - P.job_shift[j][0]) * P.alpha : 1.0;
+#pragma unroll 1
+                    for (int ch = 0; ch < kUN / 32; ++ch) {
+                        uint32_t r0[32], r1[32];
+                        tmem_ld_32x32b_x32(lane_addr + ch * 32, r0);
+                        if (two) tmem_ld_32x32b_x32(lane_addr + kUN + ch * 32, r1);
+                        tmem_ld_wait();
+                        const int col0 = tn * kUN + ch * 32;
+                        if (!row_ok) continue;
+                        const bool full_chunk = col0 + 32 <= P.n;
+                        if (EPI == EPI_OZAKI_F64) {
+                            double* cb = static_cast<double*>(P.c) + (long)col0 * P.ldc + row;
+                            double cin[32];
+                            const bool need_c = !first || P.beta != 0.0;
+                            if (need_c) {
+#pragma unroll
+                                for (int c = 0; c < 32; ++c)
+                                    cin[c] = (full_chunk || col0 + c < P.n) ? __ldcg(cb + (long)c * P.ldc) : 0.0;
+                            }
+                            const double* cs = colscale + ch * 32;
+#pragma unroll
+                            for (int c = 0; c < 32; ++c) {
+                                long long d = (int)r0[c];
+                                if (two) d += (long long)(int)r1[c] << 7;
+                                const double v = (double)d * s0 * cs[c];
+                                const double out = !need_c ? v : (first ? fma(P.beta, cin[c], v) : cin[c] + v);
+                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
+                            }
+                        } else {
+                            float* cb = static_cast<float*>(P.c) + (long)col0 * P.ldc + row;
+                            float cin[32];
+                            const bool need_c = !first || P.beta_f != 0.0f;
+                            if (need_c) {
+#pragma unroll
+                                for (int c = 0; c < 32; ++c)
+                                    cin[c] = (full_chunk || col0 + c < P.n) ? __ldcg(cb + (long)c * P.ldc) : 0.0f;
+                            }
+#pragma unroll
+                            for (int c = 0; c < 32; ++c) {
+                                const float v = P.alpha_f * __uint_as_float(r0[c]);
+                                const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
+                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
+                            }
+                        }
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_cluster(tempty_cta0);
+                    first = false;
+                }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // no CTA of the pair leaves while the other's MMAs or loads may touch it
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc_2sm(tmem_base, 512);
 }
 
 // ------------------------------------------------------------- splitting
@@ -663,6 +929,19 @@ cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const Umma
     return cudaGetLastError();
 }
 
+template <int KIND, int EPI>
+cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
+    auto kern = umma_slice_gemm_2cta<KIND, EPI>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes2);
+    if (e != cudaSuccess) return e;
+    const int pairs = std::min(P.num_tiles, sm_count_cached() / 2);
+    prof_begin(st);
+    kern<<<2 * pairs, kThreads, kSmemBytes2, st>>>(ma, mb, P);
+    count_launch();
+    prof_end(st);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 // Largest K (in 128-byte chunks) whose INT32 group sums cannot overflow:
@@ -672,13 +951,29 @@ static int max_kseg_chunks(int slices) {
     return limit < 1 ? 1 : (int)limit;
 }
 
+// The CTA-pair kernel is used from 256 rows up (ZYNUM_GPU_UMMA_2CTA=0 turns it off).
+static bool use_cta_pair(int m) {
+    static const bool enabled = [] {
+        const char* v = std::getenv("ZYNUM_GPU_UMMA_2CTA");
+        return !(v && v[0] == '0');
+    }();
+    return enabled && m >= 256;
+}
+
 bool ozaki_preferred(int m, int n, int k) { return (long)m * n >= 512L * 512 && k >= 256; }
 
 int ozaki_auto_slices(float spread_a, float spread_b) {
-    // 52 + spread bits must be covered by 7-bit digits for the truncation
-    // error to stay at or below the FP64 rounding error of native DGEMM
-    // (calibrated on U[-1,1] * 10^U[-phi,phi] data, phi in {0, 4, 8}).
-    int s = (int)ceilf((52.0f + spread_a + spread_b) / 7.0f);
+    // Truncating a row of A after s 7-bit digits leaves |dA_ik| < 2^(e_i - 7s)
+    // with 2^e_i the row maximum; the spread is log2(row max / mean |A_ik|).
+    // The error of the emulated product is then about
+    //   2^-7s (2^spread_a + 2^spread_b) sum_k |A_ik| |B_kj|,
+    // against about 2^-53 sum_k |A_ik| |B_kj| (with a data-dependent constant)
+    // for native FP64, so s = ceil((52 + log2(2^sa + 2^sb)) / 7).  Checked at
+    // 8192^3 on U[-1,1] * 10^U[-phi,phi] data for phi in {0, 2, 4, 8}: the
+    // emulated max relative error is 4x (phi 0) to 30x (phi 4) below native.
+    const float lead = fmaxf(spread_a, spread_b);
+    const float both = lead + log2f(1.0f + exp2f(fminf(spread_a, spread_b) - lead));
+    int s = (int)ceilf((52.0f + both) / 7.0f);
     if (s < 6) s = 6;
     if (s > kOzakiAutoMaxSlices) s = kOzakiAutoMaxSlices;
     return s;
@@ -694,7 +989,8 @@ OzakiPlan plan_ozaki(int m, int n, int k, int slices) {
     if (slices > kOzakiMaxSlices) slices = kOzakiMaxSlices;
     if (slices < 0) slices = 0;
     p.slices = slices;  // 0: chosen from the data at run time
-    p.m_pad = (int)round_up(m, kUM);
+    p.pair = use_cta_pair(m);
+    p.m_pad = (int)round_up(m, p.pair ? 2 * kUM : kUM);
     p.n_pad = (int)round_up(n, kUN);
     p.k_pad = (int)round_up(k, kChunkBytes);
     return p;
@@ -761,8 +1057,8 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)p.slices * p.m_pad, kUM)) !=
         cudaSuccess)
         return e;
-    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)p.slices * p.n_pad, kUN)) !=
-        cudaSuccess)
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)p.slices * p.n_pad,
+                      p.pair ? kUN / 2 : kUN)) != cudaSuccess)
         return e;
 
     UmmaParams P{};
@@ -774,7 +1070,7 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     P.kseg_chunks = max_kseg_chunks(p.slices);
     if (P.kseg_chunks > P.k_chunks) P.kseg_chunks = P.k_chunks;
     P.num_kseg = (P.k_chunks + P.kseg_chunks - 1) / P.kseg_chunks;
-    P.tiles_m = p.m_pad / kUM;
+    P.tiles_m = p.m_pad / (p.pair ? 2 * kUM : kUM);
     P.tiles_n = p.n_pad / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
     // Groups g = s+1 .. 2 (smallest contributions first), two per job: the
@@ -809,17 +1105,19 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     P.row_exp = expa;
     P.col_exp = expb;
     P.status = status;
+    if (p.pair) return launch_umma_2cta<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
     return launch_umma<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
 }
 
 size_t bf16x3_workspace_bytes(int m, int n, int k) {
-    const long mp = round_up(m, kUM), np = round_up(n, kUN), kp = round_up(k, 128);
+    const long mp = round_up(m, use_cta_pair(m) ? 2 * kUM : kUM), np = round_up(n, kUN), kp = round_up(k, 128);
     return (size_t)(2 * mp * kp * 2 + 2 * np * kp * 2 + 1024);
 }
 
 cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     // K is padded to 128 elements: the split kernel writes 128 columns per block.
-    const int mp = (int)round_up(g.m, kUM), np = (int)round_up(g.n, kUN), kp = (int)round_up(g.k, 128);
+    const bool pair = use_cta_pair(g.m);
+    const int mp = (int)round_up(g.m, pair ? 2 * kUM : kUM), np = (int)round_up(g.n, kUN), kp = (int)round_up(g.k, 128);
     __nv_bfloat16* a_planes = static_cast<__nv_bfloat16*>(ws);
     __nv_bfloat16* b_planes = a_planes + 2L * mp * kp;
     ViewF va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
@@ -832,7 +1130,9 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     CUtensorMap ma, mb;
     if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * mp, kUM)) != cudaSuccess) return e;
-    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * np, kUN)) != cudaSuccess) return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * np, pair ? kUN / 2 : kUN)) !=
+        cudaSuccess)
+        return e;
     UmmaParams P{};
     P.m = g.m;
     P.n = g.n;
@@ -841,7 +1141,7 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     P.k_chunks = kp / 64;
     P.kseg_chunks = P.k_chunks;
     P.num_kseg = 1;
-    P.tiles_m = mp / kUM;
+    P.tiles_m = mp / (pair ? 2 * kUM : kUM);
     P.tiles_n = np / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
     // one job, one FP32 accumulator: hi*lo, hi*hi, lo*hi (consecutive steps
@@ -862,6 +1162,7 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     P.beta_f = g.beta;
     P.c = g.c;
     P.ldc = g.ldc;
+    if (pair) return launch_umma_2cta<KIND_BF16, EPI_F32>(ma, mb, P, st);
     return launch_umma<KIND_BF16, EPI_F32>(ma, mb, P, st);
 }
 

@@ -17,6 +17,7 @@ struct OzakiPlan {
     int m_pad = 0;    // rows of A padded to the 128-row UMMA tile
     int n_pad = 0;    // columns of B padded to the 256-column UMMA tile
     int k_pad = 0;    // K padded to the 128-byte TMA box
+    bool pair = false;  // CTA-pair (cta_group::2, M = 256) slice-product kernel; m_pad is then a multiple of 256
 };
 
 // Whether the automatic method should prefer Ozaki for this shape.
