@@ -50,7 +50,7 @@ def _peaks():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -64,7 +64,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -78,25 +78,35 @@ class ClockSampler:
                 self.proc.kill()
             self.f.close()
 
-    def summary(self):
+    def summary(self, window=None):
+        """Median SM clock under load and the throttle reasons seen; `window` = (t0, t1) wall-clock
+        seconds (time.time()) restricts the samples to a timed region."""
         if self.proc is None or not self.path.exists():
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm, mx, reasons = [], None, set()
+        import datetime
+        sm, mx, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.path.read_text().splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                clk = float(parts[2])
+                mx = float(parts[3])
+                pw = float(parts[4])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            if window is not None and not (window[0] <= ts <= window[1]):
+                continue
+            sm.append(clk)
+            power.append(pw)
+            for nm, v in zip(names, parts[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
-        load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        load = [x for x in sm if mx and x > 0.3 * mx] or sm
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "power_w": statistics.median(power) if power else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -304,6 +314,14 @@ def time_device(torch, fn, steps, warmup, stream):
     return ev0.elapsed_time(ev1) / steps
 
 
+def _ozaki_desc(n):
+    from zynum_b200 import ozaki_info
+    info = ozaki_info(n, n, n)
+    if info["scheme"] == "crt":
+        return f"scheme II (CRT): {info['moduli']} int8 moduli, {info['products']} modular products"
+    return f"scheme I: {info['slices']} int8 slices, {info['products']} slice products"
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -339,7 +357,9 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
             launches0 = L.zynum_blas_gpu_launch_count()
             L.zynum_blas_gpu_profile(1)
+            t_begin = time.time()
             ms = time_device(torch, fn, args.steps, args.warmup, stream)
+            t_end = time.time()
             # one event pair per call around the dominant kernel: keep the timed steps' records
             buf = np.zeros(4096)
             cnt = L.zynum_blas_gpu_profile_read(buf.ctypes.data, 4096)
@@ -351,8 +371,11 @@ def run_ours(args, rank, world, local_rank):
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 ms = float(t.item())
             results[name] = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12, "launches_per_step": int(launches),
-                             "kernel_ms": kern_ms}
-    clk = clocks.summary()
+                             "kernel_ms": kern_ms, "window": (t_begin, t_end)}
+        time.sleep(0.1)  # the sampler's last lines cover the end of the timed region
+    clk = clocks.summary(results[methods[0][0]]["window"])
+    for name in results:
+        results[name]["clocks"] = clocks.summary(results[name].pop("window"))
 
     # errors of both methods vs the double-double oracle (rank 0, sampled entries)
     err = {}
@@ -404,9 +427,11 @@ def run_ours(args, rank, world, local_rank):
         achieved = ops / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / int8_peak) if achieved else None, "traffic": None,
-                "kernel": "ozaki int8 slice-product GEMM (tcgen05 kind::i8)",
+                "kernel": ("ozaki int8 modular-product GEMM (CRT residues, tcgen05 kind::i8)" if info["scheme"] == "crt"
+                           else "ozaki int8 slice-product GEMM (tcgen05 kind::i8)"),
                 "peak_source": f"2 x bf16_tflops of {peaks['_source']} peaks (int8 dense rate is 2x bf16 on sm_100)",
-                "work_per_launch": f"{info['slice_products']} slice products x 2*{n}^3 int8 ops"}
+                "work_per_launch": f"{info['products']} {'modular' if info['scheme'] == 'crt' else 'slice'} products"
+                                   f" x 2*{n}^3 int8 ops"}
     else:
         achieved = flop / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
@@ -420,6 +445,7 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "f64", "data": f"synthetic u*10^e, u~U[-1,1], e~U[-{args.phi},{args.phi}], seeded",
         "config": {"workload": f"DGEMM M=N=K={n} NN column-major FP64 alpha=1 beta=0",
                    "method": head[0], "l2": "inputs 3 x 512 MiB > 126 MB L2 (no flush needed)",
+                   **({"ozaki": _ozaki_desc(n)} if head[0] == "ozaki" else {}),
                    "parallelism": "replicas" if world > 1 else "single-GPU"},
         "methods": {k: {**v, **({"error": err[k]} if k in err else {})} for k, v in results.items()},
         "roofline": roof,

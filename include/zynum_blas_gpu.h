@@ -221,9 +221,19 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_sgemm_method(int method);
 /* Ozaki slice count (2..12), 0 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_slices(int slices);
-/* Slice count the Ozaki method uses for an m x n x k DGEMM under the current
- * setting (with the automatic setting: the count the most recent call chose
- * from its data), and the number of INT8 slice-product GEMMs (s(s+1)/2). */
+/* Ozaki scheme: 0 = automatic (CRT residues unless a slice count is set or
+ * K > 130816), 1 = INT8 slices (Ozaki scheme I), 2 = CRT residues (Ozaki
+ * scheme II; slices beyond K = 130816).  Returns the previous value.
+ * No reference counterpart (the reference has no emulated DGEMM). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_scheme(int scheme);
+/* CRT moduli (2..16), 0 = default (16).  Returns the previous value. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_moduli(int moduli);
+/* Scheme (1 slices, 2 CRT), digit count (slices, or moduli) and INT8 product
+ * GEMM count (s(s+1)/2 slice products, or one per modulus) the Ozaki method
+ * uses for an m x n x k DGEMM under the current settings; with automatic
+ * slices: the count the most recent slice-scheme call chose from its data. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ozaki_plan_ex(int m, int n, int k, int *scheme, int *digits, int *products);
+/* zynum_blas_gpu_ozaki_plan_ex without the scheme. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int *slices, int *products);
 /* Text of the last error seen by this thread ("" if none). */
 ZYNUM_BLAS_GPU_API const char *zynum_blas_gpu_last_error(void);

@@ -138,6 +138,16 @@ def test_split_k_path(blas, oracle, dtype):
     _run_case(blas, oracle, dtype, "T", "T", 96, 80, 40000, 40000, 80, 96, 1.0, 0.0)
 
 
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("T", "T"), ("C", "N")])
+def test_sgemm_operand_relayout_path(blas, oracle, ta, tb):
+    """m, n >= 1024: a K-contiguous operand (A with op T/C, B with op N) is first copied out
+    MN-contiguous into the workspace; odd leading dimensions and a split-K case included."""
+    _run_case(blas, oracle, np.float32, ta, tb, 1030, 1027, 301, (1030 if ta == "N" else 301) + 3,
+              (301 if tb == "N" else 1027) + 1, 1033, 0.75, -1.25)
+    _run_case(blas, oracle, np.float32, ta, tb, 1024, 1100, 4100, (1024 if ta == "N" else 4100) + 1,
+              (4100 if tb == "N" else 1100) + 2, 1025, 1.0, 0.0)
+
+
 def test_skinny_tile_path(blas, oracle):
     """Tall-skinny N <= 64 runs the 128 x 64 tile."""
     _run_case(blas, oracle, np.float64, "N", "N", 4096, 64, 64, 4096, 64, 4096, 1.0, 1.0)

@@ -133,6 +133,154 @@ def test_ozaki_auto_slices_match_native_error(blas, oracle, phi):
     assert errs[blas.METHOD_OZAKI] <= errs[blas.METHOD_NATIVE], errs
 
 
+# ----------------------------------------------------------- CRT scheme
+CRT_MODULI = [256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193, 191]
+
+
+def _crt_bits(nmod):
+    lm = sum(np.log2(CRT_MODULI[:nmod]))
+    return min(62, int(np.floor((lm - 2.0) / 2.0)))
+
+
+def _crt_case(blas, oracle, ta, tb, m, n, k, lda, ldb, ldc, alpha, beta, rng, nmod=0, phi=0.0, mat=None):
+    """CRT-scheme DGEMM against the double-double oracle.  Bound: with row scale
+    2^{a_i} <= 2^P / H_i (H_i = sqrt(max_p |a_ip| sum_p |a_ip|), likewise for columns of op(B)),
+    |C - C_exact| <= |alpha| (2^-P H_i sum_p |b_pj| + 2^-P H_j sum_p |a_ip| + k 2^-2P 4 H_i H_j)
+                     + 4 u (|alpha| |A||B| + |beta| |C0|)."""
+    if mat is None:
+        def mat(rows, cols, ld):
+            x = rng.uniform(-1, 1, (ld, cols))
+            if phi:
+                x *= 10.0 ** rng.uniform(-phi, phi, (ld, cols))
+            x[rows:] = -999.0
+            return np.asfortranarray(x)
+    a = mat(m if ta == "N" else k, k if ta == "N" else m, lda)
+    b = mat(k if tb == "N" else n, n if tb == "N" else k, ldb)
+    c = mat(m, n, ldc)
+    c0 = c.copy(order="F")
+    blas.set_dgemm_method(blas.METHOD_OZAKI)
+    old_s = blas.set_ozaki_scheme(blas.OZAKI_CRT)
+    old_m = blas.set_ozaki_moduli(nmod)
+    try:
+        from zynum_b200 import ozaki_info
+        info = ozaki_info(m, n, k)
+        assert info["scheme"] == "crt" and info["moduli"] == (nmod or 16), info
+        blas.dgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    finally:
+        blas.set_ozaki_moduli(old_m)
+        blas.set_ozaki_scheme(old_s)
+        blas.set_dgemm_method(blas.METHOD_NATIVE)
+    hi, lo = oracle.ddgemm(ta, tb, m, n, k, a, lda, b, ldb)
+    exact = alpha * (hi + lo) + beta * c0[:m, :n]
+    A, B = _op(a, ta, m, k), _op(b, tb, k, n)
+    P = _crt_bits(nmod or 16)
+    ha = np.sqrt(np.abs(A).max(axis=1) * np.abs(A).sum(axis=1))
+    hb = np.sqrt(np.abs(B).max(axis=0) * np.abs(B).sum(axis=0))
+    sa, sb = np.abs(A).sum(axis=1), np.abs(B).sum(axis=0)
+    bound = abs(alpha) * 2.0 ** -P * (ha[:, None] * sb[None, :] + sa[:, None] * hb[None, :]
+                                      + k * 4 * 2.0 ** -P * ha[:, None] * hb[None, :]) \
+        + 4 * U64 * (abs(alpha) * (np.abs(A) @ np.abs(B)) + abs(beta) * np.abs(c0[:m, :n]))
+    err = np.abs(c[:m, :n] - exact)
+    assert np.all(err <= bound), float((err / bound).max())
+    assert np.array_equal(c[m:], c0[m:]), "padding rows of C were written"
+    return err, exact
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+def test_crt_small_all_transposes(blas, oracle, ta, tb):
+    rng = np.random.default_rng(300)
+    _crt_case(blas, oracle, ta, tb, 200, 300, 150, 211, 309, 203, 1.5, 0.5, rng)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 300, 7), (300, 1, 129), (255, 257, 128), (256, 256, 256),
+                                   (513, 130, 1000), (64, 700, 33)], ids=lambda s: "x".join(map(str, s)))
+def test_crt_shapes_one_and_two_cta(blas, oracle, shape):
+    """m < 256 runs the one-CTA kernel, m >= 256 the CTA-pair kernel; ragged m / n / k."""
+    m, n, k = shape
+    rng = np.random.default_rng(m * 7 + n * 3 + k)
+    _crt_case(blas, oracle, "N", "N", m, n, k, m + 1, k + 2, m + 3, -0.75, 0.25, rng)
+
+
+@pytest.mark.parametrize("nmod", [4, 8, 12, 15])
+def test_crt_moduli_counts(blas, oracle, nmod):
+    """Fewer moduli: fewer scaling bits P, larger (bounded) error."""
+    rng = np.random.default_rng(nmod)
+    _crt_case(blas, oracle, "T", "N", 130, 257, 300, 300, 300, 131, 1.0, 0.0, rng, nmod=nmod)
+
+
+@pytest.mark.parametrize("phi", [4.0, 8.0, 16.0])
+def test_crt_wide_dynamic_range(blas, oracle, phi):
+    rng = np.random.default_rng(int(phi) + 1)
+    _crt_case(blas, oracle, "N", "T", 96, 80, 512, 96, 80, 96, 1.0, -1.0, rng, phi=phi)
+
+
+def test_crt_zero_rows_and_nonfinite(blas, oracle):
+    """A zero row of A gives exact zeros; an Inf in a row of A (column of B) gives NaN on that row (column)."""
+    rng = np.random.default_rng(9)
+    m, n, k = 70, 40, 90
+    a = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    a[3, :] = 0.0
+    a[5, 17] = np.inf
+    b[2, 9] = np.nan
+    c = np.zeros((m, n), order="F")
+    blas.set_dgemm_method(blas.METHOD_OZAKI)
+    old = blas.set_ozaki_scheme(blas.OZAKI_CRT)
+    try:
+        blas.dgemm("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m)
+    finally:
+        blas.set_ozaki_scheme(old)
+        blas.set_dgemm_method(blas.METHOD_NATIVE)
+    assert np.all(c[3, np.arange(n) != 9] == 0.0)
+    assert np.all(np.isnan(c[5, :])) and np.all(np.isnan(c[:, 9]))
+    rest = np.ones((m, n), bool)
+    rest[5, :] = False
+    rest[:, 9] = False
+    rest[3, :] = False
+    ref = a.copy()
+    ref[5, 17] = 0.0
+    refb = b.copy()
+    refb[2, 9] = 0.0
+    np.testing.assert_allclose(c[rest], (ref @ refb)[rest], rtol=1e-12, atol=1e-13)
+
+
+def test_crt_long_k_falls_back_to_slices(blas):
+    """K beyond the INT32 bound of one modular product runs the slice scheme."""
+    from zynum_b200 import ozaki_info
+    blas.set_dgemm_method(blas.METHOD_OZAKI)
+    old = blas.set_ozaki_scheme(blas.OZAKI_CRT)
+    try:
+        assert ozaki_info(64, 64, 130816)["scheme"] == "crt"
+        assert ozaki_info(64, 64, 130817)["scheme"] == "slices"
+    finally:
+        blas.set_ozaki_scheme(old)
+        blas.set_dgemm_method(blas.METHOD_NATIVE)
+
+
+def test_crt_matches_native_error_at_2048(blas, oracle):
+    """Default CRT scheme (16 moduli) vs native FP64 on 2048^3, u * 10^U[-4,4] entries:
+    max relative error on 4096 sampled entries no worse than native."""
+    rng = np.random.default_rng(41)
+    n = 2048
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-4, 4, (n, n)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-4, 4, (n, n)))
+    rows, cols = rng.integers(0, n, 4096), rng.integers(0, n, 4096)
+    hi, lo, _ = oracle.ddgemm_sampled("N", "N", n, a, n, b, n, rows, cols)
+    exact = hi + lo
+    errs = {}
+    for name, method, scheme in (("native", blas.METHOD_NATIVE, 0), ("crt", blas.METHOD_OZAKI, blas.OZAKI_CRT)):
+        c = np.zeros((n, n), order="F")
+        blas.set_dgemm_method(method)
+        old = blas.set_ozaki_scheme(scheme)
+        try:
+            blas.dgemm("N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c, n)
+        finally:
+            blas.set_ozaki_scheme(old)
+            blas.set_dgemm_method(blas.METHOD_NATIVE)
+        errs[name] = float((np.abs(c[rows, cols] - exact) / np.abs(exact)).max())
+    assert errs["crt"] <= errs["native"], errs
+
+
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T"), ("N", "T")])
 def test_sgemm_bf16x3(blas, oracle, ta, tb):
     rng = np.random.default_rng(3)

@@ -13,8 +13,13 @@ import ctypes as _C
 
 
 def ozaki_info(m: int, n: int, k: int) -> dict:
-    """Slice count and slice-product count the Ozaki DGEMM uses for this shape."""
+    """Scheme ("slices" or "crt"), digit count (slices or moduli) and INT8 product-GEMM
+    count the Ozaki DGEMM uses for this shape under the current settings."""
     from ._lib import load
-    s, p = _C.c_int(0), _C.c_int(0)
-    load().zynum_blas_gpu_ozaki_plan(m, n, k, _C.byref(s), _C.byref(p))
-    return {"slices": s.value, "slice_products": p.value}
+    sc, s, p = _C.c_int(0), _C.c_int(0), _C.c_int(0)
+    load().zynum_blas_gpu_ozaki_plan_ex(m, n, k, _C.byref(sc), _C.byref(s), _C.byref(p))
+    scheme = "crt" if sc.value == 2 else "slices"
+    out = {"scheme": scheme, "products": p.value, "slice_products": p.value}
+    out["moduli" if scheme == "crt" else "slices"] = s.value
+    out["slices"] = s.value if scheme == "slices" else 0
+    return out

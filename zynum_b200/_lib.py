@@ -102,11 +102,14 @@ def _declare(L: C.CDLL) -> None:
     L.zynum_blas_gpu_dgemm_noalloc_device.argtypes = [ch, ch, i, i, i, d, P, i, P, i, d, P, i, i, P]
     L.zynum_blas_gpu_dgemm_noalloc_device.restype = i
     for name in ("zynum_blas_gpu_set_dgemm_method", "zynum_blas_gpu_set_sgemm_method",
-                 "zynum_blas_gpu_set_ozaki_slices"):
+                 "zynum_blas_gpu_set_ozaki_slices", "zynum_blas_gpu_set_ozaki_scheme",
+                 "zynum_blas_gpu_set_ozaki_moduli"):
         getattr(L, name).argtypes = [i]
         getattr(L, name).restype = i
     L.zynum_blas_gpu_ozaki_plan.argtypes = [i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.zynum_blas_gpu_ozaki_plan.restype = i
+    L.zynum_blas_gpu_ozaki_plan_ex.argtypes = [i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.zynum_blas_gpu_ozaki_plan_ex.restype = i
     L.zynum_blas_gpu_last_error.argtypes = []
     L.zynum_blas_gpu_last_error.restype = cp
     L.zynum_blas_gpu_inject_fault.argtypes = [i, i]

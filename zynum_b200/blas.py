@@ -205,6 +205,19 @@ def set_ozaki_slices(slices: int) -> int:
     return load().zynum_blas_gpu_set_ozaki_slices(slices)
 
 
+OZAKI_AUTO, OZAKI_SLICES, OZAKI_CRT = 0, 1, 2
+
+
+def set_ozaki_scheme(scheme: int) -> int:
+    """0 = automatic, 1 = INT8 slices (scheme I), 2 = CRT residues (scheme II)."""
+    return load().zynum_blas_gpu_set_ozaki_scheme(scheme)
+
+
+def set_ozaki_moduli(moduli: int) -> int:
+    """CRT moduli 2..16; 0 = default."""
+    return load().zynum_blas_gpu_set_ozaki_moduli(moduli)
+
+
 def inject_fault(kind: int, count: int) -> None:
     load().zynum_blas_gpu_inject_fault(kind, count)
 

@@ -90,7 +90,7 @@ cudaError_t run_dgemm(const GemmArgsF64& g, cudaStream_t st, Scratch scratch) {
     int method = cx.dgemm_method;
     if (method == METHOD_AUTO) method = ozaki_preferred(g.m, g.n, g.k) ? METHOD_OZAKI : METHOD_NATIVE;
     if (method == METHOD_OZAKI) {
-        OzakiPlan op = plan_ozaki(g.m, g.n, g.k, cx.ozaki_slices);
+        OzakiPlan op = plan_ozaki(g.m, g.n, g.k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
         void* ws = nullptr;
         cudaError_t e = scratch(ozaki_workspace_bytes(op), st, &ws);
         if (e != cudaSuccess) return e;
@@ -118,7 +118,7 @@ cudaError_t run_sgemm(const GemmArgsF32& g, cudaStream_t st, Scratch scratch) {
     }
     GemmPlan p = plan_native_gemm(g.m, g.n, g.k, 4, cx.sm_count);
     void* ws = nullptr;
-    size_t need = splitk_workspace_elems(g.m, g.n, p.splits) * sizeof(float);
+    size_t need = sgemm_native_workspace_bytes(g.transa, g.transb, g.m, g.n, g.k, p);
     if (need) {
         cudaError_t e = scratch(need, st, &ws);
         if (e != cudaSuccess) return e;
@@ -196,7 +196,14 @@ size_t real_scratch_bytes(int m, int n, int k, double*) {
     Context& cx = context();
     int method = cx.dgemm_method;
     if (method == METHOD_AUTO) method = ozaki_preferred(m, n, k) ? METHOD_OZAKI : METHOD_NATIVE;
-    if (method == METHOD_OZAKI) return ozaki_workspace_bytes(plan_ozaki(m, n, k, cx.ozaki_slices));
+    if (method == METHOD_OZAKI) {
+        size_t b = ozaki_workspace_bytes(plan_ozaki(m, n, k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli));
+        // a smaller-K product of the same call (TRSM updates) may take the CRT scheme
+        if (cx.ozaki_scheme != OZAKI_SLICES && cx.ozaki_slices == 0)
+            b = std::max(b, ozaki_workspace_bytes(plan_ozaki(m, n, std::min(k, kCrtMaxK), 0, OZAKI_CRT,
+                                                              cx.ozaki_moduli)));
+        return b;
+    }
     GemmPlan p = plan_native_gemm(m, n, k, 8, cx.sm_count);
     return splitk_workspace_elems(m, n, p.splits) * sizeof(double);
 }
@@ -204,17 +211,19 @@ size_t real_scratch_bytes(int m, int n, int k, float*) {
     Context& cx = context();
     if (cx.sgemm_method == SMETHOD_BF16X3) return bf16x3_workspace_bytes(m, n, k);
     GemmPlan p = plan_native_gemm(m, n, k, 4, cx.sm_count);
-    return splitk_workspace_elems(m, n, p.splits) * sizeof(float);
+    return sgemm_native_workspace_bytes('T', 'N', m, n, k, p);  // both operand copies, if any
 }
 
 // Scratch that covers every GEMM of shape up to m x n x k (TRSM's recursive
 // updates): split-K partials never exceed sm_count x 128 x 128 elements
-// (splits <= sm_count / tiles and tiles >= m n / 128^2), and the Ozaki planes
-// grow with every dimension.
+// (splits <= sm_count / tiles and tiles >= m n / 128^2), FP32 products may add
+// an MN-contiguous copy of each operand, and the Ozaki planes grow with every
+// dimension.
 template <typename T>
 size_t real_scratch_bound(int m, int n, int k) {
     Context& cx = context();
-    const size_t splitk = (size_t)cx.sm_count * 128 * 128 * sizeof(T) + 4096;
+    const size_t splitk = sizeof(T) == 4 ? sgemm_native_workspace_bound(m, n, k, cx.sm_count)
+                                         : (size_t)cx.sm_count * 128 * 128 * sizeof(T) + 4096;
     return std::max(splitk, real_scratch_bytes(m, n, k, (T*)nullptr));
 }
 
@@ -403,7 +412,8 @@ cudaError_t run_syrk(char uplo, char trans, int n, int k, T alpha, const T* a, l
     g.tri = (uplo == 'U') ? 1 : 2;
     GemmPlan p = plan_native_gemm(n, n, k, sizeof(T), cx.sm_count);
     void* ws = nullptr;
-    const size_t need = splitk_workspace_elems(n, n, p.splits) * sizeof(T);
+    const size_t need = sizeof(T) == 4 ? sgemm_native_workspace_bytes(g.transa, g.transb, n, n, k, p)
+                                       : splitk_workspace_elems(n, n, p.splits) * sizeof(T);
     if (need) {
         cudaError_t e = scratch(need, st, &ws);
         if (e != cudaSuccess) return e;
@@ -884,17 +894,47 @@ int zynum_blas_gpu_set_ozaki_slices(int slices) {
     return old;
 }
 
-int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int* slices, int* products) {
+int zynum_blas_gpu_set_ozaki_scheme(int scheme) {
     Context& cx = context();
-    int s;
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.ozaki_scheme;
+    if (scheme >= OZAKI_AUTO && scheme <= OZAKI_CRT) cx.ozaki_scheme = scheme;
+    return old;
+}
+
+int zynum_blas_gpu_set_ozaki_moduli(int moduli) {
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cx.init();
+    int old = cx.ozaki_moduli;
+    if (moduli == 0 || (moduli >= 2 && moduli <= kCrtMaxModuli)) cx.ozaki_moduli = moduli;
+    return old;
+}
+
+int zynum_blas_gpu_ozaki_plan_ex(int m, int n, int k, int* scheme, int* digits, int* products) {
+    Context& cx = context();
+    OzakiPlan p;
     {
         std::lock_guard<std::recursive_mutex> lock(cx.mutex);
-        s = plan_ozaki(m, n, k, cx.ozaki_slices).slices;
+        p = plan_ozaki(m, n, k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
     }
-    if (s == 0) s = ozaki_last_slices();  // automatic: the count the last call chose
-    if (slices) *slices = s;
-    if (products) *products = s * (s + 1) / 2;
+    int d, prods;
+    if (p.scheme == OZAKI_CRT) {
+        d = p.moduli;
+        prods = p.moduli;
+    } else {
+        d = p.slices ? p.slices : ozaki_last_slices();  // automatic: the count the last call chose
+        prods = d * (d + 1) / 2;
+    }
+    if (scheme) *scheme = p.scheme;
+    if (digits) *digits = d;
+    if (products) *products = prods;
     return 0;
+}
+
+int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int* slices, int* products) {
+    return zynum_blas_gpu_ozaki_plan_ex(m, n, k, nullptr, slices, products);
 }
 
 const char* zynum_blas_gpu_last_error(void) { return last_error(); }

@@ -162,8 +162,22 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
     cp_async_wait<0>();
 
     // Epilogue: c[v0 + 2 v1] sits at (row g + 8 v1, col 2 t + v0) of each 16x8 fragment.
+    // The beta * C reads of one fragment row are all issued before its stores
+    // (a store to C would otherwise order every later C load behind it).
 #pragma unroll
-    for (int i = 0; i < MI; ++i)
+    for (int i = 0; i < MI; ++i) {
+        double cin[NI][4];
+        if (!PARTIAL && beta != 0.0) {
+#pragma unroll
+            for (int j = 0; j < NI; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int row = m0 + wm + i * 16 + g + 8 * (v >> 1);
+                    const int col = n0 + wn + j * 8 + 2 * t + (v & 1);
+                    const bool in_tri = tri == 0 || (tri == 1 ? row <= col : row >= col);
+                    cin[j][v] = (row < M && col < N && in_tri) ? C[(long)col * ldc + row] : 0.0;
+                }
+        }
 #pragma unroll
         for (int j = 0; j < NI; ++j)
 #pragma unroll
@@ -175,13 +189,13 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
                     if (PARTIAL) {
                         W[(long)blockIdx.z * M * N + (long)col * M + row] = acc[i][j][v];
                     } else {
-                        double* cp = C + (long)col * ldc + row;
                         double out = alpha * acc[i][j][v];
-                        if (beta != 0.0) out = fma(beta, *cp, out);
-                        *cp = out;
+                        if (beta != 0.0) out = fma(beta, cin[j][v], out);
+                        C[(long)col * ldc + row] = out;
                     }
                 }
             }
+    }
 }
 
 __global__ void dgemm_splitk_reduce(int M, int N, int splits, const double* __restrict__ W, double alpha, double beta,

@@ -46,6 +46,11 @@ inline size_t splitk_workspace_elems(int m, int n, int splits) {
 // ---------------------------------------------------------------- kernels
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st);
 cudaError_t sgemm_native(const GemmArgsF32& g, const GemmPlan& plan, float* workspace, cudaStream_t st);
+// Workspace of sgemm_native in bytes: split-K partials plus, for large
+// products, an MN-contiguous copy of each K-contiguous operand.  The bound
+// covers every FP32 product of shape up to m x n x k and any transposes.
+size_t sgemm_native_workspace_bytes(char transa, char transb, int m, int n, int k, const GemmPlan& plan);
+size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count);
 
 // C = beta * C on the m x n window (beta == 0 writes exact zeros, clearing NaNs),
 // the reference's k == 0 / alpha == 0 quick return (gemm.zig:1407-1414).

@@ -62,7 +62,7 @@ constexpr int kMaxJobs = 16;
 constexpr size_t kSmemBytes = 1024 /*align slack*/ + kASlots * kAChunk + kBSlots * kBChunk + 256 + kUN * 8 + 3 * kMaxSteps;
 
 enum Kind : int { KIND_I8 = 0, KIND_BF16 = 1 };
-enum Epi : int { EPI_OZAKI_F64 = 0, EPI_F32 = 1 };
+enum Epi : int { EPI_OZAKI_F64 = 0, EPI_F32 = 1, EPI_RESIDUE = 2 };
 
 // Work of one C tile is a list of "group jobs".  A job owns one or two
 // accumulators (TMEM columns [0,256) and [256,512)); it sweeps K chunk by
@@ -80,7 +80,8 @@ struct UmmaParams {
     int job_first_step[kMaxJobs];
     int job_num_steps[kMaxJobs];
     int job_groups[kMaxJobs];     // 1 or 2 accumulators
-    int job_shift[kMaxJobs][2];   // 7 g of the group held by accumulator 0 / 1
+    int job_shift[kMaxJobs][2];   // 7 g of the group held by accumulator 0 / 1 (EPI_RESIDUE: modulus index)
+    int job_buf[kMaxJobs];        // EPI_RESIDUE: TMEM accumulator (0 / 1) of the job
     int step_a[kMaxSteps];        // digit plane of A
     int step_b[kMaxSteps];        // digit plane of B
     int step_acc[kMaxSteps];      // accumulator 0 / 1
@@ -91,6 +92,8 @@ struct UmmaParams {
     const int* row_exp;
     const int* col_exp;
     int* status;
+    int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad]
+    long res_plane;
 };
 
 // ------------------------------------------------------ bounded waiting
@@ -141,6 +144,98 @@ struct Ring {
         }
     }
 };
+
+// ------------------------------------------ Ozaki scheme II (CRT) tables
+// Pairwise coprime moduli <= 256: residues are int8 in [-128, 127] and a
+// modular product sums k products of magnitude <= 2^14 in INT32.
+constexpr int kCrtModuli[kCrtMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                           229, 227, 223, 211, 199, 197, 193, 191};
+
+struct CrtTable {
+    int m[kCrtMaxModuli];
+    float inv[kCrtMaxModuli];
+    uint32_t wlo[kCrtMaxModuli], whi[kCrtMaxModuli];  // int8 x4: 2^(8t) mod m for t = 0..3 / 4..7
+    int bias[kCrtMaxModuli];                          // 2^63 mod m
+};
+
+// Symmetric representative of r mod m: [-128, 127] for m = 256, |x| <= (m-1)/2 for odd m.
+constexpr int sym_residue(long long r, int m) {
+    long long x = r % m;
+    if (x < 0) x += m;
+    return (int)(x >= (m + 1) / 2 ? x - m : x);
+}
+
+constexpr CrtTable make_crt_table() {
+    CrtTable t{};
+    for (int l = 0; l < kCrtMaxModuli; ++l) {
+        const int m = kCrtModuli[l];
+        t.m[l] = m;
+        t.inv[l] = 1.0f / (float)m;
+        long long p = 1;  // 2^(8 b) mod m
+        uint32_t lo = 0, hi = 0;
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t byte = (uint32_t)(sym_residue(p, m) & 0xFF);
+            if (b < 4)
+                lo |= byte << (8 * b);
+            else
+                hi |= byte << (8 * (b - 4));
+            p = (p * 256) % m;
+        }
+        t.wlo[l] = lo;
+        t.whi[l] = hi;
+        long long q = 1;
+        for (int b = 0; b < 63; ++b) q = (q * 2) % m;
+        t.bias[l] = sym_residue(q, m);
+    }
+    return t;
+}
+
+__constant__ CrtTable kCrt = make_crt_table();
+
+// Rows holding Inf / NaN: no residues; the reconstruction writes NaN.
+constexpr int kCrtNonFinite = -0x40000000;
+
+// d = c + sum_i a.u8[i] * b.s8[i]
+ZB_DEVICE int dp4a_us(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// v mod m, symmetric, for |v| < 2^31 - 2^21: the first FP32 quotient is
+// within 2 of v / m, the second is exact, the result lies in [-m/2, m/2] and
+// +128 (m = 256 only) folds to -128.
+ZB_DEVICE int crt_reduce(int v, int m, float inv) {
+    int q = __float2int_rn(__int2float_rn(v) * inv);
+    v -= q * m;
+    q = __float2int_rn(__int2float_rn(v) * inv);
+    v -= q * m;
+    return v > 127 ? v - m : v;
+}
+
+// 32 INT32 modular products of one TMEM lane -> 32 int8 residues (32 bytes).
+ZB_DEVICE void residue_chunk(const uint32_t (&r)[32], int mod_idx, int8_t* dst) {
+    uint32_t w[8];
+    if (mod_idx == 0) {  // m = 256: the low byte of the two's-complement sum
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            w[q] = (r[4 * q] & 0xFFu) | ((r[4 * q + 1] & 0xFFu) << 8) | ((r[4 * q + 2] & 0xFFu) << 16) |
+                   (r[4 * q + 3] << 24);
+    } else {
+        const int m = kCrt.m[mod_idx];
+        const float inv = kCrt.inv[mod_idx];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            uint32_t x = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) x |= ((uint32_t)crt_reduce((int)r[4 * q + i], m, inv) & 0xFFu) << (8 * i);
+            w[q] = x;
+        }
+    }
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    __stcg(d, make_uint4(w[0], w[1], w[2], w[3]));
+    __stcg(d + 1, make_uint4(w[4], w[5], w[6], w[7]));
+}
 
 // Per-step flags of the job schedule, staged in shared memory once per CTA so
 // the single MMA-issuing thread reads one byte per step instead of indexing
@@ -221,9 +316,9 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     uint64_t* emptyA = fullA + kASlots;
     uint64_t* fullB = emptyA + kASlots;
     uint64_t* emptyB = fullB + kBSlots;
-    uint64_t* tfull = emptyB + kBSlots;
-    uint64_t* tempty = tfull + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+    uint64_t* tfull = emptyB + kBSlots;  // [2]
+    uint64_t* tempty = tfull + 2;        // [2]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     Sched* sched = reinterpret_cast<Sched*>(smem_tail_scratch(smem) + kUN * 8);
 
@@ -238,8 +333,10 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             mbar_init(&fullB[i], 1);
             mbar_init(&emptyB[i], 1);
         }
-        mbar_init(tfull, 1);
-        mbar_init(tempty, 4);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -308,14 +405,15 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         if (lane == 0) {
             const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, kUM, kUN) : umma_idesc(1, 1, kUM, kUN);
             Ring ra, rb;
-            uint32_t tphase = 0;
+            uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
             bool ok = true;
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                        // both accumulators must have been drained by the epilogue
-                        if (!(ok = wait_phase(tempty, tphase ^ 1, abort_flag, P.status, 3))) break;
-                        tphase ^= 1;
+                        // the job's accumulators must have been drained by the epilogue
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                        tphase ^= 1u << b;
                         tc_fence_after();
                         const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
                         auto mma = [idesc](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
@@ -328,7 +426,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         ok = mma_job<kASlots, kBSlots, kAChunk, kBChunk>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
                             emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
-                        if (ok) umma_commit(tfull);
+                        if (ok) umma_commit(&tfull[b]);
                     }
         }
     } else {
@@ -338,7 +436,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int et = threadIdx.x - 64;  // 0..127 among the epilogue threads
         const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
         double* colscale = reinterpret_cast<double*>(smem_tail_scratch(smem));  // kUN doubles
-        uint32_t tphase = 0;
+        uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
         bool ok = true;
         for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
             int tm, tn;
@@ -359,9 +457,26 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    if (!(ok = wait_phase(tfull, tphase, abort_flag, P.status, 6))) break;
-                    tphase ^= 1;
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    tphase ^= 1u << b;
                     tc_fence_after();
+                    if (EPI == EPI_RESIDUE) {
+                        // one modulus per job: accumulator b -> int8 residues, row-major plane
+                        int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
+                                      (long)tn * kUN;
+#pragma unroll 1
+                        for (int ch = 0; ch < kUN / 32; ++ch) {
+                            uint32_t r0[32];
+                            tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
+                            tmem_ld_wait();
+                            residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
+                        }
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&tempty[b]);
+                        continue;
+                    }
                     const bool two = P.job_groups[j] == 2;
                     // accumulator 1 holds group g_a - 1, worth 2^7 times accumulator 0:
                     // D0 + 128 D1 is exact in int64 and converts exactly to FP64.
@@ -414,7 +529,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     }
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(tempty);
+                    if (lane == 0) mbar_arrive(&tempty[0]);
                     first = false;
                 }
         }
@@ -451,9 +566,9 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     uint64_t* emptyA = fullA + kSlots2;
     uint64_t* fullB = emptyA + kSlots2;
     uint64_t* emptyB = fullB + kSlots2;
-    uint64_t* tfull = emptyB + kSlots2;
-    uint64_t* tempty = tfull + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+    uint64_t* tfull = emptyB + kSlots2;  // [2]
+    uint64_t* tempty = tfull + 2;        // [2]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     double* colscale = reinterpret_cast<double*>(sB + kSlots2 * kChunk2 + 512);
     Sched* sched = reinterpret_cast<Sched*>(sB + kSlots2 * kChunk2 + 512 + kUN * 8);
@@ -470,8 +585,10 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             mbar_init(&fullB[i], 1);
             mbar_init(&emptyB[i], 1);
         }
-        mbar_init(tfull, 1);
-        mbar_init(tempty, 8);  // 4 epilogue warps in each CTA of the pair
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 8);  // 4 epilogue warps in each CTA of the pair
+        }
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -541,13 +658,14 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         if (lane == 0 && leader) {
             const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, 256, kUN) : umma_idesc(1, 1, 256, kUN);
             Ring ra, rb;
-            uint32_t tphase = 0;
+            uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
             bool ok = true;
             for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                        if (!(ok = wait_phase(tempty, tphase ^ 1, abort_flag, P.status, 3))) break;
-                        tphase ^= 1;
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                        tphase ^= 1u << b;
                         tc_fence_after();
                         const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
                         auto mma = [idesc](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
@@ -560,7 +678,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                         ok = mma_job<kSlots2, kSlots2, kChunk2, kChunk2>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
                             emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
-                        if (ok) umma_commit_2sm(tfull, 0x3);
+                        if (ok) umma_commit_2sm(&tfull[b], 0x3);
                     }
         }
     } else {
@@ -569,8 +687,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         const int row_in_tile = rank * 128 + quarter * 32 + lane;
         const int et = threadIdx.x - 64;
         const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
-        const uint32_t tempty_cta0 = mapa_shared(smem_u32(tempty), 0);
-        uint32_t tphase = 0;
+        const uint32_t tempty_cta0 = mapa_shared(smem_u32(&tempty[0]), 0);  // buffer b: + 8 b
+        uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
         bool ok = true;
         for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
             int tm, tn;
@@ -590,9 +708,26 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    if (!(ok = wait_phase(tfull, tphase, abort_flag, P.status, 6))) break;
-                    tphase ^= 1;
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    tphase ^= 1u << b;
                     tc_fence_after();
+                    if (EPI == EPI_RESIDUE) {
+                        // one modulus per job: accumulator b -> int8 residues, row-major plane
+                        int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
+                                      (long)tn * kUN;
+#pragma unroll 1
+                        for (int ch = 0; ch < kUN / 32; ++ch) {
+                            uint32_t r0[32];
+                            tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
+                            tmem_ld_wait();
+                            residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
+                        }
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
+                        continue;
+                    }
                     const bool two = P.job_groups[j] == 2;
                     const double s0 = (EPI == EPI_OZAKI_F64) ? pow2(er - P.job_shift[j][0]) * P.alpha : 1.0;
 #pragma unroll 1
@@ -797,6 +932,172 @@ ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, 
     }
 }
 
+// ---------------------------------------------- CRT residues of operands
+// Row scale of the CRT scheme: 2^{a_r} with ||2^{a_r} x_r||_2 <= 2^P, from the
+// Hoelder bound ||x_r||_2 <= sqrt(max_r * sum_r) <= max_r * sqrt(min(sum_r / max_r, k)).
+ZB_DEVICE int crt_row_exponent(unsigned long long maxbits, double sum, int k, int P) {
+    if (maxbits == 0) return 0;
+    const double mx = __longlong_as_double((long long)maxbits);
+    if (!(mx <= 1.7976931348623157e308)) return kCrtNonFinite;  // Inf or NaN in the row
+    int e1, e2;
+    const double f1 = frexp(mx, &e1);  // mx = f1 2^e1, f1 in [0.5, 1)
+    const double ratio = fmin(sum / mx, (double)k);
+    frexp(f1 * sqrt(fmax(ratio, 1.0)) * (1.0 + 0x1p-20), &e2);  // < 2^e2
+    return P - (e1 + e2);
+}
+
+// Each block: 32 rows x 128 columns of X -> `nmod` int8 residue planes
+// (plane l: rows_pad x cols_pad bytes, K-major) of round(2^{a_r} x) and the
+// row exponents a_r.  The integer (|.| <= 2^P <= 2^62) is biased by 2^63 so
+// that its eight bytes are unsigned digits; residue = dp4a(bytes, 2^{8t} mod m)
+// - (2^63 mod m), then one exact FP32 reduction.
+__global__ void __launch_bounds__(256)
+ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const double* __restrict__ sums, int P,
+                int nmod, int rows_pad, int cols_pad, int8_t* __restrict__ planes, int* __restrict__ exps) {
+    __shared__ double tile[32 * 128];
+    __shared__ int sexp[32];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
+    const int t = threadIdx.x;
+    if (t < 32) {
+        const int r = r0 + t;
+        const int e = (r < X.rows) ? crt_row_exponent(maxbits[r], sums[r], X.cols, P) : 0;
+        sexp[t] = e;
+        if (blockIdx.x == 0 && r < rows_pad) exps[r] = e;
+    }
+#pragma unroll 4
+    for (int it = 0; it < 16; ++it) {
+        const int idx = it * 256 + t;
+        int r, c;
+        if (X.rs == 1) {
+            r = idx & 31;
+            c = idx >> 5;
+        } else {
+            r = idx >> 7;
+            c = idx & 127;
+        }
+        const int gr = r0 + r, gc = c0 + c;
+        double v = 0.0;
+        if (gr < X.rows && gc < X.cols) v = X.base[(long)gr * X.rs + (long)gc * X.cs];
+        tile[swz(r, c)] = v;
+    }
+    __syncthreads();
+    const int r = t >> 3, q = t & 7;
+    if (r0 + r >= rows_pad) return;
+    const int a = sexp[r];
+    const bool finite = a != kCrtNonFinite;
+    uint32_t lo[16], hi[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const long long v = finite ? llrint(ldexp(tile[swz(r, q * 16 + i)], a)) : 0LL;
+        const unsigned long long u = (unsigned long long)v ^ (1ull << 63);
+        lo[i] = (uint32_t)u;
+        hi[i] = (uint32_t)(u >> 32);
+    }
+    const long plane = (long)rows_pad * cols_pad;
+    int8_t* out = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
+    // modulus 256: the low byte of the integer
+    {
+        uint32_t w[4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+            w[g] = (lo[4 * g] & 0xFFu) | ((lo[4 * g + 1] & 0xFFu) << 8) | ((lo[4 * g + 2] & 0xFFu) << 16) |
+                   (lo[4 * g + 3] << 24);
+        *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    for (int l = 1; l < nmod; ++l) {
+        const int m = kCrt.m[l];
+        const float inv = kCrt.inv[l];
+        const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l];
+        const int nb = -kCrt.bias[l];
+        uint32_t w[4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint32_t x = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int v = dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, nb));  // |v| < 2^18
+                int rr = v - __float2int_rn(__int2float_rn(v) * inv) * m;             // exact: |v| < 2^24
+                x |= ((uint32_t)rr & 0xFFu) << (8 * i);
+            }
+            w[g] = x;
+        }
+        *reinterpret_cast<uint4*>(out + l * plane) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// Balanced 32-bit limbs (int32) of the CRT weights w_l = M_l (M_l^-1 mod m_l)
+// mod M and of M = prod m_l; M < 2^127 for 16 moduli, so four limbs hold it.
+constexpr int kCrtLimbs = 4;
+struct CrtCombine {
+    int nmod;
+    int w[kCrtMaxModuli][kCrtLimbs];
+    int M[kCrtLimbs];
+    double M_d;
+};
+
+// C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 64 x 64 tile.
+// The residue sum S = sum_l r_l w_l is exact in int64 limbs (|r_l w_l limb| <
+// 2^39); q = round(S / M) from an FP64 estimate (|C_bar| < M / 4 keeps S / M
+// within 1/4 of an integer); C_bar = S - q M, carried to balanced limbs and
+// rounded to FP64 from the top limb down.
+__global__ void __launch_bounds__(256)
+ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
+                  const int* __restrict__ expb, double alpha, double beta, double* __restrict__ C, long ldc,
+                  const __grid_constant__ CrtCombine K) {
+    extern __shared__ uint8_t rs[];  // [nmod][64][68]
+    constexpr int kPitch = 68;
+    const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64, t = threadIdx.x;
+    {
+        const int row = t >> 2, cc = t & 3;
+        for (int l = 0; l < K.nmod; ++l) {
+            const uint4 v = __ldcs(reinterpret_cast<const uint4*>(res + l * plane + (long)(i0 + row) * res_ld + j0 +
+                                                                  cc * 16));
+            uint32_t* d = reinterpret_cast<uint32_t*>(rs + (l * 64 + row) * kPitch + cc * 16);
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+        }
+    }
+    __syncthreads();
+    const int i = t & 63, jq = t >> 6;
+    const int gi = i0 + i;
+    if (gi >= m) return;
+    const int ea = expa[gi];
+#pragma unroll 1
+    for (int jj = 0; jj < 16; ++jj) {
+        const int j = jq * 16 + jj, gj = j0 + j;
+        if (gj >= n) break;
+        const double cin = beta != 0.0 ? C[(long)gj * ldc + gi] : 0.0;  // issued ahead of the arithmetic
+        long long acc[kCrtLimbs] = {0, 0, 0, 0};
+        for (int l = 0; l < K.nmod; ++l) {
+            const int r = (int)(int8_t)rs[(l * 64 + i) * kPitch + j];
+#pragma unroll
+            for (int z = 0; z < kCrtLimbs; ++z) acc[z] += (long long)r * K.w[l][z];
+        }
+        double sd = 0.0;
+#pragma unroll
+        for (int z = kCrtLimbs - 1; z >= 0; --z) sd = sd * 4294967296.0 + (double)acc[z];
+        const long long q = (long long)rint(sd / K.M_d);
+#pragma unroll
+        for (int z = 0; z < kCrtLimbs; ++z) acc[z] -= q * K.M[z];
+#pragma unroll
+        for (int z = 0; z < kCrtLimbs - 1; ++z) {
+            const long long c = (acc[z] + (1LL << 31)) >> 32;
+            acc[z] -= c << 32;
+            acc[z + 1] += c;
+        }
+        double v = (double)acc[kCrtLimbs - 1];
+#pragma unroll
+        for (int z = kCrtLimbs - 2; z >= 0; --z) v = v * 4294967296.0 + (double)acc[z];
+        const int eb = expb[gj];
+        double out = (ea == kCrtNonFinite || eb == kCrtNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
+                                                                  : alpha * ldexp(v, -(ea + eb));
+        if (beta != 0.0) out = fma(beta, cin, out);
+        C[(long)gj * ldc + gi] = out;
+    }
+}
+
 // 3xBF16 split of a float matrix view into hi / lo planes (bf16, K-major).
 struct ViewF {
     const float* base;
@@ -877,7 +1178,7 @@ inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
 // Workspace layout: the small statistics block first, the digit planes after it.
 struct Layout {
     long maxa_off, maxb_off, suma_off, sumb_off, expa_off, expb_off, spread_off, status_off, stats_end;
-    long a_planes_off, b_planes_off, total;
+    long a_planes_off, b_planes_off, res_off, total;
 };
 
 Layout ozaki_layout(const OzakiPlan& p) {
@@ -898,9 +1199,10 @@ Layout ozaki_layout(const OzakiPlan& p) {
     L.status_off = take(64);
     L.stats_end = off;
     off = round_up(off, 1024);
-    const int s = p.slices > 0 ? p.slices : kOzakiAutoMaxSlices;
+    const int s = p.scheme == OZAKI_CRT ? p.moduli : (p.slices > 0 ? p.slices : kOzakiAutoMaxSlices);
     L.a_planes_off = take((long)s * p.m_pad * p.k_pad);
     L.b_planes_off = take((long)s * p.n_pad * p.k_pad);
+    L.res_off = take(p.scheme == OZAKI_CRT ? (long)p.moduli * p.m_pad * p.n_pad : 0);
     L.total = off;
     return L;
 }
@@ -984,10 +1286,17 @@ std::atomic<int> g_last_slices{0};
 }
 int ozaki_last_slices() { return g_last_slices.load(); }
 
-OzakiPlan plan_ozaki(int m, int n, int k, int slices) {
+OzakiPlan plan_ozaki(int m, int n, int k, int slices, int scheme, int moduli) {
     OzakiPlan p;
     if (slices > kOzakiMaxSlices) slices = kOzakiMaxSlices;
     if (slices < 0) slices = 0;
+    const bool crt_ok = k <= kCrtMaxK;
+    if (scheme == OZAKI_AUTO)
+        scheme = (slices > 0 || !crt_ok) ? OZAKI_SLICES : OZAKI_CRT;
+    else if (scheme == OZAKI_CRT && !crt_ok)
+        scheme = OZAKI_SLICES;
+    p.scheme = scheme == OZAKI_CRT ? OZAKI_CRT : OZAKI_SLICES;
+    if (p.scheme == OZAKI_CRT) p.moduli = (moduli >= 2 && moduli <= kCrtMaxModuli) ? moduli : kCrtDefaultModuli;
     p.slices = slices;  // 0: chosen from the data at run time
     p.pair = use_cta_pair(m);
     p.m_pad = (int)round_up(m, p.pair ? 2 * kUM : kUM);
@@ -998,7 +1307,162 @@ OzakiPlan plan_ozaki(int m, int n, int k, int slices) {
 
 size_t ozaki_workspace_bytes(const OzakiPlan& p) { return (size_t)ozaki_layout(p).total; }
 
+namespace {
+// Host constants of the CRT scheme for the first n moduli (exact in 128-bit
+// integers: M < 2^127 for n <= 16) and the scaling bits P with 2^(2P) <= M / 4.
+struct CrtHost {
+    CrtCombine K;
+    int P;
+};
+
+const CrtHost& crt_host(int nmod) {
+    static CrtHost table[kCrtMaxModuli + 1];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        auto limbs = [](unsigned __int128 x, int* out) {
+            long long L[kCrtLimbs];
+            for (int z = 0; z < kCrtLimbs; ++z) L[z] = (long long)((x >> (32 * z)) & 0xFFFFFFFFu);
+            for (int z = 0; z < kCrtLimbs - 1; ++z)
+                if (L[z] >= (1LL << 31)) {
+                    L[z] -= (1LL << 32);
+                    L[z + 1] += 1;
+                }
+            for (int z = 0; z < kCrtLimbs; ++z) out[z] = (int)L[z];
+        };
+        for (int n = 1; n <= kCrtMaxModuli; ++n) {
+            unsigned __int128 M = 1;
+            for (int l = 0; l < n; ++l) M *= (unsigned)kCrtModuli[l];
+            CrtHost& h = table[n];
+            h.K = CrtCombine{};
+            h.K.nmod = n;
+            for (int l = 0; l < n; ++l) {
+                const unsigned ml = (unsigned)kCrtModuli[l];
+                const unsigned __int128 Ml = M / ml;
+                const unsigned r = (unsigned)(Ml % ml);
+                unsigned y = 1;
+                for (unsigned c = 1; c < ml; ++c)
+                    if ((r * c) % ml == 1) {
+                        y = c;
+                        break;
+                    }
+                limbs(Ml * y % M, h.K.w[l]);
+            }
+            limbs(M, h.K.M);
+            h.K.M_d = (double)M;
+            h.P = (int)std::floor((std::log2((double)M) - 2.0) / 2.0);
+            if (h.P > 62) h.P = 62;  // the scaled integers stay inside int64
+        }
+    });
+    return table[nmod];
+}
+
+std::atomic<int> g_last_moduli{0};
+
+cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st) {
+    const Layout L = ozaki_layout(p);
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    int8_t* a_planes = reinterpret_cast<int8_t*>(w + L.a_planes_off);
+    int8_t* b_planes = reinterpret_cast<int8_t*>(w + L.b_planes_off);
+    int8_t* residues = reinterpret_cast<int8_t*>(w + L.res_off);
+    auto* maxa = reinterpret_cast<unsigned long long*>(w + L.maxa_off);
+    auto* maxb = reinterpret_cast<unsigned long long*>(w + L.maxb_off);
+    auto* suma = reinterpret_cast<double*>(w + L.suma_off);
+    auto* sumb = reinterpret_cast<double*>(w + L.sumb_off);
+    int* expa = reinterpret_cast<int*>(w + L.expa_off);
+    int* expb = reinterpret_cast<int*>(w + L.expb_off);
+    int* status = reinterpret_cast<int*>(w + L.status_off);
+    const int nmod = p.moduli;
+    const CrtHost& H = crt_host(nmod);
+    g_last_moduli.store(nmod);
+
+    View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
+    View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
+    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);
+    if (e != cudaSuccess) return e;
+    for (int side = 0; side < 2; ++side) {
+        const View& v = side ? vb : va;
+        if (v.rs == 1) {
+            dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
+            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+        } else {
+            dim3 grid((v.rows + 7) / 8, (v.cols + 1023) / 1024);
+            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+        }
+        count_launch();
+    }
+    for (int side = 0; side < 2; ++side) {
+        const View& v = side ? vb : va;
+        const int rows_pad = side ? p.n_pad : p.m_pad;
+        dim3 sgrid(p.k_pad / 128, rows_pad / 32);
+        ozaki_crt_split<<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma, H.P, nmod, rows_pad,
+                                               p.k_pad, side ? b_planes : a_planes, side ? expb : expa);
+        count_launch();
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    CUtensorMap ma, mb;
+    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)nmod * p.m_pad, kUM)) !=
+        cudaSuccess)
+        return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)nmod * p.n_pad,
+                      p.pair ? kUN / 2 : kUN)) != cudaSuccess)
+        return e;
+
+    UmmaParams P{};
+    P.m = g.m;
+    P.n = g.n;
+    P.m_pad = p.m_pad;
+    P.n_pad = p.n_pad;
+    P.k_chunks = p.k_pad / kChunkBytes;
+    P.kseg_chunks = P.k_chunks;  // k <= kCrtMaxK: one INT32 segment
+    P.num_kseg = 1;
+    P.tiles_m = p.m_pad / (p.pair ? 2 * kUM : kUM);
+    P.tiles_n = p.n_pad / kUN;
+    P.num_tiles = P.tiles_m * P.tiles_n;
+    // one modulus per job; jobs alternate between the two TMEM accumulators so
+    // the epilogue of modulus l overlaps the products of modulus l + 1
+    P.num_jobs = nmod;
+    for (int l = 0; l < nmod; ++l) {
+        P.job_first_step[l] = l;
+        P.job_num_steps[l] = 1;
+        P.job_groups[l] = 1;
+        P.job_shift[l][0] = l;
+        P.job_shift[l][1] = 0;
+        P.job_buf[l] = l & 1;
+        P.step_a[l] = l;
+        P.step_b[l] = l;
+        P.step_acc[l] = l & 1;
+    }
+    P.status = status;
+    P.residues = residues;
+    P.res_plane = (long)p.m_pad * p.n_pad;
+    e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
+    if (e != cudaSuccess) return e;
+
+    const size_t smem = (size_t)nmod * 64 * 68;
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(ozaki_crt_combine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(kCrtMaxModuli * 64 * 68));
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    dim3 cgrid((g.m + 63) / 64, (g.n + 63) / 64);
+    ozaki_crt_combine<<<cgrid, 256, smem, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb, g.alpha, g.beta,
+                                                g.c, g.ldc, H.K);
+    count_launch();
+    return cudaGetLastError();
+}
+}  // namespace
+
+int ozaki_crt_bits(int moduli) {
+    if (moduli < 1 || moduli > kCrtMaxModuli) return 0;
+    return crt_host(moduli).P;
+}
+int ozaki_last_moduli() { return g_last_moduli.load(); }
+
 cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, cudaStream_t st) {
+    if (plan.scheme == OZAKI_CRT) return dgemm_ozaki_crt(g, plan, ws, st);
     OzakiPlan p = plan;
     const Layout L = ozaki_layout(p);
     uint8_t* w = static_cast<uint8_t*>(ws);

@@ -12,7 +12,17 @@ constexpr int kOzakiMaxSlices = 12;
 // The automatic slice count never exceeds this (its workspace is sized for it).
 constexpr int kOzakiAutoMaxSlices = 10;
 
+// Scheme II (CRT): products of int8 residues modulo up to 16 pairwise coprime
+// moduli <= 256; K is bounded so that a modular product cannot overflow INT32.
+constexpr int kCrtMaxModuli = 16;
+constexpr int kCrtDefaultModuli = 16;
+constexpr int kCrtMaxK = 130816;  // 1022 x 128: k_pad * 128^2 < 2^31 - 2^21
+
+enum OzakiScheme : int { OZAKI_AUTO = 0, OZAKI_SLICES = 1, OZAKI_CRT = 2 };
+
 struct OzakiPlan {
+    int scheme = OZAKI_SLICES;  // OZAKI_SLICES or OZAKI_CRT after planning
+    int moduli = 0;   // CRT: number of moduli (products)
     int slices = 0;   // INT8 slices per operand (7 bits each); 0 = chosen from the data
     int m_pad = 0;    // rows of A padded to the 128-row UMMA tile
     int n_pad = 0;    // columns of B padded to the 256-column UMMA tile
@@ -22,14 +32,22 @@ struct OzakiPlan {
 
 // Whether the automatic method should prefer Ozaki for this shape.
 bool ozaki_preferred(int m, int n, int k);
-// slices == 0 leaves the count to dgemm_ozaki, which derives it from the
-// dynamic range of the operands (and synchronises the stream to read it).
-OzakiPlan plan_ozaki(int m, int n, int k, int slices);
+// Scheme choice: OZAKI_AUTO takes the slice scheme when `slices` > 0 and the
+// CRT scheme otherwise (K <= kCrtMaxK); OZAKI_CRT falls back to slices beyond
+// kCrtMaxK.  slices == 0 leaves the slice count to dgemm_ozaki, which derives
+// it from the dynamic range of the operands (and synchronises the stream to
+// read it); moduli == 0 takes kCrtDefaultModuli.
+OzakiPlan plan_ozaki(int m, int n, int k, int slices, int scheme = OZAKI_AUTO, int moduli = 0);
+// Row / column scaling bits of the CRT scheme with `moduli` moduli: every
+// scaled row of op(A) and column of op(B) has 2-norm <= 2^P.
+int ozaki_crt_bits(int moduli);
+// Modulus count of the most recent CRT-scheme call.
+int ozaki_last_moduli();
 int ozaki_auto_slices(float spread_a, float spread_b);
 // Slice count of the most recent Ozaki call.
 int ozaki_last_slices();
 size_t ozaki_workspace_bytes(const OzakiPlan& p);
-// C = alpha op(A) op(B) + beta C through INT8 slice products; `ws` holds
+// C = alpha op(A) op(B) + beta C through INT8 slice or residue products; `ws` holds
 // ozaki_workspace_bytes(p) bytes of device scratch.
 cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st);
 

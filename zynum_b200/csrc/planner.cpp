@@ -18,10 +18,13 @@ GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count) {
     if (elem_bytes == 8 && n <= 64 && m >= 1024) p.tile = TILE_128x64;
     const int bn = (p.tile == TILE_128x64) ? 64 : 128;
     const long tiles = (long)((m + 127) / 128) * ((n + bn - 1) / bn);
+    // Fewer tiles than SMs: split K (each slice at least 256 deep) so that
+    // about one wave of CTAs covers the machine; the partials cost one
+    // (splits + 2) m n element pass.
     p.splits = 1;
-    if (tiles < sm_count && k >= 2048) {
+    if (tiles < sm_count && k >= 512) {
         long s = sm_count / std::max<long>(tiles, 1);
-        s = std::min<long>(s, k / 512);
+        s = std::min<long>(s, k / 256);
         s = std::min<long>(s, 64);
         if (s >= 2) p.splits = (int)s;
     }

@@ -29,6 +29,18 @@ int parse_complex_env() {
     const char* v = std::getenv("ZYNUM_GPU_COMPLEX_METHOD");
     return (v && !std::strcmp(v, "3m")) ? 1 : 0;
 }
+int parse_scheme_env() {
+    const char* v = std::getenv("ZYNUM_GPU_OZAKI_SCHEME");
+    if (v && !std::strcmp(v, "slices")) return 1;
+    if (v && !std::strcmp(v, "crt")) return 2;
+    return 0;
+}
+int parse_moduli_env() {
+    const char* v = std::getenv("ZYNUM_GPU_OZAKI_MODULI");
+    if (!v) return 0;
+    int s = std::atoi(v);
+    return (s >= 2 && s <= 16) ? s : 0;
+}
 int parse_slices_env() {
     const char* v = std::getenv("ZYNUM_GPU_OZAKI_SLICES");
     if (!v || !std::strcmp(v, "auto")) return 0;
@@ -102,6 +114,8 @@ cudaError_t Context::init() {
     dgemm_method = parse_method_env();
     sgemm_method = parse_smethod_env();
     ozaki_slices = parse_slices_env();
+    ozaki_scheme = parse_scheme_env();
+    ozaki_moduli = parse_moduli_env();
     complex_method = parse_complex_env();
     initialised = true;
     return cudaSuccess;

@@ -53,6 +53,8 @@ struct Context {
     int dgemm_method = METHOD_NATIVE;
     int sgemm_method = SMETHOD_NATIVE;
     int ozaki_slices = 0;  // 0 = automatic
+    int ozaki_scheme = 0;  // 0 = automatic, 1 = INT8 slices, 2 = CRT residues
+    int ozaki_moduli = 0;  // CRT moduli, 0 = default
     int complex_method = 0;  // 0 = expanded-real 4M, 1 = 3M
     InjectedFaults faults;
     bool initialised = false;
