@@ -156,6 +156,8 @@ struct CrtTable {
     float inv[kCrtMaxModuli];
     uint32_t wlo[kCrtMaxModuli], whi[kCrtMaxModuli];  // int8 x4: 2^(8t) mod m for t = 0..3 / 4..7
     int bias[kCrtMaxModuli];                          // 2^63 mod m
+    int off[kCrtMaxModuli];        // multiple of m added to make a byte-digit sum non-negative, minus bias
+    uint32_t barrett[kCrtMaxModuli];  // ceil(2^32 / m)
 };
 
 // Symmetric representative of r mod m: [-128, 127] for m = 256, |x| <= (m-1)/2 for odd m.
@@ -186,6 +188,9 @@ constexpr CrtTable make_crt_table() {
         long long q = 1;
         for (int b = 0; b < 63; ++b) q = (q * 2) % m;
         t.bias[l] = sym_residue(q, m);
+        // |sum_t byte_t w_t| <= 8 * 255 * 128 < 2^18: adding m * ceil((2^18 + 128) / m) keeps it >= 0
+        t.off[l] = m * (((1 << 18) + 128 + m - 1) / m) - t.bias[l];
+        t.barrett[l] = (uint32_t)((0x100000000ull + m - 1) / m);
     }
     return t;
 }
@@ -553,6 +558,14 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 constexpr int kSlots2 = 6;                      // A and B rings, 128 x 128 B each
 constexpr int kChunk2 = 128 * kChunkBytes;      // 16 KB
 constexpr size_t kSmemBytes2 = 1024 + 2 * kSlots2 * kChunk2 + 512 + kUN * 8 + 3 * kMaxSteps;
+// CRT residue products on the CTA pair: every step needs a fresh A and B
+// chunk, so a slot holds 256 bytes of K of both operands (two 128-byte swizzle
+// atoms each: A0 A1 B0 B1, 16 KB per atom and CTA) behind one full / empty
+// barrier pair, and a step issues 8 UMMAs per barrier round trip.
+constexpr int kCrtAtom = 128 * kChunkBytes;  // 16 KB
+constexpr int kCrtSlot = 4 * kCrtAtom;       // 64 KB
+constexpr int kCrtSlots = (2 * kSlots2 * kChunk2) / kCrtSlot;  // 3
+static_assert(kCrtSlots >= 2, "CRT ring");
 
 template <int KIND, int EPI>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
@@ -608,7 +621,73 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     const uint32_t tmem_base = *tmem_slot;
     const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
 
-    if (warp == 0) {
+    if (warp == 0 && EPI == EPI_RESIDUE) {
+        // ------------------------------------- TMA producer, CRT residue products
+        if (lane == 0) {
+            Ring rs;
+            bool ok = true;
+            const int steps = P.k_chunks / 2;  // 256-byte K steps (K padded to 256)
+            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
+                int tm, tn;
+                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
+                const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
+                for (int j = 0; ok && j < P.num_jobs; ++j) {
+                    const int l = P.job_shift[j][0];
+                    for (int ks = 0; ks < steps; ++ks) {
+                        if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, P.status, 1))) break;
+                        const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
+                        const uint32_t bar = smem_u32(&fullA[rs.slot]) & 0xFEFFFFFFu;
+                        if (leader) mbar_arrive_expect_tx(&fullA[rs.slot], 2 * kCrtSlot);
+                        const int x = ks * 2 * kChunkBytes;
+                        tma_load_2d_2sm(base, &tmA, bar, x, l * P.m_pad + arow);
+                        tma_load_2d_2sm(base + kCrtAtom, &tmA, bar, x + kChunkBytes, l * P.m_pad + arow);
+                        tma_load_2d_2sm(base + 2 * kCrtAtom, &tmB, bar, x, l * P.n_pad + brow);
+                        tma_load_2d_2sm(base + 3 * kCrtAtom, &tmB, bar, x + kChunkBytes, l * P.n_pad + brow);
+                        rs.advance(kCrtSlots);
+                    }
+                }
+            }
+            for (int i = 0; i < kCrtSlots; ++i) {
+                wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, nullptr, 0);
+                rs.advance(kCrtSlots);
+            }
+        }
+    } else if (warp == 1 && EPI == EPI_RESIDUE) {
+        // ------------------------------------ MMA issuer (even CTA), CRT products
+        if (lane == 0 && leader) {
+            const uint32_t idesc = umma_idesc(2, 1, 256, kUN);
+            Ring rs;
+            uint32_t tphase = 0;
+            bool ok = true;
+            const int steps = P.k_chunks / 2;
+            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
+                for (int j = 0; ok && j < P.num_jobs; ++j) {
+                    const int b = P.job_buf[j];
+                    if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                    tphase ^= 1u << b;
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + b * kUN;
+                    for (int ks = 0; ks < steps; ++ks) {
+                        if (!(ok = wait_phase(&fullA[rs.slot], rs.phase, abort_flag, P.status, 4))) break;
+                        const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
+                        const uint64_t a0 = umma_desc_sw128(base), a1 = umma_desc_sw128(base + kCrtAtom);
+                        const uint64_t b0 = umma_desc_sw128(base + 2 * kCrtAtom);
+                        const uint64_t b1 = umma_desc_sw128(base + 3 * kCrtAtom);
+                        umma_i8_2sm(d, a0, b0, idesc, ks > 0 ? 1u : 0u);
+                        umma_i8_2sm(d, a0 + 2, b0 + 2, idesc, 1u);
+                        umma_i8_2sm(d, a0 + 4, b0 + 4, idesc, 1u);
+                        umma_i8_2sm(d, a0 + 6, b0 + 6, idesc, 1u);
+                        umma_i8_2sm(d, a1, b1, idesc, 1u);
+                        umma_i8_2sm(d, a1 + 2, b1 + 2, idesc, 1u);
+                        umma_i8_2sm(d, a1 + 4, b1 + 4, idesc, 1u);
+                        umma_i8_2sm(d, a1 + 6, b1 + 6, idesc, 1u);
+                        umma_commit_2sm(&emptyA[rs.slot], 0x3);
+                        rs.advance(kCrtSlots);
+                    }
+                    if (ok) umma_commit_2sm(&tfull[b], 0x3);
+                }
+        }
+    } else if (warp == 0) {
         // ------------------------------------------------ TMA producer (both CTAs)
         if (lane == 0) {
             Ring ra, rb;
@@ -985,10 +1064,14 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
     if (r0 + r >= rows_pad) return;
     const int a = sexp[r];
     const bool finite = a != kCrtNonFinite;
+    // 2^a by one exact multiplication when both 2^a and the products stay normal
+    const bool plain = a >= -960 && a <= 960;
+    const double sc = plain ? pow2(a) : 0.0;
     uint32_t lo[16], hi[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const long long v = finite ? llrint(ldexp(tile[swz(r, q * 16 + i)], a)) : 0LL;
+        const double x = tile[swz(r, q * 16 + i)];
+        const long long v = !finite ? 0LL : __double2ll_rn(plain ? x * sc : ldexp(x, a));
         const unsigned long long u = (unsigned long long)v ^ (1ull << 63);
         lo[i] = (uint32_t)u;
         hi[i] = (uint32_t)(u >> 32);
@@ -1005,18 +1088,19 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
         *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     for (int l = 1; l < nmod; ++l) {
-        const int m = kCrt.m[l];
-        const float inv = kCrt.inv[l];
-        const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l];
-        const int nb = -kCrt.bias[l];
+        const int m = kCrt.m[l], half = (m + 1) / 2;
+        const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l], bm = kCrt.barrett[l];
+        const int c0 = kCrt.off[l];
         uint32_t w[4];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
             uint32_t x = 0;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const int v = dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, nb));  // |v| < 2^18
-                int rr = v - __float2int_rn(__int2float_rn(v) * inv) * m;             // exact: |v| < 2^24
+                // v in [0, 2^20): Barrett quotient floor(v / m) is exact
+                const uint32_t v = (uint32_t)dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
+                int rr = (int)(v - __umulhi(v, bm) * (uint32_t)m);
+                rr -= rr >= half ? m : 0;
                 x |= ((uint32_t)rr & 0xFFu) << (8 * i);
             }
             w[g] = x;
@@ -1035,67 +1119,79 @@ struct CrtCombine {
     double M_d;
 };
 
-// C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 64 x 64 tile.
-// The residue sum S = sum_l r_l w_l is exact in int64 limbs (|r_l w_l limb| <
-// 2^39); q = round(S / M) from an FP64 estimate (|C_bar| < M / 4 keeps S / M
-// within 1/4 of an integer); C_bar = S - q M, carried to balanced limbs and
-// rounded to FP64 from the top limb down.
-__global__ void __launch_bounds__(256)
+// C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 64 x 64 tile;
+// thread (i, q) of the block takes row i and columns 16 q .. 16 q + 15 and
+// reads its 16 residues of every modulus as one 16-byte load per plane
+// (four lanes cover one 64-byte row segment).  The residue sum S = sum_l r_l
+// w_l is exact in int64 limbs (|r_l w_l limb| < 2^39); q = round(S / M) from an
+// FP64 estimate (|C_bar| <= M / 4 keeps S / M near an integer); C_bar = S - q M,
+// carried to balanced limbs and rounded to FP64 from the top limb down.
+template <int NMOD>
+__global__ void __launch_bounds__(256, 2)
 ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
                   const int* __restrict__ expb, double alpha, double beta, double* __restrict__ C, long ldc,
                   const __grid_constant__ CrtCombine K) {
-    extern __shared__ uint8_t rs[];  // [nmod][64][68]
-    constexpr int kPitch = 68;
-    const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64, t = threadIdx.x;
-    {
-        const int row = t >> 2, cc = t & 3;
-        for (int l = 0; l < K.nmod; ++l) {
-            const uint4 v = __ldcs(reinterpret_cast<const uint4*>(res + l * plane + (long)(i0 + row) * res_ld + j0 +
-                                                                  cc * 16));
-            uint32_t* d = reinterpret_cast<uint32_t*>(rs + (l * 64 + row) * kPitch + cc * 16);
-            d[0] = v.x;
-            d[1] = v.y;
-            d[2] = v.z;
-            d[3] = v.w;
-        }
+    const int t = threadIdx.x;
+    const int i = t >> 2, q = t & 3;
+    const int gi = blockIdx.x * 64 + i, j0 = blockIdx.y * 64 + q * 16;
+    if (gi >= m || j0 >= n) return;
+    uint4 v[NMOD];
+#pragma unroll
+    for (int l = 0; l < NMOD; ++l)
+        v[l] = __ldcs(reinterpret_cast<const uint4*>(res + l * plane + (long)gi * res_ld + j0));
+    int eb[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int4 e4 = __ldg(reinterpret_cast<const int4*>(expb + j0) + c);
+        eb[4 * c] = e4.x;
+        eb[4 * c + 1] = e4.y;
+        eb[4 * c + 2] = e4.z;
+        eb[4 * c + 3] = e4.w;
     }
-    __syncthreads();
-    const int i = t & 63, jq = t >> 6;
-    const int gi = i0 + i;
-    if (gi >= m) return;
     const int ea = expa[gi];
-#pragma unroll 1
+#pragma unroll
     for (int jj = 0; jj < 16; ++jj) {
-        const int j = jq * 16 + jj, gj = j0 + j;
+        const int gj = j0 + jj;
         if (gj >= n) break;
-        const double cin = beta != 0.0 ? C[(long)gj * ldc + gi] : 0.0;  // issued ahead of the arithmetic
+        const double cin = beta != 0.0 ? C[(long)gj * ldc + gi] : 0.0;
         long long acc[kCrtLimbs] = {0, 0, 0, 0};
-        for (int l = 0; l < K.nmod; ++l) {
-            const int r = (int)(int8_t)rs[(l * 64 + i) * kPitch + j];
+#pragma unroll
+        for (int l = 0; l < NMOD; ++l) {
+            const uint32_t word = (jj >> 2) == 0 ? v[l].x : (jj >> 2) == 1 ? v[l].y : (jj >> 2) == 2 ? v[l].z : v[l].w;
+            const int r = (int)(signed char)(word >> (8 * (jj & 3)));
 #pragma unroll
             for (int z = 0; z < kCrtLimbs; ++z) acc[z] += (long long)r * K.w[l][z];
         }
         double sd = 0.0;
 #pragma unroll
         for (int z = kCrtLimbs - 1; z >= 0; --z) sd = sd * 4294967296.0 + (double)acc[z];
-        const long long q = (long long)rint(sd / K.M_d);
+        const long long qq = __double2ll_rn(sd / K.M_d);
 #pragma unroll
-        for (int z = 0; z < kCrtLimbs; ++z) acc[z] -= q * K.M[z];
+        for (int z = 0; z < kCrtLimbs; ++z) acc[z] -= qq * K.M[z];
 #pragma unroll
         for (int z = 0; z < kCrtLimbs - 1; ++z) {
             const long long c = (acc[z] + (1LL << 31)) >> 32;
             acc[z] -= c << 32;
             acc[z + 1] += c;
         }
-        double v = (double)acc[kCrtLimbs - 1];
+        double x = (double)acc[kCrtLimbs - 1];
 #pragma unroll
-        for (int z = kCrtLimbs - 2; z >= 0; --z) v = v * 4294967296.0 + (double)acc[z];
-        const int eb = expb[gj];
-        double out = (ea == kCrtNonFinite || eb == kCrtNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
-                                                                  : alpha * ldexp(v, -(ea + eb));
+        for (int z = kCrtLimbs - 2; z >= 0; --z) x = x * 4294967296.0 + (double)acc[z];
+        double out = (ea == kCrtNonFinite || eb[jj] == kCrtNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
+                                                                      : alpha * ldexp(x, -(ea + eb[jj]));
         if (beta != 0.0) out = fma(beta, cin, out);
         C[(long)gj * ldc + gi] = out;
     }
+}
+
+using CombineFn = void (*)(const int8_t*, long, int, int, int, const int*, const int*, double, double, double*, long,
+                           CrtCombine);
+template <int N>
+constexpr CombineFn combine_at(int nmod) {
+    if constexpr (N == 1)
+        return &ozaki_crt_combine<1>;
+    else
+        return nmod == N ? &ozaki_crt_combine<N> : combine_at<N - 1>(nmod);
 }
 
 // 3xBF16 split of a float matrix view into hi / lo planes (bf16, K-major).
@@ -1301,7 +1397,8 @@ OzakiPlan plan_ozaki(int m, int n, int k, int slices, int scheme, int moduli) {
     p.pair = use_cta_pair(m);
     p.m_pad = (int)round_up(m, p.pair ? 2 * kUM : kUM);
     p.n_pad = (int)round_up(n, kUN);
-    p.k_pad = (int)round_up(k, kChunkBytes);
+    // CRT: K in 256-byte steps on the CTA pair
+    p.k_pad = (int)round_up(k, p.scheme == OZAKI_CRT ? 2 * kChunkBytes : kChunkBytes);
     return p;
 }
 
@@ -1439,17 +1536,9 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
 
-    const size_t smem = (size_t)nmod * 64 * 68;
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(ozaki_crt_combine, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(kCrtMaxModuli * 64 * 68));
-    });
-    if (attr_err != cudaSuccess) return attr_err;
     dim3 cgrid((g.m + 63) / 64, (g.n + 63) / 64);
-    ozaki_crt_combine<<<cgrid, 256, smem, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb, g.alpha, g.beta,
-                                                g.c, g.ldc, H.K);
+    combine_at<kCrtMaxModuli>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
+                                                          g.alpha, g.beta, g.c, g.ldc, H.K);
     count_launch();
     return cudaGetLastError();
 }
