@@ -92,7 +92,7 @@ struct UmmaParams {
     const int* row_exp;
     const int* col_exp;
     int* status;
-    int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad]
+    int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad] (row-major)
     long res_plane;
 };
 
@@ -156,8 +156,7 @@ struct CrtTable {
     float inv[kCrtMaxModuli];
     uint32_t wlo[kCrtMaxModuli], whi[kCrtMaxModuli];  // int8 x4: 2^(8t) mod m for t = 0..3 / 4..7
     int bias[kCrtMaxModuli];                          // 2^63 mod m
-    int off[kCrtMaxModuli];        // multiple of m added to make a byte-digit sum non-negative, minus bias
-    uint32_t barrett[kCrtMaxModuli];  // ceil(2^32 / m)
+    int magic[kCrtMaxModuli];  // 0x4B400000 - bias: the dp4a sum reads as the FP32 number 1.5 2^23 + value
 };
 
 // Symmetric representative of r mod m: [-128, 127] for m = 256, |x| <= (m-1)/2 for odd m.
@@ -189,8 +188,7 @@ constexpr CrtTable make_crt_table() {
         for (int b = 0; b < 63; ++b) q = (q * 2) % m;
         t.bias[l] = sym_residue(q, m);
         // |sum_t byte_t w_t| <= 8 * 255 * 128 < 2^18: adding m * ceil((2^18 + 128) / m) keeps it >= 0
-        t.off[l] = m * (((1 << 18) + 128 + m - 1) / m) - t.bias[l];
-        t.barrett[l] = (uint32_t)((0x100000000ull + m - 1) / m);
+        t.magic[l] = 0x4B400000 - t.bias[l];
     }
     return t;
 }
@@ -218,7 +216,8 @@ ZB_DEVICE int crt_reduce(int v, int m, float inv) {
     return v > 127 ? v - m : v;
 }
 
-// 32 INT32 modular products of one TMEM lane -> 32 int8 residues (32 bytes).
+// 32 INT32 modular products of one TMEM lane -> 32 int8 residues (32 bytes of
+// one row of a row-major residue plane).
 ZB_DEVICE void residue_chunk(const uint32_t (&r)[32], int mod_idx, int8_t* dst) {
     uint32_t w[8];
     if (mod_idx == 0) {  // m = 256: the low byte of the two's-complement sum
@@ -1088,99 +1087,158 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
         *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     for (int l = 1; l < nmod; ++l) {
-        const int m = kCrt.m[l], half = (m + 1) / 2;
-        const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l], bm = kCrt.barrett[l];
-        const int c0 = kCrt.off[l];
+        const float m = (float)kCrt.m[l], inv = kCrt.inv[l];
+        const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l];
+        const int c0 = kCrt.magic[l];
         uint32_t w[4];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
-            uint32_t x = 0;
+            uint32_t rb[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                // v in [0, 2^20): Barrett quotient floor(v / m) is exact
-                const uint32_t v = (uint32_t)dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
-                int rr = (int)(v - __umulhi(v, bm) * (uint32_t)m);
-                rr -= rr >= half ? m : 0;
-                x |= ((uint32_t)rr & 0xFFu) << (8 * i);
+                // value v = sum_t byte_t (2^8t mod m) - (2^63 mod m), |v| < 2^18; the dp4a
+                // result is the bit pattern of the float 1.5 2^23 + v, so x = v exactly;
+                // q = round(v / m) by the 1.5 2^23 shift, r = v - q m is exact and
+                // |r| <= (m - 1) / 2; r + 1.5 2^23 carries r in its low byte
+                const int d = dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
+                const float x = __int_as_float(d) - 12582912.0f;
+                const float q = __fmaf_rn(x, inv, 12582912.0f) - 12582912.0f;
+                rb[i] = (uint32_t)__float_as_int(__fmaf_rn(-q, m, x) + 12582912.0f);
             }
-            w[g] = x;
+            w[g] = __byte_perm(__byte_perm(rb[0], rb[1], 0x0040), __byte_perm(rb[2], rb[3], 0x0040), 0x5410);
         }
         *reinterpret_cast<uint4*>(out + l * plane) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-// Balanced 32-bit limbs (int32) of the CRT weights w_l = M_l (M_l^-1 mod m_l)
-// mod M and of M = prod m_l; M < 2^127 for 16 moduli, so four limbs hold it.
-constexpr int kCrtLimbs = 4;
+// CRT weights w_l = M_l (M_l^-1 mod m_l) mod M and M = prod m_l (< 2^127 for
+// 16 moduli) as eight balanced 16-bit limbs.  wpair[z][g] packs limb z of the
+// weights of moduli (4g, 4g+1) (.x) and (4g+2, 4g+3) (.y) as two int16 each:
+// the operands of dp2a.lo / dp2a.hi against four packed int8 residues.
+constexpr int kCrtLimbs = 8;
 struct CrtCombine {
     int nmod;
-    int w[kCrtMaxModuli][kCrtLimbs];
+    uint2 wpair[kCrtLimbs][kCrtMaxModuli / 4];
     int M[kCrtLimbs];
-    double M_d;
+    double M_d, inv_M;
 };
 
-// C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 64 x 64 tile;
-// thread (i, q) of the block takes row i and columns 16 q .. 16 q + 15 and
-// reads its 16 residues of every modulus as one 16-byte load per plane
-// (four lanes cover one 64-byte row segment).  The residue sum S = sum_l r_l
-// w_l is exact in int64 limbs (|r_l w_l limb| < 2^39); q = round(S / M) from an
-// FP64 estimate (|C_bar| <= M / 4 keeps S / M near an integer); C_bar = S - q M,
-// carried to balanced limbs and rounded to FP64 from the top limb down.
+constexpr double pow2_const(int e) {
+    double x = 1.0;
+    for (int i = 0; i < e; ++i) x *= 2.0;
+    return x;
+}
+
+// Exact int32 -> FP64 without the conversion unit: the bits 0x43300000:(v ^ 2^31)
+// encode 2^52 + 2^31 + v.
+ZB_DEVICE double i2d(int v) {
+    return __hiloint2double(0x43300000, v ^ 0x80000000) - 4503601774854144.0;  // 2^52 + 2^31
+}
+
+// d = c + a.s16[0] * b.s8[0] + a.s16[1] * b.s8[1]  (HI: bytes 2, 3 of b)
+template <bool HI>
+ZB_DEVICE int dp2a_ss(uint32_t a, uint32_t b, int c) {
+    int d;
+    if (HI)
+        asm("dp2a.hi.s32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    else
+        asm("dp2a.lo.s32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 16 x 128 tile of
+// row-major residue planes.  Warp w takes rows w and w + 8, lane L columns
+// 4L .. 4L+3: per plane one 4-byte load (128 contiguous bytes per warp); a
+// byte transpose (PRMT) packs four moduli of one element per register; limb z
+// of S = sum_l r_l w_l is 8 dp2a (|limb sum| < 2^26, exact in int32).
+// q = round(S / M) from an FP64 estimate (|C_bar| <= M / 4 keeps S / M near an
+// integer); C_bar = S - q M is carried to balanced 16-bit limbs and rounded to
+// FP64 from the top limb down.  The scaled results pass through shared memory
+// so that C (column-major) is written 128 bytes per column.
 template <int NMOD>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256)
 ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
                   const int* __restrict__ expb, double alpha, double beta, double* __restrict__ C, long ldc,
                   const __grid_constant__ CrtCombine K) {
-    const int t = threadIdx.x;
-    const int i = t >> 2, q = t & 3;
-    const int gi = blockIdx.x * 64 + i, j0 = blockIdx.y * 64 + q * 16;
-    if (gi >= m || j0 >= n) return;
-    uint4 v[NMOD];
+    constexpr int G = (NMOD + 3) / 4;  // groups of four moduli
+    // every modulus is >= 191 > 2^7.5, so log2 M >= 7.5 NMOD
+    constexpr int Z0 = (15 * NMOD - 78) > 0 ? (15 * NMOD - 78) / 32 : 0;
+    constexpr double kScaleZ0 = pow2_const(16 * Z0);
+    __shared__ double ct[16][129];  // column 4L + e holds element (4L + e - L) & 3 of lane L
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int i0 = blockIdx.x * 16, j0 = blockIdx.y * 128;
+    const int jc = j0 + lane * 4;  // < n_pad: the planes are padded to 256 columns
+    const int4 e4 = __ldg(reinterpret_cast<const int4*>(expb + jc));
+    const int eb[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const int rl = warp + 8 * h, gi = i0 + rl;  // < m_pad: the planes are padded to 128 rows
+        const int8_t* rp = res + (long)gi * res_ld + jc;
+        int cs[4][kCrtLimbs];
 #pragma unroll
-    for (int l = 0; l < NMOD; ++l)
-        v[l] = __ldcs(reinterpret_cast<const uint4*>(res + l * plane + (long)gi * res_ld + j0));
-    int eb[16];
+        for (int e = 0; e < 4; ++e)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int4 e4 = __ldg(reinterpret_cast<const int4*>(expb + j0) + c);
-        eb[4 * c] = e4.x;
-        eb[4 * c + 1] = e4.y;
-        eb[4 * c + 2] = e4.z;
-        eb[4 * c + 3] = e4.w;
+            for (int z = 0; z < kCrtLimbs; ++z) cs[e][z] = 0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                v[u] = 4 * g + u < NMOD ? __ldcs(reinterpret_cast<const uint32_t*>(rp + (4 * g + u) * plane)) : 0u;
+            // pk[e]: residues of moduli 4g .. 4g+3 of element e
+            const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140), t1 = __byte_perm(v[2], v[3], 0x5140);
+            const uint32_t t2 = __byte_perm(v[0], v[1], 0x7362), t3 = __byte_perm(v[2], v[3], 0x7362);
+            const uint32_t pk[4] = {__byte_perm(t0, t1, 0x5410), __byte_perm(t0, t1, 0x7632),
+                                    __byte_perm(t2, t3, 0x5410), __byte_perm(t2, t3, 0x7632)};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+#pragma unroll
+                for (int z = 0; z < kCrtLimbs; ++z) {
+                    cs[e][z] = dp2a_ss<false>(K.wpair[z][g].x, pk[e], cs[e][z]);
+                    cs[e][z] = dp2a_ss<true>(K.wpair[z][g].y, pk[e], cs[e][z]);
+                }
+        }
+        const int ea = expa[gi];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int* c = cs[e];
+            // limbs below Z0 add less than 2^(16 Z0 + 27) <= M 2^-12 to S, so the
+            // upper limbs place S / M within 2^-12 of its value
+            double sd = i2d(c[kCrtLimbs - 1]);
+#pragma unroll
+            for (int z = kCrtLimbs - 2; z >= Z0; --z) sd = fma(sd, 65536.0, i2d(c[z]));
+            sd *= kScaleZ0;
+            const int q = __double2int_rn(sd * K.inv_M);
+#pragma unroll
+            for (int z = 0; z < kCrtLimbs; ++z) c[z] -= q * K.M[z];
+#pragma unroll
+            for (int z = 0; z < kCrtLimbs - 1; ++z) {
+                const int carry = (c[z] + 32768) >> 16;
+                c[z] -= carry << 16;
+                c[z + 1] += carry;
+            }
+            double x = i2d(c[kCrtLimbs - 1]);
+#pragma unroll
+            for (int z = kCrtLimbs - 2; z >= 0; --z) x = fma(x, 65536.0, i2d(c[z]));
+            const int sc = -(ea + eb[e]);
+            ct[rl][lane * 4 + ((e + lane) & 3)] = (ea == kCrtNonFinite || eb[e] == kCrtNonFinite)
+                                       ? __longlong_as_double(0x7ff8000000000000LL)
+                                       : alpha * (sc >= -1022 && sc <= 1023 ? x * pow2(sc) : ldexp(x, sc));
+        }
     }
-    const int ea = expa[gi];
-#pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-        const int gj = j0 + jj;
+    __syncthreads();
+    // column-major write: 16 consecutive rows (128 bytes) of one column per half-warp
+    const int r = t & 15;
+    const int gi = i0 + r;
+    if (gi >= m) return;
+#pragma unroll 4
+    for (int cc = t >> 4; cc < 128; cc += 16) {
+        const int gj = j0 + cc;
         if (gj >= n) break;
-        const double cin = beta != 0.0 ? C[(long)gj * ldc + gi] : 0.0;
-        long long acc[kCrtLimbs] = {0, 0, 0, 0};
-#pragma unroll
-        for (int l = 0; l < NMOD; ++l) {
-            const uint32_t word = (jj >> 2) == 0 ? v[l].x : (jj >> 2) == 1 ? v[l].y : (jj >> 2) == 2 ? v[l].z : v[l].w;
-            const int r = (int)(signed char)(word >> (8 * (jj & 3)));
-#pragma unroll
-            for (int z = 0; z < kCrtLimbs; ++z) acc[z] += (long long)r * K.w[l][z];
-        }
-        double sd = 0.0;
-#pragma unroll
-        for (int z = kCrtLimbs - 1; z >= 0; --z) sd = sd * 4294967296.0 + (double)acc[z];
-        const long long qq = __double2ll_rn(sd / K.M_d);
-#pragma unroll
-        for (int z = 0; z < kCrtLimbs; ++z) acc[z] -= qq * K.M[z];
-#pragma unroll
-        for (int z = 0; z < kCrtLimbs - 1; ++z) {
-            const long long c = (acc[z] + (1LL << 31)) >> 32;
-            acc[z] -= c << 32;
-            acc[z + 1] += c;
-        }
-        double x = (double)acc[kCrtLimbs - 1];
-#pragma unroll
-        for (int z = kCrtLimbs - 2; z >= 0; --z) x = x * 4294967296.0 + (double)acc[z];
-        double out = (ea == kCrtNonFinite || eb[jj] == kCrtNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
-                                                                      : alpha * ldexp(x, -(ea + eb[jj]));
-        if (beta != 0.0) out = fma(beta, cin, out);
-        C[(long)gj * ldc + gi] = out;
+        double* cp = C + (long)gj * ldc + gi;
+        double out = ct[r][(cc & ~3) | (((cc & 3) + (cc >> 2)) & 3)];
+        if (beta != 0.0) out = fma(beta, *cp, out);
+        *cp = out;
     }
 }
 
@@ -1416,12 +1474,13 @@ const CrtHost& crt_host(int nmod) {
     static CrtHost table[kCrtMaxModuli + 1];
     static std::once_flag once;
     std::call_once(once, [] {
+        // balanced 16-bit limbs: x = sum_z out[z] 2^(16 z), out[z] in [-2^15, 2^15) (top limb: the rest)
         auto limbs = [](unsigned __int128 x, int* out) {
             long long L[kCrtLimbs];
-            for (int z = 0; z < kCrtLimbs; ++z) L[z] = (long long)((x >> (32 * z)) & 0xFFFFFFFFu);
+            for (int z = 0; z < kCrtLimbs; ++z) L[z] = (long long)((x >> (16 * z)) & 0xFFFFu);
             for (int z = 0; z < kCrtLimbs - 1; ++z)
-                if (L[z] >= (1LL << 31)) {
-                    L[z] -= (1LL << 32);
+                if (L[z] >= (1LL << 15)) {
+                    L[z] -= (1LL << 16);
                     L[z + 1] += 1;
                 }
             for (int z = 0; z < kCrtLimbs; ++z) out[z] = (int)L[z];
@@ -1432,6 +1491,7 @@ const CrtHost& crt_host(int nmod) {
             CrtHost& h = table[n];
             h.K = CrtCombine{};
             h.K.nmod = n;
+            int w[kCrtMaxModuli][kCrtLimbs] = {};  // moduli beyond n keep zero weights
             for (int l = 0; l < n; ++l) {
                 const unsigned ml = (unsigned)kCrtModuli[l];
                 const unsigned __int128 Ml = M / ml;
@@ -1442,10 +1502,17 @@ const CrtHost& crt_host(int nmod) {
                         y = c;
                         break;
                     }
-                limbs(Ml * y % M, h.K.w[l]);
+                limbs(Ml * y % M, w[l]);
             }
+            for (int z = 0; z < kCrtLimbs; ++z)
+                for (int g = 0; g < kCrtMaxModuli / 4; ++g) {
+                    auto pack = [](int lo, int hi) { return (uint32_t)(uint16_t)lo | ((uint32_t)(uint16_t)hi << 16); };
+                    h.K.wpair[z][g].x = pack(w[4 * g][z], w[4 * g + 1][z]);
+                    h.K.wpair[z][g].y = pack(w[4 * g + 2][z], w[4 * g + 3][z]);
+                }
             limbs(M, h.K.M);
             h.K.M_d = (double)M;
+            h.K.inv_M = 1.0 / h.K.M_d;
             h.P = (int)std::floor((std::log2((double)M) - 2.0) / 2.0);
             if (h.P > 62) h.P = 62;  // the scaled integers stay inside int64
         }
@@ -1536,7 +1603,7 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
 
-    dim3 cgrid((g.m + 63) / 64, (g.n + 63) / 64);
+    dim3 cgrid((g.m + 15) / 16, (g.n + 127) / 128);
     combine_at<kCrtMaxModuli>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
                                                           g.alpha, g.beta, g.c, g.ldc, H.K);
     count_launch();
