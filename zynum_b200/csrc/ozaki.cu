@@ -94,6 +94,7 @@ struct UmmaParams {
     int* status;
     int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad] (row-major)
     long res_plane;
+    int band_rows;     // EPI_RESIDUE on the CTA pair: tile-rows per raster band
 };
 
 // ------------------------------------------------------ bounded waiting
@@ -109,10 +110,9 @@ ZB_DEVICE bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort_fl
     return false;
 }
 
-ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn) {
-    // Bands of 8 tile-rows sweep the tile-columns, so CTAs running together
+ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn, int G = 8) {
+    // Bands of G tile-rows sweep the tile-columns, so CTAs running together
     // share A row blocks and B column blocks in L2.
-    constexpr int G = 8;
     int band = tile / (G * tiles_n);
     int rows_in_band = min(G, tiles_m - band * G);
     int r = tile - band * G * tiles_n;
@@ -236,9 +236,11 @@ ZB_DEVICE void residue_chunk(const uint32_t (&r)[32], int mod_idx, int8_t* dst) 
             w[q] = x;
         }
     }
+    // streaming stores: the residues are read once, by the reconstruction, and
+    // should not displace the operand planes the other tiles still read from L2
     uint4* d = reinterpret_cast<uint4*>(dst);
-    __stcg(d, make_uint4(w[0], w[1], w[2], w[3]));
-    __stcg(d + 1, make_uint4(w[4], w[5], w[6], w[7]));
+    __stcs(d, make_uint4(w[0], w[1], w[2], w[3]));
+    __stcs(d + 1, make_uint4(w[4], w[5], w[6], w[7]));
 }
 
 // Per-step flags of the job schedule, staged in shared memory once per CTA so
@@ -626,11 +628,13 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             Ring rs;
             bool ok = true;
             const int steps = P.k_chunks / 2;  // 256-byte K steps (K padded to 256)
-            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
-                int tm, tn;
-                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
-                const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
-                for (int j = 0; ok && j < P.num_jobs; ++j) {
+            // modulus-major: every tile of modulus l before modulus l + 1, so the
+            // running pairs share one modulus' planes in L2
+            for (int j = 0; ok && j < P.num_jobs; ++j)
+                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
+                    int tm, tn;
+                    tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
+                    const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
                     const int l = P.job_shift[j][0];
                     for (int ks = 0; ks < steps; ++ks) {
                         if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, P.status, 1))) break;
@@ -645,7 +649,6 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                         rs.advance(kCrtSlots);
                     }
                 }
-            }
             for (int i = 0; i < kCrtSlots; ++i) {
                 wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, nullptr, 0);
                 rs.advance(kCrtSlots);
@@ -659,9 +662,10 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             uint32_t tphase = 0;
             bool ok = true;
             const int steps = P.k_chunks / 2;
-            for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
-                for (int j = 0; ok && j < P.num_jobs; ++j) {
-                    const int b = P.job_buf[j];
+            int inst = 0;  // job instances alternate between the two accumulators
+            for (int j = 0; ok && j < P.num_jobs; ++j)
+                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs, ++inst) {
+                    const int b = inst & 1;
                     if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
@@ -768,7 +772,33 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         const uint32_t tempty_cta0 = mapa_shared(smem_u32(&tempty[0]), 0);  // buffer b: + 8 b
         uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
         bool ok = true;
-        for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
+        if (EPI == EPI_RESIDUE) {
+            // modulus-major, in the order of the MMA issuer
+            int inst = 0;
+            for (int j = 0; ok && j < P.num_jobs; ++j)
+                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs, ++inst) {
+                    int tm, tn;
+                    tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
+                    const int b = inst & 1;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    tphase ^= 1u << b;
+                    tc_fence_after();
+                    const int row = tm * 256 + row_in_tile;
+                    int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
+                                  (long)tn * kUN;
+#pragma unroll 1
+                    for (int ch = 0; ch < kUN / 32; ++ch) {
+                        uint32_t r0[32];
+                        tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
+                        tmem_ld_wait();
+                        residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
+                }
+        }
+        for (int tile = pair; EPI != EPI_RESIDUE && ok && tile < P.num_tiles; tile += npairs) {
             int tm, tn;
             tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
             const int row = tm * 256 + row_in_tile;
@@ -790,22 +820,6 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
-                    if (EPI == EPI_RESIDUE) {
-                        // one modulus per job: accumulator b -> int8 residues, row-major plane
-                        int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
-                                      (long)tn * kUN;
-#pragma unroll 1
-                        for (int ch = 0; ch < kUN / 32; ++ch) {
-                            uint32_t r0[32];
-                            tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
-                            tmem_ld_wait();
-                            residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
-                        }
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
-                        continue;
-                    }
                     const bool two = P.job_groups[j] == 2;
                     const double s0 = (EPI == EPI_OZAKI_F64) ? pow2(er - P.job_shift[j][0]) * P.alpha : 1.0;
 #pragma unroll 1
@@ -1600,6 +1614,10 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     P.status = status;
     P.residues = residues;
     P.res_plane = (long)p.m_pad * p.n_pad;
+    // CTA pair, modulus-major: bands of tile-rows whose A rows of one modulus
+    // (band x 256 rows x k_pad bytes) stay within ~48 MB of L2 while the band
+    // sweeps the tile-columns
+    P.band_rows = (int)std::max(1L, std::min<long>(P.tiles_m, (48L << 20) / (256L * p.k_pad)));
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
 
