@@ -35,6 +35,10 @@ sys.path.insert(0, str(ROOT))
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12  # 64 DFMA/clk/SM at the 1965 MHz max clock
 METRIC = "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error; batch GFLOP/s"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel on the
+# 8192^3 headline workload, from one-pass ncu captures of this script's default run:
+# CRT modular-product GEMM 11.76 GB + 1.07 GB; native DMMA DGEMM 15.80 GB + 0.53 GB.
+TRAFFIC_8192 = {"crt": 11.76e9 + 1.07e9, "native": 15.80e9 + 0.53e9}
 
 
 def _peaks():
@@ -280,6 +284,8 @@ def bench_differentiation(torch, steps, warmup, n=4096, r=512, seed=11):
     """X = TRSM(L, B), C = SYRK(X^T) = X^T X, loss = sum(sin(C)); forward + backward with X recomputed.
     L: n x n lower, off-diagonals N(0, 1/n), diagonal 1 + |N(0,1)|; B: n x r N(0,1)."""
     from zynum_b200 import autograd as ag
+    from zynum_b200 import blas
+    old = blas.set_dgemm_method(blas.METHOD_NATIVE)  # the adjoint workload runs native FP64
     g = torch.Generator(device="cuda").manual_seed(seed)
     L = torch.tril(torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64) / np.sqrt(n), -1)
     L += torch.diag(1 + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
@@ -292,11 +298,12 @@ def bench_differentiation(torch, steps, warmup, n=4096, r=512, seed=11):
         torch.autograd.grad(loss, (L, B))
 
     ms = time_device(torch, step, steps, warmup, torch.cuda.current_stream())
+    blas.set_dgemm_method(old)
     # nominal flops: forward TRSM n^2 r + SYRK r(r+1)n; backward TRSM (dB) n^2 r + recompute n^2 r
     # + dL = -tril(dB X^T) n^2 r + dX = X (G + G^T) 4 n r^2
     gflop = (3 * n * n * r + n * n * r + r * (r + 1) * n + 4 * n * r * r) / 1e9
     return {"n": n, "nrhs": r, "ms_fwd_bwd": ms, "gflop_nominal": gflop, "gflops": gflop / (ms * 1e-3),
-            "recompute": True}
+            "recompute": True, "dgemm_method": "native FP64"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -426,7 +433,8 @@ def run_ours(args, rank, world, local_rank):
         int8_peak = 2.0 * peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"])
         achieved = ops / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (int8)",
-                "frac": (achieved / int8_peak) if achieved else None, "traffic": None,
+                "frac": (achieved / int8_peak) if achieved else None,
+                "traffic": TRAFFIC_8192["crt"] if (n == 8192 and info["scheme"] == "crt") else None,
                 "kernel": ("ozaki int8 modular-product GEMM (CRT residues, tcgen05 kind::i8)" if info["scheme"] == "crt"
                            else "ozaki int8 slice-product GEMM (tcgen05 kind::i8)"),
                 "peak_source": f"2 x bf16_tflops of {peaks['_source']} peaks (int8 dense rate is 2x bf16 on sm_100)",
@@ -435,7 +443,8 @@ def run_ours(args, rank, world, local_rank):
     else:
         achieved = flop / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-                "frac": (achieved / FP64_NOMINAL_TFLOPS) if achieved else None, "traffic": None,
+                "frac": (achieved / FP64_NOMINAL_TFLOPS) if achieved else None,
+                "traffic": TRAFFIC_8192["native"] if n == 8192 else None,
                 "kernel": "native DGEMM (DMMA m16n8k8 f64)",
                 "peak_source": "nominal FP64 pipe: 148 SMs x 128 flop/clk x 1.965 GHz (no measured FP64 peak)"}
     line = {

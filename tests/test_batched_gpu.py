@@ -83,13 +83,17 @@ def test_gemm_batch_tune_cache(blas, tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-@pytest.mark.parametrize("uplo,trans", [("L", "N"), ("U", "N"), ("L", "T")])
-def test_trsm_batch(blas, oracle, dtype, uplo, trans):
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "N"), ("U", "N", "N"), ("L", "T", "N"), ("U", "T", "U")])
+def test_trsm_batch(blas, oracle, dtype, uplo, trans, diag):
+    """Sizes 16..300 plus a few large problems (several 64-row blocks and 64-row panel chunks,
+    ragged last block), 1..64 right-hand sides, alpha = 0.5."""
     import torch
-    rng = np.random.default_rng(hash((dtype, uplo, trans)) % 2**32)
+    rng = np.random.default_rng(sum(map(ord, dtype + uplo + trans + diag)))
     cnt = 120
     nn = _loguniform(rng, 16, 300, cnt)
+    nn[:4] = [1100, 777, 640, 193]
     rr = rng.integers(1, 65, cnt).astype(np.int32)
+    rr[:4] = [64, 33, 1, 17]
     npdt = np.float64 if dtype == "f64" else np.float32
     tdt = torch.float64 if dtype == "f64" else torch.float32
     Ls = []
@@ -101,13 +105,13 @@ def test_trsm_batch(blas, oracle, dtype, uplo, trans):
     Bs = [rng.standard_normal((nn[q], rr[q])).astype(npdt) for q in range(cnt)]
     tl, pa, la = _pack(torch, Ls, tdt)
     tbb, pb, lb = _pack(torch, Bs, tdt)
-    batch = blas.TrsmBatch(nn, rr, dtype=dtype, uplo=uplo, transa=trans)
+    batch = blas.TrsmBatch(nn, rr, dtype=dtype, uplo=uplo, transa=trans, diag=diag)
     batch.run(0.5, pa, la, pb, lb, use_graph=True)
     torch.cuda.synchronize()
     tol = 1e-11 if dtype == "f64" else 2e-4
     for q in range(cnt):
         ref = np.asfortranarray(Bs[q].copy())
-        oracle.trsm("L", uplo, trans, "N", nn[q], rr[q], 0.5, np.asfortranarray(Ls[q]), nn[q], ref, nn[q])
+        oracle.trsm("L", uplo, trans, diag, nn[q], rr[q], 0.5, np.asfortranarray(Ls[q]), nn[q], ref, nn[q])
         got = tbb[q].cpu().numpy().T
         assert np.all(np.abs(got - ref) <= tol * (1 + np.abs(ref))), q
 

@@ -284,16 +284,68 @@ ZB_DEVICE T tri_el(const T* a, long lda, char uplo, char trans, char diag, int r
     return a[ar + (long)ac * lda];
 }
 
-// One CTA per problem (left side): B (n x r) := alpha op(A)^-1 B.
+// One CTA per problem (left side): B (n x r) := alpha op(A)^-1 B, r <= 64.
+// For each 64-row diagonal block in solve order:
+//  * D (the block of op(A), masked to the stored triangle / unit diagonal) and
+//    the block rows X of B go to shared memory;
+//  * warp-synchronous substitution: warp w owns right-hand sides w, w + 8, ...,
+//    lane l owns block rows l and l + 32; the solved value of row i is
+//    broadcast by shuffle and the lanes update their later rows (no block
+//    barrier inside the substitution);
+//  * the rank-64 update of the rows still to solve runs over 64-row chunks of
+//    the op(A) panel staged in shared memory by coalesced cp.async copies:
+//    thread (row, group of 16 right-hand sides) accumulates 16 products per
+//    panel column from shared-memory operands.
+constexpr int kTP = kTB + 1;  // pitch of the diagonal block (column reads conflict-free)
+constexpr int kPP = kTB + 4;  // pitch of the transposed panel and of X (16-byte aligned rows)
+
+// One element, zero-filled (and `fallback`, a valid address, not read) when !ok.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+ZB_DEVICE void cp_async_el(T* dst, const T* src, const T* fallback, bool ok) {
+    if (sizeof(T) == 8)
+        cp_async_8(smem_u32(dst), ok ? src : fallback, ok ? 8 : 0);
+    else
+        cp_async_4(smem_u32(dst), ok ? src : fallback, ok ? 4 : 0);
+}
+
+// Pt[cc][rr] = op(A)[c0 + rr][kb + cc] for rr < rows, cc < sz (zero elsewhere):
+// the panel chunk transposed (K-major), loaded coalesced along A's contiguous index.
+template <typename T>
+ZB_DEVICE void load_panel(T (*Pt)[kPP], const T* A, long la, char trans, int c0, int rows, int kb, int sz) {
+    for (int e = threadIdx.x; e < kTB * kTB; e += kThreads) {
+        int rr, cc;
+        const T* src;
+        if (trans == 'N') {
+            rr = e % kTB;
+            cc = e / kTB;
+            src = A + (c0 + rr) + (long)(kb + cc) * la;
+        } else {
+            cc = e % kTB;
+            rr = e / kTB;
+            src = A + (kb + cc) + (long)(c0 + rr) * la;
+        }
+        cp_async_el(&Pt[cc][rr], src, A, rr < rows && cc < sz);
+    }
+    cp_async_commit();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2)
 trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
                     char diag, T alpha, const T* const* __restrict__ a, const int* __restrict__ lda,
                     T* const* __restrict__ b, const int* __restrict__ ldb) {
     extern __shared__ __align__(16) unsigned char trsm_smem[];
-    T(*D)[kTB + 1] = reinterpret_cast<T(*)[kTB + 1]>(trsm_smem);             // diagonal block of op(A)
-    T(*X)[kMaxRhs + 1] = reinterpret_cast<T(*)[kMaxRhs + 1]>(D + kTB);       // solved rows of this block
+    // Two 64 x kPP buffers: the diagonal block D (pitch kTP) during the
+    // substitution, then the second buffer of transposed panel chunks.
+    T* buf0 = reinterpret_cast<T*>(trsm_smem);
+    T(*D)[kTP] = reinterpret_cast<T(*)[kTP]>(buf0);
+    T(*Pd)[kPP] = reinterpret_cast<T(*)[kPP]>(buf0);
+    T(*X)[kPP] = reinterpret_cast<T(*)[kPP]>(buf0 + kTB * kPP);      // block rows of B
+    T(*Pn)[kPP] = reinterpret_cast<T(*)[kPP]>(buf0 + 2 * kTB * kPP);  // panel chunk (transposed)
+    T* dinv = buf0 + 3 * kTB * kPP;                                     // 1 / D[i][i]
     const bool upper = (trans == 'N' && uplo == 'U') || (trans != 'N' && uplo == 'L');
+    const bool unit = diag == 'U';
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int w = blockIdx.x; w < count; w += gridDim.x) {
         const int q = order[w];
         if (q < 0) continue;  // padding item of the per-CTA schedule
@@ -315,48 +367,110 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
                 const int rr = e % kTB, cc = e / kTB;
                 D[rr][cc] = (rr < sz && cc < sz) ? tri_el(A, la, uplo, trans, diag, kb + rr, kb + cc) : T(0);
             }
+            for (int e = threadIdx.x; e < kTB * kMaxRhs; e += kThreads) {
+                const int rr = e % kTB, cc = e / kTB;
+                X[rr][cc] = (rr < sz && cc < r) ? B[kb + rr + (long)cc * lb] : T(0);
+            }
+            __syncthreads();
+            if (threadIdx.x < kTB) dinv[threadIdx.x] = (unit || threadIdx.x >= sz) ? T(1) : T(1) / D[threadIdx.x][threadIdx.x];
+            // rows still to solve after this block; their first panel chunk loads
+            // during the substitution
+            const int u0 = upper ? 0 : kb + sz, u1 = upper ? kb : n;
+            if (u0 < u1) load_panel(Pn, A, la, trans, u0, min(kTB, u1 - u0), kb, sz);
+            __syncthreads();
+            // ---- substitution: warp w, right-hand sides w + 8 c; lane rows lane, lane + 32
+            {
+                T x[2][8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
+                for (int it = 0; it < sz; ++it) {
+                    const int i = upper ? sz - 1 - it : it;
+                    const int hi = i >> 5, li = i & 31;
+                    const T di = dinv[i];
+                    T xi[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const T own = (hi ? x[1][c] : x[0][c]) * di;
+                        xi[c] = __shfl_sync(0xffffffffu, own, li);
+                    }
+                    if (lane == li) {
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            if (hi) x[1][c] = xi[c]; else x[0][c] = xi[c];
+                        }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int p = lane + 32 * h;
+                        if (upper ? p < i : (p > i && p < sz)) {
+                            const T dpi = D[p][i];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) x[h][c] = fma(-dpi, xi[c], x[h][c]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c];
+            }
+            __syncthreads();
             for (int e = threadIdx.x; e < kTB * r; e += kThreads) {
                 const int rr = e % kTB, cc = e / kTB;
-                X[rr][cc] = (rr < sz) ? B[kb + rr + (long)cc * lb] : T(0);
+                if (rr < sz) B[kb + rr + (long)cc * lb] = X[rr][cc];
             }
-            __syncthreads();
-            // substitution: one thread per right-hand side
-            if (threadIdx.x < r) {
-                const int j = threadIdx.x;
-                if (!upper) {
-                    for (int i = 0; i < sz; ++i) {
-                        T v = X[i][j];
-                        for (int p = 0; p < i; ++p) v -= D[i][p] * X[p][j];
-                        X[i][j] = (diag == 'U') ? v : v / D[i][i];
-                    }
+            // ---- rank-sz update of the rows still to solve, 64 rows at a time; the
+            // panel chunks alternate between Pn and D (free after the substitution)
+            // thread: rows 4 rg .. 4 rg + 3 of the chunk, right-hand sides 4 cg .. 4 cg + 3
+            const int rg = threadIdx.x & 15, cg = threadIdx.x >> 4;
+            for (int c0 = u0, ci = 0; c0 < u1; c0 += kTB, ++ci) {
+                const int rows = min(kTB, u1 - c0);
+                T(*P)[kPP] = (ci & 1) ? Pd : Pn;
+                if (c0 + kTB < u1) {
+                    load_panel((ci & 1) ? Pn : Pd, A, la, trans, c0 + kTB, min(kTB, u1 - c0 - kTB), kb, sz);
+                    cp_async_wait<1>();
                 } else {
-                    for (int i = sz - 1; i >= 0; --i) {
-                        T v = X[i][j];
-                        for (int p = i + 1; p < sz; ++p) v -= D[i][p] * X[p][j];
-                        X[i][j] = (diag == 'U') ? v : v / D[i][i];
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                if (4 * cg < r) {
+                    // the B values this thread updates, fetched before the K loop
+                    T bv[4][4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int col = 4 * cg + j, row = 4 * rg + i;
+                            bv[i][j] = (col < r && row < rows) ? B[c0 + row + (long)col * lb] : T(0);
+                        }
+                    T acc[4][4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+                    for (int p = 0; p < sz; ++p) {
+                        T av[4], xv[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) av[i] = P[p][4 * rg + i];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) xv[j] = X[p][4 * cg + j];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], xv[j], acc[i][j]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (4 * cg + j >= r) break;
+                        T* bp = B + c0 + (long)(4 * cg + j) * lb;
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            if (4 * rg + i < rows) bp[4 * rg + i] = bv[i][j] - acc[i][j];
                     }
                 }
-            }
-            __syncthreads();
-            for (int e = threadIdx.x; e < sz * r; e += kThreads) {
-                const int rr = e % sz, cc = e / sz;
-                B[kb + rr + (long)cc * lb] = X[rr][cc];
-            }
-            // rank-sz update of the rows still to solve
-            const int u0 = upper ? 0 : kb + sz, u1 = upper ? kb : n;
-            for (int row = u0 + threadIdx.x; row < u1; row += kThreads) {
-                T acc[kMaxRhs];
-#pragma unroll
-                for (int j = 0; j < kMaxRhs; ++j) acc[j] = T(0);
-                for (int p = 0; p < sz; ++p) {
-                    const T l = tri_el(A, la, uplo, trans, diag, row, kb + p);
-#pragma unroll
-                    for (int j = 0; j < kMaxRhs; ++j)
-                        if (j < r) acc[j] = fma(l, X[p][j], acc[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < kMaxRhs; ++j)
-                    if (j < r) B[row + (long)j * lb] -= acc[j];
+                __syncthreads();
             }
             __syncthreads();
         }
@@ -419,7 +533,7 @@ cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, in
                                 char diag, const void* alpha, const void* const* a, const int* lda, void* const* b,
                                 const int* ldb, int grid, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
-    const int sm = (kTB * (kTB + 1) + kTB * (kMaxRhs + 1)) * (dtype == BATCH_F64 ? 8 : 4);
+    const int sm = (3 * kTB * (kTB + 4) + kTB) * (dtype == BATCH_F64 ? 8 : 4);
     cudaError_t e = dtype == BATCH_F64
                         ? cudaFuncSetAttribute(trsm_batched_kernel<double>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, sm)

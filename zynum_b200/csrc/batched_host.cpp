@@ -443,7 +443,7 @@ int zynum_blas_gpu_trsm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
     b->count = count;
     b->m.assign(m, m + count);
     b->n.assign(n, n + count);
-    b->grid = sm_count();
+    b->grid = 2 * sm_count();  // two solver CTAs per SM (registers and shared memory allow it)
     std::vector<int> dims;
     std::vector<double> cost;
     for (int q = 0; q < count; ++q) {

@@ -1430,7 +1430,18 @@ static bool use_cta_pair(int m) {
     return enabled && m >= 256;
 }
 
-bool ozaki_preferred(int m, int n, int k) { return (long)m * n >= 512L * 512 && k >= 256; }
+// Automatic method choice: Ozaki when its modelled time (16 INT8 products at
+// ~3 POPS, ~32 B per operand element and ~40 B per C element of statistics,
+// residue and reconstruction traffic at ~2.5 TB/s, ~60 us of launches) is
+// below 0.8 x native FP64 at ~30 TFLOP/s; K beyond one CRT segment falls back
+// to the slice scheme, which needs larger products still.
+bool ozaki_preferred(int m, int n, int k) {
+    const double mnk2 = 2.0 * m * n * (double)k;
+    const double native_s = mnk2 / 30e12;
+    const double ozaki_s = 16.0 * mnk2 / 3.0e15 + (32.0 * ((double)m * k + (double)k * n) + 40.0 * (double)m * n) / 2.5e12 +
+                           60e-6;
+    return k <= kCrtMaxK ? ozaki_s < 0.8 * native_s : mnk2 >= 2e12;
+}
 
 int ozaki_auto_slices(float spread_a, float spread_b) {
     // Truncating a row of A after s 7-bit digits leaves |dA_ik| < 2^(e_i - 7s)
