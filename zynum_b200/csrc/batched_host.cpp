@@ -394,7 +394,7 @@ int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
     b->m.assign(m, m + count);
     b->n.assign(n, n + count);
     b->k.assign(k, k + count);
-    b->grid = sm_count();
+    b->grid = 2 * sm_count();  // two tile CTAs per SM
     std::vector<int> dims;
     for (int q = 0; q < count; ++q) {
         dims.push_back(m[q]);
