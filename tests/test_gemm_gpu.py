@@ -148,6 +148,19 @@ def test_sgemm_operand_relayout_path(blas, oracle, ta, tb):
               (4100 if tb == "N" else 1100) + 2, 1025, 1.0, 0.0)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+@pytest.mark.parametrize("shape", [(5000, 64, 64), (2049, 1, 1), (3001, 37, 50), (2300, 64, 9)],
+                         ids=lambda s: "x".join(map(str, s)))
+def test_skinny_route(blas, oracle, dtype, ta, tb, shape):
+    """n <= 64, k <= 64, m >= 2048: op(B) staged once per CTA, op(A) streamed in 128-row blocks;
+    ragged m / n / k, padded leading dimensions, alpha and beta."""
+    m, n, k = shape
+    lda = (m if ta == "N" else k) + 3
+    ldb = (k if tb == "N" else n) + 1
+    _run_case(blas, oracle, dtype, ta, tb, m, n, k, lda, ldb, m + 2, -1.25, 0.5)
+
+
 def test_skinny_tile_path(blas, oracle):
     """Tall-skinny N <= 64 runs the 128 x 64 tile."""
     _run_case(blas, oracle, np.float64, "N", "N", 4096, 64, 64, 4096, 64, 4096, 1.0, 1.0)

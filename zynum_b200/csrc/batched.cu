@@ -495,7 +495,7 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
 #define ZB_DB(AKV, BKV)                                                                                         \
     if (ak == AKV && bk == BKV) {                                                                               \
         auto kern = dgemm_batched_kernel<AKV, BKV>;                                                             \
-        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess) \
+        if ((e = ensure_dynamic_smem(kern, (int)sm)) != cudaSuccess) \
             return e;                                                                                           \
         prof_begin(st);                                                                                         \
         kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
@@ -515,7 +515,7 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
 #define ZB_SB(AMV, BMV)                                                                                         \
     if (am == AMV && bm == BMV) {                                                                               \
         auto kern = sgemm_batched_kernel<AMV, BMV>;                                                             \
-        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess) \
+        if ((e = ensure_dynamic_smem(kern, (int)sm)) != cudaSuccess) \
             return e;                                                                                           \
         prof_begin(st);                                                                                         \
         kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
@@ -535,10 +535,8 @@ cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, in
     if (count == 0) return cudaSuccess;
     const int sm = (3 * kTB * (kTB + 4) + kTB) * (dtype == BATCH_F64 ? 8 : 4);
     cudaError_t e = dtype == BATCH_F64
-                        ? cudaFuncSetAttribute(trsm_batched_kernel<double>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm)
-                        : cudaFuncSetAttribute(trsm_batched_kernel<float>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+                        ? ensure_dynamic_smem(trsm_batched_kernel<double>, sm)
+                        : ensure_dynamic_smem(trsm_batched_kernel<float>, sm);
     if (e != cudaSuccess) return e;
     prof_begin(st);
     if (dtype == BATCH_F64)

@@ -246,7 +246,7 @@ cudaError_t launch_f32(const GemmArgsF32& g, int splits, int k_chunk, float* W, 
     constexpr size_t SMEM =
         (size_t)Cfg<BN>::STAGES * Cfg<BN>::BK * (pitch(kBM) + pitch(BN)) * sizeof(float);
     auto kern = sgemm_ffma_kernel<AM, BM_, VEC, PARTIAL, BN>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    cudaError_t e = ensure_dynamic_smem(kern, (int)SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + kBM - 1) / kBM, (g.n + BN - 1) / BN, splits);
     prof_begin(st);
@@ -347,6 +347,7 @@ size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count) {
 }
 
 cudaError_t sgemm_native(const GemmArgsF32& g_in, const GemmPlan& plan, float* workspace, cudaStream_t st) {
+    if (skinny_gemm_applies(g_in.m, g_in.n, g_in.k, g_in.tri)) return sgemm_skinny(g_in, st);
     GemmArgsF32 g = g_in;
     const Relayout r = relayout_plan(g.transa, g.transb, g.m, g.n, g.k, plan);
     if ((r.a || r.b || r.splitk) && !workspace) return cudaErrorInvalidValue;

@@ -220,7 +220,7 @@ cudaError_t launch_one(const GemmArgsF64& g, int splits, int k_chunk, double* W,
     constexpr int B_ROWS = BK_ ? BN : kBK, B_COLS = BK_ ? kBK : BN;
     constexpr size_t SMEM = (size_t)STAGES * (A_ROWS * (A_COLS + 4) + B_ROWS * (B_COLS + 4)) * sizeof(double);
     auto kern = dgemm_dmma_kernel<BM, BN, WM, WN, STAGES, AK, BK_, VEC, PARTIAL>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    cudaError_t e = ensure_dynamic_smem(kern, (int)SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, splits);
     prof_begin(st);
@@ -248,6 +248,7 @@ cudaError_t dispatch_layout(const GemmArgsF64& g, int vec, int splits, int k_chu
 // Entry used by the planner: `tile` selects the block shape, `splits` > 1
 // requires a workspace of splits * m * n doubles.
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st) {
+    if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) return dgemm_skinny(g, st);
     const bool aligned = ((reinterpret_cast<uintptr_t>(g.a) | reinterpret_cast<uintptr_t>(g.b)) % 16 == 0) &&
                          (g.lda % 2 == 0) && (g.ldb % 2 == 0);
     const int vec = aligned ? 2 : 1;

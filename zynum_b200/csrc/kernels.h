@@ -50,6 +50,11 @@ cudaError_t sgemm_native(const GemmArgsF32& g, const GemmPlan& plan, float* work
 // products, an MN-contiguous copy of each K-contiguous operand.  The bound
 // covers every FP32 product of shape up to m x n x k and any transposes.
 size_t sgemm_native_workspace_bytes(char transa, char transb, int m, int n, int k, const GemmPlan& plan);
+// Tall-skinny route (n <= 64, k <= 64, m >= 2048, no triangle mode): op(B)
+// staged once per persistent CTA, op(A) streamed in 128-row blocks.
+bool skinny_gemm_applies(int m, int n, int k, int tri);
+cudaError_t dgemm_skinny(const GemmArgsF64& g, cudaStream_t st);
+cudaError_t sgemm_skinny(const GemmArgsF32& g, cudaStream_t st);
 size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count);
 
 // C = beta * C on the m x n window (beta == 0 writes exact zeros, clearing NaNs),
@@ -68,6 +73,14 @@ void prof_begin(cudaStream_t st);
 // Every kernel launch of the library is counted (reported by
 // zynum_blas_gpu_launch_count) so a caller can see the GPU work it caused.
 void count_launch();
+// cudaFuncSetAttribute(func, MaxDynamicSharedMemorySize, bytes) once per
+// function, device and size (the attribute persists; repeating it per launch
+// costs a driver call on every small GEMM).
+cudaError_t ensure_dynamic_smem(const void* func, int bytes);
+template <typename F>
+cudaError_t ensure_dynamic_smem(F* func, int bytes) {
+    return ensure_dynamic_smem(reinterpret_cast<const void*>(func), bytes);
+}
 void prof_end(cudaStream_t st);
 
 // Fortran GEMM argument check (fortran.zig:88-102 gemmError): 0 or the index

@@ -1389,7 +1389,7 @@ int sm_count_cached() {
 template <int KIND, int EPI>
 cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
     auto kern = umma_slice_gemm<KIND, EPI>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    cudaError_t e = ensure_dynamic_smem(kern, (int)kSmemBytes);
     if (e != cudaSuccess) return e;
     const int grid = P.num_tiles < sm_count_cached() ? P.num_tiles : sm_count_cached();
     prof_begin(st);
@@ -1402,7 +1402,7 @@ cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const Umma
 template <int KIND, int EPI>
 cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
     auto kern = umma_slice_gemm_2cta<KIND, EPI>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes2);
+    cudaError_t e = ensure_dynamic_smem(kern, (int)kSmemBytes2);
     if (e != cudaSuccess) return e;
     const int pairs = std::min(P.num_tiles, sm_count_cached() / 2);
     prof_begin(st);

@@ -4,6 +4,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#include <mutex>
+#include <tuple>
+#include <set>
 #include <atomic>
 
 #include "kernels.h"
@@ -205,6 +208,20 @@ namespace {
 std::atomic<long long> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+cudaError_t ensure_dynamic_smem(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::set<std::tuple<int, const void*, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const auto key = std::make_tuple(dev, func, bytes);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count(key)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.insert(key);
+    return e;
+}
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 int profile_control(int enable) {

@@ -151,7 +151,7 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     T* inv = static_cast<T*>(planes);
     T* W = inv + (long)nblk * kNB * kNB;
     const int tri_smem = 2 * kNB * (kNB + 1) * (int)sizeof(T);
-    if ((e = cudaFuncSetAttribute(tri_inv_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem)) !=
+    if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) !=
         cudaSuccess)
         return e;
     tri_inv_blocks<T><<<nblk, kNB, tri_smem, st>>>(t.a, t.lda, t.uplo, t.trans, t.diag, na, inv);
