@@ -569,6 +569,63 @@ def suite_sweep(args):
     return 0
 
 
+def suite_vector(args):
+    """Vector-edge GEMM (n == 1 / m == 1, the matrix-vector kernels): HBM GB/s of the
+    matrix read against the measured copy bandwidth, every transpose pair, a long-K
+    case that takes the K-split partials, a short-K tall case; torch.mv (cuBLAS GEMV)
+    on the same NN data as a library reference.  Every matrix is larger than L2."""
+    import torch
+    from zynum_b200 import blas
+    stream = torch.cuda.current_stream()
+    peak = _peaks()["hbm_gbs"]
+    rows = []
+    cases = [(16384, 1, 16384), (1, 16384, 16384), (2048, 1, 262144), (4194304, 1, 64), (1, 4194304, 64)]
+    for dt, tdt, fn in (("f64", torch.float64, blas.dgemm_device), ("f32", torch.float32, blas.sgemm_device)):
+        esz = 8 if dt == "f64" else 4
+        for (m, n, k) in cases:
+            rm, rk = (m, k) if n == 1 else (n, k)          # the matrix is rm x rk or rk x rm
+            g = torch.Generator(device="cuda").manual_seed(rm + rk)
+            M = torch.rand((rm * rk,), generator=g, device="cuda", dtype=tdt) * 2 - 1
+            x = torch.rand((k,), generator=g, device="cuda", dtype=tdt) * 2 - 1
+            y = torch.zeros((max(m, n),), device="cuda", dtype=tdt)
+            for t in ("N", "T"):
+                if n == 1:      # op(A) = A (m x k, ld m) or A^T (A k x m, ld k); x = B (k x 1)
+                    lda = m if t == "N" else k
+                    f = lambda: fn(t, "N", m, 1, k, 1.0, M, lda, x, k, 0.0, y, m)  # noqa: E731
+                else:           # op(B) = B (k x n, ld k) or B^T (B n x k, ld n); x = A (1 x k, ld 1)
+                    ldb = k if t == "N" else n
+                    f = lambda: fn("N", t, 1, n, k, 1.0, x, 1, M, ldb, 0.0, y, 1)  # noqa: E731
+                ms = time_device(torch, f, max(5, args.steps), max(3, args.warmup), stream)
+                byts = esz * (rm * rk + k + max(m, n))
+                gbs = byts / (ms * 1e-3) / 1e9
+                rows.append({"dtype": dt, "m": m, "n": n, "k": k, "trans": t, "ms": ms, "gbs": gbs,
+                             "frac_of_measured_hbm": gbs / peak})
+            if n == 1:  # cuBLAS GEMV through torch on the NN layout (row-major view of A^T)
+                Mv = M.view(k, m).t()
+                f = lambda: torch.mv(Mv, x, out=y)  # noqa: E731
+                ms = time_device(torch, f, max(5, args.steps), max(3, args.warmup), stream)
+                gbs = esz * (rm * rk + k + m) / (ms * 1e-3) / 1e9
+                rows.append({"dtype": dt, "m": m, "n": 1, "k": k, "trans": "N", "impl": "torch.mv", "ms": ms,
+                             "gbs": gbs, "frac_of_measured_hbm": gbs / peak})
+            del M, x, y
+        # narrow n / narrow m (2..16 vectors): one matrix read serves every vector
+        for nv in (2, 4, 8, 16):
+            for side in ("n", "m"):
+                m, n, k = (16384, nv, 16384) if side == "n" else (nv, 16384, 16384)
+                g = torch.Generator(device="cuda").manual_seed(nv)
+                A = torch.rand((m * k,), generator=g, device="cuda", dtype=tdt) * 2 - 1
+                B = torch.rand((k * n,), generator=g, device="cuda", dtype=tdt) * 2 - 1
+                C = torch.zeros((m * n,), device="cuda", dtype=tdt)
+                f = lambda: fn("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+                ms = time_device(torch, f, max(5, args.steps), max(3, args.warmup), stream)
+                gbs = esz * (m * k + k * n + m * n) / (ms * 1e-3) / 1e9
+                rows.append({"dtype": dt, "m": m, "n": n, "k": k, "trans": "NN", "ms": ms, "gbs": gbs,
+                             "frac_of_measured_hbm": gbs / peak, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12})
+                del A, B, C
+    print(json.dumps({"suite": "vector", "hbm_peak_gbs": peak, "rows": rows}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -581,7 +638,7 @@ def main(argv=None):
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--suite", choices=["headline", "precision", "sweep"], default="headline",
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector"], default="headline",
                     help="precision / sweep: secondary measurement suites (one JSON line each)")
     args = ap.parse_args(argv)
 
@@ -603,6 +660,8 @@ def main(argv=None):
             return suite_precision(args)
         if args.suite == "sweep":
             return suite_sweep(args)
+        if args.suite == "vector":
+            return suite_vector(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -208,3 +208,71 @@ def test_injected_sync_error_leaves_c_unchanged(blas):
     blas.inject_fault(2, 700)  # report cudaErrorIllegalAddress from the host-side sync (no GPU fault)
     blas.dgemm("N", "N", 32, 32, 32, 1.0, a, 32, a, 32, 0.5, c, 32)
     assert np.array_equal(c, c0)
+
+
+GEMV_SHAPES = [
+    # (m, n, k): n == 1 and m == 1 with ragged output counts; long K takes the
+    # K-split partials + ordered reduction, short K a single pass
+    (5000, 1, 3000),
+    (1, 4099, 2500),
+    (70001, 1, 37),
+    (1, 33333, 19),
+    (300, 1, 100000),
+    (1, 1, 5000),
+    (129, 1, 1),
+    (3001, 1, 64),
+    (1, 2999, 9),
+]
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+@pytest.mark.parametrize("shape", GEMV_SHAPES, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("pad", [0, 1], ids=["vec", "odd_ld"])
+def test_gemv_route(blas, oracle, dtype, ta, tb, shape, pad):
+    """n == 1 / m == 1 run the matrix-vector kernels (gemm.zig:189-224, :228-240 route these
+    to GEMV): every transpose pair, so both the outputs-contiguous and the dot-product kernel
+    run with unit and strided vectors; pad = 0 keeps leading dimensions 16-byte multiples
+    (vector loads), pad = 1 makes them odd (scalar loads)."""
+    m, n, k = shape
+    lda = (m if ta == "N" else k)
+    ldb = (k if tb == "N" else n)
+    lda = (lda + 3) // 4 * 4 + pad
+    ldb = (ldb + 3) // 4 * 4 + pad
+    _run_case(blas, oracle, dtype, ta, tb, m, n, k, lda, ldb, m + 2, -1.25, 0.5)
+    _run_case(blas, oracle, dtype, ta, tb, m, n, k, lda, ldb, m, 0.75, 0.0, salt=3)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+def test_gemv_beta_zero_clears_nan(blas, dtype):
+    """beta == 0 overwrites C without reading it (NaN in C does not propagate), on both
+    matrix-vector kernels and through the K-split reduction."""
+    rng = np.random.default_rng(11)
+    for m, n, k in [(4000, 1, 5000), (1, 4000, 5000), (4000, 1, 64)]:
+        a = np.asfortranarray(rng.uniform(-1, 1, (m, k)).astype(dtype))
+        b = np.asfortranarray(rng.uniform(-1, 1, (k, n)).astype(dtype))
+        c = np.full((m, n), np.nan, dtype=dtype, order="F")
+        fn = blas.dgemm if dtype == np.float64 else blas.sgemm
+        fn("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m)
+        ref = a.astype(np.float64) @ b.astype(np.float64)
+        assert np.all(np.isfinite(c))
+        tol = 1e-12 if dtype == np.float64 else 2e-4
+        assert np.max(np.abs(c - ref)) <= tol * max(1.0, float(np.max(np.abs(ref))))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+@pytest.mark.parametrize("shape", [(3000, 7, 5000), (5000, 16, 3000), (7, 3001, 4000), (16, 4100, 1030),
+                                   (513, 2, 2000), (2, 777, 300), (4099, 13, 700), (3, 1200, 33)],
+                         ids=lambda s: "x".join(map(str, s)))
+def test_gemm_narrow_route(blas, oracle, dtype, ta, tb, shape):
+    """n <= 16 (m <= 16) against a wide other side: FP64 128 x 16 (16 x 128) DMMA tiles, FP32
+    the narrow FFMA kernel (2, 4, 8 or 16 vector slots); split K over long reductions, ragged
+    tiles, odd leading dimensions (element copies) and 16-byte-multiple ones (vector copies)."""
+    m, n, k = shape
+    for pad, alpha, beta in ((1, -1.25, 0.5), (0, 1.0, 0.0)):
+        lda = (m if ta == "N" else k) + pad
+        ldb = (k if tb == "N" else n) + pad
+        if pad == 0:
+            lda, ldb = (lda + 3) // 4 * 4, (ldb + 3) // 4 * 4
+        _run_case(blas, oracle, dtype, ta, tb, m, n, k, lda, ldb, m + 1, alpha, beta)

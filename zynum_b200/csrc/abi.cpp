@@ -216,14 +216,16 @@ size_t real_scratch_bytes(int m, int n, int k, float*) {
 
 // Scratch that covers every GEMM of shape up to m x n x k (TRSM's recursive
 // updates): split-K partials never exceed sm_count x 128 x 128 elements
-// (splits <= sm_count / tiles and tiles >= m n / 128^2), FP32 products may add
+// (splits <= sm_count / tiles and tiles >= m n / 128^2) and matrix-vector
+// partials kGemvMaxPartials, FP32 products may add
 // an MN-contiguous copy of each operand, and the Ozaki planes grow with every
 // dimension.
 template <typename T>
 size_t real_scratch_bound(int m, int n, int k) {
     Context& cx = context();
+    const long partials = std::max<long>((long)cx.sm_count * 128 * 128, kGemvMaxPartials);
     const size_t splitk = sizeof(T) == 4 ? sgemm_native_workspace_bound(m, n, k, cx.sm_count)
-                                         : (size_t)cx.sm_count * 128 * 128 * sizeof(T) + 4096;
+                                         : (size_t)partials * sizeof(T) + 4096;
     return std::max(splitk, real_scratch_bytes(m, n, k, (T*)nullptr));
 }
 

@@ -324,6 +324,8 @@ struct Relayout {
 Relayout relayout_plan(char transa, char transb, int m, int n, int k, const GemmPlan& plan) {
     Relayout r;
     r.splitk = align_elems(splitk_workspace_elems(m, n, plan.splits));
+    // the matrix-vector and narrow kernels read either layout directly
+    if (plan.tile == TILE_GEMV || plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M) return r;
     const size_t a_elems = align_elems((size_t)pad4(m) * (size_t)k);
     const size_t b_elems = align_elems((size_t)pad4(n) * (size_t)k);
     r.a = transa != 'N' && n >= kRelayoutMinOther && a_elems * sizeof(float) <= kRelayoutMaxBytes;
@@ -341,13 +343,19 @@ size_t sgemm_native_workspace_bytes(char transa, char transb, int m, int n, int 
 }
 
 size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count) {
-    // split-K partials never exceed sm_count x 128 x 128; both copies at most
-    return (align_elems((size_t)sm_count * 128 * 128) + align_elems((size_t)pad4(m) * k) +
+    // split-K partials never exceed sm_count x 128 x 128 (GEMV partials
+    // kGemvMaxPartials); both copies at most
+    return (align_elems((size_t)std::max<long>((long)sm_count * 128 * 128, kGemvMaxPartials)) +
+            align_elems((size_t)pad4(m) * k) +
             align_elems((size_t)pad4(n) * k)) * sizeof(float);
 }
 
 cudaError_t sgemm_native(const GemmArgsF32& g_in, const GemmPlan& plan, float* workspace, cudaStream_t st) {
+    if (plan.tile == TILE_GEMV && gemv_applies(g_in.m, g_in.n, g_in.k, g_in.tri))
+        return sgemv_route(g_in, plan.splits, workspace, st);
     if (skinny_gemm_applies(g_in.m, g_in.n, g_in.k, g_in.tri)) return sgemm_skinny(g_in, st);
+    if ((plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M) && narrow_gemm_applies(g_in.m, g_in.n, g_in.tri))
+        return sgemm_narrow(g_in, plan.splits, workspace, st);
     GemmArgsF32 g = g_in;
     const Relayout r = relayout_plan(g.transa, g.transb, g.m, g.n, g.k, plan);
     if ((r.a || r.b || r.splitk) && !workspace) return cudaErrorInvalidValue;

@@ -35,10 +35,11 @@ ZB_DEVICE void load_tile(double* smem, const double* __restrict__ base, long ld,
                          int c_lim) {
     constexpr int CHUNKS_PER_ROW = COLS / VEC;
     constexpr int CHUNKS = ROWS * CHUNKS_PER_ROW;
-    static_assert(CHUNKS % NTHREADS == 0, "tile copy must divide evenly over the block");
+    static_assert(CHUNKS % NTHREADS == 0 || CHUNKS < NTHREADS, "tile copy must divide evenly over the block");
 #pragma unroll
-    for (int it = 0; it < CHUNKS / NTHREADS; ++it) {
+    for (int it = 0; it < (CHUNKS + NTHREADS - 1) / NTHREADS; ++it) {
         int q = it * NTHREADS + threadIdx.x;
+        if (CHUNKS < NTHREADS && q >= CHUNKS) break;  // narrow tiles: fewer chunks than threads
         int r = q / CHUNKS_PER_ROW;
         int c = (q % CHUNKS_PER_ROW) * VEC;
         int gr = r0 + r, gc = c0 + c;
@@ -243,11 +244,27 @@ cudaError_t dispatch_layout(const GemmArgsF64& g, int vec, int splits, int k_chu
     return cudaErrorInvalidValue;
 }
 
+template <int BM, int BN, int WM, int WN, int STAGES>
+cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chunk, double* workspace,
+                      cudaStream_t st) {
+    if (used_splits == 1) return dispatch_layout<BM, BN, WM, WN, STAGES, false>(g, vec, 1, k_chunk, nullptr, st);
+    if (!workspace) return cudaErrorInvalidValue;
+    cudaError_t e = dispatch_layout<BM, BN, WM, WN, STAGES, true>(g, vec, used_splits, k_chunk, workspace, st);
+    if (e != cudaSuccess) return e;
+    long total = (long)g.m * g.n;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    dgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used_splits, workspace, g.alpha, g.beta, g.c, g.ldc, g.tri);
+    count_launch();
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 // Entry used by the planner: `tile` selects the block shape, `splits` > 1
 // requires a workspace of splits * m * n doubles.
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st) {
+    if (plan.tile == TILE_GEMV && gemv_applies(g.m, g.n, g.k, g.tri)) return dgemv_route(g, plan.splits, workspace, st);
     if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) return dgemm_skinny(g, st);
     const bool aligned = ((reinterpret_cast<uintptr_t>(g.a) | reinterpret_cast<uintptr_t>(g.b)) % 16 == 0) &&
                          (g.lda % 2 == 0) && (g.ldb % 2 == 0);
@@ -255,26 +272,17 @@ cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* wor
     const int splits = plan.splits < 1 ? 1 : plan.splits;
     int k_chunk = (g.k + splits - 1) / splits;
     k_chunk = (k_chunk + kBK - 1) / kBK * kBK;
-    const int used_splits = (g.k + k_chunk - 1) / k_chunk;
-    cudaError_t e;
-    if (used_splits > 1) {
-        if (!workspace) return cudaErrorInvalidValue;
-        if (plan.tile == TILE_128x64)
-            e = dispatch_layout<128, 64, 64, 32, 4, true>(g, vec, used_splits, k_chunk, workspace, st);
-        else
-            e = dispatch_layout<128, 128, 64, 32, 4, true>(g, vec, used_splits, k_chunk, workspace, st);
-        if (e != cudaSuccess) return e;
-        long total = (long)g.m * g.n;
-        int blocks = (int)((total + 255) / 256);
-        if (blocks > 148 * 16) blocks = 148 * 16;
-        dgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used_splits, workspace, g.alpha, g.beta, g.c, g.ldc,
-                                                    g.tri);
-        count_launch();
-        return cudaGetLastError();
+    const int used = (g.k + k_chunk - 1) / k_chunk;
+    switch (plan.tile) {
+        case TILE_128x64:
+            return run_tiles<128, 64, 64, 32, 4>(g, vec, used, k_chunk, workspace, st);
+        case TILE_NARROW_N:  // n <= 16: 128 x 16 tiles, warps 4 x 2 of 32 x 8
+            return run_tiles<128, 16, 32, 8, 4>(g, vec, used, k_chunk, workspace, st);
+        case TILE_NARROW_M:  // m <= 16: 16 x 128 tiles, warps 1 x 8 of 16 x 16
+            return run_tiles<16, 128, 16, 16, 4>(g, vec, used, k_chunk, workspace, st);
+        default:
+            return run_tiles<128, 128, 64, 32, 4>(g, vec, used, k_chunk, workspace, st);
     }
-    if (plan.tile == TILE_128x64)
-        return dispatch_layout<128, 64, 64, 32, 4, false>(g, vec, 1, k_chunk, nullptr, st);
-    return dispatch_layout<128, 128, 64, 32, 4, false>(g, vec, 1, k_chunk, nullptr, st);
 }
 
 }  // namespace zb

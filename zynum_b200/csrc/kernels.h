@@ -30,7 +30,12 @@ struct GemmArgs {
 using GemmArgsF64 = GemmArgs<double>;
 using GemmArgsF32 = GemmArgs<float>;
 
-enum TileShape : int { TILE_128x128 = 0, TILE_128x64 = 1 };
+// TILE_GEMV: n == 1 or m == 1, served by the matrix-vector kernels (splits =
+// K splits of the GEMV partials, workspace splits * m * n elements as for split-K).
+// TILE_NARROW_N / TILE_NARROW_M: n <= 16 / m <= 16 (the other side >= 512):
+// FP64 128 x 16 / 16 x 128 DMMA tiles, FP32 the narrow FFMA kernel (HBM-bound;
+// a 64- or 128-wide tile would be compute-bound on padding).
+enum TileShape : int { TILE_128x128 = 0, TILE_128x64 = 1, TILE_GEMV = 2, TILE_NARROW_N = 3, TILE_NARROW_M = 4 };
 
 // What the planner decided for one native GEMM call.
 struct GemmPlan {
@@ -56,6 +61,20 @@ bool skinny_gemm_applies(int m, int n, int k, int tri);
 cudaError_t dgemm_skinny(const GemmArgsF64& g, cudaStream_t st);
 cudaError_t sgemm_skinny(const GemmArgsF32& g, cudaStream_t st);
 size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count);
+// Vector-edge route (n == 1 or m == 1, no triangle mode): HBM-bound
+// matrix-vector kernels; `splits` > 1 needs splits * max(m, n) elements of workspace.
+bool gemv_applies(int m, int n, int k, int tri);
+constexpr long kGemvSplitTarget = 1L << 20;   // outputs x K splits the planner aims for
+constexpr long kGemvMaxPartials = 2L << 20;   // bound on splits * outputs (workspace elements)
+int gemv_split_count(int rows, int k);
+cudaError_t dgemv_route(const GemmArgsF64& g, int splits, double* ws, cudaStream_t st);
+cudaError_t sgemv_route(const GemmArgsF32& g, int splits, float* ws, cudaStream_t st);
+// Narrow route (n <= 16 with m >= 512, or m <= 16 with n >= 512; n, m > 1):
+// K split count for 128-output tiles, and the FP32 kernel (splits * m * n
+// elements of workspace when splits > 1).
+bool narrow_gemm_applies(int m, int n, int tri);
+int narrow_split_count(int m, int n, int k, int sm_count);
+cudaError_t sgemm_narrow(const GemmArgsF32& g, int splits, float* workspace, cudaStream_t st);
 
 // C = beta * C on the m x n window (beta == 0 writes exact zeros, clearing NaNs),
 // the reference's k == 0 / alpha == 0 quick return (gemm.zig:1407-1414).

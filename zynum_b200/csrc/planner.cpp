@@ -13,6 +13,20 @@ namespace zb {
 
 GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count) {
     GemmPlan p;
+    // n == 1 or m == 1: matrix-vector kernels, K split only while the outputs
+    // alone leave SMs idle.
+    if (n == 1 || m == 1) {
+        p.tile = TILE_GEMV;
+        p.splits = gemv_split_count(n == 1 ? m : n, k);
+        return p;
+    }
+    // At most 16 columns (rows) of C: 128 x 16 (16 x 128) FP64 tiles or the
+    // FP32 narrow kernel, K split while the output tiles leave SMs idle.
+    if ((n <= 16 && m >= 512) || (m <= 16 && n >= 512)) {
+        p.tile = n <= 16 ? TILE_NARROW_N : TILE_NARROW_M;
+        p.splits = narrow_split_count(m, n, k, sm_count);
+        return p;
+    }
     // Narrow-N, tall-M shapes (e.g. 131072 x 64 x 64) are HBM-bound: a 64-wide
     // tile avoids computing (and staging) a half-empty 128-wide tile.
     if (elem_bytes == 8 && n <= 64 && m >= 1024) p.tile = TILE_128x64;
