@@ -77,6 +77,27 @@ ZYNUM_BLAS_GPU_API void ssyrk_(const char *uplo, const char *trans, const zynum_
 ZYNUM_BLAS_GPU_API void dsyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
                                const double *alpha, const double *a, const zynum_blas_int *lda, const double *beta,
                                double *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:777-783 ssymm_ / dsymm_ (C := alpha A B + beta C or alpha B A + beta C, A symmetric) */
+ZYNUM_BLAS_GPU_API void ssymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const float *alpha, const float *a, const zynum_blas_int *lda, const float *b,
+                               const zynum_blas_int *ldb, const float *beta, float *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void dsymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const double *alpha, const double *a, const zynum_blas_int *lda, const double *b,
+                               const zynum_blas_int *ldb, const double *beta, double *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:852-858 strmm_ / dtrmm_ (B := alpha op(A) B or alpha B op(A), A triangular) */
+ZYNUM_BLAS_GPU_API void strmm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const float *alpha, const float *a,
+                               const zynum_blas_int *lda, float *b, const zynum_blas_int *ldb);
+ZYNUM_BLAS_GPU_API void dtrmm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const double *alpha, const double *a,
+                               const zynum_blas_int *lda, double *b, const zynum_blas_int *ldb);
+/* src/blas/abi/fortran.zig:827-833 ssyr2k_ / dsyr2k_ (C := alpha (op(A) op(B)^T + op(B) op(A)^T) + beta C, one triangle) */
+ZYNUM_BLAS_GPU_API void ssyr2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const float *alpha, const float *a, const zynum_blas_int *lda, const float *b,
+                                const zynum_blas_int *ldb, const float *beta, float *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void dsyr2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const double *alpha, const double *a, const zynum_blas_int *lda, const double *b,
+                                const zynum_blas_int *ldb, const double *beta, double *c, const zynum_blas_int *ldc);
 
 /* ---------------------------------------------------------------- CBLAS ABI */
 
@@ -110,6 +131,21 @@ ZYNUM_BLAS_GPU_API void cblas_ssyrk(int layout, int uplo, int trans, int n, int 
                                     int lda, float beta, float *c, int ldc);
 ZYNUM_BLAS_GPU_API void cblas_dsyrk(int layout, int uplo, int trans, int n, int k, double alpha, const double *a,
                                     int lda, double beta, double *c, int ldc);
+/* src/blas/abi/cblas.zig:1467-1489 cblas_ssymm / cblas_dsymm */
+ZYNUM_BLAS_GPU_API void cblas_ssymm(int layout, int side, int uplo, int m, int n, float alpha, const float *a, int lda,
+                                    const float *b, int ldb, float beta, float *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_dsymm(int layout, int side, int uplo, int m, int n, double alpha, const double *a,
+                                    int lda, const double *b, int ldb, double beta, double *c, int ldc);
+/* src/blas/abi/cblas.zig:1677-1701 cblas_strmm / cblas_dtrmm */
+ZYNUM_BLAS_GPU_API void cblas_strmm(int layout, int side, int uplo, int transa, int diag, int m, int n, float alpha,
+                                    const float *a, int lda, float *b, int ldb);
+ZYNUM_BLAS_GPU_API void cblas_dtrmm(int layout, int side, int uplo, int transa, int diag, int m, int n, double alpha,
+                                    const double *a, int lda, double *b, int ldb);
+/* src/blas/abi/cblas.zig:1605-1627 cblas_ssyr2k / cblas_dsyr2k */
+ZYNUM_BLAS_GPU_API void cblas_ssyr2k(int layout, int uplo, int trans, int n, int k, float alpha, const float *a,
+                                     int lda, const float *b, int ldb, float beta, float *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_dsyr2k(int layout, int uplo, int trans, int n, int k, double alpha, const double *a,
+                                     int lda, const double *b, int ldb, double beta, double *c, int ldc);
 
 /* ------------------------------------------------------ GPU device entry points
  * Added by the GPU backend (no counterpart in the reference's ABI; the planned
@@ -163,6 +199,29 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n,
                                                    int lda, double beta, double *c, int ldc, void *stream);
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
                                                    int lda, float beta, float *c, int ldc, void *stream);
+/* SYMM on device pointers: the stored triangle of A is mirrored into a dense scratch copy, then one
+ * GEMM (following the DGEMM / SGEMM method).  Argument numbering as dsymm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsymm_device(char side, char uplo, int m, int n, double alpha, const double *a,
+                                                   int lda, const double *b, int ldb, double beta, double *c, int ldc,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssymm_device(char side, char uplo, int m, int n, float alpha, const float *a,
+                                                   int lda, const float *b, int ldb, float beta, float *c, int ldc,
+                                                   void *stream);
+/* TRMM on device pointers: dense 256 x 256 diagonal blocks + off-diagonal GEMMs on a copy of B
+ * (following the DGEMM / SGEMM method).  Argument numbering as dtrmm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrmm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   double alpha, const double *a, int lda, double *b, int ldb,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_strmm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   float alpha, const float *a, int lda, float *b, int ldb,
+                                                   void *stream);
+/* SYR2K on device pointers: two native triangle-mode GEMMs.  Argument numbering as dsyr2k_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyr2k_device(char uplo, char trans, int n, int k, double alpha,
+                                                    const double *a, int lda, const double *b, int ldb, double beta,
+                                                    double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyr2k_device(char uplo, char trans, int n, int k, float alpha, const float *a,
+                                                    int lda, const float *b, int ldb, float beta, float *c, int ldc,
+                                                    void *stream);
 
 /* Triangle-restricted GEMM ("gemmt"; no counterpart in the reference, used by
  * the TRSM adjoint): C := alpha op(A) op(B) + beta C computed and written only

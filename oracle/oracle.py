@@ -45,6 +45,12 @@ def _declare(L):
     L.oracle_strsm.argtypes = [ch, ch, ch, ch, i32, i32, f32, vp, i32, vp, i32]
     L.oracle_dsyrk.argtypes = [ch, ch, i32, i32, f64, vp, i32, f64, vp, i32]
     L.oracle_ssyrk.argtypes = [ch, ch, i32, i32, f32, vp, i32, f32, vp, i32]
+    L.oracle_dsymm.argtypes = [ch, ch, i32, i32, f64, vp, i32, vp, i32, f64, vp, i32]
+    L.oracle_ssymm.argtypes = [ch, ch, i32, i32, f32, vp, i32, vp, i32, f32, vp, i32]
+    L.oracle_dtrmm.argtypes = [ch, ch, ch, ch, i32, i32, f64, vp, i32, vp, i32]
+    L.oracle_strmm.argtypes = [ch, ch, ch, ch, i32, i32, f32, vp, i32, vp, i32]
+    L.oracle_dsyr2k.argtypes = [ch, ch, i32, i32, f64, vp, i32, vp, i32, f64, vp, i32]
+    L.oracle_ssyr2k.argtypes = [ch, ch, i32, i32, f32, vp, i32, vp, i32, f32, vp, i32]
 
 
 def _p(a: np.ndarray):
@@ -107,4 +113,25 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     L = lib()
     f = L.oracle_dsyrk if c.dtype == np.float64 else L.oracle_ssyrk
     f(_b(uplo), _b(trans), n, k, alpha, _p(a), lda, beta, _p(c), ldc)
+    return c
+
+
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    L = lib()
+    f = L.oracle_dsymm if c.dtype == np.float64 else L.oracle_ssymm
+    f(_b(side), _b(uplo), m, n, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
+    return c
+
+
+def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    L = lib()
+    f = L.oracle_dtrmm if b.dtype == np.float64 else L.oracle_strmm
+    f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha, _p(a), lda, _p(b), ldb)
+    return b
+
+
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    L = lib()
+    f = L.oracle_dsyr2k if c.dtype == np.float64 else L.oracle_ssyr2k
+    f(_b(uplo), _b(trans), n, k, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
     return c

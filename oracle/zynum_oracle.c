@@ -17,6 +17,10 @@
  *                  :400-435, triValue access.zig:54-64) and the right-side
  *                  row solve solveRightRow triangular.zig:72-88.
  *   oracle_?syrk   symmetric.zig:180-199 (runSyrkColumns).
+ *   oracle_?symm   symmetric.zig:56-70 (runSymmColumns, symValue access.zig:31-42).
+ *   oracle_?trmm   triangular.zig:202-231 (left: trmv + alpha scale per column,
+ *                  runLeftColumns :105-110; right: row products :212-229).
+ *   oracle_?syr2k  symmetric.zig:301-329 (runSyr2kColumns, real case).
  *   oracle_ddgemm  a double-double (error-free TwoProd/TwoSum, Dekker 1971 /
  *                  Knuth) accumulation of op(A)op(B); used to state the error
  *                  of every GPU result.  No counterpart in the reference.
@@ -311,6 +315,123 @@ DEFINE_REAL_TRSM(oracle_strsm, float, tri_s)
 
 DEFINE_REAL_SYRK(oracle_dsyrk, double)
 DEFINE_REAL_SYRK(oracle_ssyrk, float)
+
+/* ---------------------------------------------------------------- real SYMM */
+
+/* symmetric.zig:56-70 runSymmColumns with symValue (access.zig:31-42): the
+ * element (i, p) of the symmetric A comes from the stored uplo triangle. */
+#define DEFINE_REAL_SYMM(NAME, T)                                                                    \
+    void NAME(char side, char uplo, blas_int m, blas_int n, T alpha, const T *a, blas_int lda,      \
+              const T *b, blas_int ldb, T beta, T *c, blas_int ldc) {                                \
+        side = (char)upc(side); uplo = (char)upc(uplo);                                              \
+        if (m <= 0 || n <= 0) return;                                                                \
+        for (size_t j = 0; j < (size_t)n; ++j)                                                       \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                 \
+                T sum = 0;                                                                           \
+                if (side == 'L') {                                                                   \
+                    for (size_t p = 0; p < (size_t)m; ++p) {                                         \
+                        int st = (uplo == 'U') ? (i <= p) : (i >= p);                                \
+                        T av = st ? a[ix(lda, i, p)] : a[ix(lda, p, i)];                             \
+                        sum = sum + av * b[ix(ldb, p, j)];                                           \
+                    }                                                                                \
+                } else {                                                                             \
+                    for (size_t p = 0; p < (size_t)n; ++p) {                                         \
+                        int st = (uplo == 'U') ? (p <= j) : (p >= j);                                \
+                        T av = st ? a[ix(lda, p, j)] : a[ix(lda, j, p)];                             \
+                        sum = sum + b[ix(ldb, i, p)] * av;                                           \
+                    }                                                                                \
+                }                                                                                    \
+                size_t q = ix(ldc, i, j);                                                            \
+                c[q] = alpha * sum + ((beta == (T)0) ? (T)0 : beta * c[q]);                          \
+            }                                                                                        \
+    }
+
+DEFINE_REAL_SYMM(oracle_dsymm, double)
+DEFINE_REAL_SYMM(oracle_ssymm, float)
+
+/* ---------------------------------------------------------------- real TRMM */
+
+/* triangular.zig:202-231: left side, per column x := op(A) x (trmv) then
+ * x := alpha x when alpha != 1 (runLeftColumns :105-110, scaleDenseColumns
+ * :52-59); right side, per row b(i, :) := alpha b(i, :) op(A), columns taken
+ * in the order that leaves the inputs of later columns unchanged (:212-229). */
+#define DEFINE_REAL_TRMM(NAME, T, TRI)                                                                  \
+    void NAME(char side, char uplo, char trans, char diag, blas_int m, blas_int n, T alpha,           \
+              const T *a, blas_int lda, T *b, blas_int ldb) {                                           \
+        side = (char)upc(side); uplo = (char)upc(uplo); trans = (char)upc(trans); diag = (char)upc(diag); \
+        if (m <= 0 || n <= 0) return;                                                                   \
+        int upper = op_is_upper(uplo, trans);                                                           \
+        if (side == 'L') {                                                                              \
+            for (size_t j = 0; j < (size_t)n; ++j) {                                                    \
+                T *x = b + (size_t)ldb * j;                                                             \
+                if (upper) {                                                                            \
+                    for (size_t r = 0; r < (size_t)m; ++r) {                                            \
+                        T t = 0;                                                                        \
+                        for (size_t q = r; q < (size_t)m; ++q) t = t + TRI(uplo, diag, trans, a, lda, r, q) * x[q]; \
+                        x[r] = t;                                                                       \
+                    }                                                                                   \
+                } else {                                                                                \
+                    for (size_t r = (size_t)m; r-- > 0;) {                                              \
+                        T t = 0;                                                                        \
+                        for (size_t q = 0; q <= r; ++q) t = t + TRI(uplo, diag, trans, a, lda, r, q) * x[q]; \
+                        x[r] = t;                                                                       \
+                    }                                                                                   \
+                }                                                                                       \
+                if (alpha != (T)1)                                                                      \
+                    for (size_t r = 0; r < (size_t)m; ++r) x[r] = alpha * x[r];                         \
+            }                                                                                           \
+        } else {                                                                                        \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                    \
+                if (upper) {                                                                            \
+                    for (size_t cc = (size_t)n; cc-- > 0;) {                                            \
+                        T sum = 0;                                                                      \
+                        for (size_t p = 0; p < (size_t)n; ++p)                                          \
+                            sum = sum + b[ix(ldb, i, p)] * TRI(uplo, diag, trans, a, lda, p, cc);       \
+                        b[ix(ldb, i, cc)] = alpha * sum;                                                \
+                    }                                                                                   \
+                } else {                                                                                \
+                    for (size_t cc = 0; cc < (size_t)n; ++cc) {                                         \
+                        T sum = 0;                                                                      \
+                        for (size_t p = 0; p < (size_t)n; ++p)                                          \
+                            sum = sum + b[ix(ldb, i, p)] * TRI(uplo, diag, trans, a, lda, p, cc);       \
+                        b[ix(ldb, i, cc)] = alpha * sum;                                                \
+                    }                                                                                   \
+                }                                                                                       \
+            }                                                                                           \
+        }                                                                                               \
+    }
+
+DEFINE_REAL_TRMM(oracle_dtrmm, double, tri_d)
+DEFINE_REAL_TRMM(oracle_strmm, float, tri_s)
+
+/* --------------------------------------------------------------- real SYR2K */
+
+/* symmetric.zig:301-329 runSyr2kColumns (real case): one accumulator of
+ * a_i b_j + b_i a_j over p, then alpha sum + beta c on the uplo triangle. */
+#define DEFINE_REAL_SYR2K(NAME, T)                                                                      \
+    void NAME(char uplo, char trans, blas_int n, blas_int k, T alpha, const T *a, blas_int lda,        \
+              const T *b, blas_int ldb, T beta, T *c, blas_int ldc) {                                   \
+        uplo = (char)upc(uplo); trans = (char)upc(trans);                                               \
+        if (n <= 0) return;                                                                             \
+        for (size_t j = 0; j < (size_t)n; ++j) {                                                        \
+            size_t r0 = (uplo == 'U') ? 0 : j, r1 = (uplo == 'U') ? j + 1 : (size_t)n;                  \
+            for (size_t i = r0; i < r1; ++i) {                                                          \
+                T sum = 0;                                                                              \
+                for (size_t p = 0; p < (size_t)(k > 0 ? k : 0); ++p) {                                   \
+                    T ai = (trans == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];                        \
+                    T bi = (trans == 'N') ? b[ix(ldb, i, p)] : b[ix(ldb, p, i)];                        \
+                    T aj = (trans == 'N') ? a[ix(lda, j, p)] : a[ix(lda, p, j)];                        \
+                    T bj = (trans == 'N') ? b[ix(ldb, j, p)] : b[ix(ldb, p, j)];                        \
+                    sum = sum + (ai * bj + bi * aj);                                                    \
+                }                                                                                       \
+                size_t q = ix(ldc, i, j);                                                               \
+                c[q] = alpha * sum + ((beta == (T)0) ? (T)0 : beta * c[q]);                             \
+            }                                                                                           \
+        }                                                                                               \
+    }
+
+DEFINE_REAL_SYR2K(oracle_dsyr2k, double)
+DEFINE_REAL_SYR2K(oracle_ssyr2k, float)
 
 /* Library self-identification for the loader in the tests. */
 int oracle_version(void) { return 1; }

@@ -73,6 +73,32 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
                  "zynum_blas_gpu_ssyrk_device"):
         getattr(L, name).restype = i
+    for name in ("dsymm_", "ssymm_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("dtrmm_", "strmm_"):
+        getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("dsyr2k_", "ssyr2k_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    L.cblas_dsymm.argtypes = [i, i, i, i, i, d, P, i, P, i, d, P, i]
+    L.cblas_ssymm.argtypes = [i, i, i, i, i, f, P, i, P, i, f, P, i]
+    L.cblas_dtrmm.argtypes = [i, i, i, i, i, i, i, d, P, i, P, i]
+    L.cblas_strmm.argtypes = [i, i, i, i, i, i, i, f, P, i, P, i]
+    L.cblas_dsyr2k.argtypes = [i, i, i, i, i, d, P, i, P, i, d, P, i]
+    L.cblas_ssyr2k.argtypes = [i, i, i, i, i, f, P, i, P, i, f, P, i]
+    for name in ("cblas_dsymm", "cblas_ssymm", "cblas_dtrmm", "cblas_strmm", "cblas_dsyr2k", "cblas_ssyr2k"):
+        getattr(L, name).restype = None
+    L.zynum_blas_gpu_dsymm_device.argtypes = [ch, ch, i, i, d, P, i, P, i, d, P, i, P]
+    L.zynum_blas_gpu_ssymm_device.argtypes = [ch, ch, i, i, f, P, i, P, i, f, P, i, P]
+    L.zynum_blas_gpu_dtrmm_device.argtypes = [ch, ch, ch, ch, i, i, d, P, i, P, i, P]
+    L.zynum_blas_gpu_strmm_device.argtypes = [ch, ch, ch, ch, i, i, f, P, i, P, i, P]
+    L.zynum_blas_gpu_dsyr2k_device.argtypes = [ch, ch, i, i, d, P, i, P, i, d, P, i, P]
+    L.zynum_blas_gpu_ssyr2k_device.argtypes = [ch, ch, i, i, f, P, i, P, i, f, P, i, P]
+    for name in ("zynum_blas_gpu_dsymm_device", "zynum_blas_gpu_ssymm_device", "zynum_blas_gpu_dtrmm_device",
+                 "zynum_blas_gpu_strmm_device", "zynum_blas_gpu_dsyr2k_device", "zynum_blas_gpu_ssyr2k_device"):
+        getattr(L, name).restype = i
     L.zynum_blas_gpu_dgemmt_device.argtypes = [ch, ch, ch, i, i, d, P, i, P, i, d, P, i, P]
     L.zynum_blas_gpu_dgemmt_device.restype = i
     L.zynum_blas_gpu_dsymmetrize_device.argtypes = [ch, i, P, i, P]

@@ -123,6 +123,60 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     return c
 
 
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran dsymm_ / ssymm_ on host arrays (dtype from c; in-place on c)."""
+    L = load()
+    fn, dt = (L.dsymm_, np.float64) if c.dtype == np.float64 else (L.ssymm_, np.float32)
+    al, be = np.array([alpha], dt), np.array([beta], dt)
+    fn(_ch(side), _ch(uplo), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb), be.ctypes.data,
+       _ptr(c), _i(ldc))
+    return c
+
+
+def trmm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """Fortran dtrmm_ / strmm_ on host arrays (dtype from b; in-place on b)."""
+    L = load()
+    fn, dt = (L.dtrmm_, np.float64) if b.dtype == np.float64 else (L.strmm_, np.float32)
+    al = np.array([alpha], dt)
+    fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+       _i(ldb))
+    return b
+
+
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran dsyr2k_ / ssyr2k_ on host arrays (dtype from c; in-place on c's triangle)."""
+    L = load()
+    fn, dt = (L.dsyr2k_, np.float64) if c.dtype == np.float64 else (L.ssyr2k_, np.float32)
+    al, be = np.array([alpha], dt), np.array([beta], dt)
+    fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb), be.ctypes.data,
+       _ptr(c), _i(ldc))
+    return c
+
+
+def cblas_symm(layout, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    """cblas_dsymm / cblas_ssymm (dtype from c)."""
+    L = load()
+    fn, cast = (L.cblas_dsymm, float) if c.dtype == np.float64 else (L.cblas_ssymm, float)
+    fn(layout, side, uplo, m, n, cast(alpha), _ptr(a), lda, _ptr(b), ldb, cast(beta), _ptr(c), ldc)
+    return c
+
+
+def cblas_trmm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """cblas_dtrmm / cblas_strmm (dtype from b)."""
+    L = load()
+    fn = L.cblas_dtrmm if b.dtype == np.float64 else L.cblas_strmm
+    fn(layout, side, uplo, transa, diag, m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb)
+    return b
+
+
+def cblas_syr2k(layout, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """cblas_dsyr2k / cblas_ssyr2k (dtype from c)."""
+    L = load()
+    fn = L.cblas_dsyr2k if c.dtype == np.float64 else L.cblas_ssyr2k
+    fn(layout, uplo, trans, n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc)
+    return c
+
+
 def cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
     load().cblas_dtrsm(layout, side, uplo, transa, diag, m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb)
     return b
@@ -190,6 +244,42 @@ def dsyrk_device(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
     st = load().zynum_blas_gpu_dsyrk_device(_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, float(beta),
                                             _ptr(c), ldc, _stream(stream))
     check(st, "zynum_blas_gpu_dsyrk_device")
+    return c
+
+
+def symm_device(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    """Device dsymm / ssymm on torch CUDA tensors (dtype from c)."""
+    import torch
+    L = load()
+    fn, name = ((L.zynum_blas_gpu_dsymm_device, "dsymm") if c.dtype == torch.float64
+                else (L.zynum_blas_gpu_ssymm_device, "ssymm"))
+    st = fn(_ch(side), _ch(uplo), m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc,
+            _stream(stream))
+    check(st, f"zynum_blas_gpu_{name}_device")
+    return c
+
+
+def trmm_device(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream=None):
+    """Device dtrmm / strmm on torch CUDA tensors (dtype from b; in-place on b)."""
+    import torch
+    L = load()
+    fn, name = ((L.zynum_blas_gpu_dtrmm_device, "dtrmm") if b.dtype == torch.float64
+                else (L.zynum_blas_gpu_strmm_device, "strmm"))
+    st = fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb,
+            _stream(stream))
+    check(st, f"zynum_blas_gpu_{name}_device")
+    return b
+
+
+def syr2k_device(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    """Device dsyr2k / ssyr2k on torch CUDA tensors (dtype from c)."""
+    import torch
+    L = load()
+    fn, name = ((L.zynum_blas_gpu_dsyr2k_device, "dsyr2k") if c.dtype == torch.float64
+                else (L.zynum_blas_gpu_ssyr2k_device, "ssyr2k"))
+    st = fn(_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc,
+            _stream(stream))
+    check(st, f"zynum_blas_gpu_{name}_device")
     return c
 
 

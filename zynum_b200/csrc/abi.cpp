@@ -19,7 +19,7 @@
 #include "kernels.h"
 #include "complex.h"
 #include "ozaki.h"
-#include "trsm_syrk.h"
+#include "level3.h"
 #include "runtime.h"
 
 using namespace zb;
@@ -381,6 +381,32 @@ int syrk_error(char uplo, char trans, int n, int k, int lda, int ldc) {
     return 0;
 }
 
+// fortran.zig:239-250 symmetricMatrixError
+int symm_error(char side, char uplo, int m, int n, int lda, int ldb, int ldc) {
+    if (!valid_side(side)) return 1;
+    if (!valid_uplo(uplo)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    const int nrowa = (side == 'L') ? m : n;
+    if (lda < max1(nrowa)) return 7;
+    if (ldb < max1(m)) return 9;
+    if (ldc < max1(m)) return 12;
+    return 0;
+}
+
+// fortran.zig:264-275 rank2KMatrixError
+int syr2k_error(char uplo, char trans, int n, int k, int lda, int ldb, int ldc) {
+    if (!valid_uplo(uplo)) return 1;
+    if (!valid_trans(trans)) return 2;
+    if (n < 0) return 3;
+    if (k < 0) return 4;
+    const int nrow = (trans == 'N') ? n : k;
+    if (lda < max1(nrow)) return 7;
+    if (ldb < max1(nrow)) return 9;
+    if (ldc < max1(n)) return 12;
+    return 0;
+}
+
 // GEMMs inside TRSM: the real GEMM route with a fixed scratch region.
 template <typename T>
 GemmFn<T> gemm_fn(cudaStream_t st, FixedScratch* fs) {
@@ -426,9 +452,67 @@ cudaError_t run_syrk(char uplo, char trans, int n, int k, T alpha, const T* a, l
         return sgemm_native(g, p, static_cast<float*>(ws), st);
 }
 
+template <typename T, typename Scratch>
+cudaError_t run_trmm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
+    if (t.m <= 0 || t.n <= 0) return cudaSuccess;
+    const size_t planes = trmm_plane_bytes<T>(t.side, t.m, t.n);
+    const int na = (t.side == 'L') ? t.m : t.n;
+    const size_t real = real_scratch_bound<T>(t.m, t.n, na);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return trmm<T>(t, ws, gemm_fn<T>(st, &fs), st);
+}
+
+template <typename T, typename Scratch>
+cudaError_t run_symm(char side, char uplo, int m, int n, T alpha, const T* a, long lda, const T* b, long ldb, T beta,
+                     T* c, long ldc, cudaStream_t st, Scratch scratch) {
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    if (alpha == T(0)) return scale_matrix<T>(m, n, beta, c, ldc, st);
+    const size_t planes = symm_plane_bytes<T>(side, m, n);
+    const int na = (side == 'L') ? m : n;
+    const size_t real = real_scratch_bytes(m, n, na, (T*)nullptr);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return symm<T>(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, ws, gemm_fn<T>(st, &fs), st);
+}
+
+// SYR2K: two triangle-mode GEMMs, alpha op(A) op(B)^T + beta C, then
+// alpha op(B) op(A)^T added with beta = 1.
+template <typename T, typename Scratch>
+cudaError_t run_syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, long lda, const T* b, long ldb,
+                      T beta, T* c, long ldc, cudaStream_t st, Scratch scratch) {
+    if (n <= 0) return cudaSuccess;
+    if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
+    Context& cx = context();
+    const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
+    GemmArgs<T> g1{t1, t2, n, n, k, alpha, a, lda, b, ldb, beta, c, ldc};
+    GemmArgs<T> g2{t1, t2, n, n, k, alpha, b, ldb, a, lda, T(1), c, ldc};
+    g1.tri = g2.tri = (uplo == 'U') ? 1 : 2;
+    GemmPlan p = plan_native_gemm(n, n, k, sizeof(T), cx.sm_count);
+    void* ws = nullptr;
+    const size_t need = sizeof(T) == 4 ? sgemm_native_workspace_bytes(t1, t2, n, n, k, p)
+                                       : splitk_workspace_elems(n, n, p.splits) * sizeof(T);
+    if (need) {
+        cudaError_t e = scratch(need, st, &ws);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e;
+    if constexpr (sizeof(T) == 8) {
+        if ((e = dgemm_native(g1, p, static_cast<double*>(ws), st)) != cudaSuccess) return e;
+        return dgemm_native(g2, p, static_cast<double*>(ws), st);
+    } else {
+        if ((e = sgemm_native(g1, p, static_cast<float*>(ws), st)) != cudaSuccess) return e;
+        return sgemm_native(g2, p, static_cast<float*>(ws), st);
+    }
+}
+
 template <typename T>
 void host_trsm(const char* routine, char side, char uplo, char trans, char diag, int m, int n, T alpha, const T* a,
-               int lda, T* b, int ldb) {
+               int lda, T* b, int ldb, bool multiply = false) {
     if (m <= 0 || n <= 0) return;
     Context& cx = context();
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
@@ -452,8 +536,10 @@ void host_trsm(const char* routine, char side, char uplo, char trans, char diag,
     e = cudaMemcpy2DAsync(da, (size_t)na * es, a, (size_t)lda * es, (size_t)na * es, na, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(db, (size_t)m * es, b, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = run_trsm(TrsmArgs<T>{side, uplo, trans, diag, m, n, alpha, da, na, db, m}, st,
-                                       HostScratch{&cx});
+    if (e == cudaSuccess) {
+        const TrsmArgs<T> t{side, uplo, trans, diag, m, n, alpha, da, na, db, m};
+        e = multiply ? run_trmm(t, st, HostScratch{&cx}) : run_trsm(t, st, HostScratch{&cx});
+    }
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
         cuda_status(e, "GPU execution");
@@ -513,9 +599,112 @@ void host_syrk(const char* routine, char uplo, char trans, int n, int k, T alpha
     }
 }
 
+// SYMM on host arrays: A's na x na window, B and C staged; only C's m x n window comes back.
+template <typename T>
+void host_symm(const char* routine, char side, char uplo, int m, int n, T alpha, const T* a, int lda, const T* b,
+               int ldb, T beta, T* c, int ldc) {
+    if (m <= 0 || n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const int na = (side == 'L') ? m : n;
+    const size_t es = sizeof(T);
+    if ((e = cx.reserve(cx.stage_a, (size_t)na * na * es, st)) != cudaSuccess ||
+        (e = cx.reserve(cx.stage_b, (size_t)m * n * es, st)) != cudaSuccess ||
+        (e = cx.reserve(cx.stage_c, (size_t)m * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* db = static_cast<T*>(cx.stage_b.ptr);
+    T* dc = static_cast<T*>(cx.stage_c.ptr);
+    e = cudaSuccess;
+    if (alpha != T(0)) {
+        e = cudaMemcpy2DAsync(da, (size_t)na * es, a, (size_t)lda * es, (size_t)na * es, na, cudaMemcpyHostToDevice,
+                              st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(db, (size_t)m * es, b, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice,
+                                  st);
+    }
+    if (e == cudaSuccess && beta != T(0))
+        e = cudaMemcpy2DAsync(dc, (size_t)m * es, c, (size_t)ldc * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = run_symm<T>(side, uplo, m, n, alpha, da, na, db, m, beta, dc, m, st, HostScratch{&cx});
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)m * es, (size_t)m * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+// SYR2K on host arrays: C is staged whole so the other triangle comes back bit-identical.
+template <typename T>
+void host_syr2k(const char* routine, char uplo, char trans, int n, int k, T alpha, const T* a, int lda, const T* b,
+                int ldb, T beta, T* c, int ldc) {
+    if (n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const int ra = (trans == 'N') ? n : k, ca = (trans == 'N') ? k : n;
+    const size_t es = sizeof(T);
+    if ((k > 0 && ((e = cx.reserve(cx.stage_a, (size_t)ra * ca * es, st)) != cudaSuccess ||
+                   (e = cx.reserve(cx.stage_b, (size_t)ra * ca * es, st)) != cudaSuccess)) ||
+        (e = cx.reserve(cx.stage_c, (size_t)n * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    T* da = static_cast<T*>(cx.stage_a.ptr);
+    T* db = static_cast<T*>(cx.stage_b.ptr);
+    T* dc = static_cast<T*>(cx.stage_c.ptr);
+    e = cudaSuccess;
+    if (k > 0) {
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice,
+                              st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(db, (size_t)ra * es, b, (size_t)ldb * es, (size_t)ra * es, ca,
+                                  cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dc, (size_t)n * es, c, (size_t)ldc * es, (size_t)n * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = run_syr2k<T>(uplo, trans, n, k, alpha, da, ra, db, ra, beta, dc, n, st, HostScratch{&cx});
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)n * es, (size_t)n * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
 template <typename T>
 int device_trsm(const char* what, char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
-                int lda, T* b, int ldb, void* stream) {
+                int lda, T* b, int ldb, void* stream, bool multiply = false) {
     const char sd = up(&side), ul = up(&uplo), tr = up(&transa), dg = up(&diag);
     int info = trsm_error(sd, ul, tr, dg, m, n, lda, ldb);
     if (info) return info;
@@ -527,9 +716,9 @@ int device_trsm(const char* what, char side, char uplo, char transa, char diag, 
         e = cx.init();
     }
     if (e != cudaSuccess) return cuda_status(e, "initialisation");
-    return cuda_status(run_trsm(TrsmArgs<T>{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb},
-                                static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
-                       what);
+    const TrsmArgs<T> t{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb};
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return cuda_status(multiply ? run_trmm(t, st, StreamScratch{&cx}) : run_trsm(t, st, StreamScratch{&cx}), what);
 }
 
 template <typename T>
@@ -549,6 +738,44 @@ int device_syrk(const char* what, char uplo, char trans, int n, int k, T alpha, 
     return cuda_status(
         run_syrk<T>(ul, tr, n, k, alpha, a, lda, beta, c, ldc, static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
         what);
+}
+
+template <typename T>
+int device_symm(const char* what, char side, char uplo, int m, int n, T alpha, const T* a, int lda, const T* b,
+                int ldb, T beta, T* c, int ldc, void* stream) {
+    const char sd = up(&side), ul = up(&uplo);
+    int info = symm_error(sd, ul, m, n, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_symm<T>(sd, ul, m, n, alpha, a, lda, b, ldb, beta, c, ldc,
+                                   static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+                       what);
+}
+
+template <typename T>
+int device_syr2k(const char* what, char uplo, char trans, int n, int k, T alpha, const T* a, int lda, const T* b,
+                 int ldb, T beta, T* c, int ldc, void* stream) {
+    const char ul = up(&uplo), tr = up(&trans);
+    int info = syr2k_error(ul, tr, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_syr2k<T>(ul, tr, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                                    static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+                       what);
 }
 
 inline char cblas_uplo_char(int u) { return u == CblasUpper ? 'U' : (u == CblasLower ? 'L' : 'X'); }
@@ -795,6 +1022,133 @@ int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alph
 int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float* a, int lda, float beta,
                                 float* c, int ldc, void* stream) {
     return device_syrk<float>("ssyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
+}
+
+// fortran.zig:777-783 ?symm_, :852-858 ?trmm_, :827-833 ?syr2k_
+#define ZB_SYMM(NAME, T, RNAME)                                                                                   \
+    void NAME(const char* side, const char* uplo, const zynum_blas_int* m, const zynum_blas_int* n, const T* alpha, \
+              const T* a, const zynum_blas_int* lda, const T* b, const zynum_blas_int* ldb, const T* beta, T* c,   \
+              const zynum_blas_int* ldc) {                                                                         \
+        const char sd = up(side), ul = up(uplo);                                                                   \
+        int info = symm_error(sd, ul, *m, *n, *lda, *ldb, *ldc);                                                   \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        host_symm<T>(RNAME, sd, ul, *m, *n, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                            \
+    }
+ZB_SYMM(dsymm_, double, "DSYMM ")
+ZB_SYMM(ssymm_, float, "SSYMM ")
+#undef ZB_SYMM
+
+#define ZB_TRMM(NAME, T, RNAME)                                                                                    \
+    void NAME(const char* side, const char* uplo, const char* transa, const char* diag, const zynum_blas_int* m,  \
+              const zynum_blas_int* n, const T* alpha, const T* a, const zynum_blas_int* lda, T* b,               \
+              const zynum_blas_int* ldb) {                                                                        \
+        const char sd = up(side), ul = up(uplo), tr = up(transa), dg = up(diag);                                   \
+        int info = trsm_error(sd, ul, tr, dg, *m, *n, *lda, *ldb);                                                 \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        host_trsm<T>(RNAME, sd, ul, tr, dg, *m, *n, *alpha, a, *lda, b, *ldb, true);                               \
+    }
+ZB_TRMM(dtrmm_, double, "DTRMM ")
+ZB_TRMM(strmm_, float, "STRMM ")
+#undef ZB_TRMM
+
+#define ZB_SYR2K(NAME, T, RNAME)                                                                                    \
+    void NAME(const char* uplo, const char* trans, const zynum_blas_int* n, const zynum_blas_int* k, const T* alpha, \
+              const T* a, const zynum_blas_int* lda, const T* b, const zynum_blas_int* ldb, const T* beta, T* c,    \
+              const zynum_blas_int* ldc) {                                                                          \
+        const char ul = up(uplo), tr = up(trans);                                                                   \
+        int info = syr2k_error(ul, tr, *n, *k, *lda, *ldb, *ldc);                                                   \
+        if (info) {                                                                                                 \
+            report_xerbla(RNAME, info);                                                                             \
+            return;                                                                                                 \
+        }                                                                                                           \
+        host_syr2k<T>(RNAME, ul, tr, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                             \
+    }
+ZB_SYR2K(dsyr2k_, double, "DSYR2K")
+ZB_SYR2K(ssyr2k_, float, "SSYR2K")
+#undef ZB_SYR2K
+
+// cblas.zig:1479-1489 cblas_?symm: only the layout is checked here (a bad side
+// or uplo reaches the Fortran routine as 'X' and is reported by xerbla);
+// row-major flips side and uplo and swaps m / n.
+#define ZB_CBLAS_SYMM(NAME, FNAME, T)                                                                         \
+    void NAME(int layout, int side, int uplo, int m, int n, T alpha, const T* a, int lda, const T* b, int ldb, \
+              T beta, T* c, int ldc) {                                                                        \
+        if (!cblas_valid_layout(layout)) return;                                                              \
+        const bool rm = layout == CblasRowMajor;                                                              \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                     \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                     \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb, lc = ldc;                        \
+        FNAME(&ss, &uu, &mm, &nn, &alpha, a, &la, b, &lb, &beta, c, &lc);                                     \
+    }
+ZB_CBLAS_SYMM(cblas_dsymm, dsymm_, double)
+ZB_CBLAS_SYMM(cblas_ssymm, ssymm_, float)
+#undef ZB_CBLAS_SYMM
+
+// cblas.zig:1690-1701 cblas_?trmm: invalid enums return silently; row-major
+// flips side and uplo and swaps m / n, keeping the transpose.
+#define ZB_CBLAS_TRMM(NAME, FNAME, T)                                                                            \
+    void NAME(int layout, int side, int uplo, int transa, int diag, int m, int n, T alpha, const T* a, int lda, \
+              T* b, int ldb) {                                                                                   \
+        if (!cblas_valid_layout(layout) || (side != CblasLeft && side != CblasRight) ||                          \
+            (uplo != CblasUpper && uplo != CblasLower) || !cblas_valid_trans(transa) ||                          \
+            (diag != CblasNonUnit && diag != CblasUnit))                                                         \
+            return;                                                                                              \
+        const bool rm = layout == CblasRowMajor;                                                                 \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                        \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                        \
+        char tt = cblas_trans_char(transa), dd = cblas_diag_char(diag);                                          \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb;                                     \
+        FNAME(&ss, &uu, &tt, &dd, &mm, &nn, &alpha, a, &la, b, &lb);                                             \
+    }
+ZB_CBLAS_TRMM(cblas_dtrmm, dtrmm_, double)
+ZB_CBLAS_TRMM(cblas_strmm, strmm_, float)
+#undef ZB_CBLAS_TRMM
+
+// cblas.zig:1617-1627 cblas_?syr2k: only the layout is checked here; row-major
+// flips uplo and the transpose.
+#define ZB_CBLAS_SYR2K(NAME, FNAME, T)                                                                            \
+    void NAME(int layout, int uplo, int trans, int n, int k, T alpha, const T* a, int lda, const T* b, int ldb,  \
+              T beta, T* c, int ldc) {                                                                           \
+        if (!cblas_valid_layout(layout)) return;                                                                 \
+        const bool rm = layout == CblasRowMajor;                                                                 \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                        \
+        char tt = rm ? cblas_row_trans_char(trans) : cblas_trans_char(trans);                                    \
+        zynum_blas_int nn = n, kk = k, la = lda, lb = ldb, lc = ldc;                                             \
+        FNAME(&uu, &tt, &nn, &kk, &alpha, a, &la, b, &lb, &beta, c, &lc);                                        \
+    }
+ZB_CBLAS_SYR2K(cblas_dsyr2k, dsyr2k_, double)
+ZB_CBLAS_SYR2K(cblas_ssyr2k, ssyr2k_, float)
+#undef ZB_CBLAS_SYR2K
+
+int zynum_blas_gpu_dsymm_device(char side, char uplo, int m, int n, double alpha, const double* a, int lda,
+                                const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+    return device_symm<double>("dsymm_device", side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, stream);
+}
+int zynum_blas_gpu_ssymm_device(char side, char uplo, int m, int n, float alpha, const float* a, int lda,
+                                const float* b, int ldb, float beta, float* c, int ldc, void* stream) {
+    return device_symm<float>("ssymm_device", side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, stream);
+}
+int zynum_blas_gpu_dtrmm_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+                                const double* a, int lda, double* b, int ldb, void* stream) {
+    return device_trsm<double>("dtrmm_device", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream, true);
+}
+int zynum_blas_gpu_strmm_device(char side, char uplo, char transa, char diag, int m, int n, float alpha,
+                                const float* a, int lda, float* b, int ldb, void* stream) {
+    return device_trsm<float>("strmm_device", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream, true);
+}
+int zynum_blas_gpu_dsyr2k_device(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+                                 const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+    return device_syr2k<double>("dsyr2k_device", uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream);
+}
+int zynum_blas_gpu_ssyr2k_device(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+                                 const float* b, int ldb, float beta, float* c, int ldc, void* stream) {
+    return device_syr2k<float>("ssyr2k_device", uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream);
 }
 
 // GEMM restricted to one triangle of C (the "gemmt" extension): only elements

@@ -1,4 +1,5 @@
-// TRSM and SYRK on the GEMM tiles.
+// Triangular and symmetric Level-3 routines on the GEMM tiles: TRSM, SYRK,
+// SYMM, TRMM and SYR2K.
 //
 // TRSM  B := alpha * op(A)^-1 * B  (side L)  or  B * op(A)^-1  (side R)
 //   Reference: core/matrix_matrix/triangular.zig:233 trsm (alpha pre-scale
@@ -14,11 +15,27 @@
 //   Reference: core/matrix_matrix/symmetric.zig:237 syrk / runSyrkColumns :180
 //   (one dot product per (i, j) of the triangle).  GPU algorithm: the GEMM
 //   kernel in triangle mode: tiles outside the triangle are skipped and
-//   elements outside it are never written.
+//   elements outside it are never written.  SYR2K (symmetric.zig:366 /
+//   runSyr2kColumns :301) is two such GEMMs, the second with beta = 1.
+//
+// SYMM  C := alpha * A * B + beta * C (side L) or alpha * B * A + beta * C,
+//   A symmetric with one stored triangle (symmetric.zig:107 / runSymmColumns
+//   :56, symValue access.zig:31).  GPU algorithm: the stored triangle is
+//   mirrored into a dense scratch copy (one O(n^2) pass through shared-memory
+//   transposes), then one GEMM on the native (or Ozaki) tiles.
+//
+// TRMM  B := alpha * op(A) * B (side L) or alpha * B * op(A), A triangular,
+//   in place (triangular.zig:202; left side trmv + scale per column :103-110,
+//   right side row products :212-229).  GPU algorithm: B is copied to a
+//   scratch W; every 256 x 256 diagonal block of op(A) is written out dense
+//   (zeros outside the triangle, ones on a unit diagonal) in one launch and
+//   applied as B_J = alpha D_J W_J; the off-diagonal part of op(A) is added by
+//   recursive halving on block boundaries, one GEMM (beta = 1) per level and
+//   half.  Reading W rather than B makes every GEMM independent of the order.
 #include <functional>
 
 #include "common.cuh"
-#include "trsm_syrk.h"
+#include "level3.h"
 
 namespace zb {
 namespace {
@@ -116,7 +133,141 @@ __global__ void symmetrize(int n, int from_upper, T* __restrict__ c, long ldc) {
     }
 }
 
+// Dense symmetric S (n x n, ld lds) from the uplo triangle of A.  A 32 x 32
+// output tile takes its stored elements straight from A and its mirrored
+// elements from a shared-memory transpose of the opposite tile, so global
+// reads and writes are all coalesced.  Block (32, 8).
+template <typename T>
+__global__ void sym_expand(int n, int from_upper, const T* __restrict__ a, long lda, T* __restrict__ s, long lds) {
+    __shared__ T t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    // does the tile hold any element of the unstored triangle?
+    const bool mirror = from_upper ? (r0 + 31 > c0) : (r0 < c0 + 31);
+    if (mirror) {  // t[y][x] = A(c0 + x, r0 + y)
+        for (int y = ty; y < 32; y += 8) {
+            const int ar = c0 + tx, ac = r0 + y;
+            t[y][tx] = (ar < n && ac < n) ? a[ar + (long)ac * lda] : T(0);
+        }
+    }
+    __syncthreads();
+    for (int y = ty; y < 32; y += 8) {
+        const int i = r0 + tx, j = c0 + y;
+        if (i >= n || j >= n) continue;
+        const bool stored = from_upper ? i <= j : i >= j;
+        s[i + (long)j * lds] = stored ? a[i + (long)j * lda] : t[tx][y];
+    }
+}
+
+// Block (x, y): the dense diagonal block y of op(A), rows / columns y*nb ..
+// (size s <= nb), column-major with ld nb; zeros outside the triangle and
+// outside s x s, ones on a unit diagonal.
+template <typename T>
+__global__ void tri_dense_blocks(const T* __restrict__ a, long lda, char uplo, char trans, char diag, int n, int nb,
+                                 T* __restrict__ out) {
+    const int b0 = blockIdx.y * nb;
+    const int s = min(nb, n - b0);
+    T* o = out + (long)blockIdx.y * nb * nb;
+    const long total = (long)nb * nb;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(q % nb), c = (int)(q / nb);
+        o[q] = (r < s && c < s) ? op_tri(a, lda, uplo, trans, diag, b0 + r, b0 + c) : T(0);
+    }
+}
+
+constexpr int kTrmmNB = 256;
+
 }  // namespace
+
+template <typename T>
+size_t symm_plane_bytes(char side, int m, int n) {
+    const long na = (side == 'L') ? m : n;
+    return ((size_t)(na * na) * sizeof(T) + 1023) & ~size_t(1023);
+}
+
+template <typename T>
+cudaError_t symm(char side, char uplo, int m, int n, T alpha, const T* a, long lda, const T* b, long ldb, T beta,
+                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st) {
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    const int na = (side == 'L') ? m : n;
+    T* S = static_cast<T*>(planes);
+    dim3 grid((na + 31) / 32, (na + 31) / 32);
+    sym_expand<T><<<grid, dim3(32, 8), 0, st>>>(na, uplo == 'U' ? 1 : 0, a, lda, S, na);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (side == 'L') return gemm({'N', 'N', m, n, m, alpha, S, na, b, ldb, beta, c, ldc});
+    return gemm({'N', 'N', m, n, n, alpha, b, ldb, S, na, beta, c, ldc});
+}
+
+template <typename T>
+size_t trmm_plane_bytes(char side, int m, int n) {
+    const long na = (side == 'L') ? m : n;
+    const long nblk = (na + kTrmmNB - 1) / kTrmmNB;
+    const size_t d = ((size_t)(nblk * kTrmmNB * kTrmmNB) * sizeof(T) + 1023) & ~size_t(1023);
+    return d + (((size_t)m * n * sizeof(T) + 1023) & ~size_t(1023));
+}
+
+template <typename T>
+cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st) {
+    const int m = t.m, n = t.n;
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    const bool left = t.side == 'L';
+    const int na = left ? m : n;
+    const int nblk = (na + kTrmmNB - 1) / kTrmmNB;
+    T* D = static_cast<T*>(planes);
+    T* W = reinterpret_cast<T*>(static_cast<char*>(planes) +
+                                (((size_t)nblk * kTrmmNB * kTrmmNB * sizeof(T) + 1023) & ~size_t(1023)));
+    cudaError_t e = cudaMemcpy2DAsync(W, (size_t)m * sizeof(T), t.b, (size_t)t.ldb * sizeof(T), (size_t)m * sizeof(T),
+                                      n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    tri_dense_blocks<T><<<dim3(64, nblk), 256, 0, st>>>(t.a, t.lda, t.uplo, t.trans, t.diag, na, kTrmmNB, D);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const long ldb = t.ldb, lda = t.lda;
+    // diagonal blocks: B_J := alpha D_J W_J (left) or alpha W_J D_J (right)
+    for (int J = 0; J < nblk; ++J) {
+        const int p0 = J * kTrmmNB, len = std::min(kTrmmNB, na - p0);
+        const T* dj = D + (long)J * kTrmmNB * kTrmmNB;
+        if (left)
+            e = gemm({'N', 'N', len, n, len, t.alpha, dj, kTrmmNB, W + p0, m, T(0), t.b + p0, ldb});
+        else
+            e = gemm({'N', 'N', m, len, len, t.alpha, W + (long)p0 * m, m, dj, kTrmmNB, T(0), t.b + (long)p0 * ldb,
+                      ldb});
+        if (e != cudaSuccess) return e;
+    }
+    const bool upper = op_is_upper(t.uplo, t.trans);
+    const char ta = (t.trans == 'N') ? 'N' : 'T';
+    auto opa = [&](int r0, int c0) -> const T* {
+        return (ta == 'N') ? t.a + r0 + (long)c0 * lda : t.a + c0 + (long)r0 * lda;
+    };
+    // off-diagonal blocks of op(A), halved on block boundaries: B += alpha op(A)_off W
+    std::function<cudaError_t(int, int)> add_off = [&](int p0, int p1) -> cudaError_t {
+        const int len = p1 - p0;
+        if (len <= kTrmmNB) return cudaSuccess;
+        const int mid = p0 + ((len / 2 + kTrmmNB - 1) / kTrmmNB) * kTrmmNB;
+        const int h1 = mid - p0, h2 = p1 - mid;
+        cudaError_t err;
+        if (left) {
+            if (!upper)  // rows mid..p1 gain op(A)[mid:p1, p0:mid] W[p0:mid]
+                err = gemm({ta, 'N', h2, n, h1, t.alpha, opa(mid, p0), lda, W + p0, m, T(1), t.b + mid, ldb});
+            else  // rows p0..mid gain op(A)[p0:mid, mid:p1] W[mid:p1]
+                err = gemm({ta, 'N', h1, n, h2, t.alpha, opa(p0, mid), lda, W + mid, m, T(1), t.b + p0, ldb});
+        } else {
+            if (upper)  // columns mid..p1 gain W[:, p0:mid] op(A)[p0:mid, mid:p1]
+                err = gemm({'N', ta, m, h2, h1, t.alpha, W + (long)p0 * m, m, opa(p0, mid), lda, T(1),
+                            t.b + (long)mid * ldb, ldb});
+            else  // columns p0..mid gain W[:, mid:p1] op(A)[mid:p1, p0:mid]
+                err = gemm({'N', ta, m, h1, h2, t.alpha, W + (long)mid * m, m, opa(mid, p0), lda, T(1),
+                            t.b + (long)p0 * ldb, ldb});
+        }
+        if (err != cudaSuccess) return err;
+        if ((err = add_off(p0, mid)) != cudaSuccess) return err;
+        return add_off(mid, p1);
+    };
+    if ((e = add_off(0, na)) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
 
 template <typename T>
 cudaError_t symmetrize_matrix(char uplo, int n, T* c, long ldc, cudaStream_t st) {
@@ -230,5 +381,15 @@ template cudaError_t trsm<double>(const TrsmArgs<double>&, void*, const GemmFn<d
 template cudaError_t trsm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t);
 template cudaError_t syrk_scale_only<double>(int, char, double, double*, long, cudaStream_t);
 template cudaError_t syrk_scale_only<float>(int, char, float, float*, long, cudaStream_t);
+template size_t symm_plane_bytes<double>(char, int, int);
+template size_t symm_plane_bytes<float>(char, int, int);
+template cudaError_t symm<double>(char, char, int, int, double, const double*, long, const double*, long, double,
+                                  double*, long, void*, const GemmFn<double>&, cudaStream_t);
+template cudaError_t symm<float>(char, char, int, int, float, const float*, long, const float*, long, float, float*,
+                                 long, void*, const GemmFn<float>&, cudaStream_t);
+template size_t trmm_plane_bytes<double>(char, int, int);
+template size_t trmm_plane_bytes<float>(char, int, int);
+template cudaError_t trmm<double>(const TrsmArgs<double>&, void*, const GemmFn<double>&, cudaStream_t);
+template cudaError_t trmm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t);
 
 }  // namespace zb

@@ -1,4 +1,4 @@
-// TRSM and SYRK built on the GEMM tiles.
+// TRSM, SYRK, SYMM, TRMM and SYR2K built on the GEMM tiles.
 #pragma once
 
 #include <algorithm>
@@ -32,6 +32,24 @@ size_t trsm_plane_bytes(char side, int m, int n);
 
 template <typename T>
 cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
+
+// Device scratch SYMM needs besides its GEMM's scratch: the dense symmetric copy of A.
+template <typename T>
+size_t symm_plane_bytes(char side, int m, int n);
+
+// C := alpha A B + beta C (side L) or alpha B A + beta C (side R), A symmetric
+// with its uplo triangle stored; arguments validated, device pointers.
+template <typename T>
+cudaError_t symm(char side, char uplo, int m, int n, T alpha, const T* a, long lda, const T* b, long ldb, T beta,
+                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
+
+// Device scratch TRMM needs besides its GEMMs' scratch: dense diagonal blocks and a copy of B.
+template <typename T>
+size_t trmm_plane_bytes(char side, int m, int n);
+
+// B := alpha op(A) B (side L) or alpha B op(A) (side R), A triangular (TrsmArgs fields).
+template <typename T>
+cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
 
 // Copy the uplo triangle of the n x n matrix c onto the other triangle.
 template <typename T>
