@@ -626,6 +626,52 @@ def suite_vector(args):
     return 0
 
 
+def suite_level3(args):
+    """Triangular / symmetric Level-3 routines on device pointers, n = 8192 (TRSM and
+    TRMM with 8192 right-hand sides, SYRK / SYR2K with k = 8192), FP64 under the native
+    and the automatic (Ozaki-capable) method and FP32 native.  TFLOP/s counts the
+    useful flops: TRSM / TRMM m^2 n, SYMM 2 m^2 n, SYRK n^2 k, SYR2K 2 n^2 k."""
+    import torch
+    from zynum_b200 import blas
+    stream = torch.cuda.current_stream()
+    n = args.size
+    rows = []
+    for dt, tdt in (("f64", torch.float64), ("f32", torch.float32)):
+        g = torch.Generator(device="cuda").manual_seed(3)
+        A = torch.rand((n, n), generator=g, device="cuda", dtype=tdt) * 2 - 1
+        A += n * torch.eye(n, device="cuda", dtype=tdt)   # well-conditioned triangles for TRSM
+        B = torch.rand((n, n), generator=g, device="cuda", dtype=tdt) * 2 - 1
+        C = torch.zeros((n, n), device="cuda", dtype=tdt)
+        X = B.clone()
+        ops = {
+            "trsm": (lambda: (X.copy_(B), blas.dtrsm_device("L", "L", "N", "N", n, n, 1.0, A, n, X, n)),
+                     float(n) ** 3),
+            "trmm": (lambda: (X.copy_(B), blas.trmm_device("L", "L", "N", "N", n, n, 1.0, A, n, X, n)),
+                     float(n) ** 3),
+            "symm": (lambda: blas.symm_device("L", "U", n, n, 1.0, A, n, B, n, 0.0, C, n), 2.0 * float(n) ** 3),
+            "syr2k": (lambda: blas.syr2k_device("L", "N", n, n, 1.0, A, n, B, n, 0.0, C, n), 2.0 * float(n) ** 3),
+        }
+        if dt == "f64":
+            ops["syrk"] = (lambda: blas.dsyrk_device("L", "N", n, n, 1.0, A, n, 0.0, C, n), float(n) ** 3)
+        else:
+            ops.pop("trsm")
+        methods = (("native", blas.METHOD_NATIVE), ("auto", blas.METHOD_AUTO)) if dt == "f64" else (("native", None),)
+        for mname, mval in methods:
+            old = blas.set_dgemm_method(mval) if mval is not None else None
+            for name, (fn, flops) in ops.items():
+                ms = time_device(torch, fn, max(3, min(args.steps, 5)), max(3, args.warmup), stream)
+                if name in ("trsm", "trmm"):  # the timed call includes an n x n device copy of B
+                    ms_copy = time_device(torch, lambda: X.copy_(B), 5, 2, stream)
+                    ms -= ms_copy
+                rows.append({"op": name, "dtype": dt, "method": mname, "n": n, "ms": ms,
+                             "tflops": flops / (ms * 1e-3) / 1e12})
+            if old is not None:
+                blas.set_dgemm_method(old)
+        del A, B, C, X
+    print(json.dumps({"suite": "level3", "rows": rows}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -638,7 +684,7 @@ def main(argv=None):
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector"], default="headline",
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3"], default="headline",
                     help="precision / sweep: secondary measurement suites (one JSON line each)")
     args = ap.parse_args(argv)
 
@@ -662,6 +708,8 @@ def main(argv=None):
             return suite_sweep(args)
         if args.suite == "vector":
             return suite_vector(args)
+        if args.suite == "level3":
+            return suite_level3(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -218,3 +218,44 @@ def test_device_entry_points(blas, oracle, dtype):
     got = host(Cs)
     assert np.abs(got - ref)[up].max() <= tol * max(1.0, np.abs(ref).max())
     assert np.all(got[~up] == 0.0)
+
+
+@pytest.mark.parametrize("routine", ["syrk", "syr2k"])
+@pytest.mark.parametrize("uplo,trans", list(itertools.product("UL", "NT")))
+def test_rank_k_ozaki_route(blas, oracle, routine, uplo, trans):
+    """DSYRK / DSYR2K under the Ozaki method: one full emulated product W into scratch, then
+    alpha (W [+ W^T]) + beta C on the triangle; the other triangle and padding stay bit-identical,
+    beta = 0 clears NaN."""
+    rng = np.random.default_rng(ord(uplo) * 3 + ord(trans) + len(routine))
+    n, k = 301, 190
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = _mat(rng, ra, ca, ra + 1, np.float64)
+    b = _mat(rng, ra, ca, ra + 2, np.float64)
+    old = blas.set_dgemm_method(blas.METHOD_OZAKI)
+    try:
+        for alpha, beta in ((0.75, -0.5), (1.0, 0.0)):
+            c = _mat(rng, n, n, n + 3, np.float64, -777.0)
+            tri = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+            if beta == 0.0:
+                c[:n, :n][tri] = np.nan
+            c0 = c.copy(order="F")
+            ref = c.copy(order="F")
+            if routine == "syrk":
+                oracle.syrk(uplo, trans, n, k, alpha, a, ra + 1, beta, ref, n + 3)
+                blas.syrk(uplo, trans, n, k, alpha, a, ra + 1, beta, c, n + 3)
+                A = np.abs(a[:ra, :ca]) if trans == "N" else np.abs(a[:ra, :ca]).T
+                prod = A @ A.T
+            else:
+                oracle.syr2k(uplo, trans, n, k, alpha, a, ra + 1, b, ra + 2, beta, ref, n + 3)
+                blas.syr2k(uplo, trans, n, k, alpha, a, ra + 1, b, ra + 2, beta, c, n + 3)
+                A = np.abs(a[:ra, :ca]) if trans == "N" else np.abs(a[:ra, :ca]).T
+                B = np.abs(b[:ra, :ca]) if trans == "N" else np.abs(b[:ra, :ca]).T
+                prod = A @ B.T + B @ A.T
+            bound = 8 * k * U[np.float64] * (abs(alpha) * prod + abs(beta) * np.nan_to_num(np.abs(c0[:n, :n])))
+            err = np.abs(c[:n, :n] - ref[:n, :n])
+            assert np.all(np.isfinite(c[:n, :n][tri]))
+            assert np.all(err[tri] <= bound[tri] + 1e-300), float(err[tri].max())
+            assert np.array_equal(c[:n, :n][~tri], c0[:n, :n][~tri]), "the other triangle changed"
+            assert np.array_equal(c[n:], c0[n:]), "padding rows of C were written"
+    finally:
+        blas.set_dgemm_method(old)

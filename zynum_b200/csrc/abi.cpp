@@ -430,11 +430,43 @@ cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
     return trsm<T>(t, ws, gemm_fn<T>(st, &fs), st);
 }
 
+// SYRK / SYR2K in FP64 take the emulated product when the DGEMM method is
+// Ozaki, or automatic and the model prefers one full emulated DGEMM (plus a
+// W write and the triangle pass) over native triangle-mode tiles (half the flops).
+inline bool rank_k_uses_ozaki(int n, int k) {
+    const int method = context().dgemm_method;
+    if (method == METHOD_OZAKI) return true;
+    return method == METHOD_AUTO && ozaki_preferred_scaled(n, n, k, 0.5, 24.0 * n * (double)n);
+}
+
+// W = op(A) op(B)^T as one full emulated DGEMM into scratch, then
+// C := alpha (W [+ W^T]) + beta C on the triangle (op(B) op(A)^T = W^T).
+template <typename Scratch>
+cudaError_t run_rank_k_ozaki(char uplo, char trans, bool two, int n, int k, double alpha, const double* a, long lda,
+                             const double* b, long ldb, double beta, double* c, long ldc, cudaStream_t st,
+                             Scratch scratch) {
+    Context& cx = context();
+    const OzakiPlan op = plan_ozaki(n, n, k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
+    const size_t wbytes = ((size_t)n * n * sizeof(double) + 1023) & ~size_t(1023);
+    void* ws = nullptr;
+    cudaError_t e = scratch(wbytes + ozaki_workspace_bytes(op), st, &ws);
+    if (e != cudaSuccess) return e;
+    double* W = static_cast<double*>(ws);
+    const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
+    const GemmArgsF64 g{t1, t2, n, n, k, 1.0, a, lda, b, ldb, 0.0, W, n};
+    if ((e = dgemm_ozaki(g, op, static_cast<char*>(ws) + wbytes, st)) != cudaSuccess) return e;
+    return triangle_update<double>(uplo, two, n, alpha, W, n, beta, c, ldc, st);
+}
+
 template <typename T, typename Scratch>
 cudaError_t run_syrk(char uplo, char trans, int n, int k, T alpha, const T* a, long lda, T beta, T* c, long ldc,
                      cudaStream_t st, Scratch scratch) {
     if (n <= 0) return cudaSuccess;
     if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
+    if constexpr (sizeof(T) == 8) {
+        if (rank_k_uses_ozaki(n, k)) return run_rank_k_ozaki(uplo, trans, false, n, k, alpha, a, lda, a, lda, beta, c,
+                                                             ldc, st, scratch);
+    }
     Context& cx = context();
     GemmArgs<T> g{trans == 'N' ? 'N' : 'T', trans == 'N' ? 'T' : 'N', n, n, k, alpha, a, lda, a, lda, beta, c, ldc};
     g.tri = (uplo == 'U') ? 1 : 2;
@@ -487,6 +519,10 @@ cudaError_t run_syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, 
                       T beta, T* c, long ldc, cudaStream_t st, Scratch scratch) {
     if (n <= 0) return cudaSuccess;
     if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
+    if constexpr (sizeof(T) == 8) {
+        if (rank_k_uses_ozaki(n, k)) return run_rank_k_ozaki(uplo, trans, true, n, k, alpha, a, lda, b, ldb, beta, c,
+                                                             ldc, st, scratch);
+    }
     Context& cx = context();
     const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
     GemmArgs<T> g1{t1, t2, n, n, k, alpha, a, lda, b, ldb, beta, c, ldc};

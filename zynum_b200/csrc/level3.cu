@@ -177,7 +177,49 @@ __global__ void tri_dense_blocks(const T* __restrict__ a, long lda, char uplo, c
 
 constexpr int kTrmmNB = 256;
 
+// C := alpha (W + W^T) + beta C (two) or alpha W + beta C on the uplo triangle,
+// W n x n with ld ldw; beta == 0 writes without reading C.  32 x 32 tiles, W^T
+// through a shared-memory transpose; tiles outside the triangle return at once.
+// Block (32, 8).
+template <typename T>
+__global__ void tri_update(int n, int upper, int two, T alpha, const T* __restrict__ w, long ldw, T beta,
+                           T* __restrict__ c, long ldc) {
+    __shared__ T t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    if (upper ? r0 > c0 + 31 : r0 + 31 < c0) return;  // the whole block: no element of the triangle
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (two) {  // t[y][x] = W(c0 + x, r0 + y)
+        for (int y = ty; y < 32; y += 8) {
+            const int wr = c0 + tx, wc = r0 + y;
+            t[y][tx] = (wr < n && wc < n) ? w[wr + (long)wc * ldw] : T(0);
+        }
+    }
+    __syncthreads();
+    for (int y = ty; y < 32; y += 8) {
+        const int i = r0 + tx, j = c0 + y;
+        if (i >= n || j >= n || (upper ? i > j : i < j)) continue;
+        T v = w[i + (long)j * ldw];
+        if (two) v = v + t[tx][y];
+        T* cp = c + i + (long)j * ldc;
+        *cp = beta == T(0) ? alpha * v : fma(beta, *cp, alpha * v);
+    }
+}
+
 }  // namespace
+
+template <typename T>
+cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
+                            cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    dim3 grid((n + 31) / 32, (n + 31) / 32);
+    tri_update<T><<<grid, dim3(32, 8), 0, st>>>(n, uplo == 'U' ? 1 : 0, two ? 1 : 0, alpha, w, ldw, beta, c, ldc);
+    count_launch();
+    return cudaGetLastError();
+}
+template cudaError_t triangle_update<double>(char, bool, int, double, const double*, long, double, double*, long,
+                                             cudaStream_t);
+template cudaError_t triangle_update<float>(char, bool, int, float, const float*, long, float, float*, long,
+                                            cudaStream_t);
 
 template <typename T>
 size_t symm_plane_bytes(char side, int m, int n) {

@@ -51,6 +51,13 @@ size_t trmm_plane_bytes(char side, int m, int n);
 template <typename T>
 cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
 
+// C := alpha (W + W^T) + beta C (two) or alpha W + beta C on the uplo triangle
+// of the n x n C (SYRK / SYR2K from a full product W; beta == 0 writes zeros
+// over NaN).
+template <typename T>
+cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
+                            cudaStream_t st);
+
 // Copy the uplo triangle of the n x n matrix c onto the other triangle.
 template <typename T>
 cudaError_t symmetrize_matrix(char uplo, int n, T* c, long ldc, cudaStream_t st);

@@ -1435,13 +1435,16 @@ static bool use_cta_pair(int m) {
 // residue and reconstruction traffic at ~2.5 TB/s, ~60 us of launches) is
 // below 0.8 x native FP64 at ~30 TFLOP/s; K beyond one CRT segment falls back
 // to the slice scheme, which needs larger products still.
-bool ozaki_preferred(int m, int n, int k) {
+bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double extra_bytes) {
     const double mnk2 = 2.0 * m * n * (double)k;
-    const double native_s = mnk2 / 30e12;
-    const double ozaki_s = 16.0 * mnk2 / 3.0e15 + (32.0 * ((double)m * k + (double)k * n) + 40.0 * (double)m * n) / 2.5e12 +
+    const double native_s = native_fraction * mnk2 / 30e12;
+    const double ozaki_s = 16.0 * mnk2 / 3.0e15 +
+                           (32.0 * ((double)m * k + (double)k * n) + 40.0 * (double)m * n + extra_bytes) / 2.5e12 +
                            60e-6;
-    return k <= kCrtMaxK ? ozaki_s < 0.8 * native_s : mnk2 >= 2e12;
+    return k <= kCrtMaxK ? ozaki_s < 0.8 * native_s : native_fraction * mnk2 >= 2e12;
 }
+
+bool ozaki_preferred(int m, int n, int k) { return ozaki_preferred_scaled(m, n, k, 1.0, 0.0); }
 
 int ozaki_auto_slices(float spread_a, float spread_b) {
     // Truncating a row of A after s 7-bit digits leaves |dA_ik| < 2^(e_i - 7s)
