@@ -104,3 +104,29 @@ def test_lsame_and_xerbla_trim(lib):
             "L=_lib.load(); L.xerbla_(b'DGEMM ', C.byref(C.c_int32(3)))\n" % str(ROOT))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=60)
     assert " ** On entry to DGEMM parameter number 3 had an illegal value" in r.stderr
+
+
+def test_abi_manifest_is_current_and_matches_reference():
+    """include/abi_manifest.json is what include/make_abi_manifest.py writes for the current
+    header, and every reference Level-3 export the library provides (tests/golden/
+    reference_abi_subset.json, from the reference's own manifest) has the same return type and
+    argument types in the same order."""
+    sys.path.insert(0, str(ROOT / "include"))
+    try:
+        import make_abi_manifest as mk
+    finally:
+        sys.path.pop(0)
+    import json
+    man = mk.build_manifest()
+    committed = json.loads((ROOT / "include" / "abi_manifest.json").read_text())
+    assert man == committed, "include/abi_manifest.json is stale: rerun include/make_abi_manifest.py"
+    ref = json.loads((ROOT / "tests" / "golden" / "reference_abi_subset.json").read_text())
+    report = mk.diff(man, ref)
+    for part in ("fortran", "cblas"):
+        assert report[part]["differ"] == [], report[part]["differ"]
+        provided = set(report[part]["same"])
+        for fam in ("gemm", "trsm", "syrk", "symm", "trmm", "syr2k"):
+            for p in "sd":
+                name = f"cblas_{p}{fam}" if part == "cblas" else f"{p}{fam}_"
+                assert name in provided, name
+    assert {"xerbla_", "lsame_", "zynum_blas_shutdown"} <= set(report["fortran"]["same"])
