@@ -276,3 +276,45 @@ def test_gemm_narrow_route(blas, oracle, dtype, ta, tb, shape):
         if pad == 0:
             lda, ldb = (lda + 3) // 4 * 4, (ldb + 3) // 4 * 4
         _run_case(blas, oracle, dtype, ta, tb, m, n, k, lda, ldb, m + 1, alpha, beta)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+def test_host_column_panel_pipeline(blas, dtype, ta, tb):
+    """Host calls with n >= 2048 and 2mnk >= 8e9 run as column panels of C (uploads, products
+    and downloads overlapped on three streams); ragged last panel, padded leading dimensions,
+    beta != 0, and the padding rows of C untouched."""
+    m, n, k = 601, 2100, 3400
+    rng = np.random.default_rng(5 + ord(ta) + 2 * ord(tb))
+    ar, ac = _op_shape(ta, m, k)
+    br, bc = _op_shape(tb, k, n)
+    lda, ldb, ldc = ar + 3, br + 1, m + 2
+    a = np.asfortranarray(np.full((lda, ac), -999.0)); a[:ar] = rng.uniform(-1, 1, (ar, ac))
+    b = np.asfortranarray(np.full((ldb, bc), -999.0)); b[:br] = rng.uniform(-1, 1, (br, bc))
+    c = np.asfortranarray(np.full((ldc, n), -777.0)); c[:m] = rng.uniform(-1, 1, (m, n))
+    a, b, c = (np.asfortranarray(x.astype(dtype)) for x in (a, b, c))
+    c0 = c.copy(order="F")
+    A = a[:ar, :ac].astype(np.float64); A = A if ta == "N" else A.T
+    B = b[:br, :bc].astype(np.float64); B = B if tb == "N" else B.T
+    ref = 0.75 * (A @ B) - 0.5 * c0[:m].astype(np.float64)
+    fn = blas.dgemm if dtype == np.float64 else blas.sgemm
+    fn(ta, tb, m, n, k, 0.75, a, lda, b, ldb, -0.5, c, ldc)
+    u = U64 if dtype == np.float64 else U32
+    bound = 4 * k * u * (0.75 * (np.abs(A) @ np.abs(B)) + 0.5 * np.abs(c0[:m].astype(np.float64)))
+    assert np.all(np.abs(c[:m].astype(np.float64) - ref) <= bound)
+    assert np.array_equal(c[m:], c0[m:]), "padding rows of C were written"
+
+
+def test_host_column_panel_injected_sync_error_leaves_c_unchanged(blas):
+    """An error reported before the first panel's download leaves all of C untouched."""
+    rng = np.random.default_rng(3)
+    m, n, k = 512, 2048, 4096
+    a = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    c = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    c0 = c.copy(order="F")
+    blas.inject_fault(2, 700)
+    blas.dgemm("N", "N", m, n, k, 1.0, a, m, b, k, 0.5, c, m)
+    assert np.array_equal(c, c0)
+    blas.dgemm("N", "N", m, n, k, 1.0, a, m, b, k, 0.5, c, m)  # works again
+    assert np.abs(c - (a @ b + 0.5 * c0)).max() <= 1e-11 * k

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/zynum_blas_gpu.h"
 #include "kernels.h"
@@ -129,6 +130,102 @@ cudaError_t run_sgemm(const GemmArgsF32& g, cudaStream_t st, Scratch scratch) {
 cudaError_t run_gemm(const GemmArgsF64& g, cudaStream_t st, HostScratch s) { return run_dgemm(g, st, s); }
 cudaError_t run_gemm(const GemmArgsF32& g, cudaStream_t st, HostScratch s) { return run_sgemm(g, st, s); }
 
+// Large host GEMMs run as column panels of C over three streams: the upload
+// stream copies A and then, panel by panel, B (and C when beta != 0); the
+// compute stream runs a panel's GEMM once its inputs are in; each C panel is
+// downloaded on the download stream as soon as the host has seen its GEMM
+// finish without error.  Uploads, products and downloads of different panels
+// overlap (the link is full duplex).  Every device buffer is reserved before
+// the first copy; a GPU error in panel j leaves panels 0 .. j-1 of C holding
+// their final values and the rest of C untouched.
+constexpr double kPanelMinFlops = 8.0e9;  // 2 m n k
+
+size_t real_scratch_bytes(int m, int n, int k, double*);
+size_t real_scratch_bytes(int m, int n, int k, float*);
+
+int host_panel_count(int m, int n, int k) {
+    if (n < 2048 || 2.0 * m * (double)n * k < kPanelMinFlops) return 1;
+    return std::min(8, std::max(2, n / 2048));
+}
+
+template <typename T>
+void host_gemm_panels(const char* routine, Context& cx, int panels, char ta, char tb, int m, int n, int k, T alpha,
+                      const T* a, int lda, const T* b, int ldb, T beta, T* c, int ldc, T* da, T* db, T* dc) {
+    const cudaStream_t st = cx.stream, up = cx.stream_in, down = cx.stream_out;
+    const int ra = (ta == 'N') ? m : k, ca = (ta == 'N') ? k : m;
+    const int rb = (tb == 'N') ? k : n;
+    const size_t es = sizeof(T);
+    const int nb = ((n + panels - 1) / panels + 255) / 256 * 256;
+    panels = (n + nb - 1) / nb;
+    cudaError_t e = cx.reserve(cx.work, real_scratch_bytes(m, nb, k, (T*)nullptr), st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    std::vector<cudaEvent_t> ev(2 * panels, nullptr);
+    auto release = [&]() {
+        cudaStreamSynchronize(up);
+        cudaStreamSynchronize(st);
+        cudaStreamSynchronize(down);
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    };
+    for (auto& x : ev)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+    // uploads: A, then per panel op(B)[:, j0:j1] (and C[:, j0:j1]); in_j after panel j
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice,
+                              up);
+    for (int j = 0; j < panels && e == cudaSuccess; ++j) {
+        const int j0 = j * nb, w = std::min(nb, n - j0);
+        if (tb == 'N')  // B is k x n: columns j0 .. j0 + w
+            e = cudaMemcpy2DAsync(db + (long)j0 * rb, (size_t)rb * es, b + (long)j0 * ldb, (size_t)ldb * es,
+                                  (size_t)rb * es, w, cudaMemcpyHostToDevice, up);
+        else  // B is n x k: rows j0 .. j0 + w
+            e = cudaMemcpy2DAsync(db + j0, (size_t)rb * es, b + j0, (size_t)ldb * es, (size_t)w * es, k,
+                                  cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess && beta != T(0))
+            e = cudaMemcpy2DAsync(dc + (long)j0 * m, (size_t)m * es, c + (long)j0 * ldc, (size_t)ldc * es,
+                                  (size_t)m * es, w, cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * j], up);
+    }
+    // products
+    for (int j = 0; j < panels && e == cudaSuccess; ++j) {
+        const int j0 = j * nb, w = std::min(nb, n - j0);
+        e = cudaStreamWaitEvent(st, ev[2 * j], 0);
+        if (e != cudaSuccess) break;
+        const T* bj = (tb == 'N') ? db + (long)j0 * rb : db + j0;
+        GemmArgs<T> g{ta, tb, m, w, k, alpha, da, ra, bj, rb, beta, dc + (long)j0 * m, m};
+        if ((e = run_gemm(g, st, HostScratch{&cx})) == cudaSuccess) e = cudaEventRecord(ev[2 * j + 1], st);
+    }
+    if (e != cudaSuccess) {  // nothing of C was written yet
+        release();
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    // downloads, each after its panel is known to have finished without error
+    for (int j = 0; j < panels; ++j) {
+        const int j0 = j * nb, w = std::min(nb, n - j0);
+        if ((e = cx.wait_event(ev[2 * j + 1])) != cudaSuccess) {
+            release();
+            cuda_status(e, "GPU execution");
+            report_gpu_failure(routine);
+            return;
+        }
+        e = cudaMemcpy2DAsync(c + (long)j0 * ldc, (size_t)ldc * es, dc + (long)j0 * m, (size_t)m * es,
+                              (size_t)m * es, w, cudaMemcpyDeviceToHost, down);
+        if (e != cudaSuccess) break;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(down);
+    release();
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
 // Host-pointer GEMM: stage -> compute -> copy the C window back.
 template <typename T>
 void host_gemm(const char* routine, char ta, char tb, int m, int n, int k, T alpha, const T* a, int lda, const T* b,
@@ -164,6 +261,11 @@ void host_gemm(const char* routine, char ta, char tb, int m, int n, int k, T alp
     T* da = static_cast<T*>(cx.stage_a.ptr);
     T* db = static_cast<T*>(cx.stage_b.ptr);
     T* dc = static_cast<T*>(cx.stage_c.ptr);
+    const int panels = quick ? 1 : host_panel_count(m, n, k);
+    if (panels > 1) {
+        host_gemm_panels<T>(routine, cx, panels, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, da, db, dc);
+        return;
+    }
     if (!quick) {
         e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)

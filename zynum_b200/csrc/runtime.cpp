@@ -113,6 +113,8 @@ cudaError_t Context::init() {
     }
     sm_count = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_out, cudaStreamNonBlocking);
     if (e != cudaSuccess) return e;
     dgemm_method = parse_method_env();
     sgemm_method = parse_smethod_env();
@@ -137,8 +139,12 @@ void Context::shutdown() {
         kv.second.release();
     }
     stream_work.clear();
+    cudaStreamSynchronize(stream_in);
+    cudaStreamSynchronize(stream_out);
     cudaStreamDestroy(stream);
-    stream = nullptr;
+    cudaStreamDestroy(stream_in);
+    cudaStreamDestroy(stream_out);
+    stream = stream_in = stream_out = nullptr;
     initialised = false;
 }
 
@@ -166,6 +172,16 @@ cudaError_t Context::sync(cudaStream_t s) {
         return e;
     }
     return cudaStreamSynchronize(s);
+}
+
+cudaError_t Context::wait_event(cudaEvent_t ev) {
+    if (faults.fail_next_sync) {
+        cudaError_t e = static_cast<cudaError_t>(faults.fail_next_sync);
+        faults.fail_next_sync = 0;
+        cudaEventSynchronize(ev);
+        return e;
+    }
+    return cudaEventSynchronize(ev);
 }
 
 namespace {

@@ -44,6 +44,8 @@ struct Context {
     int device = -1;
     int sm_count = 148;
     cudaStream_t stream = nullptr;  // stream of the host (Fortran / CBLAS) entry points
+    // Upload / download streams of the column-panel pipeline of large host GEMMs.
+    cudaStream_t stream_in = nullptr, stream_out = nullptr;
     std::recursive_mutex mutex;     // host entry points are callable from any thread
     DeviceBuffer stage_a, stage_b, stage_c;
     DeviceBuffer work;  // scratch of the host entry points (split-K partials, slices)
@@ -64,6 +66,8 @@ struct Context {
     cudaError_t stream_scratch(cudaStream_t stream, size_t bytes, void** out);
     cudaError_t reserve(DeviceBuffer& buf, size_t bytes, cudaStream_t stream);
     cudaError_t sync(cudaStream_t stream);
+    // Host wait for an event; reports an injected synchronisation error like sync().
+    cudaError_t wait_event(cudaEvent_t ev);
 };
 
 Context& context();
