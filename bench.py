@@ -668,6 +668,27 @@ def suite_level3(args):
             if old is not None:
                 blas.set_dgemm_method(old)
         del A, B, C, X
+    # the differentiation chain's shapes: TRSM L 4096 x 4096 with 512 right-hand sides, SYRK 512 x 4096
+    for mname, mval in (("native", blas.METHOD_NATIVE), ("auto", blas.METHOD_AUTO)):
+        old = blas.set_dgemm_method(mval)
+        g = torch.Generator(device="cuda").manual_seed(11)
+        nn, r = 4096, 512
+        L = torch.tril(torch.randn((nn, nn), generator=g, device="cuda", dtype=torch.float64) / nn ** 0.5, -1)
+        L += torch.diag(1 + torch.randn(nn, generator=g, device="cuda", dtype=torch.float64).abs())
+        Lc = L.t().contiguous()  # column-major storage of L
+        B = torch.randn((r, nn), generator=g, device="cuda", dtype=torch.float64)  # column-major 4096 x 512
+        X = B.clone()
+        C = torch.zeros((r, r), device="cuda", dtype=torch.float64)
+        fn = lambda: (X.copy_(B), blas.dtrsm_device("L", "L", "N", "N", nn, r, 1.0, Lc, nn, X, nn))  # noqa: E731
+        ms = time_device(torch, fn, 10, 3, stream) - time_device(torch, lambda: X.copy_(B), 10, 3, stream)
+        rows.append({"op": "trsm_4096x512", "dtype": "f64", "method": mname, "ms": ms,
+                     "tflops": float(nn) ** 2 * r / (ms * 1e-3) / 1e12})
+        fn = lambda: blas.dsyrk_device("L", "T", r, nn, 1.0, X, nn, 0.0, C, r)  # noqa: E731
+        ms = time_device(torch, fn, 10, 3, stream)
+        rows.append({"op": "syrk_512x4096", "dtype": "f64", "method": mname, "ms": ms,
+                     "tflops": float(r) * r * nn / (ms * 1e-3) / 1e12})
+        blas.set_dgemm_method(old)
+        del L, Lc, B, X, C
     print(json.dumps({"suite": "level3", "rows": rows}), flush=True)
     return 0
 

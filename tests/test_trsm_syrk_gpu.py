@@ -43,6 +43,44 @@ def test_dtrsm_all_cases(blas, oracle, side, uplo, trans, diag):
     assert np.array_equal(b[m:], b0[m:])
 
 
+@pytest.mark.parametrize("side,uplo,trans,diag", list(itertools.product("LR", "UL", "NT", "NU")))
+def test_dtrsm_multi_leaf(blas, oracle, side, uplo, trans, diag):
+    """Orders of 700 cross three 256-row leaves (the last one partial, with a partial 64-block);
+    45 right-hand sides leave the last 16-column group of each leaf launch partial."""
+    rng = np.random.default_rng(int.from_bytes((side + uplo + trans + diag).encode(), "little") % 2**32)
+    m, n = (700, 45) if side == "L" else (45, 700)
+    na = m if side == "L" else n
+    lda, ldb = na + 1, m + 3
+    # off-diagonals N(0, 1/na): well conditioned also with a unit diagonal at this order
+    a = rng.standard_normal((lda, na)) / np.sqrt(na)
+    for i in range(na):
+        a[i, i] = 2.0 + abs(a[i, i])
+    a[na:] = -999.0
+    a = np.asfortranarray(a)
+    b = np.asfortranarray(rng.standard_normal((ldb, n)))
+    b[m:] = -999.0
+    b0 = b.copy(order="F")
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, trans, diag, m, n, -1.5, a, lda, ref, ldb)
+    blas.trsm(side, uplo, trans, diag, m, n, -1.5, a, lda, b, ldb)
+    err = np.abs(b[:m] - ref[:m])
+    assert np.all(err <= 1e-11 * (1 + np.abs(ref[:m]))), float(err.max())
+    assert np.array_equal(b[m:], b0[m:])
+
+
+@pytest.mark.parametrize("side,uplo", [("L", "L"), ("R", "U"), ("L", "U"), ("R", "L")])
+def test_strsm_multi_leaf(blas, oracle, side, uplo):
+    rng = np.random.default_rng(4)
+    m, n = (530, 20) if side == "L" else (20, 530)
+    na = m if side == "L" else n
+    a = _tri_matrix(rng, na, na, np.float32)
+    b = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, "T", "N", m, n, 1.0, a, na, ref, m)
+    blas.trsm(side, uplo, "T", "N", m, n, 1.0, a, na, b, m)
+    assert np.all(np.abs(b - ref) <= 2e-4 * (1 + np.abs(ref)))
+
+
 @pytest.mark.parametrize("side,uplo", [("L", "L"), ("R", "U")])
 def test_strsm(blas, oracle, side, uplo):
     rng = np.random.default_rng(2)

@@ -280,6 +280,8 @@ cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* wor
             return run_tiles<128, 16, 32, 8, 4>(g, vec, used, k_chunk, workspace, st);
         case TILE_NARROW_M:  // m <= 16: 16 x 128 tiles, warps 1 x 8 of 16 x 16
             return run_tiles<16, 128, 16, 16, 4>(g, vec, used, k_chunk, workspace, st);
+        case TILE_64x64:  // few output tiles: 64 x 64 tiles, warps 2 x 2 of 32 x 32
+            return run_tiles<64, 64, 32, 32, 4>(g, vec, used, k_chunk, workspace, st);
         default:
             return run_tiles<128, 128, 64, 32, 4>(g, vec, used, k_chunk, workspace, st);
     }

@@ -35,7 +35,15 @@ using GemmArgsF32 = GemmArgs<float>;
 // TILE_NARROW_N / TILE_NARROW_M: n <= 16 / m <= 16 (the other side >= 512):
 // FP64 128 x 16 / 16 x 128 DMMA tiles, FP32 the narrow FFMA kernel (HBM-bound;
 // a 64- or 128-wide tile would be compute-bound on padding).
-enum TileShape : int { TILE_128x128 = 0, TILE_128x64 = 1, TILE_GEMV = 2, TILE_NARROW_N = 3, TILE_NARROW_M = 4 };
+// TILE_64x64: FP64 products whose 128 x 128 tiles would leave most SMs idle.
+enum TileShape : int {
+    TILE_128x128 = 0,
+    TILE_128x64 = 1,
+    TILE_GEMV = 2,
+    TILE_NARROW_N = 3,
+    TILE_NARROW_M = 4,
+    TILE_64x64 = 5
+};
 
 // What the planner decided for one native GEMM call.
 struct GemmPlan {

@@ -8,8 +8,10 @@
 //   updates with alpha = -1, beta = 1 at :344/:365).
 //   GPU algorithm: all 64 x 64 diagonal blocks of op(A) are inverted in one
 //   launch (tri_inv_blocks, exact substitution per column in shared memory);
-//   then, block by block in solve order, X_J = inv(A_JJ) B_J and the trailing
-//   update B_rest -= op(A)_rest,J X_J are GEMMs on the native (or Ozaki) tiles.
+//   the order is halved recursively on 256-row boundaries, the halves coupled
+//   by GEMMs on the native (or Ozaki) tiles (B_rest -= op(A)_rest,J X_J), and
+//   each 256-row leaf is solved in place by one trsm_leaf launch (inverted
+//   64-blocks and the leaf's own off-diagonal blocks applied in shared memory).
 //
 // SYRK  C := alpha * op(A) op(A)^T + beta * C on one triangle
 //   Reference: core/matrix_matrix/symmetric.zig:237 syrk / runSyrkColumns :180
@@ -98,6 +100,215 @@ __global__ void __launch_bounds__(kNB) tri_inv_blocks(const T* __restrict__ a, l
     __syncthreads();
     T* o = out + (long)blockIdx.x * kNB * kNB;
     for (int r = 0; r < kNB; ++r) o[r + (long)j * kNB] = X[r][j];
+}
+
+// One TRSM leaf of up to kLeaf rows (up to four diagonal 64-blocks), solved in
+// place for the 16 right-hand sides of this CTA: M Y = Z, where for side L
+// M = op(A)[p0.., p0..] and Z = B[p0.., c0 .. c0+15]; for side R (X op(A) = B,
+// i.e. op(A)^T X^T = B^T) M = op(A)[p0.., p0..]^T and Z = B[c0 .. c0+15, p0..]^T.
+// Z lives in shared memory; step by step (forward for a lower M, backward for
+// an upper one) Y_s = inv(M_ss) Z_s with the inverted 64-block of op(A) (read
+// transposed for side R), then Z_t -= M_ts Y_s for the later blocks t of the
+// leaf.  Each thread owns 4 rows x 1 column of a 64 x 16 block.
+constexpr int kLeaf = 256;
+constexpr int kLeafCols = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+trsm_leaf(const T* __restrict__ a, long lda, int trans_n, int left, int fwd, const T* __restrict__ inv, int p0,
+          int len, T* __restrict__ b, long ldb, int ncols) {
+    extern __shared__ __align__(16) unsigned char leaf_smem[];
+    T(*Z)[kLeafCols + 1] = reinterpret_cast<T(*)[kLeafCols + 1]>(leaf_smem);
+    T(*W)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(leaf_smem + sizeof(T) * kLeaf * (kLeafCols + 1));
+    const int t = threadIdx.x;
+    const int c0 = blockIdx.x * kLeafCols;
+    const int nc = min(kLeafCols, ncols - c0);
+    // Z(r, c): side L b[(p0 + r) + (c0 + c) ldb], side R b[(c0 + c) + (p0 + r) ldb]
+    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
+        const int r = left ? idx % kLeaf : idx / kLeafCols, c = left ? idx / kLeaf : idx % kLeafCols;
+        T v = T(0);
+        if (r < len && c < nc)
+            v = left ? b[(p0 + r) + (long)(c0 + c) * ldb] : b[(c0 + c) + (long)(p0 + r) * ldb];
+        Z[r][c] = v;
+    }
+    // M(i, j) = op(A)(p0 + i, p0 + j) (side L) or op(A)(p0 + j, p0 + i) (side R); op(A)(r, c) is
+    // a[r + c lda] for trans N, a[c + r lda] otherwise; the storage row is contiguous
+    const bool i_contig = (left != 0) == (trans_n != 0);
+    auto load_m = [&](int bt, int bs) {  // W = M[bt*64 .., bs*64 ..], zero outside the leaf
+        for (int idx = t; idx < kNB * kNB; idx += 256) {
+            const int i = i_contig ? idx % kNB : idx / kNB, j = i_contig ? idx / kNB : idx % kNB;
+            const int gi = bt * kNB + i, gj = bs * kNB + j;
+            T v = T(0);
+            if (gi < len && gj < len) {
+                const int r = left ? p0 + gi : p0 + gj, c = left ? p0 + gj : p0 + gi;
+                v = trans_n ? a[r + (long)c * lda] : a[c + (long)r * lda];
+            }
+            W[i][j] = v;
+        }
+    };
+    const int nsb = (len + kNB - 1) / kNB;
+    const int c = t & (kLeafCols - 1), rg = (t >> 4) * 4;  // 4 rows rg .. rg+3 of a 64-block, column c
+    for (int step = 0; step < nsb; ++step) {
+        const int sb = fwd ? step : nsb - 1 - step;
+        const T* ib = inv + (long)(p0 / kNB + sb) * kNB * kNB;
+        __syncthreads();
+        for (int idx = t; idx < kNB * kNB; idx += 256) {  // W = inv(M_ss): inv block, transposed for side R
+            const int i = idx % kNB, j = idx / kNB;
+            W[i][j] = left ? ib[i + j * kNB] : ib[j + i * kNB];
+        }
+        __syncthreads();
+        T y[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) y[u] = T(0);
+        for (int q = 0; q < kNB; ++q) {
+            const T z = Z[sb * kNB + q][c];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) y[u] = fma(W[rg + u][q], z, y[u]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) Z[sb * kNB + rg + u][c] = y[u];
+        for (int o = 1; o < nsb; ++o) {  // the later blocks of the solve order
+            const int tb = fwd ? sb + o : sb - o;
+            if (tb < 0 || tb >= nsb) break;
+            __syncthreads();
+            load_m(tb, sb);
+            __syncthreads();
+            T acc[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[u] = Z[tb * kNB + rg + u][c];
+            for (int q = 0; q < kNB; ++q) {
+                const T z = Z[sb * kNB + q][c];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u] = fma(-W[rg + u][q], z, acc[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) Z[tb * kNB + rg + u][c] = acc[u];
+        }
+    }
+    __syncthreads();
+    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
+        const int r = left ? idx % kLeaf : idx / kLeafCols, cc = left ? idx / kLeaf : idx % kLeafCols;
+        if (r < len && cc < nc) {
+            if (left)
+                b[(p0 + r) + (long)(c0 + cc) * ldb] = Z[r][cc];
+            else
+                b[(c0 + cc) + (long)(p0 + r) * ldb] = Z[r][cc];
+        }
+    }
+}
+
+// FP64 TRSM leaf on the tensor pipe: the same solve as trsm_leaf, with each
+// 64 x 64 by 64 x 16 product as one 16 x 8 DMMA tile per warp (8 warps) and
+// the 64 x 64 operand of every phase (an inverted diagonal block, then the
+// leaf's off-diagonal blocks in solve order) staged by cp.async into one of two
+// shared buffers while the previous phase computes.
+__device__ __forceinline__ void leaf_phase(int p, int nsb, int fwd, int* kind, int* tb, int* sb) {
+    // phase order: step s solves block sb(s) (kind 0) and then updates each later block (kind 1)
+    int q = p;
+    for (int step = 0; step < nsb; ++step) {
+        const int b = fwd ? step : nsb - 1 - step;
+        const int later = nsb - 1 - step;
+        if (q == 0) {
+            *kind = 0, *tb = b, *sb = b;
+            return;
+        }
+        --q;
+        if (q < later) {
+            *kind = 1, *sb = b, *tb = fwd ? b + 1 + q : b - 1 - q;
+            return;
+        }
+        q -= later;
+    }
+    *kind = 0, *tb = 0, *sb = 0;
+}
+
+__global__ void __launch_bounds__(256)
+trsm_leaf_dmma(const double* __restrict__ a, long lda, int trans_n, int left, int fwd,
+               const double* __restrict__ inv, int p0, int len, double* __restrict__ b, long ldb, int ncols) {
+    extern __shared__ __align__(16) unsigned char leaf_smem[];
+    double(*Z)[kLeafCols + 1] = reinterpret_cast<double(*)[kLeafCols + 1]>(leaf_smem);
+    double(*Wb)[kNB][kNB + 1] =
+        reinterpret_cast<double(*)[kNB][kNB + 1]>(leaf_smem + sizeof(double) * kLeaf * (kLeafCols + 1));
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int g = lane >> 2, tq = lane & 3;
+    const int c0 = blockIdx.x * kLeafCols;
+    const int nc = min(kLeafCols, ncols - c0);
+    const bool i_contig = (left != 0) == (trans_n != 0);
+    const int nsb = (len + kNB - 1) / kNB;
+    const int nphase = nsb + nsb * (nsb - 1) / 2;
+    // stage phase p's operand into buffer p & 1 (element copies: any layout, zero outside the leaf)
+    auto stage = [&](int p) {
+        int kind, tb, sb;
+        leaf_phase(p, nsb, fwd, &kind, &tb, &sb);
+        double(*W)[kNB + 1] = Wb[p & 1];
+        const double* ib = inv + (long)(p0 / kNB + sb) * kNB * kNB;
+        for (int idx = t; idx < kNB * kNB; idx += 256) {
+            int i, j;
+            const double* src;
+            bool ok;
+            if (kind == 0) {  // inv(M_ss): the inverted block of op(A), transposed for side R
+                i = idx % kNB, j = idx / kNB;
+                src = left ? ib + i + j * kNB : ib + j + i * kNB;
+                ok = true;
+            } else {
+                i = i_contig ? idx % kNB : idx / kNB, j = i_contig ? idx / kNB : idx % kNB;
+                const int gi = tb * kNB + i, gj = sb * kNB + j;
+                ok = gi < len && gj < len;
+                const int r = left ? p0 + gi : p0 + gj, c = left ? p0 + gj : p0 + gi;
+                src = trans_n ? a + r + (long)c * lda : a + c + (long)r * lda;
+            }
+            cp_async_8(smem_u32(&W[i][j]), ok ? src : a, ok ? 8 : 0);
+        }
+    };
+    stage(0);
+    cp_async_commit();
+    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
+        const int r = left ? idx % kLeaf : idx / kLeafCols, c = left ? idx / kLeaf : idx % kLeafCols;
+        double v = 0.0;
+        if (r < len && c < nc)
+            v = left ? b[(p0 + r) + (long)(c0 + c) * ldb] : b[(c0 + c) + (long)(p0 + r) * ldb];
+        Z[r][c] = v;
+    }
+    const int rt = warp >> 1, ct = warp & 1;  // this warp's 16 x 8 output tile
+    for (int p = 0; p < nphase; ++p) {
+        if (p + 1 < nphase) stage(p + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        int kind, tb, sb;
+        leaf_phase(p, nsb, fwd, &kind, &tb, &sb);
+        double(*W)[kNB + 1] = Wb[p & 1];
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int kb = 0; kb < kNB / 8; ++kb) {
+            double af[4], bf[2];
+#pragma unroll
+            for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+                for (int v0 = 0; v0 < 2; ++v0) af[v0 + 2 * v1] = W[16 * rt + g + 8 * v0][8 * kb + tq + 4 * v1];
+#pragma unroll
+            for (int v = 0; v < 2; ++v) bf[v] = Z[sb * kNB + 8 * kb + tq + 4 * v][8 * ct + g];
+            dmma_16x8x8(acc, af, bf);
+        }
+        if (kind == 0) __syncthreads();  // every warp has read Z_s before it is overwritten
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int row = tb * kNB + 16 * rt + g + 8 * (v >> 1), col = 8 * ct + 2 * tq + (v & 1);
+            Z[row][col] = kind == 0 ? acc[v] : Z[row][col] - acc[v];
+        }
+        __syncthreads();  // buffer p & 1 is free and Z is complete before the next phase
+    }
+    cp_async_wait<0>();
+    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
+        const int r = left ? idx % kLeaf : idx / kLeafCols, cc = left ? idx / kLeaf : idx % kLeafCols;
+        if (r < len && cc < nc) {
+            if (left)
+                b[(p0 + r) + (long)(c0 + cc) * ldb] = Z[r][cc];
+            else
+                b[(c0 + cc) + (long)(p0 + r) * ldb] = Z[r][cc];
+        }
+    }
 }
 
 // B := alpha B on the m x n window (plain product, like the reference's
@@ -325,8 +536,9 @@ template <typename T>
 size_t trsm_plane_bytes(char side, int m, int n) {
     const int na = (side == 'L') ? m : n;
     const long nblk = (na + kNB - 1) / kNB;
-    const long w = (side == 'L') ? (long)kNB * n : (long)m * kNB;
-    return ((size_t)(nblk * kNB * kNB + w) * sizeof(T) + 1023) & ~size_t(1023);
+    (void)m;
+    (void)n;
+    return ((size_t)(nblk * kNB * kNB) * sizeof(T) + 1023) & ~size_t(1023);
 }
 
 template <typename T>
@@ -342,7 +554,6 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     const int na = left ? m : n;
     const int nblk = (na + kNB - 1) / kNB;
     T* inv = static_cast<T*>(planes);
-    T* W = inv + (long)nblk * kNB * kNB;
     const int tri_smem = 2 * kNB * (kNB + 1) * (int)sizeof(T);
     if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) !=
         cudaSuccess)
@@ -357,26 +568,36 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     auto opa = [&](int r0, int c0) -> const T* {
         return (ta == 'N') ? t.a + r0 + (long)c0 * lda : t.a + c0 + (long)r0 * lda;
     };
-    // Recursive halving on 64-aligned boundaries: the two halves are solved
-    // recursively and coupled by one GEMM whose K is half the range, so most
-    // of the work runs as large GEMMs; 64-blocks use the inverted diagonal.
+    // Recursive halving on kLeaf-aligned boundaries: the two halves are solved
+    // recursively and coupled by one GEMM whose K is half the range, so most of
+    // the work runs as large GEMMs; each leaf of up to kLeaf rows is one
+    // trsm_leaf launch over the right-hand sides, in place.
+    constexpr bool kDmmaLeaf = sizeof(T) == 8;
+    const int leaf_smem =
+        (int)sizeof(T) * (kLeaf * (kLeafCols + 1) + (kDmmaLeaf ? 2 : 1) * kNB * (kNB + 1));
+    if constexpr (kDmmaLeaf)
+        e = ensure_dynamic_smem(trsm_leaf_dmma, leaf_smem);
+    else
+        e = ensure_dynamic_smem(trsm_leaf<T>, leaf_smem);
+    if (e != cudaSuccess) return e;
+    const int ncols = left ? n : m;
+    const int fwd = left ? !upper : upper;
     std::function<cudaError_t(int, int)> solve = [&](int p0, int p1) -> cudaError_t {
         cudaError_t err;
         const int len = p1 - p0;
-        if (len <= kNB) {
-            const T* invb = inv + (long)(p0 / kNB) * kNB * kNB;
-            if (left) {
-                if ((err = gemm({'N', 'N', len, n, len, T(1), invb, kNB, t.b + p0, ldb, T(0), W, len})) != cudaSuccess)
-                    return err;
-                return cudaMemcpy2DAsync(t.b + p0, ldb * sizeof(T), W, (size_t)len * sizeof(T), (size_t)len * sizeof(T),
-                                         n, cudaMemcpyDeviceToDevice, st);
-            }
-            T* bj = t.b + (long)p0 * ldb;
-            if ((err = gemm({'N', 'N', m, len, len, T(1), bj, ldb, invb, kNB, T(0), W, m})) != cudaSuccess) return err;
-            return cudaMemcpy2DAsync(bj, ldb * sizeof(T), W, (size_t)m * sizeof(T), (size_t)m * sizeof(T), len,
-                                     cudaMemcpyDeviceToDevice, st);
+        if (len <= kLeaf) {
+            const int grid = (ncols + kLeafCols - 1) / kLeafCols;
+            if constexpr (kDmmaLeaf)
+                trsm_leaf_dmma<<<grid, 256, leaf_smem, st>>>(reinterpret_cast<const double*>(t.a), lda, ta == 'N',
+                                                             left, fwd, reinterpret_cast<const double*>(inv), p0, len,
+                                                             reinterpret_cast<double*>(t.b), ldb, ncols);
+            else
+                trsm_leaf<T><<<grid, 256, leaf_smem, st>>>(t.a, lda, ta == 'N', left, fwd, inv, p0, len, t.b, ldb,
+                                                           ncols);
+            count_launch();
+            return cudaGetLastError();
         }
-        const int mid = p0 + ((len / 2 + kNB - 1) / kNB) * kNB;
+        const int mid = p0 + ((len / 2 + kLeaf - 1) / kLeaf) * kLeaf;
         const int h1 = mid - p0, h2 = p1 - mid;
         if (left) {
             if (!upper) {  // rows p0..mid first, then update mid..p1
