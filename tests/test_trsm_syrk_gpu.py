@@ -68,6 +68,28 @@ def test_dtrsm_multi_leaf(blas, oracle, side, uplo, trans, diag):
     assert np.array_equal(b[m:], b0[m:])
 
 
+@pytest.mark.parametrize("side,uplo,trans,diag", [("L", "L", "N", "N"), ("L", "U", "T", "U"), ("R", "U", "N", "N"),
+                                                   ("R", "L", "T", "U")])
+def test_dtrsm_wide_right_hand_sides(blas, oracle, side, uplo, trans, diag):
+    """More than 1024 right-hand sides: each leaf inverse is applied as a GEMM from a copy of the
+    leaf's rows (columns for side R)."""
+    rng = np.random.default_rng(int.from_bytes((side + uplo + trans + diag).encode(), "little") % 2**32)
+    m, n = (600, 1100) if side == "L" else (1100, 600)
+    na = m if side == "L" else n
+    a = rng.standard_normal((na, na)) / np.sqrt(na)
+    for i in range(na):
+        a[i, i] = 2.0 + abs(a[i, i])
+    a = np.asfortranarray(a)
+    b = np.asfortranarray(rng.standard_normal((m + 1, n)))
+    b0 = b.copy(order="F")
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, trans, diag, m, n, 0.5, a, na, ref, m + 1)
+    blas.trsm(side, uplo, trans, diag, m, n, 0.5, a, na, b, m + 1)
+    err = np.abs(b[:m] - ref[:m])
+    assert np.all(err <= 1e-11 * (1 + np.abs(ref[:m]))), float(err.max())
+    assert np.array_equal(b[m:], b0[m:])
+
+
 @pytest.mark.parametrize("side,uplo", [("L", "L"), ("R", "U"), ("L", "U"), ("R", "L")])
 def test_strsm_multi_leaf(blas, oracle, side, uplo):
     rng = np.random.default_rng(4)

@@ -198,70 +198,170 @@ trsm_leaf(const T* __restrict__ a, long lda, int trans_n, int left, int fwd, con
     }
 }
 
-// FP64 TRSM leaf on the tensor pipe: the same solve as trsm_leaf, with each
-// 64 x 64 by 64 x 16 product as one 16 x 8 DMMA tile per warp (8 warps) and
-// the 64 x 64 operand of every phase (an inverted diagonal block, then the
-// leaf's off-diagonal blocks in solve order) staged by cp.async into one of two
-// shared buffers while the previous phase computes.
-__device__ __forceinline__ void leaf_phase(int p, int nsb, int fwd, int* kind, int* tb, int* sb) {
-    // phase order: step s solves block sb(s) (kind 0) and then updates each later block (kind 1)
-    int q = p;
-    for (int step = 0; step < nsb; ++step) {
-        const int b = fwd ? step : nsb - 1 - step;
-        const int later = nsb - 1 - step;
-        if (q == 0) {
-            *kind = 0, *tb = b, *sb = b;
-            return;
-        }
-        --q;
-        if (q < later) {
-            *kind = 1, *sb = b, *tb = fwd ? b + 1 + q : b - 1 - q;
-            return;
-        }
-        q -= later;
+// FP64 TRSM leaves through their inverses.  tri_inv_leaf turns the inverted
+// 64-blocks into the full inverse of every kLeaf-row diagonal block of op(A)
+// (one launch for all leaves, off the solve's critical chain); each leaf of
+// the solve is then one trsm_leaf_apply launch, Y = inv(M) Z, a single pass
+// of DMMA tiles with no dependent phases.
+constexpr int kStagePitch = kNB + 2;  // 66 doubles: 16-byte aligned shared rows
+
+// Stage the 64 x 64 block whose element (r, c) sits at base[r * sr + c * sc],
+// exactly one of sr / sc being 1, into W with the contiguous index innermost
+// (W[c][r] when sr == 1, W[r][c] otherwise) by 16-byte cp.async; elements with
+// r >= rlim or c >= clim are zero.  Needs base, the other stride and the
+// shared rows 16-byte aligned.
+ZB_DEVICE void stage_block(double (*W)[kStagePitch], const double* base, long sr, long sc, int rlim, int clim,
+                           const double* dummy) {
+    const bool rfast = sr == 1;
+    const long ld = rfast ? sc : sr;
+    const int lim_in = rfast ? rlim : clim, lim_out = rfast ? clim : rlim;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        const int q = it * 256 + threadIdx.x;
+        const int inner = (q & 31) * 2, outer = q >> 5;
+        const int valid = outer < lim_out ? max(0, min(2, lim_in - inner)) : 0;
+        const double* src = valid ? base + inner + (long)outer * ld : dummy;
+        cp_async_16(smem_u32(&W[outer][inner]), src, valid * 8);
     }
-    *kind = 0, *tb = 0, *sb = 0;
 }
 
-__global__ void __launch_bounds__(256)
-trsm_leaf_dmma(const double* __restrict__ a, long lda, int trans_n, int left, int fwd,
-               const double* __restrict__ inv, int p0, int len, double* __restrict__ b, long ldb, int ncols) {
-    extern __shared__ __align__(16) unsigned char leaf_smem[];
-    double(*Z)[kLeafCols + 1] = reinterpret_cast<double(*)[kLeafCols + 1]>(leaf_smem);
-    double(*Wb)[kNB][kNB + 1] =
-        reinterpret_cast<double(*)[kNB][kNB + 1]>(leaf_smem + sizeof(double) * kLeaf * (kLeafCols + 1));
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int g = lane >> 2, tq = lane & 3;
-    const int c0 = blockIdx.x * kLeafCols;
-    const int nc = min(kLeafCols, ncols - c0);
-    const bool i_contig = (left != 0) == (trans_n != 0);
-    const int nsb = (len + kNB - 1) / kNB;
-    const int nphase = nsb + nsb * (nsb - 1) / 2;
-    // stage phase p's operand into buffer p & 1 (element copies: any layout, zero outside the leaf)
-    auto stage = [&](int p) {
-        int kind, tb, sb;
-        leaf_phase(p, nsb, fwd, &kind, &tb, &sb);
-        double(*W)[kNB + 1] = Wb[p & 1];
-        const double* ib = inv + (long)(p0 / kNB + sb) * kNB * kNB;
-        for (int idx = t; idx < kNB * kNB; idx += 256) {
-            int i, j;
-            const double* src;
-            bool ok;
-            if (kind == 0) {  // inv(M_ss): the inverted block of op(A), transposed for side R
-                i = idx % kNB, j = idx / kNB;
-                src = left ? ib + i + j * kNB : ib + j + i * kNB;
-                ok = true;
-            } else {
-                i = i_contig ? idx % kNB : idx / kNB, j = i_contig ? idx / kNB : idx % kNB;
-                const int gi = tb * kNB + i, gj = sb * kNB + j;
-                ok = gi < len && gj < len;
-                const int r = left ? p0 + gi : p0 + gj, c = left ? p0 + gj : p0 + gi;
-                src = trans_n ? a + r + (long)c * lda : a + c + (long)r * lda;
-            }
-            cp_async_8(smem_u32(&W[i][j]), ok ? src : a, ok ? 8 : 0);
+// element (r, c) of a block staged by stage_block
+ZB_DEVICE double staged(const double (*W)[kStagePitch], bool rfast, int r, int c) {
+    return rfast ? W[c][r] : W[r][c];
+}
+
+// acc[u] += A (64 x 64, staged) * B (64 x 64 in X[k][c]) for this warp's tiles:
+// row tile rt = warp / 2, column tiles 4 (warp % 2) + u.
+ZB_DEVICE void mma_64(double (&acc)[4][4], const double (*A)[kStagePitch], bool arfast, const double (*B)[kNB + 1]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tq = lane & 3, rt = warp >> 1, ct0 = (warp & 1) * 4;
+#pragma unroll
+    for (int kb = 0; kb < kNB / 8; ++kb) {
+        double af[4];
+#pragma unroll
+        for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+            for (int v0 = 0; v0 < 2; ++v0)
+                af[v0 + 2 * v1] = staged(A, arfast, 16 * rt + g + 8 * v0, 8 * kb + tq + 4 * v1);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            double bf[2];
+#pragma unroll
+            for (int v = 0; v < 2; ++v) bf[v] = B[8 * kb + tq + 4 * v][8 * (ct0 + u) + g];
+            dmma_16x8x8(acc[u], af, bf);
         }
-    };
-    stage(0);
+    }
+}
+
+// Block (leaf, j): column block j of the inverse of the diagonal kLeaf-block
+// `leaf` of op(A), written to inv_leaf + leaf kLeaf^2 (column-major, ld kLeaf;
+// zero outside the triangle and the leaf).  Lower op(A): X_jj = inv(A_jj),
+// X_ij = -inv(A_ii) sum_{k=j}^{i-1} A_ik X_kj for i = j+1, ...; upper op(A):
+// the same for i = j-1, ..., 0 with k = i+1 .. j.
+__global__ void __launch_bounds__(256)
+tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int na, const double* __restrict__ inv64,
+             double* __restrict__ inv_leaf) {
+    extern __shared__ __align__(16) unsigned char til_smem[];
+    double(*X)[kNB][kNB + 1] = reinterpret_cast<double(*)[kNB][kNB + 1]>(til_smem);
+    double(*S)[kStagePitch] =
+        reinterpret_cast<double(*)[kStagePitch]>(til_smem + sizeof(double) * 4 * kNB * (kNB + 1));
+    const int leaf = blockIdx.x, j = blockIdx.y, t = threadIdx.x;
+    const int P = leaf * kLeaf, len = min(kLeaf, na - P), nsb = (len + kNB - 1) / kNB;
+    double* out = inv_leaf + (long)leaf * kLeaf * kLeaf;
+    bool have[4] = {false, false, false, false};
+    if (j < nsb) {
+        // op(A)(r, c) = a[r + c lda] (trans N) or a[c + r lda]; block (bi, bk) of the leaf
+        const long sr = trans_n ? 1 : lda, sc = trans_n ? lda : 1;
+        auto ablock = [&](int bi, int bk) { return a + (long)(P + bi * kNB) * sr + (long)(P + bk * kNB) * sc; };
+        auto iblock = [&](int bi) { return inv64 + (long)(P / kNB + bi) * kNB * kNB; };
+        // X_jj = inv(A_jj)
+        stage_block(S, iblock(j), 1, kNB, kNB, kNB, inv64);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int q = t; q < kNB * kNB; q += 256) X[j][q % kNB][q / kNB] = staged(S, true, q % kNB, q / kNB);
+        have[j] = true;
+        const int lane = t & 31, warp = t >> 5, g = lane >> 2, tq = lane & 3, rt = warp >> 1, ct0 = (warp & 1) * 4;
+        for (int o = 1; o < nsb; ++o) {
+            const int i = upper ? j - o : j + o;
+            if (i < 0 || i >= nsb) break;
+            double acc[4][4] = {};
+            const int k0 = upper ? i + 1 : j, k1 = upper ? j : i - 1;
+            for (int k = k0; k <= k1; ++k) {  // acc += A_ik X_kj
+                __syncthreads();
+                stage_block(S, ablock(i, k), sr, sc, len - i * kNB, len - k * kNB, a);
+                cp_async_commit();
+                cp_async_wait<0>();
+                __syncthreads();
+                mma_64(acc, S, sr == 1, X[k]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 4; ++u)  // the sum into X[i], then X_ij = -inv(A_ii) * sum
+#pragma unroll
+                for (int v = 0; v < 4; ++v) X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = acc[u][v];
+            stage_block(S, iblock(i), 1, kNB, kNB, kNB, inv64);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+            double y[4][4] = {};
+            mma_64(y, S, true, X[i]);
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = -y[u][v];
+            have[i] = true;
+        }
+        __syncthreads();
+    }
+    // column block j of the leaf inverse: rows of computed blocks, zeros elsewhere
+    for (int q = t; q < kLeaf * kNB; q += 256) {
+        const int r = q % kLeaf, c = q / kLeaf, bi = r / kNB;
+        out[r + (long)(j * kNB + c) * kLeaf] = (j < nsb && have[bi]) ? X[bi][r % kNB][c] : 0.0;
+    }
+}
+
+// One leaf of the solve in place: Y = inv(M) Z, inv(M) = the leaf inverse
+// (side L) or its transpose (side R), Z = B[p0.., c..] (side L) or
+// B[c.., p0..]^T (side R).  A cluster of four CTAs takes 16 right-hand sides;
+// CTA r of the cluster computes output rows 64 r .. 64 r + 63 over the nonzero
+// K range of the triangular inverse.  Every CTA loads all of Z (the leaf's
+// rows are read by all four) and the cluster barrier orders those reads
+// before any CTA writes its rows back.  Warp w: row tile w / 2, column tile
+// w % 2, two accumulators.
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
+trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, int len, double* __restrict__ b,
+                long ldb, int ncols) {
+    extern __shared__ __align__(16) unsigned char ap_smem[];
+    double(*Z)[kLeafCols + 1] = reinterpret_cast<double(*)[kLeafCols + 1]>(ap_smem);
+    double* A = reinterpret_cast<double*>(ap_smem + sizeof(double) * kLeaf * (kLeafCols + 1));
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, g = lane >> 2, tq = lane & 3;
+    const int rb = (int)cluster_ctarank();
+    const int c0 = (blockIdx.x / 4) * kLeafCols, nc = min(kLeafCols, ncols - c0);
+    // nonzero K range of rows 64 rb .. of the (lower when fwd) inverse, within the leaf
+    const int kbeg = fwd ? 0 : kNB * rb, kend = min(len, fwd ? kNB * (rb + 1) : kLeaf);
+    const int klen = max(0, kend - kbeg);
+    const int klen8 = (klen + 7) & ~7;
+    // rows 64 rb + i, columns kbeg + kk of inv(M): side L inv[i' + k' kLeaf] (runs along i, staged
+    // [kk][i], pitch 66); side R inv[k' + i' kLeaf] (runs along kk, staged [i][kk], pitch kLeaf + 2)
+    if (64 * rb < len && klen > 0) {
+        if (left) {
+            for (int q = t; q < klen8 * (kNB / 2); q += 256) {
+                const int kk = q / (kNB / 2), i = (q % (kNB / 2)) * 2;
+                const bool ok = kk < klen;
+                cp_async_16(smem_u32(A + kk * kStagePitch + i),
+                            ok ? inv_leaf + (kNB * rb + i) + (long)(kbeg + kk) * kLeaf : inv_leaf, ok ? 16 : 0);
+            }
+        } else {
+            for (int q = t; q < kNB * (klen8 / 2); q += 256) {
+                const int i = q / (klen8 / 2), kk = (q % (klen8 / 2)) * 2;
+                const bool ok = kk < klen;
+                cp_async_16(smem_u32(A + i * (kLeaf + 2) + kk),
+                            ok ? inv_leaf + (kbeg + kk) + (long)(kNB * rb + i) * kLeaf : inv_leaf, ok ? 16 : 0);
+            }
+        }
+    }
     cp_async_commit();
     for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
         const int r = left ? idx % kLeaf : idx / kLeafCols, c = left ? idx / kLeaf : idx % kLeafCols;
@@ -270,43 +370,37 @@ trsm_leaf_dmma(const double* __restrict__ a, long lda, int trans_n, int left, in
             v = left ? b[(p0 + r) + (long)(c0 + c) * ldb] : b[(c0 + c) + (long)(p0 + r) * ldb];
         Z[r][c] = v;
     }
-    const int rt = warp >> 1, ct = warp & 1;  // this warp's 16 x 8 output tile
-    for (int p = 0; p < nphase; ++p) {
-        if (p + 1 < nphase) stage(p + 1);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        int kind, tb, sb;
-        leaf_phase(p, nsb, fwd, &kind, &tb, &sb);
-        double(*W)[kNB + 1] = Wb[p & 1];
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int kb = 0; kb < kNB / 8; ++kb) {
-            double af[4], bf[2];
-#pragma unroll
-            for (int v1 = 0; v1 < 2; ++v1)
-#pragma unroll
-                for (int v0 = 0; v0 < 2; ++v0) af[v0 + 2 * v1] = W[16 * rt + g + 8 * v0][8 * kb + tq + 4 * v1];
-#pragma unroll
-            for (int v = 0; v < 2; ++v) bf[v] = Z[sb * kNB + 8 * kb + tq + 4 * v][8 * ct + g];
-            dmma_16x8x8(acc, af, bf);
-        }
-        if (kind == 0) __syncthreads();  // every warp has read Z_s before it is overwritten
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int row = tb * kNB + 16 * rt + g + 8 * (v >> 1), col = 8 * ct + 2 * tq + (v & 1);
-            Z[row][col] = kind == 0 ? acc[v] : Z[row][col] - acc[v];
-        }
-        __syncthreads();  // buffer p & 1 is free and Z is complete before the next phase
-    }
+    cluster_sync();  // every CTA of the cluster has read its Z from B
     cp_async_wait<0>();
-    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
-        const int r = left ? idx % kLeaf : idx / kLeafCols, cc = left ? idx / kLeaf : idx % kLeafCols;
+    __syncthreads();
+    if (64 * rb >= len) return;
+    const int rt = warp >> 1, ct = warp & 1;
+    double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int kb = 0; kb < klen8 / 8; ++kb) {
+        double af[4], bf[2];
+#pragma unroll
+        for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+            for (int v0 = 0; v0 < 2; ++v0) {
+                const int i = 16 * rt + g + 8 * v0, kk = 8 * kb + tq + 4 * v1;
+                af[v0 + 2 * v1] = left ? A[kk * kStagePitch + i] : A[i * (kLeaf + 2) + kk];
+            }
+#pragma unroll
+        for (int v = 0; v < 2; ++v) bf[v] = Z[kbeg + 8 * kb + tq + 4 * v][8 * ct + g];
+        if (kb & 1)
+            dmma_16x8x8(acc1, af, bf);
+        else
+            dmma_16x8x8(acc0, af, bf);
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int r = kNB * rb + 16 * rt + g + 8 * (v >> 1), cc = 8 * ct + 2 * tq + (v & 1);
         if (r < len && cc < nc) {
+            const double y = acc0[v] + acc1[v];
             if (left)
-                b[(p0 + r) + (long)(c0 + cc) * ldb] = Z[r][cc];
+                b[(p0 + r) + (long)(c0 + cc) * ldb] = y;
             else
-                b[(c0 + cc) + (long)(p0 + r) * ldb] = Z[r][cc];
+                b[(c0 + cc) + (long)(p0 + r) * ldb] = y;
         }
     }
 }
@@ -532,13 +626,28 @@ cudaError_t symmetrize_matrix(char uplo, int n, T* c, long ldc, cudaStream_t st)
 template cudaError_t symmetrize_matrix<double>(char, int, double*, long, cudaStream_t);
 template cudaError_t symmetrize_matrix<float>(char, int, float*, long, cudaStream_t);
 
+// inverted 64-blocks, then (FP64) the kLeaf-block inverses
+template <typename T>
+size_t inv_plane_bytes(int na) {
+    const long nblk = (na + kNB - 1) / kNB;
+    return ((size_t)(nblk * kNB * kNB) * sizeof(T) + 1023) & ~size_t(1023);
+}
+
+// Wider right-hand-side sets apply each leaf inverse as a GEMM from a copy of
+// the leaf's rows (columns for side R) instead of the cluster kernel.
+constexpr int kApplyMaxCols = 1024;
+
+template <typename T>
+size_t leaf_plane_bytes(int na) {
+    const long nleaf = (na + kLeaf - 1) / kLeaf;
+    return sizeof(T) == 8 ? (((size_t)nleaf * kLeaf * kLeaf * sizeof(T) + 1023) & ~size_t(1023)) : 0;
+}
+
 template <typename T>
 size_t trsm_plane_bytes(char side, int m, int n) {
-    const int na = (side == 'L') ? m : n;
-    const long nblk = (na + kNB - 1) / kNB;
-    (void)m;
-    (void)n;
-    return ((size_t)(nblk * kNB * kNB) * sizeof(T) + 1023) & ~size_t(1023);
+    const int na = (side == 'L') ? m : n, ncols = (side == 'L') ? n : m;
+    const size_t copy = (sizeof(T) == 8 && ncols > kApplyMaxCols) ? (size_t)kLeaf * ncols * sizeof(T) : 0;
+    return inv_plane_bytes<T>(na) + leaf_plane_bytes<T>(na) + copy;
 }
 
 template <typename T>
@@ -570,27 +679,59 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     };
     // Recursive halving on kLeaf-aligned boundaries: the two halves are solved
     // recursively and coupled by one GEMM whose K is half the range, so most of
-    // the work runs as large GEMMs; each leaf of up to kLeaf rows is one
-    // trsm_leaf launch over the right-hand sides, in place.
-    constexpr bool kDmmaLeaf = sizeof(T) == 8;
-    const int leaf_smem =
-        (int)sizeof(T) * (kLeaf * (kLeafCols + 1) + (kDmmaLeaf ? 2 : 1) * kNB * (kNB + 1));
-    if constexpr (kDmmaLeaf)
-        e = ensure_dynamic_smem(trsm_leaf_dmma, leaf_smem);
-    else
-        e = ensure_dynamic_smem(trsm_leaf<T>, leaf_smem);
-    if (e != cudaSuccess) return e;
+    // the work runs as large GEMMs; each leaf of up to kLeaf rows is one launch
+    // over the right-hand sides, in place.  FP64 with a 16-byte aligned A and an
+    // even lda (16-byte operand copies) applies precomputed leaf inverses on
+    // the tensor pipe; otherwise trsm_leaf solves phase by phase.
+    const bool inv_leaves = sizeof(T) == 8 && reinterpret_cast<uintptr_t>(t.a) % 16 == 0 && t.lda % 2 == 0;
     const int ncols = left ? n : m;
     const int fwd = left ? !upper : upper;
+    int leaf_smem;
+    double* inv_leaf = nullptr;
+    if (inv_leaves) {
+        const int nleaf = (na + kLeaf - 1) / kLeaf;
+        inv_leaf = reinterpret_cast<double*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na));
+        const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + kNB * kStagePitch);
+        if ((e = ensure_dynamic_smem(tri_inv_leaf, til_smem)) != cudaSuccess) return e;
+        tri_inv_leaf<<<dim3(nleaf, kLeaf / kNB), 256, til_smem, st>>>(
+            reinterpret_cast<const double*>(t.a), lda, ta == 'N', upper, na, reinterpret_cast<const double*>(inv),
+            inv_leaf);
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        // Z plus 64 rows of the inverse over up to kLeaf columns (either staging layout)
+        constexpr int kRows = kLeaf * kStagePitch > kNB * (kLeaf + 2) ? kLeaf * kStagePitch : kNB * (kLeaf + 2);
+        leaf_smem = (int)sizeof(double) * (kLeaf * (kLeafCols + 1) + kRows);
+        e = ensure_dynamic_smem(trsm_leaf_apply, leaf_smem);
+    } else {
+        leaf_smem = (int)sizeof(T) * (kLeaf * (kLeafCols + 1) + kNB * (kNB + 1));
+        e = ensure_dynamic_smem(trsm_leaf<T>, leaf_smem);
+    }
+    if (e != cudaSuccess) return e;
     std::function<cudaError_t(int, int)> solve = [&](int p0, int p1) -> cudaError_t {
         cudaError_t err;
         const int len = p1 - p0;
         if (len <= kLeaf) {
             const int grid = (ncols + kLeafCols - 1) / kLeafCols;
-            if constexpr (kDmmaLeaf)
-                trsm_leaf_dmma<<<grid, 256, leaf_smem, st>>>(reinterpret_cast<const double*>(t.a), lda, ta == 'N',
-                                                             left, fwd, reinterpret_cast<const double*>(inv), p0, len,
-                                                             reinterpret_cast<double*>(t.b), ldb, ncols);
+            if (inv_leaves && ncols > kApplyMaxCols) {  // copy of the leaf's rows / columns, then one GEMM
+                const T* il = reinterpret_cast<const T*>(inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf);
+                T* W = reinterpret_cast<T*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na) +
+                                            leaf_plane_bytes<T>(na));
+                if (left) {
+                    if ((err = cudaMemcpy2DAsync(W, (size_t)len * sizeof(T), t.b + p0, ldb * sizeof(T),
+                                                 (size_t)len * sizeof(T), n, cudaMemcpyDeviceToDevice, st)) !=
+                        cudaSuccess)
+                        return err;
+                    return gemm({'N', 'N', len, n, len, T(1), il, kLeaf, W, len, T(0), t.b + p0, ldb});
+                }
+                if ((err = cudaMemcpy2DAsync(W, (size_t)m * sizeof(T), t.b + (long)p0 * ldb, ldb * sizeof(T),
+                                             (size_t)m * sizeof(T), len, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+                    return err;
+                return gemm({'N', 'N', m, len, len, T(1), W, m, il, kLeaf, T(0), t.b + (long)p0 * ldb, ldb});
+            }
+            if (inv_leaves)  // clusters of four CTAs per 16 right-hand sides
+                trsm_leaf_apply<<<4 * grid, 256, leaf_smem, st>>>(inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf, left,
+                                                                  fwd, p0, len, reinterpret_cast<double*>(t.b), ldb,
+                                                                  ncols);
             else
                 trsm_leaf<T><<<grid, 256, leaf_smem, st>>>(t.a, lda, ta == 'N', left, fwd, inv, p0, len, t.b, ldb,
                                                            ncols);
