@@ -65,41 +65,50 @@ ZB_DEVICE T op_tri(const T* a, long lda, char uplo, char trans, char diag, int r
 }
 
 // Block b: inverse of the diagonal block op(A)[b*64 .. , b*64 ..] of size
-// s <= 64, written column-major with ld 64 (zero outside s x s).  Thread j
-// solves op(A)_bb x = e_j by substitution.
+// s <= 64, written column-major with ld 64 (zero outside s x s).  Column j of
+// the inverse is solved by the four lanes of quad j % 8 of warp j / 8 (256
+// threads): for each row in solve order the lanes add every fourth term of
+// sum_q L[r][q] X[q][j], two shuffles combine them, and the row's reciprocal
+// diagonal (computed once per block) scales the result.
 template <typename T>
-__global__ void __launch_bounds__(kNB) tri_inv_blocks(const T* __restrict__ a, long lda, char uplo, char trans,
+__global__ void __launch_bounds__(256) tri_inv_blocks(const T* __restrict__ a, long lda, char uplo, char trans,
                                                       char diag, int n, T* __restrict__ out) {
-    extern __shared__ __align__(16) unsigned char tri_smem[];  // 2 x 64 x 65 elements
+    extern __shared__ __align__(16) unsigned char tri_smem[];  // 2 x 64 x 65 elements + 64 reciprocals
     T(*L)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(tri_smem);
     T(*X)[kNB + 1] = L + kNB;
+    T* dinv = reinterpret_cast<T*>(X + kNB);
     const int b0 = blockIdx.x * kNB;
     const int s = min(kNB, n - b0);
-    const int j = threadIdx.x;
-    for (int r = 0; r < kNB; ++r) {
-        L[r][j] = (r < s && j < s) ? op_tri(a, lda, uplo, trans, diag, b0 + r, b0 + j) : T(0);
-        X[r][j] = T(0);
+    const int t = threadIdx.x;
+    for (int q = t; q < kNB * kNB; q += 256) {
+        const int r = q % kNB, c = q / kNB;
+        L[r][c] = (r < s && c < s) ? op_tri(a, lda, uplo, trans, diag, b0 + r, b0 + c) : T(0);
+        X[r][c] = T(0);
     }
     __syncthreads();
+    if (t < kNB) dinv[t] = (t < s && diag != 'U') ? T(1) / L[t][t] : T(1);
+    __syncthreads();
     const bool upper = op_is_upper(uplo, trans);
-    if (j < s) {
-        if (!upper) {
-            for (int r = j; r < s; ++r) {
-                T v = (r == j) ? T(1) : T(0);
-                for (int q = j; q < r; ++q) v -= L[r][q] * X[q][j];
-                X[r][j] = (diag == 'U') ? v : v / L[r][r];
-            }
-        } else {
-            for (int r = j; r >= 0; --r) {
-                T v = (r == j) ? T(1) : T(0);
-                for (int q = r + 1; q <= j; ++q) v -= L[r][q] * X[q][j];
-                X[r][j] = (diag == 'U') ? v : v / L[r][r];
+    const int lane = t & 31, j = (t >> 5) * 8 + (lane >> 2), part = lane & 3;
+    for (int step = 0; step < kNB; ++step) {
+        const int r = upper ? kNB - 1 - step : step;
+        const bool active = j < s && r < s && (upper ? r <= j : r >= j);
+        T v = T(0);
+        if (active) {
+            if (!upper) {
+                for (int q = j + part; q < r; q += 4) v = fma(L[r][q], X[q][j], v);
+            } else {
+                for (int q = r + 1 + part; q <= j; q += 4) v = fma(L[r][q], X[q][j], v);
             }
         }
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        if (active && part == 0) X[r][j] = ((r == j ? T(1) : T(0)) - v) * dinv[r];
+        __syncwarp();
     }
     __syncthreads();
     T* o = out + (long)blockIdx.x * kNB * kNB;
-    for (int r = 0; r < kNB; ++r) o[r + (long)j * kNB] = X[r][j];
+    for (int q = t; q < kNB * kNB; q += 256) o[q] = X[q % kNB][q / kNB];
 }
 
 // One TRSM leaf of up to kLeaf rows (up to four diagonal 64-blocks), solved in
@@ -663,11 +672,9 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     const int na = left ? m : n;
     const int nblk = (na + kNB - 1) / kNB;
     T* inv = static_cast<T*>(planes);
-    const int tri_smem = 2 * kNB * (kNB + 1) * (int)sizeof(T);
-    if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) !=
-        cudaSuccess)
-        return e;
-    tri_inv_blocks<T><<<nblk, kNB, tri_smem, st>>>(t.a, t.lda, t.uplo, t.trans, t.diag, na, inv);
+    const int tri_smem = (2 * kNB * (kNB + 1) + kNB) * (int)sizeof(T);
+    if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) != cudaSuccess) return e;
+    tri_inv_blocks<T><<<nblk, 256, tri_smem, st>>>(t.a, t.lda, t.uplo, t.trans, t.diag, na, inv);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const bool upper = op_is_upper(t.uplo, t.trans);
