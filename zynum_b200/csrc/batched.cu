@@ -353,30 +353,50 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
         const T* A = a[q];
         T* B = b[q];
         const long la = lda[q], lb = ldb[q];
-        if (alpha != T(1))
-            for (long e = threadIdx.x; e < (long)n * r; e += kThreads) {
-                T* p = B + (e % n) + (e / n) * lb;
-                *p = alpha * *p;
+        if (alpha != T(1))  // eight loads in flight per thread before their stores
+            for (long e0 = threadIdx.x; e0 < (long)n * r; e0 += 8L * kThreads) {
+                T v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long e = e0 + (long)u * kThreads;
+                    v[u] = e < (long)n * r ? B[(e % n) + (e / n) * lb] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long e = e0 + (long)u * kThreads;
+                    if (e < (long)n * r) B[(e % n) + (e / n) * lb] = alpha * v[u];
+                }
             }
         __syncthreads();
         const int nblk = (n + kTB - 1) / kTB;
         for (int s = 0; s < nblk; ++s) {
             const int bi = upper ? nblk - 1 - s : s;
             const int kb = bi * kTB, sz = min(kTB, n - kb);
+            // D (the stored triangle of op(A)'s block, zero elsewhere, the unit diagonal set
+            // below) and X (the block rows of B) by asynchronous copies, all in flight at once
             for (int e = threadIdx.x; e < kTB * kTB; e += kThreads) {
                 const int rr = e % kTB, cc = e / kTB;
-                D[rr][cc] = (rr < sz && cc < sz) ? tri_el(A, la, uplo, trans, diag, kb + rr, kb + cc) : T(0);
+                const bool in = rr < sz && cc < sz && (upper ? rr <= cc : rr >= cc) && !(unit && rr == cc);
+                const int ar = trans == 'N' ? kb + rr : kb + cc, ac = trans == 'N' ? kb + cc : kb + rr;
+                cp_async_el(&D[rr][cc], A + ar + (long)ac * la, A, in);
             }
             for (int e = threadIdx.x; e < kTB * kMaxRhs; e += kThreads) {
                 const int rr = e % kTB, cc = e / kTB;
-                X[rr][cc] = (rr < sz && cc < r) ? B[kb + rr + (long)cc * lb] : T(0);
+                cp_async_el(&X[rr][cc], B + kb + rr + (long)cc * lb, B, rr < sz && cc < r);
             }
-            __syncthreads();
-            if (threadIdx.x < kTB) dinv[threadIdx.x] = (unit || threadIdx.x >= sz) ? T(1) : T(1) / D[threadIdx.x][threadIdx.x];
+            cp_async_commit();
             // rows still to solve after this block; their first panel chunk loads
             // during the substitution
             const int u0 = upper ? 0 : kb + sz, u1 = upper ? kb : n;
-            if (u0 < u1) load_panel(Pn, A, la, trans, u0, min(kTB, u1 - u0), kb, sz);
+            if (u0 < u1) {
+                load_panel(Pn, A, la, trans, u0, min(kTB, u1 - u0), kb, sz);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (unit && threadIdx.x < sz) D[threadIdx.x][threadIdx.x] = T(1);
+            if (threadIdx.x < kTB) dinv[threadIdx.x] = (unit || threadIdx.x >= sz) ? T(1) : T(1) / D[threadIdx.x][threadIdx.x];
             __syncthreads();
             // ---- substitution: warp w, right-hand sides w + 8 c; lane rows lane, lane + 32
             {
@@ -435,7 +455,49 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
                     cp_async_wait<0>();
                 }
                 __syncthreads();
-                if (4 * cg < r) {
+                if constexpr (sizeof(T) == 8) {
+                    // FP64: the chunk update B[c0 .. c0 + rows) -= P^T X as 16 x 8 DMMA tiles;
+                    // warp w takes row tile w % 4 and column tiles 4 (w / 4) .. +3 (those below r)
+                    const int g = lane >> 2, tq = lane & 3, rt = warp & 3, ct0 = (warp >> 2) * 4;
+                    const int nct = (r + 7) / 8;
+                    double acc[4][4] = {}, bv[4][4];
+                    if (ct0 < nct) {
+                        // the B values this warp updates, in flight before the products
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) {
+                                const int row = 16 * rt + g + 8 * (v >> 1), col = 8 * (ct0 + u) + 2 * tq + (v & 1);
+                                bv[u][v] = (ct0 + u < nct && row < rows && col < r) ? B[c0 + row + (long)col * lb]
+                                                                                   : 0.0;
+                            }
+                        for (int k8 = 0; k8 < (sz + 7) / 8; ++k8) {
+                            double af[4];
+#pragma unroll
+                            for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+                                for (int v0 = 0; v0 < 2; ++v0)
+                                    af[v0 + 2 * v1] = P[8 * k8 + tq + 4 * v1][16 * rt + g + 8 * v0];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                if (ct0 + u >= nct) break;
+                                double bf[2];
+#pragma unroll
+                                for (int v = 0; v < 2; ++v) bf[v] = X[8 * k8 + tq + 4 * v][8 * (ct0 + u) + g];
+                                dmma_16x8x8(acc[u], af, bf);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (ct0 + u >= nct) break;
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) {
+                                const int row = 16 * rt + g + 8 * (v >> 1), col = 8 * (ct0 + u) + 2 * tq + (v & 1);
+                                if (row < rows && col < r) B[c0 + row + (long)col * lb] = bv[u][v] - acc[u][v];
+                            }
+                        }
+                    }
+                } else if (4 * cg < r) {
                     // the B values this thread updates, fetched before the K loop
                     T bv[4][4];
 #pragma unroll
