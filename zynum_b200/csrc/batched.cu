@@ -539,6 +539,202 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
     }
 }
 
+// FP64 left-looking solver, one CTA per problem (left side, r <= 64): for each
+// 64-row block in solve order, acc = sum over the solved blocks j of
+// op(A)[block, j] X_j streams 32-deep K chunks of op(A) and of the solved rows
+// X (read back from B) through a two-stage cp.async ring into 16 x 8 DMMA tiles
+// held in registers (warp w: row tile w % 4, column tiles 4 (w / 4) .. +3);
+// then X_block = B_block - acc is solved in shared memory by a warp-synchronous
+// substitution (each warp carries only the right-hand sides it has) and
+// written back to B once.  The diagonal block's copy is in flight during the
+// products.
+// Warp-synchronous substitution of one 64-row block for the right-hand sides
+// w + 8 c, c < CM, of warp w: lane l owns block rows l and l + 32; the solved
+// value of row i is broadcast by shuffle and the lanes update their later
+// rows (no block barrier inside).
+template <int CM>
+ZB_DEVICE void substitute_block(double (*X)[kPP], const double (*D)[kTP], const double* dinv, int sz, bool upper) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double x[2][CM];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int c = 0; c < CM; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
+    for (int it = 0; it < sz; ++it) {
+        const int i = upper ? sz - 1 - it : it;
+        const int hi = i >> 5, li = i & 31;
+        const double di = dinv[i];
+        double xi[CM];
+#pragma unroll
+        for (int c = 0; c < CM; ++c) xi[c] = __shfl_sync(0xffffffffu, (hi ? x[1][c] : x[0][c]) * di, li);
+        if (lane == li) {
+#pragma unroll
+            for (int c = 0; c < CM; ++c) {
+                if (hi) x[1][c] = xi[c]; else x[0][c] = xi[c];
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int p = lane + 32 * h;
+            if (upper ? p < i : (p > i && p < sz)) {
+                const double dpi = D[p][i];
+#pragma unroll
+                for (int c = 0; c < CM; ++c) x[h][c] = fma(-dpi, xi[c], x[h][c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int c = 0; c < CM; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c];
+}
+
+constexpr int kLlK = 32;                          // K chunk
+constexpr int kLlPitch = kTB + 4;                 // 68: [k][row] and [k][col] tiles
+constexpr int kLlStage = 2 * kLlK * kLlPitch;     // A chunk + X chunk, in doubles
+constexpr int kLlRing = 2 * kLlStage;             // two stages (also holds the 64 x 68 solve block)
+
+__global__ void __launch_bounds__(kThreads, 2)
+trsm_batched_ll_f64(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
+                    char diag, double alpha, const double* const* __restrict__ a, const int* __restrict__ lda,
+                    double* const* __restrict__ b, const int* __restrict__ ldb) {
+    extern __shared__ __align__(16) unsigned char ll_smem[];
+    double* ring = reinterpret_cast<double*>(ll_smem);
+    double(*X)[kPP] = reinterpret_cast<double(*)[kPP]>(ring);  // solve block, after the products
+    double(*D)[kTP] = reinterpret_cast<double(*)[kTP]>(ring + kLlRing);
+    double* dinv = ring + kLlRing + kTB * kTP;
+    const bool upper = (trans == 'N' && uplo == 'U') || (trans != 'N' && uplo == 'L');
+    const bool unit = diag == 'U';
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int rt = warp & 3, ct0 = (warp >> 2) * 4;
+    for (int w = blockIdx.x; w < count; w += gridDim.x) {
+        const int q = order[w];
+        if (q < 0) continue;
+        const int n = dims[2 * q], r = dims[2 * q + 1];
+        const double* A = a[q];
+        double* B = b[q];
+        const long la = lda[q], lb = ldb[q];
+        if (alpha != 1.0)  // eight loads in flight per thread before their stores
+            for (long e0 = t; e0 < (long)n * r; e0 += 8L * kThreads) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long e = e0 + (long)u * kThreads;
+                    v[u] = e < (long)n * r ? B[(e % n) + (e / n) * lb] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long e = e0 + (long)u * kThreads;
+                    if (e < (long)n * r) B[(e % n) + (e / n) * lb] = alpha * v[u];
+                }
+            }
+        __syncthreads();
+        const int nblk = (n + kTB - 1) / kTB, nct = (r + 7) / 8;
+        for (int s = 0; s < nblk; ++s) {
+            const int bi = upper ? nblk - 1 - s : s;
+            const int kb = bi * kTB, sz = min(kTB, n - kb);
+            // diagonal block: stored triangle of op(A), zero elsewhere (unit diagonal set below)
+            for (int e = t; e < kTB * kTB; e += kThreads) {
+                const int rr = e % kTB, cc = e / kTB;
+                const bool in = rr < sz && cc < sz && (upper ? rr <= cc : rr >= cc) && !(unit && rr == cc);
+                const int ar = trans == 'N' ? kb + rr : kb + cc, ac = trans == 'N' ? kb + cc : kb + rr;
+                cp_async_el(&D[rr][cc], A + ar + (long)ac * la, A, in);
+            }
+            cp_async_commit();
+            // this thread's B values of the block (DMMA accumulator layout), loaded ahead
+            double bv[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int row = 16 * rt + g + 8 * (v >> 1), col = 8 * (ct0 + u) + 2 * tq + (v & 1);
+                    bv[u][v] = (row < sz && col < r) ? B[kb + row + (long)col * lb] : 0.0;
+                }
+            // solved rows: [0, kb) for a lower op(A), [kb + sz, n) for an upper one
+            const int k0 = upper ? kb + sz : 0, k1 = upper ? n : kb;
+            const int nch = (k1 - k0 + kLlK - 1) / kLlK;
+            auto stage = [&](int c) {
+                double(*As)[kLlPitch] = reinterpret_cast<double(*)[kLlPitch]>(ring + (c & 1) * kLlStage);
+                double(*Xs)[kLlPitch] = As + kLlK;
+                const int kc = k0 + c * kLlK, kw = min(kLlK, k1 - kc);
+                for (int e = t; e < kTB * kLlK; e += kThreads) {  // op(A)[kb + row][kc + k] -> As[k][row]
+                    int row, k;
+                    if (trans == 'N') row = e % kTB, k = e / kTB;
+                    else k = e % kLlK, row = e / kLlK;
+                    const int ar = trans == 'N' ? kb + row : kc + k, ac = trans == 'N' ? kc + k : kb + row;
+                    cp_async_el(&As[k][row], A + ar + (long)ac * la, A, row < sz && k < kw);
+                }
+                for (int e = t; e < kLlK * kMaxRhs; e += kThreads) {  // X[kc + k][col] = B(kc + k, col) -> Xs[k][col]
+                    const int k = e % kLlK, col = e / kLlK;
+                    cp_async_el(&Xs[k][col], B + (kc + k) + (long)col * lb, B, k < kw && col < r);
+                }
+            };
+            double acc[4][4] = {};
+            if (nch > 0) stage(0);
+            cp_async_commit();
+            for (int c = 0; c < nch; ++c) {
+                if (c + 1 < nch) stage(c + 1);
+                cp_async_commit();
+                cp_async_wait<1>();
+                __syncthreads();
+                const double(*As)[kLlPitch] = reinterpret_cast<const double(*)[kLlPitch]>(ring + (c & 1) * kLlStage);
+                const double(*Xs)[kLlPitch] = As + kLlK;
+                if (ct0 < nct) {
+#pragma unroll
+                    for (int k8 = 0; k8 < kLlK / 8; ++k8) {
+                        double af[4];
+#pragma unroll
+                        for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+                            for (int v0 = 0; v0 < 2; ++v0) af[v0 + 2 * v1] = As[8 * k8 + tq + 4 * v1][16 * rt + g + 8 * v0];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (ct0 + u >= nct) break;
+                            double bf[2];
+#pragma unroll
+                            for (int v = 0; v < 2; ++v) bf[v] = Xs[8 * k8 + tq + 4 * v][8 * (ct0 + u) + g];
+                            dmma_16x8x8(acc[u], af, bf);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            cp_async_wait<0>();
+            __syncthreads();
+            // the block to solve: X = B_block - acc, zero outside sz x r
+            for (int e = t; e < kTB * kPP; e += kThreads) X[e / kPP][e % kPP] = 0.0;
+            if (unit && t < sz) D[t][t] = 1.0;
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int row = 16 * rt + g + 8 * (v >> 1), col = 8 * (ct0 + u) + 2 * tq + (v & 1);
+                    if (ct0 + u < nct && row < sz && col < r) X[row][col] = bv[u][v] - acc[u][v];
+                }
+            if (t < kTB) dinv[t] = (unit || t >= sz) ? 1.0 : 1.0 / D[t][t];
+            __syncthreads();
+            // substitution: warp w holds right-hand sides w + 8 c for the c < cw it has
+            // (cw rounded up to 1, 2, 4 or 8 slots; a warp without columns skips it)
+            const int cw = r > warp ? (r - warp + 7) / 8 : 0;
+            if (cw > 4)
+                substitute_block<8>(X, D, dinv, sz, upper);
+            else if (cw > 2)
+                substitute_block<4>(X, D, dinv, sz, upper);
+            else if (cw > 1)
+                substitute_block<2>(X, D, dinv, sz, upper);
+            else if (cw == 1)
+                substitute_block<1>(X, D, dinv, sz, upper);
+            __syncthreads();
+            for (int e = t; e < kTB * r; e += kThreads) {
+                const int rr = e % kTB, cc = e / kTB;
+                if (rr < sz) B[kb + rr + (long)cc * lb] = X[rr][cc];
+            }
+            __syncthreads();  // the solved rows are visible to the next block's copies
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host
@@ -596,13 +792,13 @@ cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, in
                                 const int* ldb, int grid, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     const int sm = (3 * kTB * (kTB + 4) + kTB) * (dtype == BATCH_F64 ? 8 : 4);
-    cudaError_t e = dtype == BATCH_F64
-                        ? ensure_dynamic_smem(trsm_batched_kernel<double>, sm)
-                        : ensure_dynamic_smem(trsm_batched_kernel<float>, sm);
+    const int sm_ll = (kLlRing + kTB * kTP + kTB) * 8;
+    cudaError_t e = dtype == BATCH_F64 ? ensure_dynamic_smem(trsm_batched_ll_f64, sm_ll)
+                                       : ensure_dynamic_smem(trsm_batched_kernel<float>, sm);
     if (e != cudaSuccess) return e;
     prof_begin(st);
     if (dtype == BATCH_F64)
-        trsm_batched_kernel<double><<<grid, kThreads, sm, st>>>(
+        trsm_batched_ll_f64<<<grid, kThreads, sm_ll, st>>>(
             order, count, dims, uplo, trans, diag, *static_cast<const double*>(alpha),
             reinterpret_cast<const double* const*>(a), lda, reinterpret_cast<double* const*>(b), ldb);
     else
