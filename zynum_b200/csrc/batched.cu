@@ -549,9 +549,44 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
 // written back to B once.  The diagonal block's copy is in flight during the
 // products.
 // Warp-synchronous substitution of one 64-row block for the right-hand sides
-// w + 8 c, c < CM, of warp w: lane l owns block rows l and l + 32; the solved
-// value of row i is broadcast by shuffle and the lanes update their later
-// rows (no block barrier inside).
+// w + 8 c, c < CM, of warp w: lane l owns block rows l and l + 32.  Row i's
+// solved value (its fully updated value times 1 / D[i][i]) is broadcast by
+// shuffle and the lanes update their later rows; a row gets no update after it
+// is solved, so each lane keeps its rows' final unscaled values and scales them
+// once at the end.  The solve runs in two halves (rows 0..31 and 32..63, in
+// solve order) so every register index is known at compile time.
+template <int CM, int HI, bool UPPER>
+ZB_DEVICE void substitute_half(double (&x)[2][CM], const double (*D)[kTP], const double* dinv, int sz) {
+    const int lane = threadIdx.x & 31;
+    const int lo = 32 * HI, hi = min(sz, lo + 32);
+    for (int it = lo; it < hi; ++it) {
+        const int i = UPPER ? hi - 1 - (it - lo) : it;
+        const int li = i & 31;
+        const double di = dinv[i];
+        double xi[CM];
+#pragma unroll
+        for (int c = 0; c < CM; ++c) xi[c] = __shfl_sync(0xffffffffu, x[HI][c] * di, li);
+        // later rows: for a lower op(A) rows p > i, for an upper one rows p < i
+        if (UPPER ? true : HI == 0) {  // the other half of this lane (rows lane + 32 (1 - HI)...)
+            const int p = lane + 32 * (1 - HI);
+            const bool upd = UPPER ? (HI == 1 && p < i) : (p < sz);
+            if (upd) {
+                const double dpi = D[p][i];
+#pragma unroll
+                for (int c = 0; c < CM; ++c) x[1 - HI][c] = fma(-dpi, xi[c], x[1 - HI][c]);
+            }
+        }
+        {
+            const int p = lane + 32 * HI;  // this half
+            if (UPPER ? p < i : (p > i && p < sz)) {
+                const double dpi = D[p][i];
+#pragma unroll
+                for (int c = 0; c < CM; ++c) x[HI][c] = fma(-dpi, xi[c], x[HI][c]);
+            }
+        }
+    }
+}
+
 template <int CM>
 ZB_DEVICE void substitute_block(double (*X)[kPP], const double (*D)[kTP], const double* dinv, int sz, bool upper) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -560,33 +595,19 @@ ZB_DEVICE void substitute_block(double (*X)[kPP], const double (*D)[kTP], const 
     for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int c = 0; c < CM; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
-    for (int it = 0; it < sz; ++it) {
-        const int i = upper ? sz - 1 - it : it;
-        const int hi = i >> 5, li = i & 31;
-        const double di = dinv[i];
-        double xi[CM];
-#pragma unroll
-        for (int c = 0; c < CM; ++c) xi[c] = __shfl_sync(0xffffffffu, (hi ? x[1][c] : x[0][c]) * di, li);
-        if (lane == li) {
-#pragma unroll
-            for (int c = 0; c < CM; ++c) {
-                if (hi) x[1][c] = xi[c]; else x[0][c] = xi[c];
-            }
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int p = lane + 32 * h;
-            if (upper ? p < i : (p > i && p < sz)) {
-                const double dpi = D[p][i];
-#pragma unroll
-                for (int c = 0; c < CM; ++c) x[h][c] = fma(-dpi, xi[c], x[h][c]);
-            }
-        }
+    if (upper) {
+        substitute_half<CM, 1, true>(x, D, dinv, sz);
+        substitute_half<CM, 0, true>(x, D, dinv, sz);
+    } else {
+        substitute_half<CM, 0, false>(x, D, dinv, sz);
+        substitute_half<CM, 1, false>(x, D, dinv, sz);
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < 2; ++h) {
+        const double s = dinv[lane + 32 * h];
 #pragma unroll
-        for (int c = 0; c < CM; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c];
+        for (int c = 0; c < CM; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c] * s;
+    }
 }
 
 constexpr int kLlK = 32;                          // K chunk
