@@ -329,6 +329,83 @@ ZB_DEVICE void load_panel(T (*Pt)[kPP], const T* A, long la, char trans, int c0,
     cp_async_commit();
 }
 
+// Warp-synchronous substitution of one 64-row block for the right-hand sides
+// w + 8 c, c < CM, of warp w: lane l owns block rows l and l + 32.  Row i's
+// solved value (its fully updated value times 1 / D[i][i]) is broadcast by
+// shuffle and the lanes update their later rows; a row gets no update after it
+// is solved, so each lane keeps its rows' final unscaled values and scales them
+// once at the end.  The solve runs in two halves (rows 0..31 and 32..63, in
+// solve order) so every register index is known at compile time.
+template <typename T, int CM, int HI, bool UPPER>
+ZB_DEVICE void substitute_half(T (&x)[2][CM], const T (*D)[kTP], const T* dinv, int sz) {
+    const int lane = threadIdx.x & 31;
+    const int lo = 32 * HI, hi = min(sz, lo + 32);
+    for (int it = lo; it < hi; ++it) {
+        const int i = UPPER ? hi - 1 - (it - lo) : it;
+        const int li = i & 31;
+        const T di = dinv[i];
+        T xi[CM];
+#pragma unroll
+        for (int c = 0; c < CM; ++c) xi[c] = __shfl_sync(0xffffffffu, x[HI][c] * di, li);
+        // later rows: for a lower op(A) rows p > i, for an upper one rows p < i
+        if (UPPER ? true : HI == 0) {  // the other half of this lane (rows lane + 32 (1 - HI)...)
+            const int p = lane + 32 * (1 - HI);
+            const bool upd = UPPER ? (HI == 1 && p < i) : (p < sz);
+            if (upd) {
+                const T dpi = D[p][i];
+#pragma unroll
+                for (int c = 0; c < CM; ++c) x[1 - HI][c] = fma(-dpi, xi[c], x[1 - HI][c]);
+            }
+        }
+        {
+            const int p = lane + 32 * HI;  // this half
+            if (UPPER ? p < i : (p > i && p < sz)) {
+                const T dpi = D[p][i];
+#pragma unroll
+                for (int c = 0; c < CM; ++c) x[HI][c] = fma(-dpi, xi[c], x[HI][c]);
+            }
+        }
+    }
+}
+
+template <typename T, int CM>
+ZB_DEVICE void substitute_block(T (*X)[kPP], const T (*D)[kTP], const T* dinv, int sz, bool upper) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T x[2][CM];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int c = 0; c < CM; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
+    if (upper) {
+        substitute_half<T, CM, 1, true>(x, D, dinv, sz);
+        substitute_half<T, CM, 0, true>(x, D, dinv, sz);
+    } else {
+        substitute_half<T, CM, 0, false>(x, D, dinv, sz);
+        substitute_half<T, CM, 1, false>(x, D, dinv, sz);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const T s = dinv[lane + 32 * h];
+#pragma unroll
+        for (int c = 0; c < CM; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c] * s;
+    }
+}
+
+// Substitution for the warp's share of r right-hand sides (1, 2, 4 or 8 slots).
+template <typename T>
+ZB_DEVICE void substitute_rhs(T (*X)[kPP], const T (*D)[kTP], const T* dinv, int sz, bool upper, int r) {
+    const int warp = threadIdx.x >> 5;
+    const int cw = r > warp ? (r - warp + 7) / 8 : 0;
+    if (cw > 4)
+        substitute_block<T, 8>(X, D, dinv, sz, upper);
+    else if (cw > 2)
+        substitute_block<T, 4>(X, D, dinv, sz, upper);
+    else if (cw > 1)
+        substitute_block<T, 2>(X, D, dinv, sz, upper);
+    else if (cw == 1)
+        substitute_block<T, 1>(X, D, dinv, sz, upper);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2)
 trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
@@ -398,44 +475,8 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
             if (unit && threadIdx.x < sz) D[threadIdx.x][threadIdx.x] = T(1);
             if (threadIdx.x < kTB) dinv[threadIdx.x] = (unit || threadIdx.x >= sz) ? T(1) : T(1) / D[threadIdx.x][threadIdx.x];
             __syncthreads();
-            // ---- substitution: warp w, right-hand sides w + 8 c; lane rows lane, lane + 32
-            {
-                T x[2][8];
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
-                for (int it = 0; it < sz; ++it) {
-                    const int i = upper ? sz - 1 - it : it;
-                    const int hi = i >> 5, li = i & 31;
-                    const T di = dinv[i];
-                    T xi[8];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const T own = (hi ? x[1][c] : x[0][c]) * di;
-                        xi[c] = __shfl_sync(0xffffffffu, own, li);
-                    }
-                    if (lane == li) {
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            if (hi) x[1][c] = xi[c]; else x[0][c] = xi[c];
-                        }
-                    }
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int p = lane + 32 * h;
-                        if (upper ? p < i : (p > i && p < sz)) {
-                            const T dpi = D[p][i];
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) x[h][c] = fma(-dpi, xi[c], x[h][c]);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c];
-            }
+            // ---- substitution (each warp carries only the right-hand sides it has)
+            substitute_rhs<T>(X, D, dinv, sz, upper, r);
             __syncthreads();
             for (int e = threadIdx.x; e < kTB * r; e += kThreads) {
                 const int rr = e % kTB, cc = e / kTB;
@@ -548,68 +589,6 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
 // substitution (each warp carries only the right-hand sides it has) and
 // written back to B once.  The diagonal block's copy is in flight during the
 // products.
-// Warp-synchronous substitution of one 64-row block for the right-hand sides
-// w + 8 c, c < CM, of warp w: lane l owns block rows l and l + 32.  Row i's
-// solved value (its fully updated value times 1 / D[i][i]) is broadcast by
-// shuffle and the lanes update their later rows; a row gets no update after it
-// is solved, so each lane keeps its rows' final unscaled values and scales them
-// once at the end.  The solve runs in two halves (rows 0..31 and 32..63, in
-// solve order) so every register index is known at compile time.
-template <int CM, int HI, bool UPPER>
-ZB_DEVICE void substitute_half(double (&x)[2][CM], const double (*D)[kTP], const double* dinv, int sz) {
-    const int lane = threadIdx.x & 31;
-    const int lo = 32 * HI, hi = min(sz, lo + 32);
-    for (int it = lo; it < hi; ++it) {
-        const int i = UPPER ? hi - 1 - (it - lo) : it;
-        const int li = i & 31;
-        const double di = dinv[i];
-        double xi[CM];
-#pragma unroll
-        for (int c = 0; c < CM; ++c) xi[c] = __shfl_sync(0xffffffffu, x[HI][c] * di, li);
-        // later rows: for a lower op(A) rows p > i, for an upper one rows p < i
-        if (UPPER ? true : HI == 0) {  // the other half of this lane (rows lane + 32 (1 - HI)...)
-            const int p = lane + 32 * (1 - HI);
-            const bool upd = UPPER ? (HI == 1 && p < i) : (p < sz);
-            if (upd) {
-                const double dpi = D[p][i];
-#pragma unroll
-                for (int c = 0; c < CM; ++c) x[1 - HI][c] = fma(-dpi, xi[c], x[1 - HI][c]);
-            }
-        }
-        {
-            const int p = lane + 32 * HI;  // this half
-            if (UPPER ? p < i : (p > i && p < sz)) {
-                const double dpi = D[p][i];
-#pragma unroll
-                for (int c = 0; c < CM; ++c) x[HI][c] = fma(-dpi, xi[c], x[HI][c]);
-            }
-        }
-    }
-}
-
-template <int CM>
-ZB_DEVICE void substitute_block(double (*X)[kPP], const double (*D)[kTP], const double* dinv, int sz, bool upper) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double x[2][CM];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int c = 0; c < CM; ++c) x[h][c] = X[lane + 32 * h][warp + 8 * c];
-    if (upper) {
-        substitute_half<CM, 1, true>(x, D, dinv, sz);
-        substitute_half<CM, 0, true>(x, D, dinv, sz);
-    } else {
-        substitute_half<CM, 0, false>(x, D, dinv, sz);
-        substitute_half<CM, 1, false>(x, D, dinv, sz);
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const double s = dinv[lane + 32 * h];
-#pragma unroll
-        for (int c = 0; c < CM; ++c) X[lane + 32 * h][warp + 8 * c] = x[h][c] * s;
-    }
-}
-
 constexpr int kLlK = 32;                          // K chunk
 constexpr int kLlPitch = kTB + 4;                 // 68: [k][row] and [k][col] tiles
 constexpr int kLlStage = 2 * kLlK * kLlPitch;     // A chunk + X chunk, in doubles
@@ -737,15 +716,7 @@ trsm_batched_ll_f64(const int* __restrict__ order, int count, const int* __restr
             __syncthreads();
             // substitution: warp w holds right-hand sides w + 8 c for the c < cw it has
             // (cw rounded up to 1, 2, 4 or 8 slots; a warp without columns skips it)
-            const int cw = r > warp ? (r - warp + 7) / 8 : 0;
-            if (cw > 4)
-                substitute_block<8>(X, D, dinv, sz, upper);
-            else if (cw > 2)
-                substitute_block<4>(X, D, dinv, sz, upper);
-            else if (cw > 1)
-                substitute_block<2>(X, D, dinv, sz, upper);
-            else if (cw == 1)
-                substitute_block<1>(X, D, dinv, sz, upper);
+            substitute_rhs<double>(X, D, dinv, sz, upper, r);
             __syncthreads();
             for (int e = t; e < kTB * r; e += kThreads) {
                 const int rr = e % kTB, cc = e / kTB;
