@@ -77,6 +77,20 @@ ZYNUM_BLAS_GPU_API void ssyrk_(const char *uplo, const char *trans, const zynum_
 ZYNUM_BLAS_GPU_API void dsyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
                                const double *alpha, const double *a, const zynum_blas_int *lda, const double *beta,
                                double *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:877-884 ctrsm_ / ztrsm_ (interleaved complex; op = C conjugates) */
+ZYNUM_BLAS_GPU_API void ctrsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const void *alpha, const void *a,
+                               const zynum_blas_int *lda, void *b, const zynum_blas_int *ldb);
+ZYNUM_BLAS_GPU_API void ztrsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const void *alpha, const void *a,
+                               const zynum_blas_int *lda, void *b, const zynum_blas_int *ldb);
+/* src/blas/abi/fortran.zig:810-817 csyrk_ / zsyrk_ (C := alpha op(A) op(A)^T + beta C, one triangle) */
+ZYNUM_BLAS_GPU_API void csyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *beta, void *c,
+                               const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zsyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *beta, void *c,
+                               const zynum_blas_int *ldc);
 /* src/blas/abi/fortran.zig:777-783 ssymm_ / dsymm_ (C := alpha A B + beta C or alpha B A + beta C, A symmetric) */
 ZYNUM_BLAS_GPU_API void ssymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
                                const float *alpha, const float *a, const zynum_blas_int *lda, const float *b,
@@ -131,6 +145,16 @@ ZYNUM_BLAS_GPU_API void cblas_ssyrk(int layout, int uplo, int trans, int n, int 
                                     int lda, float beta, float *c, int ldc);
 ZYNUM_BLAS_GPU_API void cblas_dsyrk(int layout, int uplo, int trans, int n, int k, double alpha, const double *a,
                                     int lda, double beta, double *c, int ldc);
+/* src/blas/abi/cblas.zig:1755-1779 cblas_ctrsm / cblas_ztrsm (alpha by pointer) */
+ZYNUM_BLAS_GPU_API void cblas_ctrsm(int layout, int side, int uplo, int transa, int diag, int m, int n,
+                                    const void *alpha, const void *a, int lda, void *b, int ldb);
+ZYNUM_BLAS_GPU_API void cblas_ztrsm(int layout, int side, int uplo, int transa, int diag, int m, int n,
+                                    const void *alpha, const void *a, int lda, void *b, int ldb);
+/* src/blas/abi/cblas.zig:1560-1582 cblas_csyrk / cblas_zsyrk (alpha / beta by pointer) */
+ZYNUM_BLAS_GPU_API void cblas_csyrk(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                    int lda, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zsyrk(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                    int lda, const void *beta, void *c, int ldc);
 /* src/blas/abi/cblas.zig:1467-1489 cblas_ssymm / cblas_dsymm */
 ZYNUM_BLAS_GPU_API void cblas_ssymm(int layout, int side, int uplo, int m, int n, float alpha, const float *a, int lda,
                                     const float *b, int ldb, float beta, float *c, int ldc);
@@ -199,6 +223,22 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n,
                                                    int lda, double beta, double *c, int ldc, void *stream);
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
                                                    int lda, float beta, float *c, int ldc, void *stream);
+/* Complex TRSM on device pointers (interleaved complex; alpha points to re, im): the recursive solve with
+ * complex GEMM couplings (4M / 3M per the complex method).  Argument numbering as ztrsm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ztrsm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   const double *alpha, const double *a, int lda, double *b, int ldb,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ctrsm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   const float *alpha, const float *a, int lda, float *b, int ldb,
+                                                   void *stream);
+/* Complex SYRK on device pointers: one complex GEMM into scratch and a triangle update.  Argument
+ * numbering as zsyrk_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zsyrk_device(char uplo, char trans, int n, int k, const double *alpha,
+                                                   const double *a, int lda, const double *beta, double *c, int ldc,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_csyrk_device(char uplo, char trans, int n, int k, const float *alpha,
+                                                   const float *a, int lda, const float *beta, float *c, int ldc,
+                                                   void *stream);
 /* SYMM on device pointers: the stored triangle of A is mirrored into a dense scratch copy, then one
  * GEMM (following the DGEMM / SGEMM method).  Argument numbering as dsymm_. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsymm_device(char side, char uplo, int m, int n, double alpha, const double *a,

@@ -45,6 +45,10 @@ def _declare(L):
     L.oracle_strsm.argtypes = [ch, ch, ch, ch, i32, i32, f32, vp, i32, vp, i32]
     L.oracle_dsyrk.argtypes = [ch, ch, i32, i32, f64, vp, i32, f64, vp, i32]
     L.oracle_ssyrk.argtypes = [ch, ch, i32, i32, f32, vp, i32, f32, vp, i32]
+    L.oracle_ztrsm.argtypes = [ch, ch, ch, ch, i32, i32, vp, vp, i32, vp, i32]
+    L.oracle_ctrsm.argtypes = [ch, ch, ch, ch, i32, i32, vp, vp, i32, vp, i32]
+    L.oracle_zsyrk.argtypes = [ch, ch, i32, i32, vp, vp, i32, vp, vp, i32]
+    L.oracle_csyrk.argtypes = [ch, ch, i32, i32, vp, vp, i32, vp, vp, i32]
     L.oracle_dsymm.argtypes = [ch, ch, i32, i32, f64, vp, i32, vp, i32, f64, vp, i32]
     L.oracle_ssymm.argtypes = [ch, ch, i32, i32, f32, vp, i32, vp, i32, f32, vp, i32]
     L.oracle_dtrmm.argtypes = [ch, ch, ch, ch, i32, i32, f64, vp, i32, vp, i32]
@@ -103,14 +107,26 @@ def ddgemm_sampled(ta, tb, k, a, lda, b, ldb, rows, cols):
 
 
 def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    """In place on b; dtype from b (f64, f32, c128, c64)."""
     L = lib()
+    if np.iscomplexobj(b):
+        f = L.oracle_ztrsm if b.dtype == np.complex128 else L.oracle_ctrsm
+        al = np.array([alpha], dtype=b.dtype)
+        f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, al.ctypes.data, _p(a), lda, _p(b), ldb)
+        return b
     f = L.oracle_dtrsm if b.dtype == np.float64 else L.oracle_strsm
     f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha, _p(a), lda, _p(b), ldb)
     return b
 
 
 def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """In place on c's triangle; dtype from c (f64, f32, c128, c64)."""
     L = lib()
+    if np.iscomplexobj(c):
+        f = L.oracle_zsyrk if c.dtype == np.complex128 else L.oracle_csyrk
+        al, be = np.array([alpha], dtype=c.dtype), np.array([beta], dtype=c.dtype)
+        f(_b(uplo), _b(trans), n, k, al.ctypes.data, _p(a), lda, be.ctypes.data, _p(c), ldc)
+        return c
     f = L.oracle_dsyrk if c.dtype == np.float64 else L.oracle_ssyrk
     f(_b(uplo), _b(trans), n, k, alpha, _p(a), lda, beta, _p(c), ldc)
     return c

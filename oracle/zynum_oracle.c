@@ -16,7 +16,10 @@
  *                  trsv per right-hand side, matrix_vector/triangular.zig
  *                  :400-435, triValue access.zig:54-64) and the right-side
  *                  row solve solveRightRow triangular.zig:72-88.
- *   oracle_?syrk   symmetric.zig:180-199 (runSyrkColumns).
+ *   oracle_?syrk   symmetric.zig:180-199 (runSyrkColumns), z / c with op = C
+ *                  conjugating (matrixValue).
+ *   oracle_[zc]trsm complex trsm: triValue with conj for op = C, right side per
+ *                  solveRightRow (triangular.zig:72-88).
  *   oracle_?symm   symmetric.zig:56-70 (runSymmColumns, symValue access.zig:31-42).
  *   oracle_?trmm   triangular.zig:202-231 (left: trmv + alpha scale per column,
  *                  runLeftColumns :105-110; right: row products :212-229).
@@ -432,6 +435,118 @@ DEFINE_REAL_TRMM(oracle_strmm, float, tri_s)
 
 DEFINE_REAL_SYR2K(oracle_dsyr2k, double)
 DEFINE_REAL_SYR2K(oracle_ssyr2k, float)
+
+/* ------------------------------------------------------- complex TRSM / SYRK */
+
+/* Interleaved complex with the reference's scalar arithmetic (core/shared/
+ * scalar.zig: sub :63, mul :77, divv :84, conj :92). */
+#define DEFINE_CX(CT, R)                                                                     \
+    typedef struct { R re, im; } CT;                                                         \
+    static inline CT CT##_mul(CT a, CT b) {                                                  \
+        CT r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }           \
+    static inline CT CT##_add(CT a, CT b) { CT r = {a.re + b.re, a.im + b.im}; return r; }   \
+    static inline CT CT##_sub(CT a, CT b) { CT r = {a.re - b.re, a.im - b.im}; return r; }   \
+    static inline CT CT##_div(CT a, CT b) {                                                  \
+        R den = b.re * b.re + b.im * b.im;                                                   \
+        CT r = {(a.re * b.re + a.im * b.im) / den, (a.im * b.re - a.re * b.im) / den}; return r; } \
+    static inline CT CT##_conj(CT a) { CT r = {a.re, -a.im}; return r; }                     \
+    static inline int CT##_is_one(CT a) { return a.re == (R)1 && a.im == (R)0; }             \
+    static inline int CT##_is_zero(CT a) { return a.re == (R)0 && a.im == (R)0; }            \
+    /* triValue access.zig:54-64: element (row, col) of op(A), conj for op = C */           \
+    static inline CT CT##_tri(char uplo, char diag, char trans, const CT *a, blas_int lda,   \
+                              size_t row, size_t col) {                                      \
+        size_t ar = (trans == 'N') ? row : col, ac = (trans == 'N') ? col : row;             \
+        CT one = {(R)1, (R)0}, zero = {(R)0, (R)0};                                          \
+        if (ar == ac && diag == 'U') return one;                                             \
+        if (uplo == 'U' && ar > ac) return zero;                                             \
+        if (uplo == 'L' && ar < ac) return zero;                                             \
+        CT v = a[ix(lda, ar, ac)];                                                           \
+        return trans == 'C' ? CT##_conj(v) : v;                                              \
+    }                                                                                        \
+    /* trsv (matrix_vector/triangular.zig, the unit-stride solve) on x[i * inc] */           \
+    static void CT##_trsv(char uplo, char trans, char diag, blas_int n, const CT *a,         \
+                          blas_int lda, CT *x, size_t inc) {                                 \
+        if (op_is_upper(uplo, trans)) {                                                      \
+            for (size_t r = (size_t)n; r-- > 0;) {                                           \
+                CT t = x[r * inc];                                                           \
+                for (size_t q = r + 1; q < (size_t)n; ++q)                                   \
+                    t = CT##_sub(t, CT##_mul(CT##_tri(uplo, diag, trans, a, lda, r, q), x[q * inc])); \
+                if (diag == 'N') t = CT##_div(t, CT##_tri(uplo, diag, trans, a, lda, r, r)); \
+                x[r * inc] = t;                                                              \
+            }                                                                                \
+        } else {                                                                             \
+            for (size_t r = 0; r < (size_t)n; ++r) {                                         \
+                CT t = x[r * inc];                                                           \
+                for (size_t q = 0; q < r; ++q)                                               \
+                    t = CT##_sub(t, CT##_mul(CT##_tri(uplo, diag, trans, a, lda, r, q), x[q * inc])); \
+                if (diag == 'N') t = CT##_div(t, CT##_tri(uplo, diag, trans, a, lda, r, r)); \
+                x[r * inc] = t;                                                              \
+            }                                                                                \
+        }                                                                                    \
+    }
+
+DEFINE_CX(cxd, double)
+DEFINE_CX(cxf, float)
+
+/* triangular.zig:233-249 trsm for complex types: alpha pre-scale (:51-58), one
+ * trsv per column (left side); per row (right side, solveRightRow :72-88):
+ * op N -> trsv with trans T, op T -> trsv with N, op C -> conj the row, trsv
+ * with N, conj the row. */
+#define DEFINE_CX_TRSM(NAME, CT)                                                                   \
+    void NAME(char side, char uplo, char trans, char diag, blas_int m, blas_int n, const CT *alpha, \
+              const CT *a, blas_int lda, CT *b, blas_int ldb) {                                      \
+        side = (char)upc(side); uplo = (char)upc(uplo); trans = (char)upc(trans); diag = (char)upc(diag); \
+        if (m <= 0 || n <= 0) return;                                                                \
+        if (!CT##_is_one(*alpha))                                                                    \
+            for (size_t j = 0; j < (size_t)n; ++j)                                                   \
+                for (size_t i = 0; i < (size_t)m; ++i) b[ix(ldb, i, j)] = CT##_mul(*alpha, b[ix(ldb, i, j)]); \
+        if (side == 'L') {                                                                           \
+            for (size_t j = 0; j < (size_t)n; ++j) CT##_trsv(uplo, trans, diag, m, a, lda, b + (size_t)ldb * j, 1); \
+        } else {                                                                                     \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                 \
+                CT *x = b + i;                                                                       \
+                if (trans == 'N') {                                                                  \
+                    CT##_trsv(uplo, 'T', diag, n, a, lda, x, (size_t)ldb);                           \
+                } else if (trans == 'T') {                                                           \
+                    CT##_trsv(uplo, 'N', diag, n, a, lda, x, (size_t)ldb);                           \
+                } else {                                                                             \
+                    for (size_t q = 0; q < (size_t)n; ++q) x[q * ldb] = CT##_conj(x[q * ldb]);       \
+                    CT##_trsv(uplo, 'N', diag, n, a, lda, x, (size_t)ldb);                           \
+                    for (size_t q = 0; q < (size_t)n; ++q) x[q * ldb] = CT##_conj(x[q * ldb]);       \
+                }                                                                                    \
+            }                                                                                        \
+        }                                                                                            \
+    }
+
+DEFINE_CX_TRSM(oracle_ztrsm, cxd)
+DEFINE_CX_TRSM(oracle_ctrsm, cxf)
+
+/* symmetric.zig:180-199 runSyrkColumns for complex types with herm = false:
+ * op(A)(i, p) by matrixValue (access.zig:23-29; conj for op = C). */
+#define DEFINE_CX_SYRK(NAME, CT)                                                                     \
+    void NAME(char uplo, char trans, blas_int n, blas_int k, const CT *alpha, const CT *a, blas_int lda, \
+              const CT *beta, CT *c, blas_int ldc) {                                                  \
+        uplo = (char)upc(uplo); trans = (char)upc(trans);                                             \
+        if (n <= 0) return;                                                                           \
+        for (size_t j = 0; j < (size_t)n; ++j) {                                                      \
+            size_t r0 = (uplo == 'U') ? 0 : j, r1 = (uplo == 'U') ? j + 1 : (size_t)n;                \
+            for (size_t i = r0; i < r1; ++i) {                                                        \
+                CT sum = {0, 0};                                                                      \
+                for (size_t p = 0; p < (size_t)(k > 0 ? k : 0); ++p) {                                 \
+                    CT ai = (trans == 'N') ? a[ix(lda, i, p)] : a[ix(lda, p, i)];                     \
+                    CT aj = (trans == 'N') ? a[ix(lda, j, p)] : a[ix(lda, p, j)];                     \
+                    if (trans == 'C') { ai = CT##_conj(ai); aj = CT##_conj(aj); }                     \
+                    sum = CT##_add(sum, CT##_mul(ai, aj));                                            \
+                }                                                                                     \
+                size_t q = ix(ldc, i, j);                                                             \
+                CT zero = {0, 0};                                                                     \
+                c[q] = CT##_add(CT##_mul(*alpha, sum), CT##_is_zero(*beta) ? zero : CT##_mul(*beta, c[q])); \
+            }                                                                                         \
+        }                                                                                             \
+    }
+
+DEFINE_CX_SYRK(oracle_zsyrk, cxd)
+DEFINE_CX_SYRK(oracle_csyrk, cxf)
 
 /* Library self-identification for the loader in the tests. */
 int oracle_version(void) { return 1; }

@@ -186,3 +186,109 @@ def test_syrk_k_zero_and_split(blas, oracle):
     mask = np.triu(np.ones((n, n), bool))
     assert np.abs(c - ref)[mask].max() <= 4 * k * 2.0 ** -53 * (np.abs(a).T @ np.abs(a) + 1)[mask].max()
     assert np.array_equal(c[~mask], c0[~mask])
+
+
+def _ctri(rng, na, ld, dtype):
+    """Complex triangle source: off-diagonals N(0, 1/na) (re and im), diagonal 2 + |N| + i N(0, 0.3)."""
+    a = (rng.standard_normal((ld, na)) + 1j * rng.standard_normal((ld, na))) / np.sqrt(2 * na)
+    for i in range(na):
+        a[i, i] = 2.0 + abs(rng.standard_normal()) + 0.3j * rng.standard_normal()
+    a[na:] = -999.0
+    return np.asfortranarray(a.astype(dtype))
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", list(itertools.product("LR", "UL", "NTC", "NU")))
+def test_ztrsm_all_cases(blas, oracle, side, uplo, trans, diag):
+    """ZTRSM: every side / uplo / trans (C conjugates) / diag; orders of 600 cross three 256-row
+    leaves; 37 right-hand sides; complex alpha; padding rows of B untouched."""
+    rng = np.random.default_rng(int.from_bytes((side + uplo + trans + diag).encode(), "little") % 2**32)
+    m, n = (600, 37) if side == "L" else (37, 600)
+    na = m if side == "L" else n
+    lda, ldb = na + 2, m + 3
+    a = _ctri(rng, na, lda, np.complex128)
+    b = np.asfortranarray((rng.standard_normal((ldb, n)) + 1j * rng.standard_normal((ldb, n))))
+    b[m:] = -999.0
+    b0 = b.copy(order="F")
+    ref = b.copy(order="F")
+    alpha = 0.75 - 0.5j
+    oracle.trsm(side, uplo, trans, diag, m, n, alpha, a, lda, ref, ldb)
+    blas.trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb)
+    err = np.abs(b[:m] - ref[:m])
+    assert np.all(err <= 1e-11 * (1 + np.abs(ref[:m]))), float(err.max())
+    assert np.array_equal(b[m:], b0[m:])
+
+
+@pytest.mark.parametrize("side,uplo,trans", [("L", "L", "N"), ("R", "U", "C"), ("L", "U", "C"), ("R", "L", "T")])
+def test_ctrsm(blas, oracle, side, uplo, trans):
+    rng = np.random.default_rng(7)
+    m, n = (300, 20) if side == "L" else (20, 300)
+    na = m if side == "L" else n
+    a = _ctri(rng, na, na, np.complex64)
+    b = np.asfortranarray((rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))).astype(np.complex64))
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, trans, "N", m, n, 1.0 + 0.5j, a, na, ref, m)
+    blas.trsm(side, uplo, trans, "N", m, n, 1.0 + 0.5j, a, na, b, m)
+    assert np.all(np.abs(b - ref) <= 1e-3 * (1 + np.abs(ref)))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["z", "c"])
+@pytest.mark.parametrize("uplo,trans", list(itertools.product("UL", "NTC")))
+def test_complex_syrk(blas, oracle, dtype, uplo, trans):
+    """ZSYRK / CSYRK (symmetric, no conjugation of the product; op = C conjugates op(A)):
+    the triangle within c k u (|alpha| |A||A|^T + |beta| |C|), the other triangle and the
+    padding bit-identical, beta = 0 clears NaN."""
+    rng = np.random.default_rng(ord(uplo) + 3 * ord(trans))
+    n, k = 150, 90
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = np.asfortranarray((rng.standard_normal((ra + 1, ca)) + 1j * rng.standard_normal((ra + 1, ca))).astype(dtype))
+    u = 2.0 ** -53 if dtype == np.complex128 else 2.0 ** -24
+    for alpha, beta in ((0.5 - 1.0j, 0.25 + 0.5j), (1.0 + 0.0j, 0.0)):
+        c = np.asfortranarray((rng.standard_normal((n + 2, n)) + 1j * rng.standard_normal((n + 2, n))).astype(dtype))
+        tri = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+        if beta == 0.0:
+            c[:n][tri] = np.nan
+        c0 = c.copy(order="F")
+        ref = c.copy(order="F")
+        oracle.syrk(uplo, trans, n, k, alpha, a, ra + 1, beta, ref, n + 2)
+        blas.syrk(uplo, trans, n, k, alpha, a, ra + 1, beta, c, n + 2)
+        A = np.abs(a[:ra, :ca].astype(np.complex128))
+        A = A if trans == "N" else A.T
+        bound = 8 * k * u * (abs(alpha) * (A @ A.T) + abs(beta) * np.nan_to_num(np.abs(c0[:n]))) + 1e-300
+        got, want = c[:n].astype(np.complex128), ref[:n].astype(np.complex128)
+        assert np.all(np.isfinite(got[tri]))
+        assert np.all(np.abs(got - want)[tri] <= bound[tri]), float(np.abs(got - want)[tri].max())
+        assert np.array_equal(c[:n][~tri], c0[:n][~tri], equal_nan=True), "the other triangle changed"
+        assert np.array_equal(c[n:], c0[n:], equal_nan=True)
+
+
+def test_complex_device_entry_points(blas, oracle):
+    """zynum_blas_gpu_ztrsm_device / zsyrk_device on torch tensors, and cblas_ztrsm row-major."""
+    import torch
+    rng = np.random.default_rng(13)
+    m, n = 300, 24
+    a = _ctri(rng, m, m, np.complex128)
+    b = np.asfortranarray(rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n)))
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda")  # noqa: E731
+    host = lambda t: np.asfortranarray(t.cpu().numpy().T)  # noqa: E731
+    ref = b.copy(order="F")
+    oracle.trsm("L", "L", "C", "N", m, n, 2.0 - 1.0j, a, m, ref, m)
+    B = dev(b)
+    blas.trsm_device_c("L", "L", "C", "N", m, n, 2.0 - 1.0j, dev(a), m, B, m)
+    torch.cuda.synchronize()
+    assert np.abs(host(B) - ref).max() <= 1e-11 * (1 + np.abs(ref).max())
+    ref = np.zeros((n, n), complex, order="F")
+    oracle.syrk("U", "T", n, m, 1.0, b, m, 0.0, ref, n)
+    C = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+    blas.syrk_device_c("U", "T", n, m, 1.0, dev(b), m, 0.0, C, n)
+    torch.cuda.synchronize()
+    got = host(C)
+    up = np.triu(np.ones((n, n), bool))
+    assert np.abs(got - ref)[up].max() <= 1e-12 * (1 + np.abs(ref).max())
+    # row-major CBLAS: A (m x m, row-major) solves A X = 0.5 B
+    A = np.tril(rng.standard_normal((m, m)) / np.sqrt(m) + 1j * rng.standard_normal((m, m)) / np.sqrt(m))
+    A += np.diag(2.0 + np.abs(rng.standard_normal(m)))
+    Bm = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    X = np.ascontiguousarray(Bm.copy())
+    blas.cblas_trsm_c(blas.CblasRowMajor, blas.CblasLeft, blas.CblasLower, blas.CblasNoTrans, blas.CblasNonUnit,
+                      m, n, 0.5, np.ascontiguousarray(A), m, X, n)
+    assert np.abs(A @ X - 0.5 * Bm).max() <= 1e-10

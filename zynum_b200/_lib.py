@@ -73,6 +73,24 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
                  "zynum_blas_gpu_ssyrk_device"):
         getattr(L, name).restype = i
+    for name in ("ztrsm_", "ctrsm_"):
+        getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("zsyrk_", "csyrk_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("cblas_ztrsm", "cblas_ctrsm"):
+        getattr(L, name).argtypes = [i, i, i, i, i, i, i, P, P, i, P, i]
+        getattr(L, name).restype = None
+    for name in ("cblas_zsyrk", "cblas_csyrk"):
+        getattr(L, name).argtypes = [i, i, i, i, i, P, P, i, P, P, i]
+        getattr(L, name).restype = None
+    for name in ("zynum_blas_gpu_ztrsm_device", "zynum_blas_gpu_ctrsm_device"):
+        getattr(L, name).argtypes = [ch, ch, ch, ch, i, i, P, P, i, P, i, P]
+        getattr(L, name).restype = i
+    for name in ("zynum_blas_gpu_zsyrk_device", "zynum_blas_gpu_csyrk_device"):
+        getattr(L, name).argtypes = [ch, ch, i, i, P, P, i, P, P, i, P]
+        getattr(L, name).restype = i
     for name in ("dsymm_", "ssymm_"):
         getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
         getattr(L, name).restype = None

@@ -105,8 +105,14 @@ def cblas_cgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
 
 
 def trsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
-    """Fortran dtrsm_ / strsm_ on host arrays (dtype from b; in-place on b)."""
+    """Fortran ?trsm_ on host arrays (d / s / z / c from b's dtype; in-place on b)."""
     L = load()
+    if np.iscomplexobj(b):
+        fn = L.ztrsm_ if b.dtype == np.complex128 else L.ctrsm_
+        al = np.array([alpha], b.dtype)
+        fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
+           _i(ldb))
+        return b
     fn, dt = (L.dtrsm_, np.float64) if b.dtype == np.float64 else (L.strsm_, np.float32)
     al = np.array([alpha], dt)
     fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
@@ -115,8 +121,13 @@ def trsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
 
 
 def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
-    """Fortran dsyrk_ / ssyrk_ on host arrays (dtype from c; in-place on c's triangle)."""
+    """Fortran ?syrk_ on host arrays (d / s / z / c from c's dtype; in-place on c's triangle)."""
     L = load()
+    if np.iscomplexobj(c):
+        fn = L.zsyrk_ if c.dtype == np.complex128 else L.csyrk_
+        al, be = np.array([alpha], c.dtype), np.array([beta], c.dtype)
+        fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), be.ctypes.data, _ptr(c), _i(ldc))
+        return c
     fn, dt = (L.dsyrk_, np.float64) if c.dtype == np.float64 else (L.ssyrk_, np.float32)
     al, be = np.array([alpha], dt), np.array([beta], dt)
     fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), be.ctypes.data, _ptr(c), _i(ldc))
@@ -245,6 +256,40 @@ def dsyrk_device(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
                                             _ptr(c), ldc, _stream(stream))
     check(st, "zynum_blas_gpu_dsyrk_device")
     return c
+
+
+def trsm_device_c(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream=None):
+    """Device ztrsm / ctrsm on complex128 / complex64 torch tensors (in place on b)."""
+    import torch
+    L = load()
+    z = b.dtype == torch.complex128
+    fn, dt = (L.zynum_blas_gpu_ztrsm_device, np.complex128) if z else (L.zynum_blas_gpu_ctrsm_device, np.complex64)
+    al = _cscalar(dt, alpha)
+    st = fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb,
+            _stream(stream))
+    check(st, "zynum_blas_gpu_ztrsm_device" if z else "zynum_blas_gpu_ctrsm_device")
+    return b
+
+
+def syrk_device_c(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
+    """Device zsyrk / csyrk on complex128 / complex64 torch tensors (c's triangle)."""
+    import torch
+    L = load()
+    z = c.dtype == torch.complex128
+    fn, dt = (L.zynum_blas_gpu_zsyrk_device, np.complex128) if z else (L.zynum_blas_gpu_csyrk_device, np.complex64)
+    al, be = _cscalar(dt, alpha), _cscalar(dt, beta)
+    st = fn(_ch(uplo), _ch(trans), n, k, al.ctypes.data, _ptr(a), lda, be.ctypes.data, _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_zsyrk_device" if z else "zynum_blas_gpu_csyrk_device")
+    return c
+
+
+def cblas_trsm_c(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """cblas_ztrsm / cblas_ctrsm (dtype from b)."""
+    L = load()
+    fn = L.cblas_ztrsm if b.dtype == np.complex128 else L.cblas_ctrsm
+    al = np.array([alpha], b.dtype)
+    fn(layout, side, uplo, transa, diag, m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb)
+    return b
 
 
 def symm_device(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):

@@ -648,6 +648,62 @@ cudaError_t run_syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, 
     }
 }
 
+// Scratch that covers every complex GEMM of shape up to m x n x k under either
+// complex method (the plane buffers plus the real GEMMs they run).
+template <typename R>
+size_t complex_scratch_bound(int m, int n, int k) {
+    const size_t m4 = complex_plane_bytes<R>(COMPLEX_4M, m, n, k) + real_scratch_bound<R>(2 * m, n, 2 * k);
+    const size_t m3 = complex_plane_bytes<R>(COMPLEX_3M, m, n, k) + real_scratch_bound<R>(m, n, k);
+    return std::max(m4, m3) + 4096;
+}
+
+// GEMMs inside a complex TRSM: the complex GEMM route with a fixed scratch region.
+template <typename R>
+GemmFn<cnum<R>> gemm_fn_c(cudaStream_t st, FixedScratch* fs) {
+    return [st, fs](const GemmArgs<cnum<R>>& g) -> cudaError_t {
+        if (g.m <= 0 || g.n <= 0) return cudaSuccess;
+        ComplexArgs<R> cg{g.transa, g.transb, g.m, g.n, g.k, {g.alpha.re, g.alpha.im},
+                          reinterpret_cast<const R*>(g.a), g.lda, reinterpret_cast<const R*>(g.b), g.ldb,
+                          {g.beta.re, g.beta.im}, reinterpret_cast<R*>(g.c), g.ldc};
+        return run_complex(cg, st, *fs);
+    };
+}
+
+// Complex TRSM (ztrsm_ / ctrsm_): the recursive solve with complex GEMM couplings.
+template <typename R, typename Scratch>
+cudaError_t run_trsm(const TrsmArgs<cnum<R>>& t, cudaStream_t st, Scratch scratch) {
+    if (t.m <= 0 || t.n <= 0) return cudaSuccess;
+    const size_t planes = trsm_plane_bytes<cnum<R>>(t.side, t.m, t.n);
+    const int na = (t.side == 'L') ? t.m : t.n;
+    const size_t real = complex_scratch_bound<R>(t.m, t.n, na);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return trsm<cnum<R>>(t, ws, gemm_fn_c<R>(st, &fs), st);
+}
+
+// Complex SYRK (zsyrk_ / csyrk_, symmetric.zig:180-199 with herm = false): one
+// complex GEMM W = op(A) op(A)^T into scratch, then C := alpha W + beta C on
+// the triangle.  trans = C takes op(A) = A^H, so op(A) op(A)^T = conj(A^T A).
+template <typename R, typename Scratch>
+cudaError_t run_syrk_c(char uplo, char trans, int n, int k, cnum<R> alpha, const cnum<R>* a, long lda, cnum<R> beta,
+                       cnum<R>* c, long ldc, cudaStream_t st, Scratch scratch) {
+    if (n <= 0) return cudaSuccess;
+    if (k == 0 || alpha == cnum<R>(0)) return syrk_scale_only<cnum<R>>(n, uplo, beta, c, ldc, st);
+    const size_t wbytes = ((size_t)n * n * sizeof(cnum<R>) + 1023) & ~size_t(1023);
+    const size_t cb = complex_scratch_bound<R>(n, n, k);
+    void* ws = nullptr;
+    cudaError_t e = scratch(wbytes + cb, st, &ws);
+    if (e != cudaSuccess) return e;
+    cnum<R>* W = static_cast<cnum<R>*>(ws);
+    const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
+    ComplexArgs<R> cg{t1, t2, n, n, k, {R(1), R(0)}, reinterpret_cast<const R*>(a), lda, reinterpret_cast<const R*>(a),
+                      lda, {R(0), R(0)}, reinterpret_cast<R*>(W), n};
+    if ((e = run_complex(cg, st, FixedScratch{static_cast<char*>(ws) + wbytes, cb})) != cudaSuccess) return e;
+    return triangle_update<cnum<R>>(uplo, false, n, alpha, W, n, beta, c, ldc, st, trans == 'C');
+}
+
 template <typename T>
 void host_trsm(const char* routine, char side, char uplo, char trans, char diag, int m, int n, T alpha, const T* a,
                int lda, T* b, int ldb, bool multiply = false) {
@@ -676,7 +732,10 @@ void host_trsm(const char* routine, char side, char uplo, char trans, char diag,
         e = cudaMemcpy2DAsync(db, (size_t)m * es, b, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         const TrsmArgs<T> t{side, uplo, trans, diag, m, n, alpha, da, na, db, m};
-        e = multiply ? run_trmm(t, st, HostScratch{&cx}) : run_trsm(t, st, HostScratch{&cx});
+        if constexpr (is_cnum<T>::value)
+            e = run_trsm(t, st, HostScratch{&cx});
+        else
+            e = multiply ? run_trmm(t, st, HostScratch{&cx}) : run_trsm(t, st, HostScratch{&cx});
     }
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
@@ -840,6 +899,71 @@ void host_syr2k(const char* routine, char uplo, char trans, int n, int k, T alph
     }
 }
 
+// Complex SYRK on host arrays: C staged whole so the other triangle comes back bit-identical.
+template <typename R>
+void host_syrk_c(const char* routine, char uplo, char trans, int n, int k, cnum<R> alpha, const cnum<R>* a, int lda,
+                 cnum<R> beta, cnum<R>* c, int ldc) {
+    if (n <= 0) return;
+    Context& cx = context();
+    std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+    cudaError_t e = cx.init();
+    if (e != cudaSuccess) {
+        cuda_status(e, "initialisation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cudaStream_t st = cx.stream;
+    const int ra = (trans == 'N') ? n : k, ca = (trans == 'N') ? k : n;
+    const size_t es = sizeof(cnum<R>);
+    if ((k > 0 && (e = cx.reserve(cx.stage_a, (size_t)ra * ca * es, st)) != cudaSuccess) ||
+        (e = cx.reserve(cx.stage_c, (size_t)n * n * es, st)) != cudaSuccess) {
+        cuda_status(e, "staging reservation");
+        report_gpu_failure(routine);
+        return;
+    }
+    cnum<R>* da = static_cast<cnum<R>*>(cx.stage_a.ptr);
+    cnum<R>* dc = static_cast<cnum<R>*>(cx.stage_c.ptr);
+    e = cudaSuccess;
+    if (k > 0)
+        e = cudaMemcpy2DAsync(da, (size_t)ra * es, a, (size_t)lda * es, (size_t)ra * es, ca, cudaMemcpyHostToDevice,
+                              st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dc, (size_t)n * es, c, (size_t)ldc * es, (size_t)n * es, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = run_syrk_c<R>(uplo, trans, n, k, alpha, da, ra, beta, dc, n, st, HostScratch{&cx});
+    if (e == cudaSuccess) e = cx.sync(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "GPU execution");
+        report_gpu_failure(routine);
+        return;
+    }
+    e = cudaMemcpy2DAsync(c, (size_t)ldc * es, dc, (size_t)n * es, (size_t)n * es, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cuda_status(e, "result copy");
+        report_gpu_failure(routine);
+    }
+}
+
+template <typename R>
+int device_syrk_c(const char* what, char uplo, char trans, int n, int k, const R* alpha, const R* a, int lda,
+                  const R* beta, R* c, int ldc, void* stream) {
+    const char ul = up(&uplo), tr = up(&trans);
+    int info = syrk_error(ul, tr, n, k, lda, ldc);
+    if (info) return info;
+    if (n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_syrk_c<R>(ul, tr, n, k, cnum<R>(alpha[0], alpha[1]), reinterpret_cast<const cnum<R>*>(a),
+                                     lda, cnum<R>(beta[0], beta[1]), reinterpret_cast<cnum<R>*>(c), ldc,
+                                     static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+                       what);
+}
+
 template <typename T>
 int device_trsm(const char* what, char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
                 int lda, T* b, int ldb, void* stream, bool multiply = false) {
@@ -856,7 +980,11 @@ int device_trsm(const char* what, char side, char uplo, char transa, char diag, 
     if (e != cudaSuccess) return cuda_status(e, "initialisation");
     const TrsmArgs<T> t{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb};
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return cuda_status(multiply ? run_trmm(t, st, StreamScratch{&cx}) : run_trsm(t, st, StreamScratch{&cx}), what);
+    if constexpr (is_cnum<T>::value)
+        return cuda_status(run_trsm(t, st, StreamScratch{&cx}), what);
+    else
+        return cuda_status(multiply ? run_trmm(t, st, StreamScratch{&cx}) : run_trsm(t, st, StreamScratch{&cx}),
+                           what);
 }
 
 template <typename T>
@@ -1160,6 +1288,99 @@ int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alph
 int zynum_blas_gpu_ssyrk_device(char uplo, char trans, int n, int k, float alpha, const float* a, int lda, float beta,
                                 float* c, int ldc, void* stream) {
     return device_syrk<float>("ssyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
+}
+
+// fortran.zig:877-884 ctrsm_ / ztrsm_, :810-817 csyrk_ / zsyrk_ (interleaved complex, alpha / beta by pointer)
+#define ZB_TRSM_C(NAME, R, RNAME)                                                                                  \
+    void NAME(const char* side, const char* uplo, const char* transa, const char* diag, const zynum_blas_int* m,  \
+              const zynum_blas_int* n, const void* alpha, const void* a, const zynum_blas_int* lda, void* b,      \
+              const zynum_blas_int* ldb) {                                                                        \
+        const char sd = up(side), ul = up(uplo), tr = up(transa), dg = up(diag);                                   \
+        int info = trsm_error(sd, ul, tr, dg, *m, *n, *lda, *ldb);                                                 \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        const R* al = static_cast<const R*>(alpha);                                                                \
+        host_trsm<cnum<R>>(RNAME, sd, ul, tr, dg, *m, *n, cnum<R>(al[0], al[1]), static_cast<const cnum<R>*>(a),  \
+                           *lda, static_cast<cnum<R>*>(b), *ldb);                                                  \
+    }
+ZB_TRSM_C(ztrsm_, double, "ZTRSM ")
+ZB_TRSM_C(ctrsm_, float, "CTRSM ")
+#undef ZB_TRSM_C
+
+#define ZB_SYRK_C(NAME, R, RNAME)                                                                                  \
+    void NAME(const char* uplo, const char* trans, const zynum_blas_int* n, const zynum_blas_int* k,              \
+              const void* alpha, const void* a, const zynum_blas_int* lda, const void* beta, void* c,             \
+              const zynum_blas_int* ldc) {                                                                        \
+        const char ul = up(uplo), tr = up(trans);                                                                  \
+        int info = syrk_error(ul, tr, *n, *k, *lda, *ldc);                                                         \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        const R* al = static_cast<const R*>(alpha);                                                                \
+        const R* be = static_cast<const R*>(beta);                                                                 \
+        host_syrk_c<R>(RNAME, ul, tr, *n, *k, cnum<R>(al[0], al[1]), static_cast<const cnum<R>*>(a), *lda,         \
+                       cnum<R>(be[0], be[1]), static_cast<cnum<R>*>(c), *ldc);                                     \
+    }
+ZB_SYRK_C(zsyrk_, double, "ZSYRK ")
+ZB_SYRK_C(csyrk_, float, "CSYRK ")
+#undef ZB_SYRK_C
+
+// cblas.zig:1755-1779 cblas_ctrsm / cblas_ztrsm (enums checked, silent return) and :1560-1582
+// cblas_csyrk / cblas_zsyrk (layout only)
+#define ZB_CBLAS_TRSM_C(NAME, FNAME)                                                                                \
+    void NAME(int layout, int side, int uplo, int transa, int diag, int m, int n, const void* alpha, const void* a, \
+              int lda, void* b, int ldb) {                                                                          \
+        if (!cblas_valid_layout(layout) || (side != CblasLeft && side != CblasRight) ||                             \
+            (uplo != CblasUpper && uplo != CblasLower) || !cblas_valid_trans(transa) ||                             \
+            (diag != CblasNonUnit && diag != CblasUnit))                                                            \
+            return;                                                                                                 \
+        const bool rm = layout == CblasRowMajor;                                                                    \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                           \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                           \
+        char tt = cblas_trans_char(transa), dd = cblas_diag_char(diag);                                             \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb;                                        \
+        FNAME(&ss, &uu, &tt, &dd, &mm, &nn, alpha, a, &la, b, &lb);                                                 \
+    }
+ZB_CBLAS_TRSM_C(cblas_ztrsm, ztrsm_)
+ZB_CBLAS_TRSM_C(cblas_ctrsm, ctrsm_)
+#undef ZB_CBLAS_TRSM_C
+
+#define ZB_CBLAS_SYRK_C(NAME, FNAME)                                                                            \
+    void NAME(int layout, int uplo, int trans, int n, int k, const void* alpha, const void* a, int lda,        \
+              const void* beta, void* c, int ldc) {                                                             \
+        if (!cblas_valid_layout(layout)) return;                                                                \
+        const bool rm = layout == CblasRowMajor;                                                                \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                       \
+        char tt = rm ? cblas_row_trans_char(trans) : cblas_trans_char(trans);                                   \
+        zynum_blas_int nn = n, kk = k, la = lda, lc = ldc;                                                      \
+        FNAME(&uu, &tt, &nn, &kk, alpha, a, &la, beta, c, &lc);                                                 \
+    }
+ZB_CBLAS_SYRK_C(cblas_zsyrk, zsyrk_)
+ZB_CBLAS_SYRK_C(cblas_csyrk, csyrk_)
+#undef ZB_CBLAS_SYRK_C
+
+int zynum_blas_gpu_ztrsm_device(char side, char uplo, char transa, char diag, int m, int n, const double* alpha,
+                                const double* a, int lda, double* b, int ldb, void* stream) {
+    return device_trsm<cnum<double>>("ztrsm_device", side, uplo, transa, diag, m, n, cnum<double>(alpha[0], alpha[1]),
+                                     reinterpret_cast<const cnum<double>*>(a), lda, reinterpret_cast<cnum<double>*>(b),
+                                     ldb, stream);
+}
+int zynum_blas_gpu_ctrsm_device(char side, char uplo, char transa, char diag, int m, int n, const float* alpha,
+                                const float* a, int lda, float* b, int ldb, void* stream) {
+    return device_trsm<cnum<float>>("ctrsm_device", side, uplo, transa, diag, m, n, cnum<float>(alpha[0], alpha[1]),
+                                    reinterpret_cast<const cnum<float>*>(a), lda, reinterpret_cast<cnum<float>*>(b),
+                                    ldb, stream);
+}
+int zynum_blas_gpu_zsyrk_device(char uplo, char trans, int n, int k, const double* alpha, const double* a, int lda,
+                                const double* beta, double* c, int ldc, void* stream) {
+    return device_syrk_c<double>("zsyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
+}
+int zynum_blas_gpu_csyrk_device(char uplo, char trans, int n, int k, const float* alpha, const float* a, int lda,
+                                const float* beta, float* c, int ldc, void* stream) {
+    return device_syrk_c<float>("csyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
 }
 
 // fortran.zig:777-783 ?symm_, :852-858 ?trmm_, :827-833 ?syr2k_

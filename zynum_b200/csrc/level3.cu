@@ -35,6 +35,7 @@
 //   recursive halving on block boundaries, one GEMM (beta = 1) per level and
 //   half.  Reading W rather than B makes every GEMM independent of the order.
 #include <functional>
+#include <type_traits>
 
 #include "common.cuh"
 #include "level3.h"
@@ -61,7 +62,7 @@ ZB_DEVICE T op_tri(const T* a, long lda, char uplo, char trans, char diag, int r
     if (ar == ac && diag == 'U') return T(1);
     if (uplo == 'U' && ar > ac) return T(0);
     if (uplo == 'L' && ar < ac) return T(0);
-    return a[ar + (long)ac * lda];
+    return conj_if(a[ar + (long)ac * lda], trans == 'C');  // op = C conjugates (access.zig:54-63)
 }
 
 // Block b: inverse of the diagonal block op(A)[b*64 .. , b*64 ..] of size
@@ -124,8 +125,8 @@ constexpr int kLeafCols = 16;
 
 template <typename T>
 __global__ void __launch_bounds__(256)
-trsm_leaf(const T* __restrict__ a, long lda, int trans_n, int left, int fwd, const T* __restrict__ inv, int p0,
-          int len, T* __restrict__ b, long ldb, int ncols) {
+trsm_leaf(const T* __restrict__ a, long lda, int trans_n, int conj_a, int left, int fwd, const T* __restrict__ inv,
+          int p0, int len, T* __restrict__ b, long ldb, int ncols) {
     extern __shared__ __align__(16) unsigned char leaf_smem[];
     T(*Z)[kLeafCols + 1] = reinterpret_cast<T(*)[kLeafCols + 1]>(leaf_smem);
     T(*W)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(leaf_smem + sizeof(T) * kLeaf * (kLeafCols + 1));
@@ -150,7 +151,7 @@ trsm_leaf(const T* __restrict__ a, long lda, int trans_n, int left, int fwd, con
             T v = T(0);
             if (gi < len && gj < len) {
                 const int r = left ? p0 + gi : p0 + gj, c = left ? p0 + gj : p0 + gi;
-                v = trans_n ? a[r + (long)c * lda] : a[c + (long)r * lda];
+                v = conj_if(trans_n ? a[r + (long)c * lda] : a[c + (long)r * lda], conj_a != 0);
             }
             W[i][j] = v;
         }
@@ -496,7 +497,7 @@ constexpr int kTrmmNB = 256;
 // through a shared-memory transpose; tiles outside the triangle return at once.
 // Block (32, 8).
 template <typename T>
-__global__ void tri_update(int n, int upper, int two, T alpha, const T* __restrict__ w, long ldw, T beta,
+__global__ void tri_update(int n, int upper, int two, int conj_w, T alpha, const T* __restrict__ w, long ldw, T beta,
                            T* __restrict__ c, long ldc) {
     __shared__ T t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
@@ -512,7 +513,7 @@ __global__ void tri_update(int n, int upper, int two, T alpha, const T* __restri
     for (int y = ty; y < 32; y += 8) {
         const int i = r0 + tx, j = c0 + y;
         if (i >= n || j >= n || (upper ? i > j : i < j)) continue;
-        T v = w[i + (long)j * ldw];
+        T v = conj_if(w[i + (long)j * ldw], conj_w != 0);
         if (two) v = v + t[tx][y];
         T* cp = c + i + (long)j * ldc;
         *cp = beta == T(0) ? alpha * v : fma(beta, *cp, alpha * v);
@@ -523,17 +524,22 @@ __global__ void tri_update(int n, int upper, int two, T alpha, const T* __restri
 
 template <typename T>
 cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool conj_w) {
     if (n <= 0) return cudaSuccess;
     dim3 grid((n + 31) / 32, (n + 31) / 32);
-    tri_update<T><<<grid, dim3(32, 8), 0, st>>>(n, uplo == 'U' ? 1 : 0, two ? 1 : 0, alpha, w, ldw, beta, c, ldc);
+    tri_update<T><<<grid, dim3(32, 8), 0, st>>>(n, uplo == 'U' ? 1 : 0, two ? 1 : 0, conj_w ? 1 : 0, alpha, w, ldw,
+                                                beta, c, ldc);
     count_launch();
     return cudaGetLastError();
 }
 template cudaError_t triangle_update<double>(char, bool, int, double, const double*, long, double, double*, long,
-                                             cudaStream_t);
+                                             cudaStream_t, bool);
 template cudaError_t triangle_update<float>(char, bool, int, float, const float*, long, float, float*, long,
-                                            cudaStream_t);
+                                            cudaStream_t, bool);
+template cudaError_t triangle_update<cnum<double>>(char, bool, int, cnum<double>, const cnum<double>*, long,
+                                                   cnum<double>, cnum<double>*, long, cudaStream_t, bool);
+template cudaError_t triangle_update<cnum<float>>(char, bool, int, cnum<float>, const cnum<float>*, long, cnum<float>,
+                                                  cnum<float>*, long, cudaStream_t, bool);
 
 template <typename T>
 size_t symm_plane_bytes(char side, int m, int n) {
@@ -649,13 +655,13 @@ constexpr int kApplyMaxCols = 1024;
 template <typename T>
 size_t leaf_plane_bytes(int na) {
     const long nleaf = (na + kLeaf - 1) / kLeaf;
-    return sizeof(T) == 8 ? (((size_t)nleaf * kLeaf * kLeaf * sizeof(T) + 1023) & ~size_t(1023)) : 0;
+    return std::is_same<T, double>::value ? (((size_t)nleaf * kLeaf * kLeaf * sizeof(T) + 1023) & ~size_t(1023)) : 0;
 }
 
 template <typename T>
 size_t trsm_plane_bytes(char side, int m, int n) {
     const int na = (side == 'L') ? m : n, ncols = (side == 'L') ? n : m;
-    const size_t copy = (sizeof(T) == 8 && ncols > kApplyMaxCols) ? (size_t)kLeaf * ncols * sizeof(T) : 0;
+    const size_t copy = (std::is_same<T, double>::value && ncols > kApplyMaxCols) ? (size_t)kLeaf * ncols * sizeof(T) : 0;
     return inv_plane_bytes<T>(na) + leaf_plane_bytes<T>(na) + copy;
 }
 
@@ -678,7 +684,8 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const bool upper = op_is_upper(t.uplo, t.trans);
-    const char ta = (t.trans == 'N') ? 'N' : 'T';
+    // the GEMM operand op(A): complex keeps C (conjugate transpose), real reads C as T
+    const char ta = (t.trans == 'N') ? 'N' : (is_cnum<T>::value ? t.trans : 'T');
     const long lda = t.lda, ldb = t.ldb;
     // op(A)[r0:r1, c0:c1] as a GEMM operand (pointer, transpose flag)
     auto opa = [&](int r0, int c0) -> const T* {
@@ -690,7 +697,8 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     // over the right-hand sides, in place.  FP64 with a 16-byte aligned A and an
     // even lda (16-byte operand copies) applies precomputed leaf inverses on
     // the tensor pipe; otherwise trsm_leaf solves phase by phase.
-    const bool inv_leaves = sizeof(T) == 8 && reinterpret_cast<uintptr_t>(t.a) % 16 == 0 && t.lda % 2 == 0;
+    const bool inv_leaves =
+        std::is_same<T, double>::value && reinterpret_cast<uintptr_t>(t.a) % 16 == 0 && t.lda % 2 == 0;
     const int ncols = left ? n : m;
     const int fwd = left ? !upper : upper;
     int leaf_smem;
@@ -740,8 +748,8 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
                                                                   fwd, p0, len, reinterpret_cast<double*>(t.b), ldb,
                                                                   ncols);
             else
-                trsm_leaf<T><<<grid, 256, leaf_smem, st>>>(t.a, lda, ta == 'N', left, fwd, inv, p0, len, t.b, ldb,
-                                                           ncols);
+                trsm_leaf<T><<<grid, 256, leaf_smem, st>>>(t.a, lda, ta == 'N', is_cnum<T>::value && t.trans == 'C',
+                                                           left, fwd, inv, p0, len, t.b, ldb, ncols);
             count_launch();
             return cudaGetLastError();
         }
@@ -790,6 +798,14 @@ template size_t trsm_plane_bytes<double>(char, int, int);
 template size_t trsm_plane_bytes<float>(char, int, int);
 template cudaError_t trsm<double>(const TrsmArgs<double>&, void*, const GemmFn<double>&, cudaStream_t);
 template cudaError_t trsm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t);
+template size_t trsm_plane_bytes<cnum<double>>(char, int, int);
+template size_t trsm_plane_bytes<cnum<float>>(char, int, int);
+template cudaError_t trsm<cnum<double>>(const TrsmArgs<cnum<double>>&, void*, const GemmFn<cnum<double>>&,
+                                        cudaStream_t);
+template cudaError_t trsm<cnum<float>>(const TrsmArgs<cnum<float>>&, void*, const GemmFn<cnum<float>>&,
+                                       cudaStream_t);
+template cudaError_t syrk_scale_only<cnum<double>>(int, char, cnum<double>, cnum<double>*, long, cudaStream_t);
+template cudaError_t syrk_scale_only<cnum<float>>(int, char, cnum<float>, cnum<float>*, long, cudaStream_t);
 template cudaError_t syrk_scale_only<double>(int, char, double, double*, long, cudaStream_t);
 template cudaError_t syrk_scale_only<float>(int, char, float, float*, long, cudaStream_t);
 template size_t symm_plane_bytes<double>(char, int, int);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "kernels.h"
+#include "cnum.cuh"
 
 namespace zb {
 
@@ -52,11 +53,11 @@ template <typename T>
 cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
 
 // C := alpha (W + W^T) + beta C (two) or alpha W + beta C on the uplo triangle
-// of the n x n C (SYRK / SYR2K from a full product W; beta == 0 writes zeros
-// over NaN).
+// of the n x n C (SYRK / SYR2K from a full product W, conj(W) in place of W
+// when conj_w; beta == 0 writes zeros over NaN).
 template <typename T>
 cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
-                            cudaStream_t st);
+                            cudaStream_t st, bool conj_w = false);
 
 // Copy the uplo triangle of the n x n matrix c onto the other triangle.
 template <typename T>
