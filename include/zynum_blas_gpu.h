@@ -91,6 +91,48 @@ ZYNUM_BLAS_GPU_API void csyrk_(const char *uplo, const char *trans, const zynum_
 ZYNUM_BLAS_GPU_API void zsyrk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
                                const void *alpha, const void *a, const zynum_blas_int *lda, const void *beta, void *c,
                                const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:785-799 csymm_ / zsymm_ / chemm_ / zhemm_ (A symmetric, or Hermitian:
+ * the unstored triangle is the conjugate mirror and the diagonal's imaginary part is ignored) */
+ZYNUM_BLAS_GPU_API void csymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                               const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zsymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                               const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void chemm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                               const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zhemm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
+                               const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                               const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:818-825 cherk_ / zherk_ (C := alpha op(A) op(A)^H + beta C, alpha and beta real) */
+ZYNUM_BLAS_GPU_API void cherk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const float *alpha, const void *a, const zynum_blas_int *lda, const float *beta,
+                               void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zherk_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                               const double *alpha, const void *a, const zynum_blas_int *lda, const double *beta,
+                               void *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:835-849 csyr2k_ / zsyr2k_ (C := alpha (op(A) op(B)^T + op(B) op(A)^T) + beta C),
+ * cher2k_ / zher2k_ (C := alpha op(A) op(B)^H + conj(alpha) op(B) op(A)^H + beta C, beta real) */
+ZYNUM_BLAS_GPU_API void csyr2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                                const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zsyr2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                                const zynum_blas_int *ldb, const void *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void cher2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                                const zynum_blas_int *ldb, const float *beta, void *c, const zynum_blas_int *ldc);
+ZYNUM_BLAS_GPU_API void zher2k_(const char *uplo, const char *trans, const zynum_blas_int *n, const zynum_blas_int *k,
+                                const void *alpha, const void *a, const zynum_blas_int *lda, const void *b,
+                                const zynum_blas_int *ldb, const double *beta, void *c, const zynum_blas_int *ldc);
+/* src/blas/abi/fortran.zig:860-867 ctrmm_ / ztrmm_ (B := alpha op(A) B or alpha B op(A), op = C conjugates) */
+ZYNUM_BLAS_GPU_API void ctrmm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const void *alpha, const void *a,
+                               const zynum_blas_int *lda, void *b, const zynum_blas_int *ldb);
+ZYNUM_BLAS_GPU_API void ztrmm_(const char *side, const char *uplo, const char *transa, const char *diag,
+                               const zynum_blas_int *m, const zynum_blas_int *n, const void *alpha, const void *a,
+                               const zynum_blas_int *lda, void *b, const zynum_blas_int *ldb);
 /* src/blas/abi/fortran.zig:777-783 ssymm_ / dsymm_ (C := alpha A B + beta C or alpha B A + beta C, A symmetric) */
 ZYNUM_BLAS_GPU_API void ssymm_(const char *side, const char *uplo, const zynum_blas_int *m, const zynum_blas_int *n,
                                const float *alpha, const float *a, const zynum_blas_int *lda, const float *b,
@@ -155,6 +197,34 @@ ZYNUM_BLAS_GPU_API void cblas_csyrk(int layout, int uplo, int trans, int n, int 
                                     int lda, const void *beta, void *c, int ldc);
 ZYNUM_BLAS_GPU_API void cblas_zsyrk(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
                                     int lda, const void *beta, void *c, int ldc);
+/* src/blas/abi/cblas.zig:1491-1537 cblas_csymm / cblas_zsymm / cblas_chemm / cblas_zhemm (scalars by pointer) */
+ZYNUM_BLAS_GPU_API void cblas_csymm(int layout, int side, int uplo, int m, int n, const void *alpha, const void *a,
+                                    int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zsymm(int layout, int side, int uplo, int m, int n, const void *alpha, const void *a,
+                                    int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_chemm(int layout, int side, int uplo, int m, int n, const void *alpha, const void *a,
+                                    int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zhemm(int layout, int side, int uplo, int m, int n, const void *alpha, const void *a,
+                                    int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+/* src/blas/abi/cblas.zig:1583-1603 cblas_cherk / cblas_zherk (alpha, beta real, by value) */
+ZYNUM_BLAS_GPU_API void cblas_cherk(int layout, int uplo, int trans, int n, int k, float alpha, const void *a,
+                                    int lda, float beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zherk(int layout, int uplo, int trans, int n, int k, double alpha, const void *a,
+                                    int lda, double beta, void *c, int ldc);
+/* src/blas/abi/cblas.zig:1629-1676 cblas_csyr2k / cblas_zsyr2k, cblas_cher2k / cblas_zher2k (beta real, by value) */
+ZYNUM_BLAS_GPU_API void cblas_csyr2k(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                     int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zsyr2k(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                     int lda, const void *b, int ldb, const void *beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_cher2k(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                     int lda, const void *b, int ldb, float beta, void *c, int ldc);
+ZYNUM_BLAS_GPU_API void cblas_zher2k(int layout, int uplo, int trans, int n, int k, const void *alpha, const void *a,
+                                     int lda, const void *b, int ldb, double beta, void *c, int ldc);
+/* src/blas/abi/cblas.zig:1703-1728 cblas_ctrmm / cblas_ztrmm (alpha by pointer) */
+ZYNUM_BLAS_GPU_API void cblas_ctrmm(int layout, int side, int uplo, int transa, int diag, int m, int n,
+                                    const void *alpha, const void *a, int lda, void *b, int ldb);
+ZYNUM_BLAS_GPU_API void cblas_ztrmm(int layout, int side, int uplo, int transa, int diag, int m, int n,
+                                    const void *alpha, const void *a, int lda, void *b, int ldb);
 /* src/blas/abi/cblas.zig:1467-1489 cblas_ssymm / cblas_dsymm */
 ZYNUM_BLAS_GPU_API void cblas_ssymm(int layout, int side, int uplo, int m, int n, float alpha, const float *a, int lda,
                                     const float *b, int ldb, float beta, float *c, int ldc);

@@ -55,6 +55,14 @@ def _declare(L):
     L.oracle_strmm.argtypes = [ch, ch, ch, ch, i32, i32, f32, vp, i32, vp, i32]
     L.oracle_dsyr2k.argtypes = [ch, ch, i32, i32, f64, vp, i32, vp, i32, f64, vp, i32]
     L.oracle_ssyr2k.argtypes = [ch, ch, i32, i32, f32, vp, i32, vp, i32, f32, vp, i32]
+    for name in ("oracle_zsymm", "oracle_csymm"):
+        getattr(L, name).argtypes = [ch, ch, i32, i32, vp, vp, i32, vp, i32, vp, vp, i32, C.c_int]
+    for name in ("oracle_ztrmm", "oracle_ctrmm"):
+        getattr(L, name).argtypes = [ch, ch, ch, ch, i32, i32, vp, vp, i32, vp, i32]
+    L.oracle_zherk.argtypes = [ch, ch, i32, i32, f64, vp, i32, f64, vp, i32]
+    L.oracle_cherk.argtypes = [ch, ch, i32, i32, f32, vp, i32, f32, vp, i32]
+    for name in ("oracle_zsyr2k", "oracle_csyr2k"):
+        getattr(L, name).argtypes = [ch, ch, i32, i32, vp, vp, i32, vp, i32, vp, vp, i32, C.c_int]
 
 
 def _p(a: np.ndarray):
@@ -132,8 +140,14 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     return c
 
 
-def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """In place on c; dtype from c.  herm (complex only): A Hermitian (zhemm / chemm)."""
     L = lib()
+    if np.iscomplexobj(c):
+        f = L.oracle_zsymm if c.dtype == np.complex128 else L.oracle_csymm
+        al, be = np.array([alpha], dtype=c.dtype), np.array([beta], dtype=c.dtype)
+        f(_b(side), _b(uplo), m, n, al.ctypes.data, _p(a), lda, _p(b), ldb, be.ctypes.data, _p(c), ldc, int(herm))
+        return c
     f = L.oracle_dsymm if c.dtype == np.float64 else L.oracle_ssymm
     f(_b(side), _b(uplo), m, n, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
     return c
@@ -141,13 +155,32 @@ def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
 
 def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     L = lib()
+    if np.iscomplexobj(b):
+        f = L.oracle_ztrmm if b.dtype == np.complex128 else L.oracle_ctrmm
+        al = np.array([alpha], dtype=b.dtype)
+        f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, al.ctypes.data, _p(a), lda, _p(b), ldb)
+        return b
     f = L.oracle_dtrmm if b.dtype == np.float64 else L.oracle_strmm
     f(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha, _p(a), lda, _p(b), ldb)
     return b
 
 
-def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """In place on c's triangle.  herm (complex only): zher2k / cher2k (beta real)."""
     L = lib()
+    if np.iscomplexobj(c):
+        f = L.oracle_zsyr2k if c.dtype == np.complex128 else L.oracle_csyr2k
+        al, be = np.array([alpha], dtype=c.dtype), np.array([beta], dtype=c.dtype)
+        f(_b(uplo), _b(trans), n, k, al.ctypes.data, _p(a), lda, _p(b), ldb, be.ctypes.data, _p(c), ldc, int(herm))
+        return c
     f = L.oracle_dsyr2k if c.dtype == np.float64 else L.oracle_ssyr2k
     f(_b(uplo), _b(trans), n, k, alpha, _p(a), lda, _p(b), ldb, beta, _p(c), ldc)
+    return c
+
+
+def herk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """zherk / cherk in place on c's triangle (alpha, beta real; diagonal made real)."""
+    L = lib()
+    f = L.oracle_zherk if c.dtype == np.complex128 else L.oracle_cherk
+    f(_b(uplo), _b(trans), n, k, float(alpha), _p(a), lda, float(beta), _p(c), ldc)
     return c

@@ -548,5 +548,165 @@ DEFINE_CX_TRSM(oracle_ctrsm, cxf)
 DEFINE_CX_SYRK(oracle_zsyrk, cxd)
 DEFINE_CX_SYRK(oracle_csyrk, cxf)
 
+/* ----------------------------------- complex SYMM / HEMM, TRMM, HERK, SYR2K / HER2K */
+
+/* matrixValue (access.zig:23-29): element (row, col) of op(X), conj for op = C;
+ * symValue (access.zig:31-42): stored triangle as is (diagonal real when herm),
+ * the other triangle mirrored, conjugated when herm. */
+#define DEFINE_CX_OPVAL(CT)                                                                   \
+    static inline CT CT##_opval(char trans, const CT *x, blas_int ld, size_t row, size_t col) { \
+        if (trans == 'N') return x[ix(ld, row, col)];                                         \
+        CT v = x[ix(ld, col, row)];                                                           \
+        return trans == 'C' ? CT##_conj(v) : v;                                               \
+    }                                                                                         \
+    static inline CT CT##_symval(char uplo, const CT *a, blas_int lda, size_t row, size_t col, int herm) { \
+        if ((uplo == 'U' && row <= col) || (uplo == 'L' && row >= col)) {                     \
+            CT v = a[ix(lda, row, col)];                                                      \
+            if (herm && row == col) v.im = 0;                                                 \
+            return v;                                                                         \
+        }                                                                                     \
+        CT v = a[ix(lda, col, row)];                                                          \
+        return herm ? CT##_conj(v) : v;                                                       \
+    }
+
+DEFINE_CX_OPVAL(cxd)
+DEFINE_CX_OPVAL(cxf)
+
+/* symmetric.zig:107-157 symm -> runSymmColumns: C := alpha A B + beta C (side L)
+ * or alpha B A + beta C (side R), A by symValue with herm (zsymm_ herm = false,
+ * zhemm_ herm = true, fortran.zig:785-799). */
+#define DEFINE_CX_SYMM(NAME, CT)                                                                     \
+    void NAME(char side, char uplo, blas_int m, blas_int n, const CT *alpha, const CT *a, blas_int lda, \
+              const CT *b, blas_int ldb, const CT *beta, CT *c, blas_int ldc, int herm) {             \
+        side = (char)upc(side); uplo = (char)upc(uplo);                                              \
+        if (m <= 0 || n <= 0) return;                                                                \
+        CT zero = {0, 0};                                                                            \
+        for (size_t j = 0; j < (size_t)n; ++j)                                                       \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                 \
+                CT sum = zero;                                                                       \
+                if (side == 'L') {                                                                   \
+                    for (size_t p = 0; p < (size_t)m; ++p)                                           \
+                        sum = CT##_add(sum, CT##_mul(CT##_symval(uplo, a, lda, i, p, herm), b[ix(ldb, p, j)])); \
+                } else {                                                                             \
+                    for (size_t p = 0; p < (size_t)n; ++p)                                           \
+                        sum = CT##_add(sum, CT##_mul(b[ix(ldb, i, p)], CT##_symval(uplo, a, lda, p, j, herm))); \
+                }                                                                                    \
+                size_t q = ix(ldc, i, j);                                                            \
+                c[q] = CT##_add(CT##_mul(*alpha, sum), CT##_is_zero(*beta) ? zero : CT##_mul(*beta, c[q])); \
+            }                                                                                        \
+    }
+
+DEFINE_CX_SYMM(oracle_zsymm, cxd)
+DEFINE_CX_SYMM(oracle_csymm, cxf)
+
+/* triangular.zig:202-231 trmm for complex types: left side trmv per column
+ * (op = C conjugates, triValue access.zig:54-64) then alpha when alpha != 1;
+ * right side per row, columns in the order that keeps later inputs intact. */
+#define DEFINE_CX_TRMM(NAME, CT)                                                                        \
+    void NAME(char side, char uplo, char trans, char diag, blas_int m, blas_int n, const CT *alpha,   \
+              const CT *a, blas_int lda, CT *b, blas_int ldb) {                                         \
+        side = (char)upc(side); uplo = (char)upc(uplo); trans = (char)upc(trans); diag = (char)upc(diag); \
+        if (m <= 0 || n <= 0) return;                                                                   \
+        int upper = op_is_upper(uplo, trans);                                                           \
+        CT zero = {0, 0};                                                                               \
+        if (side == 'L') {                                                                              \
+            for (size_t j = 0; j < (size_t)n; ++j) {                                                    \
+                CT *x = b + (size_t)ldb * j;                                                            \
+                if (upper) {                                                                            \
+                    for (size_t r = 0; r < (size_t)m; ++r) {                                            \
+                        CT t = zero;                                                                    \
+                        for (size_t q = r; q < (size_t)m; ++q)                                          \
+                            t = CT##_add(t, CT##_mul(CT##_tri(uplo, diag, trans, a, lda, r, q), x[q])); \
+                        x[r] = t;                                                                       \
+                    }                                                                                   \
+                } else {                                                                                \
+                    for (size_t r = (size_t)m; r-- > 0;) {                                              \
+                        CT t = zero;                                                                    \
+                        for (size_t q = 0; q <= r; ++q)                                                 \
+                            t = CT##_add(t, CT##_mul(CT##_tri(uplo, diag, trans, a, lda, r, q), x[q])); \
+                        x[r] = t;                                                                       \
+                    }                                                                                   \
+                }                                                                                       \
+                if (!CT##_is_one(*alpha))                                                               \
+                    for (size_t r = 0; r < (size_t)m; ++r) x[r] = CT##_mul(*alpha, x[r]);               \
+            }                                                                                           \
+        } else {                                                                                        \
+            for (size_t i = 0; i < (size_t)m; ++i) {                                                    \
+                for (size_t s = 0; s < (size_t)n; ++s) {                                                \
+                    size_t cc = upper ? (size_t)n - 1 - s : s;                                          \
+                    CT sum = zero;                                                                      \
+                    for (size_t p = 0; p < (size_t)n; ++p)                                              \
+                        sum = CT##_add(sum, CT##_mul(b[ix(ldb, i, p)], CT##_tri(uplo, diag, trans, a, lda, p, cc))); \
+                    b[ix(ldb, i, cc)] = CT##_mul(*alpha, sum);                                          \
+                }                                                                                       \
+            }                                                                                           \
+        }                                                                                               \
+    }
+
+DEFINE_CX_TRMM(oracle_ztrmm, cxd)
+DEFINE_CX_TRMM(oracle_ctrmm, cxf)
+
+/* symmetric.zig:180-199 runSyrkColumns with herm = true (zherk_ / cherk_,
+ * fortran.zig:818-825: alpha and beta real, widened by realScalar): sum of
+ * op(A)(i, p) conj(op(A)(j, p)), C := alpha sum + beta C, diagonal made real. */
+#define DEFINE_CX_HERK(NAME, CT, R)                                                                  \
+    void NAME(char uplo, char trans, blas_int n, blas_int k, R alpha_r, const CT *a, blas_int lda,  \
+              R beta_r, CT *c, blas_int ldc) {                                                       \
+        uplo = (char)upc(uplo); trans = (char)upc(trans);                                            \
+        if (n <= 0) return;                                                                          \
+        CT alpha = {alpha_r, 0}, beta = {beta_r, 0}, zero = {0, 0};                                  \
+        for (size_t j = 0; j < (size_t)n; ++j) {                                                     \
+            size_t r0 = (uplo == 'U') ? 0 : j, r1 = (uplo == 'U') ? j + 1 : (size_t)n;               \
+            for (size_t i = r0; i < r1; ++i) {                                                       \
+                CT sum = zero;                                                                       \
+                for (size_t p = 0; p < (size_t)(k > 0 ? k : 0); ++p)                                  \
+                    sum = CT##_add(sum, CT##_mul(CT##_opval(trans, a, lda, i, p),                    \
+                                                 CT##_conj(CT##_opval(trans, a, lda, j, p))));       \
+                size_t q = ix(ldc, i, j);                                                            \
+                c[q] = CT##_add(CT##_mul(alpha, sum), CT##_is_zero(beta) ? zero : CT##_mul(beta, c[q])); \
+                if (i == j) c[q].im = 0;                                                             \
+            }                                                                                        \
+        }                                                                                            \
+    }
+
+DEFINE_CX_HERK(oracle_zherk, cxd, double)
+DEFINE_CX_HERK(oracle_cherk, cxf, float)
+
+/* symmetric.zig:301-329 runSyr2kColumns for complex types: herm = false sums
+ * a_i b_j + b_i a_j and scales by alpha; herm = true sums alpha a_i conj(b_j) +
+ * conj(alpha) b_i conj(a_j) and makes the diagonal real (zher2k_ beta is real,
+ * fortran.zig:843-849). */
+#define DEFINE_CX_SYR2K(NAME, CT)                                                                       \
+    void NAME(char uplo, char trans, blas_int n, blas_int k, const CT *alpha, const CT *a, blas_int lda, \
+              const CT *b, blas_int ldb, const CT *beta, CT *c, blas_int ldc, int herm) {                \
+        uplo = (char)upc(uplo); trans = (char)upc(trans);                                               \
+        if (n <= 0) return;                                                                             \
+        CT zero = {0, 0};                                                                               \
+        for (size_t j = 0; j < (size_t)n; ++j) {                                                        \
+            size_t r0 = (uplo == 'U') ? 0 : j, r1 = (uplo == 'U') ? j + 1 : (size_t)n;                  \
+            for (size_t i = r0; i < r1; ++i) {                                                          \
+                CT sum = zero;                                                                          \
+                for (size_t p = 0; p < (size_t)(k > 0 ? k : 0); ++p) {                                   \
+                    CT ai = CT##_opval(trans, a, lda, i, p), bi = CT##_opval(trans, b, ldb, i, p);      \
+                    CT aj = CT##_opval(trans, a, lda, j, p), bj = CT##_opval(trans, b, ldb, j, p);      \
+                    if (herm) {                                                                         \
+                        aj = CT##_conj(aj); bj = CT##_conj(bj);                                         \
+                        sum = CT##_add(sum, CT##_add(CT##_mul(*alpha, CT##_mul(ai, bj)),                \
+                                                     CT##_mul(CT##_conj(*alpha), CT##_mul(bi, aj))));   \
+                    } else {                                                                            \
+                        sum = CT##_add(sum, CT##_add(CT##_mul(ai, bj), CT##_mul(bi, aj)));              \
+                    }                                                                                   \
+                }                                                                                       \
+                size_t q = ix(ldc, i, j);                                                               \
+                CT prod = herm ? sum : CT##_mul(*alpha, sum);                                           \
+                c[q] = CT##_add(prod, CT##_is_zero(*beta) ? zero : CT##_mul(*beta, c[q]));              \
+                if (herm && i == j) c[q].im = 0;                                                        \
+            }                                                                                           \
+        }                                                                                               \
+    }
+
+DEFINE_CX_SYR2K(oracle_zsyr2k, cxd)
+DEFINE_CX_SYR2K(oracle_csyr2k, cxf)
+
 /* Library self-identification for the loader in the tests. */
 int oracle_version(void) { return 1; }

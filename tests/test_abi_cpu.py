@@ -125,8 +125,14 @@ def test_abi_manifest_is_current_and_matches_reference():
     for part in ("fortran", "cblas"):
         assert report[part]["differ"] == [], report[part]["differ"]
         provided = set(report[part]["same"])
+        # every Level-3 export of the reference is provided: nothing reference-only
+        assert report[part]["reference_only"] == [], report[part]["reference_only"]
         for fam in ("gemm", "trsm", "syrk", "symm", "trmm", "syr2k"):
-            for p in "sd":
+            for p in "sdcz":
+                name = f"cblas_{p}{fam}" if part == "cblas" else f"{p}{fam}_"
+                assert name in provided, name
+        for fam in ("hemm", "herk", "her2k"):
+            for p in "cz":
                 name = f"cblas_{p}{fam}" if part == "cblas" else f"{p}{fam}_"
                 assert name in provided, name
     assert {"xerbla_", "lsame_", "zynum_blas_shutdown"} <= set(report["fortran"]["same"])

@@ -145,3 +145,97 @@ def test_syrk_triangle(oracle, uplo, trans):
     mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
     np.testing.assert_allclose(c[:n, :n][mask], full[mask], rtol=1e-12, atol=1e-12)
     assert np.array_equal(c[:n, :n][~mask], c0[:n, :n][~mask])
+
+
+def _cx(rng, shape, dtype=np.complex128):
+    return np.asfortranarray((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype))
+
+
+def _op(x, trans):
+    return x if trans == "N" else (x.T if trans == "T" else x.conj().T)
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("herm", [False, True])
+def test_complex_symm_hemm(oracle, side, uplo, herm):
+    """zsymm / zhemm: the stored triangle mirrored (conjugated, diagonal real for HEMM)."""
+    rng = np.random.default_rng(21)
+    m, n = 6, 5
+    na = m if side == "L" else n
+    a, b = _cx(rng, (na + 1, na)), _cx(rng, (m + 2, n))
+    c = _cx(rng, (m + 1, n))
+    c0 = c.copy(order="F")
+    al, be = 0.5 - 0.25j, 1.5 + 0.5j
+    oracle.symm(side, uplo, m, n, al, a, na + 1, b, m + 2, be, c, m + 1, herm=herm)
+    T = np.triu(a[:na, :na]) if uplo == "U" else np.tril(a[:na, :na])
+    strict = T - np.diag(np.diag(T))
+    S = T + (strict.conj().T if herm else strict.T)
+    if herm:
+        np.fill_diagonal(S, np.diag(S).real)
+    B = b[:m, :n]
+    ref = al * (S @ B if side == "L" else B @ S) + be * c0[:m, :n]
+    np.testing.assert_allclose(c[:m, :n], ref, rtol=1e-12, atol=1e-12)
+    assert np.array_equal(c[m:, :], c0[m:, :])
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+def test_complex_trmm(oracle, side, uplo, trans, diag):
+    rng = np.random.default_rng(22)
+    m, n = 6, 4
+    na = m if side == "L" else n
+    a, b = _cx(rng, (na + 1, na)), _cx(rng, (m + 1, n))
+    b0 = b.copy(order="F")
+    al = 0.75 + 0.5j
+    oracle.trmm(side, uplo, trans, diag, m, n, al, a, na + 1, b, m + 1)
+    T = np.triu(a[:na, :na]) if uplo == "U" else np.tril(a[:na, :na])
+    if diag == "U":
+        np.fill_diagonal(T, 1.0)
+    X = b0[:m, :n]
+    ref = al * (_op(T, trans) @ X if side == "L" else X @ _op(T, trans))
+    np.testing.assert_allclose(b[:m, :n], ref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+def test_complex_herk(oracle, uplo, trans):
+    """zherk: op(A) op(A)^H on the triangle, diagonal imaginary part zeroed (op = T gives
+    A^T conj(A))."""
+    rng = np.random.default_rng(23)
+    n, k = 6, 7
+    rows, cols = (n, k) if trans == "N" else (k, n)
+    a, c = _cx(rng, (rows + 1, cols)), _cx(rng, (n + 2, n))
+    c0 = c.copy(order="F")
+    oracle.herk(uplo, trans, n, k, 1.25, a, rows + 1, 0.5, c, n + 2)
+    opA = _op(a[:rows, :cols], trans)
+    full = 1.25 * opA @ opA.conj().T + 0.5 * c0[:n, :n]
+    np.fill_diagonal(full, np.diag(full).real)
+    mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    np.testing.assert_allclose(c[:n, :n][mask], full[mask], rtol=1e-12, atol=1e-12)
+    assert np.array_equal(c[:n, :n][~mask], c0[:n, :n][~mask])
+
+
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+@pytest.mark.parametrize("herm", [False, True])
+def test_complex_syr2k_her2k(oracle, uplo, trans, herm):
+    rng = np.random.default_rng(24)
+    n, k = 5, 6
+    rows, cols = (n, k) if trans == "N" else (k, n)
+    a, b, c = _cx(rng, (rows, cols)), _cx(rng, (rows, cols)), _cx(rng, (n + 1, n))
+    c0 = c.copy(order="F")
+    al = 0.5 + 0.75j
+    be = 0.25 if herm else 0.25 - 0.5j
+    oracle.syr2k(uplo, trans, n, k, al, a, rows, b, rows, be, c, n + 1, herm=herm)
+    oa, ob = _op(a, trans), _op(b, trans)
+    if herm:
+        full = al * oa @ ob.conj().T + np.conj(al) * ob @ oa.conj().T + be * c0[:n, :n]
+        np.fill_diagonal(full, np.diag(full).real)
+    else:
+        full = al * (oa @ ob.T + ob @ oa.T) + be * c0[:n, :n]
+    mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    np.testing.assert_allclose(c[:n, :n][mask], full[mask], rtol=1e-12, atol=1e-12)
+    assert np.array_equal(c[:n, :n][~mask], c0[:n, :n][~mask])

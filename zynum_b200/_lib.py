@@ -91,8 +91,32 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_zsyrk_device", "zynum_blas_gpu_csyrk_device"):
         getattr(L, name).argtypes = [ch, ch, i, i, P, P, i, P, P, i, P]
         getattr(L, name).restype = i
-    for name in ("dsymm_", "ssymm_"):
+    for name in ("dsymm_", "ssymm_", "zsymm_", "csymm_", "zhemm_", "chemm_"):
         getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("ztrmm_", "ctrmm_"):
+        getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("zsyr2k_", "csyr2k_", "zher2k_", "cher2k_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("zherk_", "cherk_"):
+        getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, P, I32P]
+        getattr(L, name).restype = None
+    for name in ("cblas_zsymm", "cblas_csymm", "cblas_zhemm", "cblas_chemm"):
+        getattr(L, name).argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i]
+        getattr(L, name).restype = None
+    for name in ("cblas_ztrmm", "cblas_ctrmm"):
+        getattr(L, name).argtypes = [i, i, i, i, i, i, i, P, P, i, P, i]
+        getattr(L, name).restype = None
+    for name in ("cblas_zsyr2k", "cblas_csyr2k"):
+        getattr(L, name).argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i]
+        getattr(L, name).restype = None
+    L.cblas_zher2k.argtypes = [i, i, i, i, i, P, P, i, P, i, d, P, i]
+    L.cblas_cher2k.argtypes = [i, i, i, i, i, P, P, i, P, i, f, P, i]
+    L.cblas_zherk.argtypes = [i, i, i, i, i, d, P, i, d, P, i]
+    L.cblas_cherk.argtypes = [i, i, i, i, i, f, P, i, f, P, i]
+    for name in ("cblas_zher2k", "cblas_cher2k", "cblas_zherk", "cblas_cherk"):
         getattr(L, name).restype = None
     for name in ("dtrmm_", "strmm_"):
         getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]

@@ -134,33 +134,72 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     return c
 
 
-def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
-    """Fortran dsymm_ / ssymm_ on host arrays (dtype from c; in-place on c)."""
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """Fortran ?symm_ on host arrays (d / s / z / c from c's dtype; in-place on c); with herm
+    (complex only) zhemm_ / chemm_."""
     L = load()
-    fn, dt = (L.dsymm_, np.float64) if c.dtype == np.float64 else (L.ssymm_, np.float32)
-    al, be = np.array([alpha], dt), np.array([beta], dt)
+    if np.iscomplexobj(c):
+        z = c.dtype == np.complex128
+        fn = (L.zhemm_ if z else L.chemm_) if herm else (L.zsymm_ if z else L.csymm_)
+        al, be = np.array([alpha], c.dtype), np.array([beta], c.dtype)
+    else:
+        fn, dt = (L.dsymm_, np.float64) if c.dtype == np.float64 else (L.ssymm_, np.float32)
+        al, be = np.array([alpha], dt), np.array([beta], dt)
     fn(_ch(side), _ch(uplo), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb), be.ctypes.data,
        _ptr(c), _i(ldc))
     return c
 
 
+def hemm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran zhemm_ / chemm_ on host arrays (dtype from c; in-place on c)."""
+    return symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, herm=True)
+
+
 def trmm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
-    """Fortran dtrmm_ / strmm_ on host arrays (dtype from b; in-place on b)."""
+    """Fortran ?trmm_ on host arrays (d / s / z / c from b's dtype; in-place on b)."""
     L = load()
-    fn, dt = (L.dtrmm_, np.float64) if b.dtype == np.float64 else (L.strmm_, np.float32)
-    al = np.array([alpha], dt)
+    if np.iscomplexobj(b):
+        fn = L.ztrmm_ if b.dtype == np.complex128 else L.ctrmm_
+        al = np.array([alpha], b.dtype)
+    else:
+        fn, dt = (L.dtrmm_, np.float64) if b.dtype == np.float64 else (L.strmm_, np.float32)
+        al = np.array([alpha], dt)
     fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), _i(m), _i(n), al.ctypes.data, _ptr(a), _i(lda), _ptr(b),
        _i(ldb))
     return b
 
 
-def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
-    """Fortran dsyr2k_ / ssyr2k_ on host arrays (dtype from c; in-place on c's triangle)."""
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """Fortran ?syr2k_ on host arrays (d / s / z / c from c's dtype; in-place on c's triangle);
+    with herm (complex only) zher2k_ / cher2k_, beta real."""
     L = load()
-    fn, dt = (L.dsyr2k_, np.float64) if c.dtype == np.float64 else (L.ssyr2k_, np.float32)
-    al, be = np.array([alpha], dt), np.array([beta], dt)
+    if np.iscomplexobj(c):
+        z = c.dtype == np.complex128
+        al = np.array([alpha], c.dtype)
+        if herm:
+            fn, be = (L.zher2k_ if z else L.cher2k_), np.array([float(np.real(beta))], np.float64 if z else np.float32)
+        else:
+            fn, be = (L.zsyr2k_ if z else L.csyr2k_), np.array([beta], c.dtype)
+    else:
+        fn, dt = (L.dsyr2k_, np.float64) if c.dtype == np.float64 else (L.ssyr2k_, np.float32)
+        al, be = np.array([alpha], dt), np.array([beta], dt)
     fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb), be.ctypes.data,
        _ptr(c), _i(ldc))
+    return c
+
+
+def her2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Fortran zher2k_ / cher2k_ on host arrays (beta real; in-place on c's triangle)."""
+    return syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, herm=True)
+
+
+def herk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """Fortran zherk_ / cherk_ on host arrays (alpha, beta real; in-place on c's triangle)."""
+    L = load()
+    z = c.dtype == np.complex128
+    fn, rt = (L.zherk_, np.float64) if z else (L.cherk_, np.float32)
+    al, be = np.array([float(alpha)], rt), np.array([float(beta)], rt)
+    fn(_ch(uplo), _ch(trans), _i(n), _i(k), al.ctypes.data, _ptr(a), _i(lda), be.ctypes.data, _ptr(c), _i(ldc))
     return c
 
 
@@ -290,6 +329,48 @@ def cblas_trsm_c(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
     al = np.array([alpha], b.dtype)
     fn(layout, side, uplo, transa, diag, m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb)
     return b
+
+
+def cblas_symm_c(layout, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """cblas_zsymm / cblas_csymm, or cblas_zhemm / cblas_chemm with herm (dtype from c)."""
+    L = load()
+    z = c.dtype == np.complex128
+    fn = (L.cblas_zhemm if z else L.cblas_chemm) if herm else (L.cblas_zsymm if z else L.cblas_csymm)
+    al, be = np.array([alpha], c.dtype), np.array([beta], c.dtype)
+    fn(layout, side, uplo, m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data, _ptr(c), ldc)
+    return c
+
+
+def cblas_trmm_c(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """cblas_ztrmm / cblas_ctrmm (dtype from b)."""
+    L = load()
+    fn = L.cblas_ztrmm if b.dtype == np.complex128 else L.cblas_ctrmm
+    al = np.array([alpha], b.dtype)
+    fn(layout, side, uplo, transa, diag, m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb)
+    return b
+
+
+def cblas_syr2k_c(layout, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, herm=False):
+    """cblas_zsyr2k / cblas_csyr2k, or cblas_zher2k / cblas_cher2k (beta real) with herm."""
+    L = load()
+    z = c.dtype == np.complex128
+    al = np.array([alpha], c.dtype)
+    if herm:
+        fn = L.cblas_zher2k if z else L.cblas_cher2k
+        fn(layout, uplo, trans, n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, float(np.real(beta)), _ptr(c), ldc)
+    else:
+        fn = L.cblas_zsyr2k if z else L.cblas_csyr2k
+        be = np.array([beta], c.dtype)
+        fn(layout, uplo, trans, n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data, _ptr(c), ldc)
+    return c
+
+
+def cblas_herk(layout, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """cblas_zherk / cblas_cherk (alpha, beta real)."""
+    L = load()
+    fn = L.cblas_zherk if c.dtype == np.complex128 else L.cblas_cherk
+    fn(layout, uplo, trans, n, k, float(alpha), _ptr(a), lda, float(beta), _ptr(c), ldc)
+    return c
 
 
 def symm_device(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):

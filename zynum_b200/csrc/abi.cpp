@@ -704,6 +704,78 @@ cudaError_t run_syrk_c(char uplo, char trans, int n, int k, cnum<R> alpha, const
     return triangle_update<cnum<R>>(uplo, false, n, alpha, W, n, beta, c, ldc, st, trans == 'C');
 }
 
+// Complex TRMM (ztrmm_ / ctrmm_): dense diagonal blocks + complex GEMM couplings.
+template <typename R, typename Scratch>
+cudaError_t run_trmm(const TrsmArgs<cnum<R>>& t, cudaStream_t st, Scratch scratch) {
+    if (t.m <= 0 || t.n <= 0) return cudaSuccess;
+    const size_t planes = trmm_plane_bytes<cnum<R>>(t.side, t.m, t.n);
+    const int na = (t.side == 'L') ? t.m : t.n;
+    const size_t real = complex_scratch_bound<R>(t.m, t.n, na);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return trmm<cnum<R>>(t, ws, gemm_fn_c<R>(st, &fs), st);
+}
+
+// Complex SYMM / HEMM (zsymm_ / zhemm_, symmetric.zig:107 with herm): the
+// stored triangle mirrored (conjugated for HEMM) into scratch, one complex GEMM.
+template <typename R, typename Scratch>
+cudaError_t run_symm(char side, char uplo, int m, int n, cnum<R> alpha, const cnum<R>* a, long lda, const cnum<R>* b,
+                     long ldb, cnum<R> beta, cnum<R>* c, long ldc, cudaStream_t st, Scratch scratch, bool herm) {
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    if (alpha == cnum<R>(0)) {
+        const R be[2] = {beta.re, beta.im};
+        return scale_complex(m, n, be, reinterpret_cast<R*>(c), ldc, st);
+    }
+    const size_t planes = symm_plane_bytes<cnum<R>>(side, m, n);
+    const int na = (side == 'L') ? m : n;
+    const size_t real = complex_scratch_bound<R>(m, n, na);
+    void* ws = nullptr;
+    cudaError_t e = scratch(planes + real, st, &ws);
+    if (e != cudaSuccess) return e;
+    FixedScratch fs{static_cast<char*>(ws) + planes, real};
+    return symm<cnum<R>>(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, ws, gemm_fn_c<R>(st, &fs), st, herm);
+}
+
+// Complex rank-k / rank-2k updates through one complex GEMM W into scratch and a
+// triangle update (symmetric.zig:180-199 / :301-329):
+//   SYR2K (herm false, two): W = op(A) op(B)^T, C := alpha (W + W^T) + beta C;
+//   HER2K (herm, two):       W = op(A) op(B)^H, C := alpha W + conj(alpha) W^H + beta C;
+//   HERK (herm, b == a, not two): W = op(A) op(A)^H, C := alpha W + beta C (alpha, beta real).
+// op = C on a symmetric update conjugates W; op = T on a Hermitian one takes the
+// conjugate of op = C's W.
+template <typename R, typename Scratch>
+cudaError_t run_rank2k_c(char uplo, char trans, bool herm, bool two, int n, int k, cnum<R> alpha, const cnum<R>* a,
+                         long lda, const cnum<R>* b, long ldb, cnum<R> beta, cnum<R>* c, long ldc, cudaStream_t st,
+                         Scratch scratch) {
+    if (n <= 0) return cudaSuccess;
+    if (k == 0 || alpha == cnum<R>(0)) {
+        if (!herm) return syrk_scale_only<cnum<R>>(n, uplo, beta, c, ldc, st);
+        // Hermitian: beta C with the diagonal made real (alpha = 0 reads no W)
+        return triangle_update_h<cnum<R>>(uplo, false, true, n, cnum<R>(0), cnum<R>(0), c, ldc, beta, c, ldc, st,
+                                          false);
+    }
+    const size_t wbytes = ((size_t)n * n * sizeof(cnum<R>) + 1023) & ~size_t(1023);
+    const size_t cb = complex_scratch_bound<R>(n, n, k);
+    void* ws = nullptr;
+    cudaError_t e = scratch(wbytes + cb, st, &ws);
+    if (e != cudaSuccess) return e;
+    cnum<R>* W = static_cast<cnum<R>*>(ws);
+    char t1, t2;
+    bool conj_w;
+    if (!herm) {
+        t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N', conj_w = trans == 'C';
+    } else {
+        t1 = trans == 'N' ? 'N' : 'C', t2 = trans == 'N' ? 'C' : 'N', conj_w = trans == 'T';
+    }
+    ComplexArgs<R> cg{t1, t2, n, n, k, {R(1), R(0)}, reinterpret_cast<const R*>(a), lda, reinterpret_cast<const R*>(b),
+                      ldb, {R(0), R(0)}, reinterpret_cast<R*>(W), n};
+    if ((e = run_complex(cg, st, FixedScratch{static_cast<char*>(ws) + wbytes, cb})) != cudaSuccess) return e;
+    const cnum<R> alpha2 = herm ? cnum<R>(alpha.re, -alpha.im) : alpha;
+    return triangle_update_h<cnum<R>>(uplo, two, herm, n, alpha, alpha2, W, n, beta, c, ldc, st, conj_w);
+}
+
 template <typename T>
 void host_trsm(const char* routine, char side, char uplo, char trans, char diag, int m, int n, T alpha, const T* a,
                int lda, T* b, int ldb, bool multiply = false) {
@@ -732,10 +804,7 @@ void host_trsm(const char* routine, char side, char uplo, char trans, char diag,
         e = cudaMemcpy2DAsync(db, (size_t)m * es, b, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         const TrsmArgs<T> t{side, uplo, trans, diag, m, n, alpha, da, na, db, m};
-        if constexpr (is_cnum<T>::value)
-            e = run_trsm(t, st, HostScratch{&cx});
-        else
-            e = multiply ? run_trmm(t, st, HostScratch{&cx}) : run_trsm(t, st, HostScratch{&cx});
+        e = multiply ? run_trmm(t, st, HostScratch{&cx}) : run_trsm(t, st, HostScratch{&cx});
     }
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
@@ -799,7 +868,7 @@ void host_syrk(const char* routine, char uplo, char trans, int n, int k, T alpha
 // SYMM on host arrays: A's na x na window, B and C staged; only C's m x n window comes back.
 template <typename T>
 void host_symm(const char* routine, char side, char uplo, int m, int n, T alpha, const T* a, int lda, const T* b,
-               int ldb, T beta, T* c, int ldc) {
+               int ldb, T beta, T* c, int ldc, bool herm = false) {
     if (m <= 0 || n <= 0) return;
     Context& cx = context();
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
@@ -832,7 +901,12 @@ void host_symm(const char* routine, char side, char uplo, int m, int n, T alpha,
     }
     if (e == cudaSuccess && beta != T(0))
         e = cudaMemcpy2DAsync(dc, (size_t)m * es, c, (size_t)ldc * es, (size_t)m * es, n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = run_symm<T>(side, uplo, m, n, alpha, da, na, db, m, beta, dc, m, st, HostScratch{&cx});
+    if (e == cudaSuccess) {
+        if constexpr (is_cnum<T>::value)
+            e = run_symm(side, uplo, m, n, alpha, da, na, db, m, beta, dc, m, st, HostScratch{&cx}, herm);
+        else
+            e = run_symm<T>(side, uplo, m, n, alpha, da, na, db, m, beta, dc, m, st, HostScratch{&cx});
+    }
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
         cuda_status(e, "GPU execution");
@@ -850,7 +924,7 @@ void host_symm(const char* routine, char side, char uplo, int m, int n, T alpha,
 // SYR2K on host arrays: C is staged whole so the other triangle comes back bit-identical.
 template <typename T>
 void host_syr2k(const char* routine, char uplo, char trans, int n, int k, T alpha, const T* a, int lda, const T* b,
-                int ldb, T beta, T* c, int ldc) {
+                int ldb, T beta, T* c, int ldc, bool herm = false) {
     if (n <= 0) return;
     Context& cx = context();
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
@@ -883,8 +957,12 @@ void host_syr2k(const char* routine, char uplo, char trans, int n, int k, T alph
     }
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(dc, (size_t)n * es, c, (size_t)ldc * es, (size_t)n * es, n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-        e = run_syr2k<T>(uplo, trans, n, k, alpha, da, ra, db, ra, beta, dc, n, st, HostScratch{&cx});
+    if (e == cudaSuccess) {
+        if constexpr (is_cnum<T>::value)
+            e = run_rank2k_c(uplo, trans, herm, true, n, k, alpha, da, ra, db, ra, beta, dc, n, st, HostScratch{&cx});
+        else
+            e = run_syr2k<T>(uplo, trans, n, k, alpha, da, ra, db, ra, beta, dc, n, st, HostScratch{&cx});
+    }
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
         cuda_status(e, "GPU execution");
@@ -902,7 +980,7 @@ void host_syr2k(const char* routine, char uplo, char trans, int n, int k, T alph
 // Complex SYRK on host arrays: C staged whole so the other triangle comes back bit-identical.
 template <typename R>
 void host_syrk_c(const char* routine, char uplo, char trans, int n, int k, cnum<R> alpha, const cnum<R>* a, int lda,
-                 cnum<R> beta, cnum<R>* c, int ldc) {
+                 cnum<R> beta, cnum<R>* c, int ldc, bool herm = false) {
     if (n <= 0) return;
     Context& cx = context();
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
@@ -929,7 +1007,10 @@ void host_syrk_c(const char* routine, char uplo, char trans, int n, int k, cnum<
                               st);
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(dc, (size_t)n * es, c, (size_t)ldc * es, (size_t)n * es, n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = run_syrk_c<R>(uplo, trans, n, k, alpha, da, ra, beta, dc, n, st, HostScratch{&cx});
+    if (e == cudaSuccess)
+        e = herm ? run_rank2k_c<R>(uplo, trans, true, false, n, k, alpha, da, ra, da, ra, beta, dc, n, st,
+                                   HostScratch{&cx})
+                 : run_syrk_c<R>(uplo, trans, n, k, alpha, da, ra, beta, dc, n, st, HostScratch{&cx});
     if (e == cudaSuccess) e = cx.sync(st);
     if (e != cudaSuccess) {
         cuda_status(e, "GPU execution");
@@ -980,11 +1061,7 @@ int device_trsm(const char* what, char side, char uplo, char transa, char diag, 
     if (e != cudaSuccess) return cuda_status(e, "initialisation");
     const TrsmArgs<T> t{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb};
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if constexpr (is_cnum<T>::value)
-        return cuda_status(run_trsm(t, st, StreamScratch{&cx}), what);
-    else
-        return cuda_status(multiply ? run_trmm(t, st, StreamScratch{&cx}) : run_trsm(t, st, StreamScratch{&cx}),
-                           what);
+    return cuda_status(multiply ? run_trmm(t, st, StreamScratch{&cx}) : run_trsm(t, st, StreamScratch{&cx}), what);
 }
 
 template <typename T>
@@ -1382,6 +1459,154 @@ int zynum_blas_gpu_csyrk_device(char uplo, char trans, int n, int k, const float
                                 const float* beta, float* c, int ldc, void* stream) {
     return device_syrk_c<float>("csyrk_device", uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream);
 }
+
+// fortran.zig:785-799 csymm_ / zsymm_ / chemm_ / zhemm_, :860-867 ctrmm_ / ztrmm_,
+// :835-849 csyr2k_ / zsyr2k_ / cher2k_ / zher2k_ (beta real), :818-825 cherk_ / zherk_ (alpha, beta real)
+#define ZB_SYMM_C(NAME, R, RNAME, HERM)                                                                          \
+    void NAME(const char* side, const char* uplo, const zynum_blas_int* m, const zynum_blas_int* n,             \
+              const void* alpha, const void* a, const zynum_blas_int* lda, const void* b,                       \
+              const zynum_blas_int* ldb, const void* beta, void* c, const zynum_blas_int* ldc) {                \
+        const char sd = up(side), ul = up(uplo);                                                                 \
+        int info = symm_error(sd, ul, *m, *n, *lda, *ldb, *ldc);                                                 \
+        if (info) {                                                                                              \
+            report_xerbla(RNAME, info);                                                                          \
+            return;                                                                                              \
+        }                                                                                                        \
+        const R* al = static_cast<const R*>(alpha);                                                              \
+        const R* be = static_cast<const R*>(beta);                                                               \
+        host_symm<cnum<R>>(RNAME, sd, ul, *m, *n, cnum<R>(al[0], al[1]), static_cast<const cnum<R>*>(a), *lda,  \
+                           static_cast<const cnum<R>*>(b), *ldb, cnum<R>(be[0], be[1]), static_cast<cnum<R>*>(c), \
+                           *ldc, HERM);                                                                          \
+    }
+ZB_SYMM_C(zsymm_, double, "ZSYMM ", false)
+ZB_SYMM_C(csymm_, float, "CSYMM ", false)
+ZB_SYMM_C(zhemm_, double, "ZHEMM ", true)
+ZB_SYMM_C(chemm_, float, "CHEMM ", true)
+#undef ZB_SYMM_C
+
+#define ZB_TRMM_C(NAME, R, RNAME)                                                                                  \
+    void NAME(const char* side, const char* uplo, const char* transa, const char* diag, const zynum_blas_int* m,  \
+              const zynum_blas_int* n, const void* alpha, const void* a, const zynum_blas_int* lda, void* b,      \
+              const zynum_blas_int* ldb) {                                                                        \
+        const char sd = up(side), ul = up(uplo), tr = up(transa), dg = up(diag);                                   \
+        int info = trsm_error(sd, ul, tr, dg, *m, *n, *lda, *ldb);                                                 \
+        if (info) {                                                                                                \
+            report_xerbla(RNAME, info);                                                                            \
+            return;                                                                                                \
+        }                                                                                                          \
+        const R* al = static_cast<const R*>(alpha);                                                                \
+        host_trsm<cnum<R>>(RNAME, sd, ul, tr, dg, *m, *n, cnum<R>(al[0], al[1]), static_cast<const cnum<R>*>(a),  \
+                           *lda, static_cast<cnum<R>*>(b), *ldb, true);                                            \
+    }
+ZB_TRMM_C(ztrmm_, double, "ZTRMM ")
+ZB_TRMM_C(ctrmm_, float, "CTRMM ")
+#undef ZB_TRMM_C
+
+// BETA_T: const void* (symmetric, complex beta) or const R* (Hermitian, real beta)
+#define ZB_SYR2K_C(NAME, R, RNAME, HERM, BETA_T, BETA_EXPR)                                                      \
+    void NAME(const char* uplo, const char* trans, const zynum_blas_int* n, const zynum_blas_int* k,            \
+              const void* alpha, const void* a, const zynum_blas_int* lda, const void* b,                       \
+              const zynum_blas_int* ldb, BETA_T beta, void* c, const zynum_blas_int* ldc) {                     \
+        const char ul = up(uplo), tr = up(trans);                                                                \
+        int info = syr2k_error(ul, tr, *n, *k, *lda, *ldb, *ldc);                                                \
+        if (info) {                                                                                              \
+            report_xerbla(RNAME, info);                                                                          \
+            return;                                                                                              \
+        }                                                                                                        \
+        const R* al = static_cast<const R*>(alpha);                                                              \
+        host_syr2k<cnum<R>>(RNAME, ul, tr, *n, *k, cnum<R>(al[0], al[1]), static_cast<const cnum<R>*>(a), *lda, \
+                            static_cast<const cnum<R>*>(b), *ldb, BETA_EXPR, static_cast<cnum<R>*>(c), *ldc,     \
+                            HERM);                                                                               \
+    }
+ZB_SYR2K_C(zsyr2k_, double, "ZSYR2K", false, const void*,
+           cnum<double>(static_cast<const double*>(beta)[0], static_cast<const double*>(beta)[1]))
+ZB_SYR2K_C(csyr2k_, float, "CSYR2K", false, const void*,
+           cnum<float>(static_cast<const float*>(beta)[0], static_cast<const float*>(beta)[1]))
+ZB_SYR2K_C(zher2k_, double, "ZHER2K", true, const double*, cnum<double>(*beta))
+ZB_SYR2K_C(cher2k_, float, "CHER2K", true, const float*, cnum<float>(*beta))
+#undef ZB_SYR2K_C
+
+#define ZB_HERK(NAME, R, RNAME)                                                                                    \
+    void NAME(const char* uplo, const char* trans, const zynum_blas_int* n, const zynum_blas_int* k, const R* alpha, \
+              const void* a, const zynum_blas_int* lda, const R* beta, void* c, const zynum_blas_int* ldc) {       \
+        const char ul = up(uplo), tr = up(trans);                                                                   \
+        int info = syrk_error(ul, tr, *n, *k, *lda, *ldc);                                                          \
+        if (info) {                                                                                                 \
+            report_xerbla(RNAME, info);                                                                             \
+            return;                                                                                                 \
+        }                                                                                                           \
+        host_syrk_c<R>(RNAME, ul, tr, *n, *k, cnum<R>(*alpha), static_cast<const cnum<R>*>(a), *lda,               \
+                       cnum<R>(*beta), static_cast<cnum<R>*>(c), *ldc, true);                                       \
+    }
+ZB_HERK(zherk_, double, "ZHERK ")
+ZB_HERK(cherk_, float, "CHERK ")
+#undef ZB_HERK
+
+// cblas.zig:1491-1537 cblas_[cz]symm / cblas_[cz]hemm, :1703-1728 cblas_[cz]trmm,
+// :1629-1676 cblas_[cz]syr2k / cblas_[cz]her2k (beta real), :1583-1603 cblas_[cz]herk (alpha, beta real)
+#define ZB_CBLAS_SYMM_C(NAME, FNAME)                                                                              \
+    void NAME(int layout, int side, int uplo, int m, int n, const void* alpha, const void* a, int lda,            \
+              const void* b, int ldb, const void* beta, void* c, int ldc) {                                       \
+        if (!cblas_valid_layout(layout)) return;                                                                  \
+        const bool rm = layout == CblasRowMajor;                                                                  \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                         \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                         \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb, lc = ldc;                            \
+        FNAME(&ss, &uu, &mm, &nn, alpha, a, &la, b, &lb, beta, c, &lc);                                           \
+    }
+ZB_CBLAS_SYMM_C(cblas_zsymm, zsymm_)
+ZB_CBLAS_SYMM_C(cblas_csymm, csymm_)
+ZB_CBLAS_SYMM_C(cblas_zhemm, zhemm_)
+ZB_CBLAS_SYMM_C(cblas_chemm, chemm_)
+#undef ZB_CBLAS_SYMM_C
+
+#define ZB_CBLAS_TRMM_C(NAME, FNAME)                                                                                \
+    void NAME(int layout, int side, int uplo, int transa, int diag, int m, int n, const void* alpha, const void* a, \
+              int lda, void* b, int ldb) {                                                                          \
+        if (!cblas_valid_layout(layout) || (side != CblasLeft && side != CblasRight) ||                             \
+            (uplo != CblasUpper && uplo != CblasLower) || !cblas_valid_trans(transa) ||                             \
+            (diag != CblasNonUnit && diag != CblasUnit))                                                            \
+            return;                                                                                                 \
+        const bool rm = layout == CblasRowMajor;                                                                    \
+        char ss = rm ? cblas_row_side_char(side) : cblas_side_char(side);                                           \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                           \
+        char tt = cblas_trans_char(transa), dd = cblas_diag_char(diag);                                             \
+        zynum_blas_int mm = rm ? n : m, nn = rm ? m : n, la = lda, lb = ldb;                                        \
+        FNAME(&ss, &uu, &tt, &dd, &mm, &nn, alpha, a, &la, b, &lb);                                                 \
+    }
+ZB_CBLAS_TRMM_C(cblas_ztrmm, ztrmm_)
+ZB_CBLAS_TRMM_C(cblas_ctrmm, ctrmm_)
+#undef ZB_CBLAS_TRMM_C
+
+#define ZB_CBLAS_SYR2K_C(NAME, FNAME, BETA_T, BETA_ARG)                                                            \
+    void NAME(int layout, int uplo, int trans, int n, int k, const void* alpha, const void* a, int lda,           \
+              const void* b, int ldb, BETA_T beta, void* c, int ldc) {                                            \
+        if (!cblas_valid_layout(layout)) return;                                                                  \
+        const bool rm = layout == CblasRowMajor;                                                                  \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                         \
+        char tt = rm ? cblas_row_trans_char(trans) : cblas_trans_char(trans);                                     \
+        zynum_blas_int nn = n, kk = k, la = lda, lb = ldb, lc = ldc;                                              \
+        FNAME(&uu, &tt, &nn, &kk, alpha, a, &la, b, &lb, BETA_ARG, c, &lc);                                       \
+    }
+ZB_CBLAS_SYR2K_C(cblas_zsyr2k, zsyr2k_, const void*, beta)
+ZB_CBLAS_SYR2K_C(cblas_csyr2k, csyr2k_, const void*, beta)
+ZB_CBLAS_SYR2K_C(cblas_zher2k, zher2k_, double, &beta)
+ZB_CBLAS_SYR2K_C(cblas_cher2k, cher2k_, float, &beta)
+#undef ZB_CBLAS_SYR2K_C
+
+#define ZB_CBLAS_HERK(NAME, FNAME, R)                                                                        \
+    void NAME(int layout, int uplo, int trans, int n, int k, R alpha, const void* a, int lda, R beta, void* c, \
+              int ldc) {                                                                                     \
+        if (!cblas_valid_layout(layout)) return;                                                             \
+        const bool rm = layout == CblasRowMajor;                                                             \
+        char uu = rm ? cblas_row_uplo_char(uplo) : cblas_uplo_char(uplo);                                    \
+        char tt = rm ? cblas_row_trans_char(trans) : cblas_trans_char(trans);                                \
+        zynum_blas_int nn = n, kk = k, la = lda, lc = ldc;                                                   \
+        FNAME(&uu, &tt, &nn, &kk, &alpha, a, &la, &beta, c, &lc);                                            \
+    }
+ZB_CBLAS_HERK(cblas_zherk, zherk_, double)
+ZB_CBLAS_HERK(cblas_cherk, cherk_, float)
+#undef ZB_CBLAS_HERK
 
 // fortran.zig:777-783 ?symm_, :852-858 ?trmm_, :827-833 ?syr2k_
 #define ZB_SYMM(NAME, T, RNAME)                                                                                   \

@@ -91,6 +91,14 @@ __host__ __device__ inline cnum<R> conj_if(cnum<R> v, bool c) {
     return c ? cnum<R>{v.re, -v.im} : v;
 }
 
+// a Hermitian matrix's diagonal: the real part only (when h, complex), v unchanged otherwise
+__host__ __device__ inline double herm_diag(double v, bool) { return v; }
+__host__ __device__ inline float herm_diag(float v, bool) { return v; }
+template <typename R>
+__host__ __device__ inline cnum<R> herm_diag(cnum<R> v, bool h) {
+    return h ? cnum<R>{v.re, R(0)} : v;
+}
+
 template <typename T>
 struct is_cnum {
     static constexpr bool value = false;

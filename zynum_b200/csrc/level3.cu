@@ -448,12 +448,14 @@ __global__ void symmetrize(int n, int from_upper, T* __restrict__ c, long ldc) {
     }
 }
 
-// Dense symmetric S (n x n, ld lds) from the uplo triangle of A.  A 32 x 32
-// output tile takes its stored elements straight from A and its mirrored
-// elements from a shared-memory transpose of the opposite tile, so global
-// reads and writes are all coalesced.  Block (32, 8).
+// Dense symmetric S (n x n, ld lds) from the uplo triangle of A; Hermitian
+// when herm (mirrored elements conjugated, diagonal real: symValue,
+// access.zig:31-42).  A 32 x 32 output tile takes its stored elements straight
+// from A and its mirrored elements from a shared-memory transpose of the
+// opposite tile, so global reads and writes are all coalesced.  Block (32, 8).
 template <typename T>
-__global__ void sym_expand(int n, int from_upper, const T* __restrict__ a, long lda, T* __restrict__ s, long lds) {
+__global__ void sym_expand(int n, int from_upper, int herm, const T* __restrict__ a, long lda, T* __restrict__ s,
+                           long lds) {
     __shared__ T t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -470,7 +472,8 @@ __global__ void sym_expand(int n, int from_upper, const T* __restrict__ a, long 
         const int i = r0 + tx, j = c0 + y;
         if (i >= n || j >= n) continue;
         const bool stored = from_upper ? i <= j : i >= j;
-        s[i + (long)j * lds] = stored ? a[i + (long)j * lda] : t[tx][y];
+        T v = stored ? a[i + (long)j * lda] : conj_if(t[tx][y], herm != 0);
+        s[i + (long)j * lds] = i == j ? herm_diag(v, herm != 0) : v;
     }
 }
 
@@ -492,13 +495,16 @@ __global__ void tri_dense_blocks(const T* __restrict__ a, long lda, char uplo, c
 
 constexpr int kTrmmNB = 256;
 
-// C := alpha (W + W^T) + beta C (two) or alpha W + beta C on the uplo triangle,
-// W n x n with ld ldw; beta == 0 writes without reading C.  32 x 32 tiles, W^T
-// through a shared-memory transpose; tiles outside the triangle return at once.
-// Block (32, 8).
+// C := alpha (W + W^T) + beta C (two) or alpha W + beta C on the uplo
+// triangle, W n x n with ld ldw, conj(W) in place of W when conj_w.  herm:
+// C := alpha W + alpha2 W^H + beta C (two, Hermitian rank 2k) and the diagonal
+// is made real.
+// beta == 0 writes without reading C; alpha == 0 reads no W.  32 x 32 tiles,
+// W^T through a shared-memory transpose; tiles outside the triangle return at
+// once.  Block (32, 8).
 template <typename T>
-__global__ void tri_update(int n, int upper, int two, int conj_w, T alpha, const T* __restrict__ w, long ldw, T beta,
-                           T* __restrict__ c, long ldc) {
+__global__ void tri_update(int n, int upper, int two, int conj_w, int herm, T alpha, T alpha2, const T* __restrict__ w,
+                           long ldw, T beta, T* __restrict__ c, long ldc) {
     __shared__ T t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     if (upper ? r0 > c0 + 31 : r0 + 31 < c0) return;  // the whole block: no element of the triangle
@@ -513,24 +519,40 @@ __global__ void tri_update(int n, int upper, int two, int conj_w, T alpha, const
     for (int y = ty; y < 32; y += 8) {
         const int i = r0 + tx, j = c0 + y;
         if (i >= n || j >= n || (upper ? i > j : i < j)) continue;
-        T v = conj_if(w[i + (long)j * ldw], conj_w != 0);
-        if (two) v = v + t[tx][y];
+        T out = T(0);
+        if (alpha != T(0)) {  // alpha = 0: W is not read (a scale-only call passes w = c)
+            const T v = conj_if(w[i + (long)j * ldw], conj_w != 0);
+            if (!two) {
+                out = alpha * v;
+            } else {
+                const T u = conj_if(t[tx][y], conj_w != 0);  // W(j, i)
+                // symmetric rank 2k: alpha (W + W^T); Hermitian: alpha W + alpha2 W^H
+                out = herm ? alpha * v + alpha2 * conj_if(u, true) : alpha * (v + u);
+            }
+        }
         T* cp = c + i + (long)j * ldc;
-        *cp = beta == T(0) ? alpha * v : fma(beta, *cp, alpha * v);
+        out = beta == T(0) ? out : fma(beta, *cp, out);
+        *cp = i == j ? herm_diag(out, herm != 0) : out;
     }
 }
 
 }  // namespace
 
 template <typename T>
-cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
-                            cudaStream_t st, bool conj_w) {
+cudaError_t triangle_update_h(char uplo, bool two, bool herm, int n, T alpha, T alpha2, const T* w, long ldw, T beta,
+                              T* c, long ldc, cudaStream_t st, bool conj_w) {
     if (n <= 0) return cudaSuccess;
     dim3 grid((n + 31) / 32, (n + 31) / 32);
-    tri_update<T><<<grid, dim3(32, 8), 0, st>>>(n, uplo == 'U' ? 1 : 0, two ? 1 : 0, conj_w ? 1 : 0, alpha, w, ldw,
-                                                beta, c, ldc);
+    tri_update<T><<<grid, dim3(32, 8), 0, st>>>(n, uplo == 'U' ? 1 : 0, two ? 1 : 0, conj_w ? 1 : 0, herm ? 1 : 0,
+                                                alpha, alpha2, w, ldw, beta, c, ldc);
     count_launch();
     return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
+                            cudaStream_t st, bool conj_w) {
+    return triangle_update_h<T>(uplo, two, false, n, alpha, alpha, w, ldw, beta, c, ldc, st, conj_w);
 }
 template cudaError_t triangle_update<double>(char, bool, int, double, const double*, long, double, double*, long,
                                              cudaStream_t, bool);
@@ -540,6 +562,12 @@ template cudaError_t triangle_update<cnum<double>>(char, bool, int, cnum<double>
                                                    cnum<double>, cnum<double>*, long, cudaStream_t, bool);
 template cudaError_t triangle_update<cnum<float>>(char, bool, int, cnum<float>, const cnum<float>*, long, cnum<float>,
                                                   cnum<float>*, long, cudaStream_t, bool);
+template cudaError_t triangle_update_h<cnum<double>>(char, bool, bool, int, cnum<double>, cnum<double>,
+                                                     const cnum<double>*, long, cnum<double>, cnum<double>*, long,
+                                                     cudaStream_t, bool);
+template cudaError_t triangle_update_h<cnum<float>>(char, bool, bool, int, cnum<float>, cnum<float>,
+                                                    const cnum<float>*, long, cnum<float>, cnum<float>*, long,
+                                                    cudaStream_t, bool);
 
 template <typename T>
 size_t symm_plane_bytes(char side, int m, int n) {
@@ -549,12 +577,12 @@ size_t symm_plane_bytes(char side, int m, int n) {
 
 template <typename T>
 cudaError_t symm(char side, char uplo, int m, int n, T alpha, const T* a, long lda, const T* b, long ldb, T beta,
-                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st) {
+                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st, bool herm) {
     if (m <= 0 || n <= 0) return cudaSuccess;
     const int na = (side == 'L') ? m : n;
     T* S = static_cast<T*>(planes);
     dim3 grid((na + 31) / 32, (na + 31) / 32);
-    sym_expand<T><<<grid, dim3(32, 8), 0, st>>>(na, uplo == 'U' ? 1 : 0, a, lda, S, na);
+    sym_expand<T><<<grid, dim3(32, 8), 0, st>>>(na, uplo == 'U' ? 1 : 0, herm ? 1 : 0, a, lda, S, na);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -599,7 +627,8 @@ cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
         if (e != cudaSuccess) return e;
     }
     const bool upper = op_is_upper(t.uplo, t.trans);
-    const char ta = (t.trans == 'N') ? 'N' : 'T';
+    // op = C keeps its conjugation in the couplings of a complex A
+    const char ta = (t.trans == 'N') ? 'N' : (is_cnum<T>::value ? t.trans : 'T');
     auto opa = [&](int r0, int c0) -> const T* {
         return (ta == 'N') ? t.a + r0 + (long)c0 * lda : t.a + c0 + (long)r0 * lda;
     };
@@ -811,12 +840,26 @@ template cudaError_t syrk_scale_only<float>(int, char, float, float*, long, cuda
 template size_t symm_plane_bytes<double>(char, int, int);
 template size_t symm_plane_bytes<float>(char, int, int);
 template cudaError_t symm<double>(char, char, int, int, double, const double*, long, const double*, long, double,
-                                  double*, long, void*, const GemmFn<double>&, cudaStream_t);
+                                  double*, long, void*, const GemmFn<double>&, cudaStream_t, bool);
 template cudaError_t symm<float>(char, char, int, int, float, const float*, long, const float*, long, float, float*,
-                                 long, void*, const GemmFn<float>&, cudaStream_t);
+                                 long, void*, const GemmFn<float>&, cudaStream_t, bool);
 template size_t trmm_plane_bytes<double>(char, int, int);
 template size_t trmm_plane_bytes<float>(char, int, int);
 template cudaError_t trmm<double>(const TrsmArgs<double>&, void*, const GemmFn<double>&, cudaStream_t);
 template cudaError_t trmm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t);
+template size_t symm_plane_bytes<cnum<double>>(char, int, int);
+template size_t symm_plane_bytes<cnum<float>>(char, int, int);
+template cudaError_t symm<cnum<double>>(char, char, int, int, cnum<double>, const cnum<double>*, long,
+                                        const cnum<double>*, long, cnum<double>, cnum<double>*, long, void*,
+                                        const GemmFn<cnum<double>>&, cudaStream_t, bool);
+template cudaError_t symm<cnum<float>>(char, char, int, int, cnum<float>, const cnum<float>*, long, const cnum<float>*,
+                                       long, cnum<float>, cnum<float>*, long, void*, const GemmFn<cnum<float>>&,
+                                       cudaStream_t, bool);
+template size_t trmm_plane_bytes<cnum<double>>(char, int, int);
+template size_t trmm_plane_bytes<cnum<float>>(char, int, int);
+template cudaError_t trmm<cnum<double>>(const TrsmArgs<cnum<double>>&, void*, const GemmFn<cnum<double>>&,
+                                        cudaStream_t);
+template cudaError_t trmm<cnum<float>>(const TrsmArgs<cnum<float>>&, void*, const GemmFn<cnum<float>>&,
+                                       cudaStream_t);
 
 }  // namespace zb

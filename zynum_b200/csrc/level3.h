@@ -39,10 +39,11 @@ template <typename T>
 size_t symm_plane_bytes(char side, int m, int n);
 
 // C := alpha A B + beta C (side L) or alpha B A + beta C (side R), A symmetric
-// with its uplo triangle stored; arguments validated, device pointers.
+// (Hermitian when herm: conjugate mirror, real diagonal) with its uplo triangle
+// stored; arguments validated, device pointers.
 template <typename T>
 cudaError_t symm(char side, char uplo, int m, int n, T alpha, const T* a, long lda, const T* b, long ldb, T beta,
-                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
+                 T* c, long ldc, void* planes, const GemmFn<T>& gemm, cudaStream_t st, bool herm = false);
 
 // Device scratch TRMM needs besides its GEMMs' scratch: dense diagonal blocks and a copy of B.
 template <typename T>
@@ -58,6 +59,13 @@ cudaError_t trmm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
 template <typename T>
 cudaError_t triangle_update(char uplo, bool two, int n, T alpha, const T* w, long ldw, T beta, T* c, long ldc,
                             cudaStream_t st, bool conj_w = false);
+
+// The general form: with herm, C := alpha W + alpha2 W^H + beta C (two, HER2K)
+// or alpha W + beta C (HERK) with the diagonal made real; without, as
+// triangle_update (alpha2 unused).  alpha == 0 reads no W.
+template <typename T>
+cudaError_t triangle_update_h(char uplo, bool two, bool herm, int n, T alpha, T alpha2, const T* w, long ldw, T beta,
+                              T* c, long ldc, cudaStream_t st, bool conj_w = false);
 
 // Copy the uplo triangle of the n x n matrix c onto the other triangle.
 template <typename T>
