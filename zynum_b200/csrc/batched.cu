@@ -25,7 +25,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBK = 16;
-constexpr int kStages = 2;  // two cp.async stages, two CTAs per SM (measured faster than 3 stages, one CTA)
+constexpr int kStages = 2;   // FP32: two cp.async stages, two CTAs per SM
+constexpr int kStagesD = 3;  // FP64: three stages of at most 30 KB, two CTAs per SM
 
 template <typename T>
 struct Prob {
@@ -36,9 +37,28 @@ struct Prob {
 };
 
 // ------------------------------------------------------------- loaders
+// smem[r][c] (pitch `pitch`) = base[(r0 + r) * ld + c0 + c], zero outside
+// r_lim x c_lim.  vec: 16-byte copies (base 16-byte aligned, ld and c0 a
+// multiple of 16 / sizeof(T), pitch likewise), a partial copy zero-filling the
+// ragged edge; otherwise one copy per element (any ld, any alignment).
 template <typename T, int ROWS, int COLS>
 ZB_DEVICE void load_tile(T* smem, int pitch, const T* __restrict__ base, long ld, int r0, int c0, int r_lim,
-                         int c_lim) {
+                         int c_lim, bool vec) {
+    constexpr int V = 16 / sizeof(T);
+    if (vec) {
+        constexpr int CPR = COLS / V, TOTAL = ROWS * CPR;
+#pragma unroll
+        for (int it = 0; it < (TOTAL + kThreads - 1) / kThreads; ++it) {
+            const int q = it * kThreads + threadIdx.x;
+            if (TOTAL % kThreads != 0 && q >= TOTAL) break;
+            const int r = q / CPR, c = (q % CPR) * V;
+            const int gr = r0 + r, gc = c0 + c;
+            const int valid = gr < r_lim ? max(0, min(V, c_lim - gc)) : 0;
+            const T* src = valid ? base + (long)gr * ld + gc : base;
+            cp_async_16(smem_u32(smem + r * pitch + c), src, valid * (int)sizeof(T));
+        }
+        return;
+    }
     constexpr int TOTAL = ROWS * COLS;
 #pragma unroll
     for (int it = 0; it < (TOTAL + kThreads - 1) / kThreads; ++it) {
@@ -55,20 +75,79 @@ ZB_DEVICE void load_tile(T* smem, int pitch, const T* __restrict__ base, long ld
     }
 }
 
+// 16-byte copies are possible for an operand whose base is 16-byte aligned and
+// whose leading dimension is a multiple of 16 bytes.
+template <typename T>
+ZB_DEVICE bool vec_ok(const T* base, int ld) {
+    return ((reinterpret_cast<uintptr_t>(base) & 15) == 0) && ((ld * (int)sizeof(T)) % 16 == 0);
+}
+
 // ------------------------------------------------------- FP64 DMMA tile
-// BM x BN tile, 8 warps as 2 x 4, warp tile (BM/2) x (BN/4).
-template <int BM, int BN, bool AK, bool BKF>
+// One kBK-deep slice of a warp's products on its first MIV x NIV fragments
+// (the others lie outside the problem).  The fragment counts are compile-time
+// so that skipped fragments issue nothing at all: a run-time test around a
+// DMMA becomes a predicated DMMA, which still occupies the pipe.
+template <int MI, int NI, int MIV, int NIV, int A_PITCH, int B_PITCH, bool AK, bool BKF>
+ZB_DEVICE void dmma_slice(double (&acc)[MI][NI][4], const double* as, const double* bs, int wm, int wn, int g,
+                          int t) {
+#pragma unroll
+    for (int ks = 0; ks < kBK; ks += 8) {
+        double af[MIV][4], bf[NIV][2];
+#pragma unroll
+        for (int i = 0; i < MIV; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int rr = wm + i * 16 + g + 8 * (v & 1), kk = ks + t + 4 * (v >> 1);
+                af[i][v] = AK ? as[rr * A_PITCH + kk] : as[kk * A_PITCH + rr];
+            }
+#pragma unroll
+        for (int j = 0; j < NIV; ++j)
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                const int cc = wn + j * 8 + g, kk = ks + t + 4 * v;
+                bf[j][v] = BKF ? bs[cc * B_PITCH + kk] : bs[kk * B_PITCH + cc];
+            }
+#pragma unroll
+        for (int i = 0; i < MIV; ++i)
+#pragma unroll
+            for (int j = 0; j < NIV; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+    }
+}
+
+// Variant V = MIV * (NI + 1) + NIV, chosen by a chain of warp-uniform branches.
+template <int MI, int NI, int V, int A_PITCH, int B_PITCH, bool AK, bool BKF>
+ZB_DEVICE void dmma_slice_var(int var, double (&acc)[MI][NI][4], const double* as, const double* bs, int wm, int wn,
+                              int g, int t) {
+    constexpr int MIV = V / (NI + 1), NIV = V % (NI + 1);
+    if (var == V) {
+        if constexpr (MIV > 0 && NIV > 0)
+            dmma_slice<MI, NI, MIV, NIV, A_PITCH, B_PITCH, AK, BKF>(acc, as, bs, wm, wn, g, t);
+        return;
+    }
+    if constexpr (V > 0) dmma_slice_var<MI, NI, V - 1, A_PITCH, B_PITCH, AK, BKF>(var, acc, as, bs, wm, wn, g, t);
+}
+
+
+// One BM x BN output tile: 8 warps as WARPS_M x (8 / WARPS_M), warp tile
+// WM x WN of 16 x 8 DMMA fragments, kStagesD cp.async stages of kBK-deep A and
+// B slices (16-byte copies where the operand allows them).
+template <int BM, int BN, int WARPS_M, bool AK, bool BKF>
 ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, double beta, double* smem) {
-    constexpr int WM = BM / 2, WN = BN / 4, MI = WM / 16, NI = WN / 8;
+    constexpr int WARPS_N = 8 / WARPS_M;
+    constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N, MI = WM / 16, NI = WN / 8;
     constexpr int A_ROWS = AK ? BM : kBK, A_COLS = AK ? kBK : BM, A_PITCH = A_COLS + 4;
     constexpr int B_ROWS = BKF ? BN : kBK, B_COLS = BKF ? kBK : BN, B_PITCH = B_COLS + 4;
     constexpr int A_STAGE = A_ROWS * A_PITCH, B_STAGE = B_ROWS * B_PITCH;
     double* As = smem;
-    double* Bs = smem + kStages * A_STAGE;
+    double* Bs = smem + kStagesD * A_STAGE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp / 4) * WM, wn = (warp % 4) * WN;
+    const int wm = (warp / WARPS_N) * WM, wn = (warp % WARPS_N) * WN;
     const int g = lane >> 2, t = lane & 3;
     const int KT = (alpha == 0.0) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
+    const bool va = vec_ok(p.a, p.lda), vb = vec_ok(p.b, p.ldb);
+    // fragments of this warp inside the problem: the first miv row and niv column fragments
+    const int miv = max(0, min(MI, (p.m - m0 - wm + 15) / 16)), niv = max(0, min(NI, (p.n - n0 - wn + 7) / 8));
+    const int var = miv * (NI + 1) + niv;
     double acc[MI][NI][4];
 #pragma unroll
     for (int i = 0; i < MI; ++i)
@@ -79,48 +158,30 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
     auto load_stage = [&](int stage, int kt) {
         const int k0 = kt * kBK;
         if (AK)
-            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, m0, k0, p.m, p.k);
+            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, m0, k0, p.m, p.k, va);
         else
-            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, k0, m0, p.k, p.m);
+            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, k0, m0, p.k, p.m, va);
         if (BKF)
-            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, n0, k0, p.n, p.k);
+            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, n0, k0, p.n, p.k, vb);
         else
-            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, k0, n0, p.k, p.n);
+            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, k0, n0, p.k, p.n, vb);
     };
 #pragma unroll
-    for (int s = 0; s < kStages - 1; ++s) {
+    for (int s = 0; s < kStagesD - 1; ++s) {
         if (s < KT) load_stage(s, s);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
-        cp_async_wait<kStages - 2>();
+        cp_async_wait<kStagesD - 2>();
         __syncthreads();
-        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
+        if (kt + kStagesD - 1 < KT) load_stage((kt + kStagesD - 1) % kStagesD, kt + kStagesD - 1);
         cp_async_commit();
-        const double* as = As + (kt % kStages) * A_STAGE;
-        const double* bs = Bs + (kt % kStages) * B_STAGE;
-#pragma unroll
-        for (int ks = 0; ks < kBK; ks += 8) {
-            double af[MI][4], bf[NI][2];
-#pragma unroll
-            for (int i = 0; i < MI; ++i)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const int rr = wm + i * 16 + g + 8 * (v & 1), kk = ks + t + 4 * (v >> 1);
-                    af[i][v] = AK ? as[rr * A_PITCH + kk] : as[kk * A_PITCH + rr];
-                }
-#pragma unroll
-            for (int j = 0; j < NI; ++j)
-#pragma unroll
-                for (int v = 0; v < 2; ++v) {
-                    const int cc = wn + j * 8 + g, kk = ks + t + 4 * v;
-                    bf[j][v] = BKF ? bs[cc * B_PITCH + kk] : bs[kk * B_PITCH + cc];
-                }
-#pragma unroll
-            for (int i = 0; i < MI; ++i)
-#pragma unroll
-                for (int j = 0; j < NI; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
-        }
+        const double* as = As + (kt % kStagesD) * A_STAGE;
+        const double* bs = Bs + (kt % kStagesD) * B_STAGE;
+        if (var == MI * (NI + 1) + NI)  // the whole warp tile inside the problem
+            dmma_slice<MI, NI, MI, NI, A_PITCH, B_PITCH, AK, BKF>(acc, as, bs, wm, wn, g, t);
+        else
+            dmma_slice_var<MI, NI, MI * (NI + 1) + NI - 1, A_PITCH, B_PITCH, AK, BKF>(var, acc, as, bs, wm, wn, g, t);
     }
     cp_async_wait<0>();
 #pragma unroll
@@ -138,7 +199,19 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
                     *cp = out;
                 }
             }
-    __syncthreads();  // shared memory is reused by the next work item
+    __syncthreads();  // shared memory is reused by the next tile
+}
+
+// A chunk of `count` consecutive output tiles t0 .. t0 + count - 1 of one
+// problem (tile t: rows (t % mt) BM.., columns (t / mt) BN.., mt = ceil(m / BM)):
+// the problem's sizes, pointers and leading dimensions are read once per chunk.
+// (Carrying the cp.async stream across the chunk's tile boundaries measured
+// slower than restarting it per tile.)
+template <int BM, int BN, int WARPS_M, bool AK, bool BKF>
+ZB_DEVICE void dgemm_chunk(const Prob<double>& p, int t0, int count, double alpha, double beta, double* smem) {
+    const int mt = (p.m + BM - 1) / BM;
+    for (int tile = t0; tile < t0 + count; ++tile)
+        dgemm_tile<BM, BN, WARPS_M, AK, BKF>(p, (tile % mt) * BM, (tile / mt) * BN, alpha, beta, smem);
 }
 
 // ------------------------------------------------------- FP32 FFMA tile
@@ -234,12 +307,13 @@ dgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* 
         const int q = it.prob;
         if (q < 0) continue;  // padding item of the per-CTA schedule
         Prob<double> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
+        // tile edges: batched_tile_m / batched_tile_n (FP64)
         if (it.cfg == TILE_CFG_128)
-            dgemm_tile<128, 128, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+            dgemm_chunk<128, 64, 4, AK, BKF>(p, it.t0, it.count, alpha, beta, sm_d);
         else if (it.cfg == TILE_CFG_64)
-            dgemm_tile<64, 64, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+            dgemm_chunk<64, 64, 2, AK, BKF>(p, it.t0, it.count, alpha, beta, sm_d);
         else
-            dgemm_tile<32, 32, AK, BKF>(p, it.m0, it.n0, alpha, beta, sm_d);
+            dgemm_chunk<32, 32, 2, AK, BKF>(p, it.t0, it.count, alpha, beta, sm_d);
     }
 }
 
@@ -255,19 +329,25 @@ sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* 
         const int q = it.prob;
         if (q < 0) continue;  // padding item of the per-CTA schedule
         Prob<float> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
-        if (it.cfg == TILE_CFG_128)
-            sgemm_tile<128, 128, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
-        else if (it.cfg == TILE_CFG_64)
-            sgemm_tile<64, 64, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
-        else
-            sgemm_tile<32, 32, AM, BMF>(p, it.m0, it.n0, alpha, beta, sm_f);
+        const int e = it.cfg == TILE_CFG_128 ? 128 : (it.cfg == TILE_CFG_64 ? 64 : 32);
+        const int mt = (p.m + e - 1) / e;
+        for (int tile = it.t0; tile < it.t0 + it.count; ++tile) {
+            const int m0 = (tile % mt) * e, n0 = (tile / mt) * e;
+            if (it.cfg == TILE_CFG_128)
+                sgemm_tile<128, 128, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+            else if (it.cfg == TILE_CFG_64)
+                sgemm_tile<64, 64, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+            else
+                sgemm_tile<32, 32, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+        }
     }
 }
 
 size_t dsmem_bytes() {
-    // largest config (128 x 128), worst orientation
-    const size_t a = (size_t)128 * (kBK + 4) > (size_t)kBK * (128 + 4) ? (size_t)128 * (kBK + 4) : (size_t)kBK * 132;
-    return kStages * 2 * a * sizeof(double);
+    // largest config (128 x 64), worst orientation of each operand
+    constexpr size_t a = 128 * (kBK + 4) > kBK * (128 + 4) ? 128 * (kBK + 4) : kBK * (128 + 4);
+    constexpr size_t b = 64 * (kBK + 4) > kBK * (64 + 4) ? 64 * (kBK + 4) : kBK * (64 + 4);
+    return kStagesD * (a + b) * sizeof(double);
 }
 size_t ssmem_bytes() { return (size_t)kStages * kBK * (132 + 132) * sizeof(float); }
 
@@ -802,6 +882,9 @@ cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, in
     return cudaGetLastError();
 }
 
-int batched_tile_edge(int cfg) { return cfg == TILE_CFG_128 ? 128 : (cfg == TILE_CFG_64 ? 64 : 32); }
+int batched_tile_m(int cfg, int) { return cfg == TILE_CFG_128 ? 128 : (cfg == TILE_CFG_64 ? 64 : 32); }
+int batched_tile_n(int cfg, int dtype) {
+    return cfg == TILE_CFG_128 ? (dtype == BATCH_F64 ? 64 : 128) : (cfg == TILE_CFG_64 ? 64 : 32);
+}
 
 }  // namespace zb

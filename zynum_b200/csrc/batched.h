@@ -11,9 +11,11 @@ namespace zb {
 enum BatchDtype : int { BATCH_F64 = 0, BATCH_F32 = 1 };
 enum TileCfg : int { TILE_CFG_32 = 0, TILE_CFG_64 = 1, TILE_CFG_128 = 2 };
 
-// One output tile of one problem (prob < 0: padding, skipped).
+// A chunk of `count` consecutive output tiles t0.. of one problem (prob < 0:
+// padding, skipped).  Tile t covers rows (t % mt) TM.. and columns (t / mt) TN..
+// with TM x TN = batched_tile_m x batched_tile_n and mt = ceil(m / TM).
 struct BatchWork {
-    int prob, m0, n0, cfg;
+    int prob, t0, count, cfg;
 };
 
 // Device side of a GEMM batch plan.
@@ -23,7 +25,10 @@ struct BatchDevice {
     const int* dims;  // m, n, k per problem
 };
 
-int batched_tile_edge(int cfg);
+// Output tile of a config: rows x columns (the FP64 large config is 128 x 64,
+// the FP32 one 128 x 128).
+int batched_tile_m(int cfg, int dtype);
+int batched_tile_n(int cfg, int dtype);
 
 // a, b, c, lda, ldb, ldc: DEVICE arrays with one entry per problem.
 cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, char transb, const void* alpha,
