@@ -215,15 +215,40 @@ ZB_DEVICE void dgemm_chunk(const Prob<double>& p, int t0, int count, double alph
 }
 
 // ------------------------------------------------------- FP32 FFMA tile
-// BM x BN tile, 256 threads as 16 x 16, each thread (BM/16) x (BN/16) outputs.
-template <int BM, int BN, bool AM, bool BMF>
+// BM x BN tile, 8 warps as WARPS_M x (8 / WARPS_M), warp tile WTM x WTN, lanes
+// as LR x (32 / LR), each thread TM x TN outputs (TM = WTM / LR).  A thread's
+// rows are TM / G groups of G consecutive rows, group h at h * WTM / (TM / G)
+// (G = min(TM, 4)), so its A values of one k are float4 (float2) shared loads
+// and the lanes of a warp read consecutive 16-byte words; columns likewise.
+// Warps whose rows or columns all lie outside the problem skip the products.
+template <int N>
+struct FVec;
+template <>
+struct FVec<4> {
+    using T = float4;
+};
+template <>
+struct FVec<2> {
+    using T = float2;
+};
+
+template <int BM, int BN, int WARPS_M, int LR, bool AM, bool BMF>
 ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, float beta, float* smem) {
-    constexpr int TM = BM / 16, TN = BN / 16;
+    constexpr int WARPS_N = 8 / WARPS_M, LC = 32 / LR;
+    constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N, TM = WTM / LR, TN = WTN / LC;
+    constexpr int GM = TM < 4 ? TM : 4, GN = TN < 4 ? TN : 4;  // vector widths
+    constexpr int HM = TM / GM, HN = TN / GN;                  // groups per thread
+    static_assert(TM * LR == WTM && TN * LC == WTN && (GM == 2 || GM == 4) && (GN == 2 || GN == 4), "layout");
     constexpr int PA = BM + 4, PB = BN + 4;
+    using VA = typename FVec<GM>::T;
+    using VB = typename FVec<GN>::T;
     float* As = smem;                        // [stage][kBK][PA]  (m fast)
     float* Bs = smem + kStages * kBK * PA;   // [stage][kBK][PB]  (n fast)
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wr = (warp / WARPS_N) * WTM, wc = (warp % WARPS_N) * WTN;
+    const int lr = lane / LC, lc = lane % LC;
     const int KT = (alpha == 0.f) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
+    const bool active = wr < p.m - m0 && wc < p.n - n0;          // uniform across the warp
     float acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
@@ -261,29 +286,41 @@ ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, flo
         __syncthreads();
         if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
         cp_async_commit();
-        const float* as = As + (kt % kStages) * kBK * PA;
-        const float* bs = Bs + (kt % kStages) * kBK * PB;
+        const float* as = As + (kt % kStages) * kBK * PA + wr + lr * GM;
+        const float* bs = Bs + (kt % kStages) * kBK * PB + wc + lc * GN;
+        if (active) {
 #pragma unroll
-        for (int kk = 0; kk < kBK; ++kk) {
-            float a[TM], b[TN];
+            for (int kk = 0; kk < kBK; ++kk) {
+                float a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = as[kk * PA + ty + 16 * i];
+                for (int h = 0; h < HM; ++h) {
+                    const VA v = *reinterpret_cast<const VA*>(as + kk * PA + h * (WTM / HM));
+                    const float* f = reinterpret_cast<const float*>(&v);
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = bs[kk * PB + tx + 16 * j];
+                    for (int e = 0; e < GM; ++e) a[h * GM + e] = f[e];
+                }
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int h = 0; h < HN; ++h) {
+                    const VB v = *reinterpret_cast<const VB*>(bs + kk * PB + h * (WTN / HN));
+                    const float* f = reinterpret_cast<const float*>(&v);
 #pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                    for (int e = 0; e < GN; ++e) b[h * GN + e] = f[e];
+                }
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            }
         }
     }
     cp_async_wait<0>();
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-        const int col = n0 + tx + 16 * j;
+        const int col = n0 + wc + (j / GN) * (WTN / HN) + lc * GN + (j % GN);
         if (col >= p.n) continue;
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
-            const int row = m0 + ty + 16 * i;
+            const int row = m0 + wr + (i / GM) * (WTM / HM) + lr * GM + (i % GM);
             if (row >= p.m) continue;
             float* cp = p.c + (long)col * p.ldc + row;
             float out = alpha * acc[i][j];
@@ -333,12 +370,12 @@ sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* 
         const int mt = (p.m + e - 1) / e;
         for (int tile = it.t0; tile < it.t0 + it.count; ++tile) {
             const int m0 = (tile % mt) * e, n0 = (tile / mt) * e;
-            if (it.cfg == TILE_CFG_128)
-                sgemm_tile<128, 128, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
-            else if (it.cfg == TILE_CFG_64)
-                sgemm_tile<64, 64, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
-            else
-                sgemm_tile<32, 32, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+            if (it.cfg == TILE_CFG_128)  // warps 2 x 4 of 64 x 32, threads 8 x 8
+                sgemm_tile<128, 128, 2, 8, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+            else if (it.cfg == TILE_CFG_64)  // warps 4 x 2 of 16 x 32, threads 4 x 4
+                sgemm_tile<64, 64, 4, 4, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
+            else  // warps 4 x 2 of 8 x 16, threads 2 x 2
+                sgemm_tile<32, 32, 4, 4, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
         }
     }
 }
