@@ -214,10 +214,11 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------------ batches
-def bench_batched(torch, blas, steps, warmup, seed=7):
+def bench_batched(torch, blas, steps, warmup, seed=7, count=20000, tcount=5000, which=("dgemm", "sgemm", "dtrsm")):
     """20,000 variable-size DGEMM and SGEMM problems (M, N, K log-uniform on [8, 512], alpha 1, beta 0)
     and 5,000 left-lower TRSMs (n log-uniform on [16, 1024], 1..64 right-hand sides, L = tril(N(0,1))
-    with diagonal 2 + |N(0,1)|), each batch one persistent launch replayed from a CUDA graph."""
+    with diagonal 2 + |N(0,1)|), each batch one persistent launch replayed from a CUDA graph.
+    count / tcount / which select a smaller sample of the same distributions (profiling)."""
     rng = np.random.default_rng(seed)
     dev = torch.device("cuda")
     out = {}
@@ -234,10 +235,11 @@ def bench_batched(torch, blas, steps, warmup, seed=7):
         ptrs = torch.from_numpy(offs * esz + buf.data_ptr()).to(dev)
         return buf, ptrs
 
-    count = 20000
     m, n, k = lu(8, 512, count), lu(8, 512, count), lu(8, 512, count)
     flops = float(np.sum(2.0 * m * n * k))
     for name, tdt in (("dgemm", torch.float64), ("sgemm", torch.float32)):
+        if name not in which:
+            continue
         g = torch.Generator(device=dev).manual_seed(seed)
         ufill = lambda b: b.uniform_(-1, 1, generator=g)  # noqa: E731
         A, pa = carve(m * k, tdt, ufill)
@@ -254,7 +256,8 @@ def bench_batched(torch, blas, steps, warmup, seed=7):
                      "plan_and_tune_s": plan_s, **batch.info()}
         batch.close()
         del A, B, Cb
-    tcount = 5000
+    if "dtrsm" not in which:
+        return out
     tn = lu(16, 1024, tcount)
     tr = rng.integers(1, 65, tcount).astype(np.int64)
     tflops = float(np.sum(tn.astype(np.float64) ** 2 * tr))
@@ -693,6 +696,16 @@ def suite_level3(args):
     return 0
 
 
+def suite_batched(args):
+    """The batched workloads alone (optionally a smaller sample of the same distributions)."""
+    import torch
+    from zynum_b200 import blas
+    out = bench_batched(torch, blas, args.steps, args.warmup, count=args.batch_count,
+                        tcount=max(1, args.batch_count // 4), which=tuple(args.batch_only.split(",")))
+    print(json.dumps({"suite": "batched", "count": args.batch_count, "rows": out}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -705,8 +718,11 @@ def main(argv=None):
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3"], default="headline",
-                    help="precision / sweep: secondary measurement suites (one JSON line each)")
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched"],
+                    default="headline", help="secondary measurement suites (one JSON line each)")
+    ap.add_argument("--batch-count", type=int, default=20000,
+                    help="batched suite: GEMM problems per batch (TRSM problems: a quarter)")
+    ap.add_argument("--batch-only", default="dgemm,sgemm,dtrsm", help="batched suite: which batches")
     args = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -731,6 +747,8 @@ def main(argv=None):
             return suite_vector(args)
         if args.suite == "level3":
             return suite_level3(args)
+        if args.suite == "batched":
+            return suite_batched(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -25,7 +25,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBK = 16;
-constexpr int kStages = 2;   // FP32: two cp.async stages, two CTAs per SM
+constexpr int kStages = 3;   // FP32: three cp.async stages, two CTAs per SM
 constexpr int kStagesD = 3;  // FP64: three stages of at most 30 KB, two CTAs per SM
 
 template <typename T>
@@ -249,6 +249,7 @@ ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, flo
     const int lr = lane / LC, lc = lane % LC;
     const int KT = (alpha == 0.f) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
     const bool active = wr < p.m - m0 && wc < p.n - n0;          // uniform across the warp
+    const bool va = AM && vec_ok(p.a, p.lda), vb = BMF && vec_ok(p.b, p.ldb);
     float acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
@@ -258,22 +259,31 @@ ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, flo
         const int k0 = kt * kBK;
         float* as = As + stage * kBK * PA;
         float* bs = Bs + stage * kBK * PB;
-        // element (mn, kk) of the tile -> shared [kk][mn]
-        for (int q = threadIdx.x; q < kBK * BM; q += kThreads) {
-            int kk, mm;
-            if (AM) { kk = q / BM; mm = q % BM; } else { mm = q / kBK; kk = q % kBK; }
-            const int gm = m0 + mm, gk = k0 + kk;
-            const bool ok = gm < p.m && gk < p.k;
-            const float* src = ok ? (AM ? p.a + gm + (long)gk * p.lda : p.a + gk + (long)gm * p.lda) : p.a;
-            cp_async_4(smem_u32(as + kk * PA + mm), src, ok ? 4 : 0);
+        // element (mn, kk) of the tile -> shared [kk][mn]; an operand contiguous along m (n)
+        // goes by 16-byte copies when aligned (va / vb)
+        if (AM && va) {
+            load_tile<float, kBK, BM>(as, PA, p.a, p.lda, k0, m0, p.k, p.m, true);
+        } else {
+            for (int q = threadIdx.x; q < kBK * BM; q += kThreads) {
+                int kk, mm;
+                if (AM) { kk = q / BM; mm = q % BM; } else { mm = q / kBK; kk = q % kBK; }
+                const int gm = m0 + mm, gk = k0 + kk;
+                const bool ok = gm < p.m && gk < p.k;
+                const float* src = ok ? (AM ? p.a + gm + (long)gk * p.lda : p.a + gk + (long)gm * p.lda) : p.a;
+                cp_async_4(smem_u32(as + kk * PA + mm), src, ok ? 4 : 0);
+            }
         }
-        for (int q = threadIdx.x; q < kBK * BN; q += kThreads) {
-            int kk, nn;
-            if (BMF) { kk = q / BN; nn = q % BN; } else { nn = q / kBK; kk = q % kBK; }
-            const int gn = n0 + nn, gk = k0 + kk;
-            const bool ok = gn < p.n && gk < p.k;
-            const float* src = ok ? (BMF ? p.b + gn + (long)gk * p.ldb : p.b + gk + (long)gn * p.ldb) : p.b;
-            cp_async_4(smem_u32(bs + kk * PB + nn), src, ok ? 4 : 0);
+        if (BMF && vb) {
+            load_tile<float, kBK, BN>(bs, PB, p.b, p.ldb, k0, n0, p.k, p.n, true);
+        } else {
+            for (int q = threadIdx.x; q < kBK * BN; q += kThreads) {
+                int kk, nn;
+                if (BMF) { kk = q / BN; nn = q % BN; } else { nn = q / kBK; kk = q % kBK; }
+                const int gn = n0 + nn, gk = k0 + kk;
+                const bool ok = gn < p.n && gk < p.k;
+                const float* src = ok ? (BMF ? p.b + gn + (long)gk * p.ldb : p.b + gk + (long)gn * p.ldb) : p.b;
+                cp_async_4(smem_u32(bs + kk * PB + nn), src, ok ? 4 : 0);
+            }
         }
     };
 #pragma unroll
