@@ -57,11 +57,11 @@ ZB_DEVICE void load_tile(double* smem, const double* __restrict__ base, long ld,
     }
 }
 
-// BM x BN block tile, WM x WN warp tile, STAGES-deep cp.async ring.
+// BM x BN block tile, WM x WN warp tile, STAGES-deep cp.async ring of BK-deep slices.
 // A_KFAST: A's shared tile is [m][k] (A stored transposed in global memory).
 // B_KFAST: B's shared tile is [n][k] (B stored untransposed in global memory).
 // PARTIAL: write raw accumulators to workspace slice blockIdx.z (ld = M).
-template <int BM, int BN, int WM, int WN, int STAGES, bool A_KFAST, bool B_KFAST, int VEC, bool PARTIAL>
+template <int BM, int BN, int WM, int WN, int STAGES, bool A_KFAST, bool B_KFAST, int VEC, bool PARTIAL, int BK>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 1)
 dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* __restrict__ A, long lda,
                   const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
@@ -71,8 +71,8 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
     constexpr int MI = WM / 16;
     constexpr int NI = WN / 8;
     // Shared tile geometry (pitch = 4 mod 16 doubles).
-    constexpr int A_ROWS = A_KFAST ? BM : kBK, A_COLS = A_KFAST ? kBK : BM, A_PITCH = A_COLS + 4;
-    constexpr int B_ROWS = B_KFAST ? BN : kBK, B_COLS = B_KFAST ? kBK : BN, B_PITCH = B_COLS + 4;
+    constexpr int A_ROWS = A_KFAST ? BM : BK, A_COLS = A_KFAST ? BK : BM, A_PITCH = A_COLS + 4;
+    constexpr int B_ROWS = B_KFAST ? BN : BK, B_COLS = B_KFAST ? BK : BN, B_PITCH = B_COLS + 4;
     constexpr int A_STAGE = A_ROWS * A_PITCH, B_STAGE = B_ROWS * B_PITCH;
 
     extern __shared__ __align__(128) double smem[];
@@ -85,7 +85,7 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
     if ((tri == 1 && m0 > n0 + BN - 1) || (tri == 2 && m0 + BM - 1 < n0)) return;
     const int kb = blockIdx.z * k_chunk;
     const int ke = min(K, kb + k_chunk);
-    const int KT = (ke - kb + kBK - 1) / kBK;
+    const int KT = (ke - kb + BK - 1) / BK;
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -102,7 +102,7 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
             for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
     auto load_stage = [&](int stage, int kt) {
-        const int k0 = kb + kt * kBK;
+        const int k0 = kb + kt * BK;
         if (A_KFAST)  // A stored k x m (op = T): rows m, contiguous k
             load_tile<A_ROWS, A_COLS, A_PITCH, VEC, NTHREADS>(As + stage * A_STAGE, A, lda, m0, k0, M, ke);
         else  // A stored m x k: rows k, contiguous m
@@ -130,7 +130,7 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
         const double* as = As + (kt % STAGES) * A_STAGE;
         const double* bs = Bs + (kt % STAGES) * B_STAGE;
 #pragma unroll
-        for (int ks = 0; ks < kBK; ks += 8) {
+        for (int ks = 0; ks < BK; ks += 8) {
             double af[MI][4], bf[NI][2];
 #pragma unroll
             for (int i = 0; i < MI; ++i) {
@@ -214,13 +214,13 @@ __global__ void dgemm_splitk_reduce(int M, int N, int splits, const double* __re
     }
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool AK, bool BK_, int VEC, bool PARTIAL>
+template <int BM, int BN, int WM, int WN, int STAGES, bool AK, bool BK_, int VEC, bool PARTIAL, int BK>
 cudaError_t launch_one(const GemmArgsF64& g, int splits, int k_chunk, double* W, cudaStream_t st) {
     constexpr int NTHREADS = (BM / WM) * (BN / WN) * 32;
-    constexpr int A_ROWS = AK ? BM : kBK, A_COLS = AK ? kBK : BM;
-    constexpr int B_ROWS = BK_ ? BN : kBK, B_COLS = BK_ ? kBK : BN;
+    constexpr int A_ROWS = AK ? BM : BK, A_COLS = AK ? BK : BM;
+    constexpr int B_ROWS = BK_ ? BN : BK, B_COLS = BK_ ? BK : BN;
     constexpr size_t SMEM = (size_t)STAGES * (A_ROWS * (A_COLS + 4) + B_ROWS * (B_COLS + 4)) * sizeof(double);
-    auto kern = dgemm_dmma_kernel<BM, BN, WM, WN, STAGES, AK, BK_, VEC, PARTIAL>;
+    auto kern = dgemm_dmma_kernel<BM, BN, WM, WN, STAGES, AK, BK_, VEC, PARTIAL, BK>;
     cudaError_t e = ensure_dynamic_smem(kern, (int)SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, splits);
@@ -232,24 +232,24 @@ cudaError_t launch_one(const GemmArgsF64& g, int splits, int k_chunk, double* W,
     return cudaGetLastError();
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool PARTIAL>
+template <int BM, int BN, int WM, int WN, int STAGES, bool PARTIAL, int BK>
 cudaError_t dispatch_layout(const GemmArgsF64& g, int vec, int splits, int k_chunk, double* W, cudaStream_t st) {
     const bool ak = g.transa != 'N', bk = g.transb == 'N';
 #define ZB_CASE(AK, BKF, V)                                                                              \
     if (ak == AK && bk == BKF && vec == V)                                                               \
-        return launch_one<BM, BN, WM, WN, STAGES, AK, BKF, V, PARTIAL>(g, splits, k_chunk, W, st);
+        return launch_one<BM, BN, WM, WN, STAGES, AK, BKF, V, PARTIAL, BK>(g, splits, k_chunk, W, st);
     ZB_CASE(false, false, 1) ZB_CASE(false, true, 1) ZB_CASE(true, false, 1) ZB_CASE(true, true, 1)
     ZB_CASE(false, false, 2) ZB_CASE(false, true, 2) ZB_CASE(true, false, 2) ZB_CASE(true, true, 2)
 #undef ZB_CASE
     return cudaErrorInvalidValue;
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES>
+template <int BM, int BN, int WM, int WN, int STAGES, int BK = kBK>
 cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chunk, double* workspace,
                       cudaStream_t st) {
-    if (used_splits == 1) return dispatch_layout<BM, BN, WM, WN, STAGES, false>(g, vec, 1, k_chunk, nullptr, st);
+    if (used_splits == 1) return dispatch_layout<BM, BN, WM, WN, STAGES, false, BK>(g, vec, 1, k_chunk, nullptr, st);
     if (!workspace) return cudaErrorInvalidValue;
-    cudaError_t e = dispatch_layout<BM, BN, WM, WN, STAGES, true>(g, vec, used_splits, k_chunk, workspace, st);
+    cudaError_t e = dispatch_layout<BM, BN, WM, WN, STAGES, true, BK>(g, vec, used_splits, k_chunk, workspace, st);
     if (e != cudaSuccess) return e;
     long total = (long)g.m * g.n;
     int blocks = (int)((total + 255) / 256);
@@ -283,6 +283,10 @@ cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* wor
         case TILE_64x64:  // few output tiles: 64 x 64 tiles, warps 2 x 2 of 32 x 32
             return run_tiles<64, 64, 32, 32, 4>(g, vec, used, k_chunk, workspace, st);
         default:
+            // op(B) k-contiguous (transb N): three 32-deep stages (212 KB), half the block
+            // barriers of 16-deep slices (+2 % measured at 2048-8192); otherwise four 16-deep
+            // stages (32-deep slices measured 1 % slower there)
+            if (g.transb == 'N') return run_tiles<128, 128, 64, 32, 3, 32>(g, vec, used, k_chunk, workspace, st);
             return run_tiles<128, 128, 64, 32, 4>(g, vec, used, k_chunk, workspace, st);
     }
 }
