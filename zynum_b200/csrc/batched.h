@@ -25,8 +25,8 @@ struct BatchDevice {
     const int* dims;  // m, n, k per problem
 };
 
-// Output tile of a config: rows x columns (the FP64 large config is 128 x 64,
-// the FP32 one 128 x 128).
+// Output tile of a config: rows x columns (square; TILE_CFG_128 is 128 x 128
+// for FP32 and runs as 64 x 64 for FP64).
 int batched_tile_m(int cfg, int dtype);
 int batched_tile_n(int cfg, int dtype);
 

@@ -61,9 +61,9 @@ int default_cfg(int m, int n) {
     return TILE_CFG_128;
 }
 
-std::vector<int> candidates(int bucket) {
+std::vector<int> candidates(int bucket, int dtype) {
     const int c = bucket / 3 + 3;  // log2 class
-    if (c <= 5) return {TILE_CFG_32, TILE_CFG_64};
+    if (c <= 5 || dtype == BATCH_F64) return {TILE_CFG_32, TILE_CFG_64};  // FP64 tiles stop at 64 x 64
     if (c <= 7) return {TILE_CFG_32, TILE_CFG_64, TILE_CFG_128};
     return {TILE_CFG_64, TILE_CFG_128};
 }
@@ -321,7 +321,7 @@ std::vector<int> choose_cfgs(Batch& b, bool tune) {
         // 5 % faster on the sample (the synthetic timing is L2-resident and noisy)
         int best_cfg = kCfgRule;
         float best_ms = time_bucket(b, probs, kCfgRule, st, buf, d_ptrs, d_lds) * 0.95f;
-        for (int c : candidates(kv.first)) {
+        for (int c : candidates(kv.first, b.dtype)) {
             const float ms = time_bucket(b, probs, c, st, buf, d_ptrs, d_lds);
             if (ms < best_ms) {
                 best_ms = ms;
@@ -407,7 +407,7 @@ int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
     b->m.assign(m, m + count);
     b->n.assign(n, n + count);
     b->k.assign(k, k + count);
-    b->grid = 2 * sm_count();  // two tile CTAs per SM
+    b->grid = (dtype == BATCH_F64 ? 4 : 2) * sm_count();  // tile CTAs per SM: FP64 four, FP32 two
     std::vector<int> dims;
     for (int q = 0; q < count; ++q) {
         dims.push_back(m[q]);
