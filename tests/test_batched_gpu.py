@@ -63,6 +63,49 @@ def test_gemm_batch(blas, dtype, ta, tb):
             assert np.all(np.abs(got - want) <= bound), (q, m[q], n[q], k[q])
 
 
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_gemm_batch_alpha_zero_and_padded_ld(blas, dtype):
+    """alpha = 0 gives C = beta C without reading A or B (NaN in A stays out); padded, odd
+    leading dimensions (ld = rows + 3) take the element-wise copies; the padding rows of C
+    stay untouched."""
+    import torch
+    rng = np.random.default_rng(99)
+    cnt = 64
+    m, n, k = (_loguniform(rng, 8, 300, cnt) for _ in range(3))
+    npdt = np.float64 if dtype == "f64" else np.float32
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    A = [rng.uniform(-1, 1, (m[q] + 3, k[q])).astype(npdt) for q in range(cnt)]
+    B = [rng.uniform(-1, 1, (k[q] + 3, n[q])).astype(npdt) for q in range(cnt)]
+    C0 = [rng.uniform(-1, 1, (m[q] + 3, n[q])).astype(npdt) for q in range(cnt)]
+    ta_, pa, la = _pack(torch, A, tdt)
+    tb_, pb, lb = _pack(torch, B, tdt)
+    batch = blas.GemmBatch(m, n, k, dtype=dtype, tune=False)
+    u = 2.0 ** -53 if dtype == "f64" else 2.0 ** -24
+    for alpha in (0.0, 1.5):
+        if alpha == 0.0:
+            for q in range(cnt):
+                ta_[q][0, 0] = float("nan")  # element (0, 0) of A: never read when alpha = 0
+        else:
+            for q in range(cnt):
+                ta_[q].copy_(torch.from_numpy(np.ascontiguousarray(A[q].T)))
+        tc_, pc, lc = _pack(torch, C0, tdt)
+        batch.run(alpha, pa, la, pb, lb, 0.5, pc, lc)
+        torch.cuda.synchronize()
+        for q in range(cnt):
+            got = tc_[q].cpu().numpy().T.astype(np.float64)
+            c0 = C0[q].astype(np.float64)
+            if alpha == 0.0:
+                want = 0.5 * c0[: m[q]]
+                assert np.array_equal(got[: m[q]], want.astype(npdt).astype(np.float64)), q
+            else:
+                a, b = A[q].astype(np.float64)[: m[q]], B[q].astype(np.float64)[: k[q]]
+                want = 1.5 * (a @ b) + 0.5 * c0[: m[q]]
+                bound = 4 * k[q] * u * (1.5 * np.abs(a) @ np.abs(b) + 0.5 * np.abs(c0[: m[q]])) + 1e-300
+                assert np.all(np.abs(got[: m[q]] - want) <= bound), q
+            assert np.array_equal(got[m[q]:], c0[m[q]:]), "padding rows of C changed"
+    batch.close()
+
+
 def test_gemm_batch_tune_cache(blas, tmp_path, monkeypatch):
     """The autotuner's table is written to the JSON cache named by ZYNUM_GPU_TUNE_CACHE (fresh process)."""
     import subprocess
