@@ -309,6 +309,47 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zsyrk_device(char uplo, char trans, int n,
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_csyrk_device(char uplo, char trans, int n, int k, const float *alpha,
                                                    const float *a, int lda, const float *beta, float *c, int ldc,
                                                    void *stream);
+/* Complex SYMM / HEMM on device pointers (interleaved complex; alpha, beta point to re, im): the stored
+ * triangle mirrored (conjugated for HEMM, real diagonal) into scratch, one complex GEMM.  Argument
+ * numbering as zsymm_ / zhemm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zsymm_device(char side, char uplo, int m, int n, const double *alpha,
+                                                   const double *a, int lda, const double *b, int ldb,
+                                                   const double *beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zhemm_device(char side, char uplo, int m, int n, const double *alpha,
+                                                   const double *a, int lda, const double *b, int ldb,
+                                                   const double *beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_csymm_device(char side, char uplo, int m, int n, const float *alpha,
+                                                   const float *a, int lda, const float *b, int ldb,
+                                                   const float *beta, float *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_chemm_device(char side, char uplo, int m, int n, const float *alpha,
+                                                   const float *a, int lda, const float *b, int ldb,
+                                                   const float *beta, float *c, int ldc, void *stream);
+/* Complex TRMM on device pointers (op = C conjugates).  Argument numbering as ztrmm_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ztrmm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   const double *alpha, const double *a, int lda, double *b, int ldb,
+                                                   void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ctrmm_device(char side, char uplo, char transa, char diag, int m, int n,
+                                                   const float *alpha, const float *a, int lda, float *b, int ldb,
+                                                   void *stream);
+/* Complex SYR2K / HER2K / HERK on device pointers: one complex GEMM into scratch and a triangle update
+ * (HER2K: beta real; HERK: alpha and beta real, diagonal made real).  Argument numbering as zsyr2k_,
+ * zher2k_, zherk_. */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zsyr2k_device(char uplo, char trans, int n, int k, const double *alpha,
+                                                    const double *a, int lda, const double *b, int ldb,
+                                                    const double *beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zher2k_device(char uplo, char trans, int n, int k, const double *alpha,
+                                                    const double *a, int lda, const double *b, int ldb, double beta,
+                                                    double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_zherk_device(char uplo, char trans, int n, int k, double alpha, const double *a,
+                                                   int lda, double beta, double *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_csyr2k_device(char uplo, char trans, int n, int k, const float *alpha,
+                                                    const float *a, int lda, const float *b, int ldb,
+                                                    const float *beta, float *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_cher2k_device(char uplo, char trans, int n, int k, const float *alpha,
+                                                    const float *a, int lda, const float *b, int ldb, float beta,
+                                                    float *c, int ldc, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_cherk_device(char uplo, char trans, int n, int k, float alpha, const float *a,
+                                                   int lda, float beta, float *c, int ldc, void *stream);
 /* SYMM on device pointers: the stored triangle of A is mirrored into a dense scratch copy, then one
  * GEMM (following the DGEMM / SGEMM method).  Argument numbering as dsymm_. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsymm_device(char side, char uplo, int m, int n, double alpha, const double *a,

@@ -241,3 +241,57 @@ def test_complex_argument_errors_leave_outputs(blas):
     blas.herk("X", "N", 8, 8, 1.0, a, 8, 0.0, c, 8)
     blas.syr2k("U", "N", 8, 8, 1.0, a, 8, a, 8, 0.0, c, 4, herm=True)
     assert np.array_equal(c, c0)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["z", "c"])
+def test_complex_level3_device_entry_points(blas, oracle, dtype):
+    """zynum_blas_gpu_{z,c}{symm,hemm,trmm,syr2k,her2k,herk}_device on torch tensors against the
+    oracle on the same column-major data (device pointers, the caller's stream)."""
+    import torch
+    rng = np.random.default_rng(51 if dtype == np.complex128 else 52)
+    tol = 1e-11 if dtype == np.complex128 else 2e-4
+    tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda", tdt)  # noqa: E731
+    host = lambda t: np.asfortranarray(t.cpu().numpy().T)  # noqa: E731
+    m, n, k = 140, 90, 70
+    rel = lambda got, ref: np.abs(got - ref).max() / (1 + np.abs(ref).max())  # noqa: E731
+    for herm in (False, True):  # SYMM / HEMM, side L, uplo U
+        a, b, c = _cx(rng, (m, m), dtype), _cx(rng, (m, n), dtype), _cx(rng, (m, n), dtype)
+        ref = c.copy(order="F")
+        oracle.symm("L", "U", m, n, 0.5 + 0.25j, a, m, b, m, 1.5 - 0.5j, ref, m, herm=herm)
+        C = dev(c)
+        blas.symm_device_c("L", "U", m, n, 0.5 + 0.25j, dev(a), m, dev(b), m, 1.5 - 0.5j, C, m, herm=herm)
+        torch.cuda.synchronize()
+        assert rel(host(C), ref) <= tol, ("symm", herm)
+    # TRMM, side R, lower, op = C
+    a, b = _ctri(rng, n, n, dtype), _cx(rng, (m, n), dtype)
+    ref = b.copy(order="F")
+    oracle.trmm("R", "L", "C", "N", m, n, 2.0 - 1.0j, a, n, ref, m)
+    B = dev(b)
+    blas.trmm_device_c("R", "L", "C", "N", m, n, 2.0 - 1.0j, dev(a), n, B, m)
+    torch.cuda.synchronize()
+    assert rel(host(B), ref) <= tol, "trmm"
+    up = np.triu(np.ones((n, n), bool))
+    for herm in (False, True):  # SYR2K / HER2K, upper, op = C
+        a, b, c = _cx(rng, (k, n), dtype), _cx(rng, (k, n), dtype), _cx(rng, (n, n), dtype)
+        beta = 0.5 if herm else 0.5 + 0.5j
+        ref = c.copy(order="F")
+        oracle.syr2k("U", "C", n, k, 1.0 - 0.5j, a, k, b, k, beta, ref, n, herm=herm)
+        C = dev(c)
+        blas.syr2k_device_c("U", "C", n, k, 1.0 - 0.5j, dev(a), k, dev(b), k, beta, C, n, herm=herm)
+        torch.cuda.synchronize()
+        got = host(C)
+        assert rel(got[up], ref[up]) <= tol, ("syr2k", herm)
+        assert np.array_equal(got[~up], c[~up])
+    # HERK, lower, op = N
+    a, c = _cx(rng, (n, k), dtype), _cx(rng, (n, n), dtype)
+    ref = c.copy(order="F")
+    oracle.herk("L", "N", n, k, 1.25, a, n, -0.5, ref, n)
+    C = dev(c)
+    blas.herk_device("L", "N", n, k, 1.25, dev(a), n, -0.5, C, n)
+    torch.cuda.synchronize()
+    got = host(C)
+    lo = np.tril(np.ones((n, n), bool))
+    assert rel(got[lo], ref[lo]) <= tol, "herk"
+    assert np.all(np.diag(got).imag == 0)
+    assert np.array_equal(got[~lo], c[~lo])

@@ -91,6 +91,23 @@ def _declare(L: C.CDLL) -> None:
     for name in ("zynum_blas_gpu_zsyrk_device", "zynum_blas_gpu_csyrk_device"):
         getattr(L, name).argtypes = [ch, ch, i, i, P, P, i, P, P, i, P]
         getattr(L, name).restype = i
+    for name in ("zynum_blas_gpu_zsymm_device", "zynum_blas_gpu_csymm_device", "zynum_blas_gpu_zhemm_device",
+                 "zynum_blas_gpu_chemm_device"):
+        getattr(L, name).argtypes = [ch, ch, i, i, P, P, i, P, i, P, P, i, P]
+        getattr(L, name).restype = i
+    for name in ("zynum_blas_gpu_ztrmm_device", "zynum_blas_gpu_ctrmm_device"):
+        getattr(L, name).argtypes = [ch, ch, ch, ch, i, i, P, P, i, P, i, P]
+        getattr(L, name).restype = i
+    for name in ("zynum_blas_gpu_zsyr2k_device", "zynum_blas_gpu_csyr2k_device"):
+        getattr(L, name).argtypes = [ch, ch, i, i, P, P, i, P, i, P, P, i, P]
+        getattr(L, name).restype = i
+    L.zynum_blas_gpu_zher2k_device.argtypes = [ch, ch, i, i, P, P, i, P, i, d, P, i, P]
+    L.zynum_blas_gpu_cher2k_device.argtypes = [ch, ch, i, i, P, P, i, P, i, f, P, i, P]
+    L.zynum_blas_gpu_zherk_device.argtypes = [ch, ch, i, i, d, P, i, d, P, i, P]
+    L.zynum_blas_gpu_cherk_device.argtypes = [ch, ch, i, i, f, P, i, f, P, i, P]
+    for name in ("zynum_blas_gpu_zher2k_device", "zynum_blas_gpu_cher2k_device", "zynum_blas_gpu_zherk_device",
+                 "zynum_blas_gpu_cherk_device"):
+        getattr(L, name).restype = i
     for name in ("dsymm_", "ssymm_", "zsymm_", "csymm_", "zhemm_", "chemm_"):
         getattr(L, name).argtypes = [cp, cp, I32P, I32P, P, P, I32P, P, I32P, P, P, I32P]
         getattr(L, name).restype = None

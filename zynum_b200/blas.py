@@ -322,6 +322,66 @@ def syrk_device_c(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
     return c
 
 
+def symm_device_c(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, herm=False, stream=None):
+    """Device zsymm / csymm (zhemm / chemm with herm) on complex128 / complex64 torch tensors."""
+    import torch
+    L = load()
+    z = c.dtype == torch.complex128
+    p = "z" if z else "c"
+    name = f"zynum_blas_gpu_{p}{'hemm' if herm else 'symm'}_device"
+    dt = np.complex128 if z else np.complex64
+    al, be = _cscalar(dt, alpha), _cscalar(dt, beta)
+    st = getattr(L, name)(_ch(side), _ch(uplo), m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data,
+                          _ptr(c), ldc, _stream(stream))
+    check(st, name)
+    return c
+
+
+def trmm_device_c(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream=None):
+    """Device ztrmm / ctrmm on complex128 / complex64 torch tensors (in place on b)."""
+    import torch
+    L = load()
+    z = b.dtype == torch.complex128
+    fn, dt = (L.zynum_blas_gpu_ztrmm_device, np.complex128) if z else (L.zynum_blas_gpu_ctrmm_device, np.complex64)
+    al = _cscalar(dt, alpha)
+    st = fn(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb,
+            _stream(stream))
+    check(st, "zynum_blas_gpu_ztrmm_device" if z else "zynum_blas_gpu_ctrmm_device")
+    return b
+
+
+def syr2k_device_c(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, herm=False, stream=None):
+    """Device zsyr2k / csyr2k (zher2k / cher2k with herm: beta real) on complex torch tensors."""
+    import torch
+    L = load()
+    z = c.dtype == torch.complex128
+    p = "z" if z else "c"
+    dt = np.complex128 if z else np.complex64
+    al = _cscalar(dt, alpha)
+    if herm:
+        name = f"zynum_blas_gpu_{p}her2k_device"
+        st = getattr(L, name)(_ch(uplo), _ch(trans), n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb,
+                              float(np.real(beta)), _ptr(c), ldc, _stream(stream))
+    else:
+        name = f"zynum_blas_gpu_{p}syr2k_device"
+        be = _cscalar(dt, beta)
+        st = getattr(L, name)(_ch(uplo), _ch(trans), n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb,
+                              be.ctypes.data, _ptr(c), ldc, _stream(stream))
+    check(st, name)
+    return c
+
+
+def herk_device(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
+    """Device zherk / cherk on complex torch tensors (alpha, beta real; c's triangle, real diagonal)."""
+    import torch
+    L = load()
+    z = c.dtype == torch.complex128
+    fn = L.zynum_blas_gpu_zherk_device if z else L.zynum_blas_gpu_cherk_device
+    st = fn(_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, float(beta), _ptr(c), ldc, _stream(stream))
+    check(st, "zynum_blas_gpu_zherk_device" if z else "zynum_blas_gpu_cherk_device")
+    return c
+
+
 def cblas_trsm_c(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
     """cblas_ztrsm / cblas_ctrsm (dtype from b)."""
     L = load()

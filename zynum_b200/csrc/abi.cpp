@@ -1121,6 +1121,47 @@ int device_syr2k(const char* what, char uplo, char trans, int n, int k, T alpha,
                        what);
 }
 
+// Complex SYMM / HEMM on device pointers (run_symm's complex overload).
+template <typename R>
+int device_symm_c(const char* what, char side, char uplo, int m, int n, cnum<R> alpha, const cnum<R>* a, int lda,
+                  const cnum<R>* b, int ldb, cnum<R> beta, cnum<R>* c, int ldc, void* stream, bool herm) {
+    const char sd = up(&side), ul = up(&uplo);
+    int info = symm_error(sd, ul, m, n, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_symm(sd, ul, m, n, alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream),
+                                StreamScratch{&cx}, herm),
+                       what);
+}
+
+// Complex SYR2K / HER2K (two) and HERK (b == a) on device pointers (run_rank2k_c).
+template <typename R>
+int device_rank2k_c(const char* what, char uplo, char trans, int n, int k, cnum<R> alpha, const cnum<R>* a, int lda,
+                    const cnum<R>* b, int ldb, cnum<R> beta, cnum<R>* c, int ldc, void* stream, bool herm,
+                    bool two) {
+    const char ul = up(&uplo), tr = up(&trans);
+    int info = two ? syr2k_error(ul, tr, n, k, lda, ldb, ldc) : syrk_error(ul, tr, n, k, lda, ldc);
+    if (info) return info;
+    if (n == 0) return 0;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    return cuda_status(run_rank2k_c<R>(ul, tr, herm, two, n, k, alpha, a, lda, two ? b : a, two ? ldb : lda, beta, c,
+                                       ldc, static_cast<cudaStream_t>(stream), StreamScratch{&cx}),
+                       what);
+}
+
 inline char cblas_uplo_char(int u) { return u == CblasUpper ? 'U' : (u == CblasLower ? 'L' : 'X'); }
 inline char cblas_row_uplo_char(int u) { return u == CblasUpper ? 'L' : (u == CblasLower ? 'U' : 'X'); }
 inline char cblas_side_char(int s) { return s == CblasLeft ? 'L' : (s == CblasRight ? 'R' : 'X'); }
@@ -1734,6 +1775,67 @@ int zynum_blas_gpu_ssyr2k_device(char uplo, char trans, int n, int k, float alph
                                  const float* b, int ldb, float beta, float* c, int ldc, void* stream) {
     return device_syr2k<float>("ssyr2k_device", uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream);
 }
+
+// Complex SYMM / HEMM / TRMM / SYR2K / HER2K / HERK on device pointers
+// (interleaved complex; complex scalars point to re, im; HERK alpha, beta and
+// HER2K beta are real, by value, as in cblas_zherk / cblas_zher2k).
+#define ZB_DEV_SYMM_C(NAME, R, WHAT, HERM)                                                                       \
+    int NAME(char side, char uplo, int m, int n, const R* alpha, const R* a, int lda, const R* b, int ldb,      \
+             const R* beta, R* c, int ldc, void* stream) {                                                      \
+        return device_symm_c<R>(WHAT, side, uplo, m, n, cnum<R>(alpha[0], alpha[1]),                            \
+                                reinterpret_cast<const cnum<R>*>(a), lda, reinterpret_cast<const cnum<R>*>(b), ldb, \
+                                cnum<R>(beta[0], beta[1]), reinterpret_cast<cnum<R>*>(c), ldc, stream, HERM);   \
+    }
+ZB_DEV_SYMM_C(zynum_blas_gpu_zsymm_device, double, "zsymm_device", false)
+ZB_DEV_SYMM_C(zynum_blas_gpu_csymm_device, float, "csymm_device", false)
+ZB_DEV_SYMM_C(zynum_blas_gpu_zhemm_device, double, "zhemm_device", true)
+ZB_DEV_SYMM_C(zynum_blas_gpu_chemm_device, float, "chemm_device", true)
+#undef ZB_DEV_SYMM_C
+
+int zynum_blas_gpu_ztrmm_device(char side, char uplo, char transa, char diag, int m, int n, const double* alpha,
+                                const double* a, int lda, double* b, int ldb, void* stream) {
+    return device_trsm<cnum<double>>("ztrmm_device", side, uplo, transa, diag, m, n, cnum<double>(alpha[0], alpha[1]),
+                                     reinterpret_cast<const cnum<double>*>(a), lda, reinterpret_cast<cnum<double>*>(b),
+                                     ldb, stream, true);
+}
+int zynum_blas_gpu_ctrmm_device(char side, char uplo, char transa, char diag, int m, int n, const float* alpha,
+                                const float* a, int lda, float* b, int ldb, void* stream) {
+    return device_trsm<cnum<float>>("ctrmm_device", side, uplo, transa, diag, m, n, cnum<float>(alpha[0], alpha[1]),
+                                    reinterpret_cast<const cnum<float>*>(a), lda, reinterpret_cast<cnum<float>*>(b),
+                                    ldb, stream, true);
+}
+
+#define ZB_DEV_SYR2K_C(NAME, R, WHAT)                                                                              \
+    int NAME(char uplo, char trans, int n, int k, const R* alpha, const R* a, int lda, const R* b, int ldb,        \
+             const R* beta, R* c, int ldc, void* stream) {                                                         \
+        return device_rank2k_c<R>(WHAT, uplo, trans, n, k, cnum<R>(alpha[0], alpha[1]),                            \
+                                  reinterpret_cast<const cnum<R>*>(a), lda, reinterpret_cast<const cnum<R>*>(b), ldb, \
+                                  cnum<R>(beta[0], beta[1]), reinterpret_cast<cnum<R>*>(c), ldc, stream, false, true); \
+    }
+ZB_DEV_SYR2K_C(zynum_blas_gpu_zsyr2k_device, double, "zsyr2k_device")
+ZB_DEV_SYR2K_C(zynum_blas_gpu_csyr2k_device, float, "csyr2k_device")
+#undef ZB_DEV_SYR2K_C
+
+#define ZB_DEV_HER2K(NAME, R, WHAT)                                                                                \
+    int NAME(char uplo, char trans, int n, int k, const R* alpha, const R* a, int lda, const R* b, int ldb,        \
+             R beta, R* c, int ldc, void* stream) {                                                                \
+        return device_rank2k_c<R>(WHAT, uplo, trans, n, k, cnum<R>(alpha[0], alpha[1]),                            \
+                                  reinterpret_cast<const cnum<R>*>(a), lda, reinterpret_cast<const cnum<R>*>(b), ldb, \
+                                  cnum<R>(beta), reinterpret_cast<cnum<R>*>(c), ldc, stream, true, true);          \
+    }
+ZB_DEV_HER2K(zynum_blas_gpu_zher2k_device, double, "zher2k_device")
+ZB_DEV_HER2K(zynum_blas_gpu_cher2k_device, float, "cher2k_device")
+#undef ZB_DEV_HER2K
+
+#define ZB_DEV_HERK(NAME, R, WHAT)                                                                                   \
+    int NAME(char uplo, char trans, int n, int k, R alpha, const R* a, int lda, R beta, R* c, int ldc,             \
+             void* stream) {                                                                                       \
+        return device_rank2k_c<R>(WHAT, uplo, trans, n, k, cnum<R>(alpha), reinterpret_cast<const cnum<R>*>(a), lda, \
+                                  nullptr, 0, cnum<R>(beta), reinterpret_cast<cnum<R>*>(c), ldc, stream, true, false); \
+    }
+ZB_DEV_HERK(zynum_blas_gpu_zherk_device, double, "zherk_device")
+ZB_DEV_HERK(zynum_blas_gpu_cherk_device, float, "cherk_device")
+#undef ZB_DEV_HERK
 
 // GEMM restricted to one triangle of C (the "gemmt" extension): only elements
 // with row <= col (uplo 'U') or row >= col ('L') are computed and written.
