@@ -304,3 +304,30 @@ def test_sgemm_bf16x3(blas, oracle, ta, tb):
     err = np.abs(c[:m, :n] - exact)
     assert np.all(err <= bound), float((err / bound).max())
     assert np.array_equal(c[m:], c0[m:])
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
+def test_host_panels_reuse_a_residues_bit_identical(blas, ta, tb):
+    """dgemm_ with host buffers large enough for column panels (here 4, the last one ragged)
+    computes op(A)'s CRT residues once and reuses them for every panel: the result is
+    bit-identical to the unpanelled device-pointer call on the same data."""
+    import torch
+    m, n, k = 600, 4100, 3400
+    rng = np.random.default_rng(17 + ord(ta))
+    ar, ac = (m, k) if ta == "N" else (k, m)
+    br, bc = (k, n) if tb == "N" else (n, k)
+    a = np.asfortranarray(rng.uniform(-1, 1, (ar, ac)) * 10.0 ** rng.uniform(-2, 2, (ar, ac)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (br, bc)))
+    c = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    old = blas.set_dgemm_method(blas.METHOD_OZAKI)
+    try:
+        dev = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda")  # noqa: E731
+        C = dev(c)
+        blas.dgemm_device(ta, tb, m, n, k, 1.25, dev(a), ar, dev(b), br, -0.5, C, m)
+        torch.cuda.synchronize()
+        want = np.asfortranarray(C.cpu().numpy().T)
+        got = c.copy(order="F")
+        blas.dgemm(ta, tb, m, n, k, 1.25, a, ar, b, br, -0.5, got, m)
+    finally:
+        blas.set_dgemm_method(old)
+    assert np.array_equal(got, want)

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/zynum_blas_gpu.h"
@@ -145,7 +146,7 @@ size_t real_scratch_bytes(int m, int n, int k, float*);
 
 int host_panel_count(int m, int n, int k) {
     if (n < 2048 || 2.0 * m * (double)n * k < kPanelMinFlops) return 1;
-    return std::min(8, std::max(2, n / 2048));
+    return std::min(8, std::max(2, n / 1024));
 }
 
 template <typename T>
@@ -190,14 +191,34 @@ void host_gemm_panels(const char* routine, Context& cx, int panels, char ta, cha
                                   (size_t)m * es, w, cudaMemcpyHostToDevice, up);
         if (e == cudaSuccess) e = cudaEventRecord(ev[2 * j], up);
     }
-    // products
+    // products.  FP64 through the CRT Ozaki scheme: one plan for the full panel width,
+    // op(A)'s residues computed by the first panel and reused by the others (its row
+    // scaling depends on op(A) alone, each column of op(B) is scaled independently, so
+    // the result equals the unpanelled product's)
+    bool crt = false;
+    OzakiPlan op{};
+    if constexpr (std::is_same<T, double>::value) {
+        int method = cx.dgemm_method;
+        if (method == METHOD_AUTO) method = ozaki_preferred(m, nb, k) ? METHOD_OZAKI : METHOD_NATIVE;
+        if (method == METHOD_OZAKI && k > 0 && alpha != 0.0) {
+            op = plan_ozaki(m, nb, k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
+            crt = op.scheme == OZAKI_CRT;
+        }
+    }
+    void* ows = nullptr;
+    if (crt && e == cudaSuccess) e = HostScratch{&cx}(ozaki_workspace_bytes(op), st, &ows);
     for (int j = 0; j < panels && e == cudaSuccess; ++j) {
         const int j0 = j * nb, w = std::min(nb, n - j0);
         e = cudaStreamWaitEvent(st, ev[2 * j], 0);
         if (e != cudaSuccess) break;
         const T* bj = (tb == 'N') ? db + (long)j0 * rb : db + j0;
         GemmArgs<T> g{ta, tb, m, w, k, alpha, da, ra, bj, rb, beta, dc + (long)j0 * m, m};
-        if ((e = run_gemm(g, st, HostScratch{&cx})) == cudaSuccess) e = cudaEventRecord(ev[2 * j + 1], st);
+        if constexpr (std::is_same<T, double>::value) {
+            e = crt ? dgemm_ozaki(g, op, ows, st, j > 0) : run_gemm(g, st, HostScratch{&cx});
+        } else {
+            e = run_gemm(g, st, HostScratch{&cx});
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * j + 1], st);
     }
     if (e != cudaSuccess) {  // nothing of C was written yet
         release();

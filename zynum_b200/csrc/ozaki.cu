@@ -1550,7 +1550,7 @@ const CrtHost& crt_host(int nmod) {
 
 std::atomic<int> g_last_moduli{0};
 
-cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st) {
+cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready) {
     const Layout L = ozaki_layout(p);
     uint8_t* w = static_cast<uint8_t*>(ws);
     int8_t* a_planes = reinterpret_cast<int8_t*>(w + L.a_planes_off);
@@ -1569,9 +1569,13 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
 
     View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
-    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);
+    // a_ready: A's statistics, exponents and planes stay; only B's accumulators and the status are cleared
+    cudaError_t e = a_ready ? cudaMemsetAsync(w + L.maxb_off, 0, L.suma_off - L.maxb_off, st)
+                            : cudaMemsetAsync(w, 0, L.stats_end, st);
+    if (e == cudaSuccess && a_ready) e = cudaMemsetAsync(w + L.sumb_off, 0, L.expa_off - L.sumb_off, st);
+    if (e == cudaSuccess && a_ready) e = cudaMemsetAsync(w + L.status_off, 0, L.stats_end - L.status_off, st);
     if (e != cudaSuccess) return e;
-    for (int side = 0; side < 2; ++side) {
+    for (int side = a_ready ? 1 : 0; side < 2; ++side) {
         const View& v = side ? vb : va;
         if (v.rs == 1) {
             dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
@@ -1582,7 +1586,7 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
         }
         count_launch();
     }
-    for (int side = 0; side < 2; ++side) {
+    for (int side = a_ready ? 1 : 0; side < 2; ++side) {
         const View& v = side ? vb : va;
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
@@ -1649,8 +1653,9 @@ int ozaki_crt_bits(int moduli) {
 }
 int ozaki_last_moduli() { return g_last_moduli.load(); }
 
-cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, cudaStream_t st) {
-    if (plan.scheme == OZAKI_CRT) return dgemm_ozaki_crt(g, plan, ws, st);
+cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, cudaStream_t st, bool a_ready) {
+    if (plan.scheme == OZAKI_CRT) return dgemm_ozaki_crt(g, plan, ws, st, a_ready);
+    // the slice scheme (its slice count depends on both operands) always recomputes op(A)
     OzakiPlan p = plan;
     const Layout L = ozaki_layout(p);
     uint8_t* w = static_cast<uint8_t*>(ws);
@@ -1669,7 +1674,7 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
 
-    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);
+    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);  // the slice scheme recomputes both operands
     if (e != cudaSuccess) return e;
     for (int side = 0; side < 2; ++side) {
         const View& v = side ? vb : va;

@@ -52,8 +52,11 @@ int ozaki_auto_slices(float spread_a, float spread_b);
 int ozaki_last_slices();
 size_t ozaki_workspace_bytes(const OzakiPlan& p);
 // C = alpha op(A) op(B) + beta C through INT8 slice or residue products; `ws` holds
-// ozaki_workspace_bytes(p) bytes of device scratch.
-cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st);
+// ozaki_workspace_bytes(p) bytes of device scratch.  a_ready (CRT scheme only):
+// op(A)'s row statistics, exponents and residue planes are already in `ws` from an
+// earlier call on the same op(A), plan and workspace (column panels of one product);
+// they are reused, not recomputed.  The plan may cover more columns than g.n.
+cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready = false);
 
 size_t bf16x3_workspace_bytes(int m, int n, int k);
 // C = alpha op(A) op(B) + beta C as a 3xBF16 split product with FP32 accumulation.
