@@ -46,6 +46,23 @@ KNOWN = {
         "source": "test/api/zynum_test.zig:28-41",
         "c": [76, 100, 103, 136],
     },
+    # test/abi/fortran_compat_test.zig:1676-1800 "level3 symmetric hermitian rank-k and triangular
+    # fallbacks": 2 x 2 problems, ld 2, side L, uplo U, trans N, alpha 1, beta 0 (complex values as
+    # [re, im]; C entries outside the updated triangle keep their sentinel)
+    "level3_known_answers": {
+        "source": "test/abi/fortran_compat_test.zig:1676-1800",
+        "dsymm": {"a": [1, 777, 2, 3], "b": [4, 6, 5, 7], "c": [16, 26, 19, 31]},
+        "zhemm": {"a": [[1, 99], [777, 777], [2, 1], [3, -7]], "b": [[1, 0], [0, 0], [0, 0], [1, 0]],
+                  "c": [[1, 0], [2, -1], [2, 1], [3, 0]]},
+        "dsyrk": {"a": [1, 3, 2, 4], "c0": [0, 777, 0, 0], "c": [5, 777, 11, 25]},
+        "zherk": {"a": [[1, 1], [3, 0], [2, 0], [-1, 1]], "c0": [[0, 0], [777, 777], [0, 0], [0, 0]],
+                  "c": [[6, 0], [777, 777], [1, 1], [11, 0]]},
+        "dsyr2k": {"a": [1, 3, 2, 4], "b": [5, 7, 6, 8], "c0": [0, 777, 0, 0], "c": [34, 777, 62, 106]},
+        "zher2k": {"a": [[1, 0], [3, 0], [2, 0], [4, 0]], "b": [[5, 0], [7, 0], [6, 0], [8, 0]],
+                   "c0": [[0, 0], [777, 777], [0, 0], [0, 0]], "c": [[34, 0], [777, 777], [62, 0], [106, 0]]},
+        "dtrmm": {"a": [1, 777, 2, 3], "b": [4, 6, 5, 7], "b_out": [16, 18, 19, 21]},
+        "dtrsm": {"a": [1, 777, 2, 3], "b": [16, 18, 19, 21], "b_out": [4, 6, 5, 7]},
+    },
     # tolerances the reference's tests use (gemm_registry_test.zig:198-202,
     # fortran_compat_test.zig:371/406, gemm_sweep.zig:247-258)
     "tolerances": {

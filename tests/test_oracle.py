@@ -239,3 +239,41 @@ def test_complex_syr2k_her2k(oracle, uplo, trans, herm):
     mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
     np.testing.assert_allclose(c[:n, :n][mask], full[mask], rtol=1e-12, atol=1e-12)
     assert np.array_equal(c[:n, :n][~mask], c0[:n, :n][~mask])
+
+
+def _lv(vals, dtype=np.float64):
+    """2 x 2 column-major array from the reference's flat lists ([re, im] pairs for complex)."""
+    if isinstance(vals[0], list):
+        vals = [complex(re, im) for re, im in vals]
+        dtype = np.complex128
+    return np.asfortranarray(np.array(vals, dtype=dtype).reshape(2, 2).T)
+
+
+def test_level3_known_answers(oracle):
+    """The oracle's SYMM / HEMM / SYRK / HERK / SYR2K / HER2K / TRMM / TRSM restatements reproduce
+    the reference's own 2 x 2 known answers (side L, uplo U, trans N, alpha 1, beta 0)."""
+    g = GOLDEN["level3_known_answers"]
+    c = np.zeros((2, 2), order="F")
+    oracle.symm("L", "U", 2, 2, 1.0, _lv(g["dsymm"]["a"]), 2, _lv(g["dsymm"]["b"]), 2, 0.0, c, 2)
+    assert np.array_equal(c, _lv(g["dsymm"]["c"]))
+    c = np.zeros((2, 2), np.complex128, order="F")
+    oracle.symm("L", "U", 2, 2, 1.0, _lv(g["zhemm"]["a"]), 2, _lv(g["zhemm"]["b"]), 2, 0.0, c, 2, herm=True)
+    assert np.array_equal(c, _lv(g["zhemm"]["c"]))
+    c = _lv(g["dsyrk"]["c0"])
+    oracle.syrk("U", "N", 2, 2, 1.0, _lv(g["dsyrk"]["a"]), 2, 0.0, c, 2)
+    assert np.array_equal(c, _lv(g["dsyrk"]["c"]))
+    c = _lv(g["zherk"]["c0"])
+    oracle.herk("U", "N", 2, 2, 1.0, _lv(g["zherk"]["a"]), 2, 0.0, c, 2)
+    assert np.array_equal(c, _lv(g["zherk"]["c"]))
+    c = _lv(g["dsyr2k"]["c0"])
+    oracle.syr2k("U", "N", 2, 2, 1.0, _lv(g["dsyr2k"]["a"]), 2, _lv(g["dsyr2k"]["b"]), 2, 0.0, c, 2)
+    assert np.array_equal(c, _lv(g["dsyr2k"]["c"]))
+    c = _lv(g["zher2k"]["c0"])
+    oracle.syr2k("U", "N", 2, 2, 1.0, _lv(g["zher2k"]["a"]), 2, _lv(g["zher2k"]["b"]), 2, 0.0, c, 2, herm=True)
+    assert np.array_equal(c, _lv(g["zher2k"]["c"]))
+    b = _lv(g["dtrmm"]["b"])
+    oracle.trmm("L", "U", "N", "N", 2, 2, 1.0, _lv(g["dtrmm"]["a"]), 2, b, 2)
+    assert np.array_equal(b, _lv(g["dtrmm"]["b_out"]))
+    b = _lv(g["dtrsm"]["b"])
+    oracle.trsm("L", "U", "N", "N", 2, 2, 1.0, _lv(g["dtrsm"]["a"]), 2, b, 2)
+    assert np.array_equal(b, _lv(g["dtrsm"]["b_out"]))
