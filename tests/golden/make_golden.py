@@ -63,6 +63,16 @@ KNOWN = {
         "dtrmm": {"a": [1, 777, 2, 3], "b": [4, 6, 5, 7], "b_out": [16, 18, 19, 21]},
         "dtrsm": {"a": [1, 777, 2, 3], "b": [16, 18, 19, 21], "b_out": [4, 6, 5, 7]},
     },
+    # test/abi/cblas_compat_test.zig:596-658 "cblas row-major level3 triangular and rank2k wrappers":
+    # row-major 2 x 2 buffers (ld 2), side L, uplo U, trans N, alpha 1, beta 0
+    "cblas_level3_row_major": {
+        "source": "test/abi/cblas_compat_test.zig:596-658",
+        "dtrmm": {"a": [1, 2, 777, 3], "b": [4, 5, 6, 7], "b_out": [16, 19, 18, 21]},
+        "dtrsm": {"a": [1, 2, 777, 3], "b": [16, 19, 18, 21], "b_out": [4, 5, 6, 7]},
+        "dsyr2k": {"a": [1, 2, 3, 4], "b": [5, 6, 7, 8], "c0": [0, 0, 777, 0], "c": [34, 62, 777, 106]},
+        "zher2k": {"a": [[1, 0], [2, 0], [3, 0], [4, 0]], "b": [[5, 0], [6, 0], [7, 0], [8, 0]],
+                   "c0": [[0, 0], [0, 0], [777, 7], [0, 0]], "c": [[34, 0], [62, 0], [777, 7], [106, 0]]},
+    },
     # tolerances the reference's tests use (gemm_registry_test.zig:198-202,
     # fortran_compat_test.zig:371/406, gemm_sweep.zig:247-258)
     "tolerances": {

@@ -51,3 +51,29 @@ def test_level3_known_answers_fortran_abi(blas):
     b = _lv(g["dtrsm"]["b"])
     blas.trsm("L", "U", "N", "N", 2, 2, 1.0, _lv(g["dtrsm"]["a"]), 2, b, 2)
     _close(b, _lv(g["dtrsm"]["b_out"]))
+
+
+def _rm(vals):
+    """Row-major 2 x 2 buffer (C-contiguous) from the reference's flat list."""
+    if isinstance(vals[0], list):
+        return np.ascontiguousarray(np.array([complex(r, i) for r, i in vals], np.complex128).reshape(2, 2))
+    return np.ascontiguousarray(np.array(vals, np.float64).reshape(2, 2))
+
+
+def test_cblas_row_major_level3_known_answers(blas):
+    """cblas_dtrmm / cblas_dtrsm / cblas_dsyr2k / cblas_zher2k in row-major layout reproduce the
+    reference's answers (test/abi/cblas_compat_test.zig:596-658), the untouched triangle included."""
+    g = json.loads((Path(__file__).parent / "golden" / "known_answers.json").read_text())["cblas_level3_row_major"]
+    R, L, U, N, NU = blas.CblasRowMajor, blas.CblasLeft, blas.CblasUpper, blas.CblasNoTrans, blas.CblasNonUnit
+    b = _rm(g["dtrmm"]["b"])
+    blas.cblas_trmm(R, L, U, N, NU, 2, 2, 1.0, _rm(g["dtrmm"]["a"]), 2, b, 2)
+    _close(b, _rm(g["dtrmm"]["b_out"]))
+    b = _rm(g["dtrsm"]["b"])
+    blas.cblas_dtrsm(R, L, U, N, NU, 2, 2, 1.0, _rm(g["dtrsm"]["a"]), 2, b, 2)
+    _close(b, _rm(g["dtrsm"]["b_out"]))
+    c = _rm(g["dsyr2k"]["c0"])
+    blas.cblas_syr2k(R, U, N, 2, 2, 1.0, _rm(g["dsyr2k"]["a"]), 2, _rm(g["dsyr2k"]["b"]), 2, 0.0, c, 2)
+    _close(c, _rm(g["dsyr2k"]["c"]))
+    c = _rm(g["zher2k"]["c0"])
+    blas.cblas_syr2k_c(R, U, N, 2, 2, 1.0, _rm(g["zher2k"]["a"]), 2, _rm(g["zher2k"]["b"]), 2, 0.0, c, 2, herm=True)
+    _close(c, _rm(g["zher2k"]["c"]))
