@@ -277,3 +277,12 @@ def test_level3_known_answers(oracle):
     b = _lv(g["dtrsm"]["b"])
     oracle.trsm("L", "U", "N", "N", 2, 2, 1.0, _lv(g["dtrsm"]["a"]), 2, b, 2)
     assert np.array_equal(b, _lv(g["dtrsm"]["b_out"]))
+
+
+def test_golden_file_is_current():
+    """tests/golden/known_answers.json is what tests/golden/make_golden.py writes."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", Path(__file__).parent / "golden" / "make_golden.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert json.loads(json.dumps(mod.KNOWN)) == GOLDEN, "rerun tests/golden/make_golden.py"
