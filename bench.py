@@ -34,6 +34,7 @@ sys.path.insert(0, str(ROOT))
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12  # 64 DFMA/clk/SM at the 1965 MHz max clock
+FP32_NOMINAL_TFLOPS = 148 * 256 * 1.965e9 / 1e12  # 128 FFMA/clk/SM at the 1965 MHz max clock
 METRIC = "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error; batch GFLOP/s"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel on the
 # 8192^3 headline workload, from one-pass ncu captures of this script's default run:
@@ -252,8 +253,15 @@ def bench_batched(torch, blas, steps, warmup, seed=7, count=20000, tcount=5000, 
         plan_s = time.perf_counter() - t0
         run = lambda: batch.run(1.0, pa, la, pb, lb, 0.0, pc, la, use_graph=True)  # noqa: E731
         ms = time_device(torch, run, steps, warmup, torch.cuda.current_stream())
-        out[name] = {"problems": count, "gflop": flops / 1e9, "ms": ms, "gflops": flops / (ms * 1e-3) / 1e9,
-                     "plan_and_tune_s": plan_s, **batch.info()}
+        gf = flops / (ms * 1e-3) / 1e9
+        peak = FP64_NOMINAL_TFLOPS if name == "dgemm" else FP32_NOMINAL_TFLOPS
+        out[name] = {"problems": count, "gflop": flops / 1e9, "ms": ms, "gflops": gf,
+                     "plan_and_tune_s": plan_s, **batch.info(),
+                     "roofline": {"bound": "tensor" if name == "dgemm" else "fp32 fma", "achieved": gf / 1e3,
+                                  "peak": peak, "unit": "TFLOP/s", "frac": gf / 1e3 / peak,
+                                  "peak_source": ("nominal FP64 DMMA pipe, 148 SMs x 128 flop/clk x 1.965 GHz"
+                                                  if name == "dgemm" else
+                                                  "nominal FP32 FFMA, 148 SMs x 256 flop/clk x 1.965 GHz")}}
         batch.close()
         del A, B, Cb
     if "dtrsm" not in which:
@@ -276,8 +284,12 @@ def bench_batched(torch, blas, steps, warmup, seed=7, count=20000, tcount=5000, 
     batch = blas.TrsmBatch(tn, tr, dtype="f64", uplo="L")
     run = lambda: batch.run(1.0, pa, la, pb, la, use_graph=True)  # noqa: E731
     ms = time_device(torch, run, steps, warmup, torch.cuda.current_stream())
-    out["dtrsm"] = {"problems": tcount, "gflop": tflops / 1e9, "ms": ms, "gflops": tflops / (ms * 1e-3) / 1e9,
-                    "note": "GFLOP = sum n^2 * nrhs", **batch.info()}
+    gf = tflops / (ms * 1e-3) / 1e9
+    out["dtrsm"] = {"problems": tcount, "gflop": tflops / 1e9, "ms": ms, "gflops": gf,
+                    "note": "GFLOP = sum n^2 * nrhs", **batch.info(),
+                    "roofline": {"bound": "tensor", "achieved": gf / 1e3, "peak": FP64_NOMINAL_TFLOPS,
+                                 "unit": "TFLOP/s", "frac": gf / 1e3 / FP64_NOMINAL_TFLOPS,
+                                 "peak_source": "nominal FP64 DMMA pipe (substitution steps are latency-bound)"}}
     batch.close()
     return out
 
@@ -305,8 +317,12 @@ def bench_differentiation(torch, steps, warmup, n=4096, r=512, seed=11):
     # nominal flops: forward TRSM n^2 r + SYRK r(r+1)n; backward TRSM (dB) n^2 r + recompute n^2 r
     # + dL = -tril(dB X^T) n^2 r + dX = X (G + G^T) 4 n r^2
     gflop = (3 * n * n * r + n * n * r + r * (r + 1) * n + 4 * n * r * r) / 1e9
-    return {"n": n, "nrhs": r, "ms_fwd_bwd": ms, "gflop_nominal": gflop, "gflops": gflop / (ms * 1e-3),
-            "recompute": True, "dgemm_method": "native FP64"}
+    gf = gflop / (ms * 1e-3)
+    return {"n": n, "nrhs": r, "ms_fwd_bwd": ms, "gflop_nominal": gflop, "gflops": gf,
+            "recompute": True, "dgemm_method": "native FP64",
+            "roofline": {"bound": "tensor", "achieved": gf / 1e3, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                         "frac": gf / 1e3 / FP64_NOMINAL_TFLOPS,
+                         "peak_source": "nominal FP64 DMMA pipe; the chain's TRSM steps are latency-bound"}}
 
 
 # ---------------------------------------------------------------- our arm
@@ -322,6 +338,51 @@ def time_device(torch, fn, steps, warmup, stream):
     ev1.record(stream)
     ev1.synchronize()
     return ev0.elapsed_time(ev1) / steps
+
+
+def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
+    """The rest of the precision configuration on the headline size: DGEMM with
+    entries u * 10^e, e ~ U[-phi, phi], for phi = 4 and 8, Ozaki and native on the
+    same inputs; SGEMM as a 3xBF16 split product and native FP32 on U[-1, 1] data.
+    Each: time per call (CUDA events, inputs resident) and max / median relative
+    error against the double-double oracle on 2048 sampled entries."""
+    dev = torch.device("cuda")
+    flop = 2.0 * n ** 3
+    out = {}
+    for phi in (4.0, 8.0):
+        A, B = make_inputs(torch, n, phi, seed, dev)
+        C = torch.zeros((n, n), dtype=torch.float64, device=dev)
+        a_h = np.asfortranarray(A.cpu().numpy().T)
+        b_h = np.asfortranarray(B.cpu().numpy().T)
+        for name, mid in (("ozaki", blas.METHOD_OZAKI), ("native", blas.METHOD_NATIVE)):
+            blas.set_dgemm_method(mid)
+            fn = lambda: blas.dgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
+            ms = time_device(torch, fn, steps, warmup, stream)
+            fn()
+            torch.cuda.synchronize()
+            err = sampled_error(orc, a_h, b_h, np.asfortranarray(C.cpu().numpy().T), n)
+            out[f"{name}_phi{int(phi)}"] = {"phi": phi, "ms": ms, "tflops": flop / (ms * 1e-3) / 1e12,
+                                            "error": err}
+        del A, B, C
+    blas.set_dgemm_method(blas.METHOD_NATIVE)
+    g = torch.Generator(device=dev).manual_seed(seed + 99)
+    A = torch.rand((n, n), generator=g, device=dev, dtype=torch.float32) * 2 - 1
+    B = torch.rand((n, n), generator=g, device=dev, dtype=torch.float32) * 2 - 1
+    C = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    a_h = np.asfortranarray(A.cpu().numpy().T.astype(np.float64))
+    b_h = np.asfortranarray(B.cpu().numpy().T.astype(np.float64))
+    for name, mid in (("sgemm_bf16x3", blas.SMETHOD_BF16X3), ("sgemm_native", blas.SMETHOD_NATIVE)):
+        blas.set_sgemm_method(mid)
+        fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
+        ms = time_device(torch, fn, steps, warmup, stream)
+        fn()
+        torch.cuda.synchronize()
+        err = sampled_error(orc, a_h, b_h, np.asfortranarray(C.cpu().numpy().T.astype(np.float64)), n)
+        out[name] = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12, "error": err,
+                     "data": "U[-1,1] float32"}
+    blas.set_sgemm_method(blas.SMETHOD_NATIVE)
+    del A, B, C
+    return out
 
 
 def _ozaki_desc(n):
@@ -380,8 +441,8 @@ def run_ours(args, rank, world, local_rank):
                 t = torch.tensor([ms], device=dev)
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 ms = float(t.item())
-            results[name] = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12, "launches_per_step": int(launches),
-                             "kernel_ms": kern_ms, "window": (t_begin, t_end)}
+            results[name] = {"phi": args.phi, "ms": ms, "tflops": flop / (ms * 1e-3) / 1e12,
+                             "launches_per_step": int(launches), "kernel_ms": kern_ms, "window": (t_begin, t_end)}
         time.sleep(0.1)  # the sampler's last lines cover the end of the timed region
     clk = clocks.summary(results[methods[0][0]]["window"])
     for name in results:
@@ -467,6 +528,13 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8,
                 "path": "dgemm_ Fortran ABI, pinned host buffers"},
     }
+    if not args.no_precision and not args.no_error and head[0] == "ozaki" and len(methods) == 2:
+        from oracle import oracle as orc
+        extra = precision_methods(torch, blas, orc, n, max(3, min(args.steps, 10)), max(3, args.warmup), stream,
+                                  1234 + rank)
+        line["methods"].update(extra)
+        line["config"]["precision"] = ("methods: ozaki / native at phi = 0 (headline), 4, 8 on the same inputs per "
+                                       "phi; sgemm_bf16x3 / sgemm_native on U[-1,1]; errors vs double-double")
     if not args.no_batched:
         line["batched"] = bench_batched(torch, blas, max(3, args.steps), args.warmup)
         line["differentiation"] = bench_differentiation(torch, max(3, args.steps), args.warmup)
@@ -706,6 +774,44 @@ def suite_batched(args):
     return 0
 
 
+def suite_one(args):
+    """One GEMM shape, for profiling a single kernel: --dtype f64|f32|z|c, --m/--n/--k,
+    --method (native or ozaki for f64; ozaki means 3xBF16 for f32), beta 0, NN,
+    column-major U[-1,1] inputs; `--warmup` untimed calls, then `--steps` timed ones."""
+    import torch
+    from zynum_b200 import blas
+    m, n, k = args.m, args.n, args.k
+    dt = args.dtype
+    tdt = {"f64": torch.float64, "f32": torch.float32, "z": torch.complex128, "c": torch.complex64}[dt]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    real = torch.float64 if dt in ("f64", "z") else torch.float32
+
+    def rnd(rows, cols):
+        x = torch.rand((cols, rows), generator=g, device="cuda", dtype=real) * 2 - 1
+        if dt in ("z", "c"):
+            x = torch.complex(x, torch.rand((cols, rows), generator=g, device="cuda", dtype=real) * 2 - 1)
+        return x
+
+    A, B = rnd(m, k), rnd(k, n)
+    C = torch.zeros((n, m), device="cuda", dtype=tdt)
+    if dt == "f64":
+        blas.set_dgemm_method(blas.METHOD_OZAKI if args.method == "ozaki" else blas.METHOD_NATIVE)
+        fn = lambda: blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+    elif dt == "f32":
+        blas.set_sgemm_method(blas.SMETHOD_BF16X3 if args.method == "ozaki" else blas.SMETHOD_NATIVE)
+        fn = lambda: blas.sgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+    else:
+        f = blas.zgemm_device if dt == "z" else blas.cgemm_device
+        fn = lambda: f("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+    ms = time_device(torch, fn, args.steps, args.warmup, torch.cuda.current_stream())
+    flop = (8.0 if dt in ("z", "c") else 2.0) * m * n * k
+    esz = C.element_size()
+    byts = esz * (m * k + k * n + m * n)
+    print(json.dumps({"suite": "one", "dtype": dt, "m": m, "n": n, "k": k, "method": args.method, "ms": ms,
+                      "tflops": flop / (ms * 1e-3) / 1e12, "gbs": byts / (ms * 1e-3) / 1e9}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -718,7 +824,12 @@ def main(argv=None):
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched"],
+    ap.add_argument("--no-precision", action="store_true", help="skip the phi = 4 / 8 and SGEMM methods")
+    ap.add_argument("--dtype", choices=["f64", "f32", "z", "c"], default="f64", help="suite one: element type")
+    ap.add_argument("--m", type=int, default=4096, help="suite one: rows of C")
+    ap.add_argument("--n", type=int, default=4096, help="suite one: columns of C")
+    ap.add_argument("--k", type=int, default=4096, help="suite one: inner dimension")
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched", "one"],
                     default="headline", help="secondary measurement suites (one JSON line each)")
     ap.add_argument("--batch-count", type=int, default=20000,
                     help="batched suite: GEMM problems per batch (TRSM problems: a quarter)")
@@ -749,6 +860,8 @@ def main(argv=None):
             return suite_level3(args)
         if args.suite == "batched":
             return suite_batched(args)
+        if args.suite == "one":
+            return suite_one(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -259,14 +259,19 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_sgemm_device(char transa, char transb, int
  * code whose device memory belongs to its own pool allocator, or latency-
  * critical loops where cudaMalloc/cudaFree would synchronise the device.
  * Same arguments and result as zynum_blas_gpu_dgemm_device with the native
- * method; `splits` > 0 forces that many split-K ranges, 0 lets the planner
- * choose.  Split-K partial sums go to a fixed 32 MiB device array inside the
- * library (held on every GPU that loads it until exit), so
- * splits * m * n must not exceed 4194304; larger requests are rejected with a
- * negative status and a message in zynum_blas_gpu_last_error().  The first
- * call on a device looks up that array's device address (make that first call
- * before any stream capture).  All calls share the one array: calls that
- * overlap on the GPU (other streams, other threads) race on it. */
+ * method (the Ozaki method setting does not apply here); `splits` > 0 forces
+ * that many split-K ranges (at most 64), 0 lets the planner choose.  Split-K
+ * partial sums go to a fixed 32 MiB device array inside the library, so the
+ * partial sums of the K ranges the call really uses (splits * m * n; none on
+ * the tall-skinny route) must not exceed 4194304 doubles; larger requests are
+ * rejected with a negative status and a message in zynum_blas_gpu_last_error().
+ * The array's memory is committed on a GPU when the library's module for it
+ * loads there: with CUDA's lazy module loading (the default) that is the
+ * first call on that GPU, which also looks up the array's device address and
+ * checks that the GPU is an sm_100 part.  So make one call per GPU before
+ * reserving a memory pool and before any stream capture; later calls on that
+ * GPU allocate nothing.  All calls share the one array: calls that overlap on
+ * the GPU (other streams, other threads) race on it. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_noalloc_device(char transa, char transb, int m, int n, int k, double alpha,
                                                            const double *a, int lda, const double *b, int ldb,
                                                            double beta, double *c, int ldc, int splits, void *stream);
@@ -448,9 +453,20 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_ozaki_plan(int m, int n, int k, int *slice
 /* Text of the last error seen by this thread ("" if none). */
 ZYNUM_BLAS_GPU_API const char *zynum_blas_gpu_last_error(void);
 /* Host-side fault injection for tests: the next `count` device-memory
- * reservations fail (kind 1), or the next stream synchronisation reports
- * CUDA error `count` (kind 2).  Never touches the GPU. */
+ * reservations fail (kind 1), the next stream synchronisation reports
+ * CUDA error `count` (kind 2), or the next `count` Ozaki DGEMM product
+ * kernels run with a hold (kind 3): their MMA issuer first waits on a
+ * barrier that nothing arrives on, with a 1 ms limit, so the kernel's
+ * bounded-wait abort path runs (no GPU fault, trap or hang is made).
+ * No reference counterpart (the reference has no GPU). */
 ZYNUM_BLAS_GPU_API void zynum_blas_gpu_inject_fault(int kind, int count);
+/* Synchronises `stream` and reports whether a tensor-core product kernel of
+ * this device abandoned its work because a bounded wait ran out since the
+ * last call: 0 if none, else -(cudaErrorLaunchTimeout) with the site in
+ * zynum_blas_gpu_last_error().  Such a CRT-scheme Ozaki call leaves C as it
+ * was.  Host entry points make this check themselves before copying C back.
+ * No reference counterpart (the reference has no GPU). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_device_status(void *stream);
 /* Dominant-kernel timing: enable != 0 starts recording CUDA events around the
  * main contraction kernel of every call (on the launching stream) and clears
  * earlier records; returns the previous state. */

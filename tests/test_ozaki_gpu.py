@@ -214,16 +214,92 @@ def test_crt_wide_dynamic_range(blas, oracle, phi):
     _crt_case(blas, oracle, "N", "T", 96, 80, 512, 96, 80, 96, 1.0, -1.0, rng, phi=phi)
 
 
-def test_crt_zero_rows_and_nonfinite(blas, oracle):
-    """A zero row of A gives exact zeros; an Inf in a row of A (column of B) gives NaN on that row (column)."""
+def _nonfinite_case(blas, oracle, scheme, ta, tb, m, n, k, ld, rng):
+    """Inf / NaN in single entries of op(A), op(B) and C, compared entry by entry
+    with the reference's loop (gemm.zig:1422-1429, the oracle): the same entries are
+    NaN, +Inf and -Inf, and every finite entry meets the scheme's bound."""
+    def store(rows, cols):
+        return np.asfortranarray(rng.uniform(-1, 1, (ld, cols)))
+    a = store(m if ta == "N" else k, k if ta == "N" else m)
+    b = store(k if tb == "N" else n, n if tb == "N" else k)
+    c = store(m, n)
+
+    def put_a(i, p, v):  # op(A)[i, p]
+        if ta == "N":
+            a[i, p] = v
+        else:
+            a[p, i] = v
+
+    def put_b(p, j, v):  # op(B)[p, j]
+        if tb == "N":
+            b[p, j] = v
+        else:
+            b[j, p] = v
+
+    put_a(5, 17, np.inf)        # row 5: +-Inf times B's column entries
+    put_b(17, 40, 0.0)          # ... Inf * 0 = NaN at C[5, 40]
+    put_a(9, 100, -np.inf)      # row 9
+    put_b(100, 41, np.nan)      # column 41 holds NaN: NaN down the column
+    put_a(700 % m, 3, np.nan)   # row 700: NaN across the row
+    put_b(64, 300 % n, np.inf)  # column 300: +-Inf down the column
+    put_a(9, 64, np.inf)        # C[9, 300] meets +Inf * +Inf and -Inf * B: NaN or Inf by sign
+    c[11, 12] = -np.inf         # beta * C: -Inf in an otherwise finite entry
+    c[5, 13] = np.nan           # beta * C: NaN in an already non-finite row
+    c0 = c.copy(order="F")
+    alpha, beta = 1.5, 0.5
+    blas.set_dgemm_method(blas.METHOD_OZAKI)
+    old_s = blas.set_ozaki_scheme(blas.OZAKI_CRT if scheme == "crt" else blas.OZAKI_SLICES)
+    old_n = blas.set_ozaki_slices(8 if scheme == "slices" else 0)
+    try:
+        blas.dgemm(ta, tb, m, n, k, alpha, a, ld, b, ld, beta, c, ld)
+    finally:
+        blas.set_ozaki_slices(old_n)
+        blas.set_ozaki_scheme(old_s)
+        blas.set_dgemm_method(blas.METHOD_NATIVE)
+    ref = c0.copy(order="F")
+    oracle.gemm(ta, tb, m, n, k, alpha, a, ld, b, ld, beta, ref, ld)
+    got, want = c[:m, :n], ref[:m, :n]
+    assert np.array_equal(np.isnan(got), np.isnan(want)), "NaN entries differ"
+    assert np.array_equal(np.isposinf(got), np.isposinf(want)), "+Inf entries differ"
+    assert np.array_equal(np.isneginf(got), np.isneginf(want)), "-Inf entries differ"
+    assert np.isnan(want).sum() > n and np.isinf(want).sum() > n  # the case really spreads non-finite values
+    fin = np.isfinite(want)
+    A = np.nan_to_num(np.abs(_op(a, ta, m, k)), nan=0.0, posinf=0.0)
+    B = np.nan_to_num(np.abs(_op(b, tb, k, n)), nan=0.0, posinf=0.0)
+    ab = A @ B
+    # finite entries lie in rows / columns free of Inf / NaN; the slice scheme (8 digits) and
+    # the CRT scheme both stay within 64 k u |A||B| + 4 u |beta C0| on U[-1, 1] data
+    bound = 64 * k * U64 * (abs(alpha) * ab) + 4 * U64 * abs(beta) * np.abs(np.nan_to_num(c0[:m, :n]))
+    err = np.abs(got[fin] - want[fin])
+    assert np.all(err <= bound[fin]), float((err / bound[fin]).max())
+    assert np.array_equal(c[m:], c0[m:]), "padding rows of C were written"
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+def test_crt_nonfinite_entries_match_reference_loop(blas, oracle, ta, tb):
+    """1024^3 with ld 1031 (CTA-pair kernel), Inf / NaN in single entries of A, B and C."""
+    _nonfinite_case(blas, oracle, "crt", ta, tb, 1024, 1024, 1024, 1031, np.random.default_rng(41))
+
+
+@pytest.mark.parametrize("shape", [(200, 320, 150), (1024, 333, 257)], ids=lambda s: "x".join(map(str, s)))
+def test_crt_nonfinite_one_and_two_cta(blas, oracle, shape):
+    m, n, k = shape
+    _nonfinite_case(blas, oracle, "crt", "N", "T", m, n, k, max(m, n, k) + 3, np.random.default_rng(m + n))
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
+def test_slices_nonfinite_entries_match_reference_loop(blas, oracle, ta, tb):
+    _nonfinite_case(blas, oracle, "slices", ta, tb, 1024, 512, 384, 1031, np.random.default_rng(43))
+
+
+def test_crt_zero_rows_give_exact_zeros(blas, oracle):
+    """A zero row of op(A) gives exact zeros in its row of C (beta = 0)."""
     rng = np.random.default_rng(9)
     m, n, k = 70, 40, 90
     a = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
     b = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
     a[3, :] = 0.0
-    a[5, 17] = np.inf
-    b[2, 9] = np.nan
-    c = np.zeros((m, n), order="F")
+    c = np.full((m, n), np.nan, order="F")
     blas.set_dgemm_method(blas.METHOD_OZAKI)
     old = blas.set_ozaki_scheme(blas.OZAKI_CRT)
     try:
@@ -231,17 +307,8 @@ def test_crt_zero_rows_and_nonfinite(blas, oracle):
     finally:
         blas.set_ozaki_scheme(old)
         blas.set_dgemm_method(blas.METHOD_NATIVE)
-    assert np.all(c[3, np.arange(n) != 9] == 0.0)
-    assert np.all(np.isnan(c[5, :])) and np.all(np.isnan(c[:, 9]))
-    rest = np.ones((m, n), bool)
-    rest[5, :] = False
-    rest[:, 9] = False
-    rest[3, :] = False
-    ref = a.copy()
-    ref[5, 17] = 0.0
-    refb = b.copy()
-    refb[2, 9] = 0.0
-    np.testing.assert_allclose(c[rest], (ref @ refb)[rest], rtol=1e-12, atol=1e-13)
+    assert np.all(c[3, :] == 0.0)
+    np.testing.assert_allclose(c, a @ b, rtol=1e-12, atol=1e-13)
 
 
 def test_crt_long_k_falls_back_to_slices(blas):

@@ -199,6 +199,8 @@ def _declare(L: C.CDLL) -> None:
     L.zynum_blas_gpu_last_error.restype = cp
     L.zynum_blas_gpu_inject_fault.argtypes = [i, i]
     L.zynum_blas_gpu_inject_fault.restype = None
+    L.zynum_blas_gpu_device_status.argtypes = [P]
+    L.zynum_blas_gpu_device_status.restype = i
     L.zynum_blas_gpu_profile.argtypes = [i]
     L.zynum_blas_gpu_profile.restype = i
     L.zynum_blas_gpu_profile_read.argtypes = [P, i]

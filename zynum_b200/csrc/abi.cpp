@@ -49,7 +49,12 @@ int gemm_error(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc)
 
 int cuda_status(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return 0;
-    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    const int site = e == cudaErrorLaunchTimeout ? take_wait_site() : 0;
+    if (site)
+        set_last_error(std::string(what) + ": a bounded wait in a tensor-core product kernel ran out (site " +
+                       std::to_string(site) + "); the product was abandoned and C was not written");
+    else
+        set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
     return -(int)e;
 }
 
@@ -93,6 +98,7 @@ cudaError_t run_dgemm(const GemmArgsF64& g, cudaStream_t st, Scratch scratch) {
     if (method == METHOD_AUTO) method = ozaki_preferred(g.m, g.n, g.k) ? METHOD_OZAKI : METHOD_NATIVE;
     if (method == METHOD_OZAKI) {
         OzakiPlan op = plan_ozaki(g.m, g.n, g.k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
+        op.hold = cx.faults.take_hold();
         void* ws = nullptr;
         cudaError_t e = scratch(ozaki_workspace_bytes(op), st, &ws);
         if (e != cudaSuccess) return e;
@@ -202,6 +208,7 @@ void host_gemm_panels(const char* routine, Context& cx, int panels, char ta, cha
         if (method == METHOD_AUTO) method = ozaki_preferred(m, nb, k) ? METHOD_OZAKI : METHOD_NATIVE;
         if (method == METHOD_OZAKI && k > 0 && alpha != 0.0) {
             op = plan_ozaki(m, nb, k, cx.ozaki_slices, cx.ozaki_scheme, cx.ozaki_moduli);
+            op.hold = cx.faults.take_hold();
             crt = op.scheme == OZAKI_CRT;
         }
     }
@@ -2011,6 +2018,21 @@ void zynum_blas_gpu_inject_fault(int kind, int count) {
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
     if (kind == 1) cx.faults.fail_next_reservations = count;
     if (kind == 2) cx.faults.fail_next_sync = count;
+    if (kind == 3) cx.faults.hold_next_products.store(count);
+}
+
+int zynum_blas_gpu_device_status(void* stream) {
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "device_status");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = check_wait_report(st);
+    return cuda_status(e, "device_status");
 }
 
 }  // extern "C"

@@ -22,6 +22,8 @@
 // Split-K (for K-dominant shapes, e.g. 256 x 256 x 262144) writes per-split
 // partial tiles to a workspace; dgemm_splitk_reduce sums them in split order
 // (deterministic) and applies alpha/beta.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -244,13 +246,7 @@ cudaError_t dispatch_layout(const GemmArgsF64& g, int vec, int splits, int k_chu
     return cudaErrorInvalidValue;
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int BK = kBK>
-cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chunk, double* workspace,
-                      cudaStream_t st) {
-    if (used_splits == 1) return dispatch_layout<BM, BN, WM, WN, STAGES, false, BK>(g, vec, 1, k_chunk, nullptr, st);
-    if (!workspace) return cudaErrorInvalidValue;
-    cudaError_t e = dispatch_layout<BM, BN, WM, WN, STAGES, true, BK>(g, vec, used_splits, k_chunk, workspace, st);
-    if (e != cudaSuccess) return e;
+cudaError_t splitk_reduce(const GemmArgsF64& g, int used_splits, double* workspace, cudaStream_t st) {
     long total = (long)g.m * g.n;
     int blocks = (int)((total + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
@@ -259,7 +255,36 @@ cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chun
     return cudaGetLastError();
 }
 
+template <int BM, int BN, int WM, int WN, int STAGES, int BK = kBK>
+cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chunk, double* workspace,
+                      cudaStream_t st) {
+    if (used_splits == 1) return dispatch_layout<BM, BN, WM, WN, STAGES, false, BK>(g, vec, 1, k_chunk, nullptr, st);
+    if (!workspace) return cudaErrorInvalidValue;
+    cudaError_t e = dispatch_layout<BM, BN, WM, WN, STAGES, true, BK>(g, vec, used_splits, k_chunk, workspace, st);
+    if (e != cudaSuccess) return e;
+    return splitk_reduce(g, used_splits, workspace, st);
+}
+
 }  // namespace
+
+// The 128 x 128 route takes the TMA kernel for operands TMA can describe when
+// ZYNUM_GPU_DGEMM_TMA=1 (otherwise the cp.async kernel).
+static bool use_tma_tiles(const GemmArgsF64& g, const GemmPlan& plan) {
+    static const bool enabled = [] {
+        const char* v = std::getenv("ZYNUM_GPU_DGEMM_TMA");
+        return v && v[0] == '1';
+    }();
+    return enabled && plan.tile == TILE_128x128 && dgemm_tma_applies(g);
+}
+
+int dgemm_native_used_splits(const GemmArgsF64& g, const GemmPlan& plan) {
+    const int splits = plan.splits < 1 ? 1 : plan.splits;
+    if (plan.tile == TILE_GEMV && gemv_applies(g.m, g.n, g.k, g.tri)) return gemv_used_splits(g.k, splits);
+    if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) return 1;
+    int k_chunk = use_tma_tiles(g, plan) ? dgemm_tma_k_chunk(g.k, splits) : (g.k + splits - 1) / splits;
+    k_chunk = (k_chunk + kBK - 1) / kBK * kBK;
+    return (g.k + k_chunk - 1) / k_chunk;
+}
 
 // Entry used by the planner: `tile` selects the block shape, `splits` > 1
 // requires a workspace of splits * m * n doubles.
@@ -283,6 +308,14 @@ cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* wor
         case TILE_64x64:  // few output tiles: 64 x 64 tiles, warps 2 x 2 of 32 x 32
             return run_tiles<64, 64, 32, 32, 4>(g, vec, used, k_chunk, workspace, st);
         default:
+            if (use_tma_tiles(g, plan)) {
+                const int kc = dgemm_tma_k_chunk(g.k, splits);
+                const int used_t = (g.k + kc - 1) / kc;
+                if (used_t > 1 && !workspace) return cudaErrorInvalidValue;
+                cudaError_t e = dgemm_tma(g, splits, workspace, st);
+                if (e != cudaSuccess || used_t == 1) return e;
+                return splitk_reduce(g, used_t, workspace, st);
+            }
             // op(B) k-contiguous (transb N): three 32-deep stages (212 KB), half the block
             // barriers of 16-deep slices (+2 % measured at 2048-8192); otherwise four 16-deep
             // stages (32-deep slices measured 1 % slower there)

@@ -344,6 +344,13 @@ int gemv_split_count(int rows, int k) {
     return (int)std::max<long>(1, sp);
 }
 
+int gemv_used_splits(int k, int splits) {
+    splits = std::max(1, splits);
+    int kchunk = (k + splits - 1) / splits;
+    kchunk = (kchunk + kGvChunk - 1) / kGvChunk * kGvChunk;
+    return (k + kchunk - 1) / kchunk;
+}
+
 cudaError_t dgemv_route(const GemmArgsF64& g, int splits, double* ws, cudaStream_t st) {
     return gemv_run<double>(g, splits, ws, st);
 }

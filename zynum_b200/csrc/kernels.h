@@ -58,6 +58,18 @@ inline size_t splitk_workspace_elems(int m, int n, int splits) {
 
 // ---------------------------------------------------------------- kernels
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st);
+// TMA-fed, warp-specialised 128 x 128 DGEMM tiles (gemm_f64_tma.cu): for
+// 16-byte aligned operands with even leading dimensions.  K is split into
+// ranges of dgemm_tma_k_chunk(k, splits) (a multiple of the 32-deep slice);
+// with more than one range the raw sums go to `workspace` (range z at
+// z * m * n, ld m) and the caller reduces them.
+bool dgemm_tma_applies(const GemmArgsF64& g);
+int dgemm_tma_k_chunk(int k, int splits);
+cudaError_t dgemm_tma(const GemmArgsF64& g, int splits, double* workspace, cudaStream_t st);
+// K ranges dgemm_native will actually use for this plan (1: no workspace); the
+// route (GEMV, tall-skinny, tiles) and the rounding of K slices can only lower
+// it below plan.splits.
+int dgemm_native_used_splits(const GemmArgsF64& g, const GemmPlan& plan);
 cudaError_t sgemm_native(const GemmArgsF32& g, const GemmPlan& plan, float* workspace, cudaStream_t st);
 // Workspace of sgemm_native in bytes: split-K partials plus, for large
 // products, an MN-contiguous copy of each K-contiguous operand.  The bound
@@ -75,6 +87,8 @@ bool gemv_applies(int m, int n, int k, int tri);
 constexpr long kGemvSplitTarget = 1L << 20;   // outputs x K splits the planner aims for
 constexpr long kGemvMaxPartials = 2L << 20;   // bound on splits * outputs (workspace elements)
 int gemv_split_count(int rows, int k);
+// K splits the GEMV kernels use when asked for `splits` (K slices are rounded up).
+int gemv_used_splits(int k, int splits);
 cudaError_t dgemv_route(const GemmArgsF64& g, int splits, double* ws, cudaStream_t st);
 cudaError_t sgemv_route(const GemmArgsF32& g, int splits, float* ws, cudaStream_t st);
 // Narrow route (n <= 16 with m >= 512, or m <= 16 with n >= 512; n, m > 1):
@@ -113,6 +127,9 @@ void prof_end(cudaStream_t st);
 // Fortran GEMM argument check (fortran.zig:88-102 gemmError): 0 or the index
 // of the first illegal argument.  trans characters must already be upper case.
 int gemm_arg_error(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc);
+
+// cuTensorMapEncodeTiled from the driver (nullptr if unavailable), looked up once.
+void* tensor_map_encoder();
 
 // ---------------------------------------------------------------- planner
 GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count);

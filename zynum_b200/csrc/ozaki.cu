@@ -41,6 +41,7 @@
 #include <cstdlib>
 #include <mutex>
 
+#include "bounded_wait.cuh"
 #include "common.cuh"
 #include "kernels.h"
 #include "ozaki.h"
@@ -95,20 +96,10 @@ struct UmmaParams {
     int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad] (row-major)
     long res_plane;
     int band_rows;     // EPI_RESIDUE on the CTA pair: tile-rows per raster band
+    int* report;       // per-device report word of bounded waits that ran out
+    unsigned long long wait_ns;  // time limit of every mbarrier wait
+    int hold;          // test-only: the MMA issuer first waits on a barrier nothing arrives on
 };
-
-// ------------------------------------------------------ bounded waiting
-// Wait for phase `parity` of `bar`; give up (and raise the CTA abort flag and
-// the device status) after ~2^28 polls or as soon as another role aborted.
-ZB_DEVICE bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status, int where) {
-    for (uint32_t i = 0; i < (1u << 28); ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 1023) == 1023 && *abort_flag) return false;
-    }
-    *abort_flag = 1;
-    if (status) atomicCAS(status, 0, where);
-    return false;
-}
 
 ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn, int G = 8) {
     // Bands of G tile-rows sweep the tile-columns, so CTAs running together
@@ -132,6 +123,18 @@ ZB_DEVICE uint8_t* smem_tail_scratch(uint8_t* smem) {
 }
 // Barrier among the four epilogue warps only (named barrier 1, 128 threads).
 ZB_DEVICE void epilogue_bar_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+// The same barrier, returning the AND of every epilogue thread's `ok`: the
+// four warps leave the tile loop together when any of them saw a wait fail
+// (a warp that left alone would strand the others at the next barrier).
+ZB_DEVICE bool epilogue_bar_and(bool ok) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)ok)
+        : "memory");
+    return r != 0;
+}
 
 // Slot ring bookkeeping shared by the producer and the MMA issuer.
 struct Ring {
@@ -195,8 +198,10 @@ constexpr CrtTable make_crt_table() {
 
 __constant__ CrtTable kCrt = make_crt_table();
 
-// Rows holding Inf / NaN: no residues; the reconstruction writes NaN.
-constexpr int kCrtNonFinite = -0x40000000;
+// Exponent marker of a row of op(A) (column of op(B)) holding Inf or NaN: its
+// digits / residues are zero, the emulated product leaves its entries of C
+// alone and ozaki_nonfinite_patch computes them in IEEE FP64 afterwards.
+constexpr int kNonFinite = -0x40000000;
 
 // d = c + sum_i a.u8[i] * b.s8[i]
 ZB_DEVICE int dp4a_us(uint32_t a, uint32_t b, int c) {
@@ -277,7 +282,7 @@ ZB_DEVICE void build_sched(const UmmaParams& P, Sched* s) {
 template <int ASLOTS, int BSLOTS, int ACHUNK, int BCHUNK, class Mma, class Commit>
 ZB_DEVICE bool mma_job(const uint8_t* flags, int n_steps, int c0, int c1, Ring& ra, Ring& rb, uint64_t* fullA,
                        uint64_t* fullB, uint64_t* emptyA, uint64_t* emptyB, uint32_t sA0, uint32_t sB0,
-                       uint32_t tmem_base, volatile int* abort_flag, int* status, Mma mma, Commit commit) {
+                       uint32_t tmem_base, const WaitCtl& w, Mma mma, Commit commit) {
     uint32_t started = 0;
     uint64_t adesc = 0, bdesc = 0;
     int a_slot = 0, b_slot = 0;
@@ -286,13 +291,13 @@ ZB_DEVICE bool mma_job(const uint8_t* flags, int n_steps, int c0, int c1, Ring& 
             const uint32_t f = flags[q];
             if (f & SF_NEW_A) {
                 a_slot = ra.slot;
-                if (!wait_phase(&fullA[a_slot], ra.phase, abort_flag, status, 4)) return false;
+                if (!wait_phase(&fullA[a_slot], ra.phase, w, WAIT_MMA_FULL_A)) return false;
                 ra.advance(ASLOTS);
                 adesc = umma_desc_sw128(sA0 + a_slot * ACHUNK);
             }
             if (f & SF_NEW_B) {
                 b_slot = rb.slot;
-                if (!wait_phase(&fullB[b_slot], rb.phase, abort_flag, status, 5)) return false;
+                if (!wait_phase(&fullB[b_slot], rb.phase, w, WAIT_MMA_FULL_B)) return false;
                 rb.advance(BSLOTS);
                 bdesc = umma_desc_sw128(sB0 + b_slot * BCHUNK);
             }
@@ -324,9 +329,12 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     uint64_t* emptyB = fullB + kBSlots;
     uint64_t* tfull = emptyB + kBSlots;  // [2]
     uint64_t* tempty = tfull + 2;        // [2]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* hold_bar = tempty + 2;     // test-only: nothing ever arrives on it
+    uint64_t* drain_bar = hold_bar + 1;  // abort path: the MMA issuer's last commit
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     Sched* sched = reinterpret_cast<Sched*>(smem_tail_scratch(smem) + kUN * 8);
+    const WaitCtl W{abort_flag, P.status, P.report, P.wait_ns};
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 32) build_sched(P, sched);
@@ -343,6 +351,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], 4);
         }
+        mbar_init(hold_bar, 1);
+        mbar_init(drain_bar, 1);
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -365,6 +375,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         // ------------------------------------------------ TMA producer
         if (lane == 0) {
             Ring ra, rb;
+            Issued ia, ib;
             bool ok = true;
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
                 int tm, tn;
@@ -377,33 +388,41 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                             for (int q = 0; q < n_steps; ++q) {
                                 const uint32_t f = sched->flags[f0 + q];
                                 if (f & SF_NEW_A) {
-                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, P.status, 1)))
+                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, W, WAIT_PRODUCER_EMPTY_A)))
                                         break;
                                     mbar_arrive_expect_tx(&fullA[ra.slot], kAChunk);
                                     tma_load_2d(smem_u32(sA + ra.slot * kAChunk), &tmA, &fullA[ra.slot],
                                                 kc * elems_per_chunk, sched->a[f0 + q] * P.m_pad + tm * kUM);
+                                    ia.note(ra.slot, ra.phase);
                                     ra.advance(kASlots);
                                 }
                                 if (f & SF_NEW_B) {
-                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, P.status, 2)))
+                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, W, WAIT_PRODUCER_EMPTY_B)))
                                         break;
                                     mbar_arrive_expect_tx(&fullB[rb.slot], kBChunk);
                                     tma_load_2d(smem_u32(sB + rb.slot * kBChunk), &tmB, &fullB[rb.slot],
                                                 kc * elems_per_chunk, sched->b[f0 + q] * P.n_pad + tn * kUN);
+                                    ib.note(rb.slot, rb.phase);
                                     rb.advance(kBSlots);
                                 }
                             }
                         }
                     }
             }
-            // Let every issued copy land before the CTA can retire (bounded).
-            for (int i = 0; i < kASlots; ++i) {
-                wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, nullptr, 0);
-                ra.advance(kASlots);
-            }
-            for (int i = 0; i < kBSlots; ++i) {
-                wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, nullptr, 0);
-                rb.advance(kBSlots);
+            if (ok) {
+                // every issued copy was consumed by an MMA before the CTA retires
+                for (int i = 0; i < kASlots; ++i) {
+                    wait_phase(&emptyA[ra.slot], ra.phase ^ 1, W, 0);
+                    ra.advance(kASlots);
+                }
+                for (int i = 0; i < kBSlots; ++i) {
+                    wait_phase(&emptyB[rb.slot], rb.phase ^ 1, W, 0);
+                    rb.advance(kBSlots);
+                }
+            } else {
+                // aborted: let the bytes of every issued copy land before the CTA retires
+                ia.drain(fullA, kASlots, P.wait_ns);
+                ib.drain(fullB, kBSlots, P.wait_ns);
             }
         }
     } else if (warp == 1) {
@@ -412,13 +431,13 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, kUM, kUN) : umma_idesc(1, 1, kUM, kUN);
             Ring ra, rb;
             uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
-            bool ok = true;
+            bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         // the job's accumulators must have been drained by the epilogue
                         const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
-                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
                         tc_fence_after();
                         const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
@@ -431,9 +450,15 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         auto commit = [](uint64_t* bar) { umma_commit(bar); };
                         ok = mma_job<kASlots, kBSlots, kAChunk, kBChunk>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
-                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, W, mma, commit);
                         if (ok) umma_commit(&tfull[b]);
                     }
+            if (!ok) {
+                // aborted: the MMAs already issued read shared memory and write
+                // TMEM; wait for them before either is released
+                umma_commit(drain_bar);
+                drain_phase(drain_bar, 0, P.wait_ns);
+            }
         }
     } else {
         // ---------------------------------------------- epilogue warps
@@ -444,27 +469,33 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         double* colscale = reinterpret_cast<double*>(smem_tail_scratch(smem));  // kUN doubles
         uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
         bool ok = true;
-        for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x) {
+        for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x) {
             int tm, tn;
             tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
             const int row = tm * kUM + row_in_tile;
-            const bool row_ok = row < P.m;
+            bool row_ok = row < P.m;
             int er = 0;
             if (EPI == EPI_OZAKI_F64) {
+                // all four warps leave together; the previous tile's readers are done
+                if (!epilogue_bar_and(ok)) break;
                 if (row_ok) er = P.row_exp[row];
-                // 2^{f_j} of this tile's columns, staged once per tile
-                epilogue_bar_sync();  // previous tile's readers are done
+                row_ok = row_ok && er != kNonFinite;  // left to the non-finite patch
+                // 2^{f_j} of this tile's columns, staged once per tile (-1: a
+                // column of op(B) holding Inf / NaN, left to the patch)
                 for (int c = et; c < kUN; c += 128) {
                     const int col = tn * kUN + c;
-                    colscale[c] = (col < P.n) ? pow2(P.col_exp[col]) : 0.0;
+                    const int ec = (col < P.n) ? P.col_exp[col] : 0;
+                    colscale[c] = (col < P.n) ? (ec == kNonFinite ? -1.0 : pow2(ec)) : 0.0;
                 }
                 epilogue_bar_sync();
+            } else if (!ok) {
+                break;
             }
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                     const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
-                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
                     if (EPI == EPI_RESIDUE) {
@@ -514,7 +545,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                                 if (two) d += (long long)(int)r1[c] << 7;
                                 const double v = (double)d * s0 * cs[c];
                                 const double out = !need_c ? v : (first ? fma(P.beta, cin[c], v) : cin[c] + v);
-                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
+                                if ((full_chunk || col0 + c < P.n) && cs[c] >= 0.0) __stcg(cb + (long)c * P.ldc, out);
                             }
                         } else {
                             float* cb = static_cast<float*>(P.c) + (long)col0 * P.ldc + row;
@@ -568,6 +599,11 @@ constexpr int kCrtSlot = 4 * kCrtAtom;       // 64 KB
 constexpr int kCrtSlots = (2 * kSlots2 * kChunk2) / kCrtSlot;  // 3
 static_assert(kCrtSlots >= 2, "CRT ring");
 
+// A CTA of the pair cannot observe its own copies land (their bytes are
+// counted on the even CTA's barriers); after an abort it waits this long for
+// them (a TMA copy of one slot takes a few microseconds).
+constexpr unsigned long long kPeerCopyGraceNs = 200000;
+
 template <int KIND, int EPI>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -582,7 +618,9 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     uint64_t* emptyB = fullB + kSlots2;
     uint64_t* tfull = emptyB + kSlots2;  // [2]
     uint64_t* tempty = tfull + 2;        // [2]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* hold_bar = tempty + 2;     // test-only: nothing ever arrives on it
+    uint64_t* drain_bar = hold_bar + 1;  // abort path: the MMA issuer's last commit (even CTA)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     double* colscale = reinterpret_cast<double*>(sB + kSlots2 * kChunk2 + 512);
     Sched* sched = reinterpret_cast<Sched*>(sB + kSlots2 * kChunk2 + 512 + kUN * 8);
@@ -592,6 +630,9 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     const uint32_t rank = cluster_ctarank();
     const bool leader = rank == 0;
     const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    // an abort raised in either CTA is raised in both
+    const WaitCtl W{abort_flag, P.status, P.report, P.wait_ns,
+                    mapa_shared(smem_u32(const_cast<int*>(abort_flag)), rank ^ 1u)};
     if (threadIdx.x == 0) {
         for (int i = 0; i < kSlots2; ++i) {
             mbar_init(&fullA[i], 1);
@@ -603,6 +644,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], 8);  // 4 epilogue warps in each CTA of the pair
         }
+        mbar_init(hold_bar, 1);
+        mbar_init(drain_bar, 1);
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -617,7 +660,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     }
     tc_fence_before();
     __syncthreads();
-    cluster_sync();  // the peer's barriers exist before any remote arrival
+    cluster_sync();  // the peer's barriers (and abort flag) exist before any remote access
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
@@ -626,6 +669,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         // ------------------------------------- TMA producer, CRT residue products
         if (lane == 0) {
             Ring rs;
+            Issued is;
             bool ok = true;
             const int steps = P.k_chunks / 2;  // 256-byte K steps (K padded to 256)
             // modulus-major: every tile of modulus l before modulus l + 1, so the
@@ -637,7 +681,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
                     const int l = P.job_shift[j][0];
                     for (int ks = 0; ks < steps; ++ks) {
-                        if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, P.status, 1))) break;
+                        if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, W, WAIT_PRODUCER_EMPTY_A))) break;
                         const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
                         const uint32_t bar = smem_u32(&fullA[rs.slot]) & 0xFEFFFFFFu;
                         if (leader) mbar_arrive_expect_tx(&fullA[rs.slot], 2 * kCrtSlot);
@@ -646,12 +690,19 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                         tma_load_2d_2sm(base + kCrtAtom, &tmA, bar, x + kChunkBytes, l * P.m_pad + arow);
                         tma_load_2d_2sm(base + 2 * kCrtAtom, &tmB, bar, x, l * P.n_pad + brow);
                         tma_load_2d_2sm(base + 3 * kCrtAtom, &tmB, bar, x + kChunkBytes, l * P.n_pad + brow);
+                        is.note(rs.slot, rs.phase);
                         rs.advance(kCrtSlots);
                     }
                 }
-            for (int i = 0; i < kCrtSlots; ++i) {
-                wait_phase(&emptyA[rs.slot], rs.phase ^ 1, abort_flag, nullptr, 0);
-                rs.advance(kCrtSlots);
+            if (ok) {
+                for (int i = 0; i < kCrtSlots; ++i) {
+                    wait_phase(&emptyA[rs.slot], rs.phase ^ 1, W, 0);
+                    rs.advance(kCrtSlots);
+                }
+            } else if (leader) {
+                is.drain(fullA, kCrtSlots, P.wait_ns);  // both CTAs' bytes of every issued slot
+            } else {
+                spin_ns(kPeerCopyGraceNs);
             }
         }
     } else if (warp == 1 && EPI == EPI_RESIDUE) {
@@ -660,18 +711,18 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             const uint32_t idesc = umma_idesc(2, 1, 256, kUN);
             Ring rs;
             uint32_t tphase = 0;
-            bool ok = true;
+            bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
             const int steps = P.k_chunks / 2;
             int inst = 0;  // job instances alternate between the two accumulators
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int tile = pair; ok && tile < P.num_tiles; tile += npairs, ++inst) {
                     const int b = inst & 1;
-                    if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                    if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
                     const uint32_t d = tmem_base + b * kUN;
                     for (int ks = 0; ks < steps; ++ks) {
-                        if (!(ok = wait_phase(&fullA[rs.slot], rs.phase, abort_flag, P.status, 4))) break;
+                        if (!(ok = wait_phase(&fullA[rs.slot], rs.phase, W, WAIT_MMA_FULL_A))) break;
                         const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
                         const uint64_t a0 = umma_desc_sw128(base), a1 = umma_desc_sw128(base + kCrtAtom);
                         const uint64_t b0 = umma_desc_sw128(base + 2 * kCrtAtom);
@@ -689,11 +740,17 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     }
                     if (ok) umma_commit_2sm(&tfull[b], 0x3);
                 }
+            if (!ok) {
+                // aborted: wait for the MMAs already issued before TMEM and the ring are released
+                umma_commit_2sm(drain_bar, 0x1);
+                drain_phase(drain_bar, 0, P.wait_ns);
+            }
         }
     } else if (warp == 0) {
         // ------------------------------------------------ TMA producer (both CTAs)
         if (lane == 0) {
             Ring ra, rb;
+            Issued ia, ib;
             bool ok = true;
             for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
                 int tm, tn;
@@ -707,32 +764,41 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                             for (int q = 0; q < n_steps; ++q) {
                                 const uint32_t f = sched->flags[f0 + q];
                                 if (f & SF_NEW_A) {
-                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, P.status, 1)))
+                                    if (!(ok = wait_phase(&emptyA[ra.slot], ra.phase ^ 1, W, WAIT_PRODUCER_EMPTY_A)))
                                         break;
                                     if (leader) mbar_arrive_expect_tx(&fullA[ra.slot], 2 * kChunk2);
                                     tma_load_2d_2sm(smem_u32(sA + ra.slot * kChunk2), &tmA,
                                                     smem_u32(&fullA[ra.slot]) & 0xFEFFFFFFu, kc * elems_per_chunk,
                                                     sched->a[f0 + q] * P.m_pad + arow);
+                                    ia.note(ra.slot, ra.phase);
                                     ra.advance(kSlots2);
                                 }
                                 if (f & SF_NEW_B) {
-                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, P.status, 2)))
+                                    if (!(ok = wait_phase(&emptyB[rb.slot], rb.phase ^ 1, W, WAIT_PRODUCER_EMPTY_B)))
                                         break;
                                     if (leader) mbar_arrive_expect_tx(&fullB[rb.slot], 2 * kChunk2);
                                     tma_load_2d_2sm(smem_u32(sB + rb.slot * kChunk2), &tmB,
                                                     smem_u32(&fullB[rb.slot]) & 0xFEFFFFFFu, kc * elems_per_chunk,
                                                     sched->b[f0 + q] * P.n_pad + brow);
+                                    ib.note(rb.slot, rb.phase);
                                     rb.advance(kSlots2);
                                 }
                             }
                         }
                     }
             }
-            for (int i = 0; i < kSlots2; ++i) {
-                wait_phase(&emptyA[ra.slot], ra.phase ^ 1, abort_flag, nullptr, 0);
-                ra.advance(kSlots2);
-                wait_phase(&emptyB[rb.slot], rb.phase ^ 1, abort_flag, nullptr, 0);
-                rb.advance(kSlots2);
+            if (ok) {
+                for (int i = 0; i < kSlots2; ++i) {
+                    wait_phase(&emptyA[ra.slot], ra.phase ^ 1, W, 0);
+                    ra.advance(kSlots2);
+                    wait_phase(&emptyB[rb.slot], rb.phase ^ 1, W, 0);
+                    rb.advance(kSlots2);
+                }
+            } else if (leader) {
+                ia.drain(fullA, kSlots2, P.wait_ns);
+                ib.drain(fullB, kSlots2, P.wait_ns);
+            } else {
+                spin_ns(kPeerCopyGraceNs);
             }
         }
     } else if (warp == 1) {
@@ -741,12 +807,12 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             const uint32_t idesc = (KIND == KIND_I8) ? umma_idesc(2, 1, 256, kUN) : umma_idesc(1, 1, 256, kUN);
             Ring ra, rb;
             uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
-            bool ok = true;
+            bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
             for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
-                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, abort_flag, P.status, 3))) break;
+                        if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
                         tc_fence_after();
                         const int c0 = ks * P.kseg_chunks, c1 = min(P.k_chunks, (ks + 1) * P.kseg_chunks);
@@ -759,9 +825,13 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                         auto commit = [](uint64_t* bar) { umma_commit_2sm(bar, 0x3); };
                         ok = mma_job<kSlots2, kSlots2, kChunk2, kChunk2>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
-                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, abort_flag, P.status, mma, commit);
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, W, mma, commit);
                         if (ok) umma_commit_2sm(&tfull[b], 0x3);
                     }
+            if (!ok) {
+                umma_commit_2sm(drain_bar, 0x1);
+                drain_phase(drain_bar, 0, P.wait_ns);
+            }
         }
     } else {
         // ---------------------------------------------- epilogue warps (both CTAs)
@@ -780,7 +850,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     int tm, tn;
                     tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
                     const int b = inst & 1;
-                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
                     const int row = tm * 256 + row_in_tile;
@@ -798,26 +868,30 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
                 }
         }
-        for (int tile = pair; EPI != EPI_RESIDUE && ok && tile < P.num_tiles; tile += npairs) {
+        for (int tile = pair; EPI != EPI_RESIDUE && tile < P.num_tiles; tile += npairs) {
             int tm, tn;
             tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn);
             const int row = tm * 256 + row_in_tile;
-            const bool row_ok = row < P.m;
+            bool row_ok = row < P.m;
             int er = 0;
             if (EPI == EPI_OZAKI_F64) {
+                if (!epilogue_bar_and(ok)) break;  // all four warps leave together
                 if (row_ok) er = P.row_exp[row];
-                epilogue_bar_sync();
+                row_ok = row_ok && er != kNonFinite;  // left to the non-finite patch
                 for (int c = et; c < kUN; c += 128) {
                     const int col = tn * kUN + c;
-                    colscale[c] = (col < P.n) ? pow2(P.col_exp[col]) : 0.0;
+                    const int ec = (col < P.n) ? P.col_exp[col] : 0;
+                    colscale[c] = (col < P.n) ? (ec == kNonFinite ? -1.0 : pow2(ec)) : 0.0;
                 }
                 epilogue_bar_sync();
+            } else if (!ok) {
+                break;
             }
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                     const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
-                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, abort_flag, P.status, 6))) break;
+                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
                     const bool two = P.job_groups[j] == 2;
@@ -847,7 +921,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                                 if (two) d += (long long)(int)r1[c] << 7;
                                 const double v = (double)d * s0 * cs[c];
                                 const double out = !need_c ? v : (first ? fma(P.beta, cin[c], v) : cin[c] + v);
-                                if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
+                                if ((full_chunk || col0 + c < P.n) && cs[c] >= 0.0) __stcg(cb + (long)c * P.ldc, out);
                             }
                         } else {
                             float* cb = static_cast<float*>(P.c) + (long)col0 * P.ldc + row;
@@ -889,6 +963,13 @@ struct View {
     long rs, cs;
     int rows, cols;
 };
+
+// |x| bit patterns at or above this one are Inf or NaN.
+constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
+
+// Append row r to the list of rows holding Inf / NaN (rows of op(A) or
+// columns of op(B)); the non-finite patch reads the list after the product.
+ZB_DEVICE void note_nonfinite(int r, int* count, int* list) { list[atomicAdd(count, 1)] = r; }
 
 // Row maxima of |X| as FP64 bit patterns (non-negative doubles order like
 // unsigned integers; NaN patterns sort above +Inf and so propagate).
@@ -938,7 +1019,7 @@ __global__ void ozaki_spread(const unsigned long long* __restrict__ maxbits, con
                              int rows, int cols, float* __restrict__ out) {
     float best = 0.f;
     for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-        if (maxbits[r] == 0 || sums[r] <= 0.0) continue;
+        if (maxbits[r] == 0 || maxbits[r] >= kInfBits || !(sums[r] > 0.0)) continue;  // zero or non-finite row
         int e;
         frexp(__longlong_as_double((long long)maxbits[r]), &e);
         const float sp = (float)(e - log2(sums[r] / cols));
@@ -955,9 +1036,11 @@ __global__ void ozaki_spread(const unsigned long long* __restrict__ maxbits, con
     }
 }
 
-// Exponent e with max * 2^-e in [0.5, 1): the frexp exponent of the maximum.
+// Exponent e with max * 2^-e in [0.5, 1): the frexp exponent of the maximum
+// (kNonFinite for a row holding Inf or NaN).
 ZB_DEVICE int row_exponent(unsigned long long bits) {
     if (bits == 0) return 0;
+    if (bits >= kInfBits) return kNonFinite;
     int e;
     frexp(__longlong_as_double((long long)bits), &e);
     return e;
@@ -974,7 +1057,7 @@ ZB_DEVICE int swz(int r, int c) {
 // (plane t: rows_pad x cols_pad bytes, K-major) and the row exponents.
 __global__ void __launch_bounds__(256)
 ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, int rows_pad, int cols_pad,
-            int8_t* __restrict__ planes, int* __restrict__ exps) {
+            int8_t* __restrict__ planes, int* __restrict__ exps, int* __restrict__ nf_count, int* __restrict__ nf_list) {
     __shared__ double tile[32 * 128];
     __shared__ int sexp[32];
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
@@ -984,6 +1067,7 @@ ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, 
         const int e = (r < X.rows) ? row_exponent(maxbits[r]) : 0;
         sexp[t] = e;
         if (blockIdx.x == 0 && r < rows_pad) exps[r] = e;
+        if (blockIdx.x == 0 && r < X.rows && e == kNonFinite) note_nonfinite(r, nf_count, nf_list);
     }
     // load (coalesced along the contiguous dimension of X)
 #pragma unroll 4
@@ -1005,10 +1089,11 @@ ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, 
     __syncthreads();
     // digits: thread -> row t / 8, 16 consecutive columns
     const int r = t >> 3, q = t & 7;
-    const double sc = ldexp(1.0, -sexp[r]);
+    // a row holding Inf / NaN gets zero digits (its entries of C are patched)
+    const double sc = sexp[r] == kNonFinite ? 0.0 : ldexp(1.0, -sexp[r]);
     double y[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) y[i] = tile[swz(r, q * 16 + i)] * sc;
+    for (int i = 0; i < 16; ++i) y[i] = sc == 0.0 ? 0.0 : tile[swz(r, q * 16 + i)] * sc;
     const long plane = (long)rows_pad * cols_pad;
     int8_t* out = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
     for (int s = 0; s < slices; ++s) {
@@ -1030,7 +1115,7 @@ ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, 
 ZB_DEVICE int crt_row_exponent(unsigned long long maxbits, double sum, int k, int P) {
     if (maxbits == 0) return 0;
     const double mx = __longlong_as_double((long long)maxbits);
-    if (!(mx <= 1.7976931348623157e308)) return kCrtNonFinite;  // Inf or NaN in the row
+    if (!(mx <= 1.7976931348623157e308)) return kNonFinite;  // Inf or NaN in the row
     int e1, e2;
     const double f1 = frexp(mx, &e1);  // mx = f1 2^e1, f1 in [0.5, 1)
     const double ratio = fmin(sum / mx, (double)k);
@@ -1045,7 +1130,8 @@ ZB_DEVICE int crt_row_exponent(unsigned long long maxbits, double sum, int k, in
 // - (2^63 mod m), then one exact FP32 reduction.
 __global__ void __launch_bounds__(256)
 ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const double* __restrict__ sums, int P,
-                int nmod, int rows_pad, int cols_pad, int8_t* __restrict__ planes, int* __restrict__ exps) {
+                int nmod, int rows_pad, int cols_pad, int8_t* __restrict__ planes, int* __restrict__ exps,
+                int* __restrict__ nf_count, int* __restrict__ nf_list) {
     __shared__ double tile[32 * 128];
     __shared__ int sexp[32];
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
@@ -1055,6 +1141,7 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
         const int e = (r < X.rows) ? crt_row_exponent(maxbits[r], sums[r], X.cols, P) : 0;
         sexp[t] = e;
         if (blockIdx.x == 0 && r < rows_pad) exps[r] = e;
+        if (blockIdx.x == 0 && r < X.rows && e == kNonFinite) note_nonfinite(r, nf_count, nf_list);
     }
 #pragma unroll 4
     for (int it = 0; it < 16; ++it) {
@@ -1076,7 +1163,7 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
     const int r = t >> 3, q = t & 7;
     if (r0 + r >= rows_pad) return;
     const int a = sexp[r];
-    const bool finite = a != kCrtNonFinite;
+    const bool finite = a != kNonFinite;
     // 2^a by one exact multiplication when both 2^a and the products stay normal
     const bool plain = a >= -960 && a <= 960;
     const double sc = plain ? pow2(a) : 0.0;
@@ -1173,17 +1260,25 @@ template <int NMOD>
 __global__ void __launch_bounds__(256)
 ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
                   const int* __restrict__ expb, double alpha, double beta, double* __restrict__ C, long ldc,
-                  const __grid_constant__ CrtCombine K) {
+                  const __grid_constant__ CrtCombine K, const int* __restrict__ status) {
     constexpr int G = (NMOD + 3) / 4;  // groups of four moduli
     // every modulus is >= 191 > 2^7.5, so log2 M >= 7.5 NMOD
     constexpr int Z0 = (15 * NMOD - 78) > 0 ? (15 * NMOD - 78) / 32 : 0;
     constexpr double kScaleZ0 = pow2_const(16 * Z0);
+    // The modular products did not all complete (a bounded wait ran out): C stays as it was.
+    if (*status) return;
     __shared__ double ct[16][129];  // column 4L + e holds element (4L + e - L) & 3 of lane L
+    __shared__ bool skip_row[16], skip_col[128];  // Inf / NaN in the row of op(A) / column of op(B)
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int i0 = blockIdx.x * 16, j0 = blockIdx.y * 128;
     const int jc = j0 + lane * 4;  // < n_pad: the planes are padded to 256 columns
     const int4 e4 = __ldg(reinterpret_cast<const int4*>(expb + jc));
     const int eb[4] = {e4.x, e4.y, e4.z, e4.w};
+    if (warp == 0) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) skip_col[lane * 4 + e] = eb[e] == kNonFinite;
+        if (lane < 16) skip_row[lane] = expa[i0 + lane] == kNonFinite;  // < m_pad
+    }
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
         const int rl = warp + 8 * h, gi = i0 + rl;  // < m_pad: the planes are padded to 128 rows
@@ -1235,20 +1330,19 @@ ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m,
 #pragma unroll
             for (int z = kCrtLimbs - 2; z >= 0; --z) x = fma(x, 65536.0, i2d(c[z]));
             const int sc = -(ea + eb[e]);
-            ct[rl][lane * 4 + ((e + lane) & 3)] = (ea == kCrtNonFinite || eb[e] == kCrtNonFinite)
-                                       ? __longlong_as_double(0x7ff8000000000000LL)
-                                       : alpha * (sc >= -1022 && sc <= 1023 ? x * pow2(sc) : ldexp(x, sc));
+            ct[rl][lane * 4 + ((e + lane) & 3)] = alpha * (sc >= -1022 && sc <= 1023 ? x * pow2(sc) : ldexp(x, sc));
         }
     }
     __syncthreads();
     // column-major write: 16 consecutive rows (128 bytes) of one column per half-warp
     const int r = t & 15;
     const int gi = i0 + r;
-    if (gi >= m) return;
+    if (gi >= m || skip_row[r]) return;  // rows holding Inf / NaN: left to the non-finite patch
 #pragma unroll 4
     for (int cc = t >> 4; cc < 128; cc += 16) {
         const int gj = j0 + cc;
         if (gj >= n) break;
+        if (skip_col[cc]) continue;
         double* cp = C + (long)gj * ldc + gi;
         double out = ct[r][(cc & ~3) | (((cc & 3) + (cc >> 2)) & 3)];
         if (beta != 0.0) out = fma(beta, *cp, out);
@@ -1257,13 +1351,106 @@ ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m,
 }
 
 using CombineFn = void (*)(const int8_t*, long, int, int, int, const int*, const int*, double, double, double*, long,
-                           CrtCombine);
+                           CrtCombine, const int*);
 template <int N>
 constexpr CombineFn combine_at(int nmod) {
     if constexpr (N == 1)
         return &ozaki_crt_combine<1>;
     else
         return nmod == N ? &ozaki_crt_combine<N> : combine_at<N - 1>(nmod);
+}
+
+// IEEE semantics for rows of op(A) / columns of op(B) that hold Inf or NaN.
+// Their integer digits / residues are zero and the emulated product leaves
+// their entries of C untouched; this kernel then computes exactly those
+// entries as plain FP64 dot products, C = alpha * sum_p A_ip B_pj (+ beta C
+// when beta != 0), the reference's loop (gemm.zig:1422-1429).  Every such
+// entry is Inf or NaN, and which one does not depend on the summation order.
+// Work items are 64 x 64 output tiles: rows listed in list_a x all columns,
+// then all rows (except listed ones) x columns listed in list_b; a persistent
+// grid reads the two counts, so with no Inf / NaN in the operands every CTA
+// returns at once.  A warp whose listed rows / columns lie past the count
+// skips its arithmetic.
+constexpr int kPatchTile = 64, kPatchK = 16;
+
+__global__ void __launch_bounds__(256)
+ozaki_nonfinite_patch(View va, View vb, int m, int n, int k, double alpha, double beta, double* __restrict__ C,
+                      long ldc, const int* __restrict__ cnt_a, const int* __restrict__ list_a,
+                      const int* __restrict__ cnt_b, const int* __restrict__ list_b, const int* __restrict__ expa,
+                      const int* __restrict__ status) {
+    if (*status) return;  // the product did not complete: C stays as it was
+    const int na = *cnt_a, nb = *cnt_b;
+    if (na == 0 && nb == 0) return;
+    __shared__ double Gs[kPatchK][kPatchTile + 1];  // [p][listed row / column]
+    __shared__ double Ds[kPatchK][kPatchTile + 1];  // [p][dense row / column]
+    const int t = threadIdx.x, warp = t >> 5;
+    const int ty = t >> 4, tx = t & 15;  // outputs: listed ty*4 + u, dense tx + 16 v
+    const long items_a = (long)((na + kPatchTile - 1) / kPatchTile) * ((n + kPatchTile - 1) / kPatchTile);
+    const long items_b = (long)((nb + kPatchTile - 1) / kPatchTile) * ((m + kPatchTile - 1) / kPatchTile);
+    for (long item = blockIdx.x; item < items_a + items_b; item += gridDim.x) {
+        // listed side G (rows of op(A), or columns of op(B) = rows of op(B)^T), dense side D
+        const bool rows = item < items_a;
+        const long it = rows ? item : item - items_a;
+        const int dense_ext = rows ? n : m;
+        const int dense_tiles = (dense_ext + kPatchTile - 1) / kPatchTile;
+        const int g0 = (int)(it / dense_tiles) * kPatchTile, d0 = (int)(it % dense_tiles) * kPatchTile;
+        const int gcount = min(kPatchTile, (rows ? na : nb) - g0);
+        const int* list = rows ? list_a : list_b;
+        const View& G = rows ? va : vb;
+        const View& D = rows ? vb : va;
+        const bool warp_busy = warp * 8 < gcount;
+        double acc[4][4] = {};
+        for (int p0 = 0; p0 < k; p0 += kPatchK) {
+            __syncthreads();  // the previous slice's readers are done
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = t + 256 * q;
+                // contiguous index fastest in global memory
+                int gr, gp;
+                if (G.cs == 1) { gp = e % kPatchK; gr = e / kPatchK; } else { gr = e % kPatchTile; gp = e / kPatchTile; }
+                double v = 0.0;
+                if (gr < gcount && p0 + gp < k) v = G.base[(long)list[g0 + gr] * G.rs + (long)(p0 + gp) * G.cs];
+                Gs[gp][gr] = v;
+                int dr, dp;
+                if (D.cs == 1) { dp = e % kPatchK; dr = e / kPatchK; } else { dr = e % kPatchTile; dp = e / kPatchTile; }
+                double w = 0.0;
+                if (d0 + dr < dense_ext && p0 + dp < k) w = D.base[(long)(d0 + dr) * D.rs + (long)(p0 + dp) * D.cs];
+                Ds[dp][dr] = w;
+            }
+            __syncthreads();
+            if (warp_busy) {
+#pragma unroll 4
+                for (int p = 0; p < kPatchK; ++p) {
+                    double gv[4], dv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) gv[u] = Gs[p][ty * 4 + u];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) dv[v] = Ds[p][tx + 16 * v];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) acc[u][v] = fma(gv[u], dv[v], acc[u][v]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int g = ty * 4 + u;
+            if (g >= gcount) continue;
+            const int listed = list[g0 + g];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int d = d0 + tx + 16 * v;
+                if (d >= dense_ext) continue;
+                const int i = rows ? listed : d, j = rows ? d : listed;
+                if (!rows && expa[i] == kNonFinite) continue;  // the row pass wrote it
+                double* cp = C + (long)j * ldc + i;
+                double out = alpha * acc[u][v];
+                if (beta != 0.0) out = out + beta * *cp;
+                *cp = out;
+            }
+        }
+    }
 }
 
 // 3xBF16 split of a float matrix view into hi / lo planes (bf16, K-major).
@@ -1314,16 +1501,7 @@ bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ plan
 
 // ------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
 }
 
 // 2-D K-major digit tensor: inner dim = K (cols_pad elements), outer = planes * rows_pad rows.
@@ -1344,8 +1522,11 @@ cudaError_t make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
 inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
 
 // Workspace layout: the small statistics block first, the digit planes after it.
+// The statistics of op(A) come first and those of op(B) (with the status word)
+// after them, so that a call reusing op(A) (a_ready) clears one range.
 struct Layout {
-    long maxa_off, maxb_off, suma_off, sumb_off, expa_off, expb_off, spread_off, status_off, stats_end;
+    long maxa_off, suma_off, cnta_off, maxb_off, sumb_off, cntb_off, status_off, spread_off, b_clear_end;
+    long expa_off, expb_off, lista_off, listb_off, stats_end;
     long a_planes_off, b_planes_off, res_off, total;
 };
 
@@ -1358,13 +1539,18 @@ Layout ozaki_layout(const OzakiPlan& p) {
         return o;
     };
     L.maxa_off = take((long)p.m_pad * 8);
-    L.maxb_off = take((long)p.n_pad * 8);
     L.suma_off = take((long)p.m_pad * 8);
+    L.cnta_off = take(16);
+    L.maxb_off = take((long)p.n_pad * 8);
     L.sumb_off = take((long)p.n_pad * 8);
+    L.cntb_off = take(16);
+    L.status_off = take(64);
+    L.spread_off = take(16);
+    L.b_clear_end = off;
     L.expa_off = take((long)p.m_pad * 4);
     L.expb_off = take((long)p.n_pad * 4);
-    L.spread_off = take(16);
-    L.status_off = take(64);
+    L.lista_off = take((long)p.m_pad * 4);
+    L.listb_off = take((long)p.n_pad * 4);
     L.stats_end = off;
     off = round_up(off, 1024);
     const int s = p.scheme == OZAKI_CRT ? p.moduli : (p.slices > 0 ? p.slices : kOzakiAutoMaxSlices);
@@ -1384,6 +1570,52 @@ int sm_count_cached() {
         if (n <= 0) n = 148;
     }
     return n;
+}
+
+// Per-device report word of bounded waits that ran out (0: none since the host
+// last read it).  Host code reaches it through its device address, looked up
+// once per device with that device current.
+__device__ int g_wait_report;
+
+constexpr int kMaxReportDevices = 64;
+struct ReportSlot {
+    std::once_flag once;
+    int* ptr = nullptr;
+    cudaError_t err = cudaSuccess;
+};
+ReportSlot g_report_slots[kMaxReportDevices];
+// Set once any product kernel has been launched in this process (until then
+// there is nothing to read, and reading would load this file's module).
+std::atomic<bool> g_products_launched{false};
+
+cudaError_t report_word(int** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxReportDevices) return cudaErrorInvalidDevice;
+    ReportSlot& r = g_report_slots[dev];
+    std::call_once(r.once, [&r] {
+        void* q = nullptr;
+        r.err = cudaGetSymbolAddress(&q, g_wait_report);
+        r.ptr = static_cast<int*>(q);
+    });
+    *out = r.ptr;
+    return r.err;
+}
+
+// Time limit of every mbarrier wait: generous for any legitimate wait (a job's
+// products take microseconds, a context switch milliseconds); the test hold
+// uses 1 ms so that the whole abort path runs in a few milliseconds.
+constexpr unsigned long long kWaitLimitNs = 4000000000ull;
+constexpr unsigned long long kHoldWaitLimitNs = 1000000ull;
+
+cudaError_t set_wait_params(UmmaParams& P, bool hold) {
+    cudaError_t e = report_word(&P.report);
+    if (e != cudaSuccess) return e;
+    P.hold = hold ? 1 : 0;
+    P.wait_ns = hold ? kHoldWaitLimitNs : kWaitLimitNs;
+    g_products_launched.store(true);
+    return cudaSuccess;
 }
 
 template <int KIND, int EPI>
@@ -1550,6 +1782,20 @@ const CrtHost& crt_host(int nmod) {
 
 std::atomic<int> g_last_moduli{0};
 
+// Rows of op(A) / columns of op(B) holding Inf or NaN: their entries of C are
+// computed in IEEE FP64 after the emulated product (which leaves them alone).
+cudaError_t launch_nonfinite_patch(const GemmArgsF64& g, const View& va, const View& vb, const Layout& L, uint8_t* w,
+                                   cudaStream_t st) {
+    const int* cnta = reinterpret_cast<const int*>(w + L.cnta_off);
+    const int* cntb = reinterpret_cast<const int*>(w + L.cntb_off);
+    ozaki_nonfinite_patch<<<2 * sm_count_cached(), 256, 0, st>>>(
+        va, vb, g.m, g.n, g.k, g.alpha, g.beta, g.c, g.ldc, cnta, reinterpret_cast<const int*>(w + L.lista_off), cntb,
+        reinterpret_cast<const int*>(w + L.listb_off), reinterpret_cast<const int*>(w + L.expa_off),
+        reinterpret_cast<const int*>(w + L.status_off));
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready) {
     const Layout L = ozaki_layout(p);
     uint8_t* w = static_cast<uint8_t*>(ws);
@@ -1562,6 +1808,10 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     auto* sumb = reinterpret_cast<double*>(w + L.sumb_off);
     int* expa = reinterpret_cast<int*>(w + L.expa_off);
     int* expb = reinterpret_cast<int*>(w + L.expb_off);
+    int* cnta = reinterpret_cast<int*>(w + L.cnta_off);
+    int* cntb = reinterpret_cast<int*>(w + L.cntb_off);
+    int* lista = reinterpret_cast<int*>(w + L.lista_off);
+    int* listb = reinterpret_cast<int*>(w + L.listb_off);
     int* status = reinterpret_cast<int*>(w + L.status_off);
     const int nmod = p.moduli;
     const CrtHost& H = crt_host(nmod);
@@ -1569,11 +1819,10 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
 
     View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
-    // a_ready: A's statistics, exponents and planes stay; only B's accumulators and the status are cleared
-    cudaError_t e = a_ready ? cudaMemsetAsync(w + L.maxb_off, 0, L.suma_off - L.maxb_off, st)
-                            : cudaMemsetAsync(w, 0, L.stats_end, st);
-    if (e == cudaSuccess && a_ready) e = cudaMemsetAsync(w + L.sumb_off, 0, L.expa_off - L.sumb_off, st);
-    if (e == cudaSuccess && a_ready) e = cudaMemsetAsync(w + L.status_off, 0, L.stats_end - L.status_off, st);
+    // a_ready: op(A)'s statistics, exponents, Inf / NaN row list and planes stay;
+    // op(B)'s accumulators, its list count and the status word are cleared
+    cudaError_t e = a_ready ? cudaMemsetAsync(w + L.maxb_off, 0, L.b_clear_end - L.maxb_off, st)
+                            : cudaMemsetAsync(w, 0, L.b_clear_end, st);
     if (e != cudaSuccess) return e;
     for (int side = a_ready ? 1 : 0; side < 2; ++side) {
         const View& v = side ? vb : va;
@@ -1591,7 +1840,8 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
         ozaki_crt_split<<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma, H.P, nmod, rows_pad,
-                                               p.k_pad, side ? b_planes : a_planes, side ? expb : expa);
+                                               p.k_pad, side ? b_planes : a_planes, side ? expb : expa,
+                                               side ? cntb : cnta, side ? listb : lista);
         count_launch();
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1636,14 +1886,16 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     // (band x 256 rows x k_pad bytes) stay within ~48 MB of L2 while the band
     // sweeps the tile-columns
     P.band_rows = (int)std::max(1L, std::min<long>(P.tiles_m, (48L << 20) / (256L * p.k_pad)));
+    if ((e = set_wait_params(P, p.hold)) != cudaSuccess) return e;
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
 
     dim3 cgrid((g.m + 15) / 16, (g.n + 127) / 128);
     combine_at<kCrtMaxModuli>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
-                                                          g.alpha, g.beta, g.c, g.ldc, H.K);
+                                                          g.alpha, g.beta, g.c, g.ldc, H.K, status);
     count_launch();
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return launch_nonfinite_patch(g, va, vb, L, w, st);
 }
 }  // namespace
 
@@ -1669,12 +1921,16 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     int* expb = reinterpret_cast<int*>(w + L.expb_off);
     float* spread = reinterpret_cast<float*>(w + L.spread_off);
     int* status = reinterpret_cast<int*>(w + L.status_off);
+    int* cnta = reinterpret_cast<int*>(w + L.cnta_off);
+    int* cntb = reinterpret_cast<int*>(w + L.cntb_off);
+    int* lista = reinterpret_cast<int*>(w + L.lista_off);
+    int* listb = reinterpret_cast<int*>(w + L.listb_off);
 
     // op(A) as rows i / cols p; op(B)^T as rows j / cols p.
     View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
 
-    cudaError_t e = cudaMemsetAsync(w, 0, L.stats_end, st);  // the slice scheme recomputes both operands
+    cudaError_t e = cudaMemsetAsync(w, 0, L.b_clear_end, st);  // the slice scheme recomputes both operands
     if (e != cudaSuccess) return e;
     for (int side = 0; side < 2; ++side) {
         const View& v = side ? vb : va;
@@ -1705,7 +1961,8 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
         ozaki_split<<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, p.slices, rows_pad, p.k_pad,
-                                           side ? b_planes : a_planes, side ? expb : expa);
+                                           side ? b_planes : a_planes, side ? expb : expa, side ? cntb : cnta,
+                                           side ? listb : lista);
         count_launch();
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1762,8 +2019,31 @@ cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, c
     P.row_exp = expa;
     P.col_exp = expb;
     P.status = status;
-    if (p.pair) return launch_umma_2cta<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
-    return launch_umma<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
+    if ((e = set_wait_params(P, p.hold)) != cudaSuccess) return e;
+    e = p.pair ? launch_umma_2cta<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st)
+               : launch_umma<KIND_I8, EPI_OZAKI_F64>(ma, mb, P, st);
+    if (e != cudaSuccess) return e;
+    return launch_nonfinite_patch(g, va, vb, L, w, st);
+}
+
+cudaError_t wait_report_word(int** out) {
+    cudaError_t e = report_word(out);
+    if (e == cudaSuccess) g_products_launched.store(true);
+    return e;
+}
+
+int ozaki_take_wait_report(cudaStream_t stream, cudaError_t* err) {
+    *err = cudaSuccess;
+    if (!g_products_launched.load()) return 0;
+    int* word = nullptr;
+    cudaError_t e = report_word(&word);
+    int v = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&v, word, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && v != 0) e = cudaMemsetAsync(word, 0, sizeof(int), stream);
+    if (e == cudaSuccess && v != 0) e = cudaStreamSynchronize(stream);
+    *err = e;
+    return e == cudaSuccess ? v : 0;
 }
 
 size_t bf16x3_workspace_bytes(int m, int n, int k) {
@@ -1819,6 +2099,7 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     P.beta_f = g.beta;
     P.c = g.c;
     P.ldc = g.ldc;
+    if ((e = set_wait_params(P, false)) != cudaSuccess) return e;
     if (pair) return launch_umma_2cta<KIND_BF16, EPI_F32>(ma, mb, P, st);
     return launch_umma<KIND_BF16, EPI_F32>(ma, mb, P, st);
 }

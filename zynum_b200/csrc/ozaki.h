@@ -28,7 +28,19 @@ struct OzakiPlan {
     int n_pad = 0;    // columns of B padded to the 256-column UMMA tile
     int k_pad = 0;    // K padded to the 128-byte TMA box
     bool pair = false;  // CTA-pair (cta_group::2, M = 256) slice-product kernel; m_pad is then a multiple of 256
+    bool hold = false;  // test-only: the product kernel's MMA issuer waits on a barrier nothing arrives on
 };
+
+// Bounded waits of the tensor-core product kernels: every mbarrier wait gives
+// up after a time limit, records its site in the device's report word and
+// leaves C untouched (CRT scheme; the slice scheme's fused epilogue may have
+// updated part of C).  Reads and clears the current device's report word
+// after synchronising `stream`: 0 if no wait ran out since the last read, else
+// the site (1 .. 7); *err receives a CUDA error of the read itself.
+int ozaki_take_wait_report(cudaStream_t stream, cudaError_t* err);
+// Device address of the current device's report word, for other kernels with
+// bounded waits (looked up once per device; marks the word as worth reading).
+cudaError_t wait_report_word(int** out);
 
 // Whether the automatic method should prefer Ozaki for this shape.
 bool ozaki_preferred(int m, int n, int k);

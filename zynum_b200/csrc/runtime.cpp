@@ -10,6 +10,7 @@
 #include <atomic>
 
 #include "kernels.h"
+#include "ozaki.h"
 
 namespace zb {
 
@@ -164,6 +165,27 @@ cudaError_t Context::stream_scratch(cudaStream_t s, size_t bytes, void** out) {
     return e;
 }
 
+namespace {
+thread_local int g_wait_site = 0;  // site of the last bounded wait seen to run out on this thread
+}
+
+cudaError_t check_wait_report(cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    const int site = ozaki_take_wait_report(s, &err);
+    if (err != cudaSuccess) return err;
+    if (site) {
+        g_wait_site = site;
+        return cudaErrorLaunchTimeout;
+    }
+    return cudaSuccess;
+}
+
+int take_wait_site() {
+    const int v = g_wait_site;
+    g_wait_site = 0;
+    return v;
+}
+
 cudaError_t Context::sync(cudaStream_t s) {
     if (faults.fail_next_sync) {
         cudaError_t e = static_cast<cudaError_t>(faults.fail_next_sync);
@@ -171,7 +193,8 @@ cudaError_t Context::sync(cudaStream_t s) {
         cudaStreamSynchronize(s);
         return e;
     }
-    return cudaStreamSynchronize(s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? check_wait_report(s) : e;
 }
 
 cudaError_t Context::wait_event(cudaEvent_t ev) {
@@ -181,7 +204,9 @@ cudaError_t Context::wait_event(cudaEvent_t ev) {
         cudaEventSynchronize(ev);
         return e;
     }
-    return cudaEventSynchronize(ev);
+    cudaError_t e = cudaEventSynchronize(ev);
+    // the report is read on the download stream, which is idle or copying finished panels
+    return e == cudaSuccess ? check_wait_report(stream_out) : e;
 }
 
 namespace {
@@ -260,6 +285,19 @@ int profile_read(double* ms, int max) {
         ms[n++] = t;
     }
     return n;
+}
+
+void* tensor_map_encoder() {
+    static void* fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = p;
+    });
+    return fn;
 }
 
 Context& context() {

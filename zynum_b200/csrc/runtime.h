@@ -10,6 +10,7 @@
 // fails.
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <mutex>
@@ -33,11 +34,22 @@ struct DeviceBuffer {
 };
 
 // Host-side fault injection used by the tests (no GPU fault is ever made):
-// the next reservation fails with cudaErrorMemoryAllocation, or the next
-// stream synchronisation reports the given error.
+// the next reservation fails with cudaErrorMemoryAllocation, the next stream
+// synchronisation reports the given error, or the next tensor-core product
+// kernels run with a hold (their MMA issuer first waits on a barrier that
+// nothing arrives on, with a 1 ms limit, so the kernel's bounded-wait abort
+// path runs and the call reports it).
 struct InjectedFaults {
     int fail_next_reservations = 0;
     int fail_next_sync = 0;  // cudaError_t code
+    std::atomic<int> hold_next_products{0};
+    // True (and one fewer left) if the next product kernel is to run with the hold.
+    bool take_hold() {
+        int v = hold_next_products.load();
+        while (v > 0 && !hold_next_products.compare_exchange_weak(v, v - 1)) {
+        }
+        return v > 0;
+    }
 };
 
 struct Context {
@@ -65,12 +77,22 @@ struct Context {
     // Scratch for a device entry point running on `stream`.
     cudaError_t stream_scratch(cudaStream_t stream, size_t bytes, void** out);
     cudaError_t reserve(DeviceBuffer& buf, size_t bytes, cudaStream_t stream);
+    // Synchronise `stream`; afterwards a bounded wait that ran out in a
+    // product kernel (the device's report word) is returned as
+    // cudaErrorLaunchTimeout with its site in the last-error text.
     cudaError_t sync(cudaStream_t stream);
     // Host wait for an event; reports an injected synchronisation error like sync().
     cudaError_t wait_event(cudaEvent_t ev);
 };
 
 Context& context();
+
+// Read (and clear) the device's bounded-wait report after `s` was
+// synchronised: cudaErrorLaunchTimeout if a product kernel's wait ran out
+// (its site is kept for take_wait_site), else cudaSuccess or the read's error.
+cudaError_t check_wait_report(cudaStream_t s);
+// Site recorded by the last check_wait_report on this thread that found one (0: none); clears it.
+int take_wait_site();
 
 void set_last_error(const std::string& msg);
 const char* last_error();
