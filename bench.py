@@ -487,6 +487,13 @@ def run_ours(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
+    # measured raw issue rates of the two tensor pipes (denominators beside the nominal ones)
+    import ctypes as C
+    raw = {}
+    for pipe, key in ((0, "fp64_dmma_tflops"), (1, "int8_tcgen05_tops")):
+        r = C.c_double(0.0)
+        if L.zynum_blas_gpu_measure_pipe_rate(pipe, C.byref(r), stream.cuda_stream) == 0:
+            raw[key] = r.value
     hr = results[head[0]]
     value = world * hr["tflops"]
     # roofline of the dominant kernel
@@ -498,6 +505,9 @@ def run_ours(args, rank, world, local_rank):
         achieved = ops / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / int8_peak) if achieved else None,
+                "peak_raw_issue": raw.get("int8_tcgen05_tops"),
+                "frac_of_raw_issue": (achieved / raw["int8_tcgen05_tops"])
+                if achieved and raw.get("int8_tcgen05_tops") else None,
                 "traffic": TRAFFIC_8192["crt"] if (n == 8192 and info["scheme"] == "crt") else None,
                 "kernel": ("ozaki int8 modular-product GEMM (CRT residues, tcgen05 kind::i8)" if info["scheme"] == "crt"
                            else "ozaki int8 slice-product GEMM (tcgen05 kind::i8)"),
@@ -508,6 +518,9 @@ def run_ours(args, rank, world, local_rank):
         achieved = flop / (hr["kernel_ms"] * 1e-3) / 1e12 if hr["kernel_ms"] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
                 "frac": (achieved / FP64_NOMINAL_TFLOPS) if achieved else None,
+                "peak_raw_issue": raw.get("fp64_dmma_tflops"),
+                "frac_of_raw_issue": (achieved / raw["fp64_dmma_tflops"])
+                if achieved and raw.get("fp64_dmma_tflops") else None,
                 "traffic": TRAFFIC_8192["native"] if n == 8192 else None,
                 "kernel": "native DGEMM (DMMA m16n8k8 f64)",
                 "peak_source": "nominal FP64 pipe: 148 SMs x 128 flop/clk x 1.965 GHz (no measured FP64 peak)"}
@@ -522,12 +535,20 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": "replicas" if world > 1 else "single-GPU"},
         "methods": {k: {**v, **({"error": err[k]} if k in err else {})} for k, v in results.items()},
         "roofline": roof,
+        "raw_pipe_rates": {**raw, "how": "zynum_blas_gpu_measure_pipe_rate: register-only DMMA loop on every SM; "
+                                          "tcgen05 cta_group::2 i8 M256 N256 K32 chain on shared-memory operands"},
         "clocks": clk,
         "gpu_launches": int(hr["launches_per_step"] * args.steps),
         "e2e": {"value": world * flop / e2e_s / 1e12, "unit": "TFLOP/s", "ms_per_step": e2e_s * 1e3,
                 "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8,
                 "path": "dgemm_ Fortran ABI, pinned host buffers"},
     }
+    if "native" in results and results["native"].get("kernel_ms") and raw.get("fp64_dmma_tflops"):
+        nat = flop / (results["native"]["kernel_ms"] * 1e-3) / 1e12
+        line["methods"]["native"]["roofline"] = {
+            "bound": "tensor", "achieved": nat, "unit": "TFLOP/s", "peak": FP64_NOMINAL_TFLOPS,
+            "frac": nat / FP64_NOMINAL_TFLOPS, "peak_raw_issue": raw["fp64_dmma_tflops"],
+            "frac_of_raw_issue": nat / raw["fp64_dmma_tflops"], "kernel": "native DGEMM (TMA-fed DMMA tiles)"}
     if not args.no_precision and not args.no_error and head[0] == "ozaki" and len(methods) == 2:
         from oracle import oracle as orc
         extra = precision_methods(torch, blas, orc, n, max(3, min(args.steps, 10)), max(3, args.warmup), stream,

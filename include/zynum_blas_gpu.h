@@ -467,6 +467,14 @@ ZYNUM_BLAS_GPU_API void zynum_blas_gpu_inject_fault(int kind, int count);
  * was.  Host entry points make this check themselves before copying C back.
  * No reference counterpart (the reference has no GPU). */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_device_status(void *stream);
+/* Measured raw issue rate of a tensor pipe on the current GPU, for roofline
+ * fractions against a measured denominator: pipe 0 = FP64 DMMA (register-only
+ * mma.sync m16n8k8 loop on every SM; TFLOP/s), pipe 1 = INT8 tcgen05
+ * (cta_group::2 M = 256, N = 256, K = 32 MMAs on shared-memory operands, one
+ * CTA pair per two SMs; TOP/s).  Runs on `stream` and synchronises it; takes
+ * about 0.1 s.  Returns 0 and writes *rate, 1 for a bad argument, or a
+ * negative CUDA status.  No reference counterpart (measurement only). */
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_measure_pipe_rate(int pipe, double *rate, void *stream);
 /* Dominant-kernel timing: enable != 0 starts recording CUDA events around the
  * main contraction kernel of every call (on the launching stream) and clears
  * earlier records; returns the previous state. */

@@ -201,6 +201,8 @@ def _declare(L: C.CDLL) -> None:
     L.zynum_blas_gpu_inject_fault.restype = None
     L.zynum_blas_gpu_device_status.argtypes = [P]
     L.zynum_blas_gpu_device_status.restype = i
+    L.zynum_blas_gpu_measure_pipe_rate.argtypes = [i, C.POINTER(C.c_double), P]
+    L.zynum_blas_gpu_measure_pipe_rate.restype = i
     L.zynum_blas_gpu_profile.argtypes = [i]
     L.zynum_blas_gpu_profile.restype = i
     L.zynum_blas_gpu_profile_read.argtypes = [P, i]

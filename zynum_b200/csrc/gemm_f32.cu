@@ -14,6 +14,8 @@
 // op = N for B) is transposed on the fly by per-element copies.
 #include <algorithm>
 
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -353,7 +355,13 @@ size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count) {
 cudaError_t sgemm_native(const GemmArgsF32& g_in, const GemmPlan& plan, float* workspace, cudaStream_t st) {
     if (plan.tile == TILE_GEMV && gemv_applies(g_in.m, g_in.n, g_in.k, g_in.tri))
         return sgemv_route(g_in, plan.splits, workspace, st);
-    if (skinny_gemm_applies(g_in.m, g_in.n, g_in.k, g_in.tri)) return sgemm_skinny(g_in, st);
+    if (skinny_gemm_applies(g_in.m, g_in.n, g_in.k, g_in.tri)) {
+        static const bool tma = [] {  // opt-in until measured: ZYNUM_GPU_SKINNY_TMA=1
+            const char* v = std::getenv("ZYNUM_GPU_SKINNY_TMA");
+            return v && v[0] == '1';
+        }();
+        return (tma && sgemm_skinny_tma_applies(g_in)) ? sgemm_skinny_tma(g_in, st) : sgemm_skinny(g_in, st);
+    }
     if ((plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M) && narrow_gemm_applies(g_in.m, g_in.n, g_in.tri))
         return sgemm_narrow(g_in, plan.splits, workspace, st);
     GemmArgsF32 g = g_in;

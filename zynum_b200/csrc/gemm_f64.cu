@@ -267,12 +267,12 @@ cudaError_t run_tiles(const GemmArgsF64& g, int vec, int used_splits, int k_chun
 
 }  // namespace
 
-// The 128 x 128 route takes the TMA kernel for operands TMA can describe when
-// ZYNUM_GPU_DGEMM_TMA=1 (otherwise the cp.async kernel).
+// The 128 x 128 route takes the TMA kernel for operands TMA can describe
+// (ZYNUM_GPU_DGEMM_TMA=0 keeps the cp.async kernel, for comparisons).
 static bool use_tma_tiles(const GemmArgsF64& g, const GemmPlan& plan) {
     static const bool enabled = [] {
         const char* v = std::getenv("ZYNUM_GPU_DGEMM_TMA");
-        return v && v[0] == '1';
+        return !(v && v[0] == '0');
     }();
     return enabled && plan.tile == TILE_128x128 && dgemm_tma_applies(g);
 }
@@ -290,7 +290,13 @@ int dgemm_native_used_splits(const GemmArgsF64& g, const GemmPlan& plan) {
 // requires a workspace of splits * m * n doubles.
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st) {
     if (plan.tile == TILE_GEMV && gemv_applies(g.m, g.n, g.k, g.tri)) return dgemv_route(g, plan.splits, workspace, st);
-    if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) return dgemm_skinny(g, st);
+    if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) {
+        static const bool tma = [] {  // opt-in until measured: ZYNUM_GPU_SKINNY_TMA=1
+            const char* v = std::getenv("ZYNUM_GPU_SKINNY_TMA");
+            return v && v[0] == '1';
+        }();
+        return (tma && dgemm_skinny_tma_applies(g)) ? dgemm_skinny_tma(g, st) : dgemm_skinny(g, st);
+    }
     const bool aligned = ((reinterpret_cast<uintptr_t>(g.a) | reinterpret_cast<uintptr_t>(g.b)) % 16 == 0) &&
                          (g.lda % 2 == 0) && (g.ldb % 2 == 0);
     const int vec = aligned ? 2 : 1;

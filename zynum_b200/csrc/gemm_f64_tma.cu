@@ -17,11 +17,13 @@
 //   K-major  (A 'T', B 'N'): 2 boxes of 128 rows x 16 k (128 B).
 // Within a k8 step the MMA's k index kappa reads physical k = 2 (kappa mod 4)
 // + kappa / 4, and within a 16-row fragment MMA row r = g + 8 v reads
-// physical row 2 g + v (g = lane / 4).  Both are bijections, applied to A, B
-// and C alike, so the product is unchanged; they make every A fragment pair
-// and every K-major B fragment pair one 16-byte shared load, and with the
-// 128-byte swizzle every fragment load runs at the minimum number of
-// shared-memory wavefronts.
+// physical row 2 g + v (g = lane / 4); for a K-major op(B) the MMA's column n
+// reads physical column (n >> 1) | ((n & 1) << 2) of its 8-column block.  All
+// are bijections, applied to A, B and C alike, so the product is unchanged;
+// they make every A fragment pair and every K-major B fragment pair one
+// 16-byte shared load, and with the 128-byte swizzle every fragment load runs
+// at the minimum number of shared-memory wavefronts (the two rows of a K-major
+// quarter-warp fall in opposite halves of the swizzle).
 //
 // Every mbarrier wait is bounded in time; a wait that runs out records its
 // site in the device's report word and the warp leaves its part of C alone.
@@ -37,7 +39,13 @@ namespace {
 
 constexpr int kTBM = 128, kTBN = 128, kTBK = 32, kTStages = 3;
 constexpr int kTMathWarps = 8;                     // 2 (M) x 4 (N) warps of 64 x 32
-constexpr int kTThreads = (kTMathWarps + 1) * 32;  // + the TMA producer warp
+constexpr int kTThreads = (kTMathWarps + 4) * 32;  // + a producer warpgroup (one TMA thread)
+// Register split: 384 threads launch with 168 registers each (64512); the
+// producer warpgroup drops to 40 and the two math warpgroups rise to 232:
+// 128 x 40 + 256 x 232 = 64512.  Per SM sub-partition: 2 x 32 x 232 + 32 x 40
+// = 16128 of its 16384 registers.
+constexpr int kTProducerRegs = 40, kTMathRegs = 232;
+static_assert(128 * kTProducerRegs + 256 * kTMathRegs <= kTThreads * 168, "register split exceeds the launch");
 constexpr int kTWM = 64, kTWN = 32;
 constexpr int kTOpBytes = kTBM * kTBK * 8;  // 32 KB per operand and stage
 constexpr int kTStageBytes = 2 * kTOpBytes;
@@ -61,15 +69,6 @@ ZB_DEVICE uint32_t mn_major_off(int mn, int k) {
 }
 ZB_DEVICE uint32_t k_major_off(int mn, int k) {
     return (uint32_t)((k >> 4) * 16384 + mn * 128 + ((((k & 15) >> 1) ^ (mn & 7)) << 4) + ((k & 1) << 3));
-}
-
-ZB_DEVICE void lds2(uint32_t addr, double& x, double& y) {
-    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n" : "=d"(x), "=d"(y) : "r"(addr));
-}
-ZB_DEVICE double lds1(uint32_t addr) {
-    double x;
-    asm volatile("ld.shared.f64 %0, [%1];\n" : "=d"(x) : "r"(addr));
-    return x;
 }
 
 // A_MN: op(A) is stored m-contiguous (transa 'N'); B_K: op(B) is stored
@@ -107,9 +106,10 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     __syncthreads();
     const WaitCtl W{abort_flag, nullptr, P.report, P.wait_ns};
 
-    if (warp == kTMathWarps) {
+    if (warp >= kTMathWarps) {
         // ------------------------------------------------------ TMA producer
-        if (lane == 0) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kTProducerRegs));
+        if (warp == kTMathWarps && lane == 0) {
             Issued issued;
             bool ok = true;
             int s = 0;
@@ -146,6 +146,7 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     }
 
     // ---------------------------------------------------------- math warps
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kTMathRegs));
     const int wm = (warp >> 2) * kTWM, wn = (warp & 3) * kTWN;
     const int g = lane >> 2, t = lane & 3;
     double acc[4][4][4];
@@ -169,43 +170,49 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int v = 0; v < 2; ++v)
-            b_off[j][v] = B_K ? k_major_off(wn + 8 * j + g, 2 * t) : mn_major_off(wn + 8 * j + g, 2 * t + v);
+            b_off[j][v] = B_K ? k_major_off(wn + 8 * j + ((g >> 1) | ((g & 1) << 2)), 2 * t)
+                              : mn_major_off(wn + 8 * j + g, 2 * t + v);
 
     bool ok = true;
     int s = 0;
     uint32_t ph = 0;
     for (int kt = 0; kt < KT; ++kt) {
         if (!(ok = wait_phase(&full[s], ph, W, WAIT_MMA_FULL_A))) break;
-        const uint32_t sa = smem_u32(smem + s * kTStageBytes), sb = sa + kTOpBytes;
-#pragma unroll
+        const uint8_t* sa = smem + s * kTStageBytes;
+        const uint8_t* sb = sa + kTOpBytes;
+        // one k8 step per iteration (deeper unrolling spilled and measured up to 0.7 % slower)
+#pragma unroll 1
         for (int ks = 0; ks < kTBK; ks += 8) {
-            // step offset: MN-major tiles advance 8 rows (1 KB); K-major tiles
-            // advance 8 k, i.e. 64 B within a 16-k box, or the next box
-            const uint32_t ka = A_MN ? ks * 128 : (ks >> 4) * 16384 + (((ks & 15) >> 1) << 4);
-            const uint32_t kbo = B_K ? (ks >> 4) * 16384 + (((ks & 15) >> 1) << 4) : ks * 128;
+            // k8 step ks: MN-major tiles advance 8 rows of 128 B; K-major tiles
+            // move 4 chunks within a 16-k box (an XOR on the chunk index, as
+            // t < 4) and to the second box from ks = 16
+            const uint32_t mn_step = ks * 128;
+            const uint32_t k_xor = ((ks & 15) >> 1) << 4, k_box = (ks >> 4) * 16384;
             double af[4][4], bf[4][2];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if (A_MN) {
-                    lds2(sa + a_off[i][0] + ka, af[i][0], af[i][1]);  // a[0], a[1]: rows 2g, 2g+1, k 2t
-                    lds2(sa + a_off[i][1] + ka, af[i][2], af[i][3]);  // a[2], a[3]: k 2t+1
+                    // a[0], a[1]: rows 2g, 2g+1 at k 2t; a[2], a[3]: at k 2t+1
+                    const double2 p0 = *reinterpret_cast<const double2*>(sa + a_off[i][0] + mn_step);
+                    const double2 p1 = *reinterpret_cast<const double2*>(sa + a_off[i][1] + mn_step);
+                    af[i][0] = p0.x, af[i][1] = p0.y, af[i][2] = p1.x, af[i][3] = p1.y;
                 } else {
-                    // K-major: the swizzle XOR of chunk (ks/2 + t) is taken on the chunk index,
-                    // so the step offset is applied inside the XOR
-                    lds2(sa + (a_off[i][0] ^ (((ks & 15) >> 1) << 4)) + (ks >> 4) * 16384, af[i][0], af[i][2]);
-                    lds2(sa + (a_off[i][1] ^ (((ks & 15) >> 1) << 4)) + (ks >> 4) * 16384, af[i][1], af[i][3]);
+                    // a[0], a[2]: row 2g at k 2t, 2t+1; a[1], a[3]: row 2g+1
+                    const double2 p0 = *reinterpret_cast<const double2*>(sa + ((a_off[i][0] ^ k_xor) + k_box));
+                    const double2 p1 = *reinterpret_cast<const double2*>(sa + ((a_off[i][1] ^ k_xor) + k_box));
+                    af[i][0] = p0.x, af[i][2] = p0.y, af[i][1] = p1.x, af[i][3] = p1.y;
                 }
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (B_K) {
-                    lds2(sb + (b_off[j][0] ^ (((ks & 15) >> 1) << 4)) + (ks >> 4) * 16384, bf[j][0], bf[j][1]);
+                    const double2 q = *reinterpret_cast<const double2*>(sb + ((b_off[j][0] ^ k_xor) + k_box));
+                    bf[j][0] = q.x, bf[j][1] = q.y;
                 } else {
-                    bf[j][0] = lds1(sb + b_off[j][0] + kbo);
-                    bf[j][1] = lds1(sb + b_off[j][1] + kbo);
+                    bf[j][0] = *reinterpret_cast<const double*>(sb + b_off[j][0] + mn_step);
+                    bf[j][1] = *reinterpret_cast<const double*>(sb + b_off[j][1] + mn_step);
                 }
             }
-            (void)ka;
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -220,8 +227,9 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     }
     if (!ok || *abort_flag) return;  // an incomplete sum is never written
 
-    // Epilogue: c[v0 + 2 v1] holds physical row 2 g + v1, column 2 t + v0 of the
-    // fragment.  The beta * C reads of a fragment row are issued before its stores.
+    // Epilogue: c[v0 + 2 v1] holds physical row 2 g + v1 and column 2 t + v0 of
+    // the fragment (K-major op(B): column t + 4 v0).  The beta * C reads of a
+    // fragment row are issued before its stores.
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         double cin[4][4];
@@ -231,7 +239,7 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     const int row = m0 + wm + 16 * i + 2 * g + (v >> 1);
-                    const int col = n0 + wn + 8 * j + 2 * t + (v & 1);
+                    const int col = n0 + wn + 8 * j + (B_K ? t + 4 * (v & 1) : 2 * t + (v & 1));
                     const bool in_tri = P.tri == 0 || (P.tri == 1 ? row <= col : row >= col);
                     cin[j][v] = (row < P.M && col < P.N && in_tri) ? P.C[(long)col * P.ldc + row] : 0.0;
                 }
@@ -241,7 +249,7 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 const int row = m0 + wm + 16 * i + 2 * g + (v >> 1);
-                const int col = n0 + wn + 8 * j + 2 * t + (v & 1);
+                const int col = n0 + wn + 8 * j + (B_K ? t + 4 * (v & 1) : 2 * t + (v & 1));
                 const bool in_tri = P.tri == 0 || (P.tri == 1 ? row <= col : row >= col);
                 if (row < P.M && col < P.N && in_tri) {
                     if (PARTIAL) {

@@ -79,6 +79,13 @@ size_t sgemm_native_workspace_bytes(char transa, char transb, int m, int n, int 
 // staged once per persistent CTA, op(A) streamed in 128-row blocks.
 bool skinny_gemm_applies(int m, int n, int k, int tri);
 cudaError_t dgemm_skinny(const GemmArgsF64& g, cudaStream_t st);
+// FP64 tall-skinny route on TMA-fed op(A) row blocks (gemm_skinny_tma.cu): for a
+// 16-byte aligned op(A) with an even leading dimension.
+bool dgemm_skinny_tma_applies(const GemmArgsF64& g);
+cudaError_t dgemm_skinny_tma(const GemmArgsF64& g, cudaStream_t st);
+// FP32 tall-skinny route on TMA-fed op(A) row blocks: 16-byte aligned op(A), lda a multiple of 4.
+bool sgemm_skinny_tma_applies(const GemmArgsF32& g);
+cudaError_t sgemm_skinny_tma(const GemmArgsF32& g, cudaStream_t st);
 cudaError_t sgemm_skinny(const GemmArgsF32& g, cudaStream_t st);
 size_t sgemm_native_workspace_bound(int m, int n, int k, int sm_count);
 // Vector-edge route (n == 1 or m == 1, no triangle mode): HBM-bound

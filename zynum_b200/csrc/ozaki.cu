@@ -432,11 +432,15 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             Ring ra, rb;
             uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
             bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
+            int inst = 0;
             for (int tile = blockIdx.x; ok && tile < P.num_tiles; tile += gridDim.x)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         // the job's accumulators must have been drained by the epilogue
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                        // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
+                        // so a tile's epilogue overlaps the next tile's products
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                        ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
                         tc_fence_after();
@@ -450,7 +454,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         auto commit = [](uint64_t* bar) { umma_commit(bar); };
                         ok = mma_job<kASlots, kBSlots, kAChunk, kBChunk>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
-                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, W, mma, commit);
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base + (EPI == EPI_F32 ? b * kUN : 0), W, mma,
+                            commit);
                         if (ok) umma_commit(&tfull[b]);
                     }
             if (!ok) {
@@ -468,6 +473,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
         double* colscale = reinterpret_cast<double*>(smem_tail_scratch(smem));  // kUN doubles
         uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
+        int inst = 0;  // accumulator instances, in the MMA issuer's order
         bool ok = true;
         for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x) {
             int tm, tn;
@@ -494,7 +500,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                    ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
@@ -521,7 +528,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll 1
                     for (int ch = 0; ch < kUN / 32; ++ch) {
                         uint32_t r0[32], r1[32];
-                        tmem_ld_32x32b_x32(lane_addr + ch * 32, r0);
+                        tmem_ld_32x32b_x32(lane_addr + (EPI == EPI_F32 ? b * kUN : 0) + ch * 32, r0);
                         if (two) tmem_ld_32x32b_x32(lane_addr + kUN + ch * 32, r1);
                         tmem_ld_wait();
                         const int col0 = tn * kUN + ch * 32;
@@ -566,7 +573,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     }
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(&tempty[0]);
+                    if (lane == 0) mbar_arrive(&tempty[b]);
                     first = false;
                 }
         }
@@ -672,28 +679,31 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             Issued is;
             bool ok = true;
             const int steps = P.k_chunks / 2;  // 256-byte K steps (K padded to 256)
-            // modulus-major: every tile of modulus l before modulus l + 1, so the
-            // running pairs share one modulus' planes in L2
-            for (int j = 0; ok && j < P.num_jobs; ++j)
-                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs) {
-                    int tm, tn;
-                    tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
-                    const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
-                    const int l = P.job_shift[j][0];
-                    for (int ks = 0; ks < steps; ++ks) {
-                        if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, W, WAIT_PRODUCER_EMPTY_A))) break;
-                        const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
-                        const uint32_t bar = smem_u32(&fullA[rs.slot]) & 0xFEFFFFFFu;
-                        if (leader) mbar_arrive_expect_tx(&fullA[rs.slot], 2 * kCrtSlot);
-                        const int x = ks * 2 * kChunkBytes;
-                        tma_load_2d_2sm(base, &tmA, bar, x, l * P.m_pad + arow);
-                        tma_load_2d_2sm(base + kCrtAtom, &tmA, bar, x + kChunkBytes, l * P.m_pad + arow);
-                        tma_load_2d_2sm(base + 2 * kCrtAtom, &tmB, bar, x, l * P.n_pad + brow);
-                        tma_load_2d_2sm(base + 3 * kCrtAtom, &tmB, bar, x + kChunkBytes, l * P.n_pad + brow);
-                        is.note(rs.slot, rs.phase);
-                        rs.advance(kCrtSlots);
-                    }
+            // modulus-major over one flat sequence q = (modulus, tile), dealt
+            // round-robin to the pairs: every pair gets the same number of
+            // items (within one), so the running pairs stay on neighbouring
+            // tiles of one modulus and share its planes in L2 (a per-modulus
+            // deal of 13 or 14 tiles let the pairs drift moduli apart)
+            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs) {
+                const int j = q / P.num_tiles, tile = q - j * P.num_tiles;
+                int tm, tn;
+                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
+                const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
+                const int l = P.job_shift[j][0];
+                for (int ks = 0; ks < steps; ++ks) {
+                    if (!(ok = wait_phase(&emptyA[rs.slot], rs.phase ^ 1, W, WAIT_PRODUCER_EMPTY_A))) break;
+                    const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
+                    const uint32_t bar = smem_u32(&fullA[rs.slot]) & 0xFEFFFFFFu;
+                    if (leader) mbar_arrive_expect_tx(&fullA[rs.slot], 2 * kCrtSlot);
+                    const int x = ks * 2 * kChunkBytes;
+                    tma_load_2d_2sm(base, &tmA, bar, x, l * P.m_pad + arow);
+                    tma_load_2d_2sm(base + kCrtAtom, &tmA, bar, x + kChunkBytes, l * P.m_pad + arow);
+                    tma_load_2d_2sm(base + 2 * kCrtAtom, &tmB, bar, x, l * P.n_pad + brow);
+                    tma_load_2d_2sm(base + 3 * kCrtAtom, &tmB, bar, x + kChunkBytes, l * P.n_pad + brow);
+                    is.note(rs.slot, rs.phase);
+                    rs.advance(kCrtSlots);
                 }
+            }
             if (ok) {
                 for (int i = 0; i < kCrtSlots; ++i) {
                     wait_phase(&emptyA[rs.slot], rs.phase ^ 1, W, 0);
@@ -714,32 +724,31 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
             const int steps = P.k_chunks / 2;
             int inst = 0;  // job instances alternate between the two accumulators
-            for (int j = 0; ok && j < P.num_jobs; ++j)
-                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs, ++inst) {
-                    const int b = inst & 1;
-                    if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
-                    tphase ^= 1u << b;
-                    tc_fence_after();
-                    const uint32_t d = tmem_base + b * kUN;
-                    for (int ks = 0; ks < steps; ++ks) {
-                        if (!(ok = wait_phase(&fullA[rs.slot], rs.phase, W, WAIT_MMA_FULL_A))) break;
-                        const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
-                        const uint64_t a0 = umma_desc_sw128(base), a1 = umma_desc_sw128(base + kCrtAtom);
-                        const uint64_t b0 = umma_desc_sw128(base + 2 * kCrtAtom);
-                        const uint64_t b1 = umma_desc_sw128(base + 3 * kCrtAtom);
-                        umma_i8_2sm(d, a0, b0, idesc, ks > 0 ? 1u : 0u);
-                        umma_i8_2sm(d, a0 + 2, b0 + 2, idesc, 1u);
-                        umma_i8_2sm(d, a0 + 4, b0 + 4, idesc, 1u);
-                        umma_i8_2sm(d, a0 + 6, b0 + 6, idesc, 1u);
-                        umma_i8_2sm(d, a1, b1, idesc, 1u);
-                        umma_i8_2sm(d, a1 + 2, b1 + 2, idesc, 1u);
-                        umma_i8_2sm(d, a1 + 4, b1 + 4, idesc, 1u);
-                        umma_i8_2sm(d, a1 + 6, b1 + 6, idesc, 1u);
-                        umma_commit_2sm(&emptyA[rs.slot], 0x3);
-                        rs.advance(kCrtSlots);
-                    }
-                    if (ok) umma_commit_2sm(&tfull[b], 0x3);
+            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs, ++inst) {
+                const int b = inst & 1;
+                if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
+                tphase ^= 1u << b;
+                tc_fence_after();
+                const uint32_t d = tmem_base + b * kUN;
+                for (int ks = 0; ks < steps; ++ks) {
+                    if (!(ok = wait_phase(&fullA[rs.slot], rs.phase, W, WAIT_MMA_FULL_A))) break;
+                    const uint32_t base = smem_u32(smem) + rs.slot * kCrtSlot;
+                    const uint64_t a0 = umma_desc_sw128(base), a1 = umma_desc_sw128(base + kCrtAtom);
+                    const uint64_t b0 = umma_desc_sw128(base + 2 * kCrtAtom);
+                    const uint64_t b1 = umma_desc_sw128(base + 3 * kCrtAtom);
+                    umma_i8_2sm(d, a0, b0, idesc, ks > 0 ? 1u : 0u);
+                    umma_i8_2sm(d, a0 + 2, b0 + 2, idesc, 1u);
+                    umma_i8_2sm(d, a0 + 4, b0 + 4, idesc, 1u);
+                    umma_i8_2sm(d, a0 + 6, b0 + 6, idesc, 1u);
+                    umma_i8_2sm(d, a1, b1, idesc, 1u);
+                    umma_i8_2sm(d, a1 + 2, b1 + 2, idesc, 1u);
+                    umma_i8_2sm(d, a1 + 4, b1 + 4, idesc, 1u);
+                    umma_i8_2sm(d, a1 + 6, b1 + 6, idesc, 1u);
+                    umma_commit_2sm(&emptyA[rs.slot], 0x3);
+                    rs.advance(kCrtSlots);
                 }
+                if (ok) umma_commit_2sm(&tfull[b], 0x3);
+            }
             if (!ok) {
                 // aborted: wait for the MMAs already issued before TMEM and the ring are released
                 umma_commit_2sm(drain_bar, 0x1);
@@ -808,10 +817,14 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             Ring ra, rb;
             uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
             bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
+            int inst = 0;
             for (int tile = pair; ok && tile < P.num_tiles; tile += npairs)
                 for (int j = 0; ok && j < P.num_jobs; ++j)
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                        // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
+                        // so a tile's epilogue overlaps the next tile's products
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                        ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
                         tc_fence_after();
@@ -825,7 +838,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                         auto commit = [](uint64_t* bar) { umma_commit_2sm(bar, 0x3); };
                         ok = mma_job<kSlots2, kSlots2, kChunk2, kChunk2>(
                             sched->flags + P.job_first_step[j], P.job_num_steps[j], c0, c1, ra, rb, fullA, fullB,
-                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base, W, mma, commit);
+                            emptyA, emptyB, smem_u32(sA), smem_u32(sB), tmem_base + (EPI == EPI_F32 ? b * kUN : 0), W, mma,
+                            commit);
                         if (ok) umma_commit_2sm(&tfull[b], 0x3);
                     }
             if (!ok) {
@@ -841,32 +855,33 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const uint32_t tempty_cta0 = mapa_shared(smem_u32(&tempty[0]), 0);  // buffer b: + 8 b
         uint32_t tphase = 0;  // bit b: phase parity of accumulator buffer b
+        int inst = 0;  // accumulator instances, in the MMA issuer's order
         bool ok = true;
         if (EPI == EPI_RESIDUE) {
             // modulus-major, in the order of the MMA issuer
             int inst = 0;
-            for (int j = 0; ok && j < P.num_jobs; ++j)
-                for (int tile = pair; ok && tile < P.num_tiles; tile += npairs, ++inst) {
-                    int tm, tn;
-                    tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
-                    const int b = inst & 1;
-                    if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
-                    tphase ^= 1u << b;
-                    tc_fence_after();
-                    const int row = tm * 256 + row_in_tile;
-                    int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
-                                  (long)tn * kUN;
+            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs, ++inst) {
+                const int j = q / P.num_tiles, tile = q - j * P.num_tiles;
+                int tm, tn;
+                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
+                const int b = inst & 1;
+                if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
+                tphase ^= 1u << b;
+                tc_fence_after();
+                const int row = tm * 256 + row_in_tile;
+                int8_t* dst = P.residues + (long)P.job_shift[j][0] * P.res_plane + (long)row * P.n_pad +
+                              (long)tn * kUN;
 #pragma unroll 1
-                    for (int ch = 0; ch < kUN / 32; ++ch) {
-                        uint32_t r0[32];
-                        tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
-                        tmem_ld_wait();
-                        residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
-                    }
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
+                for (int ch = 0; ch < kUN / 32; ++ch) {
+                    uint32_t r0[32];
+                    tmem_ld_32x32b_x32(lane_addr + b * kUN + ch * 32, r0);
+                    tmem_ld_wait();
+                    residue_chunk(r0, P.job_shift[j][0], dst + ch * 32);
                 }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
+            }
         }
         for (int tile = pair; EPI != EPI_RESIDUE && tile < P.num_tiles; tile += npairs) {
             int tm, tn;
@@ -890,7 +905,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : 0;
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                    ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
                     tc_fence_after();
@@ -899,7 +915,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
 #pragma unroll 1
                     for (int ch = 0; ch < kUN / 32; ++ch) {
                         uint32_t r0[32], r1[32];
-                        tmem_ld_32x32b_x32(lane_addr + ch * 32, r0);
+                        tmem_ld_32x32b_x32(lane_addr + (EPI == EPI_F32 ? b * kUN : 0) + ch * 32, r0);
                         if (two) tmem_ld_32x32b_x32(lane_addr + kUN + ch * 32, r1);
                         tmem_ld_wait();
                         const int col0 = tn * kUN + ch * 32;
@@ -942,7 +958,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     }
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive_cluster(tempty_cta0);
+                    if (lane == 0) mbar_arrive_cluster(tempty_cta0 + 8u * b);
                     first = false;
                 }
         }
@@ -1885,7 +1901,12 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     // CTA pair, modulus-major: bands of tile-rows whose A rows of one modulus
     // (band x 256 rows x k_pad bytes) stay within ~48 MB of L2 while the band
     // sweeps the tile-columns
-    P.band_rows = (int)std::max(1L, std::min<long>(P.tiles_m, (48L << 20) / (256L * p.k_pad)));
+    static const long band_bytes = [] {
+        const char* v = std::getenv("ZYNUM_GPU_CRT_BAND_MB");
+        const long mb = v ? std::atol(v) : 48;
+        return (mb >= 4 && mb <= 120 ? mb : 48) << 20;
+    }();
+    P.band_rows = (int)std::max(1L, std::min<long>(P.tiles_m, band_bytes / (256L * p.k_pad)));
     if ((e = set_wait_params(P, p.hold)) != cudaSuccess) return e;
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
