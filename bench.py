@@ -37,9 +37,9 @@ FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12  # 64 DFMA/clk/SM at the 1965 M
 FP32_NOMINAL_TFLOPS = 148 * 256 * 1.965e9 / 1e12  # 128 FFMA/clk/SM at the 1965 MHz max clock
 METRIC = "DGEMM TFLOP/s @8192^3: Ozaki-emulated vs native FP64 at equal error; batch GFLOP/s"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel on the
-# 8192^3 headline workload, from one-pass ncu captures of this script's default run:
-# CRT modular-product GEMM 11.76 GB + 1.07 GB; native DMMA DGEMM 15.80 GB + 0.53 GB.
-TRAFFIC_8192 = {"crt": 11.76e9 + 1.07e9, "native": 15.80e9 + 0.53e9}
+# 8192^3 headline workload, one launch each in one-pass ncu captures (profiles/ozaki_crt_umma_gemm_dram_8192.md):
+# CRT modular-product GEMM 5.38 GB + 1.06 GB; native TMA DGEMM 15.82 GB + 0.53 GB.
+TRAFFIC_8192 = {"crt": 5.38e9 + 1.06e9, "native": 15.82e9 + 0.53e9}
 
 
 def _peaks():
@@ -343,7 +343,8 @@ def time_device(torch, fn, steps, warmup, stream):
 def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
     """The rest of the precision configuration on the headline size: DGEMM with
     entries u * 10^e, e ~ U[-phi, phi], for phi = 4 and 8, Ozaki and native on the
-    same inputs; SGEMM as a 3xBF16 split product and native FP32 on U[-1, 1] data.
+    same inputs; SGEMM as a 3xBF16 and a 6xBF16 (FP32-accurate) split product and
+    native FP32 on U[-1, 1] data.
     Each: time per call (CUDA events, inputs resident) and max / median relative
     error against the double-double oracle on 2048 sampled entries."""
     dev = torch.device("cuda")
@@ -371,7 +372,8 @@ def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
     C = torch.zeros((n, n), dtype=torch.float32, device=dev)
     a_h = np.asfortranarray(A.cpu().numpy().T.astype(np.float64))
     b_h = np.asfortranarray(B.cpu().numpy().T.astype(np.float64))
-    for name, mid in (("sgemm_bf16x3", blas.SMETHOD_BF16X3), ("sgemm_native", blas.SMETHOD_NATIVE)):
+    for name, mid in (("sgemm_bf16x3", blas.SMETHOD_BF16X3), ("sgemm_bf16x6", blas.SMETHOD_BF16X6),
+                      ("sgemm_native", blas.SMETHOD_NATIVE)):
         blas.set_sgemm_method(mid)
         fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
         ms = time_device(torch, fn, steps, warmup, stream)
@@ -383,6 +385,64 @@ def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
     blas.set_sgemm_method(blas.SMETHOD_NATIVE)
     del A, B, C
     return out
+
+
+def sweep_subset(torch, blas, stream, peaks, steps, warmup):
+    """The shape-sweep rows the default line carries (each a few ms of work):
+    tall-skinny 131072 x 64 x 64 FP64 / FP32 at beta 0 and 1 with achieved HBM GB/s
+    against the measured copy bandwidth and the compute bound of the pipe it uses;
+    K-dominant 256 x 256 x 262144 FP64 (split K); ZGEMM / CGEMM 4096^3 (4M and 3M)."""
+    rows = []
+    hbm = peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    for dt, tdt, fn, pipe in (("f64", torch.float64, blas.dgemm_device, FP64_NOMINAL_TFLOPS),
+                              ("f32", torch.float32, blas.sgemm_device, FP32_NOMINAL_TFLOPS)):
+        m, n, k = 131072, 64, 64
+        g = torch.Generator(device="cuda").manual_seed(7)
+        A = torch.rand((k, m), generator=g, device="cuda", dtype=tdt) * 2 - 1
+        B = torch.rand((n, k), generator=g, device="cuda", dtype=tdt) * 2 - 1
+        C = torch.rand((n, m), generator=g, device="cuda", dtype=tdt) * 2 - 1
+        esz = 8 if dt == "f64" else 4
+        for beta in (0.0, 1.0):
+            f = lambda: fn("N", "N", m, n, k, 1.0, A, m, B, k, beta, C, m)  # noqa: E731
+            ms = time_device(torch, f, max(20, steps), max(5, warmup), stream)
+            byts = esz * (m * k + k * n + m * n * (2 if beta else 1))
+            t_hbm = byts / (hbm * 1e9) * 1e3
+            t_pipe = 2.0 * m * n * k / (pipe * 1e12) * 1e3
+            rows.append({"shape": "tall-skinny", "dtype": dt, "m": m, "n": n, "k": k, "beta": beta, "ms": ms,
+                         "gbs": byts / (ms * 1e-3) / 1e9, "frac_of_measured_hbm": byts / (ms * 1e-3) / 1e9 / hbm,
+                         "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12,
+                         "bound": "hbm" if t_hbm >= t_pipe else ("fp64 dmma" if dt == "f64" else "fp32 ffma"),
+                         "frac_of_bound": max(t_hbm, t_pipe) / ms})
+        del A, B, C
+    m, n, k = 256, 256, 262144
+    g = torch.Generator(device="cuda").manual_seed(8)
+    A = torch.rand((k, m), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    B = torch.rand((n, k), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    C = torch.zeros((n, m), device="cuda", dtype=torch.float64)
+    f = lambda: blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+    ms = time_device(torch, f, max(5, steps // 2), max(3, warmup), stream)
+    tf = 2.0 * m * n * k / (ms * 1e-3) / 1e12
+    rows.append({"shape": "K-dominant", "dtype": "f64", "m": m, "n": n, "k": k, "beta": 0.0, "ms": ms, "tflops": tf,
+                 "bound": "fp64 dmma", "frac_of_bound": tf / FP64_NOMINAL_TFLOPS})
+    del A, B, C
+    for dt, tdt, fn, real in (("z", torch.complex128, blas.zgemm_device, torch.float64),
+                              ("c", torch.complex64, blas.cgemm_device, torch.float32)):
+        nn = 4096
+        g = torch.Generator(device="cuda").manual_seed(5)
+        A = torch.complex(torch.rand((nn, nn), generator=g, device="cuda", dtype=real) * 2 - 1,
+                          torch.rand((nn, nn), generator=g, device="cuda", dtype=real) * 2 - 1)
+        B = torch.complex(torch.rand((nn, nn), generator=g, device="cuda", dtype=real) * 2 - 1,
+                          torch.rand((nn, nn), generator=g, device="cuda", dtype=real) * 2 - 1)
+        C = torch.zeros((nn, nn), device="cuda", dtype=tdt)
+        for cm, cname in ((blas.COMPLEX_4M, "4M"), (blas.COMPLEX_3M, "3M")):
+            old = blas.set_complex_method(cm)
+            f = lambda: fn("N", "N", nn, nn, nn, 1.0, A, nn, B, nn, 0.0, C, nn)  # noqa: E731
+            ms = time_device(torch, f, max(3, steps // 4), max(3, warmup), stream)
+            blas.set_complex_method(old)
+            rows.append({"shape": "square", "dtype": dt, "method": cname, "m": nn, "n": nn, "k": nn, "ms": ms,
+                         "tflops": 8.0 * nn ** 3 / (ms * 1e-3) / 1e12, "note": "8mnk flops"})
+        del A, B, C
+    return rows
 
 
 def _ozaki_desc(n):
@@ -556,6 +616,8 @@ def run_ours(args, rank, world, local_rank):
         line["methods"].update(extra)
         line["config"]["precision"] = ("methods: ozaki / native at phi = 0 (headline), 4, 8 on the same inputs per "
                                        "phi; sgemm_bf16x3 / sgemm_native on U[-1,1]; errors vs double-double")
+    if not args.no_sweep:
+        line["sweep"] = sweep_subset(torch, blas, stream, peaks, args.steps, args.warmup)
     if not args.no_batched:
         line["batched"] = bench_batched(torch, blas, max(3, args.steps), args.warmup)
         line["differentiation"] = bench_differentiation(torch, max(3, args.steps), args.warmup)
@@ -602,7 +664,8 @@ def suite_precision(args):
     C = torch.zeros((n, n), dtype=torch.float32, device="cuda")
     a_h = np.asfortranarray(A.cpu().numpy().T)
     b_h = np.asfortranarray(B.cpu().numpy().T)
-    for name, mid in (("native_fp32", blas.SMETHOD_NATIVE), ("bf16x3", blas.SMETHOD_BF16X3)):
+    for name, mid in (("native_fp32", blas.SMETHOD_NATIVE), ("bf16x3", blas.SMETHOD_BF16X3),
+                      ("bf16x6", blas.SMETHOD_BF16X6)):
         blas.set_sgemm_method(mid)
         fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
         ms = time_device(torch, fn, args.steps, args.warmup, stream)
@@ -781,6 +844,28 @@ def suite_level3(args):
                      "tflops": float(r) * r * nn / (ms * 1e-3) / 1e12})
         blas.set_dgemm_method(old)
         del L, Lc, B, X, C
+    # complex rank-k / rank-2k updates, n = k = 4096: ZHERK / ZSYRK form one triangle of the
+    # product (useful flops 4 n^2 k), ZHER2K / ZSYR2K the full n x n product W (8 n^2 k)
+    nc = 4096
+    g = torch.Generator(device="cuda").manual_seed(13)
+    A = torch.complex(torch.rand((nc, nc), generator=g, device="cuda", dtype=torch.float64) * 2 - 1,
+                      torch.rand((nc, nc), generator=g, device="cuda", dtype=torch.float64) * 2 - 1)
+    B = A.flip(0).contiguous()
+    C = torch.zeros((nc, nc), device="cuda", dtype=torch.complex128)
+    for cname, cm in (("4M", blas.COMPLEX_4M), ("3M", blas.COMPLEX_3M)):
+        old = blas.set_complex_method(cm)
+        ops = {
+            "zherk": (lambda: blas.herk_device("L", "N", nc, nc, 1.0, A, nc, 0.0, C, nc), 4.0 * nc ** 3),
+            "zsyrk": (lambda: blas.syrk_device_c("L", "N", nc, nc, 1.0, A, nc, 0.0, C, nc), 4.0 * nc ** 3),
+            "zher2k": (lambda: blas.syr2k_device_c("L", "N", nc, nc, 1.0, A, nc, B, nc, 0.0, C, nc, herm=True),
+                       8.0 * nc ** 3),
+        }
+        for name, (fn, flops) in ops.items():
+            ms = time_device(torch, fn, max(3, min(args.steps, 5)), max(3, args.warmup), stream)
+            rows.append({"op": name, "dtype": "z", "method": cname, "n": nc, "k": nc, "ms": ms,
+                         "tflops": flops / (ms * 1e-3) / 1e12})
+        blas.set_complex_method(old)
+    del A, B, C
     print(json.dumps({"suite": "level3", "rows": rows}), flush=True)
     return 0
 
@@ -797,7 +882,7 @@ def suite_batched(args):
 
 def suite_one(args):
     """One GEMM shape, for profiling a single kernel: --dtype f64|f32|z|c, --m/--n/--k,
-    --method (native or ozaki for f64; ozaki means 3xBF16 for f32), beta 0, NN,
+    --method (native or ozaki for f64; ozaki means 3xBF16 for f32), --beta, NN,
     column-major U[-1,1] inputs; `--warmup` untimed calls, then `--steps` timed ones."""
     import torch
     from zynum_b200 import blas
@@ -817,18 +902,19 @@ def suite_one(args):
     C = torch.zeros((n, m), device="cuda", dtype=tdt)
     if dt == "f64":
         blas.set_dgemm_method(blas.METHOD_OZAKI if args.method == "ozaki" else blas.METHOD_NATIVE)
-        fn = lambda: blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+        fn = lambda: blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, args.beta, C, m)  # noqa: E731
     elif dt == "f32":
         blas.set_sgemm_method(blas.SMETHOD_BF16X3 if args.method == "ozaki" else blas.SMETHOD_NATIVE)
-        fn = lambda: blas.sgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+        fn = lambda: blas.sgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, args.beta, C, m)  # noqa: E731
     else:
         f = blas.zgemm_device if dt == "z" else blas.cgemm_device
-        fn = lambda: f("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)  # noqa: E731
+        fn = lambda: f("N", "N", m, n, k, 1.0, A, m, B, k, args.beta, C, m)  # noqa: E731
     ms = time_device(torch, fn, args.steps, args.warmup, torch.cuda.current_stream())
     flop = (8.0 if dt in ("z", "c") else 2.0) * m * n * k
     esz = C.element_size()
-    byts = esz * (m * k + k * n + m * n)
-    print(json.dumps({"suite": "one", "dtype": dt, "m": m, "n": n, "k": k, "method": args.method, "ms": ms,
+    byts = esz * (m * k + k * n + m * n * (2 if args.beta else 1))
+    print(json.dumps({"suite": "one", "dtype": dt, "m": m, "n": n, "k": k, "beta": args.beta, "method": args.method,
+                      "ms": ms,
                       "tflops": flop / (ms * 1e-3) / 1e12, "gbs": byts / (ms * 1e-3) / 1e9}), flush=True)
     return 0
 
@@ -846,10 +932,12 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the phi = 4 / 8 and SGEMM methods")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the tall-skinny / K-dominant / complex rows")
     ap.add_argument("--dtype", choices=["f64", "f32", "z", "c"], default="f64", help="suite one: element type")
     ap.add_argument("--m", type=int, default=4096, help="suite one: rows of C")
     ap.add_argument("--n", type=int, default=4096, help="suite one: columns of C")
     ap.add_argument("--k", type=int, default=4096, help="suite one: inner dimension")
+    ap.add_argument("--beta", type=float, default=0.0, help="suite one: beta")
     ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched", "one"],
                     default="headline", help="secondary measurement suites (one JSON line each)")
     ap.add_argument("--batch-count", type=int, default=20000,

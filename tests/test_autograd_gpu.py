@@ -122,3 +122,21 @@ def test_gemm_and_syrk_gradcheck():
     X = torch.randn(40, 12, generator=g, dtype=torch.float64).cuda().requires_grad_(True)
     assert torch.autograd.gradcheck(lambda x: ag.syrk(x, True, 0.75), (X,), eps=1e-6, atol=1e-7)
     assert torch.autograd.gradcheck(lambda x: ag.syrk(x, False), (X,), eps=1e-6, atol=1e-7)
+
+
+def test_auto_recompute_follows_free_memory(monkeypatch):
+    """recompute="auto": X is kept when it is small against the free device memory and
+    recomputed when it is not; the gradients agree either way."""
+    import torch
+    from zynum_b200 import autograd as ag
+    L, B = _chain_inputs(torch, 256, 32, 5)
+    grads = {}
+    for free, expect in ((1 << 40, False), (256 * 32 * 8, True)):
+        monkeypatch.setattr(torch.cuda, "mem_get_info", lambda device=None, f=free: (f, 1 << 40))
+        Lr, Br = L.clone().requires_grad_(True), B.clone().requires_grad_(True)
+        x = ag.trsm(Lr, Br)  # recompute="auto"
+        assert x.grad_fn.recompute is expect
+        torch.sin(ag.syrk(x)).sum().backward()
+        grads[expect] = (Lr.grad, Br.grad)
+    assert torch.allclose(grads[False][0], grads[True][0], rtol=1e-12, atol=1e-14)
+    assert torch.allclose(grads[False][1], grads[True][1], rtol=1e-12, atol=1e-14)

@@ -295,3 +295,36 @@ def test_complex_level3_device_entry_points(blas, oracle, dtype):
     assert rel(got[lo], ref[lo]) <= tol, "herk"
     assert np.all(np.diag(got).imag == 0)
     assert np.array_equal(got[~lo], c[~lo])
+
+
+@pytest.mark.parametrize("method", ["4M", "3M"])
+@pytest.mark.parametrize("uplo,trans", [("U", "N"), ("L", "C"), ("L", "T")])
+def test_herk_zsyrk_triangle_products_large(blas, oracle, method, uplo, trans):
+    """ZHERK / ZSYRK compute only the stored triangle of the product (128 x 128 real tiles in
+    triangle mode, K beyond 1024), through both complex forms; the other triangle stays untouched."""
+    rng = np.random.default_rng(_seed(uplo, trans, method))
+    n, k = 700, 1100
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = _cx(rng, (ra, ca), np.complex128)
+    tri = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    A = np.abs(a)
+    A = A if trans == "N" else A.T
+    old = blas.set_complex_method(blas.COMPLEX_3M if method == "3M" else blas.COMPLEX_4M)
+    try:
+        for herm in (True, False):
+            if not herm and trans == "C":
+                continue  # zsyrk takes N / T
+            c = _cx(rng, (n, n), np.complex128)
+            c0 = c.copy(order="F")
+            ref = c.copy(order="F")
+            if herm:
+                oracle.herk(uplo, trans, n, k, 0.75, a, ra, -0.5, ref, n)
+                blas.herk(uplo, trans, n, k, 0.75, a, ra, -0.5, c, n)
+            else:
+                oracle.syrk(uplo, trans, n, k, 0.75 - 0.25j, a, ra, -0.5 + 0.5j, ref, n)
+                blas.syrk(uplo, trans, n, k, 0.75 - 0.25j, a, ra, -0.5 + 0.5j, c, n)
+            bound = 16 * k * _u(np.complex128) * ((A @ A.T) + np.abs(c0)) + 1e-300
+            assert np.all(np.abs(c - ref)[tri] <= bound[tri]), float(np.abs(c - ref)[tri].max())
+            assert np.array_equal(c[~tri], c0[~tri]), "the other triangle changed"
+    finally:
+        blas.set_complex_method(old)

@@ -15,7 +15,10 @@ Adjoints (G = upstream gradient):
   syrk   C = alpha X^T X (trans)   dX = alpha X (G + G^T)
          C = alpha X X^T           dX = alpha (G + G^T) X
 With recompute=True the TRSM backward solves Y again from (L, B) instead of
-keeping X alive between forward and backward.
+keeping X alive between forward and backward; recompute="auto" (the default of
+trsm()) decides at forward time from the device memory still free: X is
+recomputed when keeping it until backward would take more than
+RECOMPUTE_FRACTION of the free bytes (recompute_policy).
 """
 from __future__ import annotations
 
@@ -24,6 +27,17 @@ import torch
 from . import blas
 
 _FLIP = {"U": "L", "L": "U"}
+
+# Share of the free device memory a saved TRSM output may take before the
+# backward recomputes it instead.
+RECOMPUTE_FRACTION = 0.25
+
+
+def recompute_policy(nbytes: int, free_bytes: int, fraction: float | None = None) -> bool:
+    """True when keeping `nbytes` alive from forward to backward would use more than
+    `fraction` (default RECOMPUTE_FRACTION) of the `free_bytes` the device still has."""
+    f = RECOMPUTE_FRACTION if fraction is None else fraction
+    return nbytes > f * free_bytes
 
 
 def _check(t):
@@ -106,6 +120,9 @@ class Trsm(torch.autograd.Function):
         l, b = _check(l), _check(b)
         x = b.clone()
         rm_trsm_left(uplo, trans, diag, alpha, l, x)
+        if recompute == "auto":
+            free, _ = torch.cuda.mem_get_info(x.device)
+            recompute = recompute_policy(x.numel() * x.element_size(), free)
         ctx.uplo, ctx.trans, ctx.diag, ctx.alpha, ctx.recompute = uplo, trans, diag, alpha, recompute
         if recompute:
             ctx.save_for_backward(l, b)  # X is solved again in backward
@@ -164,8 +181,8 @@ def gemm(a, b, alpha=1.0):
     return Gemm.apply(a, b, alpha)
 
 
-def trsm(l, b, uplo="L", trans="N", diag="N", alpha=1.0, recompute=False):
-    """X = alpha op(L)^-1 B (left side)."""
+def trsm(l, b, uplo="L", trans="N", diag="N", alpha=1.0, recompute="auto"):
+    """X = alpha op(L)^-1 B (left side); recompute True / False / "auto" (from free device memory)."""
     return Trsm.apply(l, b, uplo, trans, diag, alpha, recompute)
 
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -118,11 +119,12 @@ template <typename Scratch>
 cudaError_t run_sgemm(const GemmArgsF32& g, cudaStream_t st, Scratch scratch) {
     Context& cx = context();
     if (g.k == 0 || g.alpha == 0.0f) return scale_matrix<float>(g.m, g.n, g.beta, g.c, g.ldc, st);
-    if (cx.sgemm_method == SMETHOD_BF16X3) {
+    if (cx.sgemm_method == SMETHOD_BF16X3 || cx.sgemm_method == SMETHOD_BF16X6) {
+        const int terms = cx.sgemm_method == SMETHOD_BF16X6 ? 3 : 2;
         void* ws = nullptr;
-        cudaError_t e = scratch(bf16x3_workspace_bytes(g.m, g.n, g.k), st, &ws);
+        cudaError_t e = scratch(bf16_split_workspace_bytes(g.m, g.n, g.k, terms), st, &ws);
         if (e != cudaSuccess) return e;
-        return sgemm_bf16x3(g, ws, st);
+        return sgemm_bf16_split(g, terms, ws, st);
     }
     GemmPlan p = plan_native_gemm(g.m, g.n, g.k, 4, cx.sm_count);
     void* ws = nullptr;
@@ -152,7 +154,12 @@ size_t real_scratch_bytes(int m, int n, int k, float*);
 
 int host_panel_count(int m, int n, int k) {
     if (n < 2048 || 2.0 * m * (double)n * k < kPanelMinFlops) return 1;
-    return std::min(8, std::max(2, n / 1024));
+    static const int cap = [] {  // ZYNUM_GPU_HOST_PANELS: most panels per call (2..32, default 8)
+        const char* v = std::getenv("ZYNUM_GPU_HOST_PANELS");
+        const int x = v ? std::atoi(v) : 8;
+        return (x >= 2 && x <= 32) ? x : 8;
+    }();
+    return std::min(cap, std::max(2, n / 1024 * cap / 8));
 }
 
 template <typename T>
@@ -339,7 +346,8 @@ size_t real_scratch_bytes(int m, int n, int k, double*) {
 }
 size_t real_scratch_bytes(int m, int n, int k, float*) {
     Context& cx = context();
-    if (cx.sgemm_method == SMETHOD_BF16X3) return bf16x3_workspace_bytes(m, n, k);
+    if (cx.sgemm_method == SMETHOD_BF16X3 || cx.sgemm_method == SMETHOD_BF16X6)
+        return bf16_split_workspace_bytes(m, n, k, cx.sgemm_method == SMETHOD_BF16X6 ? 3 : 2);
     GemmPlan p = plan_native_gemm(m, n, k, 4, cx.sm_count);
     return sgemm_native_workspace_bytes('T', 'N', m, n, k, p);  // both operand copies, if any
 }
@@ -394,8 +402,9 @@ cudaError_t run_complex(const ComplexArgs<T>& g, cudaStream_t st, Scratch scratc
     cudaError_t e = scratch(planes + real, st, &ws);
     if (e != cudaSuccess) return e;
     FixedScratch fs{static_cast<char*>(ws) + planes, real};
-    RealGemm<T> rg = [&](int m, int n, int k, const T* a, long lda, const T* b, long ldb, T* c, long ldc) {
+    RealGemm<T> rg = [&](int m, int n, int k, const T* a, long lda, const T* b, long ldb, T* c, long ldc, int tri) {
         GemmArgs<T> rgs{'N', 'N', m, n, k, T(1), a, lda, b, ldb, T(0), c, ldc};
+        rgs.tri = tri;
         return run_real(rgs, st, fs);
     };
     return complex_gemm<T>(g, method, ws, rg, st);
@@ -728,6 +737,7 @@ cudaError_t run_syrk_c(char uplo, char trans, int n, int k, cnum<R> alpha, const
     const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
     ComplexArgs<R> cg{t1, t2, n, n, k, {R(1), R(0)}, reinterpret_cast<const R*>(a), lda, reinterpret_cast<const R*>(a),
                       lda, {R(0), R(0)}, reinterpret_cast<R*>(W), n};
+    cg.tri = uplo == 'U' ? 1 : 2;  // the update reads only the stored triangle of W
     if ((e = run_complex(cg, st, FixedScratch{static_cast<char*>(ws) + wbytes, cb})) != cudaSuccess) return e;
     return triangle_update<cnum<R>>(uplo, false, n, alpha, W, n, beta, c, ldc, st, trans == 'C');
 }
@@ -799,6 +809,8 @@ cudaError_t run_rank2k_c(char uplo, char trans, bool herm, bool two, int n, int 
     }
     ComplexArgs<R> cg{t1, t2, n, n, k, {R(1), R(0)}, reinterpret_cast<const R*>(a), lda, reinterpret_cast<const R*>(b),
                       ldb, {R(0), R(0)}, reinterpret_cast<R*>(W), n};
+    // HERK reads only the stored triangle of W; SYR2K / HER2K also read its transpose
+    if (!two) cg.tri = uplo == 'U' ? 1 : 2;
     if ((e = run_complex(cg, st, FixedScratch{static_cast<char*>(ws) + wbytes, cb})) != cudaSuccess) return e;
     const cnum<R> alpha2 = herm ? cnum<R>(alpha.re, -alpha.im) : alpha;
     return triangle_update_h<cnum<R>>(uplo, two, herm, n, alpha, alpha2, W, n, beta, c, ldc, st, conj_w);
@@ -1951,7 +1963,7 @@ int zynum_blas_gpu_set_sgemm_method(int method) {
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
     cx.init();
     int old = cx.sgemm_method;
-    if (method == SMETHOD_NATIVE || method == SMETHOD_BF16X3) cx.sgemm_method = method;
+    if (method == SMETHOD_NATIVE || method == SMETHOD_BF16X3 || method == SMETHOD_BF16X6) cx.sgemm_method = method;
     return old;
 }
 

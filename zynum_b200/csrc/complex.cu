@@ -65,11 +65,12 @@ __global__ void stack_b(const T* __restrict__ b, long ldb, char tb, int k, int n
 // C = alpha (Cr + i Ci) + beta C, with Cr / Ci the two halves of a 2m x n real result.
 template <typename T>
 __global__ void combine_expanded(const T* __restrict__ cst, int m, int n, T ar, T ai, T br, T bi, T* __restrict__ c,
-                                 long ldc) {
+                                 long ldc, int tri) {
     const long total = (long)m * n;
     const bool beta0 = (br == T(0) && bi == T(0));
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
         const long i = q % m, j = q / m;
+        if (tri == 1 ? i > j : (tri == 2 && i < j)) continue;  // outside the computed triangle
         const T xr = cst[i + j * 2L * m], xi = cst[m + i + j * 2L * m];
         T* cp = c + 2 * (i + j * ldc);
         T rr = ar * xr - ai * xi, ri = ar * xi + ai * xr;
@@ -114,11 +115,12 @@ __global__ void planes_b3(const T* __restrict__ b, long ldb, char tb, int k, int
 // Re = cr - tmp, Im = cr + ci, then alpha / beta.
 template <typename T>
 __global__ void combine_3m(const T* __restrict__ prod, int m, int n, T ar, T ai, T br, T bi, T* __restrict__ c,
-                           long ldc) {
+                           long ldc, int tri) {
     const long total = (long)m * n;
     const bool beta0 = (br == T(0) && bi == T(0));
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
         const long i = q % m, j = q / m;
+        if (tri == 1 ? i > j : (tri == 2 && i < j)) continue;  // outside the computed triangle
         const T cr = prod[q], tmp = prod[total + q], ci = prod[2 * total + q];
         const T xr = cr - tmp, xi = cr + ci;
         T* cp = c + 2 * (i + j * ldc);
@@ -163,11 +165,11 @@ cudaError_t complex_gemm(const ComplexArgs<T>& g, int method, void* planes, cons
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         const long mk = (long)m * k, kn = (long)k * n, mn = (long)m * n;
         // cr = ar * bp, tmp = as * bi, ci = am * br
-        if ((e = real_gemm(m, n, k, pa, m, pb + 2 * kn, k, pc, m)) != cudaSuccess) return e;
-        if ((e = real_gemm(m, n, k, pa + mk, m, pb + kn, k, pc + mn, m)) != cudaSuccess) return e;
-        if ((e = real_gemm(m, n, k, pa + 2 * mk, m, pb, k, pc + 2 * mn, m)) != cudaSuccess) return e;
+        if ((e = real_gemm(m, n, k, pa, m, pb + 2 * kn, k, pc, m, g.tri)) != cudaSuccess) return e;
+        if ((e = real_gemm(m, n, k, pa + mk, m, pb + kn, k, pc + mn, m, g.tri)) != cudaSuccess) return e;
+        if ((e = real_gemm(m, n, k, pa + 2 * mk, m, pb, k, pc + 2 * mn, m, g.tri)) != cudaSuccess) return e;
         combine_3m<T><<<grid_for(mn), 256, 0, st>>>(pc, m, n, g.alpha[0], g.alpha[1], g.beta[0], g.beta[1], g.c,
-                                                    g.ldc);
+                                                    g.ldc, g.tri);
         count_launch();
         return cudaGetLastError();
     }
@@ -179,9 +181,16 @@ cudaError_t complex_gemm(const ComplexArgs<T>& g, int method, void* planes, cons
     stack_b<T><<<grid_for((long)k * n), 256, 0, st>>>(g.b, g.ldb, g.transb, k, n, bs);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = real_gemm(2 * m, n, 2 * k, ax, 2 * m, bs, 2 * k, cs, 2 * m)) != cudaSuccess) return e;
+    if (g.tri == 0) {
+        if ((e = real_gemm(2 * m, n, 2 * k, ax, 2 * m, bs, 2 * k, cs, 2 * m, 0)) != cudaSuccess) return e;
+    } else {
+        // one triangle: the real and imaginary halves as two m-row products in
+        // triangle mode, [Ar, -Ai] [Br; Bi] and [Ai, Ar] [Br; Bi]
+        if ((e = real_gemm(m, n, 2 * k, ax, 2 * m, bs, 2 * k, cs, 2 * m, g.tri)) != cudaSuccess) return e;
+        if ((e = real_gemm(m, n, 2 * k, ax + m, 2 * m, bs, 2 * k, cs + m, 2 * m, g.tri)) != cudaSuccess) return e;
+    }
     combine_expanded<T><<<grid_for((long)m * n), 256, 0, st>>>(cs, m, n, g.alpha[0], g.alpha[1], g.beta[0],
-                                                               g.beta[1], g.c, g.ldc);
+                                                               g.beta[1], g.c, g.ldc, g.tri);
     count_launch();
     return cudaGetLastError();
 }

@@ -25,12 +25,16 @@ struct ComplexArgs {
     T beta[2];
     T* c;
     long ldc;
+    // m == n only: 0 = all of C; 1 = only the upper triangle (row <= col), 2 =
+    // only the lower one (row >= col) is computed and written (rank-k updates)
+    int tri = 0;
 };
 
-// C (m x n, ldc) = A (m x k, lda) * B (k x n, ldb), real, alpha = 1, beta = 0.
+// C (m x n, ldc) = A (m x k, lda) * B (k x n, ldb), real, alpha = 1, beta = 0;
+// tri as in GemmArgs (tiles outside the triangle are skipped, C there is left alone).
 template <typename T>
 using RealGemm = std::function<cudaError_t(int m, int n, int k, const T* a, long lda, const T* b, long ldb, T* c,
-                                           long ldc)>;
+                                           long ldc, int tri)>;
 
 // Device scratch the complex route needs for its planes (the real GEMMs'
 // own scratch comes on top of it).

@@ -27,6 +27,8 @@
 // 3xBF16 SGEMM: x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and
 // C ~= hi_A hi_B + hi_A lo_B + lo_A hi_B, one FP32 TMEM accumulator
 // (kind::f16 with BF16 inputs), same GEMM kernel with a FP32 epilogue.
+// 6xBF16 SGEMM: three terms per operand (x0 + x1 + x2 holds all 24 bits of
+// the FP32 significand) and the six products with t + u <= 2.
 //
 // Replaces, for the GPU, the reference's dense real GEMM body
 // (kernels/shared/matrix_matrix/packed_simd.zig:306) when the Ozaki method is
@@ -439,7 +441,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         // the job's accumulators must have been drained by the epilogue
                         // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
                         // so a tile's epilogue overlaps the next tile's products
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
+                                                            : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
                         ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
@@ -500,7 +503,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
+                                                        : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
                     ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
@@ -565,7 +569,12 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                             }
 #pragma unroll
                             for (int c = 0; c < 32; ++c) {
-                                const float v = P.alpha_f * __uint_as_float(r0[c]);
+                                // two accumulators: the products of order t + u <= 1 and those of
+                                // order 2, added exactly in FP64 and rounded once
+                                const float sum = two ? (float)((double)__uint_as_float(r0[c]) +
+                                                                (double)__uint_as_float(r1[c]))
+                                                      : __uint_as_float(r0[c]);
+                                const float v = P.alpha_f * sum;
                                 const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
                                 if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
                             }
@@ -823,7 +832,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
                         // so a tile's epilogue overlaps the next tile's products
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
+                                                            : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
                         ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
@@ -905,7 +915,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
+                                                        : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
                     ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
@@ -950,7 +961,12 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                             }
 #pragma unroll
                             for (int c = 0; c < 32; ++c) {
-                                const float v = P.alpha_f * __uint_as_float(r0[c]);
+                                // two accumulators: the products of order t + u <= 1 and those of
+                                // order 2, added exactly in FP64 and rounded once
+                                const float sum = two ? (float)((double)__uint_as_float(r0[c]) +
+                                                                (double)__uint_as_float(r1[c]))
+                                                      : __uint_as_float(r0[c]);
+                                const float v = P.alpha_f * sum;
                                 const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
                                 if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
                             }
@@ -1476,6 +1492,10 @@ struct ViewF {
     int rows, cols;
 };
 
+// Split of a float matrix view into TERMS bfloat16 planes (K-major):
+// x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1); each remainder is
+// exact in FP32, so TERMS = 3 carries the full 24-bit significand.
+template <int TERMS>
 __global__ void __launch_bounds__(256)
 bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ planes) {
     __shared__ float tile[32][129];
@@ -1501,18 +1521,22 @@ bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ plan
     const int r = t >> 3, q = t & 7;
     if (r0 + r >= rows_pad) return;
     const long plane = (long)rows_pad * cols_pad;
-    __nv_bfloat16 hi[16], lo[16];
+    __nv_bfloat16 part[TERMS][16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const float x = tile[r][q * 16 + i];
-        hi[i] = __float2bfloat16_rn(x);
-        lo[i] = __float2bfloat16_rn(x - __bfloat162float(hi[i]));
+        float x = tile[r][q * 16 + i];
+#pragma unroll
+        for (int u = 0; u < TERMS; ++u) {
+            part[u][i] = __float2bfloat16_rn(x);
+            x -= __bfloat162float(part[u][i]);
+        }
     }
     __nv_bfloat16* o = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
-    *reinterpret_cast<uint4*>(o) = *reinterpret_cast<uint4*>(hi);
-    *reinterpret_cast<uint4*>(o + 8) = *reinterpret_cast<uint4*>(hi + 8);
-    *reinterpret_cast<uint4*>(o + plane) = *reinterpret_cast<uint4*>(lo);
-    *reinterpret_cast<uint4*>(o + plane + 8) = *reinterpret_cast<uint4*>(lo + 8);
+#pragma unroll
+    for (int u = 0; u < TERMS; ++u) {
+        *reinterpret_cast<uint4*>(o + u * plane) = *reinterpret_cast<uint4*>(part[u]);
+        *reinterpret_cast<uint4*>(o + u * plane + 8) = *reinterpret_cast<uint4*>(part[u] + 8);
+    }
 }
 
 // ------------------------------------------------------------ host side
@@ -2067,28 +2091,30 @@ int ozaki_take_wait_report(cudaStream_t stream, cudaError_t* err) {
     return e == cudaSuccess ? v : 0;
 }
 
-size_t bf16x3_workspace_bytes(int m, int n, int k) {
+size_t bf16_split_workspace_bytes(int m, int n, int k, int terms) {
     const long mp = round_up(m, use_cta_pair(m) ? 2 * kUM : kUM), np = round_up(n, kUN), kp = round_up(k, 128);
-    return (size_t)(2 * mp * kp * 2 + 2 * np * kp * 2 + 1024);
+    return (size_t)(terms * mp * kp * 2 + terms * np * kp * 2 + 1024);
 }
 
-cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
+cudaError_t sgemm_bf16_split(const GemmArgsF32& g, int terms, void* ws, cudaStream_t st) {
     // K is padded to 128 elements: the split kernel writes 128 columns per block.
     const bool pair = use_cta_pair(g.m);
     const int mp = (int)round_up(g.m, pair ? 2 * kUM : kUM), np = (int)round_up(g.n, kUN), kp = (int)round_up(g.k, 128);
     __nv_bfloat16* a_planes = static_cast<__nv_bfloat16*>(ws);
-    __nv_bfloat16* b_planes = a_planes + 2L * mp * kp;
+    __nv_bfloat16* b_planes = a_planes + (long)terms * mp * kp;
     ViewF va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     ViewF vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
-    bf16_split<<<dim3((kp + 127) / 128, mp / 32), 256, 0, st>>>(va, mp, kp, a_planes);
+    auto split = terms == 3 ? bf16_split<3> : bf16_split<2>;
+    split<<<dim3((kp + 127) / 128, mp / 32), 256, 0, st>>>(va, mp, kp, a_planes);
     count_launch();
-    bf16_split<<<dim3((kp + 127) / 128, np / 32), 256, 0, st>>>(vb, np, kp, b_planes);
+    split<<<dim3((kp + 127) / 128, np / 32), 256, 0, st>>>(vb, np, kp, b_planes);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     CUtensorMap ma, mb;
-    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * mp, kUM)) != cudaSuccess) return e;
-    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * np, pair ? kUN / 2 : kUN)) !=
+    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, (long)terms * mp, kUM)) != cudaSuccess)
+        return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, (long)terms * np, pair ? kUN / 2 : kUN)) !=
         cudaSuccess)
         return e;
     UmmaParams P{};
@@ -2097,24 +2123,33 @@ cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     P.m_pad = mp;
     P.n_pad = np;
     P.k_chunks = kp / 64;
-    P.kseg_chunks = P.k_chunks;
-    P.num_kseg = 1;
+    // K segments (64-deep chunks each; 0 = all of K): each segment starts a fresh
+    // accumulator and its sum is added to C in FP32 by the epilogue
+    int seg = 0;
+    if (const char* v = std::getenv("ZYNUM_GPU_BF16_KSEG")) seg = std::atoi(v);
+    P.kseg_chunks = seg > 0 && seg < P.k_chunks ? seg : P.k_chunks;
+    P.num_kseg = (P.k_chunks + P.kseg_chunks - 1) / P.kseg_chunks;
     P.tiles_m = mp / (pair ? 2 * kUM : kUM);
     P.tiles_n = np / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
-    // one job, one FP32 accumulator: hi*lo, hi*hi, lo*hi (consecutive steps
-    // share an operand); plane 0 = hi, 1 = lo
+    // one job, consecutive steps share a plane:
+    //   2 terms: x0 y1, x0 y0, x1 y0 (products with t + u <= 1) in one FP32 accumulator;
+    //   3 terms: x0 y2, x0 y1, x0 y0, x1 y0, x1 y1, x2 y0 (t + u <= 2), the order-2
+    //   products in the second accumulator: about 2^-16 of the order-0 ones, they
+    //   would fall below half an ulp of a running sum that holds the rest
+    static const int sa2[3] = {0, 0, 1}, sb2[3] = {1, 0, 0};
+    static const int sa3[6] = {0, 0, 0, 1, 1, 2}, sb3[6] = {2, 1, 0, 0, 1, 0};
+    const int nsteps = terms == 3 ? 6 : 3;
     P.num_jobs = 1;
     P.job_first_step[0] = 0;
-    P.job_num_steps[0] = 3;
-    P.job_groups[0] = 1;
+    P.job_num_steps[0] = nsteps;
+    P.job_groups[0] = terms == 3 ? 2 : 1;
     P.job_shift[0][0] = 0;
     P.job_shift[0][1] = 0;
-    const int sa[3] = {0, 0, 1}, sb[3] = {1, 0, 0};
-    for (int q = 0; q < 3; ++q) {
-        P.step_a[q] = sa[q];
-        P.step_b[q] = sb[q];
-        P.step_acc[q] = 0;
+    for (int q = 0; q < nsteps; ++q) {
+        P.step_a[q] = terms == 3 ? sa3[q] : sa2[q];
+        P.step_b[q] = terms == 3 ? sb3[q] : sb2[q];
+        P.step_acc[q] = terms == 3 ? (P.step_a[q] + P.step_b[q] == 2 ? 1 : 0) : 0;
     }
     P.alpha_f = g.alpha;
     P.beta_f = g.beta;

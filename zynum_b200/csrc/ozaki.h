@@ -70,8 +70,11 @@ size_t ozaki_workspace_bytes(const OzakiPlan& p);
 // they are reused, not recomputed.  The plan may cover more columns than g.n.
 cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready = false);
 
-size_t bf16x3_workspace_bytes(int m, int n, int k);
-// C = alpha op(A) op(B) + beta C as a 3xBF16 split product with FP32 accumulation.
-cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st);
+// C = alpha op(A) op(B) + beta C as a split product of `terms` bfloat16
+// planes per operand with FP32 accumulation in TMEM: terms = 2 takes the 3
+// products with t + u <= 1 (about 16 bits), terms = 3 the 6 products with
+// t + u <= 2 (the FP32 significand); `ws` holds bf16_split_workspace_bytes.
+size_t bf16_split_workspace_bytes(int m, int n, int k, int terms);
+cudaError_t sgemm_bf16_split(const GemmArgsF32& g, int terms, void* ws, cudaStream_t st);
 
 }  // namespace zb
