@@ -372,7 +372,7 @@ def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
     C = torch.zeros((n, n), dtype=torch.float32, device=dev)
     a_h = np.asfortranarray(A.cpu().numpy().T.astype(np.float64))
     b_h = np.asfortranarray(B.cpu().numpy().T.astype(np.float64))
-    for name, mid in (("sgemm_bf16x3", blas.SMETHOD_BF16X3), ("sgemm_bf16x6", blas.SMETHOD_BF16X6),
+    for name, mid in (("sgemm_bf16x3", blas.SMETHOD_BF16X3), ("sgemm_ozaki", blas.SMETHOD_OZAKI),
                       ("sgemm_native", blas.SMETHOD_NATIVE)):
         blas.set_sgemm_method(mid)
         fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
@@ -665,7 +665,7 @@ def suite_precision(args):
     a_h = np.asfortranarray(A.cpu().numpy().T)
     b_h = np.asfortranarray(B.cpu().numpy().T)
     for name, mid in (("native_fp32", blas.SMETHOD_NATIVE), ("bf16x3", blas.SMETHOD_BF16X3),
-                      ("bf16x6", blas.SMETHOD_BF16X6)):
+                      ("ozaki_int8", blas.SMETHOD_OZAKI)):
         blas.set_sgemm_method(mid)
         fn = lambda: blas.sgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # noqa: E731
         ms = time_device(torch, fn, args.steps, args.warmup, stream)

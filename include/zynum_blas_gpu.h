@@ -432,8 +432,8 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_strsm_batch_run(zynum_blas_gpu_batch_t bat
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_complex_method(int method);
 /* 0 = native FP64, 1 = Ozaki INT8 emulation, 2 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_dgemm_method(int method);
-/* 0 = native FP32, 1 = 3xBF16 split product (about 16 bits), 2 = 6xBF16 split
- * product (three bf16 terms per operand, FP32-accurate).  Returns the previous value. */
+/* 0 = native FP32, 1 = 3xBF16 split product (about 16 bits), 2 = INT8 CRT
+ * emulation (exact integer products, one rounding to FP32).  Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_sgemm_method(int method);
 /* Ozaki slice count (2..12), 0 = automatic. Returns the previous value. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_set_ozaki_slices(int slices);

@@ -373,39 +373,6 @@ def test_sgemm_bf16x3(blas, oracle, ta, tb):
     assert np.array_equal(c[m:], c0[m:])
 
 
-@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
-def test_sgemm_bf16x6_fp32_accurate(blas, oracle, ta, tb):
-    """6xBF16 split product (three bf16 terms per operand, six products): within the
-    componentwise bound native FP32 GEMM is held to, 4 k u32 (|alpha| |A||B| + |beta| |C0|),
-    and no less accurate than the native FP32 kernel on the same data."""
-    rng = np.random.default_rng(4)
-    m, n, k = 300, 257, 1500
-    lda = (m if ta == "N" else k) + 3
-    ldb = (k if tb == "N" else n) + 1
-    ldc = m + 2
-    a = np.asfortranarray(rng.uniform(-1, 1, (lda, k if ta == "N" else m)).astype(np.float32))
-    b = np.asfortranarray(rng.uniform(-1, 1, (ldb, n if tb == "N" else k)).astype(np.float32))
-    c = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)).astype(np.float32))
-    c0 = c.copy(order="F")
-    A = _op(a.astype(np.float64), ta, m, k)
-    B = _op(b.astype(np.float64), tb, k, n)
-    exact = 1.25 * (A @ B) - 0.5 * c0[:m, :n].astype(np.float64)
-    errs = {}
-    for method in (blas.SMETHOD_BF16X6, blas.SMETHOD_NATIVE):
-        out = c0.copy(order="F")
-        blas.set_sgemm_method(method)
-        try:
-            blas.sgemm(ta, tb, m, n, k, 1.25, a, lda, b, ldb, -0.5, out, ldc)
-        finally:
-            blas.set_sgemm_method(blas.SMETHOD_NATIVE)
-        errs[method] = np.abs(out[:m, :n] - exact)
-        assert np.array_equal(out[m:], c0[m:])
-    bound = 4 * k * 2.0 ** -24 * (1.25 * (np.abs(A) @ np.abs(B)) + 0.5 * np.abs(c0[:m, :n]))
-    assert np.all(errs[blas.SMETHOD_BF16X6] <= bound), float((errs[blas.SMETHOD_BF16X6] / bound).max())
-    ab = np.abs(A) @ np.abs(B)
-    assert (errs[blas.SMETHOD_BF16X6] / ab).max() <= 1.5 * (errs[blas.SMETHOD_NATIVE] / ab).max()
-
-
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
 def test_host_panels_reuse_a_residues_bit_identical(blas, ta, tb):
     """dgemm_ with host buffers large enough for column panels (here 4, the last one ragged)

@@ -25,7 +25,7 @@ CblasNonUnit, CblasUnit = 131, 132
 CblasLeft, CblasRight = 141, 142
 
 METHOD_NATIVE, METHOD_OZAKI, METHOD_AUTO = 0, 1, 2
-SMETHOD_NATIVE, SMETHOD_BF16X3, SMETHOD_BF16X6 = 0, 1, 2
+SMETHOD_NATIVE, SMETHOD_BF16X3, SMETHOD_OZAKI = 0, 1, 2
 
 
 def _i(v: int):

@@ -119,12 +119,27 @@ template <typename Scratch>
 cudaError_t run_sgemm(const GemmArgsF32& g, cudaStream_t st, Scratch scratch) {
     Context& cx = context();
     if (g.k == 0 || g.alpha == 0.0f) return scale_matrix<float>(g.m, g.n, g.beta, g.c, g.ldc, st);
-    if (cx.sgemm_method == SMETHOD_BF16X3 || cx.sgemm_method == SMETHOD_BF16X6) {
-        const int terms = cx.sgemm_method == SMETHOD_BF16X6 ? 3 : 2;
+    if (cx.sgemm_method == SMETHOD_BF16X3) {
         void* ws = nullptr;
-        cudaError_t e = scratch(bf16_split_workspace_bytes(g.m, g.n, g.k, terms), st, &ws);
+        cudaError_t e = scratch(bf16x3_workspace_bytes(g.m, g.n, g.k), st, &ws);
         if (e != cudaSuccess) return e;
-        return sgemm_bf16_split(g, terms, ws, st);
+        return sgemm_bf16x3(g, ws, st);
+    }
+    if (cx.sgemm_method == SMETHOD_OZAKI) {
+        // K beyond the INT32 bound of one modular product: K panels, each added to C
+        const int kp = std::min(g.k, kCrtMaxK);
+        const OzakiPlan op = plan_ozaki(g.m, g.n, kp, 0, OZAKI_CRT, sgemm_crt_moduli(kp));
+        void* ws = nullptr;
+        cudaError_t e = scratch(ozaki_workspace_bytes(op), st, &ws);
+        for (int k0 = 0; e == cudaSuccess && k0 < g.k; k0 += kp) {
+            GemmArgsF32 p = g;
+            p.k = std::min(kp, g.k - k0);
+            p.a = g.a + (g.transa == 'N' ? (long)k0 * g.lda : k0);
+            p.b = g.b + (g.transb == 'N' ? k0 : (long)k0 * g.ldb);
+            if (k0 > 0) p.beta = 1.0f;
+            e = sgemm_ozaki(p, op, ws, st);
+        }
+        return e;
     }
     GemmPlan p = plan_native_gemm(g.m, g.n, g.k, 4, cx.sm_count);
     void* ws = nullptr;
@@ -346,8 +361,11 @@ size_t real_scratch_bytes(int m, int n, int k, double*) {
 }
 size_t real_scratch_bytes(int m, int n, int k, float*) {
     Context& cx = context();
-    if (cx.sgemm_method == SMETHOD_BF16X3 || cx.sgemm_method == SMETHOD_BF16X6)
-        return bf16_split_workspace_bytes(m, n, k, cx.sgemm_method == SMETHOD_BF16X6 ? 3 : 2);
+    if (cx.sgemm_method == SMETHOD_BF16X3) return bf16x3_workspace_bytes(m, n, k);
+    if (cx.sgemm_method == SMETHOD_OZAKI) {
+        const int kp = std::min(k, kCrtMaxK);
+        return ozaki_workspace_bytes(plan_ozaki(m, n, kp, 0, OZAKI_CRT, sgemm_crt_moduli(kp)));
+    }
     GemmPlan p = plan_native_gemm(m, n, k, 4, cx.sm_count);
     return sgemm_native_workspace_bytes('T', 'N', m, n, k, p);  // both operand copies, if any
 }
@@ -1963,7 +1981,7 @@ int zynum_blas_gpu_set_sgemm_method(int method) {
     std::lock_guard<std::recursive_mutex> lock(cx.mutex);
     cx.init();
     int old = cx.sgemm_method;
-    if (method == SMETHOD_NATIVE || method == SMETHOD_BF16X3 || method == SMETHOD_BF16X6) cx.sgemm_method = method;
+    if (method >= SMETHOD_NATIVE && method <= SMETHOD_OZAKI) cx.sgemm_method = method;
     return old;
 }
 

@@ -391,296 +391,6 @@ sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* 
     }
 }
 
-// ------------------------------------------------ FP32 warp-owned tiles
-// Every warp owns whole 32 x 32 output tiles: its own two-stage cp.async ring
-// of 16-deep slices (A as [k][32 m], B as [k][32 n], pitch 36 floats), and
-// warp-level synchronisation only (cp.async.wait_group + __syncwarp), so the
-// 24 warps of an SM run independent tiles and hide one another's operand
-// latency; small problems waste at most a 32 x 32 tile.  Lane (lr = lane mod 8,
-// lc = lane / 8) owns rows 4 lr .. 4 lr + 3 and columns 8 lc .. 8 lc + 7: one
-// 16-byte A load and two 16-byte B loads per k for 32 FMAs.
-constexpr int kWT = 32, kWK = 16, kWP = kWT + 4;
-constexpr int kWStage = 2 * kWK * kWP;                    // floats: A and B of one slice
-constexpr size_t kWarpSmem = (size_t)8 * 2 * kWStage * 4;  // eight warps x two stages
-
-template <bool AM, bool BMF>
-ZB_DEVICE void sgemm_warp_tile(const Prob<float>& p, int m0, int n0, float alpha, float beta, float* ws, int lane) {
-    const int lr = lane & 7, lc = lane >> 3;
-    const int KT = (alpha == 0.f) ? 0 : (p.k + kWK - 1) / kWK;  // alpha == 0: A and B are not read
-    const bool va = AM && vec_ok(p.a, p.lda), vb = BMF && vec_ok(p.b, p.ldb);
-    float acc[4][8];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-    auto load = [&](int stage, int kt) {
-        float* As = ws + stage * kWStage;
-        float* Bs = As + kWK * kWP;
-        const int k0 = kt * kWK;
-        // A element (row i, k) -> As[k][i]
-        if (AM && va) {  // m contiguous, 16-byte copies: 16 k x 8 quads
-#pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int q = it * 32 + lane, kk = q >> 3, i4 = (q & 7) * 4;
-                const int gm = m0 + i4, gk = k0 + kk;
-                const int valid = gk < p.k ? max(0, min(4, p.m - gm)) : 0;
-                cp_async_16(smem_u32(As + kk * kWP + i4), valid ? p.a + gm + (long)gk * p.lda : p.a, valid * 4);
-            }
-        } else {  // one element per copy: lane = row
-#pragma unroll 4
-            for (int kk = 0; kk < kWK; ++kk) {
-                const int gm = m0 + lane, gk = k0 + kk;
-                const bool ok = gm < p.m && gk < p.k;
-                const float* src = AM ? p.a + gm + (long)gk * p.lda : p.a + gk + (long)gm * p.lda;
-                cp_async_4(smem_u32(As + kk * kWP + lane), ok ? src : p.a, ok ? 4 : 0);
-            }
-        }
-        // B element (k, column j) -> Bs[k][j]
-        if (BMF && vb) {  // n contiguous, 16-byte copies
-#pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int q = it * 32 + lane, kk = q >> 3, j4 = (q & 7) * 4;
-                const int gn = n0 + j4, gk = k0 + kk;
-                const int valid = gk < p.k ? max(0, min(4, p.n - gn)) : 0;
-                cp_async_16(smem_u32(Bs + kk * kWP + j4), valid ? p.b + gn + (long)gk * p.ldb : p.b, valid * 4);
-            }
-        } else {  // lane = column
-#pragma unroll 4
-            for (int kk = 0; kk < kWK; ++kk) {
-                const int gn = n0 + lane, gk = k0 + kk;
-                const bool ok = gn < p.n && gk < p.k;
-                const float* src = BMF ? p.b + gn + (long)gk * p.ldb : p.b + gk + (long)gn * p.ldb;
-                cp_async_4(smem_u32(Bs + kk * kWP + lane), ok ? src : p.b, ok ? 4 : 0);
-            }
-        }
-    };
-    if (KT > 0) load(0, 0);
-    cp_async_commit();
-    for (int kt = 0; kt < KT; ++kt) {
-        if (kt + 1 < KT) load((kt + 1) & 1, kt + 1);
-        cp_async_commit();
-        cp_async_wait<1>();  // this lane's copies of slice kt have landed
-        __syncwarp();        // ... and every other lane's
-        const float* As = ws + (kt & 1) * kWStage;
-        const float* Bs = As + kWK * kWP;
-#pragma unroll
-        for (int kk = 0; kk < kWK; ++kk) {
-            const float4 a = *reinterpret_cast<const float4*>(As + kk * kWP + 4 * lr);
-            const float4 b0 = *reinterpret_cast<const float4*>(Bs + kk * kWP + 8 * lc);
-            const float4 b1 = *reinterpret_cast<const float4*>(Bs + kk * kWP + 8 * lc + 4);
-            const float av[4] = {a.x, a.y, a.z, a.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-        }
-        __syncwarp();  // every lane has read slice kt before its stage is refilled
-    }
-    cp_async_wait<0>();
-    __syncwarp();
-    const int row0 = m0 + 4 * lr;
-    const bool vc = row0 + 4 <= p.m && (p.ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(p.c) & 15) == 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int col = n0 + 8 * lc + j;
-        if (col >= p.n) break;
-        float* cp = p.c + row0 + (long)col * p.ldc;
-        if (vc) {
-            float4 o = make_float4(alpha * acc[0][j], alpha * acc[1][j], alpha * acc[2][j], alpha * acc[3][j]);
-            if (beta != 0.f) {
-                const float4 ci = *reinterpret_cast<const float4*>(cp);
-                o.x = fmaf(beta, ci.x, o.x);
-                o.y = fmaf(beta, ci.y, o.y);
-                o.z = fmaf(beta, ci.z, o.z);
-                o.w = fmaf(beta, ci.w, o.w);
-            }
-            *reinterpret_cast<float4*>(cp) = o;
-        } else {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                if (row0 + i >= p.m) break;
-                float out = alpha * acc[i][j];
-                if (beta != 0.f) out = fmaf(beta, cp[i], out);
-                cp[i] = out;
-            }
-        }
-    }
-}
-
-template <bool AM, bool BMF>
-__global__ void __launch_bounds__(kThreads, kWarpTileCtasPerSm)
-sgemm_batched_warp_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
-                          const float* const* __restrict__ a, const int* __restrict__ lda,
-                          const float* const* __restrict__ b, const int* __restrict__ ldb, float alpha, float beta,
-                          float* const* __restrict__ c, const int* __restrict__ ldc) {
-    extern __shared__ __align__(16) float sm_w[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* ws = sm_w + warp * 2 * kWStage;
-    const int nw = gridDim.x * (kThreads / 32);
-    for (int w = blockIdx.x * (kThreads / 32) + warp; w < n_work; w += nw) {
-        const BatchWork it = work[w];
-        const int q = it.prob;
-        if (q < 0) continue;  // padding item of the per-warp schedule
-        Prob<float> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
-        const int mt = (p.m + kWT - 1) / kWT;
-        for (int tile = it.t0; tile < it.t0 + it.count; ++tile)
-            sgemm_warp_tile<AM, BMF>(p, (tile % mt) * kWT, (tile / mt) * kWT, alpha, beta, ws, lane);
-    }
-}
-
-// ------------------------------------------------ FP64 warp-owned tiles
-// The same scheme with DMMA: a warp owns 32 x 32 tiles (2 x 4 fragments of
-// 16 x 8), streams 8-deep slices through its own three-stage cp.async ring
-// (A as [k][32 m], B as [k][32 n], pitch 40 doubles so that the fragment
-// loads of a warp spread evenly over the banks) and issues only the fragments
-// inside the problem (compile-time counts).  Four warps per CTA, three CTAs
-// per SM.
-constexpr int kDWK = 8, kDWP = 40, kDWStages = 3;
-constexpr int kDWStage = 2 * kDWK * kDWP;                                  // doubles
-constexpr int kDWarps = 4;
-constexpr size_t kDWarpSmem = (size_t)kDWarps * kDWStages * kDWStage * 8;  // 61440 B
-
-template <int MIV, int NIV>
-ZB_DEVICE void dwarp_step(double (&acc)[2][4][4], const double* As, const double* Bs, int g, int t) {
-    double af[MIV][4], bf[NIV][2];
-#pragma unroll
-    for (int i = 0; i < MIV; ++i)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) af[i][v] = As[(t + 4 * (v >> 1)) * kDWP + 16 * i + g + 8 * (v & 1)];
-#pragma unroll
-    for (int j = 0; j < NIV; ++j)
-#pragma unroll
-        for (int v = 0; v < 2; ++v) bf[j][v] = Bs[(t + 4 * v) * kDWP + 8 * j + g];
-#pragma unroll
-    for (int i = 0; i < MIV; ++i)
-#pragma unroll
-        for (int j = 0; j < NIV; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
-}
-
-template <bool AK, bool BKF>
-ZB_DEVICE void dgemm_warp_tile(const Prob<double>& p, int m0, int n0, double alpha, double beta, double* ws,
-                               int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    const int KT = (alpha == 0.0) ? 0 : (p.k + kDWK - 1) / kDWK;  // alpha == 0: A and B are not read
-    const bool va = !AK && vec_ok(p.a, p.lda), vb = !BKF && vec_ok(p.b, p.ldb);
-    const int miv = min(2, (p.m - m0 + 15) / 16), niv = min(4, (p.n - n0 + 7) / 8);
-    double acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
-    auto load = [&](int stage, int kt) {
-        double* As = ws + stage * kDWStage;
-        double* Bs = As + kDWK * kDWP;
-        const int k0 = kt * kDWK;
-        // A element (row i, k) -> As[k][i]
-        if (!AK && va) {  // m contiguous, 16-byte copies: 8 k x 16 pairs
-#pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int q = it * 32 + lane, kk = q >> 4, i2 = (q & 15) * 2;
-                const int gm = m0 + i2, gk = k0 + kk;
-                const int valid = gk < p.k ? max(0, min(2, p.m - gm)) : 0;
-                cp_async_16(smem_u32(As + kk * kDWP + i2), valid ? p.a + gm + (long)gk * p.lda : p.a, valid * 8);
-            }
-        } else {  // one element per copy: lane = row
-#pragma unroll
-            for (int kk = 0; kk < kDWK; ++kk) {
-                const int gm = m0 + lane, gk = k0 + kk;
-                const bool ok = gm < p.m && gk < p.k;
-                const double* src = AK ? p.a + gk + (long)gm * p.lda : p.a + gm + (long)gk * p.lda;
-                cp_async_8(smem_u32(As + kk * kDWP + lane), ok ? src : p.a, ok ? 8 : 0);
-            }
-        }
-        // B element (k, column j) -> Bs[k][j]
-        if (!BKF && vb) {  // n contiguous, 16-byte copies
-#pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int q = it * 32 + lane, kk = q >> 4, j2 = (q & 15) * 2;
-                const int gn = n0 + j2, gk = k0 + kk;
-                const int valid = gk < p.k ? max(0, min(2, p.n - gn)) : 0;
-                cp_async_16(smem_u32(Bs + kk * kDWP + j2), valid ? p.b + gn + (long)gk * p.ldb : p.b, valid * 8);
-            }
-        } else {  // lane = column
-#pragma unroll
-            for (int kk = 0; kk < kDWK; ++kk) {
-                const int gn = n0 + lane, gk = k0 + kk;
-                const bool ok = gn < p.n && gk < p.k;
-                const double* src = BKF ? p.b + gk + (long)gn * p.ldb : p.b + gn + (long)gk * p.ldb;
-                cp_async_8(smem_u32(Bs + kk * kDWP + lane), ok ? src : p.b, ok ? 8 : 0);
-            }
-        }
-    };
-#pragma unroll
-    for (int s = 0; s < kDWStages - 1; ++s) {
-        if (s < KT) load(s, s);
-        cp_async_commit();
-    }
-    for (int kt = 0; kt < KT; ++kt) {
-        if (kt + kDWStages - 1 < KT) load((kt + kDWStages - 1) % kDWStages, kt + kDWStages - 1);
-        cp_async_commit();
-        cp_async_wait<kDWStages - 1>();  // this lane's copies of slice kt have landed
-        __syncwarp();                    // ... and every other lane's
-        const double* As = ws + (kt % kDWStages) * kDWStage;
-        const double* Bs = As + kDWK * kDWP;
-        if (miv == 2 && niv == 4) {
-            dwarp_step<2, 4>(acc, As, Bs, g, t);
-        } else {
-            switch (miv * 4 + niv) {
-                case 5: dwarp_step<1, 1>(acc, As, Bs, g, t); break;
-                case 6: dwarp_step<1, 2>(acc, As, Bs, g, t); break;
-                case 7: dwarp_step<1, 3>(acc, As, Bs, g, t); break;
-                case 8: dwarp_step<1, 4>(acc, As, Bs, g, t); break;
-                case 9: dwarp_step<2, 1>(acc, As, Bs, g, t); break;
-                case 10: dwarp_step<2, 2>(acc, As, Bs, g, t); break;
-                case 11: dwarp_step<2, 3>(acc, As, Bs, g, t); break;
-                default: break;
-            }
-        }
-        __syncwarp();  // every lane has read slice kt before its stage is refilled
-    }
-    cp_async_wait<0>();
-    __syncwarp();
-    // c[v0 + 2 v1] at (row g + 8 v1, col 2 t + v0) of fragment (i, j)
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int row = m0 + 16 * i + g + 8 * (v >> 1), col = n0 + 8 * j + 2 * t + (v & 1);
-                if (row < p.m && col < p.n) {
-                    double* cp = p.c + (long)col * p.ldc + row;
-                    double out = alpha * acc[i][j][v];
-                    if (beta != 0.0) out = fma(beta, *cp, out);
-                    *cp = out;
-                }
-            }
-}
-
-template <bool AK, bool BKF>
-__global__ void __launch_bounds__(kDWarps * 32, 3)
-dgemm_batched_warp_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
-                          const double* const* __restrict__ a, const int* __restrict__ lda,
-                          const double* const* __restrict__ b, const int* __restrict__ ldb, double alpha,
-                          double beta, double* const* __restrict__ c, const int* __restrict__ ldc) {
-    extern __shared__ __align__(16) double sm_dw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* ws = sm_dw + warp * kDWStages * kDWStage;
-    const int nw = gridDim.x * kDWarps;
-    for (int w = blockIdx.x * kDWarps + warp; w < n_work; w += nw) {
-        const BatchWork it = work[w];
-        const int q = it.prob;
-        if (q < 0) continue;  // padding item of the per-warp schedule
-        Prob<double> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
-        const int mt = (p.m + 31) / 32;
-        for (int tile = it.t0; tile < it.t0 + it.count; ++tile)
-            dgemm_warp_tile<AK, BKF>(p, (tile % mt) * 32, (tile / mt) * 32, alpha, beta, ws, lane);
-    }
-}
-
 size_t dsmem_bytes() {
     // largest FP64 config (64 x 64), worst orientation of each operand
     constexpr size_t a = 64 * (kBK + 4) > kBK * (64 + 4) ? 64 * (kBK + 4) : kBK * (64 + 4);
@@ -1159,20 +869,6 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
         auto A = reinterpret_cast<const double* const*>(a);
         auto B = reinterpret_cast<const double* const*>(b);
         auto Cp = reinterpret_cast<double* const*>(c);
-        if (d.warp_tiles) {
-#define ZB_DW(AKV, BKV)                                                                                         \
-    if (ak == AKV && bk == BKV) {                                                                               \
-        auto kern = dgemm_batched_warp_kernel<AKV, BKV>;                                                        \
-        if ((e = ensure_dynamic_smem(kern, (int)kDWarpSmem)) != cudaSuccess) return e;                          \
-        prof_begin(st);                                                                                         \
-        kern<<<grid, kDWarps * 32, kDWarpSmem, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc); \
-        count_launch();                                                                                         \
-        prof_end(st);                                                                                           \
-        return cudaGetLastError();                                                                              \
-    }
-            ZB_DW(false, false) ZB_DW(false, true) ZB_DW(true, false) ZB_DW(true, true)
-#undef ZB_DW
-        }
         const size_t sm = dsmem_bytes();
 #define ZB_DB(AKV, BKV)                                                                                         \
     if (ak == AKV && bk == BKV) {                                                                               \
@@ -1193,11 +889,6 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
         auto A = reinterpret_cast<const float* const*>(a);
         auto B = reinterpret_cast<const float* const*>(b);
         auto Cp = reinterpret_cast<float* const*>(c);
-        if (d.warp_tiles) {
-#define ZB_SW(AMV, BMV)                                                                                             if (am == AMV && bm == BMV) {                                                                                       auto kern = sgemm_batched_warp_kernel<AMV, BMV>;                                                                if ((e = ensure_dynamic_smem(kern, (int)kWarpSmem)) != cudaSuccess) return e;                                   prof_begin(st);                                                                                                 kern<<<grid, kThreads, kWarpSmem, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);             count_launch();                                                                                                 prof_end(st);                                                                                                   return cudaGetLastError();                                                                                  }
-            ZB_SW(false, false) ZB_SW(false, true) ZB_SW(true, false) ZB_SW(true, true)
-#undef ZB_SW
-        }
         const size_t sm = ssmem_bytes();
 #define ZB_SB(AMV, BMV)                                                                                         \
     if (am == AMV && bm == BMV) {                                                                               \
@@ -1240,7 +931,6 @@ cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, in
 }
 
 int batched_tile_n(int cfg, int dtype) {
-    if (cfg == TILE_CFG_W32) return kWT;
     return cfg == TILE_CFG_128 ? (dtype == BATCH_F64 ? 64 : 128) : (cfg == TILE_CFG_64 ? 64 : 32);
 }
 int batched_tile_m(int cfg, int dtype) { return batched_tile_n(cfg, dtype); }

@@ -9,9 +9,7 @@
 namespace zb {
 
 enum BatchDtype : int { BATCH_F64 = 0, BATCH_F32 = 1 };
-enum TileCfg : int { TILE_CFG_32 = 0, TILE_CFG_64 = 1, TILE_CFG_128 = 2, TILE_CFG_W32 = 3 };
-// TILE_CFG_W32: 32 x 32 tiles owned by single warps; a batch planned with it
-// uses it for every problem and deals work items to warps, not CTAs.
+enum TileCfg : int { TILE_CFG_32 = 0, TILE_CFG_64 = 1, TILE_CFG_128 = 2 };
 
 // A chunk of `count` consecutive output tiles t0.. of one problem (prob < 0:
 // padding, skipped).  Tile t covers rows (t % mt) TM.. and columns (t / mt) TN..
@@ -25,13 +23,7 @@ struct BatchDevice {
     const BatchWork* work;
     int n_work;
     const int* dims;  // m, n, k per problem
-    int warp_tiles = 0;  // items are dealt to warps (TILE_CFG_W32)
 };
-
-// CTAs per SM and warps per CTA of the warp-tile kernels (FP32: 8 warps,
-// FP64: 4 warps).
-constexpr int kWarpTileCtasPerSm = 3;
-inline int warp_tile_warps_per_cta(int dtype) { return dtype == BATCH_F64 ? 4 : 8; }
 
 // Output tile of a config: rows x columns (square; TILE_CFG_128 is 128 x 128
 // for FP32 and runs as 64 x 64 for FP64).

@@ -173,8 +173,7 @@ struct Batch {
     BatchWork* d_work = nullptr;
     int* d_order = nullptr;
     int n_items = 0;
-    int cfg_counts[4] = {0, 0, 0, 0};
-    bool warp_tiles = false;  // FP32: every problem on warp-owned 32 x 32 tiles
+    int cfg_counts[3] = {0, 0, 0};
     // graph replay
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -196,8 +195,7 @@ namespace {
 // Build the GEMM work list with one tile config per problem.
 constexpr int kChunkTiles = 4;  // tiles per work item (measured: 4 > 2 > 1)
 
-// slots: CTAs (or, for warp-owned tiles, warps) the items are dealt to.
-std::vector<BatchWork> build_work(const Batch& b, const std::vector<int>& cfg, int slots, std::vector<int>* counts) {
+std::vector<BatchWork> build_work(const Batch& b, const std::vector<int>& cfg, int grid, std::vector<int>* counts) {
     std::vector<BatchWork> items;
     std::vector<double> cost;
     for (int q = 0; q < b.count; ++q) {
@@ -214,7 +212,7 @@ std::vector<BatchWork> build_work(const Batch& b, const std::vector<int>& cfg, i
             if (counts) (*counts)[cfg[q]] += cnt;
         }
     }
-    std::vector<int> order = lpt_schedule(cost, slots);
+    std::vector<int> order = lpt_schedule(cost, grid);
     std::vector<BatchWork> out(order.size());
     for (size_t i = 0; i < order.size(); ++i) out[i] = order[i] < 0 ? BatchWork{-1, 0, 0, 0} : items[order[i]];
     return out;
@@ -410,12 +408,6 @@ int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
     b->n.assign(n, n + count);
     b->k.assign(k, k + count);
     b->grid = (dtype == BATCH_F64 ? 4 : 2) * sm_count();  // tile CTAs per SM: FP64 four, FP32 two
-    {
-        // warp-owned 32 x 32 tiles for every problem (opt-in until measured: ZYNUM_GPU_BATCH_WARP_TILES=1)
-        const char* v = std::getenv("ZYNUM_GPU_BATCH_WARP_TILES");
-        b->warp_tiles = v && v[0] == '1';
-        if (b->warp_tiles) b->grid = kWarpTileCtasPerSm * sm_count();
-    }
     std::vector<int> dims;
     for (int q = 0; q < count; ++q) {
         dims.push_back(m[q]);
@@ -428,12 +420,10 @@ int zynum_blas_gpu_gemm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
             e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) {
-        std::vector<int> cfg = b->warp_tiles ? std::vector<int>(count, TILE_CFG_W32) : choose_cfgs(*b, tune != 0);
-        std::vector<int> counts(4, 0);
-        e = upload_work(*b, build_work(*b, cfg, b->warp_tiles ? b->grid * warp_tile_warps_per_cta(dtype) : b->grid,
-                                       &counts));
-        for (int i = 0; i < 4; ++i) b->cfg_counts[i] = counts[i];
-        b->cfg_counts[TILE_CFG_32] += counts[TILE_CFG_W32];  // reported with the other 32 x 32 tiles
+        std::vector<int> cfg = choose_cfgs(*b, tune != 0);
+        std::vector<int> counts(3, 0);
+        e = upload_work(*b, build_work(*b, cfg, b->grid, &counts));
+        for (int i = 0; i < 3; ++i) b->cfg_counts[i] = counts[i];
     }
     if (e != cudaSuccess) {
         delete b;
@@ -527,7 +517,7 @@ int zynum_blas_gpu_batch_info(zynum_blas_gpu_batch_t batch, int* items, int* gri
         args.ldb = ldb;                                                                                             \
         args.c = c;                                                                                                 \
         args.ldc = ldc;                                                                                             \
-        BatchDevice dev{bt->d_work, bt->n_items, bt->d_dims, bt->warp_tiles ? 1 : 0};                               \
+        BatchDevice dev{bt->d_work, bt->n_items, bt->d_dims};                                                       \
         auto fn = [&](cudaStream_t s) {                                                                             \
             return launch_gemm_batched(dev, DT, bt->ta, bt->tb, &alpha, (const void* const*)a, lda,                \
                                        (const void* const*)b, ldb, &beta, (void* const*)c, ldc, bt->grid, s);       \

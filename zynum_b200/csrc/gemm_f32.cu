@@ -356,9 +356,9 @@ cudaError_t sgemm_native(const GemmArgsF32& g_in, const GemmPlan& plan, float* w
     if (plan.tile == TILE_GEMV && gemv_applies(g_in.m, g_in.n, g_in.k, g_in.tri))
         return sgemv_route(g_in, plan.splits, workspace, st);
     if (skinny_gemm_applies(g_in.m, g_in.n, g_in.k, g_in.tri)) {
-        static const bool tma = [] {  // opt-in until measured: ZYNUM_GPU_SKINNY_TMA=1
+        static const bool tma = [] {  // TMA-fed kernel unless ZYNUM_GPU_SKINNY_TMA=0
             const char* v = std::getenv("ZYNUM_GPU_SKINNY_TMA");
-            return v && v[0] == '1';
+            return !(v && v[0] == '0');
         }();
         return (tma && sgemm_skinny_tma_applies(g_in)) ? sgemm_skinny_tma(g_in, st) : sgemm_skinny(g_in, st);
     }

@@ -291,9 +291,9 @@ int dgemm_native_used_splits(const GemmArgsF64& g, const GemmPlan& plan) {
 cudaError_t dgemm_native(const GemmArgsF64& g, const GemmPlan& plan, double* workspace, cudaStream_t st) {
     if (plan.tile == TILE_GEMV && gemv_applies(g.m, g.n, g.k, g.tri)) return dgemv_route(g, plan.splits, workspace, st);
     if (skinny_gemm_applies(g.m, g.n, g.k, g.tri)) {
-        static const bool tma = [] {  // opt-in until measured: ZYNUM_GPU_SKINNY_TMA=1
+        static const bool tma = [] {  // TMA-fed kernel unless ZYNUM_GPU_SKINNY_TMA=0
             const char* v = std::getenv("ZYNUM_GPU_SKINNY_TMA");
-            return v && v[0] == '1';
+            return !(v && v[0] == '0');
         }();
         return (tma && dgemm_skinny_tma_applies(g)) ? dgemm_skinny_tma(g, st) : dgemm_skinny(g, st);
     }

@@ -27,8 +27,6 @@
 // 3xBF16 SGEMM: x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and
 // C ~= hi_A hi_B + hi_A lo_B + lo_A hi_B, one FP32 TMEM accumulator
 // (kind::f16 with BF16 inputs), same GEMM kernel with a FP32 epilogue.
-// 6xBF16 SGEMM: three terms per operand (x0 + x1 + x2 holds all 24 bits of
-// the FP32 significand) and the six products with t + u <= 2.
 //
 // Replaces, for the GPU, the reference's dense real GEMM body
 // (kernels/shared/matrix_matrix/packed_simd.zig:306) when the Ozaki method is
@@ -441,8 +439,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         // the job's accumulators must have been drained by the epilogue
                         // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
                         // so a tile's epilogue overlaps the next tile's products
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
-                                                            : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
                         ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
@@ -503,8 +500,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
-                                                        : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
                     ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
@@ -569,12 +565,7 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                             }
 #pragma unroll
                             for (int c = 0; c < 32; ++c) {
-                                // two accumulators: the products of order t + u <= 1 and those of
-                                // order 2, added exactly in FP64 and rounded once
-                                const float sum = two ? (float)((double)__uint_as_float(r0[c]) +
-                                                                (double)__uint_as_float(r1[c]))
-                                                      : __uint_as_float(r0[c]);
-                                const float v = P.alpha_f * sum;
+                                const float v = P.alpha_f * __uint_as_float(r0[c]);
                                 const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
                                 if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
                             }
@@ -832,8 +823,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                     for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
                         // EPI_F32 (one accumulator per tile) alternates the two TMEM buffers
                         // so a tile's epilogue overlaps the next tile's products
-                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
-                                                            : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
+                        const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
                         ++inst;
                         if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                         tphase ^= 1u << b;
@@ -915,8 +905,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool first = true;
             for (int j = 0; ok && j < P.num_jobs; ++j)
                 for (int ks = 0; ok && ks < P.num_kseg; ++ks) {
-                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j]
-                                                        : (EPI == EPI_F32 && P.job_groups[j] == 1 ? (inst & 1) : 0);
+                    const int b = (EPI == EPI_RESIDUE) ? P.job_buf[j] : (EPI == EPI_F32 ? (inst & 1) : 0);
                     ++inst;
                     if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                     tphase ^= 1u << b;
@@ -961,12 +950,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
                             }
 #pragma unroll
                             for (int c = 0; c < 32; ++c) {
-                                // two accumulators: the products of order t + u <= 1 and those of
-                                // order 2, added exactly in FP64 and rounded once
-                                const float sum = two ? (float)((double)__uint_as_float(r0[c]) +
-                                                                (double)__uint_as_float(r1[c]))
-                                                      : __uint_as_float(r0[c]);
-                                const float v = P.alpha_f * sum;
+                                const float v = P.alpha_f * __uint_as_float(r0[c]);
                                 const float out = !need_c ? v : (first ? fmaf(P.beta_f, cin[c], v) : cin[c] + v);
                                 if (full_chunk || col0 + c < P.n) __stcg(cb + (long)c * P.ldc, out);
                             }
@@ -990,11 +974,14 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
 // ------------------------------------------------------------- splitting
 // View of a matrix X (rows r, cols c): element at base[r * rs + c * cs];
 // exactly one of rs / cs is 1.
-struct View {
-    const double* base;
+template <typename T>
+struct ViewT {
+    const T* base;
     long rs, cs;
     int rows, cols;
 };
+using View = ViewT<double>;
+using ViewF = ViewT<float>;
 
 // |x| bit patterns at or above this one are Inf or NaN.
 constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
@@ -1005,8 +992,10 @@ ZB_DEVICE void note_nonfinite(int r, int* count, int* list) { list[atomicAdd(cou
 
 // Row maxima of |X| as FP64 bit patterns (non-negative doubles order like
 // unsigned integers; NaN patterns sort above +Inf and so propagate).
-// Also accumulates the row sums of |x| (used by the automatic slice count).
-__global__ void ozaki_absmax(View X, unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
+// Also accumulates the row sums of |x| (used by the automatic slice count and
+// the CRT row scale).  T = float reads FP32 operands, widened exactly.
+template <typename T>
+__global__ void ozaki_absmax(ViewT<T> X, unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
     if (X.rs == 1) {
         const int r = blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= X.rows) return;
@@ -1014,7 +1003,7 @@ __global__ void ozaki_absmax(View X, unsigned long long* __restrict__ maxbits, d
         unsigned long long mx = 0;
         double sm = 0.0;
         for (int c = c0; c < c1; ++c) {
-            const double a = fabs(X.base[r + (long)c * X.cs]);
+            const double a = fabs((double)X.base[r + (long)c * X.cs]);
             const unsigned long long v = (unsigned long long)__double_as_longlong(a);
             mx = v > mx ? v : mx;
             sm += a;
@@ -1029,7 +1018,7 @@ __global__ void ozaki_absmax(View X, unsigned long long* __restrict__ maxbits, d
         unsigned long long mx = 0;
         double sm = 0.0;
         for (int c = c0 + lane; c < c1; c += 32) {
-            const double a = fabs(X.base[(long)r * X.rs + c]);
+            const double a = fabs((double)X.base[(long)r * X.rs + c]);
             const unsigned long long v = (unsigned long long)__double_as_longlong(a);
             mx = v > mx ? v : mx;
             sm += a;
@@ -1115,7 +1104,7 @@ ozaki_split(View X, const unsigned long long* __restrict__ maxbits, int slices, 
         }
         const int gr = r0 + r, gc = c0 + c;
         double v = 0.0;
-        if (gr < X.rows && gc < X.cols) v = X.base[(long)gr * X.rs + (long)gc * X.cs];
+        if (gr < X.rows && gc < X.cols) v = (double)X.base[(long)gr * X.rs + (long)gc * X.cs];
         tile[swz(r, c)] = v;
     }
     __syncthreads();
@@ -1159,9 +1148,11 @@ ZB_DEVICE int crt_row_exponent(unsigned long long maxbits, double sum, int k, in
 // (plane l: rows_pad x cols_pad bytes, K-major) of round(2^{a_r} x) and the
 // row exponents a_r.  The integer (|.| <= 2^P <= 2^62) is biased by 2^63 so
 // that its eight bytes are unsigned digits; residue = dp4a(bytes, 2^{8t} mod m)
-// - (2^63 mod m), then one exact FP32 reduction.
+// - (2^63 mod m), then one exact FP32 reduction.  T = float: FP32 operands,
+// widened exactly to FP64 on load.
+template <typename T>
 __global__ void __launch_bounds__(256)
-ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const double* __restrict__ sums, int P,
+ozaki_crt_split(ViewT<T> X, const unsigned long long* __restrict__ maxbits, const double* __restrict__ sums, int P,
                 int nmod, int rows_pad, int cols_pad, int8_t* __restrict__ planes, int* __restrict__ exps,
                 int* __restrict__ nf_count, int* __restrict__ nf_list) {
     __shared__ double tile[32 * 128];
@@ -1188,7 +1179,7 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
         }
         const int gr = r0 + r, gc = c0 + c;
         double v = 0.0;
-        if (gr < X.rows && gc < X.cols) v = X.base[(long)gr * X.rs + (long)gc * X.cs];
+        if (gr < X.rows && gc < X.cols) v = (double)X.base[(long)gr * X.rs + (long)gc * X.cs];
         tile[swz(r, c)] = v;
     }
     __syncthreads();
@@ -1230,13 +1221,13 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 // value v = sum_t byte_t (2^8t mod m) - (2^63 mod m), |v| < 2^18; the dp4a
-                // result is the bit pattern of the float 1.5 2^23 + v, so x = v exactly;
-                // q = round(v / m) by the 1.5 2^23 shift, r = v - q m is exact and
-                // |r| <= (m - 1) / 2; r + 1.5 2^23 carries r in its low byte
+                // result is the bit pattern of the float f = 1.5 2^23 + v, so x = v exactly;
+                // q = round(v / m) by the 1.5 2^23 shift; f - q m = 1.5 2^23 + r is exact
+                // with |r| <= (m - 1) / 2 and carries r in the low byte of its pattern
                 const int d = dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
-                const float x = __int_as_float(d) - 12582912.0f;
-                const float q = __fmaf_rn(x, inv, 12582912.0f) - 12582912.0f;
-                rb[i] = (uint32_t)__float_as_int(__fmaf_rn(-q, m, x) + 12582912.0f);
+                const float f = __int_as_float(d);
+                const float q = __fmaf_rn(f - 12582912.0f, inv, 12582912.0f) - 12582912.0f;
+                rb[i] = (uint32_t)__float_as_int(__fmaf_rn(-q, m, f));
             }
             w[g] = __byte_perm(__byte_perm(rb[0], rb[1], 0x0040), __byte_perm(rb[2], rb[3], 0x0040), 0x5410);
         }
@@ -1245,13 +1236,14 @@ ozaki_crt_split(View X, const unsigned long long* __restrict__ maxbits, const do
 }
 
 // CRT weights w_l = M_l (M_l^-1 mod m_l) mod M and M = prod m_l (< 2^127 for
-// 16 moduli) as eight balanced 16-bit limbs.  wpair[z][g] packs limb z of the
-// weights of moduli (4g, 4g+1) (.x) and (4g+2, 4g+3) (.y) as two int16 each:
-// the operands of dp2a.lo / dp2a.hi against four packed int8 residues.
+// 16 moduli).  The weights are held as 16 balanced base-256 digits d_{l,z} in
+// [-128, 127], packed as the B operand of an int8 m16n8k16 MMA: wb[h][t][g]
+// holds d_{4t+i, 8h+g} in byte i (moduli 4t .. 4t+3, digit 8h + g).  M itself
+// is kept as eight balanced 16-bit limbs for the reduction S - q M.
 constexpr int kCrtLimbs = 8;
 struct CrtCombine {
     int nmod;
-    uint2 wpair[kCrtLimbs][kCrtMaxModuli / 4];
+    uint32_t wb[2][4][8];
     int M[kCrtLimbs];
     double M_d, inv_M;
 };
@@ -1268,90 +1260,103 @@ ZB_DEVICE double i2d(int v) {
     return __hiloint2double(0x43300000, v ^ 0x80000000) - 4503601774854144.0;  // 2^52 + 2^31
 }
 
-// d = c + a.s16[0] * b.s8[0] + a.s16[1] * b.s8[1]  (HI: bytes 2, 3 of b)
-template <bool HI>
-ZB_DEVICE int dp2a_ss(uint32_t a, uint32_t b, int c) {
-    int d;
-    if (HI)
-        asm("dp2a.hi.s32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
-    else
-        asm("dp2a.lo.s32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
-    return d;
+// D (16 x 8, s32) = A (16 x 16, s8, row) B (16 x 8, s8, col): lane (g, t) holds
+// a0 = A[g][4t .. 4t+3], a1 = A[g+8][4t .. 4t+3], b = B[4t .. 4t+3][g] and
+// receives D[g][2t, 2t+1] (d0, d1), D[g+8][2t, 2t+1] (d2, d3).
+ZB_DEVICE void imma_16x8x16(int (&d)[4], uint32_t a0, uint32_t a1, uint32_t b) {
+    asm("mma.sync.aligned.m16n8k16.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%7,%7,%7,%7};\n"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3])
+        : "r"(a0), "r"(a1), "r"(b), "r"(0));
 }
 
+constexpr int kLimbStride = 9;  // words per element in the limb buffer: conflict-free stores and loads
+
 // C = alpha 2^{-(a_i + b_j)} CRT(r_0..r_{n-1}) + beta C on a 16 x 128 tile of
-// row-major residue planes.  Warp w takes rows w and w + 8, lane L columns
-// 4L .. 4L+3: per plane one 4-byte load (128 contiguous bytes per warp); a
-// byte transpose (PRMT) packs four moduli of one element per register; limb z
-// of S = sum_l r_l w_l is 8 dp2a (|limb sum| < 2^26, exact in int32).
+// row-major residue planes.  Warp w takes rows w and w + 8 in two 64-column
+// segments each.  The digit sums S_z = sum_l r_l d_{l,z} of 64 elements x 16
+// digits are a product (64 x 16 residues) (16 x 16 digits) on the int8 tensor
+// pipe: MMA tile u holds the columns 4x + u (x = 0..15) of the segment, so the
+// four bytes at columns 4g .. 4g+3 of moduli 4t .. 4t+3 (one 4-byte load per
+// modulus) byte-transpose into the A fragments of all four tiles.  Lane (g, t)
+// then holds the 16-bit limbs S_{2y} + 256 S_{2y+1} (y = t, 4 + t) of eight
+// elements; a per-warp shared buffer regroups them so that lane L owns all
+// eight limbs of columns L and 32 + L (|limb| < 2^27, exact in int32).
 // q = round(S / M) from an FP64 estimate (|C_bar| <= M / 4 keeps S / M near an
 // integer); C_bar = S - q M is carried to balanced 16-bit limbs and rounded to
 // FP64 from the top limb down.  The scaled results pass through shared memory
-// so that C (column-major) is written 128 bytes per column.
-template <int NMOD>
+// so that C (column-major) is written 128 bytes per column.  T = float: the
+// FP64 value alpha x + beta C is rounded once to FP32.
+template <int NMOD, typename T>
 __global__ void __launch_bounds__(256)
 ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
-                  const int* __restrict__ expb, double alpha, double beta, double* __restrict__ C, long ldc,
+                  const int* __restrict__ expb, double alpha, double beta, T* __restrict__ C, long ldc,
                   const __grid_constant__ CrtCombine K, const int* __restrict__ status) {
-    constexpr int G = (NMOD + 3) / 4;  // groups of four moduli
     // every modulus is >= 191 > 2^7.5, so log2 M >= 7.5 NMOD
     constexpr int Z0 = (15 * NMOD - 78) > 0 ? (15 * NMOD - 78) / 32 : 0;
     constexpr double kScaleZ0 = pow2_const(16 * Z0);
     // The modular products did not all complete (a bounded wait ran out): C stays as it was.
     if (*status) return;
-    __shared__ double ct[16][129];  // column 4L + e holds element (4L + e - L) & 3 of lane L
-    __shared__ bool skip_row[16], skip_col[128];  // Inf / NaN in the row of op(A) / column of op(B)
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    __shared__ double ct[16][129];
+    __shared__ int lb[8][64 * kLimbStride];
+    __shared__ int sexa[16], sexb[128];  // row / column exponents (kNonFinite: Inf / NaN in the row / column)
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, g = lane >> 2, q4 = lane & 3;
     const int i0 = blockIdx.x * 16, j0 = blockIdx.y * 128;
-    const int jc = j0 + lane * 4;  // < n_pad: the planes are padded to 256 columns
-    const int4 e4 = __ldg(reinterpret_cast<const int4*>(expb + jc));
-    const int eb[4] = {e4.x, e4.y, e4.z, e4.w};
-    if (warp == 0) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) skip_col[lane * 4 + e] = eb[e] == kNonFinite;
-        if (lane < 16) skip_row[lane] = expa[i0 + lane] == kNonFinite;  // < m_pad
-    }
+    if (t < 128) sexb[t] = expb[j0 + t];  // < n_pad: the planes are padded to 256 columns
+    if (t < 16) sexa[t] = expa[i0 + t];   // < m_pad: the planes are padded to 128 rows
+    const uint32_t b_lo = K.wb[0][q4][g], b_hi = K.wb[1][q4][g];
+    int* my = lb[warp];
+    __syncthreads();
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-        const int rl = warp + 8 * h, gi = i0 + rl;  // < m_pad: the planes are padded to 128 rows
-        const int8_t* rp = res + (long)gi * res_ld + jc;
-        int cs[4][kCrtLimbs];
+    for (int unit = 0; unit < 4; ++unit) {
+        const int rl = warp + 8 * (unit >> 1), seg = unit & 1, gi = i0 + rl;
+        const int8_t* rp = res + (long)gi * res_ld + j0 + seg * 64 + 4 * g;
+        uint32_t v[2][4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
+        for (int e2 = 0; e2 < 2; ++e2)
 #pragma unroll
-            for (int z = 0; z < kCrtLimbs; ++z) cs[e][z] = 0;
+            for (int i = 0; i < 4; ++i) {
+                const int l = 4 * q4 + i;
+                v[e2][i] = l < NMOD ? __ldcs(reinterpret_cast<const uint32_t*>(rp + l * plane + 32 * e2)) : 0u;
+            }
+        // a[e2][u]: residues of moduli 4t .. 4t+3 of column 4g + 32 e2 + u
+        uint32_t a[2][4];
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-            uint32_t v[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                v[u] = 4 * g + u < NMOD ? __ldcs(reinterpret_cast<const uint32_t*>(rp + (4 * g + u) * plane)) : 0u;
-            // pk[e]: residues of moduli 4g .. 4g+3 of element e
-            const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140), t1 = __byte_perm(v[2], v[3], 0x5140);
-            const uint32_t t2 = __byte_perm(v[0], v[1], 0x7362), t3 = __byte_perm(v[2], v[3], 0x7362);
-            const uint32_t pk[4] = {__byte_perm(t0, t1, 0x5410), __byte_perm(t0, t1, 0x7632),
-                                    __byte_perm(t2, t3, 0x5410), __byte_perm(t2, t3, 0x7632)};
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-#pragma unroll
-                for (int z = 0; z < kCrtLimbs; ++z) {
-                    cs[e][z] = dp2a_ss<false>(K.wpair[z][g].x, pk[e], cs[e][z]);
-                    cs[e][z] = dp2a_ss<true>(K.wpair[z][g].y, pk[e], cs[e][z]);
-                }
+        for (int e2 = 0; e2 < 2; ++e2) {
+            const uint32_t t0 = __byte_perm(v[e2][0], v[e2][1], 0x5140), t1 = __byte_perm(v[e2][2], v[e2][3], 0x5140);
+            const uint32_t t2 = __byte_perm(v[e2][0], v[e2][1], 0x7362), t3 = __byte_perm(v[e2][2], v[e2][3], 0x7362);
+            a[e2][0] = __byte_perm(t0, t1, 0x5410);
+            a[e2][1] = __byte_perm(t0, t1, 0x7632);
+            a[e2][2] = __byte_perm(t2, t3, 0x5410);
+            a[e2][3] = __byte_perm(t2, t3, 0x7632);
         }
-        const int ea = expa[gi];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            int* c = cs[e];
+        for (int u = 0; u < 4; ++u) {
+            int dl[4], dh[4];
+            imma_16x8x16(dl, a[0][u], a[1][u], b_lo);  // digits 2t, 2t+1
+            imma_16x8x16(dh, a[0][u], a[1][u], b_hi);  // digits 8 + 2t, 9 + 2t
+            const int e0 = 4 * g + u, e1 = 32 + 4 * g + u;
+            my[e0 * kLimbStride + q4] = dl[0] + 256 * dl[1];
+            my[e0 * kLimbStride + 4 + q4] = dh[0] + 256 * dh[1];
+            my[e1 * kLimbStride + q4] = dl[2] + 256 * dl[3];
+            my[e1 * kLimbStride + 4 + q4] = dh[2] + 256 * dh[3];
+        }
+        __syncwarp();
+        const int ea = sexa[rl];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int e = lane + 32 * s;
+            int c[kCrtLimbs];
+#pragma unroll
+            for (int z = 0; z < kCrtLimbs; ++z) c[z] = my[e * kLimbStride + z];
             // limbs below Z0 add less than 2^(16 Z0 + 27) <= M 2^-12 to S, so the
             // upper limbs place S / M within 2^-12 of its value
             double sd = i2d(c[kCrtLimbs - 1]);
 #pragma unroll
             for (int z = kCrtLimbs - 2; z >= Z0; --z) sd = fma(sd, 65536.0, i2d(c[z]));
             sd *= kScaleZ0;
-            const int q = __double2int_rn(sd * K.inv_M);
+            const int qq = __double2int_rn(sd * K.inv_M);
 #pragma unroll
-            for (int z = 0; z < kCrtLimbs; ++z) c[z] -= q * K.M[z];
+            for (int z = 0; z < kCrtLimbs; ++z) c[z] -= qq * K.M[z];
 #pragma unroll
             for (int z = 0; z < kCrtLimbs - 1; ++z) {
                 const int carry = (c[z] + 32768) >> 16;
@@ -1361,35 +1366,37 @@ ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m,
             double x = i2d(c[kCrtLimbs - 1]);
 #pragma unroll
             for (int z = kCrtLimbs - 2; z >= 0; --z) x = fma(x, 65536.0, i2d(c[z]));
-            const int sc = -(ea + eb[e]);
-            ct[rl][lane * 4 + ((e + lane) & 3)] = alpha * (sc >= -1022 && sc <= 1023 ? x * pow2(sc) : ldexp(x, sc));
+            const int sc = -(ea + sexb[seg * 64 + e]);
+            ct[rl][seg * 64 + e] = alpha * (sc >= -1022 && sc <= 1023 ? x * pow2(sc) : ldexp(x, sc));
         }
+        __syncwarp();  // the buffer is refilled by the next unit
     }
     __syncthreads();
     // column-major write: 16 consecutive rows (128 bytes) of one column per half-warp
     const int r = t & 15;
     const int gi = i0 + r;
-    if (gi >= m || skip_row[r]) return;  // rows holding Inf / NaN: left to the non-finite patch
+    if (gi >= m || sexa[r] == kNonFinite) return;  // rows holding Inf / NaN: left to the non-finite patch
 #pragma unroll 4
     for (int cc = t >> 4; cc < 128; cc += 16) {
         const int gj = j0 + cc;
         if (gj >= n) break;
-        if (skip_col[cc]) continue;
-        double* cp = C + (long)gj * ldc + gi;
-        double out = ct[r][(cc & ~3) | (((cc & 3) + (cc >> 2)) & 3)];
-        if (beta != 0.0) out = fma(beta, *cp, out);
-        *cp = out;
+        if (sexb[cc] == kNonFinite) continue;
+        T* cp = C + (long)gj * ldc + gi;
+        double out = ct[r][cc];
+        if (beta != 0.0) out = fma(beta, (double)*cp, out);
+        *cp = (T)out;
     }
 }
 
-using CombineFn = void (*)(const int8_t*, long, int, int, int, const int*, const int*, double, double, double*, long,
+template <typename T>
+using CombineFn = void (*)(const int8_t*, long, int, int, int, const int*, const int*, double, double, T*, long,
                            CrtCombine, const int*);
-template <int N>
-constexpr CombineFn combine_at(int nmod) {
+template <int N, typename T>
+constexpr CombineFn<T> combine_at(int nmod) {
     if constexpr (N == 1)
-        return &ozaki_crt_combine<1>;
+        return &ozaki_crt_combine<1, T>;
     else
-        return nmod == N ? &ozaki_crt_combine<N> : combine_at<N - 1>(nmod);
+        return nmod == N ? &ozaki_crt_combine<N, T> : combine_at<N - 1, T>(nmod);
 }
 
 // IEEE semantics for rows of op(A) / columns of op(B) that hold Inf or NaN.
@@ -1405,8 +1412,9 @@ constexpr CombineFn combine_at(int nmod) {
 // skips its arithmetic.
 constexpr int kPatchTile = 64, kPatchK = 16;
 
+template <typename T>
 __global__ void __launch_bounds__(256)
-ozaki_nonfinite_patch(View va, View vb, int m, int n, int k, double alpha, double beta, double* __restrict__ C,
+ozaki_nonfinite_patch(ViewT<T> va, ViewT<T> vb, int m, int n, int k, double alpha, double beta, T* __restrict__ C,
                       long ldc, const int* __restrict__ cnt_a, const int* __restrict__ list_a,
                       const int* __restrict__ cnt_b, const int* __restrict__ list_b, const int* __restrict__ expa,
                       const int* __restrict__ status) {
@@ -1428,8 +1436,8 @@ ozaki_nonfinite_patch(View va, View vb, int m, int n, int k, double alpha, doubl
         const int g0 = (int)(it / dense_tiles) * kPatchTile, d0 = (int)(it % dense_tiles) * kPatchTile;
         const int gcount = min(kPatchTile, (rows ? na : nb) - g0);
         const int* list = rows ? list_a : list_b;
-        const View& G = rows ? va : vb;
-        const View& D = rows ? vb : va;
+        const ViewT<T>& G = rows ? va : vb;
+        const ViewT<T>& D = rows ? vb : va;
         const bool warp_busy = warp * 8 < gcount;
         double acc[4][4] = {};
         for (int p0 = 0; p0 < k; p0 += kPatchK) {
@@ -1441,12 +1449,12 @@ ozaki_nonfinite_patch(View va, View vb, int m, int n, int k, double alpha, doubl
                 int gr, gp;
                 if (G.cs == 1) { gp = e % kPatchK; gr = e / kPatchK; } else { gr = e % kPatchTile; gp = e / kPatchTile; }
                 double v = 0.0;
-                if (gr < gcount && p0 + gp < k) v = G.base[(long)list[g0 + gr] * G.rs + (long)(p0 + gp) * G.cs];
+                if (gr < gcount && p0 + gp < k) v = (double)G.base[(long)list[g0 + gr] * G.rs + (long)(p0 + gp) * G.cs];
                 Gs[gp][gr] = v;
                 int dr, dp;
                 if (D.cs == 1) { dp = e % kPatchK; dr = e / kPatchK; } else { dr = e % kPatchTile; dp = e / kPatchTile; }
                 double w = 0.0;
-                if (d0 + dr < dense_ext && p0 + dp < k) w = D.base[(long)(d0 + dr) * D.rs + (long)(p0 + dp) * D.cs];
+                if (d0 + dr < dense_ext && p0 + dp < k) w = (double)D.base[(long)(d0 + dr) * D.rs + (long)(p0 + dp) * D.cs];
                 Ds[dp][dr] = w;
             }
             __syncthreads();
@@ -1476,26 +1484,16 @@ ozaki_nonfinite_patch(View va, View vb, int m, int n, int k, double alpha, doubl
                 if (d >= dense_ext) continue;
                 const int i = rows ? listed : d, j = rows ? d : listed;
                 if (!rows && expa[i] == kNonFinite) continue;  // the row pass wrote it
-                double* cp = C + (long)j * ldc + i;
+                T* cp = C + (long)j * ldc + i;
                 double out = alpha * acc[u][v];
-                if (beta != 0.0) out = out + beta * *cp;
-                *cp = out;
+                if (beta != 0.0) out = out + beta * (double)*cp;
+                *cp = (T)out;
             }
         }
     }
 }
 
 // 3xBF16 split of a float matrix view into hi / lo planes (bf16, K-major).
-struct ViewF {
-    const float* base;
-    long rs, cs;
-    int rows, cols;
-};
-
-// Split of a float matrix view into TERMS bfloat16 planes (K-major):
-// x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1); each remainder is
-// exact in FP32, so TERMS = 3 carries the full 24-bit significand.
-template <int TERMS>
 __global__ void __launch_bounds__(256)
 bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ planes) {
     __shared__ float tile[32][129];
@@ -1521,22 +1519,18 @@ bf16_split(ViewF X, int rows_pad, int cols_pad, __nv_bfloat16* __restrict__ plan
     const int r = t >> 3, q = t & 7;
     if (r0 + r >= rows_pad) return;
     const long plane = (long)rows_pad * cols_pad;
-    __nv_bfloat16 part[TERMS][16];
+    __nv_bfloat16 hi[16], lo[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        float x = tile[r][q * 16 + i];
-#pragma unroll
-        for (int u = 0; u < TERMS; ++u) {
-            part[u][i] = __float2bfloat16_rn(x);
-            x -= __bfloat162float(part[u][i]);
-        }
+        const float x = tile[r][q * 16 + i];
+        hi[i] = __float2bfloat16_rn(x);
+        lo[i] = __float2bfloat16_rn(x - __bfloat162float(hi[i]));
     }
     __nv_bfloat16* o = planes + (long)(r0 + r) * cols_pad + c0 + q * 16;
-#pragma unroll
-    for (int u = 0; u < TERMS; ++u) {
-        *reinterpret_cast<uint4*>(o + u * plane) = *reinterpret_cast<uint4*>(part[u]);
-        *reinterpret_cast<uint4*>(o + u * plane + 8) = *reinterpret_cast<uint4*>(part[u] + 8);
-    }
+    *reinterpret_cast<uint4*>(o) = *reinterpret_cast<uint4*>(hi);
+    *reinterpret_cast<uint4*>(o + 8) = *reinterpret_cast<uint4*>(hi + 8);
+    *reinterpret_cast<uint4*>(o + plane) = *reinterpret_cast<uint4*>(lo);
+    *reinterpret_cast<uint4*>(o + plane + 8) = *reinterpret_cast<uint4*>(lo + 8);
 }
 
 // ------------------------------------------------------------ host side
@@ -1785,13 +1779,24 @@ const CrtHost& crt_host(int nmod) {
                 }
             for (int z = 0; z < kCrtLimbs; ++z) out[z] = (int)L[z];
         };
+        // balanced base-256 digits: x = sum_z out[z] 256^z, out[z] in [-128, 128) (x < 2^126: the top one is small)
+        auto digits = [](unsigned __int128 x, int* out) {
+            long long D[16];
+            for (int z = 0; z < 16; ++z) D[z] = (long long)((x >> (8 * z)) & 0xFFu);
+            for (int z = 0; z < 15; ++z)
+                if (D[z] >= 128) {
+                    D[z] -= 256;
+                    D[z + 1] += 1;
+                }
+            for (int z = 0; z < 16; ++z) out[z] = (int)D[z];
+        };
         for (int n = 1; n <= kCrtMaxModuli; ++n) {
             unsigned __int128 M = 1;
             for (int l = 0; l < n; ++l) M *= (unsigned)kCrtModuli[l];
             CrtHost& h = table[n];
             h.K = CrtCombine{};
             h.K.nmod = n;
-            int w[kCrtMaxModuli][kCrtLimbs] = {};  // moduli beyond n keep zero weights
+            int d[kCrtMaxModuli][16] = {};  // base-256 digits; moduli beyond n keep zero weights
             for (int l = 0; l < n; ++l) {
                 const unsigned ml = (unsigned)kCrtModuli[l];
                 const unsigned __int128 Ml = M / ml;
@@ -1802,14 +1807,15 @@ const CrtHost& crt_host(int nmod) {
                         y = c;
                         break;
                     }
-                limbs(Ml * y % M, w[l]);
+                digits(Ml * y % M, d[l]);
             }
-            for (int z = 0; z < kCrtLimbs; ++z)
-                for (int g = 0; g < kCrtMaxModuli / 4; ++g) {
-                    auto pack = [](int lo, int hi) { return (uint32_t)(uint16_t)lo | ((uint32_t)(uint16_t)hi << 16); };
-                    h.K.wpair[z][g].x = pack(w[4 * g][z], w[4 * g + 1][z]);
-                    h.K.wpair[z][g].y = pack(w[4 * g + 2][z], w[4 * g + 3][z]);
-                }
+            for (int hh = 0; hh < 2; ++hh)
+                for (int t = 0; t < 4; ++t)
+                    for (int g = 0; g < 8; ++g) {
+                        uint32_t word = 0;
+                        for (int i = 0; i < 4; ++i) word |= (uint32_t)(uint8_t)(int8_t)d[4 * t + i][8 * hh + g] << (8 * i);
+                        h.K.wb[hh][t][g] = word;
+                    }
             limbs(M, h.K.M);
             h.K.M_d = (double)M;
             h.K.inv_M = 1.0 / h.K.M_d;
@@ -1824,19 +1830,21 @@ std::atomic<int> g_last_moduli{0};
 
 // Rows of op(A) / columns of op(B) holding Inf or NaN: their entries of C are
 // computed in IEEE FP64 after the emulated product (which leaves them alone).
-cudaError_t launch_nonfinite_patch(const GemmArgsF64& g, const View& va, const View& vb, const Layout& L, uint8_t* w,
-                                   cudaStream_t st) {
+template <typename T>
+cudaError_t launch_nonfinite_patch(const GemmArgs<T>& g, const ViewT<T>& va, const ViewT<T>& vb, const Layout& L,
+                                   uint8_t* w, cudaStream_t st) {
     const int* cnta = reinterpret_cast<const int*>(w + L.cnta_off);
     const int* cntb = reinterpret_cast<const int*>(w + L.cntb_off);
-    ozaki_nonfinite_patch<<<2 * sm_count_cached(), 256, 0, st>>>(
-        va, vb, g.m, g.n, g.k, g.alpha, g.beta, g.c, g.ldc, cnta, reinterpret_cast<const int*>(w + L.lista_off), cntb,
+    ozaki_nonfinite_patch<T><<<2 * sm_count_cached(), 256, 0, st>>>(
+        va, vb, g.m, g.n, g.k, (double)g.alpha, (double)g.beta, g.c, g.ldc, cnta, reinterpret_cast<const int*>(w + L.lista_off), cntb,
         reinterpret_cast<const int*>(w + L.listb_off), reinterpret_cast<const int*>(w + L.expa_off),
         reinterpret_cast<const int*>(w + L.status_off));
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready) {
+template <typename T>
+cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready) {
     const Layout L = ozaki_layout(p);
     uint8_t* w = static_cast<uint8_t*>(ws);
     int8_t* a_planes = reinterpret_cast<int8_t*>(w + L.a_planes_off);
@@ -1857,29 +1865,29 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     const CrtHost& H = crt_host(nmod);
     g_last_moduli.store(nmod);
 
-    View va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
-    View vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
+    ViewT<T> va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
+    ViewT<T> vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
     // a_ready: op(A)'s statistics, exponents, Inf / NaN row list and planes stay;
     // op(B)'s accumulators, its list count and the status word are cleared
     cudaError_t e = a_ready ? cudaMemsetAsync(w + L.maxb_off, 0, L.b_clear_end - L.maxb_off, st)
                             : cudaMemsetAsync(w, 0, L.b_clear_end, st);
     if (e != cudaSuccess) return e;
     for (int side = a_ready ? 1 : 0; side < 2; ++side) {
-        const View& v = side ? vb : va;
+        const ViewT<T>& v = side ? vb : va;
         if (v.rs == 1) {
             dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
-            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+            ozaki_absmax<T><<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
         } else {
             dim3 grid((v.rows + 7) / 8, (v.cols + 1023) / 1024);
-            ozaki_absmax<<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
+            ozaki_absmax<T><<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
         }
         count_launch();
     }
     for (int side = a_ready ? 1 : 0; side < 2; ++side) {
-        const View& v = side ? vb : va;
+        const ViewT<T>& v = side ? vb : va;
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
-        ozaki_crt_split<<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma, H.P, nmod, rows_pad,
+        ozaki_crt_split<T><<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma, H.P, nmod, rows_pad,
                                                p.k_pad, side ? b_planes : a_planes, side ? expb : expa,
                                                side ? cntb : cnta, side ? listb : lista);
         count_launch();
@@ -1936,8 +1944,9 @@ cudaError_t dgemm_ozaki_crt(const GemmArgsF64& g, const OzakiPlan& p, void* ws, 
     if (e != cudaSuccess) return e;
 
     dim3 cgrid((g.m + 15) / 16, (g.n + 127) / 128);
-    combine_at<kCrtMaxModuli>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
-                                                          g.alpha, g.beta, g.c, g.ldc, H.K, status);
+    combine_at<kCrtMaxModuli, T>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
+                                                             (double)g.alpha, (double)g.beta, g.c, g.ldc, H.K,
+                                                             status);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_nonfinite_patch(g, va, vb, L, w, st);
@@ -1950,8 +1959,23 @@ int ozaki_crt_bits(int moduli) {
 }
 int ozaki_last_moduli() { return g_last_moduli.load(); }
 
+int sgemm_crt_moduli(int k) {
+    // scaling bits P >= 25 + log2(sqrt(k)): a row whose entries all have the
+    // magnitude of its largest has 2-norm max sqrt(k), so every such entry keeps
+    // its 24-bit significand and a guard bit
+    const double need = 25.0 + 0.5 * std::log2((double)std::max(k, 1));
+    for (int n = 2; n <= kCrtMaxModuli; ++n)
+        if (crt_host(n).P >= need) return n;
+    return kCrtMaxModuli;
+}
+
+cudaError_t sgemm_ozaki(const GemmArgsF32& g, const OzakiPlan& p, void* ws, cudaStream_t st) {
+    if (p.scheme != OZAKI_CRT || g.k > kCrtMaxK) return cudaErrorInvalidValue;
+    return gemm_ozaki_crt<float>(g, p, ws, st, false);
+}
+
 cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& plan, void* ws, cudaStream_t st, bool a_ready) {
-    if (plan.scheme == OZAKI_CRT) return dgemm_ozaki_crt(g, plan, ws, st, a_ready);
+    if (plan.scheme == OZAKI_CRT) return gemm_ozaki_crt<double>(g, plan, ws, st, a_ready);
     // the slice scheme (its slice count depends on both operands) always recomputes op(A)
     OzakiPlan p = plan;
     const Layout L = ozaki_layout(p);
@@ -2091,30 +2115,28 @@ int ozaki_take_wait_report(cudaStream_t stream, cudaError_t* err) {
     return e == cudaSuccess ? v : 0;
 }
 
-size_t bf16_split_workspace_bytes(int m, int n, int k, int terms) {
+size_t bf16x3_workspace_bytes(int m, int n, int k) {
     const long mp = round_up(m, use_cta_pair(m) ? 2 * kUM : kUM), np = round_up(n, kUN), kp = round_up(k, 128);
-    return (size_t)(terms * mp * kp * 2 + terms * np * kp * 2 + 1024);
+    return (size_t)(2 * mp * kp * 2 + 2 * np * kp * 2 + 1024);
 }
 
-cudaError_t sgemm_bf16_split(const GemmArgsF32& g, int terms, void* ws, cudaStream_t st) {
+cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st) {
     // K is padded to 128 elements: the split kernel writes 128 columns per block.
     const bool pair = use_cta_pair(g.m);
     const int mp = (int)round_up(g.m, pair ? 2 * kUM : kUM), np = (int)round_up(g.n, kUN), kp = (int)round_up(g.k, 128);
     __nv_bfloat16* a_planes = static_cast<__nv_bfloat16*>(ws);
-    __nv_bfloat16* b_planes = a_planes + (long)terms * mp * kp;
+    __nv_bfloat16* b_planes = a_planes + 2L * mp * kp;
     ViewF va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     ViewF vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
-    auto split = terms == 3 ? bf16_split<3> : bf16_split<2>;
-    split<<<dim3((kp + 127) / 128, mp / 32), 256, 0, st>>>(va, mp, kp, a_planes);
+    bf16_split<<<dim3((kp + 127) / 128, mp / 32), 256, 0, st>>>(va, mp, kp, a_planes);
     count_launch();
-    split<<<dim3((kp + 127) / 128, np / 32), 256, 0, st>>>(vb, np, kp, b_planes);
+    bf16_split<<<dim3((kp + 127) / 128, np / 32), 256, 0, st>>>(vb, np, kp, b_planes);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     CUtensorMap ma, mb;
-    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, (long)terms * mp, kUM)) != cudaSuccess)
-        return e;
-    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, (long)terms * np, pair ? kUN / 2 : kUN)) !=
+    if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * mp, kUM)) != cudaSuccess) return e;
+    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kp, 2L * np, pair ? kUN / 2 : kUN)) !=
         cudaSuccess)
         return e;
     UmmaParams P{};
@@ -2123,33 +2145,24 @@ cudaError_t sgemm_bf16_split(const GemmArgsF32& g, int terms, void* ws, cudaStre
     P.m_pad = mp;
     P.n_pad = np;
     P.k_chunks = kp / 64;
-    // K segments (64-deep chunks each; 0 = all of K): each segment starts a fresh
-    // accumulator and its sum is added to C in FP32 by the epilogue
-    int seg = 0;
-    if (const char* v = std::getenv("ZYNUM_GPU_BF16_KSEG")) seg = std::atoi(v);
-    P.kseg_chunks = seg > 0 && seg < P.k_chunks ? seg : P.k_chunks;
-    P.num_kseg = (P.k_chunks + P.kseg_chunks - 1) / P.kseg_chunks;
+    P.kseg_chunks = P.k_chunks;
+    P.num_kseg = 1;
     P.tiles_m = mp / (pair ? 2 * kUM : kUM);
     P.tiles_n = np / kUN;
     P.num_tiles = P.tiles_m * P.tiles_n;
-    // one job, consecutive steps share a plane:
-    //   2 terms: x0 y1, x0 y0, x1 y0 (products with t + u <= 1) in one FP32 accumulator;
-    //   3 terms: x0 y2, x0 y1, x0 y0, x1 y0, x1 y1, x2 y0 (t + u <= 2), the order-2
-    //   products in the second accumulator: about 2^-16 of the order-0 ones, they
-    //   would fall below half an ulp of a running sum that holds the rest
-    static const int sa2[3] = {0, 0, 1}, sb2[3] = {1, 0, 0};
-    static const int sa3[6] = {0, 0, 0, 1, 1, 2}, sb3[6] = {2, 1, 0, 0, 1, 0};
-    const int nsteps = terms == 3 ? 6 : 3;
+    // one job, one FP32 accumulator: hi*lo, hi*hi, lo*hi (consecutive steps
+    // share an operand); plane 0 = hi, 1 = lo
     P.num_jobs = 1;
     P.job_first_step[0] = 0;
-    P.job_num_steps[0] = nsteps;
-    P.job_groups[0] = terms == 3 ? 2 : 1;
+    P.job_num_steps[0] = 3;
+    P.job_groups[0] = 1;
     P.job_shift[0][0] = 0;
     P.job_shift[0][1] = 0;
-    for (int q = 0; q < nsteps; ++q) {
-        P.step_a[q] = terms == 3 ? sa3[q] : sa2[q];
-        P.step_b[q] = terms == 3 ? sb3[q] : sb2[q];
-        P.step_acc[q] = terms == 3 ? (P.step_a[q] + P.step_b[q] == 2 ? 1 : 0) : 0;
+    const int sa[3] = {0, 0, 1}, sb[3] = {1, 0, 0};
+    for (int q = 0; q < 3; ++q) {
+        P.step_a[q] = sa[q];
+        P.step_b[q] = sb[q];
+        P.step_acc[q] = 0;
     }
     P.alpha_f = g.alpha;
     P.beta_f = g.beta;

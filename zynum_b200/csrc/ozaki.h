@@ -1,4 +1,4 @@
-// Ozaki-scheme DGEMM (INT8 tcgen05 slices) and 3xBF16 SGEMM.
+// Ozaki-scheme DGEMM and SGEMM (INT8 tcgen05 slices / CRT residues) and 3xBF16 SGEMM.
 #pragma once
 
 #include <cstddef>
@@ -70,11 +70,17 @@ size_t ozaki_workspace_bytes(const OzakiPlan& p);
 // they are reused, not recomputed.  The plan may cover more columns than g.n.
 cudaError_t dgemm_ozaki(const GemmArgsF64& g, const OzakiPlan& p, void* ws, cudaStream_t st, bool a_ready = false);
 
-// C = alpha op(A) op(B) + beta C as a split product of `terms` bfloat16
-// planes per operand with FP32 accumulation in TMEM: terms = 2 takes the 3
-// products with t + u <= 1 (about 16 bits), terms = 3 the 6 products with
-// t + u <= 2 (the FP32 significand); `ws` holds bf16_split_workspace_bytes.
-size_t bf16_split_workspace_bytes(int m, int n, int k, int terms);
-cudaError_t sgemm_bf16_split(const GemmArgsF32& g, int terms, void* ws, cudaStream_t st);
+// FP32 GEMM through the CRT scheme: FP32 operands are scaled per row of op(A) /
+// column of op(B) to integers (exact FP64 widening first), multiplied modulo
+// sgemm_crt_moduli(k) int8 moduli with exact INT32 accumulation, reconstructed
+// in FP64 and rounded once to FP32 (alpha x + beta C in FP64).  Rows / columns
+// holding Inf or NaN get IEEE results from a plain dot-product patch.
+// The plan comes from plan_ozaki(m, n, k, 0, OZAKI_CRT, moduli), k <= kCrtMaxK.
+int sgemm_crt_moduli(int k);
+cudaError_t sgemm_ozaki(const GemmArgsF32& g, const OzakiPlan& p, void* ws, cudaStream_t st);
+
+size_t bf16x3_workspace_bytes(int m, int n, int k);
+// C = alpha op(A) op(B) + beta C as a 3xBF16 split product with FP32 accumulation.
+cudaError_t sgemm_bf16x3(const GemmArgsF32& g, void* ws, cudaStream_t st);
 
 }  // namespace zb

@@ -27,7 +27,7 @@ int parse_method_env() {
 int parse_smethod_env() {
     const char* v = std::getenv("ZYNUM_GPU_SGEMM_METHOD");
     if (v && !std::strcmp(v, "bf16x3")) return SMETHOD_BF16X3;
-    if (v && !std::strcmp(v, "bf16x6")) return SMETHOD_BF16X6;
+    if (v && !std::strcmp(v, "ozaki")) return SMETHOD_OZAKI;
     return SMETHOD_NATIVE;
 }
 int parse_complex_env() {

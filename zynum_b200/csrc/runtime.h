@@ -22,7 +22,7 @@
 namespace zb {
 
 enum DgemmMethod : int { METHOD_NATIVE = 0, METHOD_OZAKI = 1, METHOD_AUTO = 2 };
-enum SgemmMethod : int { SMETHOD_NATIVE = 0, SMETHOD_BF16X3 = 1, SMETHOD_BF16X6 = 2 };
+enum SgemmMethod : int { SMETHOD_NATIVE = 0, SMETHOD_BF16X3 = 1, SMETHOD_OZAKI = 2 };
 
 // A device buffer that only grows.  Growing synchronises `stream` first so the
 // old allocation is no longer in use.
