@@ -3,11 +3,11 @@
 // No counterpart in the reference (Zynum has no batched API); the per-problem
 // semantics are those of gemm.zig:1392 and triangular.zig:233.
 //
-// GEMM: the host turns the batch into a list of output tiles (problem, m0, n0,
-// tile config) ordered longest-first and dealt round-robin to a fixed grid of
-// persistent CTAs (deterministic, no atomics, so one launch is graph-capturable
-// and replayable).  Each size bucket gets its tile config from the autotuner
-// (tuner.cpp).  FP64 tiles use DMMA (mma.sync m16n8k8 .f64), FP32 tiles FFMA;
+// GEMM: the host turns the batch into a list of work items (chunks of output
+// tiles of one problem, with their tile config) ordered longest-first; the
+// persistent CTAs claim items in that order from a counter the launch zeroes
+// (a memset and the kernel, both graph-capturable and replayable).  Each size
+// bucket gets its tile config from the autotuner (batched_host.cpp).  FP64 tiles use DMMA (mma.sync m16n8k8 .f64), FP32 tiles FFMA;
 // operands are staged with cp.async (8- / 4-byte copies: per-problem leading
 // dimensions need not be aligned).
 //
@@ -342,40 +342,59 @@ ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, flo
 }
 
 // ------------------------------------------------- persistent kernels
+// Work items are claimed in list order (the host sorts them longest first)
+// from a device counter the launch zeroes: a CTA that finishes early takes
+// the next item, so the batch ends within about one item of its ideal
+// (greedy longest-first list scheduling).  Thread 0 claims the following item
+// while the CTA works on the current one.  Every tile is computed the same
+// way whichever CTA takes it, so results do not depend on the schedule.
+template <typename Fn>
+ZB_DEVICE void for_each_claimed(int* next, int n_work, Fn fn) {
+    __shared__ int s_item[2];
+    if (threadIdx.x == 0) s_item[0] = atomicAdd(next, 1);
+    __syncthreads();
+    int buf = 0;
+    for (int w = s_item[0]; w < n_work;) {
+        if (threadIdx.x == 0) s_item[buf ^ 1] = atomicAdd(next, 1);
+        fn(w);
+        __syncthreads();
+        buf ^= 1;
+        w = s_item[buf];
+    }
+}
+
 // FP64: 64 x 64 tiles at most, four CTAs per SM (measured: 4 CTAs x 2 stages of 64 x 64 >
 // 3 x 3 of 64 x 64 > 2 x 3 with 128 x 64 tiles, 15.8 / 15.4 / 13.9 TFLOP/s on the 20,000-problem
 // batch: more tiles in flight hide each tile's start-up latency)
 template <bool AK, bool BKF>
 __global__ void __launch_bounds__(kThreads, 4)
-dgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
-                     const double* const* __restrict__ a, const int* __restrict__ lda,
+dgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, int* __restrict__ next,
+                     const int* __restrict__ dims, const double* const* __restrict__ a, const int* __restrict__ lda,
                      const double* const* __restrict__ b, const int* __restrict__ ldb, double alpha, double beta,
                      double* const* __restrict__ c, const int* __restrict__ ldc) {
     extern __shared__ __align__(128) double sm_d[];
-    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    for_each_claimed(next, n_work, [&](int w) {
         const BatchWork it = work[w];
         const int q = it.prob;
-        if (q < 0) continue;  // padding item of the per-CTA schedule
         Prob<double> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
         // tile edges: batched_tile_m / batched_tile_n (FP64: TILE_CFG_128 runs as 64 x 64)
         if (it.cfg == TILE_CFG_128 || it.cfg == TILE_CFG_64)
             dgemm_chunk<64, 64, 2, AK, BKF>(p, it.t0, it.count, alpha, beta, sm_d);
         else
             dgemm_chunk<32, 32, 2, AK, BKF>(p, it.t0, it.count, alpha, beta, sm_d);
-    }
+    });
 }
 
 template <bool AM, bool BMF>
 __global__ void __launch_bounds__(kThreads, 2)
-sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* __restrict__ dims,
-                     const float* const* __restrict__ a, const int* __restrict__ lda,
+sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, int* __restrict__ next,
+                     const int* __restrict__ dims, const float* const* __restrict__ a, const int* __restrict__ lda,
                      const float* const* __restrict__ b, const int* __restrict__ ldb, float alpha, float beta,
                      float* const* __restrict__ c, const int* __restrict__ ldc) {
     extern __shared__ __align__(128) float sm_f[];
-    for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    for_each_claimed(next, n_work, [&](int w) {
         const BatchWork it = work[w];
         const int q = it.prob;
-        if (q < 0) continue;  // padding item of the per-CTA schedule
         Prob<float> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
         const int e = it.cfg == TILE_CFG_128 ? 128 : (it.cfg == TILE_CFG_64 ? 64 : 32);
         const int mt = (p.m + e - 1) / e;
@@ -388,7 +407,7 @@ sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, const int* 
             else  // warps 4 x 2 of 8 x 16, threads 2 x 2
                 sgemm_tile<32, 32, 4, 4, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
         }
-    }
+    });
 }
 
 size_t dsmem_bytes() {
@@ -875,8 +894,9 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
         auto kern = dgemm_batched_kernel<AKV, BKV>;                                                             \
         if ((e = ensure_dynamic_smem(kern, (int)sm)) != cudaSuccess) \
             return e;                                                                                           \
+        if ((e = cudaMemsetAsync(d.next, 0, sizeof(int), st)) != cudaSuccess) return e;                        \
         prof_begin(st);                                                                                         \
-        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
+        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.next, d.dims, A, lda, B, ldb, al, be, Cp, ldc);   \
         count_launch();                                                                                         \
         prof_end(st);                                                                                           \
         return cudaGetLastError();                                                                              \
@@ -895,8 +915,9 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
         auto kern = sgemm_batched_kernel<AMV, BMV>;                                                             \
         if ((e = ensure_dynamic_smem(kern, (int)sm)) != cudaSuccess) \
             return e;                                                                                           \
+        if ((e = cudaMemsetAsync(d.next, 0, sizeof(int), st)) != cudaSuccess) return e;                        \
         prof_begin(st);                                                                                         \
-        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.dims, A, lda, B, ldb, al, be, Cp, ldc);            \
+        kern<<<grid, kThreads, sm, st>>>(d.work, d.n_work, d.next, d.dims, A, lda, B, ldb, al, be, Cp, ldc);   \
         count_launch();                                                                                         \
         prof_end(st);                                                                                           \
         return cudaGetLastError();                                                                              \

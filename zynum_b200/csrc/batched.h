@@ -11,8 +11,7 @@ namespace zb {
 enum BatchDtype : int { BATCH_F64 = 0, BATCH_F32 = 1 };
 enum TileCfg : int { TILE_CFG_32 = 0, TILE_CFG_64 = 1, TILE_CFG_128 = 2 };
 
-// A chunk of `count` consecutive output tiles t0.. of one problem (prob < 0:
-// padding, skipped).  Tile t covers rows (t % mt) TM.. and columns (t / mt) TN..
+// A chunk of `count` consecutive output tiles t0.. of one problem.  Tile t covers rows (t % mt) TM.. and columns (t / mt) TN..
 // with TM x TN = batched_tile_m x batched_tile_n and mt = ceil(m / TM).
 struct BatchWork {
     int prob, t0, count, cfg;
@@ -20,9 +19,10 @@ struct BatchWork {
 
 // Device side of a GEMM batch plan.
 struct BatchDevice {
-    const BatchWork* work;
+    const BatchWork* work;  // longest first; CTAs claim items in this order
     int n_work;
     const int* dims;  // m, n, k per problem
+    int* next;        // claim counter, zeroed by each launch
 };
 
 // Output tile of a config: rows x columns (square; TILE_CFG_128 is 128 x 128

@@ -1,13 +1,16 @@
-// Host side of the batched GEMM / TRSM: plans, LPT schedule, autotuner with a
-// persistent JSON cache, and CUDA-graph replay.
+// Host side of the batched GEMM / TRSM: plans, longest-first schedules,
+// autotuner with a persistent JSON cache, and CUDA-graph replay.
 //
 // Plan (create): the problem sizes are given once on the host.  Each problem
-// is assigned a tile config by its size bucket (the autotuner's table), cut
-// into output tiles, and the tiles (TRSM: whole problems) are scheduled onto
-// a fixed grid of persistent CTAs longest-processing-time first; the
-// per-CTA lists are interleaved so that CTA b runs items b, b + G, b + 2G, ...
-// Run: one kernel launch (optionally replayed from a captured CUDA graph),
-// no allocation, so it can itself be captured by the caller.
+// is assigned a tile config by its size bucket (the autotuner's table) and cut
+// into chunks of output tiles.  GEMM: the chunks are sorted by estimated cost,
+// longest first, and the kernel's persistent CTAs claim them in that order
+// from a device counter (greedy list scheduling on the measured durations).
+// TRSM (whole problems): a static longest-processing-time assignment onto the
+// grid, the per-CTA lists interleaved so that CTA b runs items b, b + G, ...
+// Run: a counter reset (GEMM) and one kernel launch, optionally replayed from
+// a captured CUDA graph, no allocation, so it can itself be captured by the
+// caller.
 //
 // Autotuner: for every size bucket present in a batch (bucket = ceil(log2 of
 // max(m, n)), K class), each candidate tile config is timed on that bucket's
@@ -170,7 +173,8 @@ struct Batch {
     int grid = 148;
     // device
     int* d_dims = nullptr;
-    BatchWork* d_work = nullptr;
+    BatchWork* d_work = nullptr;  // work items, followed by the claim counter d_next
+    int* d_next = nullptr;
     int* d_order = nullptr;
     int n_items = 0;
     int cfg_counts[3] = {0, 0, 0};
@@ -212,19 +216,27 @@ std::vector<BatchWork> build_work(const Batch& b, const std::vector<int>& cfg, i
             if (counts) (*counts)[cfg[q]] += cnt;
         }
     }
-    std::vector<int> order = lpt_schedule(cost, grid);
+    // longest first: the kernel's CTAs claim items in this order
+    std::vector<int> order(items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
     std::vector<BatchWork> out(order.size());
-    for (size_t i = 0; i < order.size(); ++i) out[i] = order[i] < 0 ? BatchWork{-1, 0, 0, 0} : items[order[i]];
+    for (size_t i = 0; i < order.size(); ++i) out[i] = items[order[i]];
+    (void)grid;
     return out;
 }
 
 cudaError_t upload_work(Batch& b, const std::vector<BatchWork>& w) {
     cudaFree(b.d_work);
     b.d_work = nullptr;
+    b.d_next = nullptr;
     b.n_items = (int)w.size();
     if (w.empty()) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&b.d_work, w.size() * sizeof(BatchWork));
+    // the items, then the claim counter (16-byte aligned after them)
+    const size_t items_bytes = (w.size() * sizeof(BatchWork) + 15) / 16 * 16;
+    cudaError_t e = cudaMalloc(&b.d_work, items_bytes + 16);
     if (e != cudaSuccess) return e;
+    b.d_next = reinterpret_cast<int*>(reinterpret_cast<char*>(b.d_work) + items_bytes);
     return cudaMemcpy(b.d_work, w.data(), w.size() * sizeof(BatchWork), cudaMemcpyHostToDevice);
 }
 
@@ -260,7 +272,7 @@ float time_bucket(const Batch& b, const std::vector<int>& probs, int cfg, cudaSt
     std::vector<int> lds(sub.count, 512);
     cudaMemcpy(d_ptrs, ptrs.data(), sub.count * sizeof(void*), cudaMemcpyHostToDevice);
     cudaMemcpy(d_lds, lds.data(), sub.count * sizeof(int), cudaMemcpyHostToDevice);
-    BatchDevice dev{sub.d_work, sub.n_items, sub.d_dims};
+    BatchDevice dev{sub.d_work, sub.n_items, sub.d_dims, sub.d_next};
     const double one = 1.0, zero = 0.0;
     const float onef = 1.f, zerof = 0.f;
     const void* al = b.dtype == BATCH_F64 ? (const void*)&one : (const void*)&onef;
@@ -517,7 +529,7 @@ int zynum_blas_gpu_batch_info(zynum_blas_gpu_batch_t batch, int* items, int* gri
         args.ldb = ldb;                                                                                             \
         args.c = c;                                                                                                 \
         args.ldc = ldc;                                                                                             \
-        BatchDevice dev{bt->d_work, bt->n_items, bt->d_dims};                                                       \
+        BatchDevice dev{bt->d_work, bt->n_items, bt->d_dims, bt->d_next};                                                       \
         auto fn = [&](cudaStream_t s) {                                                                             \
             return launch_gemm_batched(dev, DT, bt->ta, bt->tb, &alpha, (const void* const*)a, lda,                \
                                        (const void* const*)b, ldb, &beta, (void* const*)c, ldc, bt->grid, s);       \

@@ -325,6 +325,9 @@ struct Relayout {
 
 Relayout relayout_plan(char transa, char transb, int m, int n, int k, const GemmPlan& plan) {
     Relayout r;
+    // the tall-skinny kernels read either layout and keep no partial sums: no workspace
+    // (so the route needs no allocation, e.g. on a stream under graph capture)
+    if (skinny_gemm_applies(m, n, k, 0)) return r;
     r.splitk = align_elems(splitk_workspace_elems(m, n, plan.splits));
     // the matrix-vector and narrow kernels read either layout directly
     if (plan.tile == TILE_GEMV || plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M) return r;
