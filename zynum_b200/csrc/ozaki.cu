@@ -1144,6 +1144,20 @@ ZB_DEVICE int crt_row_exponent(unsigned long long maxbits, double sum, int k, in
     return P - (e1 + e2);
 }
 
+// Two FP32 lanes per instruction (sm_100 packed FP32): d = a * b + c, d = a + b.
+ZB_DEVICE uint64_t ffma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;\n" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+ZB_DEVICE uint64_t fadd2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;\n" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+ZB_DEVICE uint64_t pack2(uint32_t lo, uint32_t hi) { return (uint64_t)hi << 32 | lo; }
+ZB_DEVICE uint64_t pack2f(float lo, float hi) { return pack2(__float_as_uint(lo), __float_as_uint(hi)); }
+
 // Each block: 32 rows x 128 columns of X -> `nmod` int8 residue planes
 // (plane l: rows_pad x cols_pad bytes, K-major) of round(2^{a_r} x) and the
 // row exponents a_r.  The integer (|.| <= 2^P <= 2^62) is biased by 2^63 so
@@ -1210,24 +1224,30 @@ ozaki_crt_split(ViewT<T> X, const unsigned long long* __restrict__ maxbits, cons
                    (lo[4 * g + 3] << 24);
         *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    const uint64_t kMagic2 = pack2f(12582912.0f, 12582912.0f), kNegMagic2 = pack2f(-12582912.0f, -12582912.0f);
     for (int l = 1; l < nmod; ++l) {
         const float m = (float)kCrt.m[l], inv = kCrt.inv[l];
+        const uint64_t m2 = pack2f(-m, -m), inv2 = pack2f(inv, inv);
         const uint32_t wl = kCrt.wlo[l], wh = kCrt.whi[l];
         const int c0 = kCrt.magic[l];
         uint32_t w[4];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
-            uint32_t rb[4];
+            // value v = sum_t byte_t (2^8t mod m) - (2^63 mod m), |v| < 2^18; the dp4a
+            // result is the bit pattern of the float f = 1.5 2^23 + v, so x = v exactly;
+            // q = round(v / m) by the 1.5 2^23 shift; f - q m = 1.5 2^23 + r is exact
+            // with |r| <= (m - 1) / 2 and carries r in the low byte of its pattern.  The
+            // FP32 steps run on two entries per instruction (f32x2).
+            uint32_t d[4], rb[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                // value v = sum_t byte_t (2^8t mod m) - (2^63 mod m), |v| < 2^18; the dp4a
-                // result is the bit pattern of the float f = 1.5 2^23 + v, so x = v exactly;
-                // q = round(v / m) by the 1.5 2^23 shift; f - q m = 1.5 2^23 + r is exact
-                // with |r| <= (m - 1) / 2 and carries r in the low byte of its pattern
-                const int d = dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
-                const float f = __int_as_float(d);
-                const float q = __fmaf_rn(f - 12582912.0f, inv, 12582912.0f) - 12582912.0f;
-                rb[i] = (uint32_t)__float_as_int(__fmaf_rn(-q, m, f));
+            for (int i = 0; i < 4; ++i) d[i] = (uint32_t)dp4a_us(lo[4 * g + i], wl, dp4a_us(hi[4 * g + i], wh, c0));
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint64_t f = pack2(d[2 * h], d[2 * h + 1]);
+                const uint64_t q = fadd2(ffma2(fadd2(f, kNegMagic2), inv2, kMagic2), kNegMagic2);
+                const uint64_t r = ffma2(q, m2, f);
+                rb[2 * h] = (uint32_t)r;
+                rb[2 * h + 1] = (uint32_t)(r >> 32);
             }
             w[g] = __byte_perm(__byte_perm(rb[0], rb[1], 0x0040), __byte_perm(rb[2], rb[3], 0x0040), 0x5410);
         }
