@@ -343,7 +343,7 @@ def time_device(torch, fn, steps, warmup, stream):
 def precision_methods(torch, blas, orc, n, steps, warmup, stream, seed):
     """The rest of the precision configuration on the headline size: DGEMM with
     entries u * 10^e, e ~ U[-phi, phi], for phi = 4 and 8, Ozaki and native on the
-    same inputs; SGEMM as a 3xBF16 and a 6xBF16 (FP32-accurate) split product and
+    same inputs; SGEMM as a 3xBF16 split product, as INT8 CRT residue products (exact, one rounding) and
     native FP32 on U[-1, 1] data.
     Each: time per call (CUDA events, inputs resident) and max / median relative
     error against the double-double oracle on 2048 sampled entries."""

@@ -250,7 +250,7 @@ ZYNUM_BLAS_GPU_API void cblas_dsyr2k(int layout, int uplo, int trans, int n, int
  * zynum_blas_gpu_set_dgemm_method / ZYNUM_GPU_DGEMM_METHOD (default native). */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dgemm_device(char transa, char transb, int m, int n, int k, double alpha, const double *a,
                                 int lda, const double *b, int ldb, double beta, double *c, int ldc, void *stream);
-/* Native FP32 (FFMA) or 3xBF16 SGEMM, chosen by zynum_blas_gpu_set_sgemm_method. */
+/* Native FP32 (FFMA), 3xBF16 or INT8 CRT SGEMM, chosen by zynum_blas_gpu_set_sgemm_method. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_sgemm_device(char transa, char transb, int m, int n, int k, float alpha, const float *a, int lda,
                                 const float *b, int ldb, float beta, float *c, int ldc, void *stream);
 

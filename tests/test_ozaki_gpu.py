@@ -375,7 +375,7 @@ def test_sgemm_bf16x3(blas, oracle, ta, tb):
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
 def test_host_panels_reuse_a_residues_bit_identical(blas, ta, tb):
-    """dgemm_ with host buffers large enough for column panels (here 4, the last one ragged)
+    """dgemm_ with host buffers large enough for column panels (here 8, the last one ragged)
     computes op(A)'s CRT residues once and reuses them for every panel: the result is
     bit-identical to the unpanelled device-pointer call on the same data."""
     import torch
