@@ -393,10 +393,10 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsymmetrize_device(char uplo, int n, doubl
 /* ------------------------------------------------- variable-size batches
  * No counterpart in the reference (Zynum has no batched API).  A batch plan is
  * created once from HOST arrays of problem sizes; running it is one
- * persistent-kernel launch (GEMM: preceded by a 4-byte reset of the plan's
- * work counter), or a replay of a CUDA graph holding them when use_graph != 0,
- * with no allocation.  Runs of one GEMM plan must not overlap on the GPU (they
- * share its work counter); separate plans may.  The per-problem operand arrays
+ * persistent-kernel launch, preceded by a 4-byte reset of the plan's work
+ * counter (or a replay of a CUDA graph holding both when use_graph != 0), with
+ * no allocation.  Runs of one plan must not overlap on the GPU (they share its
+ * work counter); separate plans may.  The per-problem operand arrays
  * passed to *_run (pointers and leading dimensions) are DEVICE arrays with one
  * entry per problem.  dtype: 0 = FP64, 1 = FP32.  Create returns 0 or the
  * index of the first illegal argument; run returns 0 or a negated CUDA error. */

@@ -363,6 +363,28 @@ ZB_DEVICE void for_each_claimed(int* next, int n_work, Fn fn) {
     }
 }
 
+// The same claiming as a loop header, for bodies that use `continue`:
+//   ZB_CLAIMED_LOOP(w, next, count) { ... }
+// (the increment step holds the CTA-wide barrier that publishes the next claim).
+struct Claim {
+    int* next;
+    int* slot;  // two shared-memory slots
+    int buf = 0;
+    ZB_DEVICE int first() {
+        if (threadIdx.x == 0) slot[0] = atomicAdd(next, 1);
+        __syncthreads();
+        return slot[0];
+    }
+    ZB_DEVICE void prefetch() {
+        if (threadIdx.x == 0) slot[buf ^ 1] = atomicAdd(next, 1);
+    }
+    ZB_DEVICE int advance() {
+        __syncthreads();
+        buf ^= 1;
+        return slot[buf];
+    }
+};
+
 // FP64: 64 x 64 tiles at most, four CTAs per SM (measured: 4 CTAs x 2 stages of 64 x 64 >
 // 3 x 3 of 64 x 64 > 2 x 3 with 128 x 64 tiles, 15.8 / 15.4 / 13.9 TFLOP/s on the 20,000-problem
 // batch: more tiles in flight hide each tile's start-up latency)
@@ -555,7 +577,7 @@ ZB_DEVICE void substitute_rhs(T (*X)[kPP], const T (*D)[kTP], const T* dinv, int
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2)
-trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
+trsm_batched_kernel(const int* __restrict__ order, int count, int* __restrict__ next, const int* __restrict__ dims, char uplo, char trans,
                     char diag, T alpha, const T* const* __restrict__ a, const int* __restrict__ lda,
                     T* const* __restrict__ b, const int* __restrict__ ldb) {
     extern __shared__ __align__(16) unsigned char trsm_smem[];
@@ -570,9 +592,11 @@ trsm_batched_kernel(const int* __restrict__ order, int count, const int* __restr
     const bool upper = (trans == 'N' && uplo == 'U') || (trans != 'N' && uplo == 'L');
     const bool unit = diag == 'U';
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int w = blockIdx.x; w < count; w += gridDim.x) {
+    __shared__ int claim_slot[2];
+    Claim cl{next, claim_slot};
+    for (int w = cl.first(); w < count; w = cl.advance()) {
+        cl.prefetch();
         const int q = order[w];
-        if (q < 0) continue;  // padding item of the per-CTA schedule
         const int n = dims[2 * q], r = dims[2 * q + 1];
         const T* A = a[q];
         T* B = b[q];
@@ -742,7 +766,7 @@ constexpr int kLlStage = 2 * kLlK * kLlPitch;     // A chunk + X chunk, in doubl
 constexpr int kLlRing = 2 * kLlStage;             // two stages (also holds the 64 x 68 solve block)
 
 __global__ void __launch_bounds__(kThreads, 2)
-trsm_batched_ll_f64(const int* __restrict__ order, int count, const int* __restrict__ dims, char uplo, char trans,
+trsm_batched_ll_f64(const int* __restrict__ order, int count, int* __restrict__ next, const int* __restrict__ dims, char uplo, char trans,
                     char diag, double alpha, const double* const* __restrict__ a, const int* __restrict__ lda,
                     double* const* __restrict__ b, const int* __restrict__ ldb) {
     extern __shared__ __align__(16) unsigned char ll_smem[];
@@ -754,9 +778,11 @@ trsm_batched_ll_f64(const int* __restrict__ order, int count, const int* __restr
     const bool unit = diag == 'U';
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
     const int rt = warp & 3, ct0 = (warp >> 2) * 4;
-    for (int w = blockIdx.x; w < count; w += gridDim.x) {
+    __shared__ int claim_slot[2];
+    Claim cl{next, claim_slot};
+    for (int w = cl.first(); w < count; w = cl.advance()) {
+        cl.prefetch();
         const int q = order[w];
-        if (q < 0) continue;
         const int n = dims[2 * q], r = dims[2 * q + 1];
         const double* A = a[q];
         double* B = b[q];
@@ -928,23 +954,24 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, int dtype, char uplo, char trans,
-                                char diag, const void* alpha, const void* const* a, const int* lda, void* const* b,
-                                const int* ldb, int grid, cudaStream_t st) {
+cudaError_t launch_trsm_batched(const int* order, int count, int* next, const int* dims, int dtype, char uplo,
+                                char trans, char diag, const void* alpha, const void* const* a, const int* lda,
+                                void* const* b, const int* ldb, int grid, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     const int sm = (3 * kTB * (kTB + 4) + kTB) * (dtype == BATCH_F64 ? 8 : 4);
     const int sm_ll = (kLlRing + kTB * kTP + kTB) * 8;
     cudaError_t e = dtype == BATCH_F64 ? ensure_dynamic_smem(trsm_batched_ll_f64, sm_ll)
                                        : ensure_dynamic_smem(trsm_batched_kernel<float>, sm);
     if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(next, 0, sizeof(int), st)) != cudaSuccess) return e;
     prof_begin(st);
     if (dtype == BATCH_F64)
         trsm_batched_ll_f64<<<grid, kThreads, sm_ll, st>>>(
-            order, count, dims, uplo, trans, diag, *static_cast<const double*>(alpha),
+            order, count, next, dims, uplo, trans, diag, *static_cast<const double*>(alpha),
             reinterpret_cast<const double* const*>(a), lda, reinterpret_cast<double* const*>(b), ldb);
     else
         trsm_batched_kernel<float><<<grid, kThreads, sm, st>>>(
-            order, count, dims, uplo, trans, diag, *static_cast<const float*>(alpha),
+            order, count, next, dims, uplo, trans, diag, *static_cast<const float*>(alpha),
             reinterpret_cast<const float* const*>(a), lda, reinterpret_cast<float* const*>(b), ldb);
     count_launch();
     prof_end(st);

@@ -35,9 +35,10 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
                                 const void* const* a, const int* lda, const void* const* b, const int* ldb,
                                 const void* beta, void* const* c, const int* ldc, int grid, cudaStream_t st);
 
-// order: per-CTA interleaved problem order (-1 = padding); dims: n, nrhs per problem.
-cudaError_t launch_trsm_batched(const int* order, int count, const int* dims, int dtype, char uplo, char trans,
-                                char diag, const void* alpha, const void* const* a, const int* lda, void* const* b,
-                                const int* ldb, int grid, cudaStream_t st);
+// order: problems longest first (CTAs claim them through the counter `next`, zeroed
+// by the launch); dims: n, nrhs per problem.
+cudaError_t launch_trsm_batched(const int* order, int count, int* next, const int* dims, int dtype, char uplo,
+                                char trans, char diag, const void* alpha, const void* const* a, const int* lda,
+                                void* const* b, const int* ldb, int grid, cudaStream_t st);
 
 }  // namespace zb

@@ -1,15 +1,14 @@
 // Host side of the batched GEMM / TRSM: plans, longest-first schedules,
 // autotuner with a persistent JSON cache, and CUDA-graph replay.
 //
-// Plan (create): the problem sizes are given once on the host.  Each problem
-// is assigned a tile config by its size bucket (the autotuner's table) and cut
-// into chunks of output tiles.  GEMM: the chunks are sorted by estimated cost,
-// longest first, and the kernel's persistent CTAs claim them in that order
-// from a device counter (greedy list scheduling on the measured durations).
-// TRSM (whole problems): a static longest-processing-time assignment onto the
-// grid, the per-CTA lists interleaved so that CTA b runs items b, b + G, ...
-// Run: a counter reset (GEMM) and one kernel launch, optionally replayed from
-// a captured CUDA graph, no allocation, so it can itself be captured by the
+// Plan (create): the problem sizes are given once on the host.  GEMM: each
+// problem is assigned a tile config by its size bucket (the autotuner's table)
+// and cut into chunks of output tiles; TRSM: one item per problem.  The items
+// are sorted by estimated cost, longest first, and the kernel's persistent
+// CTAs claim them in that order from a device counter (greedy list scheduling
+// on the real durations).
+// Run: a counter reset and one kernel launch, optionally replayed from a
+// captured CUDA graph, no allocation, so it can itself be captured by the
 // caller.
 //
 // Autotuner: for every size bucket present in a batch (bucket = ceil(log2 of
@@ -28,7 +27,6 @@
 #include <map>
 #include <mutex>
 #include <numeric>
-#include <queue>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -136,30 +134,6 @@ int sm_count() {
     return n;
 }
 
-// LPT: returns per-CTA interleaved order of item indices (-1 padding).
-std::vector<int> lpt_schedule(const std::vector<double>& cost, int grid) {
-    std::vector<int> idx(cost.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-    std::vector<std::vector<int>> lists(grid);
-    using Slot = std::pair<double, int>;
-    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> pq;
-    for (int g = 0; g < grid; ++g) pq.push({0.0, g});
-    for (int i : idx) {
-        Slot s = pq.top();
-        pq.pop();
-        lists[s.second].push_back(i);
-        s.first += cost[i];
-        pq.push(s);
-    }
-    size_t depth = 0;
-    for (auto& l : lists) depth = std::max(depth, l.size());
-    std::vector<int> out(depth * grid, -1);
-    for (int g = 0; g < grid; ++g)
-        for (size_t r = 0; r < lists[g].size(); ++r) out[r * grid + g] = lists[g][r];
-    return out;
-}
-
 }  // namespace
 
 // ------------------------------------------------------------ batch object
@@ -173,8 +147,8 @@ struct Batch {
     int grid = 148;
     // device
     int* d_dims = nullptr;
-    BatchWork* d_work = nullptr;  // work items, followed by the claim counter d_next
-    int* d_next = nullptr;
+    BatchWork* d_work = nullptr;  // GEMM work items, followed by the claim counter
+    int* d_next = nullptr;        // claim counter (after the GEMM items or the TRSM order)
     int* d_order = nullptr;
     int n_items = 0;
     int cfg_counts[3] = {0, 0, 0};
@@ -483,16 +457,22 @@ int zynum_blas_gpu_trsm_batch_create(zynum_blas_gpu_batch_t* out, int dtype, cha
         const double nb = (m[q] + 63) / 64;
         cost.push_back(nb * (nb - 1.0) / 2.0 * (2.0 + 0.066 * n[q]) + 5.0 * nb + 1.0);
     }
-    std::vector<int> order = lpt_schedule(cost, b->grid);
-    for (int& o : order)
-        if (o >= 0 && (m[o] == 0 || n[o] == 0)) o = -1;
+    // longest first (empty problems left out): the kernel's CTAs claim problems in this order
+    std::vector<int> order;
+    for (int q = 0; q < count; ++q)
+        if (m[q] > 0 && n[q] > 0) order.push_back(q);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
     b->n_items = (int)order.size();
     cudaError_t e = cudaSuccess;
     if (count) {
         if ((e = cudaMalloc(&b->d_dims, dims.size() * sizeof(int))) == cudaSuccess)
             e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && (e = cudaMalloc(&b->d_order, order.size() * sizeof(int))) == cudaSuccess)
+        // the order, then the claim counter (16-byte aligned after it)
+        const size_t order_bytes = (order.size() * sizeof(int) + 15) / 16 * 16;
+        if (e == cudaSuccess && (e = cudaMalloc(&b->d_order, order_bytes + 16)) == cudaSuccess) {
+            b->d_next = b->d_order + order_bytes / sizeof(int);
             e = cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+        }
     }
     if (e != cudaSuccess) {
         delete b;
@@ -560,8 +540,9 @@ ZB_GEMM_BATCH_RUN(zynum_blas_gpu_sgemm_batch_run, float, BATCH_F32)
         args.b = b;                                                                                                 \
         args.ldb = ldb;                                                                                             \
         auto fn = [&](cudaStream_t s) {                                                                             \
-            return launch_trsm_batched(bt->d_order, bt->n_items, bt->d_dims, DT, bt->uplo, bt->ta, bt->diag,       \
-                                       &alpha, (const void* const*)a, lda, (void* const*)b, ldb, bt->grid, s);     \
+            return launch_trsm_batched(bt->d_order, bt->n_items, bt->d_next, bt->d_dims, DT, bt->uplo, bt->ta,     \
+                                       bt->diag, &alpha, (const void* const*)a, lda, (void* const*)b, ldb, bt->grid, \
+                                       s);                                                                           \
         };                                                                                                          \
         return status_of(run_maybe_graph(*bt, &args, sizeof(args), use_graph != 0, (cudaStream_t)stream, fn),      \
                          #NAME);                                                                                    \
