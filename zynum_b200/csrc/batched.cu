@@ -7,8 +7,11 @@
 // tiles of one problem, with their tile config) ordered longest-first; the
 // persistent CTAs claim items in that order from a counter the launch zeroes
 // (a memset and the kernel, both graph-capturable and replayable).  Each size
-// bucket gets its tile config from the autotuner (batched_host.cpp).  FP64 tiles use DMMA (mma.sync m16n8k8 .f64), FP32 tiles FFMA;
-// operands are staged with cp.async (8- / 4-byte copies: per-problem leading
+// bucket gets its tile config from the autotuner (batched_host.cpp).  Both
+// dtypes run on DMMA tiles (mma.sync m16n8k8 .f64): FP32 operands are widened
+// exactly to FP64 in the fragments and C is rounded to FP32 once (18.8 against
+// 15.4 TFLOP/s for FFMA tiles on the 20,000-problem batch, and more accurate).
+// Operands are staged with cp.async (8- / 4-byte copies: per-problem leading
 // dimensions need not be aligned).
 //
 // TRSM (left side): one CTA solves one whole problem B := alpha op(A)^-1 B:
@@ -25,8 +28,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBK = 16;
-constexpr int kStages = 3;   // FP32: three cp.async stages, two CTAs per SM
-constexpr int kStagesD = 2;  // FP64: two stages of 20 KB (64 x 64 tiles), four CTAs per SM
+constexpr int kStagesD = 2;  // two cp.async stages (64 x 64 tiles: 20 KB FP64), four CTAs per SM
 
 template <typename T>
 struct Prob {
@@ -87,9 +89,8 @@ ZB_DEVICE bool vec_ok(const T* base, int ld) {
 // (the others lie outside the problem).  The fragment counts are compile-time
 // so that skipped fragments issue nothing at all: a run-time test around a
 // DMMA becomes a predicated DMMA, which still occupies the pipe.
-template <int MI, int NI, int MIV, int NIV, int A_PITCH, int B_PITCH, bool AK, bool BKF>
-ZB_DEVICE void dmma_slice(double (&acc)[MI][NI][4], const double* as, const double* bs, int wm, int wn, int g,
-                          int t) {
+template <int MI, int NI, int MIV, int NIV, int A_PITCH, int B_PITCH, bool AK, bool BKF, typename T>
+ZB_DEVICE void dmma_slice(double (&acc)[MI][NI][4], const T* as, const T* bs, int wm, int wn, int g, int t) {
 #pragma unroll
     for (int ks = 0; ks < kBK; ks += 8) {
         double af[MIV][4], bf[NIV][2];
@@ -98,14 +99,14 @@ ZB_DEVICE void dmma_slice(double (&acc)[MI][NI][4], const double* as, const doub
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 const int rr = wm + i * 16 + g + 8 * (v & 1), kk = ks + t + 4 * (v >> 1);
-                af[i][v] = AK ? as[rr * A_PITCH + kk] : as[kk * A_PITCH + rr];
+                af[i][v] = (double)(AK ? as[rr * A_PITCH + kk] : as[kk * A_PITCH + rr]);
             }
 #pragma unroll
         for (int j = 0; j < NIV; ++j)
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
                 const int cc = wn + j * 8 + g, kk = ks + t + 4 * v;
-                bf[j][v] = BKF ? bs[cc * B_PITCH + kk] : bs[kk * B_PITCH + cc];
+                bf[j][v] = (double)(BKF ? bs[cc * B_PITCH + kk] : bs[kk * B_PITCH + cc]);
             }
 #pragma unroll
         for (int i = 0; i < MIV; ++i)
@@ -115,9 +116,9 @@ ZB_DEVICE void dmma_slice(double (&acc)[MI][NI][4], const double* as, const doub
 }
 
 // Variant V = MIV * (NI + 1) + NIV, chosen by a chain of warp-uniform branches.
-template <int MI, int NI, int V, int A_PITCH, int B_PITCH, bool AK, bool BKF>
-ZB_DEVICE void dmma_slice_var(int var, double (&acc)[MI][NI][4], const double* as, const double* bs, int wm, int wn,
-                              int g, int t) {
+template <int MI, int NI, int V, int A_PITCH, int B_PITCH, bool AK, bool BKF, typename T>
+ZB_DEVICE void dmma_slice_var(int var, double (&acc)[MI][NI][4], const T* as, const T* bs, int wm, int wn, int g,
+                              int t) {
     constexpr int MIV = V / (NI + 1), NIV = V % (NI + 1);
     if (var == V) {
         if constexpr (MIV > 0 && NIV > 0)
@@ -130,16 +131,24 @@ ZB_DEVICE void dmma_slice_var(int var, double (&acc)[MI][NI][4], const double* a
 
 // One BM x BN output tile: 8 warps as WARPS_M x (8 / WARPS_M), warp tile
 // WM x WN of 16 x 8 DMMA fragments, kStagesD cp.async stages of kBK-deep A and
-// B slices (16-byte copies where the operand allows them).
-template <int BM, int BN, int WARPS_M, bool AK, bool BKF>
-ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, double beta, double* smem) {
+// B slices (16-byte copies where the operand allows them).  T = float: FP32
+// operands staged as FP32 and widened exactly to FP64 in the fragments; the
+// products and sums are FP64 and C = alpha acc + beta C is rounded to FP32 once.
+// Row pitches: 4 extra elements for k-contiguous rows; m- / n-contiguous rows
+// 4 extra doubles or 8 extra floats, which keeps the fragment loads conflict-free.
+template <typename T>
+constexpr int mn_pad() {
+    return sizeof(T) == 8 ? 4 : 8;
+}
+template <int BM, int BN, int WARPS_M, bool AK, bool BKF, typename T = double>
+ZB_DEVICE void dgemm_tile(const Prob<T>& p, int m0, int n0, double alpha, double beta, T* smem) {
     constexpr int WARPS_N = 8 / WARPS_M;
     constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N, MI = WM / 16, NI = WN / 8;
-    constexpr int A_ROWS = AK ? BM : kBK, A_COLS = AK ? kBK : BM, A_PITCH = A_COLS + 4;
-    constexpr int B_ROWS = BKF ? BN : kBK, B_COLS = BKF ? kBK : BN, B_PITCH = B_COLS + 4;
+    constexpr int A_ROWS = AK ? BM : kBK, A_COLS = AK ? kBK : BM, A_PITCH = A_COLS + (AK ? 4 : mn_pad<T>());
+    constexpr int B_ROWS = BKF ? BN : kBK, B_COLS = BKF ? kBK : BN, B_PITCH = B_COLS + (BKF ? 4 : mn_pad<T>());
     constexpr int A_STAGE = A_ROWS * A_PITCH, B_STAGE = B_ROWS * B_PITCH;
-    double* As = smem;
-    double* Bs = smem + kStagesD * A_STAGE;
+    T* As = smem;
+    T* Bs = smem + kStagesD * A_STAGE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = (warp / WARPS_N) * WM, wn = (warp % WARPS_N) * WN;
     const int g = lane >> 2, t = lane & 3;
@@ -158,13 +167,13 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
     auto load_stage = [&](int stage, int kt) {
         const int k0 = kt * kBK;
         if (AK)
-            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, m0, k0, p.m, p.k, va);
+            load_tile<T, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, m0, k0, p.m, p.k, va);
         else
-            load_tile<double, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, k0, m0, p.k, p.m, va);
+            load_tile<T, A_ROWS, A_COLS>(As + stage * A_STAGE, A_PITCH, p.a, p.lda, k0, m0, p.k, p.m, va);
         if (BKF)
-            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, n0, k0, p.n, p.k, vb);
+            load_tile<T, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, n0, k0, p.n, p.k, vb);
         else
-            load_tile<double, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, k0, n0, p.k, p.n, vb);
+            load_tile<T, B_ROWS, B_COLS>(Bs + stage * B_STAGE, B_PITCH, p.b, p.ldb, k0, n0, p.k, p.n, vb);
     };
 #pragma unroll
     for (int s = 0; s < kStagesD - 1; ++s) {
@@ -176,8 +185,8 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
         __syncthreads();
         if (kt + kStagesD - 1 < KT) load_stage((kt + kStagesD - 1) % kStagesD, kt + kStagesD - 1);
         cp_async_commit();
-        const double* as = As + (kt % kStagesD) * A_STAGE;
-        const double* bs = Bs + (kt % kStagesD) * B_STAGE;
+        const T* as = As + (kt % kStagesD) * A_STAGE;
+        const T* bs = Bs + (kt % kStagesD) * B_STAGE;
         if (var == MI * (NI + 1) + NI)  // the whole warp tile inside the problem
             dmma_slice<MI, NI, MI, NI, A_PITCH, B_PITCH, AK, BKF>(acc, as, bs, wm, wn, g, t);
         else
@@ -193,10 +202,10 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
                 const int row = m0 + wm + i * 16 + g + 8 * (v >> 1);
                 const int col = n0 + wn + j * 8 + 2 * t + (v & 1);
                 if (row < p.m && col < p.n) {
-                    double* cp = p.c + (long)col * p.ldc + row;
+                    T* cp = p.c + (long)col * p.ldc + row;
                     double out = alpha * acc[i][j][v];
-                    if (beta != 0.0) out = fma(beta, *cp, out);
-                    *cp = out;
+                    if (beta != 0.0) out = fma(beta, (double)*cp, out);
+                    *cp = (T)out;
                 }
             }
     __syncthreads();  // shared memory is reused by the next tile
@@ -207,138 +216,11 @@ ZB_DEVICE void dgemm_tile(const Prob<double>& p, int m0, int n0, double alpha, d
 // the problem's sizes, pointers and leading dimensions are read once per chunk.
 // (Carrying the cp.async stream across the chunk's tile boundaries measured
 // slower than restarting it per tile.)
-template <int BM, int BN, int WARPS_M, bool AK, bool BKF>
-ZB_DEVICE void dgemm_chunk(const Prob<double>& p, int t0, int count, double alpha, double beta, double* smem) {
+template <int BM, int BN, int WARPS_M, bool AK, bool BKF, typename T = double>
+ZB_DEVICE void dgemm_chunk(const Prob<T>& p, int t0, int count, double alpha, double beta, T* smem) {
     const int mt = (p.m + BM - 1) / BM;
     for (int tile = t0; tile < t0 + count; ++tile)
-        dgemm_tile<BM, BN, WARPS_M, AK, BKF>(p, (tile % mt) * BM, (tile / mt) * BN, alpha, beta, smem);
-}
-
-// ------------------------------------------------------- FP32 FFMA tile
-// BM x BN tile, 8 warps as WARPS_M x (8 / WARPS_M), warp tile WTM x WTN, lanes
-// as LR x (32 / LR), each thread TM x TN outputs (TM = WTM / LR).  A thread's
-// rows are TM / G groups of G consecutive rows, group h at h * WTM / (TM / G)
-// (G = min(TM, 4)), so its A values of one k are float4 (float2) shared loads
-// and the lanes of a warp read consecutive 16-byte words; columns likewise.
-// Warps whose rows or columns all lie outside the problem skip the products.
-template <int N>
-struct FVec;
-template <>
-struct FVec<4> {
-    using T = float4;
-};
-template <>
-struct FVec<2> {
-    using T = float2;
-};
-
-template <int BM, int BN, int WARPS_M, int LR, bool AM, bool BMF>
-ZB_DEVICE void sgemm_tile(const Prob<float>& p, int m0, int n0, float alpha, float beta, float* smem) {
-    constexpr int WARPS_N = 8 / WARPS_M, LC = 32 / LR;
-    constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N, TM = WTM / LR, TN = WTN / LC;
-    constexpr int GM = TM < 4 ? TM : 4, GN = TN < 4 ? TN : 4;  // vector widths
-    constexpr int HM = TM / GM, HN = TN / GN;                  // groups per thread
-    static_assert(TM * LR == WTM && TN * LC == WTN && (GM == 2 || GM == 4) && (GN == 2 || GN == 4), "layout");
-    constexpr int PA = BM + 4, PB = BN + 4;
-    using VA = typename FVec<GM>::T;
-    using VB = typename FVec<GN>::T;
-    float* As = smem;                        // [stage][kBK][PA]  (m fast)
-    float* Bs = smem + kStages * kBK * PA;   // [stage][kBK][PB]  (n fast)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wr = (warp / WARPS_N) * WTM, wc = (warp % WARPS_N) * WTN;
-    const int lr = lane / LC, lc = lane % LC;
-    const int KT = (alpha == 0.f) ? 0 : (p.k + kBK - 1) / kBK;  // alpha == 0: A and B are not read
-    const bool active = wr < p.m - m0 && wc < p.n - n0;          // uniform across the warp
-    const bool va = AM && vec_ok(p.a, p.lda), vb = BMF && vec_ok(p.b, p.ldb);
-    float acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
-    auto load_stage = [&](int stage, int kt) {
-        const int k0 = kt * kBK;
-        float* as = As + stage * kBK * PA;
-        float* bs = Bs + stage * kBK * PB;
-        // element (mn, kk) of the tile -> shared [kk][mn]; an operand contiguous along m (n)
-        // goes by 16-byte copies when aligned (va / vb)
-        if (AM && va) {
-            load_tile<float, kBK, BM>(as, PA, p.a, p.lda, k0, m0, p.k, p.m, true);
-        } else {
-            for (int q = threadIdx.x; q < kBK * BM; q += kThreads) {
-                int kk, mm;
-                if (AM) { kk = q / BM; mm = q % BM; } else { mm = q / kBK; kk = q % kBK; }
-                const int gm = m0 + mm, gk = k0 + kk;
-                const bool ok = gm < p.m && gk < p.k;
-                const float* src = ok ? (AM ? p.a + gm + (long)gk * p.lda : p.a + gk + (long)gm * p.lda) : p.a;
-                cp_async_4(smem_u32(as + kk * PA + mm), src, ok ? 4 : 0);
-            }
-        }
-        if (BMF && vb) {
-            load_tile<float, kBK, BN>(bs, PB, p.b, p.ldb, k0, n0, p.k, p.n, true);
-        } else {
-            for (int q = threadIdx.x; q < kBK * BN; q += kThreads) {
-                int kk, nn;
-                if (BMF) { kk = q / BN; nn = q % BN; } else { nn = q / kBK; kk = q % kBK; }
-                const int gn = n0 + nn, gk = k0 + kk;
-                const bool ok = gn < p.n && gk < p.k;
-                const float* src = ok ? (BMF ? p.b + gn + (long)gk * p.ldb : p.b + gk + (long)gn * p.ldb) : p.b;
-                cp_async_4(smem_u32(bs + kk * PB + nn), src, ok ? 4 : 0);
-            }
-        }
-    };
-#pragma unroll
-    for (int s = 0; s < kStages - 1; ++s) {
-        if (s < KT) load_stage(s, s);
-        cp_async_commit();
-    }
-    for (int kt = 0; kt < KT; ++kt) {
-        cp_async_wait<kStages - 2>();
-        __syncthreads();
-        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
-        cp_async_commit();
-        const float* as = As + (kt % kStages) * kBK * PA + wr + lr * GM;
-        const float* bs = Bs + (kt % kStages) * kBK * PB + wc + lc * GN;
-        if (active) {
-#pragma unroll
-            for (int kk = 0; kk < kBK; ++kk) {
-                float a[TM], b[TN];
-#pragma unroll
-                for (int h = 0; h < HM; ++h) {
-                    const VA v = *reinterpret_cast<const VA*>(as + kk * PA + h * (WTM / HM));
-                    const float* f = reinterpret_cast<const float*>(&v);
-#pragma unroll
-                    for (int e = 0; e < GM; ++e) a[h * GM + e] = f[e];
-                }
-#pragma unroll
-                for (int h = 0; h < HN; ++h) {
-                    const VB v = *reinterpret_cast<const VB*>(bs + kk * PB + h * (WTN / HN));
-                    const float* f = reinterpret_cast<const float*>(&v);
-#pragma unroll
-                    for (int e = 0; e < GN; ++e) b[h * GN + e] = f[e];
-                }
-#pragma unroll
-                for (int i = 0; i < TM; ++i)
-#pragma unroll
-                    for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-            }
-        }
-    }
-    cp_async_wait<0>();
-#pragma unroll
-    for (int j = 0; j < TN; ++j) {
-        const int col = n0 + wc + (j / GN) * (WTN / HN) + lc * GN + (j % GN);
-        if (col >= p.n) continue;
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            const int row = m0 + wr + (i / GM) * (WTM / HM) + lr * GM + (i % GM);
-            if (row >= p.m) continue;
-            float* cp = p.c + (long)col * p.ldc + row;
-            float out = alpha * acc[i][j];
-            if (beta != 0.f) out = fmaf(beta, *cp, out);
-            *cp = out;
-        }
-    }
-    __syncthreads();
+        dgemm_tile<BM, BN, WARPS_M, AK, BKF, T>(p, (tile % mt) * BM, (tile / mt) * BN, alpha, beta, smem);
 }
 
 // ------------------------------------------------- persistent kernels
@@ -407,8 +289,12 @@ dgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, int* __rest
     });
 }
 
-template <bool AM, bool BMF>
-__global__ void __launch_bounds__(kThreads, 2)
+// FP32 batches run on the same DMMA tiles: operands staged as FP32 and widened
+// exactly to FP64, FP64 products and sums, one rounding of alpha acc + beta C
+// to FP32 (measured against FFMA tiles on the 20,000-problem batch: see the
+// design notes).
+template <bool AK, bool BKF>
+__global__ void __launch_bounds__(kThreads, 4)
 sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, int* __restrict__ next,
                      const int* __restrict__ dims, const float* const* __restrict__ a, const int* __restrict__ lda,
                      const float* const* __restrict__ b, const int* __restrict__ ldb, float alpha, float beta,
@@ -418,17 +304,10 @@ sgemm_batched_kernel(const BatchWork* __restrict__ work, int n_work, int* __rest
         const BatchWork it = work[w];
         const int q = it.prob;
         Prob<float> p{dims[3 * q], dims[3 * q + 1], dims[3 * q + 2], lda[q], ldb[q], ldc[q], a[q], b[q], c[q]};
-        const int e = it.cfg == TILE_CFG_128 ? 128 : (it.cfg == TILE_CFG_64 ? 64 : 32);
-        const int mt = (p.m + e - 1) / e;
-        for (int tile = it.t0; tile < it.t0 + it.count; ++tile) {
-            const int m0 = (tile % mt) * e, n0 = (tile / mt) * e;
-            if (it.cfg == TILE_CFG_128)  // warps 2 x 4 of 64 x 32, threads 8 x 8
-                sgemm_tile<128, 128, 2, 8, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
-            else if (it.cfg == TILE_CFG_64)  // warps 4 x 2 of 16 x 32, threads 4 x 4
-                sgemm_tile<64, 64, 4, 4, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
-            else  // warps 4 x 2 of 8 x 16, threads 2 x 2
-                sgemm_tile<32, 32, 4, 4, AM, BMF>(p, m0, n0, alpha, beta, sm_f);
-        }
+        if (it.cfg == TILE_CFG_128 || it.cfg == TILE_CFG_64)
+            dgemm_chunk<64, 64, 2, AK, BKF, float>(p, it.t0, it.count, alpha, beta, sm_f);
+        else
+            dgemm_chunk<32, 32, 2, AK, BKF, float>(p, it.t0, it.count, alpha, beta, sm_f);
     });
 }
 
@@ -438,7 +317,11 @@ size_t dsmem_bytes() {
     constexpr size_t b = 64 * (kBK + 4) > kBK * (64 + 4) ? 64 * (kBK + 4) : kBK * (64 + 4);
     return kStagesD * (a + b) * sizeof(double);
 }
-size_t ssmem_bytes() { return (size_t)kStages * kBK * (132 + 132) * sizeof(float); }
+size_t ssmem_bytes() {
+    // FP32 DMMA tiles, largest config (64 x 64), worst orientation of each operand
+    constexpr size_t a = 64 * (kBK + 4) > kBK * (64 + 8) ? 64 * (kBK + 4) : kBK * (64 + 8);
+    return kStagesD * 2 * a * sizeof(float);
+}
 
 // -------------------------------------------------------- batched TRSM
 constexpr int kTB = 64;  // diagonal block
@@ -930,15 +813,15 @@ cudaError_t launch_gemm_batched(const BatchDevice& d, int dtype, char transa, ch
         ZB_DB(false, false) ZB_DB(false, true) ZB_DB(true, false) ZB_DB(true, true)
 #undef ZB_DB
     } else {
-        const bool am = transa == 'N', bm = transb != 'N';
+        const bool ak = transa != 'N', bk = transb == 'N';
         const float al = *static_cast<const float*>(alpha), be = *static_cast<const float*>(beta);
         auto A = reinterpret_cast<const float* const*>(a);
         auto B = reinterpret_cast<const float* const*>(b);
         auto Cp = reinterpret_cast<float* const*>(c);
         const size_t sm = ssmem_bytes();
-#define ZB_SB(AMV, BMV)                                                                                         \
-    if (am == AMV && bm == BMV) {                                                                               \
-        auto kern = sgemm_batched_kernel<AMV, BMV>;                                                             \
+#define ZB_SB(AKV, BKV)                                                                                         \
+    if (ak == AKV && bk == BKV) {                                                                               \
+        auto kern = sgemm_batched_kernel<AKV, BKV>;                                                             \
         if ((e = ensure_dynamic_smem(kern, (int)sm)) != cudaSuccess) \
             return e;                                                                                           \
         if ((e = cudaMemsetAsync(d.next, 0, sizeof(int), st)) != cudaSuccess) return e;                        \
@@ -979,7 +862,8 @@ cudaError_t launch_trsm_batched(const int* order, int count, int* next, const in
 }
 
 int batched_tile_n(int cfg, int dtype) {
-    return cfg == TILE_CFG_128 ? (dtype == BATCH_F64 ? 64 : 128) : (cfg == TILE_CFG_64 ? 64 : 32);
+    (void)dtype;  // TILE_CFG_128 runs as 64 x 64 (both dtypes on DMMA tiles)
+    return cfg == TILE_CFG_64 || cfg == TILE_CFG_128 ? 64 : 32;
 }
 int batched_tile_m(int cfg, int dtype) { return batched_tile_n(cfg, dtype); }
 
