@@ -325,12 +325,13 @@ struct Relayout {
 
 Relayout relayout_plan(char transa, char transb, int m, int n, int k, const GemmPlan& plan) {
     Relayout r;
-    // the tall-skinny kernels read either layout and keep no partial sums: no workspace
-    // (so the route needs no allocation, e.g. on a stream under graph capture)
-    if (skinny_gemm_applies(m, n, k, 0)) return r;
     r.splitk = align_elems(splitk_workspace_elems(m, n, plan.splits));
-    // the matrix-vector and narrow kernels read either layout directly
-    if (plan.tile == TILE_GEMV || plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M) return r;
+    // the matrix-vector, narrow and tall-skinny kernels read either layout directly (the
+    // tall-skinny route, K <= 64, never splits K either, so it needs no workspace at all,
+    // e.g. on a stream under graph capture)
+    if (plan.tile == TILE_GEMV || plan.tile == TILE_NARROW_N || plan.tile == TILE_NARROW_M ||
+        skinny_gemm_applies(m, n, k, 0))
+        return r;
     const size_t a_elems = align_elems((size_t)pad4(m) * (size_t)k);
     const size_t b_elems = align_elems((size_t)pad4(n) * (size_t)k);
     r.a = transa != 'N' && n >= kRelayoutMinOther && a_elems * sizeof(float) <= kRelayoutMaxBytes;
