@@ -138,3 +138,41 @@ def test_skinny_route_graph_capture(blas, dtype, beta):
     graph.replay()
     torch.cuda.synchronize()
     assert torch.equal(out, ref)
+
+
+@pytest.mark.filterwarnings("ignore:The CUDA Graph is empty")  # the refused capture records nothing
+def test_workspace_growth_refused_under_capture(blas):
+    """A call whose per-stream workspace would have to grow (cudaMalloc) on a stream under
+    CUDA-graph capture returns an error naming the remedy instead of invalidating the
+    capture; after one uncaptured call on that stream the same call captures and replays
+    to the direct result."""
+    import torch
+    from zynum_b200._lib import ZynumGpuError
+    torch.cuda.synchronize()
+    old = blas.set_dgemm_method(blas.METHOD_OZAKI)  # the CRT route keeps its planes in the workspace
+    try:
+        m, n, k = 1024, 768, 512
+        g = torch.Generator(device="cuda").manual_seed(43)
+        A = torch.rand((k, m), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+        B = torch.rand((n, k), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+        ref = torch.zeros((n, m), device="cuda", dtype=torch.float64)
+        blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, ref, m)
+        s = torch.cuda.Stream()
+        out = torch.zeros_like(ref)
+        graph = torch.cuda.CUDAGraph()
+        with pytest.raises(ZynumGpuError, match="graph capture"):
+            with torch.cuda.graph(graph, stream=s):
+                blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, out, m)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(s):  # sizes the workspace of stream s
+            blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, out, m)
+        s.synchronize()
+        out.zero_()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=s):
+            blas.dgemm_device("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, out, m)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+    finally:
+        blas.set_dgemm_method(old)

@@ -54,6 +54,8 @@ int cuda_status(cudaError_t e, const char* what) {
     if (site)
         set_last_error(std::string(what) + ": a bounded wait in a tensor-core product kernel ran out (site " +
                        std::to_string(site) + "); the product was abandoned and C was not written");
+    else if (e == cudaErrorStreamCaptureUnsupported)  // keep the workspace message of stream_scratch
+        set_last_error(std::string(what) + ": " + last_error());
     else
         set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
     return -(int)e;

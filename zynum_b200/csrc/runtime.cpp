@@ -161,6 +161,18 @@ cudaError_t Context::reserve(DeviceBuffer& buf, size_t bytes, cudaStream_t s) {
 cudaError_t Context::stream_scratch(cudaStream_t s, size_t bytes, void** out) {
     std::lock_guard<std::recursive_mutex> lock(mutex);
     DeviceBuffer& b = stream_work[s];
+    if (bytes > b.bytes) {
+        // growing means cudaMalloc, which a stream under CUDA-graph capture does not allow
+        // (it would invalidate the capture): refuse with a message instead
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            set_last_error("the stream is under graph capture and its workspace must grow to " +
+                           std::to_string(bytes) + " bytes: make the same call (or a larger one) once on this "
+                           "stream before capturing");
+            *out = nullptr;
+            return cudaErrorStreamCaptureUnsupported;
+        }
+    }
     cudaError_t e = reserve(b, bytes, s);
     *out = b.ptr;
     return e;
