@@ -259,3 +259,31 @@ def test_rank_k_ozaki_route(blas, oracle, routine, uplo, trans):
             assert np.array_equal(c[n:], c0[n:]), "padding rows of C were written"
     finally:
         blas.set_dgemm_method(old)
+
+
+@pytest.mark.parametrize("uplo,trans", list(itertools.product("UL", "NT")))
+def test_syrk_ozaki_triangle_tiles(blas, oracle, uplo, trans):
+    """DSYRK under the Ozaki method on several 256 x 256 tiles per side: the modular products
+    run only on the tiles meeting the stored triangle and op(A) is split once (op(B)^T is
+    op(A)); the stored triangle meets the oracle's bound, the other triangle is untouched."""
+    rng = np.random.default_rng(ord(uplo) * 5 + ord(trans))
+    n, k = 1100, 700
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = _mat(rng, ra, ca, ra + 2, np.float64)
+    c = _mat(rng, n, n, n + 1, np.float64, -777.0)
+    c0 = c.copy(order="F")
+    ref = c.copy(order="F")
+    alpha, beta = -0.5, 1.25
+    old = blas.set_dgemm_method(blas.METHOD_OZAKI)
+    try:
+        oracle.syrk(uplo, trans, n, k, alpha, a, ra + 2, beta, ref, n + 1)
+        blas.syrk(uplo, trans, n, k, alpha, a, ra + 2, beta, c, n + 1)
+    finally:
+        blas.set_dgemm_method(old)
+    tri = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    A = np.abs(a[:ra, :ca]) if trans == "N" else np.abs(a[:ra, :ca]).T
+    bound = 8 * k * U[np.float64] * (abs(alpha) * (A @ A.T) + abs(beta) * np.abs(c0[:n, :n]))
+    err = np.abs(c[:n, :n] - ref[:n, :n])
+    assert np.all(err[tri] <= bound[tri] + 1e-300), float(err[tri].max())
+    assert np.array_equal(c[:n, :n][~tri], c0[:n, :n][~tri]), "the other triangle changed"
+    assert np.array_equal(c[n:], c0[n:]), "padding rows of C were written"

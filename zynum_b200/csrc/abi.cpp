@@ -600,8 +600,10 @@ inline bool rank_k_uses_ozaki(int n, int k) {
     return method == METHOD_AUTO && ozaki_preferred_scaled(n, n, k, 0.5, 24.0 * n * (double)n);
 }
 
-// W = op(A) op(B)^T as one full emulated DGEMM into scratch, then
-// C := alpha (W [+ W^T]) + beta C on the triangle (op(B) op(A)^T = W^T).
+// W = op(A) op(B)^T as one emulated DGEMM into scratch, then
+// C := alpha (W [+ W^T]) + beta C on the triangle (op(B) op(A)^T = W^T).  SYRK
+// (one term) needs only W's stored triangle: the product runs in triangle mode
+// and, op(B)^T being op(A), splits op(A) once.
 template <typename Scratch>
 cudaError_t run_rank_k_ozaki(char uplo, char trans, bool two, int n, int k, double alpha, const double* a, long lda,
                              const double* b, long ldb, double beta, double* c, long ldc, cudaStream_t st,
@@ -614,7 +616,8 @@ cudaError_t run_rank_k_ozaki(char uplo, char trans, bool two, int n, int k, doub
     if (e != cudaSuccess) return e;
     double* W = static_cast<double*>(ws);
     const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';
-    const GemmArgsF64 g{t1, t2, n, n, k, 1.0, a, lda, b, ldb, 0.0, W, n};
+    GemmArgsF64 g{t1, t2, n, n, k, 1.0, a, lda, b, ldb, 0.0, W, n};
+    if (!two) g.tri = uplo == 'U' ? 1 : 2;
     if ((e = dgemm_ozaki(g, op, static_cast<char*>(ws) + wbytes, st)) != cudaSuccess) return e;
     return triangle_update<double>(uplo, two, n, alpha, W, n, beta, c, ldc, st);
 }

@@ -96,6 +96,8 @@ struct UmmaParams {
     int8_t* residues;  // EPI_RESIDUE: residue planes [modulus][m_pad][n_pad] (row-major)
     long res_plane;
     int band_rows;     // EPI_RESIDUE on the CTA pair: tile-rows per raster band
+    int tri;           // EPI_RESIDUE on the CTA pair: 1 / 2 = only the tiles meeting the upper / lower
+                       // triangle (num_tiles of them, tiles_m == tiles_n), enumerated by crt_job_tile
     int* report;       // per-device report word of bounded waits that ran out
     unsigned long long wait_ns;  // time limit of every mbarrier wait
     int hold;          // test-only: the MMA issuer first waits on a barrier nothing arrives on
@@ -109,6 +111,28 @@ ZB_DEVICE void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn,
     int r = tile - band * G * tiles_n;
     tm = band * G + r % rows_in_band;
     tn = r / rows_in_band;
+}
+
+// Tile of CRT job index `tile`: the raster bands of tile_coords, or in triangle
+// mode the T (T + 1) / 2 tiles meeting the stored triangle (rows <= columns for
+// tri = 1, >= for tri = 2), row after row of the triangle: index t lies in
+// triangle row r = floor((sqrt(8 t + 1) - 1) / 2) at position t - r (r + 1) / 2.
+ZB_DEVICE void crt_job_tile(int tri, int tile, int tiles_m, int tiles_n, int band_rows, int& tm, int& tn) {
+    if (!tri) {
+        tile_coords(tile, tiles_m, tiles_n, tm, tn, band_rows);
+        return;
+    }
+    int r = (int)((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
+    while ((r + 1) * (r + 2) / 2 <= tile) ++r;  // exact integer fix-up of the FP64 estimate
+    while (r * (r + 1) / 2 > tile) --r;
+    const int pos = tile - r * (r + 1) / 2;
+    if (tri == 2) {  // lower: row r of tiles, columns 0 .. r
+        tm = r;
+        tn = pos;
+    } else {  // upper: column r of tiles, rows 0 .. r
+        tn = r;
+        tm = pos;
+    }
 }
 
 ZB_DEVICE double pow2(int e) {
@@ -687,7 +711,7 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs) {
                 const int j = q / P.num_tiles, tile = q - j * P.num_tiles;
                 int tm, tn;
-                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
+                crt_job_tile(P.tri, tile, P.tiles_m, P.tiles_n, P.band_rows, tm, tn);
                 const int arow = tm * 256 + rank * 128, brow = tn * kUN + rank * 128;
                 const int l = P.job_shift[j][0];
                 for (int ks = 0; ks < steps; ++ks) {
@@ -724,8 +748,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
             bool ok = !P.hold || wait_phase(hold_bar, 0, W, WAIT_MMA_HOLD);
             const int steps = P.k_chunks / 2;
             int inst = 0;  // job instances alternate between the two accumulators
-            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs, ++inst) {
-                const int b = inst & 1;
+            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs) {
+                const int b = inst++ & 1;
                 if (!(ok = wait_phase(&tempty[b], ((tphase >> b) & 1u) ^ 1u, W, WAIT_MMA_TEMPTY))) break;
                 tphase ^= 1u << b;
                 tc_fence_after();
@@ -860,11 +884,11 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
         if (EPI == EPI_RESIDUE) {
             // modulus-major, in the order of the MMA issuer
             int inst = 0;
-            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs, ++inst) {
+            for (int q = pair; ok && q < P.num_jobs * P.num_tiles; q += npairs) {
                 const int j = q / P.num_tiles, tile = q - j * P.num_tiles;
                 int tm, tn;
-                tile_coords(tile, P.tiles_m, P.tiles_n, tm, tn, P.band_rows);
-                const int b = inst & 1;
+                crt_job_tile(P.tri, tile, P.tiles_m, P.tiles_n, P.band_rows, tm, tn);
+                const int b = inst++ & 1;
                 if (!(ok = wait_phase(&tfull[b], (tphase >> b) & 1u, W, WAIT_EPILOGUE_TFULL))) break;
                 tphase ^= 1u << b;
                 tc_fence_after();
@@ -1310,12 +1334,16 @@ template <int NMOD, typename T>
 __global__ void __launch_bounds__(256)
 ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m, int n, const int* __restrict__ expa,
                   const int* __restrict__ expb, double alpha, double beta, T* __restrict__ C, long ldc,
-                  const __grid_constant__ CrtCombine K, const int* __restrict__ status) {
+                  const __grid_constant__ CrtCombine K, const int* __restrict__ status, int tri) {
     // every modulus is >= 191 > 2^7.5, so log2 M >= 7.5 NMOD
     constexpr int Z0 = (15 * NMOD - 78) > 0 ? (15 * NMOD - 78) / 32 : 0;
     constexpr double kScaleZ0 = pow2_const(16 * Z0);
     // The modular products did not all complete (a bounded wait ran out): C stays as it was.
     if (*status) return;
+    // triangle mode: blocks with no entry of the stored triangle (their residues were not computed)
+    if ((tri == 1 && (int)blockIdx.x * 16 > (int)blockIdx.y * 128 + 127) ||
+        (tri == 2 && (int)blockIdx.x * 16 + 15 < (int)blockIdx.y * 128))
+        return;
     __shared__ double ct[16][129];
     __shared__ int lb[8][64 * kLimbStride];
     __shared__ int sexa[16], sexb[128];  // row / column exponents (kNonFinite: Inf / NaN in the row / column)
@@ -1410,7 +1438,7 @@ ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m,
 
 template <typename T>
 using CombineFn = void (*)(const int8_t*, long, int, int, int, const int*, const int*, double, double, T*, long,
-                           CrtCombine, const int*);
+                           CrtCombine, const int*, int);
 template <int N, typename T>
 constexpr CombineFn<T> combine_at(int nmod) {
     if constexpr (N == 1)
@@ -1887,12 +1915,19 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
 
     ViewT<T> va{g.a, g.transa == 'N' ? 1 : g.lda, g.transa == 'N' ? g.lda : 1, g.m, g.k};
     ViewT<T> vb{g.b, g.transb == 'N' ? g.ldb : 1, g.transb == 'N' ? 1 : g.ldb, g.n, g.k};
+    // op(B)^T is op(A) itself (C = A A^T or A^T A, as SYRK asks): op(B)'s planes,
+    // exponents and Inf / NaN list are op(A)'s, so they are computed once
+    const bool same = !a_ready && p.pair && p.m_pad == p.n_pad && g.m == g.n && g.a == g.b && g.lda == g.ldb &&
+                      ((g.transa == 'N') != (g.transb == 'N'));
+    const int sides = same ? 1 : 2;
+    // triangle mode (CTA-pair kernel): only the tiles meeting the stored triangle of C
+    const int tri = p.pair ? g.tri : 0;
     // a_ready: op(A)'s statistics, exponents, Inf / NaN row list and planes stay;
     // op(B)'s accumulators, its list count and the status word are cleared
     cudaError_t e = a_ready ? cudaMemsetAsync(w + L.maxb_off, 0, L.b_clear_end - L.maxb_off, st)
                             : cudaMemsetAsync(w, 0, L.b_clear_end, st);
     if (e != cudaSuccess) return e;
-    for (int side = a_ready ? 1 : 0; side < 2; ++side) {
+    for (int side = a_ready ? 1 : 0; side < sides; ++side) {
         const ViewT<T>& v = side ? vb : va;
         if (v.rs == 1) {
             dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
@@ -1903,7 +1938,7 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
         }
         count_launch();
     }
-    for (int side = a_ready ? 1 : 0; side < 2; ++side) {
+    for (int side = a_ready ? 1 : 0; side < sides; ++side) {
         const ViewT<T>& v = side ? vb : va;
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
@@ -1913,13 +1948,21 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
         count_launch();
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (same) {  // op(B)'s column exponents and Inf / NaN list are op(A)'s row ones
+        if ((e = cudaMemcpyAsync(expb, expa, (size_t)p.n_pad * sizeof(int), cudaMemcpyDeviceToDevice, st)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(cntb, cnta, sizeof(int), cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(listb, lista, (size_t)g.n * sizeof(int), cudaMemcpyDeviceToDevice, st)) !=
+                cudaSuccess)
+            return e;
+    }
 
     CUtensorMap ma, mb;
     if ((e = make_map(&ma, a_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)nmod * p.m_pad, kUM)) !=
         cudaSuccess)
         return e;
-    if ((e = make_map(&mb, b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad, (long)nmod * p.n_pad,
-                      p.pair ? kUN / 2 : kUN)) != cudaSuccess)
+    if ((e = make_map(&mb, same ? a_planes : b_planes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, p.k_pad,
+                      (long)nmod * p.n_pad, p.pair ? kUN / 2 : kUN)) != cudaSuccess)
         return e;
 
     UmmaParams P{};
@@ -1959,6 +2002,10 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
         return (mb >= 4 && mb <= 120 ? mb : 48) << 20;
     }();
     P.band_rows = (int)std::max(1L, std::min<long>(P.tiles_m, band_bytes / (256L * p.k_pad)));
+    if (tri && P.tiles_m == P.tiles_n) {  // the tiles meeting the stored triangle only
+        P.tri = tri;
+        P.num_tiles = P.tiles_m * (P.tiles_m + 1) / 2;
+    }
     if ((e = set_wait_params(P, p.hold)) != cudaSuccess) return e;
     e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
     if (e != cudaSuccess) return e;
@@ -1966,7 +2013,7 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
     dim3 cgrid((g.m + 15) / 16, (g.n + 127) / 128);
     combine_at<kCrtMaxModuli, T>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
                                                              (double)g.alpha, (double)g.beta, g.c, g.ldc, H.K,
-                                                             status);
+                                                             status, tri);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_nonfinite_patch(g, va, vb, L, w, st);
