@@ -373,12 +373,22 @@ trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, 
         }
     }
     cp_async_commit();
-    for (int idx = t; idx < kLeaf * kLeafCols; idx += 256) {
+    // all sixteen loads of a thread in flight before the first shared store (a
+    // load-store loop waited out one L2 round trip per element)
+    constexpr int kZIt = kLeaf * kLeafCols / 256;
+    double zv[kZIt];
+#pragma unroll
+    for (int i = 0; i < kZIt; ++i) {
+        const int idx = i * 256 + t;
         const int r = left ? idx % kLeaf : idx / kLeafCols, c = left ? idx / kLeaf : idx % kLeafCols;
-        double v = 0.0;
+        zv[i] = 0.0;
         if (r < len && c < nc)
-            v = left ? b[(p0 + r) + (long)(c0 + c) * ldb] : b[(c0 + c) + (long)(p0 + r) * ldb];
-        Z[r][c] = v;
+            zv[i] = left ? b[(p0 + r) + (long)(c0 + c) * ldb] : b[(c0 + c) + (long)(p0 + r) * ldb];
+    }
+#pragma unroll
+    for (int i = 0; i < kZIt; ++i) {
+        const int idx = i * 256 + t;
+        Z[left ? idx % kLeaf : idx / kLeafCols][left ? idx / kLeaf : idx % kLeafCols] = zv[i];
     }
     cluster_sync();  // every CTA of the cluster has read its Z from B
     cp_async_wait<0>();

@@ -1718,7 +1718,11 @@ cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const
     auto kern = umma_slice_gemm_2cta<KIND, EPI>;
     cudaError_t e = ensure_dynamic_smem(kern, (int)kSmemBytes2);
     if (e != cudaSuccess) return e;
-    const int pairs = std::min(P.num_tiles, sm_count_cached() / 2);
+    // CRT residues deal independent (modulus, tile) items to the pairs, so a
+    // product with fewer tiles than pairs still fills the GPU; the slice
+    // epilogues keep every job of a tile on one pair
+    const long items = EPI == EPI_RESIDUE ? (long)P.num_jobs * P.num_tiles : P.num_tiles;
+    const int pairs = (int)std::min<long>(items, sm_count_cached() / 2);
     prof_begin(st);
     kern<<<2 * pairs, kThreads, kSmemBytes2, st>>>(ma, mb, P);
     count_launch();
