@@ -176,3 +176,59 @@ def test_workspace_growth_refused_under_capture(blas):
         assert torch.equal(out, ref)
     finally:
         blas.set_dgemm_method(old)
+
+
+@pytest.mark.parametrize("ta,tb", TRANS)
+@pytest.mark.parametrize("shape", [
+    (256, 512, 256),   # blocked TRSM coupling: 32 tiles of 64 x 64, K split four ways
+    (200, 130, 1000),  # ragged tiles, K split into 64-deep-aligned ranges
+    (1030, 1020, 1500),  # 128 x 128 cp.async tiles (odd leading dimensions), K split in two
+], ids=lambda s: "x".join(map(str, s)))
+def test_splitk_fixup_repeats(blas, oracle, ta, tb, shape):
+    """Split K through the workspace and the ordered reduction: right on every
+    call and bit-identical across calls, with other split shapes run in
+    between on the same stream."""
+    import torch
+    m, n, k = shape
+    rng = np.random.default_rng(m + 3 * n + k)
+    ar, ac = (m, k) if ta == "N" else (k, m)
+    br, bc = (k, n) if tb == "N" else (n, k)
+    lda, ldb, ldc = ar + 1, br + 3, m + 1  # odd: the cp.async kernels
+    a = np.asfortranarray(rng.uniform(-1, 1, (lda, ac)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (ldb, bc)))
+    c0 = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)))
+    ref = c0.copy(order="F")
+    oracle.gemm(ta, tb, m, n, k, 0.75, a, lda, b, ldb, -1.5, ref, ldc)
+    ta_ = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    tb_ = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    other_a = torch.rand((300, 200), device="cuda", dtype=torch.float64)  # 200 x 300 x 300 split product
+    other_c = torch.zeros((200, 200), device="cuda", dtype=torch.float64)
+    outs = []
+    for _ in range(3):
+        tc_ = torch.from_numpy(np.ascontiguousarray(c0.T)).cuda()
+        blas.dgemm_device(ta, tb, m, n, k, 0.75, ta_, lda, tb_, ldb, -1.5, tc_, ldc)
+        blas.dgemm_device("N", "T", 200, 200, 300, 1.0, other_a, 200, other_a, 200, 0.0, other_c, 200)
+        torch.cuda.synchronize()
+        outs.append(np.asfortranarray(tc_.cpu().numpy().T))
+    bound = gemm_bound(ta, tb, m, n, k, 0.75, a, lda, b, ldb, -1.5, c0, U64)
+    err = np.abs(outs[0][:m, :n] - ref[:m, :n])
+    assert np.all(err <= bound), (float(err.max()), float((err / bound).max()))
+    assert np.array_equal(outs[0][m:], c0[m:]), "padding rows of C were written"
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0]), "split-K result changed between calls"
+
+
+@pytest.mark.parametrize("uplo", ["U", "L"])
+def test_splitk_fixup_triangle(blas, oracle, uplo):
+    """SYRK on 64 x 64 tiles with split K: the reduction writes only the stored triangle."""
+    rng = np.random.default_rng(9)
+    n, k = 300, 900
+    a = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    c = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    c0 = c.copy(order="F")
+    blas.syrk(uplo, "T", n, k, -0.5, a, k, 2.0, c, n)
+    full = -0.5 * (a.T @ a) + 2.0 * c0
+    mask = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+    bound = 4 * k * U64 * (0.5 * (np.abs(a.T) @ np.abs(a)) + 2.0 * np.abs(c0)) + 1e-300
+    assert np.all(np.abs(c - full)[mask] <= bound[mask])
+    assert np.array_equal(c[~mask], c0[~mask]), "the other triangle was written"

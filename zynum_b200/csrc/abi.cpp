@@ -592,12 +592,15 @@ cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
 }
 
 // SYRK / SYR2K in FP64 take the emulated product when the DGEMM method is
-// Ozaki, or automatic and the model prefers one full emulated DGEMM (plus a
-// W write and the triangle pass) over native triangle-mode tiles (half the flops).
-inline bool rank_k_uses_ozaki(int n, int k) {
+// Ozaki, or automatic and the model prefers it (plus the triangle pass over W)
+// to the native route.  SYRK: native triangle-mode tiles against emulated
+// products on the triangle's tiles, each half a full product; SYR2K: two
+// native triangle-mode GEMMs against one full emulated W.
+inline bool rank_k_uses_ozaki(int n, int k, bool two) {
     const int method = context().dgemm_method;
     if (method == METHOD_OZAKI) return true;
-    return method == METHOD_AUTO && ozaki_preferred_scaled(n, n, k, 0.5, 24.0 * n * (double)n);
+    const double half = two ? 1.0 : 0.5;
+    return method == METHOD_AUTO && ozaki_preferred_scaled(n, n, k, half, half, 24.0 * n * (double)n);
 }
 
 // W = op(A) op(B)^T as one emulated DGEMM into scratch, then
@@ -628,8 +631,8 @@ cudaError_t run_syrk(char uplo, char trans, int n, int k, T alpha, const T* a, l
     if (n <= 0) return cudaSuccess;
     if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
     if constexpr (sizeof(T) == 8) {
-        if (rank_k_uses_ozaki(n, k)) return run_rank_k_ozaki(uplo, trans, false, n, k, alpha, a, lda, a, lda, beta, c,
-                                                             ldc, st, scratch);
+        if (rank_k_uses_ozaki(n, k, false))
+            return run_rank_k_ozaki(uplo, trans, false, n, k, alpha, a, lda, a, lda, beta, c, ldc, st, scratch);
     }
     Context& cx = context();
     GemmArgs<T> g{trans == 'N' ? 'N' : 'T', trans == 'N' ? 'T' : 'N', n, n, k, alpha, a, lda, a, lda, beta, c, ldc};
@@ -684,8 +687,8 @@ cudaError_t run_syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, 
     if (n <= 0) return cudaSuccess;
     if (k == 0) return syrk_scale_only<T>(n, uplo, beta, c, ldc, st);
     if constexpr (sizeof(T) == 8) {
-        if (rank_k_uses_ozaki(n, k)) return run_rank_k_ozaki(uplo, trans, true, n, k, alpha, a, lda, b, ldb, beta, c,
-                                                             ldc, st, scratch);
+        if (rank_k_uses_ozaki(n, k, true))
+            return run_rank_k_ozaki(uplo, trans, true, n, k, alpha, a, lda, b, ldb, beta, c, ldc, st, scratch);
     }
     Context& cx = context();
     const char t1 = trans == 'N' ? 'N' : 'T', t2 = trans == 'N' ? 'T' : 'N';

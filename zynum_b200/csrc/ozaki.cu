@@ -1748,21 +1748,24 @@ static bool use_cta_pair(int m) {
     return enabled && m >= 256;
 }
 
-// Automatic method choice: Ozaki when its modelled time (16 INT8 products at
-// ~3 POPS, ~32 B per operand element and ~40 B per C element of statistics,
-// residue and reconstruction traffic at ~2.5 TB/s, ~60 us of launches) is
-// below 0.8 x native FP64 at ~30 TFLOP/s; K beyond one CRT segment falls back
-// to the slice scheme, which needs larger products still.
-bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double extra_bytes) {
+// Automatic method choice from call times fitted to measured B200 runs (FP64
+// through dgemm_device, 16 moduli, beta 1; shapes 256^3 .. 8192^3, 1536^3 and
+// 3072^3, N = 512 and K = 512 panels).  Emulated: the 16 modular products at
+// an effective 4.7 POPS, 7.1 ps per operand element (statistics and residues),
+// 24.2 ps per C element (residue epilogue and reconstruction), 52.6 us of
+// launches and per-kernel latency; relative error of the fit under 10 %
+// except 8192^3 (9 %).  Native: 32 TFLOP/s plus 15 us.  Ozaki is taken below
+// 0.9 x the native time; K beyond one CRT segment falls back to the slice
+// scheme, which needs larger products still.
+bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double ozaki_fraction, double extra_bytes) {
     const double mnk2 = 2.0 * m * n * (double)k;
-    const double native_s = native_fraction * mnk2 / 30e12;
-    const double ozaki_s = 16.0 * mnk2 / 3.0e15 +
-                           (32.0 * ((double)m * k + (double)k * n) + 40.0 * (double)m * n + extra_bytes) / 2.5e12 +
-                           60e-6;
-    return k <= kCrtMaxK ? ozaki_s < 0.8 * native_s : native_fraction * mnk2 >= 2e12;
+    const double native_s = native_fraction * mnk2 / 32e12 + 15e-6;
+    const double ozaki_s = ozaki_fraction * (16.0 * mnk2 / 4.7e15 + 24.2e-12 * m * (double)n) +
+                           7.1e-12 * ((double)m * k + (double)k * n) + extra_bytes / 6e12 + 52.6e-6;
+    return k <= kCrtMaxK ? ozaki_s < 0.9 * native_s : native_fraction * mnk2 >= 2e12;
 }
 
-bool ozaki_preferred(int m, int n, int k) { return ozaki_preferred_scaled(m, n, k, 1.0, 0.0); }
+bool ozaki_preferred(int m, int n, int k) { return ozaki_preferred_scaled(m, n, k, 1.0, 1.0, 0.0); }
 
 int ozaki_auto_slices(float spread_a, float spread_b) {
     // Truncating a row of A after s 7-bit digits leaves |dA_ik| < 2^(e_i - 7s)

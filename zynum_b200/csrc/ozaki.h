@@ -45,9 +45,10 @@ cudaError_t wait_report_word(int** out);
 // Whether the automatic method should prefer Ozaki for this shape.
 bool ozaki_preferred(int m, int n, int k);
 // The same model against a native route that does native_fraction of the full
-// product's flops (0.5: triangle-mode tiles) while the emulated route moves
-// extra_bytes more through HBM.
-bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double extra_bytes);
+// product's flops (0.5: triangle-mode tiles), the emulated route ozaki_fraction
+// of its products and reconstruction (0.5: triangle tiles) and extra_bytes more
+// through HBM.
+bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double ozaki_fraction, double extra_bytes);
 // Scheme choice: OZAKI_AUTO takes the slice scheme when `slices` > 0 and the
 // CRT scheme otherwise (K <= kCrtMaxK); OZAKI_CRT falls back to slices beyond
 // kCrtMaxK.  slices == 0 leaves the slice count to dgemm_ozaki, which derives
