@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -167,6 +168,29 @@ ZB_DEVICE uint64_t umma_desc_sw128(uint32_t addr) {
 //   c_format: 1 = F32, 2 = S32;  ab_format: i8 -> 1 (signed), f16 kind -> 1 (BF16)
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t c_format, uint32_t ab_format, uint32_t m, uint32_t n) {
     return (c_format << 4) | (ab_format << 7) | (ab_format << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+// ------------------------------------------- programmatic dependent launch
+// A kernel launched with launch_dependent() may start while the kernel before
+// it in the stream is still finishing; it must call grid_dependency_wait()
+// before it touches memory that kernel writes.  The wait is resolved by the
+// hardware when that kernel has completed and its writes are visible (a
+// no-op for a kernel launched without the attribute).
+ZB_DEVICE void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+template <typename... P, typename... A>
+cudaError_t launch_dependent(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
 // ------------------------------------------------------------- clusters

@@ -88,6 +88,8 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
     const int kb = blockIdx.z * k_chunk;
     const int ke = min(K, kb + k_chunk);
     const int KT = (ke - kb + BK - 1) / BK;
+    // launched during the tail of the kernel before it (which may write A, B or C)
+    grid_dependency_wait();
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -203,6 +205,7 @@ dgemm_dmma_kernel(int M, int N, int K, int k_chunk, double alpha, const double* 
 
 __global__ void dgemm_splitk_reduce(int M, int N, int splits, const double* __restrict__ W, double alpha, double beta,
                                     double* __restrict__ C, long ldc, int tri) {
+    grid_dependency_wait();  // launched during the tail of the product that writes W
     long total = (long)M * N;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
         int row = (int)(q % M), col = (int)(q / M);
@@ -227,11 +230,11 @@ cudaError_t launch_one(const GemmArgsF64& g, int splits, int k_chunk, double* W,
     if (e != cudaSuccess) return e;
     dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, splits);
     prof_begin(st);
-    kern<<<grid, NTHREADS, SMEM, st>>>(g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b, g.ldb, g.beta, g.c, g.ldc, W,
-                                       g.tri);
+    e = launch_dependent(kern, grid, dim3(NTHREADS), SMEM, st, g.m, g.n, g.k, k_chunk, g.alpha, g.a, g.lda, g.b,
+                         g.ldb, g.beta, g.c, g.ldc, W, g.tri);
     count_launch();
     prof_end(st);
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES, bool PARTIAL, int BK>
@@ -250,9 +253,10 @@ cudaError_t splitk_reduce(const GemmArgsF64& g, int used_splits, double* workspa
     long total = (long)g.m * g.n;
     int blocks = (int)((total + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    dgemm_splitk_reduce<<<blocks, 256, 0, st>>>(g.m, g.n, used_splits, workspace, g.alpha, g.beta, g.c, g.ldc, g.tri);
+    cudaError_t e = launch_dependent(dgemm_splitk_reduce, dim3(blocks), dim3(256), 0, st, g.m, g.n, used_splits,
+                                     (const double*)workspace, g.alpha, g.beta, g.c, g.ldc, g.tri);
     count_launch();
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES, int BK = kBK>

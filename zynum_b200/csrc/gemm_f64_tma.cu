@@ -104,6 +104,8 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         prefetch_tmap(&tmB);
     }
     __syncthreads();
+    // launched during the tail of the kernel before it (which may write A, B or C)
+    grid_dependency_wait();
     const WaitCtl W{abort_flag, nullptr, P.report, P.wait_ns};
 
     if (warp >= kTMathWarps) {
@@ -288,10 +290,10 @@ cudaError_t launch_tma(const CUtensorMap& ma, const CUtensorMap& mb, const TmaGe
     if (e != cudaSuccess) return e;
     dim3 grid((P.M + kTBM - 1) / kTBM, (P.N + kTBN - 1) / kTBN, splits);
     prof_begin(st);
-    kern<<<grid, kTThreads, kTSmem, st>>>(ma, mb, P);
+    e = launch_dependent(kern, grid, dim3(kTThreads), kTSmem, st, ma, mb, P);
     count_launch();
     prof_end(st);
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <bool PARTIAL>

@@ -373,6 +373,10 @@ trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, 
         }
     }
     cp_async_commit();
+    // The inverse is not written by the kernel before this one (a coupling
+    // product or its reduction): its copies above may overlap that kernel's
+    // tail; the rows of B it updates are read after it has finished.
+    grid_dependency_wait();
     // all sixteen loads of a thread in flight before the first shared store (a
     // load-store loop waited out one L2 round trip per element)
     constexpr int kZIt = kLeaf * kLeafCols / 256;
@@ -761,8 +765,9 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
         e = ensure_dynamic_smem(trsm_leaf<T>, leaf_smem);
     }
     if (e != cudaSuccess) return e;
+    bool first_leaf = true;
     std::function<cudaError_t(int, int)> solve = [&](int p0, int p1) -> cudaError_t {
-        cudaError_t err;
+        cudaError_t err = cudaSuccess;
         const int len = p1 - p0;
         if (len <= kLeaf) {
             const int grid = (ncols + kLeafCols - 1) / kLeafCols;
@@ -782,11 +787,21 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
                     return err;
                 return gemm({'N', 'N', m, len, len, T(1), W, m, il, kLeaf, T(0), t.b + (long)p0 * ldb, ldb});
             }
-            if (inv_leaves)  // clusters of four CTAs per 16 right-hand sides
-                trsm_leaf_apply<<<4 * grid, 256, leaf_smem, st>>>(inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf, left,
-                                                                  fwd, p0, len, reinterpret_cast<double*>(t.b), ldb,
-                                                                  ncols);
-            else
+            if (inv_leaves) {  // clusters of four CTAs per 16 right-hand sides
+                const double* il = inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf;
+                double* bd = reinterpret_cast<double*>(t.b);
+                // every leaf after the first follows a coupling product (or its reduction),
+                // which does not write the inverses: it may start during that kernel's tail
+                if (!first_leaf)
+                    err = launch_dependent(trsm_leaf_apply, dim3(4 * grid), dim3(256), (size_t)leaf_smem, st, il, left,
+                                           fwd, p0, len, bd, ldb, ncols);
+                else
+                    trsm_leaf_apply<<<4 * grid, 256, leaf_smem, st>>>(il, left, fwd, p0, len, bd, ldb, ncols);
+                first_leaf = false;
+                count_launch();
+                if (err != cudaSuccess) return err;
+                return cudaGetLastError();
+            } else
                 trsm_leaf<T><<<grid, 256, leaf_smem, st>>>(t.a, lda, ta == 'N', is_cnum<T>::value && t.trans == 'C',
                                                            left, fwd, inv, p0, len, t.b, ldb, ncols);
             count_launch();
