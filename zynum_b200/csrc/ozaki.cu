@@ -392,6 +392,8 @@ umma_slice_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // launched during the tail of the residue / digit split that writes the planes
+    grid_dependency_wait();
     const uint32_t tmem_base = *tmem_slot;
     const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
 
@@ -693,6 +695,8 @@ umma_slice_gemm_2cta(const __grid_constant__ CUtensorMap tmA, const __grid_const
     __syncthreads();
     cluster_sync();  // the peer's barriers (and abort flag) exist before any remote access
     tc_fence_after();
+    // launched during the tail of the residue / digit split that writes the planes
+    grid_dependency_wait();
     const uint32_t tmem_base = *tmem_slot;
     const int elems_per_chunk = (KIND == KIND_I8) ? kChunkBytes : kChunkBytes / 2;
 
@@ -1020,6 +1024,7 @@ ZB_DEVICE void note_nonfinite(int r, int* count, int* list) { list[atomicAdd(cou
 // the CRT row scale).  T = float reads FP32 operands, widened exactly.
 template <typename T>
 __global__ void ozaki_absmax(ViewT<T> X, unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
+    grid_dependency_wait();  // may be launched during the tail of the kernel before it
     if (X.rs == 1) {
         const int r = blockIdx.x * blockDim.x + threadIdx.x;
         if (r >= X.rows) return;
@@ -1197,6 +1202,7 @@ ozaki_crt_split(ViewT<T> X, const unsigned long long* __restrict__ maxbits, cons
     __shared__ int sexp[32];
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 128;
     const int t = threadIdx.x;
+    grid_dependency_wait();  // launched during the tail of the statistics pass
     if (t < 32) {
         const int r = r0 + t;
         const int e = (r < X.rows) ? crt_row_exponent(maxbits[r], sums[r], X.cols, P) : 0;
@@ -1338,6 +1344,7 @@ ozaki_crt_combine(const int8_t* __restrict__ res, long plane, int res_ld, int m,
     // every modulus is >= 191 > 2^7.5, so log2 M >= 7.5 NMOD
     constexpr int Z0 = (15 * NMOD - 78) > 0 ? (15 * NMOD - 78) / 32 : 0;
     constexpr double kScaleZ0 = pow2_const(16 * Z0);
+    grid_dependency_wait();  // launched during the tail of the products that write the residues
     // The modular products did not all complete (a bounded wait ran out): C stays as it was.
     if (*status) return;
     // triangle mode: blocks with no entry of the stored triangle (their residues were not computed)
@@ -1466,6 +1473,7 @@ ozaki_nonfinite_patch(ViewT<T> va, ViewT<T> vb, int m, int n, int k, double alph
                       long ldc, const int* __restrict__ cnt_a, const int* __restrict__ list_a,
                       const int* __restrict__ cnt_b, const int* __restrict__ list_b, const int* __restrict__ expa,
                       const int* __restrict__ status) {
+    grid_dependency_wait();  // launched during the tail of the reconstruction that writes C
     if (*status) return;  // the product did not complete: C stays as it was
     const int na = *cnt_a, nb = *cnt_b;
     if (na == 0 && nb == 0) return;
@@ -1700,21 +1708,28 @@ cudaError_t set_wait_params(UmmaParams& P, bool hold) {
     return cudaSuccess;
 }
 
+// dependent: the kernel before it in the stream is one of this library's
+// kernels (not a copy or memset), so the launch may overlap its tail.
 template <int KIND, int EPI>
-cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
+cudaError_t launch_umma(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st,
+                        bool dependent = true) {
     auto kern = umma_slice_gemm<KIND, EPI>;
     cudaError_t e = ensure_dynamic_smem(kern, (int)kSmemBytes);
     if (e != cudaSuccess) return e;
     const int grid = P.num_tiles < sm_count_cached() ? P.num_tiles : sm_count_cached();
     prof_begin(st);
-    kern<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, P);
+    if (dependent)
+        e = launch_dependent(kern, dim3(grid), dim3(kThreads), kSmemBytes, st, ma, mb, P);
+    else
+        kern<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, P);
     count_launch();
     prof_end(st);
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int KIND, int EPI>
-cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st) {
+cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const UmmaParams& P, cudaStream_t st,
+                             bool dependent = true) {
     auto kern = umma_slice_gemm_2cta<KIND, EPI>;
     cudaError_t e = ensure_dynamic_smem(kern, (int)kSmemBytes2);
     if (e != cudaSuccess) return e;
@@ -1724,10 +1739,13 @@ cudaError_t launch_umma_2cta(const CUtensorMap& ma, const CUtensorMap& mb, const
     const long items = EPI == EPI_RESIDUE ? (long)P.num_jobs * P.num_tiles : P.num_tiles;
     const int pairs = (int)std::min<long>(items, sm_count_cached() / 2);
     prof_begin(st);
-    kern<<<2 * pairs, kThreads, kSmemBytes2, st>>>(ma, mb, P);
+    if (dependent)
+        e = launch_dependent(kern, dim3(2 * pairs), dim3(kThreads), kSmemBytes2, st, ma, mb, P);
+    else
+        kern<<<2 * pairs, kThreads, kSmemBytes2, st>>>(ma, mb, P);
     count_launch();
     prof_end(st);
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace
@@ -1890,12 +1908,14 @@ cudaError_t launch_nonfinite_patch(const GemmArgs<T>& g, const ViewT<T>& va, con
                                    uint8_t* w, cudaStream_t st) {
     const int* cnta = reinterpret_cast<const int*>(w + L.cnta_off);
     const int* cntb = reinterpret_cast<const int*>(w + L.cntb_off);
-    ozaki_nonfinite_patch<T><<<2 * sm_count_cached(), 256, 0, st>>>(
-        va, vb, g.m, g.n, g.k, (double)g.alpha, (double)g.beta, g.c, g.ldc, cnta, reinterpret_cast<const int*>(w + L.lista_off), cntb,
-        reinterpret_cast<const int*>(w + L.listb_off), reinterpret_cast<const int*>(w + L.expa_off),
-        reinterpret_cast<const int*>(w + L.status_off));
+    cudaError_t e = launch_dependent(ozaki_nonfinite_patch<T>, dim3(2 * sm_count_cached()), dim3(256), 0, st, va, vb,
+                                     g.m, g.n, g.k, (double)g.alpha, (double)g.beta, g.c, g.ldc, cnta,
+                                     reinterpret_cast<const int*>(w + L.lista_off), cntb,
+                                     reinterpret_cast<const int*>(w + L.listb_off),
+                                     reinterpret_cast<const int*>(w + L.expa_off),
+                                     reinterpret_cast<const int*>(w + L.status_off));
     count_launch();
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
@@ -1936,22 +1956,25 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
     if (e != cudaSuccess) return e;
     for (int side = a_ready ? 1 : 0; side < sides; ++side) {
         const ViewT<T>& v = side ? vb : va;
-        if (v.rs == 1) {
-            dim3 grid((v.rows + 255) / 256, (v.cols + 63) / 64);
+        const dim3 grid = v.rs == 1 ? dim3((v.rows + 255) / 256, (v.cols + 63) / 64)
+                                    : dim3((v.rows + 7) / 8, (v.cols + 1023) / 1024);
+        // the first pass follows the memset of the statistics: an ordinary launch
+        if (side == (a_ready ? 1 : 0))
             ozaki_absmax<T><<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
-        } else {
-            dim3 grid((v.rows + 7) / 8, (v.cols + 1023) / 1024);
-            ozaki_absmax<T><<<grid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma);
-        }
+        else if ((e = launch_dependent(ozaki_absmax<T>, grid, dim3(256), 0, st, v, side ? maxb : maxa,
+                                       side ? sumb : suma)) != cudaSuccess)
+            return e;
         count_launch();
     }
     for (int side = a_ready ? 1 : 0; side < sides; ++side) {
         const ViewT<T>& v = side ? vb : va;
         const int rows_pad = side ? p.n_pad : p.m_pad;
         dim3 sgrid(p.k_pad / 128, rows_pad / 32);
-        ozaki_crt_split<T><<<sgrid, 256, 0, st>>>(v, side ? maxb : maxa, side ? sumb : suma, H.P, nmod, rows_pad,
-                                               p.k_pad, side ? b_planes : a_planes, side ? expb : expa,
-                                               side ? cntb : cnta, side ? listb : lista);
+        if ((e = launch_dependent(ozaki_crt_split<T>, sgrid, dim3(256), 0, st, v, (const unsigned long long*)(side ? maxb : maxa),
+                                  (const double*)(side ? sumb : suma), H.P, nmod, rows_pad, p.k_pad,
+                                  side ? b_planes : a_planes, side ? expb : expa, side ? cntb : cnta,
+                                  side ? listb : lista)) != cudaSuccess)
+            return e;
         count_launch();
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2014,13 +2037,17 @@ cudaError_t gemm_ozaki_crt(const GemmArgs<T>& g, const OzakiPlan& p, void* ws, c
         P.num_tiles = P.tiles_m * (P.tiles_m + 1) / 2;
     }
     if ((e = set_wait_params(P, p.hold)) != cudaSuccess) return e;
-    e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st) : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st);
+    // after op(A)'s exponents and lists were copied to op(B)'s (one operand split once) the
+    // kernel before the products is a copy: an ordinary launch
+    e = p.pair ? launch_umma_2cta<KIND_I8, EPI_RESIDUE>(ma, mb, P, st, !same)
+               : launch_umma<KIND_I8, EPI_RESIDUE>(ma, mb, P, st, !same);
     if (e != cudaSuccess) return e;
 
     dim3 cgrid((g.m + 15) / 16, (g.n + 127) / 128);
-    combine_at<kCrtMaxModuli, T>(nmod)<<<cgrid, 256, 0, st>>>(residues, P.res_plane, p.n_pad, g.m, g.n, expa, expb,
-                                                             (double)g.alpha, (double)g.beta, g.c, g.ldc, H.K,
-                                                             status, tri);
+    if ((e = launch_dependent(combine_at<kCrtMaxModuli, T>(nmod), cgrid, dim3(256), 0, st, (const int8_t*)residues,
+                              P.res_plane, p.n_pad, g.m, g.n, (const int*)expa, (const int*)expb, (double)g.alpha,
+                              (double)g.beta, g.c, (long)g.ldc, H.K, (const int*)status, tri)) != cudaSuccess)
+        return e;
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_nonfinite_patch(g, va, vb, L, w, st);
