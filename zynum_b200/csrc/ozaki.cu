@@ -1769,17 +1769,17 @@ static bool use_cta_pair(int m) {
 // Automatic method choice from call times fitted to measured B200 runs (FP64
 // through dgemm_device, 16 moduli, beta 1; shapes 256^3 .. 8192^3, 1536^3 and
 // 3072^3, N = 512 and K = 512 panels).  Emulated: the 16 modular products at
-// an effective 4.7 POPS, 7.1 ps per operand element (statistics and residues),
-// 24.2 ps per C element (residue epilogue and reconstruction), 52.6 us of
-// launches and per-kernel latency; relative error of the fit under 10 %
-// except 8192^3 (9 %).  Native: 32 TFLOP/s plus 15 us.  Ozaki is taken below
+// an effective 5.0 POPS, 7.0 ps per operand element (statistics and residues),
+// 25.9 ps per C element (residue epilogue and reconstruction), 38.4 us of
+// launches and per-kernel latency; relative error of the fit within 13 %.
+// Native: 32 TFLOP/s plus 15 us.  Ozaki is taken below
 // 0.9 x the native time; K beyond one CRT segment falls back to the slice
 // scheme, which needs larger products still.
 bool ozaki_preferred_scaled(int m, int n, int k, double native_fraction, double ozaki_fraction, double extra_bytes) {
     const double mnk2 = 2.0 * m * n * (double)k;
     const double native_s = native_fraction * mnk2 / 32e12 + 15e-6;
-    const double ozaki_s = ozaki_fraction * (16.0 * mnk2 / 4.7e15 + 24.2e-12 * m * (double)n) +
-                           7.1e-12 * ((double)m * k + (double)k * n) + extra_bytes / 6e12 + 52.6e-6;
+    const double ozaki_s = ozaki_fraction * (16.0 * mnk2 / 5.0e15 + 25.9e-12 * m * (double)n) +
+                           7.0e-12 * ((double)m * k + (double)k * n) + extra_bytes / 6e12 + 38.4e-6;
     return k <= kCrtMaxK ? ozaki_s < 0.9 * native_s : native_fraction * mnk2 >= 2e12;
 }
 
