@@ -29,14 +29,16 @@ GemmPlan plan_native_gemm(int m, int n, int k, int elem_bytes, int sm_count) {
     }
     // FP64 with fewer 128 x 128 tiles than half the SMs and a short K (<= 1024,
     // too short for split-K to fill the machine with 256-deep slices): 64 x 64
-    // tiles (4 warps), K split into slices down to 64 deep until about one wave
-    // of CTAs covers the machine (small products, the coupling GEMMs of blocked
-    // TRSM).  Longer K keeps the 128 x 128 tiles and their split-K below.
+    // tiles (4 warps), K split into slices down to 64 deep until about two CTAs
+    // per SM are resident (small products, the coupling GEMMs of blocked TRSM;
+    // one CTA per SM measured 5-20 % slower at 512-1024 x 512 x 512-1024, three
+    // or four no better than two).  Longer K keeps the 128 x 128 tiles and
+    // their split-K below.
     if (elem_bytes == 8 && k <= 1024 && 2L * ((m + 127) / 128) * ((n + 127) / 128) < sm_count) {
         p.tile = TILE_64x64;
         const long tiles = (long)((m + 63) / 64) * ((n + 63) / 64);
-        if (tiles < sm_count && k >= 128) {
-            long s = sm_count / std::max<long>(tiles, 1);
+        if (tiles < 2L * sm_count && k >= 128) {
+            long s = 2L * sm_count / std::max<long>(tiles, 1);
             s = std::min<long>(s, k / 64);
             s = std::min<long>(s, 64);
             if (s >= 2) p.splits = (int)s;
