@@ -880,6 +880,30 @@ def suite_batched(args):
     return 0
 
 
+def suite_chain(args):
+    """The differentiation workload's pieces alone, for launch lists: the solve
+    X = L^-1 B (L 4096 x 4096 lower, off-diagonals N(0, 1/4096), diagonal
+    1 + |N(0,1)|; B 4096 x 512 N(0,1); FP64, native method) `--warmup` untimed
+    and `--steps` timed calls, then the forward + backward chain likewise."""
+    import torch
+    from zynum_b200 import blas
+    n, r = 4096, 512
+    old = blas.set_dgemm_method(blas.METHOD_NATIVE)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    L = torch.tril(torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64) / n ** 0.5, -1)
+    L += torch.diag(1 + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
+    Lc = L.t().contiguous()  # column-major storage of L
+    B = torch.randn((r, n), generator=g, device="cuda", dtype=torch.float64)  # column-major 4096 x 512
+    X = B.clone()
+    fn = lambda: blas.dtrsm_device("L", "L", "N", "N", n, r, 1.0, Lc, n, X, n)  # noqa: E731
+    ms = time_device(torch, fn, args.steps, args.warmup, torch.cuda.current_stream())
+    blas.set_dgemm_method(old)
+    diff = bench_differentiation(torch, args.steps, args.warmup)
+    print(json.dumps({"suite": "chain", "trsm_4096x512_ms": ms, "trsm_tflops": float(n) ** 2 * r / (ms * 1e-3) / 1e12,
+                      "differentiation": diff}), flush=True)
+    return 0
+
+
 def suite_one(args):
     """One GEMM shape, for profiling a single kernel: --dtype f64|f32|z|c, --m/--n/--k,
     --method (native or ozaki for f64; ozaki means 3xBF16 for f32), --beta, NN,
@@ -938,7 +962,7 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=4096, help="suite one: columns of C")
     ap.add_argument("--k", type=int, default=4096, help="suite one: inner dimension")
     ap.add_argument("--beta", type=float, default=0.0, help="suite one: beta")
-    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched", "one"],
+    ap.add_argument("--suite", choices=["headline", "precision", "sweep", "vector", "level3", "batched", "one", "chain"],
                     default="headline", help="secondary measurement suites (one JSON line each)")
     ap.add_argument("--batch-count", type=int, default=20000,
                     help="batched suite: GEMM problems per batch (TRSM problems: a quarter)")
@@ -971,6 +995,8 @@ def main(argv=None):
             return suite_batched(args)
         if args.suite == "one":
             return suite_one(args)
+        if args.suite == "chain":
+            return suite_chain(args)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

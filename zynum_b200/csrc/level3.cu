@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(256) tri_inv_blocks(const T* __restrict__ a, l
     T(*L)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(tri_smem);
     T(*X)[kNB + 1] = L + kNB;
     T* dinv = reinterpret_cast<T*>(X + kNB);
+    grid_dependency_wait();  // may start during the tail of the kernel before it (which may write A)
     const int b0 = blockIdx.x * kNB;
     const int s = min(kNB, n - b0);
     const int t = threadIdx.x;
@@ -275,6 +276,7 @@ tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int
     double(*X)[kNB][kNB + 1] = reinterpret_cast<double(*)[kNB][kNB + 1]>(til_smem);
     double(*S)[kStagePitch] =
         reinterpret_cast<double(*)[kStagePitch]>(til_smem + sizeof(double) * 4 * kNB * (kNB + 1));
+    grid_dependency_wait();  // launched during the tail of tri_inv_blocks
     const int leaf = blockIdx.x, j = blockIdx.y, t = threadIdx.x;
     const int P = leaf * kLeaf, len = min(kLeaf, na - P), nsb = (len + kNB - 1) / kNB;
     double* out = inv_leaf + (long)leaf * kLeaf * kLeaf;
@@ -342,7 +344,7 @@ tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int
 // w % 2, two accumulators.
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
 trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, int len, double* __restrict__ b,
-                long ldb, int ncols) {
+                long ldb, int ncols, int wait_first) {
     extern __shared__ __align__(16) unsigned char ap_smem[];
     double(*Z)[kLeafCols + 1] = reinterpret_cast<double(*)[kLeafCols + 1]>(ap_smem);
     double* A = reinterpret_cast<double*>(ap_smem + sizeof(double) * kLeaf * (kLeafCols + 1));
@@ -355,6 +357,7 @@ trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, 
     const int klen8 = (klen + 7) & ~7;
     // rows 64 rb + i, columns kbeg + kk of inv(M): side L inv[i' + k' kLeaf] (runs along i, staged
     // [kk][i], pitch 66); side R inv[k' + i' kLeaf] (runs along kk, staged [i][kk], pitch kLeaf + 2)
+    if (wait_first) grid_dependency_wait();  // the kernel before this one wrote the inverses
     if (64 * rb < len && klen > 0) {
         if (left) {
             for (int q = t; q < klen8 * (kNB / 2); q += 256) {
@@ -723,7 +726,9 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     T* inv = static_cast<T*>(planes);
     const int tri_smem = (2 * kNB * (kNB + 1) + kNB) * (int)sizeof(T);
     if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) != cudaSuccess) return e;
-    tri_inv_blocks<T><<<nblk, 256, tri_smem, st>>>(t.a, t.lda, t.uplo, t.trans, t.diag, na, inv);
+    if ((e = launch_dependent(tri_inv_blocks<T>, dim3(nblk), dim3(256), (size_t)tri_smem, st, t.a, t.lda, t.uplo,
+                              t.trans, t.diag, na, inv)) != cudaSuccess)
+        return e;
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const bool upper = op_is_upper(t.uplo, t.trans);
@@ -751,9 +756,10 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
         inv_leaf = reinterpret_cast<double*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na));
         const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + kNB * kStagePitch);
         if ((e = ensure_dynamic_smem(tri_inv_leaf, til_smem)) != cudaSuccess) return e;
-        tri_inv_leaf<<<dim3(nleaf, kLeaf / kNB), 256, til_smem, st>>>(
-            reinterpret_cast<const double*>(t.a), lda, ta == 'N', upper, na, reinterpret_cast<const double*>(inv),
-            inv_leaf);
+        if ((e = launch_dependent(tri_inv_leaf, dim3(nleaf, kLeaf / kNB), dim3(256), (size_t)til_smem, st,
+                                  reinterpret_cast<const double*>(t.a), lda, (int)(ta == 'N'), (int)upper, na,
+                                  reinterpret_cast<const double*>(inv), inv_leaf)) != cudaSuccess)
+            return e;
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         // Z plus 64 rows of the inverse over up to kLeaf columns (either staging layout)
@@ -791,12 +797,10 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
                 const double* il = inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf;
                 double* bd = reinterpret_cast<double*>(t.b);
                 // every leaf after the first follows a coupling product (or its reduction),
-                // which does not write the inverses: it may start during that kernel's tail
-                if (!first_leaf)
-                    err = launch_dependent(trsm_leaf_apply, dim3(4 * grid), dim3(256), (size_t)leaf_smem, st, il, left,
-                                           fwd, p0, len, bd, ldb, ncols);
-                else
-                    trsm_leaf_apply<<<4 * grid, 256, leaf_smem, st>>>(il, left, fwd, p0, len, bd, ldb, ncols);
+                // which does not write the inverses: it stages them during that kernel's
+                // tail; the first follows tri_inv_leaf and waits before staging
+                err = launch_dependent(trsm_leaf_apply, dim3(4 * grid), dim3(256), (size_t)leaf_smem, st, il, left, fwd,
+                                       p0, len, bd, ldb, ncols, (int)first_leaf);
                 first_leaf = false;
                 count_launch();
                 if (err != cudaSuccess) return err;
