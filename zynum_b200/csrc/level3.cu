@@ -82,9 +82,18 @@ __global__ void __launch_bounds__(256) tri_inv_blocks(const T* __restrict__ a, l
     const int b0 = blockIdx.x * kNB;
     const int s = min(kNB, n - b0);
     const int t = threadIdx.x;
-    for (int q = t; q < kNB * kNB; q += 256) {
-        const int r = q % kNB, c = q / kNB;
-        L[r][c] = (r < s && c < s) ? op_tri(a, lda, uplo, trans, diag, b0 + r, b0 + c) : T(0);
+    // all sixteen loads of a thread in flight before the first shared store
+    constexpr int kIt = kNB * kNB / 256;
+    T pre[kIt];
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+        const int q = i * 256 + t, r = q % kNB, c = q / kNB;
+        pre[i] = (r < s && c < s) ? op_tri(a, lda, uplo, trans, diag, b0 + r, b0 + c) : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+        const int q = i * 256 + t, r = q % kNB, c = q / kNB;
+        L[r][c] = pre[i];
         X[r][c] = T(0);
     }
     __syncthreads();
@@ -268,14 +277,19 @@ ZB_DEVICE void mma_64(double (&acc)[4][4], const double (*A)[kStagePitch], bool 
 // `leaf` of op(A), written to inv_leaf + leaf kLeaf^2 (column-major, ld kLeaf;
 // zero outside the triangle and the leaf).  Lower op(A): X_jj = inv(A_jj),
 // X_ij = -inv(A_ii) sum_{k=j}^{i-1} A_ik X_kj for i = j+1, ...; upper op(A):
-// the same for i = j-1, ..., 0 with k = i+1 .. j.
+// the same for i = j-1, ..., 0 with k = i+1 .. j.  The 64-blocks this takes
+// (inv(A_jj), then per row block i its A_ik and inv(A_ii)) are known up front:
+// they are staged through two shared buffers, the next one loading while the
+// current one is used (a load-then-use sequence waited out one L2 or DRAM
+// round trip per block).
 __global__ void __launch_bounds__(256)
 tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int na, const double* __restrict__ inv64,
              double* __restrict__ inv_leaf) {
     extern __shared__ __align__(16) unsigned char til_smem[];
     double(*X)[kNB][kNB + 1] = reinterpret_cast<double(*)[kNB][kNB + 1]>(til_smem);
-    double(*S)[kStagePitch] =
+    double(*S0)[kStagePitch] =
         reinterpret_cast<double(*)[kStagePitch]>(til_smem + sizeof(double) * 4 * kNB * (kNB + 1));
+    double(*S1)[kStagePitch] = S0 + kNB;
     grid_dependency_wait();  // launched during the tail of tri_inv_blocks
     const int leaf = blockIdx.x, j = blockIdx.y, t = threadIdx.x;
     const int P = leaf * kLeaf, len = min(kLeaf, na - P), nsb = (len + kNB - 1) / kNB;
@@ -286,46 +300,84 @@ tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int
         const long sr = trans_n ? 1 : lda, sc = trans_n ? lda : 1;
         auto ablock = [&](int bi, int bk) { return a + (long)(P + bi * kNB) * sr + (long)(P + bk * kNB) * sc; };
         auto iblock = [&](int bi) { return inv64 + (long)(P / kNB + bi) * kNB * kNB; };
-        // X_jj = inv(A_jj)
-        stage_block(S, iblock(j), 1, kNB, kNB, kNB, inv64);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-        for (int q = t; q < kNB * kNB; q += 256) X[j][q % kNB][q / kNB] = staged(S, true, q % kNB, q / kNB);
-        have[j] = true;
+        // steps: 0 = inv(A_jj); then for o = 1, 2, ..: A_ik for k = k0(i) .. k1(i) (o blocks), inv(A_ii)
+        const int nrows = upper ? j : nsb - 1 - j;  // row blocks i below (above) j
+        const int nsteps = 1 + nrows * (nrows + 3) / 2;
+        auto info = [&](int s, bool& inv_step, int& i, int& k) {
+            inv_step = true;
+            i = j;
+            k = 0;
+            int rest = s - 1;
+            for (int o = 1; s > 0; ++o) {
+                const int ii = upper ? j - o : j + o;
+                i = ii;
+                if (rest < o) {
+                    inv_step = false;
+                    k = (upper ? ii + 1 : j) + rest;
+                    return;
+                }
+                if (rest == o) return;
+                rest -= o + 1;
+            }
+        };
+        auto issue = [&](int s) {
+            bool inv_step;
+            int i, k;
+            info(s, inv_step, i, k);
+            double(*Sb)[kStagePitch] = (s & 1) ? S1 : S0;
+            if (inv_step)
+                stage_block(Sb, iblock(i), 1, kNB, kNB, kNB, inv64);
+            else
+                stage_block(Sb, ablock(i, k), sr, sc, len - i * kNB, len - k * kNB, a);
+            cp_async_commit();
+        };
         const int lane = t & 31, warp = t >> 5, g = lane >> 2, tq = lane & 3, rt = warp >> 1, ct0 = (warp & 1) * 4;
-        for (int o = 1; o < nsb; ++o) {
-            const int i = upper ? j - o : j + o;
-            if (i < 0 || i >= nsb) break;
-            double acc[4][4] = {};
-            const int k0 = upper ? i + 1 : j, k1 = upper ? j : i - 1;
-            for (int k = k0; k <= k1; ++k) {  // acc += A_ik X_kj
-                __syncthreads();
-                stage_block(S, ablock(i, k), sr, sc, len - i * kNB, len - k * kNB, a);
-                cp_async_commit();
+        double acc[4][4] = {};
+        issue(0);
+        for (int s = 0; s < nsteps; ++s) {
+            if (s + 1 < nsteps) {
+                issue(s + 1);
+                cp_async_wait<1>();
+            } else {
                 cp_async_wait<0>();
-                __syncthreads();
-                mma_64(acc, S, sr == 1, X[k]);
             }
             __syncthreads();
+            const double(*Sb)[kStagePitch] = (s & 1) ? S1 : S0;
+            bool inv_step;
+            int i, k;
+            info(s, inv_step, i, k);
+            if (s == 0) {  // X_jj = inv(A_jj)
+                for (int q = t; q < kNB * kNB; q += 256) X[j][q % kNB][q / kNB] = staged(Sb, true, q % kNB, q / kNB);
+                have[j] = true;
+            } else if (!inv_step) {  // acc += A_ik X_kj; after the last k the sum goes to X[i]
+                const int k0 = upper ? i + 1 : j, k1 = upper ? j : i - 1;
+                if (k == k0) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u)  // the sum into X[i], then X_ij = -inv(A_ii) * sum
+                    for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = acc[u][v];
-            stage_block(S, iblock(i), 1, kNB, kNB, kNB, inv64);
-            cp_async_commit();
-            cp_async_wait<0>();
-            __syncthreads();
-            double y[4][4] = {};
-            mma_64(y, S, true, X[i]);
-            __syncthreads();
+                        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+                }
+                mma_64(acc, Sb, sr == 1, X[k]);
+                if (k == k1) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+                    for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = -y[u][v];
-            have[i] = true;
+                        for (int v = 0; v < 4; ++v)
+                            X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = acc[u][v];
+                }
+            } else {  // X_ij = -inv(A_ii) * sum
+                double y[4][4] = {};
+                mma_64(y, Sb, true, X[i]);
+                __syncthreads();
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        X[i][16 * rt + g + 8 * (v >> 1)][8 * (ct0 + u) + 2 * tq + (v & 1)] = -y[u][v];
+                have[i] = true;
+            }
+            __syncthreads();  // the buffer of step s is refilled by the issue of step s + 2
         }
-        __syncthreads();
     }
     // column block j of the leaf inverse: rows of computed blocks, zeros elsewhere
     for (int q = t; q < kLeaf * kNB; q += 256) {
@@ -754,7 +806,7 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     if (inv_leaves) {
         const int nleaf = (na + kLeaf - 1) / kLeaf;
         inv_leaf = reinterpret_cast<double*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na));
-        const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + kNB * kStagePitch);
+        const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + 2 * kNB * kStagePitch);
         if ((e = ensure_dynamic_smem(tri_inv_leaf, til_smem)) != cudaSuccess) return e;
         if ((e = launch_dependent(tri_inv_leaf, dim3(nleaf, kLeaf / kNB), dim3(256), (size_t)til_smem, st,
                                   reinterpret_cast<const double*>(t.a), lda, (int)(ta == 'N'), (int)upper, na,
