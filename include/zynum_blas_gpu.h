@@ -20,6 +20,7 @@
 #ifndef ZYNUM_BLAS_GPU_H
 #define ZYNUM_BLAS_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -293,6 +294,27 @@ ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrsm_device(char side, char uplo, char tr
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_strsm_device(char side, char uplo, char transa, char diag, int m, int n,
                                                    float alpha, const float *a, int lda, float *b, int ldb,
                                                    void *stream);
+/* Several FP64 solves with one triangular matrix.  The reference has no
+ * counterpart (its trsm, triangular.zig:233, keeps no state between calls):
+ * zynum_blas_gpu_dtrsm_device inverts the diagonal blocks of A on every call;
+ * these two split that work off so that callers solving repeatedly with the
+ * same A (forward and adjoint solves, batches of right-hand sides arriving
+ * one after another) form it once.
+ * dtrsm_inverse_bytes(n): size of the buffer for an n x n A (0 when n <= 0).
+ * dtrsm_inverse_device: inv := the inverses of A's 256-row diagonal blocks
+ *   (uplo, diag as for dtrsm_; A a 16-byte aligned device pointer with an
+ *   even lda, else -cudaErrorInvalidValue; positive returns number the bad
+ *   argument: 1 uplo, 2 diag, 3 n, 5 lda, 6 inv).
+ * dtrsm_with_inverse_device: dtrsm_device with those inverses instead of
+ *   forming them; inv must come from dtrsm_inverse_device on the same A, uplo,
+ *   diag and order (m for side L, n for side R), unchanged since; side and
+ *   transa are free.  Argument numbering as dtrsm_, 12 for inv. */
+ZYNUM_BLAS_GPU_API size_t zynum_blas_gpu_dtrsm_inverse_bytes(int n);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrsm_inverse_device(char uplo, char diag, int n, const double *a, int lda,
+                                                           double *inv, void *stream);
+ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dtrsm_with_inverse_device(char side, char uplo, char transa, char diag, int m,
+                                                                int n, double alpha, const double *a, int lda,
+                                                                double *b, int ldb, const double *inv, void *stream);
 /* SYRK on device pointers: the native GEMM tiles in triangle mode.  Argument numbering as dsyrk_. */
 ZYNUM_BLAS_GPU_API int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alpha, const double *a,
                                                    int lda, double beta, double *c, int ldc, void *stream);

@@ -90,6 +90,58 @@ def test_dtrsm_wide_right_hand_sides(blas, oracle, side, uplo, trans, diag):
     assert np.array_equal(b[m:], b0[m:])
 
 
+@pytest.mark.parametrize("side,uplo,trans,diag", list(itertools.product("LR", "UL", "NT", "NU")))
+@pytest.mark.parametrize("wide", [False, True], ids=["clusters", "wide"])
+def test_dtrsm_with_inverse(blas, oracle, side, uplo, trans, diag, wide):
+    """Diagonal-block inverses formed once (dtrsm_inverse_device) and used by several solves
+    (dtrsm_with_inverse_device): every side / transpose from one set of inverses of A, with
+    three leaves (the last partial) and 45 or 1100 right-hand sides (leaf applies by the cluster
+    kernel or as GEMMs), against the oracle, with B's padding rows untouched."""
+    import torch
+    rng = np.random.default_rng(int.from_bytes((side + uplo + trans + diag + str(wide)).encode(), "little") % 2**32)
+    na, nrhs = 700, (1100 if wide else 45)
+    m, n = (na, nrhs) if side == "L" else (nrhs, na)
+    lda, ldb = na + 2, m + 3  # even lda: the inverses need a 16-byte aligned A
+    a = rng.standard_normal((lda, na)) / np.sqrt(na)
+    for i in range(na):
+        a[i, i] = 2.0 + abs(a[i, i])
+    a[na:] = -999.0
+    a = np.asfortranarray(a)
+    b = np.asfortranarray(rng.standard_normal((ldb, n)))
+    b[m:] = -999.0
+    ref = b.copy(order="F")
+    oracle.trsm(side, uplo, trans, diag, m, n, -1.5, a, lda, ref, ldb)
+    ta = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    inv = torch.empty(blas.dtrsm_inverse_bytes(na) // 8, dtype=torch.float64, device="cuda")
+    blas.dtrsm_inverse_device(uplo, diag, na, ta, lda, inv)
+    for _ in range(2):  # the same inverses serve repeated solves
+        tb = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+        blas.dtrsm_with_inverse_device(side, uplo, trans, diag, m, n, -1.5, ta, lda, tb, ldb, inv)
+        got = np.asfortranarray(tb.cpu().numpy().T)
+        err = np.abs(got[:m] - ref[:m])
+        assert np.all(err <= 1e-11 * (1 + np.abs(ref[:m]))), float(err.max())
+        assert np.array_equal(got[m:], b[m:])
+
+
+def test_dtrsm_inverse_argument_errors(blas):
+    """Bad arguments are numbered; an unaligned A is refused with a message."""
+    import torch
+    L = blas.load()
+    a = torch.eye(64, dtype=torch.float64, device="cuda")
+    inv = torch.empty(blas.dtrsm_inverse_bytes(64) // 8, dtype=torch.float64, device="cuda")
+    assert L.zynum_blas_gpu_dtrsm_inverse_device(b"X", b"N", 64, a.data_ptr(), 64, inv.data_ptr(), None) == 1
+    assert L.zynum_blas_gpu_dtrsm_inverse_device(b"L", b"X", 64, a.data_ptr(), 64, inv.data_ptr(), None) == 2
+    assert L.zynum_blas_gpu_dtrsm_inverse_device(b"L", b"N", -1, a.data_ptr(), 64, inv.data_ptr(), None) == 3
+    assert L.zynum_blas_gpu_dtrsm_inverse_device(b"L", b"N", 64, a.data_ptr(), 32, inv.data_ptr(), None) == 5
+    assert L.zynum_blas_gpu_dtrsm_inverse_device(b"L", b"N", 64, a.data_ptr(), 64, None, None) == 6
+    st = L.zynum_blas_gpu_dtrsm_inverse_device(b"L", b"N", 63, a.data_ptr() + 8, 63, inv.data_ptr(), None)
+    assert st < 0 and b"16-byte aligned" in L.zynum_blas_gpu_last_error()
+    b = torch.zeros((8, 64), dtype=torch.float64, device="cuda")
+    assert L.zynum_blas_gpu_dtrsm_with_inverse_device(b"L", b"L", b"N", b"N", 64, 8, 1.0, a.data_ptr(), 64,
+                                                      b.data_ptr(), 64, None, None) == 12
+    assert blas.dtrsm_inverse_bytes(0) == 0
+
+
 @pytest.mark.parametrize("side,uplo", [("L", "L"), ("R", "U"), ("L", "U"), ("R", "L")])
 def test_strsm_multi_leaf(blas, oracle, side, uplo):
     rng = np.random.default_rng(4)

@@ -70,8 +70,13 @@ def _declare(L: C.CDLL) -> None:
     L.zynum_blas_gpu_strsm_device.argtypes = [ch, ch, ch, ch, i, i, f, P, i, P, i, P]
     L.zynum_blas_gpu_dsyrk_device.argtypes = [ch, ch, i, i, d, P, i, d, P, i, P]
     L.zynum_blas_gpu_ssyrk_device.argtypes = [ch, ch, i, i, f, P, i, f, P, i, P]
+    L.zynum_blas_gpu_dtrsm_inverse_bytes.argtypes = [i]
+    L.zynum_blas_gpu_dtrsm_inverse_bytes.restype = C.c_size_t
+    L.zynum_blas_gpu_dtrsm_inverse_device.argtypes = [ch, ch, i, P, i, P, P]
+    L.zynum_blas_gpu_dtrsm_with_inverse_device.argtypes = [ch, ch, ch, ch, i, i, d, P, i, P, i, P, P]
     for name in ("zynum_blas_gpu_dtrsm_device", "zynum_blas_gpu_strsm_device", "zynum_blas_gpu_dsyrk_device",
-                 "zynum_blas_gpu_ssyrk_device"):
+                 "zynum_blas_gpu_ssyrk_device", "zynum_blas_gpu_dtrsm_inverse_device",
+                 "zynum_blas_gpu_dtrsm_with_inverse_device"):
         getattr(L, name).restype = i
     for name in ("ztrsm_", "ctrsm_"):
         getattr(L, name).argtypes = [cp, cp, cp, cp, I32P, I32P, P, P, I32P, P, I32P]

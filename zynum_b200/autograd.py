@@ -14,6 +14,9 @@ Adjoints (G = upstream gradient):
                                    (strict when the diagonal is unit)
   syrk   C = alpha X^T X (trans)   dX = alpha X (G + G^T)
          C = alpha X X^T           dX = alpha (G + G^T) X
+The inverses of L's diagonal blocks are formed once in the TRSM forward and
+kept for the backward's adjoint solve and recomputation (all three solves use
+the same L; an odd order or an unaligned L forms them per solve instead).
 With recompute=True the TRSM backward solves Y again from (L, B) instead of
 keeping X alive between forward and backward; recompute="auto" (the default of
 trsm()) decides at forward time from the device memory still free: X is
@@ -68,11 +71,26 @@ def rm_gemmt(uplo, alpha, a, b, beta, c, ta=False, tb=False):
     return c
 
 
-def rm_trsm_left(uplo, trans, diag, alpha, l, b):
-    """In place on b (n x r, row-major): b := alpha op(l)^-1 b, l (n x n, row-major) triangular."""
+def rm_trsm_inverse(uplo, diag, l):
+    """The diagonal-block inverses of l (n x n, row-major) for rm_trsm_left, or None where the
+    library forms them per solve (odd n, or l not 16-byte aligned)."""
+    n = l.shape[0]
+    if n % 2 or l.data_ptr() % 16:
+        return None
+    inv = torch.empty(blas.dtrsm_inverse_bytes(n) // 8, dtype=torch.float64, device=l.device)
+    blas.dtrsm_inverse_device(_FLIP[uplo], diag, n, l, n, inv)
+    return inv
+
+
+def rm_trsm_left(uplo, trans, diag, alpha, l, b, inv=None):
+    """In place on b (n x r, row-major): b := alpha op(l)^-1 b, l (n x n, row-major) triangular;
+    inv: l's diagonal-block inverses from rm_trsm_inverse (same uplo and diag), or None."""
     n, r = b.shape
     # column-major: X^T (r x n) = alpha B^T op(L)^-T -> right-side solve with L^T (flipped triangle)
-    blas.dtrsm_device("R", _FLIP[uplo], trans, diag, r, n, alpha, l, n, b, r)
+    if inv is not None:
+        blas.dtrsm_with_inverse_device("R", _FLIP[uplo], trans, diag, r, n, alpha, l, n, b, r, inv)
+    else:
+        blas.dtrsm_device("R", _FLIP[uplo], trans, diag, r, n, alpha, l, n, b, r)
     return b
 
 
@@ -119,11 +137,13 @@ class Trsm(torch.autograd.Function):
     def forward(ctx, l, b, uplo="L", trans="N", diag="N", alpha=1.0, recompute=False):
         l, b = _check(l), _check(b)
         x = b.clone()
-        rm_trsm_left(uplo, trans, diag, alpha, l, x)
+        inv = rm_trsm_inverse(uplo, diag, l)
+        rm_trsm_left(uplo, trans, diag, alpha, l, x, inv)
         if recompute == "auto":
             free, _ = torch.cuda.mem_get_info(x.device)
             recompute = recompute_policy(x.numel() * x.element_size(), free)
         ctx.uplo, ctx.trans, ctx.diag, ctx.alpha, ctx.recompute = uplo, trans, diag, alpha, recompute
+        ctx.inv = inv  # not a differentiable input: kept on ctx for the backward's solves
         if recompute:
             ctx.save_for_backward(l, b)  # X is solved again in backward
         else:
@@ -137,12 +157,12 @@ class Trsm(torch.autograd.Function):
         flip = "T" if ctx.trans == "N" else "N"
         # dB = alpha op(L)^-T G
         db = g.clone()
-        rm_trsm_left(ctx.uplo, flip, ctx.diag, ctx.alpha, l, db)
+        rm_trsm_left(ctx.uplo, flip, ctx.diag, ctx.alpha, l, db, ctx.inv)
         dl = None
         if ctx.needs_input_grad[0]:
             if ctx.recompute:
                 y = saved.clone()
-                rm_trsm_left(ctx.uplo, ctx.trans, ctx.diag, 1.0, l, y)
+                rm_trsm_left(ctx.uplo, ctx.trans, ctx.diag, 1.0, l, y, ctx.inv)
             else:
                 y = saved / ctx.alpha if ctx.alpha != 1.0 else saved
             dl = torch.zeros_like(l)

@@ -290,6 +290,27 @@ def dtrsm_device(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream=N
     return b
 
 
+def dtrsm_inverse_bytes(n):
+    """Bytes of the diagonal-block inverses of an n x n triangular matrix."""
+    return int(load().zynum_blas_gpu_dtrsm_inverse_bytes(n))
+
+
+def dtrsm_inverse_device(uplo, diag, n, a, lda, inv, stream=None):
+    """inv (a device buffer of dtrsm_inverse_bytes(n)) := the inverses of A's diagonal blocks."""
+    st = load().zynum_blas_gpu_dtrsm_inverse_device(_ch(uplo), _ch(diag), n, _ptr(a), lda, _ptr(inv), _stream(stream))
+    check(st, "zynum_blas_gpu_dtrsm_inverse_device")
+    return inv
+
+
+def dtrsm_with_inverse_device(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, inv, stream=None):
+    """dtrsm_device with the inverses dtrsm_inverse_device formed for the same A, uplo and diag."""
+    st = load().zynum_blas_gpu_dtrsm_with_inverse_device(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n,
+                                                         float(alpha), _ptr(a), lda, _ptr(b), ldb, _ptr(inv),
+                                                         _stream(stream))
+    check(st, "zynum_blas_gpu_dtrsm_with_inverse_device")
+    return b
+
+
 def dsyrk_device(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, stream=None):
     st = load().zynum_blas_gpu_dsyrk_device(_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, float(beta),
                                             _ptr(c), ldc, _stream(stream))

@@ -578,7 +578,7 @@ GemmFn<T> gemm_fn(cudaStream_t st, FixedScratch* fs) {
 }
 
 template <typename T, typename Scratch>
-cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
+cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch, const TrsmInverses* given = nullptr) {
     if (t.m <= 0 || t.n <= 0) return cudaSuccess;
     const size_t planes = trsm_plane_bytes<T>(t.side, t.m, t.n);
     // the GEMMs of the recursive solve are at most m x n x (order of A)
@@ -588,7 +588,7 @@ cudaError_t run_trsm(const TrsmArgs<T>& t, cudaStream_t st, Scratch scratch) {
     cudaError_t e = scratch(planes + real, st, &ws);
     if (e != cudaSuccess) return e;
     FixedScratch fs{static_cast<char*>(ws) + planes, real};
-    return trsm<T>(t, ws, gemm_fn<T>(st, &fs), st);
+    return trsm<T>(t, ws, gemm_fn<T>(st, &fs), st, given);
 }
 
 // SYRK / SYR2K in FP64 take the emulated product when the DGEMM method is
@@ -1466,6 +1466,56 @@ int zynum_blas_gpu_dtrsm_device(char side, char uplo, char transa, char diag, in
 int zynum_blas_gpu_strsm_device(char side, char uplo, char transa, char diag, int m, int n, float alpha,
                                 const float* a, int lda, float* b, int ldb, void* stream) {
     return device_trsm<float>("strsm_device", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, stream);
+}
+
+size_t zynum_blas_gpu_dtrsm_inverse_bytes(int n) { return trsm_leaf_inverse_bytes(n); }
+
+int zynum_blas_gpu_dtrsm_inverse_device(char uplo, char diag, int n, const double* a, int lda, double* inv,
+                                        void* stream) {
+    const char ul = up(&uplo), dg = up(&diag);
+    if (!valid_uplo(ul)) return 1;
+    if (!valid_diag(dg)) return 2;
+    if (n < 0) return 3;
+    if (lda < max1(n)) return 5;
+    if (n == 0) return 0;
+    if (!inv) return 6;
+    if (reinterpret_cast<uintptr_t>(a) % 16 != 0 || lda % 2 != 0) {
+        set_last_error("dtrsm_inverse_device: A must be 16-byte aligned with an even lda");
+        return -(int)cudaErrorInvalidValue;
+    }
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void* ws = nullptr;
+    if ((e = cx.stream_scratch(st, trsm_leaf_inverse_scratch_bytes(n), &ws)) != cudaSuccess)
+        return cuda_status(e, "dtrsm_inverse_device");
+    return cuda_status(trsm_leaf_inverses(ul, dg, n, a, lda, ws, inv, st), "dtrsm_inverse_device");
+}
+
+int zynum_blas_gpu_dtrsm_with_inverse_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+                                             const double* a, int lda, double* b, int ldb, const double* inv,
+                                             void* stream) {
+    const char sd = up(&side), ul = up(&uplo), tr = up(&transa), dg = up(&diag);
+    int info = trsm_error(sd, ul, tr, dg, m, n, lda, ldb);
+    if (info) return info;
+    if (m == 0 || n == 0) return 0;
+    if (!inv) return 12;
+    Context& cx = context();
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(cx.mutex);
+        e = cx.init();
+    }
+    if (e != cudaSuccess) return cuda_status(e, "initialisation");
+    const TrsmArgs<double> t{sd, ul, tr, dg, m, n, alpha, a, lda, b, ldb};
+    const TrsmInverses given{inv, tr != 'N'};
+    return cuda_status(run_trsm(t, static_cast<cudaStream_t>(stream), StreamScratch{&cx}, &given),
+                       "dtrsm_with_inverse_device");
 }
 int zynum_blas_gpu_dsyrk_device(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
                                 double beta, double* c, int ldc, void* stream) {

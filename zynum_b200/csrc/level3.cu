@@ -395,8 +395,8 @@ tri_inv_leaf(const double* __restrict__ a, long lda, int trans_n, int upper, int
 // before any CTA writes its rows back.  Warp w: row tile w / 2, column tile
 // w % 2, two accumulators.
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
-trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, int len, double* __restrict__ b,
-                long ldb, int ncols, int wait_first) {
+trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int inv_t, int fwd, int p0, int len,
+                double* __restrict__ b, long ldb, int ncols, int wait_first) {
     extern __shared__ __align__(16) unsigned char ap_smem[];
     double(*Z)[kLeafCols + 1] = reinterpret_cast<double(*)[kLeafCols + 1]>(ap_smem);
     double* A = reinterpret_cast<double*>(ap_smem + sizeof(double) * kLeaf * (kLeafCols + 1));
@@ -407,11 +407,12 @@ trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, 
     const int kbeg = fwd ? 0 : kNB * rb, kend = min(len, fwd ? kNB * (rb + 1) : kLeaf);
     const int klen = max(0, kend - kbeg);
     const int klen8 = (klen + 7) & ~7;
-    // rows 64 rb + i, columns kbeg + kk of inv(M): side L inv[i' + k' kLeaf] (runs along i, staged
-    // [kk][i], pitch 66); side R inv[k' + i' kLeaf] (runs along kk, staged [i][kk], pitch kLeaf + 2)
+    // rows 64 rb + i, columns kbeg + kk of inv(M): stored as is (inv_t = 0) inv[i' + k' kLeaf] (runs
+    // along i, staged [kk][i], pitch 66); stored transposed (inv_t = 1: side R, or an inverse of A
+    // serving op(A) = A^T) inv[k' + i' kLeaf] (runs along kk, staged [i][kk], pitch kLeaf + 2)
     if (wait_first) grid_dependency_wait();  // the kernel before this one wrote the inverses
     if (64 * rb < len && klen > 0) {
-        if (left) {
+        if (!inv_t) {
             for (int q = t; q < klen8 * (kNB / 2); q += 256) {
                 const int kk = q / (kNB / 2), i = (q % (kNB / 2)) * 2;
                 const bool ok = kk < klen;
@@ -462,7 +463,7 @@ trsm_leaf_apply(const double* __restrict__ inv_leaf, int left, int fwd, int p0, 
 #pragma unroll
             for (int v0 = 0; v0 < 2; ++v0) {
                 const int i = 16 * rt + g + 8 * v0, kk = 8 * kb + tq + 4 * v1;
-                af[v0 + 2 * v1] = left ? A[kk * kStagePitch + i] : A[i * (kLeaf + 2) + kk];
+                af[v0 + 2 * v1] = !inv_t ? A[kk * kStagePitch + i] : A[i * (kLeaf + 2) + kk];
             }
 #pragma unroll
         for (int v = 0; v < 2; ++v) bf[v] = Z[kbeg + 8 * kb + tq + 4 * v][8 * ct + g];
@@ -764,7 +765,8 @@ size_t trsm_plane_bytes(char side, int m, int n) {
 }
 
 template <typename T>
-cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st) {
+cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st,
+                 const TrsmInverses* given) {
     const int m = t.m, n = t.n;
     if (m <= 0 || n <= 0) return cudaSuccess;
     cudaError_t e;
@@ -776,13 +778,18 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     const int na = left ? m : n;
     const int nblk = (na + kNB - 1) / kNB;
     T* inv = static_cast<T*>(planes);
-    const int tri_smem = (2 * kNB * (kNB + 1) + kNB) * (int)sizeof(T);
-    if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) != cudaSuccess) return e;
-    if ((e = launch_dependent(tri_inv_blocks<T>, dim3(nblk), dim3(256), (size_t)tri_smem, st, t.a, t.lda, t.uplo,
-                              t.trans, t.diag, na, inv)) != cudaSuccess)
-        return e;
-    count_launch();
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // inverses of the diagonal blocks given by the caller (FP64): none are formed here
+    const bool have_given = given != nullptr && std::is_same<T, double>::value;
+    const bool given_t = have_given && given->transposed;
+    if (!have_given) {
+        const int tri_smem = (2 * kNB * (kNB + 1) + kNB) * (int)sizeof(T);
+        if ((e = ensure_dynamic_smem(tri_inv_blocks<T>, tri_smem)) != cudaSuccess) return e;
+        if ((e = launch_dependent(tri_inv_blocks<T>, dim3(nblk), dim3(256), (size_t)tri_smem, st, t.a, t.lda, t.uplo,
+                                  t.trans, t.diag, na, inv)) != cudaSuccess)
+            return e;
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     const bool upper = op_is_upper(t.uplo, t.trans);
     // the GEMM operand op(A): complex keeps C (conjugate transpose), real reads C as T
     const char ta = (t.trans == 'N') ? 'N' : (is_cnum<T>::value ? t.trans : 'T');
@@ -797,20 +804,29 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     // over the right-hand sides, in place.  FP64 with a 16-byte aligned A and an
     // even lda (16-byte operand copies) applies precomputed leaf inverses on
     // the tensor pipe; otherwise trsm_leaf solves phase by phase.
-    const bool inv_leaves =
-        std::is_same<T, double>::value && reinterpret_cast<uintptr_t>(t.a) % 16 == 0 && t.lda % 2 == 0;
+    const bool inv_leaves = have_given || (std::is_same<T, double>::value &&
+                                           reinterpret_cast<uintptr_t>(t.a) % 16 == 0 && t.lda % 2 == 0);
     const int ncols = left ? n : m;
     const int fwd = left ? !upper : upper;
+    // the leaf's M is op(A)'s block (side L) or its transpose (side R); inverses of
+    // op(A) are stored as is, given inverses of A serving op(A) = A^T transposed
+    const int inv_t = left ? (int)given_t : (int)!given_t;
     int leaf_smem;
-    double* inv_leaf = nullptr;
-    if (inv_leaves) {
+    const double* inv_leaf = nullptr;
+    if (inv_leaves && have_given) {
+        inv_leaf = given->leaf;
+        constexpr int kRows = kLeaf * kStagePitch > kNB * (kLeaf + 2) ? kLeaf * kStagePitch : kNB * (kLeaf + 2);
+        leaf_smem = (int)sizeof(double) * (kLeaf * (kLeafCols + 1) + kRows);
+        e = ensure_dynamic_smem(trsm_leaf_apply, leaf_smem);
+    } else if (inv_leaves) {
         const int nleaf = (na + kLeaf - 1) / kLeaf;
-        inv_leaf = reinterpret_cast<double*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na));
+        double* built = reinterpret_cast<double*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na));
+        inv_leaf = built;
         const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + 2 * kNB * kStagePitch);
         if ((e = ensure_dynamic_smem(tri_inv_leaf, til_smem)) != cudaSuccess) return e;
         if ((e = launch_dependent(tri_inv_leaf, dim3(nleaf, kLeaf / kNB), dim3(256), (size_t)til_smem, st,
                                   reinterpret_cast<const double*>(t.a), lda, (int)(ta == 'N'), (int)upper, na,
-                                  reinterpret_cast<const double*>(inv), inv_leaf)) != cudaSuccess)
+                                  reinterpret_cast<const double*>(inv), built)) != cudaSuccess)
             return e;
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -831,6 +847,7 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
             const int grid = (ncols + kLeafCols - 1) / kLeafCols;
             if (inv_leaves && ncols > kApplyMaxCols) {  // copy of the leaf's rows / columns, then one GEMM
                 const T* il = reinterpret_cast<const T*>(inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf);
+                const char il_t = given_t ? 'T' : 'N';  // the leaf inverse of op(A) is the given one transposed
                 T* W = reinterpret_cast<T*>(static_cast<char*>(planes) + inv_plane_bytes<T>(na) +
                                             leaf_plane_bytes<T>(na));
                 if (left) {
@@ -838,12 +855,12 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
                                                  (size_t)len * sizeof(T), n, cudaMemcpyDeviceToDevice, st)) !=
                         cudaSuccess)
                         return err;
-                    return gemm({'N', 'N', len, n, len, T(1), il, kLeaf, W, len, T(0), t.b + p0, ldb});
+                    return gemm({il_t, 'N', len, n, len, T(1), il, kLeaf, W, len, T(0), t.b + p0, ldb});
                 }
                 if ((err = cudaMemcpy2DAsync(W, (size_t)m * sizeof(T), t.b + (long)p0 * ldb, ldb * sizeof(T),
                                              (size_t)m * sizeof(T), len, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
                     return err;
-                return gemm({'N', 'N', m, len, len, T(1), W, m, il, kLeaf, T(0), t.b + (long)p0 * ldb, ldb});
+                return gemm({'N', il_t, m, len, len, T(1), W, m, il, kLeaf, T(0), t.b + (long)p0 * ldb, ldb});
             }
             if (inv_leaves) {  // clusters of four CTAs per 16 right-hand sides
                 const double* il = inv_leaf + (long)(p0 / kLeaf) * kLeaf * kLeaf;
@@ -851,8 +868,8 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
                 // every leaf after the first follows a coupling product (or its reduction),
                 // which does not write the inverses: it stages them during that kernel's
                 // tail; the first follows tri_inv_leaf and waits before staging
-                err = launch_dependent(trsm_leaf_apply, dim3(4 * grid), dim3(256), (size_t)leaf_smem, st, il, left, fwd,
-                                       p0, len, bd, ldb, ncols, (int)first_leaf);
+                err = launch_dependent(trsm_leaf_apply, dim3(4 * grid), dim3(256), (size_t)leaf_smem, st, il, left, inv_t,
+                                       fwd, p0, len, bd, ldb, ncols, (int)first_leaf);
                 first_leaf = false;
                 count_launch();
                 if (err != cudaSuccess) return err;
@@ -897,6 +914,31 @@ cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cuda
     return cudaGetLastError();
 }
 
+size_t trsm_leaf_inverse_bytes(int n) { return n > 0 ? leaf_plane_bytes<double>(n) : 0; }
+size_t trsm_leaf_inverse_scratch_bytes(int n) { return n > 0 ? inv_plane_bytes<double>(n) : 0; }
+
+cudaError_t trsm_leaf_inverses(char uplo, char diag, int n, const double* a, long lda, void* scratch, double* leaf,
+                               cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (reinterpret_cast<uintptr_t>(a) % 16 != 0 || lda % 2 != 0) return cudaErrorInvalidValue;
+    cudaError_t e;
+    double* inv = static_cast<double*>(scratch);
+    const int nblk = (n + kNB - 1) / kNB, nleaf = (n + kLeaf - 1) / kLeaf;
+    const int tri_smem = (2 * kNB * (kNB + 1) + kNB) * (int)sizeof(double);
+    if ((e = ensure_dynamic_smem(tri_inv_blocks<double>, tri_smem)) != cudaSuccess) return e;
+    if ((e = launch_dependent(tri_inv_blocks<double>, dim3(nblk), dim3(256), (size_t)tri_smem, st, a, lda, uplo, 'N',
+                              diag, n, inv)) != cudaSuccess)
+        return e;
+    count_launch();
+    const int til_smem = (int)sizeof(double) * (4 * kNB * (kNB + 1) + 2 * kNB * kStagePitch);
+    if ((e = ensure_dynamic_smem(tri_inv_leaf, til_smem)) != cudaSuccess) return e;
+    if ((e = launch_dependent(tri_inv_leaf, dim3(nleaf, kLeaf / kNB), dim3(256), (size_t)til_smem, st, a, lda, 1,
+                              (int)(uplo == 'U'), n, (const double*)inv, leaf)) != cudaSuccess)
+        return e;
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t syrk_scale_only(int n, char uplo, T beta, T* c, long ldc, cudaStream_t st) {
     scale_triangle<T><<<grid_for((long)n * n), 256, 0, st>>>(n, uplo == 'U' ? 1 : 2, beta, c, ldc);
@@ -906,14 +948,16 @@ cudaError_t syrk_scale_only(int n, char uplo, T beta, T* c, long ldc, cudaStream
 
 template size_t trsm_plane_bytes<double>(char, int, int);
 template size_t trsm_plane_bytes<float>(char, int, int);
-template cudaError_t trsm<double>(const TrsmArgs<double>&, void*, const GemmFn<double>&, cudaStream_t);
-template cudaError_t trsm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t);
+template cudaError_t trsm<double>(const TrsmArgs<double>&, void*, const GemmFn<double>&, cudaStream_t,
+                                  const TrsmInverses*);
+template cudaError_t trsm<float>(const TrsmArgs<float>&, void*, const GemmFn<float>&, cudaStream_t,
+                                 const TrsmInverses*);
 template size_t trsm_plane_bytes<cnum<double>>(char, int, int);
 template size_t trsm_plane_bytes<cnum<float>>(char, int, int);
 template cudaError_t trsm<cnum<double>>(const TrsmArgs<cnum<double>>&, void*, const GemmFn<cnum<double>>&,
-                                        cudaStream_t);
+                                        cudaStream_t, const TrsmInverses*);
 template cudaError_t trsm<cnum<float>>(const TrsmArgs<cnum<float>>&, void*, const GemmFn<cnum<float>>&,
-                                       cudaStream_t);
+                                       cudaStream_t, const TrsmInverses*);
 template cudaError_t syrk_scale_only<cnum<double>>(int, char, cnum<double>, cnum<double>*, long, cudaStream_t);
 template cudaError_t syrk_scale_only<cnum<float>>(int, char, cnum<float>, cnum<float>*, long, cudaStream_t);
 template cudaError_t syrk_scale_only<double>(int, char, double, double*, long, cudaStream_t);

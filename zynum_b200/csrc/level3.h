@@ -31,8 +31,27 @@ using GemmFn = std::function<cudaError_t(const GemmArgs<T>&)>;
 template <typename T>
 size_t trsm_plane_bytes(char side, int m, int n);
 
+// Inverses of the 256-row diagonal blocks of an FP64 triangular A (op = N),
+// computed once for several solves with the same A (trsm_leaf_inverses); a
+// solve with op(A) = A^T reads them transposed.
+struct TrsmInverses {
+    const double* leaf;  // leaf b at leaf + b 256^2, column-major, ld 256, zero outside the triangle
+    bool transposed;     // the solve's op(A) is A^T
+};
+
+// given: precomputed inverses (FP64 only); the diagonal blocks are then not inverted again.
 template <typename T>
-cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st);
+cudaError_t trsm(const TrsmArgs<T>& t, void* planes, const GemmFn<T>& gemm, cudaStream_t st,
+                 const TrsmInverses* given = nullptr);
+
+// Bytes of the inverses of an n x n triangular matrix's 256-row diagonal blocks,
+// and the scratch (the 64-block inverses) forming them takes.
+size_t trsm_leaf_inverse_bytes(int n);
+size_t trsm_leaf_inverse_scratch_bytes(int n);
+// leaf := the inverses of the 256-row diagonal blocks of A (uplo, diag; op = N)
+// for trsm's `given`; A 16-byte aligned with an even lda.
+cudaError_t trsm_leaf_inverses(char uplo, char diag, int n, const double* a, long lda, void* scratch, double* leaf,
+                               cudaStream_t st);
 
 // Device scratch SYMM needs besides its GEMM's scratch: the dense symmetric copy of A.
 template <typename T>
