@@ -18,7 +18,8 @@ The inverses of L's diagonal blocks are formed once in the TRSM forward and
 kept for the backward's adjoint solve and recomputation (all three solves use
 the same L; an odd order or an unaligned L forms them per solve instead).
 With recompute=True the TRSM backward solves Y again from (L, B) instead of
-keeping X alive between forward and backward; recompute="auto" (the default of
+keeping X alive between forward and backward, on a second stream beside the
+adjoint solve; recompute="auto" (the default of
 trsm()) decides at forward time from the device memory still free: X is
 recomputed when keeping it until backward would take more than
 RECOMPUTE_FRACTION of the free bytes (recompute_policy).
@@ -69,6 +70,17 @@ def rm_gemmt(uplo, alpha, a, b, beta, c, ta=False, tb=False):
         b.shape[1], a.data_ptr(), a.shape[1], float(beta), c.data_ptr(), n, blas._stream(None))
     blas.check(st, "zynum_blas_gpu_dgemmt_device")
     return c
+
+
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device):
+    """One extra stream per device for work that overlaps the current stream's."""
+    key = torch.device(device).index
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(device=device)
+    return _SIDE_STREAMS[key]
 
 
 def rm_trsm_inverse(uplo, diag, l):
@@ -157,13 +169,24 @@ class Trsm(torch.autograd.Function):
         flip = "T" if ctx.trans == "N" else "N"
         # dB = alpha op(L)^-T G
         db = g.clone()
-        rm_trsm_left(ctx.uplo, flip, ctx.diag, ctx.alpha, l, db, ctx.inv)
         dl = None
-        if ctx.needs_input_grad[0]:
-            if ctx.recompute:
-                y = saved.clone()
+        if ctx.needs_input_grad[0] and ctx.recompute:
+            # Y = op(L)^-1 B and dB are independent solves, each a latency-bound
+            # chain of small kernels: Y runs on a second stream beside dB.  Y is
+            # allocated on this stream, which waits for the second one before it
+            # (or any later kernel) touches Y.
+            y = saved.clone()
+            cur = torch.cuda.current_stream(y.device)
+            side = _side_stream(y.device)
+            side.wait_stream(cur)
+            with torch.cuda.stream(side):
                 rm_trsm_left(ctx.uplo, ctx.trans, ctx.diag, 1.0, l, y, ctx.inv)
-            else:
+            rm_trsm_left(ctx.uplo, flip, ctx.diag, ctx.alpha, l, db, ctx.inv)
+            cur.wait_stream(side)
+        else:
+            rm_trsm_left(ctx.uplo, flip, ctx.diag, ctx.alpha, l, db, ctx.inv)
+        if ctx.needs_input_grad[0]:
+            if not ctx.recompute:
                 y = saved / ctx.alpha if ctx.alpha != 1.0 else saved
             dl = torch.zeros_like(l)
             if ctx.trans == "N":
