@@ -211,12 +211,11 @@ class Syrk(torch.autograd.Function):
         (x,) = ctx.saved_tensors
         g = g.contiguous()
         dx = torch.empty_like(x)
+        s = g + g.t()  # G + G^T (n x n, small): one product instead of two
         if ctx.trans_first:   # dX = alpha X (G + G^T)
-            rm_gemm(ctx.alpha, x, g, 0.0, dx)
-            rm_gemm(ctx.alpha, x, g, 1.0, dx, tb=True)
+            rm_gemm(ctx.alpha, x, s, 0.0, dx)
         else:                 # dX = alpha (G + G^T) X
-            rm_gemm(ctx.alpha, g, x, 0.0, dx)
-            rm_gemm(ctx.alpha, g, x, 1.0, dx, ta=True)
+            rm_gemm(ctx.alpha, s, x, 0.0, dx)
         return dx, None, None
 
 
